@@ -1,0 +1,285 @@
+/*
+ * prism_b200.h -- C ABI of the B200 (sm_100a) collision-kinematics substrate.
+ *
+ * This is the drop-in boundary for PrismPlan's shared collision-kinematics
+ * path (code/gpu_planning/cpp/src/planning/robot_model.cuh,
+ * runtime_kinematics.cuh, code/gpu_planning/cpp/src/collision/
+ * scene_collision*.{cuh,hh}, two_phase_cc.cuh and the kernels that wrap them).
+ *
+ * Conventions
+ *   - Every entry point returns an int status (PS_OK on success). On failure
+ *     ps_last_error() returns a thread-local, human-readable message. No
+ *     exception crosses this boundary and nothing calls exit().
+ *   - Pointers documented as "device" are CUDA global-memory pointers owned by
+ *     the caller. Pointers documented as "host" are plain host memory.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *     Every compute call is asynchronous on that stream, allocates nothing and
+ *     never synchronises, so it can be captured into a CUDA graph.
+ *   - Calls on distinct streams are thread-safe: kernels use no mutable
+ *     __device__ globals; all state lives in caller-owned buffers or in the
+ *     immutable model object.
+ *   - Joint type codes are the reference's (utils.cuh:20-26).
+ */
+#ifndef PRISM_B200_H
+#define PRISM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define PS_OK        0
+#define PS_EINVAL    1   /* bad argument, shape or capacity               */
+#define PS_ENOMEM    2   /* device or host allocation failed (create only) */
+#define PS_ECUDA     3   /* a CUDA runtime call or kernel launch failed    */
+#define PS_ETIMEOUT  4   /* a bounded device-side wait gave up             */
+
+/* ---- joint types (utils.cuh:20-26) ---------------------------------------- */
+#define PS_FIXED   (-1)
+#define PS_X_PRISM   0
+#define PS_Y_PRISM   1
+#define PS_Z_PRISM   2
+#define PS_X_ROT     3
+#define PS_Y_ROT     4
+#define PS_Z_ROT     5
+
+/* ---- limits --------------------------------------------------------------- */
+#define PS_MAX_DOF       14    /* robot_model.cuh:14 (MAX_DIM)              */
+#define PS_MAX_JOINTS    20    /* joint_in_collision has 20 slots per config
+                                  (two_phase_cc.cuh:72, scene_collision.cuh:535) */
+#define PS_MAX_SPHERES   512
+#define PS_MAX_OBBS      1024
+#define PS_MAX_LAYERS    8
+
+/* Last error message of the calling thread ("" if none). */
+const char* ps_last_error(void);
+
+/* Library version string. */
+const char* ps_version(void);
+
+/* =========================================================================
+ * Robot model
+ * Replaces ppln::RobotModelDevice::create / destroy
+ * (cpp/src/planning/robot_model.cuh:91-293) and the pybind
+ * RobotModelBuilder::build_on_device / update_joint_limits / destroy
+ * (cpp/src/python/bindings.cpp:118-225). Field meanings are the builder's.
+ * ========================================================================= */
+typedef struct ps_model_desc {
+    int          n_dof;
+    int          n_joints;
+    const float* fixed_transforms;        /* host [n_joints*16], row-major 4x4 */
+    const int*   joint_types;             /* host [n_joints]                   */
+    int          n_spheres;
+    const float* spheres;                 /* host [n_spheres*4] (x,y,z,r), link frame */
+    const int*   sphere_to_joint;         /* host [n_spheres]                  */
+    int          n_self_cc_ranges;
+    const int*   self_cc_ranges;          /* host [n*3] {sphere_i, start, end}, end inclusive */
+    int          n_approx_spheres;
+    const float* approx_spheres;          /* host [n_approx*4]                 */
+    const int*   approx_sphere_to_joint;  /* host [n_approx]                   */
+    int          n_approx_self_cc_ranges;
+    const int*   approx_self_cc_ranges;   /* host [n*3]                        */
+    const float* approx_fixed_transforms; /* host [n_joints*16] or NULL = same as full */
+    const int*   approx_joint_types;      /* host [n_joints]    or NULL = same as full */
+    const float* joint_lower;             /* host [n_dof]                      */
+    const float* joint_upper;             /* host [n_dof]                      */
+    /* Kinematic tree; any NULL array takes the serial-chain default
+       (robot_model.cuh:204-236). */
+    const int*   joint_parents;           /* host [n_joints] or NULL */
+    const int*   joint_id_to_dof;         /* host [n_joints] or NULL */
+    const int*   t_memory_idx;            /* host [n_joints] or NULL */
+    const int*   dfs_order;               /* host [n_joints] or NULL */
+} ps_model_desc;
+
+typedef struct ps_model ps_model;
+
+typedef struct ps_model_info {
+    int n_dof, n_joints, n_spheres, n_approx_spheres;
+    int n_self_pairs, n_approx_self_pairs;   /* expanded (i,j) pair counts */
+    int n_t_slots;
+    int approx_shares_chain;                 /* 1: approx FK == full FK    */
+    int device;                              /* CUDA ordinal of the upload */
+    size_t device_bytes;                     /* bytes of the device blob   */
+} ps_model_info;
+
+/* Validates the descriptor, builds the kernel layout on the host and uploads
+   it (one allocation, one copy) to the current CUDA device. Synchronous. */
+int ps_model_create(const ps_model_desc* desc, ps_model** out);
+/* Frees the device blob. Safe on NULL. */
+int ps_model_destroy(ps_model* model);
+/* Re-uploads joint limits (and the derived range) without a rebuild
+   (bindings.cpp:175-205). Host arrays of n_dof floats. Synchronous. */
+int ps_model_set_limits(ps_model* model, const float* lower, const float* upper);
+int ps_model_get_info(const ps_model* model, ps_model_info* info);
+/* Reads and clears the model's device error latch (synchronous): *code is
+   PS_OK, or PS_ETIMEOUT when a kernel using this model gave up a bounded
+   wait since the last poll (its outputs for that launch are incomplete).
+   Replaces the reference's cudaCheckError -> exit() (utils.cuh:433-439). */
+int ps_model_poll_status(ps_model* model, int* code);
+
+/* =========================================================================
+ * Scene view: non-owning device pointers in the exact layout of
+ * ppln::collision::SceneCollisionData (cpp/src/collision/scene_collision_data.hh:10-47),
+ * i.e. what prrtc.SceneCollisionDataBuilder::build() produces
+ * (cpp/src/python/bindings.cpp:363-402). Nothing is copied at bind time.
+ * ========================================================================= */
+#define PS_ESDF_NEAREST    0   /* reference lookup (scene_collision.cuh:202-331) */
+#define PS_ESDF_TRILINEAR  1   /* trilinear sampling (new; no reference counterpart) */
+
+typedef struct ps_scene_view {
+    const float*   obb_dims;        /* device [n_obbs*4]  dx,dy,dz,pad (full extents) */
+    const float*   obb_pose;        /* device [n_obbs*8]  inverse pose t,qw,qx,qy,qz,pad */
+    const uint8_t* obb_enable;      /* device [n_obbs]    0/1 */
+    int            n_obbs;
+    const float*   voxel_params;    /* device [L*4] dx,dy,dz,voxel_size */
+    const float*   voxel_pose;      /* device [L*8] inverse pose */
+    const uint8_t* voxel_enable;    /* device [L] */
+    const float*   voxel_features;  /* device [L*max_voxels_per_layer], positive = inside */
+    int            n_voxel_layers;
+    int            max_voxels_per_layer;
+    const uint8_t* sphere_acm_mask;             /* device [n_spheres*L] or NULL */
+    const uint8_t* sphere_obb_acm_mask;         /* device [n_spheres*n_obbs] or NULL */
+    const uint8_t* sphere_obb_acm_mask_approx;  /* device [n_approx*n_obbs] or NULL */
+    int            esdf_mode;       /* PS_ESDF_NEAREST or PS_ESDF_TRILINEAR */
+} ps_scene_view;
+
+/* =========================================================================
+ * Batched configuration check (config-major, one lane per configuration).
+ * Replaces pRRTC::check_collision_scene + check_collision_scene_kernel
+ * (cpp/src/planning/pRRTC.cu:2337-2423) and prrtc.check_collision_scene
+ * (cpp/src/python/bindings.cpp:493-532). The verdict is the two-phase one of
+ * two_phase_cc (cpp/src/collision/two_phase_cc.cuh:57-138): approximate
+ * spheres gate, per joint, the exact sphere tests.
+ * ========================================================================= */
+#define PS_CHECK_SELF       0x01u  /* also run the two-phase self check        */
+#define PS_CLEARANCE_OBB    0x02u  /* clearance includes sphere-OBB SDF         */
+#define PS_CLEARANCE_ESDF   0x04u  /* clearance includes ESDF (reference a13)   */
+#define PS_NO_GATE          0x08u  /* skip the approximate gate (diagnostics)   */
+
+/* q: device [n*n_dof] row-major. hit: device [n] (1 = in collision).
+   clearance: device [n] or NULL; min over spheres (radius + margin) of the
+   selected clearance sources, 1000.0 when nothing is in range. */
+int ps_check_configs(const ps_model* model, const ps_scene_view* scene,
+                     const float* q, int n, float collision_margin,
+                     unsigned flags, uint8_t* hit, float* clearance,
+                     void* stream);
+
+/* =========================================================================
+ * Edge checks. Replaces ppln::search::evaluate_edges_batch and
+ * EdgeEvalGpu::evaluate (cpp/src/planning/edge_eval.cuh:37-165,
+ * cpp/src/planning/edge_batch_bridge.hh:60-96). Samples sit at t = j/G,
+ * j = 1..G (the start configuration is not checked, edge_eval.cuh:110-121).
+ * Outputs: valid[e] (1 = free), cost[e] = L2 length if valid else FLT_MAX,
+ * clearance[e] = min ESDF clearance over the samples (only when requested;
+ * FLT_MAX otherwise), exactly as edge_eval.cuh:157-164.
+ * ========================================================================= */
+typedef struct ps_edge_params {
+    int   granularity;      /* G for every edge when samples_per_edge is NULL
+                               and both rules below are off (edge_eval.cuh:38) */
+    float resolution;       /* > 0: G = clamp(ceil(L2/resolution), 2, 1024)
+                               (edge_eval.cuh:54-60)                            */
+    float max_joint_step;   /* > 0: G = clamp(ceil(Linf/step), 1, max_samples) */
+    int   max_samples;      /* clamp for the L-inf rule; <= 0 means 1024        */
+    float collision_margin; /* added to every radius (edge_eval.cuh:39)         */
+    int   check_self;       /* also run the self check (edge_eval.cuh:40)       */
+    int   compute_clearance;/* ESDF min clearance over samples (edge_eval.cuh:41) */
+} ps_edge_params;
+
+/* Plain per-call path: one warp per edge, samples in order, early exit at the
+   first colliding sample. samples_per_edge: device [n_edges] or NULL. */
+int ps_check_edges_plain(const ps_model* model, const ps_scene_view* scene,
+                         const float* from, const float* to,
+                         const int* samples_per_edge, int n_edges,
+                         const ps_edge_params* params,
+                         uint8_t* valid, float* cost, float* clearance,
+                         void* stream);
+
+/* Device workspace the persistent edge path needs (caller allocates). */
+size_t ps_edges_workspace_bytes(int n_edges);
+
+/* Persistent work-queue path: edges are cut into warp-sized sample chunks,
+   ordered chunk-major and pulled from a global queue by a persistent grid;
+   an edge found in collision retires its remaining chunks. All launches are
+   capture-safe. workspace: device, >= ps_edges_workspace_bytes(n_edges). */
+int ps_check_edges(const ps_model* model, const ps_scene_view* scene,
+                   const float* from, const float* to,
+                   const int* samples_per_edge, int n_edges,
+                   const ps_edge_params* params,
+                   uint8_t* valid, float* cost, float* clearance,
+                   void* workspace, size_t workspace_bytes, void* stream);
+
+/* =========================================================================
+ * Trajectory cost: summed hinge + self hinge + smoothness, with its exact
+ * gradient from a hand-written adjoint.
+ * Forward cost replaces chomp_state_cost_kernel / stomp_state_cost_kernel
+ * (cpp/src/planning/chomp.cu:151-188, cpp/src/planning/stomp.cu:206-245) over
+ * scene_sum_{esdf,obb}_hinge_runtime + self_min_hinge_runtime
+ * (cpp/src/collision/scene_collision.cuh:394-495,
+ * cpp/src/planning/runtime_kinematics.cuh:295-330); the gradient replaces the
+ * central-difference chomp_obs_grad_kernel (cpp/src/planning/chomp.cu:83-144);
+ * the smoothness term replaces chomp_control_cost_kernel
+ * (cpp/src/planning/chomp.cu:196-210) with R from
+ * cpp/src/planning/chomp_precompute.cpp:20-37 applied as a banded stencil.
+ * ========================================================================= */
+#define PS_LAYOUT_BTD  0   /* q[b][t][d]  (torch-natural)                        */
+#define PS_LAYOUT_BDT  1   /* q[b][d][t]  (reference theta[d*T+t], rollouts[(r*D+d)*T+t]) */
+
+typedef struct ps_cost_params {
+    float collision_cost_weight; /* w (CHOMP_settings.hh:35)                     */
+    float world_margin;          /* hinge band eps (CHOMP_settings.hh:42)        */
+    float self_margin;           /* self hinge band (CHOMP_settings.hh:43)       */
+    int   include_self;          /* add self_min_hinge                            */
+    float smoothness_weight;     /* lambda on theta^T R theta; 0 = off            */
+    float delta_t;               /* R time step (CHOMP_settings.hh:46)            */
+    int   layout;                /* PS_LAYOUT_BTD or PS_LAYOUT_BDT                */
+} ps_cost_params;
+
+/* q: device [B*T*D] in `layout`. Outputs (each device, NULL to skip):
+     waypoint_cost [B*T]  = w * (sum esdf hinge + sum obb hinge + self hinge)
+     traj_cost     [B]    = sum_t waypoint_cost + lambda * sum_d theta_d^T R theta_d
+     grad          [B*T*D] in `layout` = d traj_cost / d q (exact adjoint).
+   The collision hinge uses the full sphere set without the approximate gate,
+   as the reference cost kernels do. */
+int ps_traj_cost(const ps_model* model, const ps_scene_view* scene,
+                 const float* q, int B, int T, const ps_cost_params* params,
+                 float* waypoint_cost, float* traj_cost, float* grad,
+                 void* stream);
+
+/* STOMP rollout costs: per (rollout, waypoint) state cost over
+   rollouts device [n_rows*D*T] (PS_LAYOUT_BDT, the reference layout) or
+   [n_rows*T*D] (PS_LAYOUT_BTD). state_cost: device [n_rows*T]; when
+   broadcast_d != 0 it is [n_rows*D*T] with the value repeated over d, as
+   stomp_state_cost_kernel writes it (stomp.cu:241-244). */
+int ps_rollout_costs(const ps_model* model, const ps_scene_view* scene,
+                     const float* rollouts, int n_rows, int T,
+                     const ps_cost_params* params, int broadcast_d,
+                     float* state_cost, void* stream);
+
+/* =========================================================================
+ * Diagnostics
+ * ========================================================================= */
+/* World-frame sphere centres for n configurations (device out [n*n_spheres*3],
+   sphere order as in the descriptor). Same arithmetic as the checks. */
+int ps_fk_spheres(const ps_model* model, const float* q, int n,
+                  float* sphere_xyz, void* stream);
+
+/* FP32 FMA throughput probe used as the roofline denominator: 8 independent
+   FMA chains per thread on every SM; returns FLOP/s (host). Synchronous; the
+   only entry point besides ps_model_create that allocates (4 bytes). */
+int ps_probe_fp32_peak(double* flops_per_s, void* stream);
+
+/* Executed-work counters for roofline accounting: when dev_counters (device,
+   8 x uint64) is non-NULL, every later launch adds [pair tests, exact
+   re-decisions, samples, FK joint steps, sphere transforms, self pairs, ESDF
+   lookups, broad-phase box tests]. Process-wide, not thread-safe; NULL
+   (the default) disables counting. No reference counterpart. */
+int ps_set_stats(unsigned long long* dev_counters);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PRISM_B200_H */

@@ -1,0 +1,27 @@
+"""B200-native (sm_100a) collision-kinematics substrate for PrismPlan's planners.
+
+Drop-in surface (names of the reference ``prrtc`` module and substrate):
+``RobotModelBuilder``, ``SceneCollisionDataBuilder``, ``PlanningScene``,
+``check_collision_scene``, ``EdgeEvalGpu``, ``load_robot_asset``,
+``build_robot_model``; device-resident torch ops ``check_configs``,
+``check_edges``, ``traj_cost``, ``rollout_costs``, ``hinge_cost``.
+The compute path is the CUDA library ``libprism_b200.so``; importing this
+package does not load it (so CPU-only tooling works), the first call does and
+fails loudly if it is missing.
+"""
+from ._lib import PrismError  # noqa: F401
+from .api import (  # noqa: F401
+    CostParams,
+    EdgeEvalGpu,
+    EdgeEvalParams,
+    check_collision_scene,
+    check_configs,
+    check_edges,
+    edges_workspace,
+    fk_spheres,
+    hinge_cost,
+    rollout_costs,
+    traj_cost,
+)
+from .robot import RobotModelBuilder, build_robot_model, load_robot_asset  # noqa: F401
+from .scene import PlanningScene, SceneCollisionDataBuilder, SceneTensors  # noqa: F401

@@ -1,0 +1,177 @@
+"""ctypes binding of the C ABI declared in include/prism_b200.h.
+
+The product path has exactly one implementation: the sm_100a CUDA library
+``prismplan_b200/libprism_b200.so``. If it is missing or fails to load, every
+entry point raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libprism_b200.so"
+
+PS_OK, PS_EINVAL, PS_ENOMEM, PS_ECUDA, PS_ETIMEOUT = 0, 1, 2, 3, 4
+_STATUS_NAMES = {1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "ETIMEOUT"}
+
+PS_CHECK_SELF = 0x01
+PS_CLEARANCE_OBB = 0x02
+PS_CLEARANCE_ESDF = 0x04
+PS_NO_GATE = 0x08
+
+PS_ESDF_NEAREST = 0
+PS_ESDF_TRILINEAR = 1
+PS_LAYOUT_BTD = 0
+PS_LAYOUT_BDT = 1
+
+PS_MAX_DOF = 14
+PS_MAX_JOINTS = 20
+
+
+class PrismError(RuntimeError):
+    """A C-ABI call returned a non-OK status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{_STATUS_NAMES.get(status, status)}] {message}")
+        self.status = status
+
+
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class ModelDesc(C.Structure):
+    """ps_model_desc (host arrays)."""
+
+    _fields_ = [
+        ("n_dof", C.c_int), ("n_joints", C.c_int),
+        ("fixed_transforms", _fp), ("joint_types", _ip),
+        ("n_spheres", C.c_int), ("spheres", _fp), ("sphere_to_joint", _ip),
+        ("n_self_cc_ranges", C.c_int), ("self_cc_ranges", _ip),
+        ("n_approx_spheres", C.c_int), ("approx_spheres", _fp),
+        ("approx_sphere_to_joint", _ip),
+        ("n_approx_self_cc_ranges", C.c_int), ("approx_self_cc_ranges", _ip),
+        ("approx_fixed_transforms", _fp), ("approx_joint_types", _ip),
+        ("joint_lower", _fp), ("joint_upper", _fp),
+        ("joint_parents", _ip), ("joint_id_to_dof", _ip),
+        ("t_memory_idx", _ip), ("dfs_order", _ip),
+    ]
+
+
+class ModelInfo(C.Structure):
+    _fields_ = [
+        ("n_dof", C.c_int), ("n_joints", C.c_int), ("n_spheres", C.c_int),
+        ("n_approx_spheres", C.c_int), ("n_self_pairs", C.c_int),
+        ("n_approx_self_pairs", C.c_int), ("n_t_slots", C.c_int),
+        ("approx_shares_chain", C.c_int), ("device", C.c_int),
+        ("device_bytes", C.c_size_t),
+    ]
+
+
+class SceneView(C.Structure):
+    """ps_scene_view (device pointers, SceneCollisionData layout)."""
+
+    _fields_ = [
+        ("obb_dims", C.c_void_p), ("obb_pose", C.c_void_p), ("obb_enable", C.c_void_p),
+        ("n_obbs", C.c_int),
+        ("voxel_params", C.c_void_p), ("voxel_pose", C.c_void_p),
+        ("voxel_enable", C.c_void_p), ("voxel_features", C.c_void_p),
+        ("n_voxel_layers", C.c_int), ("max_voxels_per_layer", C.c_int),
+        ("sphere_acm_mask", C.c_void_p), ("sphere_obb_acm_mask", C.c_void_p),
+        ("sphere_obb_acm_mask_approx", C.c_void_p),
+        ("esdf_mode", C.c_int),
+    ]
+
+
+class EdgeParams(C.Structure):
+    _fields_ = [
+        ("granularity", C.c_int), ("resolution", C.c_float),
+        ("max_joint_step", C.c_float), ("max_samples", C.c_int),
+        ("collision_margin", C.c_float), ("check_self", C.c_int),
+        ("compute_clearance", C.c_int),
+    ]
+
+
+class CostParams(C.Structure):
+    _fields_ = [
+        ("collision_cost_weight", C.c_float), ("world_margin", C.c_float),
+        ("self_margin", C.c_float), ("include_self", C.c_int),
+        ("smoothness_weight", C.c_float), ("delta_t", C.c_float),
+        ("layout", C.c_int),
+    ]
+
+
+# (name, restype, argtypes)
+_SIGNATURES = [
+    ("ps_last_error", C.c_char_p, []),
+    ("ps_version", C.c_char_p, []),
+    ("ps_model_create", C.c_int, [C.POINTER(ModelDesc), C.POINTER(C.c_void_p)]),
+    ("ps_model_destroy", C.c_int, [C.c_void_p]),
+    ("ps_model_set_limits", C.c_int, [C.c_void_p, _fp, _fp]),
+    ("ps_model_get_info", C.c_int, [C.c_void_p, C.POINTER(ModelInfo)]),
+    ("ps_model_poll_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    ("ps_check_configs", C.c_int,
+     [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_int, C.c_float, C.c_uint,
+      C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("ps_check_edges_plain", C.c_int,
+     [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+      C.POINTER(EdgeParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("ps_edges_workspace_bytes", C.c_size_t, [C.c_int]),
+    ("ps_check_edges", C.c_int,
+     [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+      C.POINTER(EdgeParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+      C.c_size_t, C.c_void_p]),
+    ("ps_traj_cost", C.c_int,
+     [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_int, C.c_int,
+      C.POINTER(CostParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("ps_rollout_costs", C.c_int,
+     [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_int, C.c_int,
+      C.POINTER(CostParams), C.c_int, C.c_void_p, C.c_void_p]),
+    ("ps_fk_spheres", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    ("ps_probe_fp32_peak", C.c_int, [C.POINTER(C.c_double), C.c_void_p]),
+    ("ps_set_stats", C.c_int, [C.c_void_p]),
+]
+
+EXPORTED_SYMBOLS = [name for name, _, _ in _SIGNATURES]
+
+_lib = None
+
+
+def load(path: os.PathLike | None = None):
+    """Load the CUDA library once and bind every symbol. Raises if absent."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.is_file():
+        raise ImportError(
+            f"prismplan_b200 CUDA library not found at {p}; build it with "
+            "`python -c 'import __graft_entry__ as g; g.build()'` or "
+            "`make -C prismplan_b200/csrc`")
+    lib = C.CDLL(str(p))
+    for name, restype, argtypes in _SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = restype
+        fn.argtypes = argtypes
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def check(status: int) -> None:
+    if status != PS_OK:
+        msg = load().ps_last_error()
+        raise PrismError(status, msg.decode() if msg else "")
+
+
+def stream_handle(stream) -> int | None:
+    """cudaStream_t of a torch.cuda.Stream (or None for the current stream)."""
+    import torch
+
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return int(stream.cuda_stream) or None

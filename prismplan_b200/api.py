@@ -1,0 +1,355 @@
+"""Python API over the C ABI (torch tensors in, torch tensors out).
+
+Reference-facing calls keep the reference's names and semantics:
+  * ``check_collision_scene(configs, scene, robot, collision_margin)``
+    -- prrtc.check_collision_scene (code/gpu_planning/cpp/src/python/
+    bindings.cpp:493-532): host numpy in, host bool numpy out, synchronous.
+  * ``EdgeEvalGpu(dim, max_edges, scene, model).evaluate(...)``
+    -- ppln::search::EdgeEvalGpu (cpp/src/planning/edge_batch_bridge.hh:27-111).
+Device-resident torch calls (``check_configs``, ``check_edges``,
+``traj_cost``, ``rollout_costs``) are asynchronous on the current stream.
+``hinge_cost`` applies a torch.autograd.Function whose backward is the
+fused hand-written adjoint.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional, Tuple
+
+import numpy as np
+
+from . import _lib
+from .robot import RobotModelBuilder
+from .scene import SceneCollisionDataBuilder, SceneTensors
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _view(scene) -> _lib.SceneView:
+    if scene is None:
+        return SceneCollisionDataBuilder().build()
+    if isinstance(scene, SceneTensors):
+        return scene.view()
+    if isinstance(scene, SceneCollisionDataBuilder):
+        return scene.build()
+    if isinstance(scene, _lib.SceneView):
+        return scene
+    raise TypeError(f"unsupported scene type {type(scene).__name__}")
+
+
+def _dev_f32(t, shape_last=None):
+    torch = _torch()
+    if not isinstance(t, torch.Tensor):
+        t = torch.as_tensor(np.asarray(t, np.float32))
+    if not t.is_cuda:
+        t = t.cuda()
+    t = t.to(torch.float32).contiguous()
+    if shape_last is not None and t.shape[-1] != shape_last:
+        raise ValueError(f"last dimension must be {shape_last}, got {tuple(t.shape)}")
+    return t
+
+
+def _stream(stream):
+    return _lib.stream_handle(stream)
+
+
+def _model(robot: RobotModelBuilder) -> C.c_void_p:
+    return robot.handle
+
+
+# ---------------------------------------------------------------------------
+# configurations
+# ---------------------------------------------------------------------------
+def check_configs(robot: RobotModelBuilder, scene, q, collision_margin: float = 0.0,
+                  clearance: Optional[str] = None, check_self: bool = False,
+                  no_gate: bool = False, stream=None):
+    """Two-phase any-collision for every row of ``q`` [N, n_dof] (CUDA).
+
+    ``clearance``: None, "obb", "esdf" or "both" -- min over spheres of the
+    selected signed clearance (radius + margin), 1000.0 when nothing applies.
+    Returns (hit uint8 [N], clearance float32 [N] or None)."""
+    torch = _torch()
+    q = _dev_f32(q, robot.n_dof)
+    n = q.shape[0]
+    hit = torch.empty(n, dtype=torch.uint8, device=q.device)
+    flags = 0
+    if clearance in ("obb", "both"):
+        flags |= _lib.PS_CLEARANCE_OBB
+    if clearance in ("esdf", "both"):
+        flags |= _lib.PS_CLEARANCE_ESDF
+    if check_self:
+        flags |= _lib.PS_CHECK_SELF
+    if no_gate:
+        flags |= _lib.PS_NO_GATE
+    clr = torch.empty(n, dtype=torch.float32, device=q.device) if clearance else None
+    v = _view(scene)
+    _lib.check(_lib.load().ps_check_configs(
+        _model(robot), C.byref(v), q.data_ptr(), n, float(collision_margin), flags,
+        hit.data_ptr(), clr.data_ptr() if clr is not None else None, _stream(stream)))
+    return hit, clr
+
+
+def check_collision_scene(configs, scene_builder, robot: RobotModelBuilder,
+                          collision_margin: float = 0.0) -> np.ndarray:
+    """Drop-in for prrtc.check_collision_scene: configs [N, n_dof] host array
+    -> bool [N] (True = in collision), synchronous."""
+    torch = _torch()
+    robot.build()
+    c = np.asarray(configs, np.float32)
+    if c.ndim != 2 or c.shape[1] != robot.n_dof:
+        raise RuntimeError("configs columns mismatch with robot n_dof")
+    if c.shape[0] == 0:
+        return np.zeros(0, bool)
+    hit, _ = check_configs(robot, scene_builder, torch.from_numpy(c).cuda(), collision_margin)
+    return hit.cpu().numpy().astype(bool)
+
+
+def fk_spheres(robot: RobotModelBuilder, q, stream=None):
+    """World sphere centres [N, n_spheres, 3] (descriptor order)."""
+    torch = _torch()
+    q = _dev_f32(q, robot.n_dof)
+    n = q.shape[0]
+    out = torch.empty((n, len(robot.sphere_to_joint), 3), dtype=torch.float32, device=q.device)
+    _lib.check(_lib.load().ps_fk_spheres(_model(robot), q.data_ptr(), n, out.data_ptr(), _stream(stream)))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# edges
+# ---------------------------------------------------------------------------
+@dataclass
+class EdgeEvalParams:
+    """ppln::search::EdgeEvalParams (edge_eval.cuh:37-51) plus the L-inf rule."""
+
+    granularity: int = 16
+    collision_margin: float = 0.0
+    check_self: bool = False
+    compute_clearance: bool = False
+    enable_mesh: bool = False
+    resolution: float = 0.0
+    max_joint_step: float = 0.0
+    max_samples: int = 1024
+
+    def to_c(self) -> _lib.EdgeParams:
+        if self.enable_mesh:
+            raise ValueError("mesh edge checks are not supported (enable_mesh must be False)")
+        p = _lib.EdgeParams()
+        p.granularity = int(self.granularity)
+        p.resolution = float(self.resolution)
+        p.max_joint_step = float(self.max_joint_step)
+        p.max_samples = int(self.max_samples)
+        p.collision_margin = float(self.collision_margin)
+        p.check_self = int(bool(self.check_self))
+        p.compute_clearance = int(bool(self.compute_clearance))
+        return p
+
+
+def edges_workspace(n_edges: int, device="cuda"):
+    torch = _torch()
+    nbytes = int(_lib.load().ps_edges_workspace_bytes(int(n_edges)))
+    return torch.empty(nbytes, dtype=torch.uint8, device=device)
+
+
+def check_edges(robot: RobotModelBuilder, scene, frm, to, samples=None,
+                params: Optional[EdgeEvalParams] = None, persistent: bool = True,
+                workspace=None, out=None, stream=None):
+    """Edge validity for rows of ``frm``/``to`` [E, n_dof] (CUDA).
+
+    ``samples`` [E] int32 (optional) fixes G per edge; otherwise ``params``
+    decides (resolution / max_joint_step / granularity). Returns
+    (valid uint8 [E], cost float32 [E], clearance float32 [E])."""
+    torch = _torch()
+    params = params or EdgeEvalParams()
+    frm = _dev_f32(frm, robot.n_dof)
+    to = _dev_f32(to, robot.n_dof)
+    E = frm.shape[0]
+    if to.shape[0] != E:
+        raise ValueError("from/to row counts differ")
+    if samples is not None:
+        samples = torch.as_tensor(samples).to(device=frm.device, dtype=torch.int32).contiguous()
+        if samples.shape[0] != E:
+            raise ValueError("samples must have one entry per edge")
+    if out is None:
+        valid = torch.empty(E, dtype=torch.uint8, device=frm.device)
+        cost = torch.empty(E, dtype=torch.float32, device=frm.device)
+        clr = torch.empty(E, dtype=torch.float32, device=frm.device)
+    else:
+        valid, cost, clr = out
+    p = params.to_c()
+    v = _view(scene)
+    lib = _lib.load()
+    sp = samples.data_ptr() if samples is not None else None
+    if persistent:
+        if workspace is None:
+            workspace = edges_workspace(E, frm.device)
+        _lib.check(lib.ps_check_edges(_model(robot), C.byref(v), frm.data_ptr(), to.data_ptr(), sp, E,
+                                      C.byref(p), valid.data_ptr(), cost.data_ptr(), clr.data_ptr(),
+                                      workspace.data_ptr(), workspace.numel(), _stream(stream)))
+    else:
+        _lib.check(lib.ps_check_edges_plain(_model(robot), C.byref(v), frm.data_ptr(), to.data_ptr(), sp, E,
+                                            C.byref(p), valid.data_ptr(), cost.data_ptr(), clr.data_ptr(),
+                                            _stream(stream)))
+    return valid, cost, clr
+
+
+class EdgeEvalGpu:
+    """Drop-in for ppln::search::EdgeEvalGpu (edge_batch_bridge.hh:27-111):
+    persistent device buffers, pinned host mirrors and a private stream;
+    ``evaluate`` copies in, runs the persistent edge kernel, copies out and
+    synchronises. Raises on num_edges > max_edges like the reference (:67-68)."""
+
+    def __init__(self, dim: int, max_edges: int, scene, model: RobotModelBuilder):
+        torch = _torch()
+        self.dim, self.max_edges, self.scene, self.model = int(dim), int(max_edges), scene, model
+        if model.n_dof != self.dim:
+            raise ValueError("dim must equal the robot's n_dof")
+        dev = torch.device("cuda")
+        self._from = torch.empty((self.max_edges, self.dim), dtype=torch.float32, device=dev)
+        self._to = torch.empty_like(self._from)
+        self._valid = torch.empty(self.max_edges, dtype=torch.uint8, device=dev)
+        self._cost = torch.empty(self.max_edges, dtype=torch.float32, device=dev)
+        self._clr = torch.empty(self.max_edges, dtype=torch.float32, device=dev)
+        self._ws = edges_workspace(self.max_edges, dev)
+        self._h_from = torch.empty((self.max_edges, self.dim), dtype=torch.float32).pin_memory()
+        self._h_to = torch.empty_like(self._h_from).pin_memory()
+        self._h_out = torch.empty((3, self.max_edges), dtype=torch.float32).pin_memory()
+        self._h_valid = torch.empty(self.max_edges, dtype=torch.uint8).pin_memory()
+        self._stream = torch.cuda.Stream()
+
+    def evaluate(self, from_flat, to_flat, num_edges: int, params: EdgeEvalParams):
+        torch = _torch()
+        n = int(num_edges)
+        if n <= 0:
+            return np.zeros(0, np.uint8), np.zeros(0, np.float32), np.zeros(0, np.float32)
+        if n > self.max_edges:
+            raise RuntimeError("EdgeEvalGpu: num_edges exceeds max_edges_")
+        self._h_from[:n].copy_(torch.from_numpy(np.asarray(from_flat, np.float32).reshape(-1, self.dim)[:n]))
+        self._h_to[:n].copy_(torch.from_numpy(np.asarray(to_flat, np.float32).reshape(-1, self.dim)[:n]))
+        with torch.cuda.stream(self._stream):
+            self._from[:n].copy_(self._h_from[:n], non_blocking=True)
+            self._to[:n].copy_(self._h_to[:n], non_blocking=True)
+            check_edges(self.model, self.scene, self._from[:n], self._to[:n], params=params, workspace=self._ws,
+                        out=(self._valid[:n], self._cost[:n], self._clr[:n]), stream=self._stream)
+            self._h_valid[:n].copy_(self._valid[:n], non_blocking=True)
+            self._h_out[0, :n].copy_(self._cost[:n], non_blocking=True)
+            if params.compute_clearance:
+                self._h_out[1, :n].copy_(self._clr[:n], non_blocking=True)
+        self._stream.synchronize()
+        valid = self._h_valid[:n].numpy().copy()
+        cost = self._h_out[0, :n].numpy().copy()
+        clr = self._h_out[1, :n].numpy().copy() if params.compute_clearance else np.zeros(0, np.float32)
+        return valid, cost, clr
+
+
+# ---------------------------------------------------------------------------
+# trajectory costs
+# ---------------------------------------------------------------------------
+@dataclass
+class CostParams:
+    """Hinge / smoothness parameters (CHOMP_settings.hh:35-46 names)."""
+
+    collision_cost_weight: float = 20.0
+    world_collision_margin: float = 0.02
+    self_collision_margin: float = 0.01
+    include_self: bool = True
+    smoothness_weight: float = 0.0
+    delta_t: float = 0.1
+
+    def to_c(self, layout: int) -> _lib.CostParams:
+        p = _lib.CostParams()
+        p.collision_cost_weight = float(self.collision_cost_weight)
+        p.world_margin = float(self.world_collision_margin)
+        p.self_margin = float(self.self_collision_margin)
+        p.include_self = int(bool(self.include_self))
+        p.smoothness_weight = float(self.smoothness_weight)
+        p.delta_t = float(self.delta_t)
+        p.layout = int(layout)
+        return p
+
+
+def traj_cost(robot: RobotModelBuilder, scene, q, params: Optional[CostParams] = None,
+              want_grad: bool = True, want_waypoint: bool = True, layout: int = _lib.PS_LAYOUT_BTD,
+              stream=None):
+    """Summed-hinge (+ self hinge, + smoothness) cost of trajectories ``q``
+    [B, T, n_dof] (or [B, n_dof, T] with PS_LAYOUT_BDT), one fused launch for
+    cost and gradient. Returns (waypoint_cost [B, T] or None, traj_cost [B],
+    grad like q or None)."""
+    torch = _torch()
+    params = params or CostParams()
+    q = _dev_f32(q)
+    if q.dim() != 3:
+        raise ValueError("q must be 3-D")
+    if layout == _lib.PS_LAYOUT_BTD:
+        B, T, D = q.shape
+    else:
+        B, D, T = q.shape
+    if D != robot.n_dof:
+        raise ValueError("DoF dimension mismatch")
+    wp = torch.empty((B, T), dtype=torch.float32, device=q.device) if want_waypoint else None
+    tc = torch.empty(B, dtype=torch.float32, device=q.device)
+    g = torch.empty_like(q) if want_grad else None
+    p = params.to_c(layout)
+    v = _view(scene)
+    _lib.check(_lib.load().ps_traj_cost(_model(robot), C.byref(v), q.data_ptr(), B, T, C.byref(p),
+                                        wp.data_ptr() if wp is not None else None, tc.data_ptr(),
+                                        g.data_ptr() if g is not None else None, _stream(stream)))
+    return wp, tc, g
+
+
+def rollout_costs(robot: RobotModelBuilder, scene, rollouts, params: Optional[CostParams] = None,
+                  broadcast_d: bool = False, stream=None):
+    """STOMP per-(rollout, waypoint) state cost of ``rollouts`` [R, n_dof, T]
+    (the reference layout). Returns [R, T] or, with broadcast_d, [R, n_dof, T]
+    as stomp_state_cost_kernel writes it."""
+    torch = _torch()
+    params = params or CostParams()
+    r = _dev_f32(rollouts)
+    R, D, T = r.shape
+    if D != robot.n_dof:
+        raise ValueError("DoF dimension mismatch")
+    out = torch.empty((R, D, T) if broadcast_d else (R, T), dtype=torch.float32, device=r.device)
+    p = params.to_c(_lib.PS_LAYOUT_BDT)
+    v = _view(scene)
+    _lib.check(_lib.load().ps_rollout_costs(_model(robot), C.byref(v), r.data_ptr(), R, T, C.byref(p),
+                                            int(bool(broadcast_d)), out.data_ptr(), _stream(stream)))
+    return out
+
+
+def _make_autograd():
+    torch = _torch()
+
+    class _TrajCost(torch.autograd.Function):
+        """traj_cost[b] = sum_t w*hinge(q[b,t]) + lambda*sum_d q_d^T R q_d.
+
+        Forward runs the fused FK + hinge + adjoint kernel once and keeps the
+        gradient; backward scales it by grad_output (no second pass)."""
+
+        @staticmethod
+        def forward(ctx, q, robot, scene, params):
+            need = q.requires_grad
+            _, tc, g = traj_cost(robot, scene, q.detach(), params, want_grad=need, want_waypoint=False)
+            ctx.save_for_backward(g if need else torch.empty(0, device=q.device))
+            return tc
+
+        @staticmethod
+        def backward(ctx, grad_out):
+            (g,) = ctx.saved_tensors
+            return grad_out.view(-1, 1, 1) * g, None, None, None
+
+    return _TrajCost
+
+
+def hinge_cost(q, robot: RobotModelBuilder, scene, params: Optional[CostParams] = None):
+    """Differentiable trajectory cost [B] of q [B, T, n_dof]."""
+    global _TRAJ_COST
+    if _TRAJ_COST is None:
+        _TRAJ_COST = _make_autograd()
+    return _TRAJ_COST.apply(q, robot, scene, params or CostParams())
+
+
+_TRAJ_COST = None

@@ -1,0 +1,357 @@
+// ps_check.cu -- batched configuration check (one lane per configuration),
+// sphere FK diagnostics and the FP32 throughput probe.
+//
+// Replaces check_collision_scene_kernel (code/gpu_planning/cpp/src/planning/
+// pRRTC.cu:2337-2389, one 4-thread block per configuration, 1/8 of a warp
+// busy) with full warps: lane = configuration, the 3x4 joint frames live in
+// registers, the model core arrives in shared memory through one bulk async
+// copy, and the obstacle table is staged once per block as prepared 3x3
+// boxes. Clearance (PS_CLEARANCE_OBB) is the min over spheres of the
+// sphere-vs-box SDF, the OBB counterpart of scene_min_clearance_runtime
+// (scene_collision.cuh:339-384, which covers ESDF only).
+#include <algorithm>
+
+#include "ps_internal.h"
+#include "ps_verdict.cuh"
+
+namespace ps {
+
+namespace {
+
+constexpr int kCfgThreads = 128;
+
+template <bool kClr>
+__global__ void __launch_bounds__(kCfgThreads) check_configs_kernel(ModelDev md, ps_scene_view sv, const float* __restrict__ q,
+                                                                   int n, float margin, unsigned flags,
+                                                                   uint8_t* __restrict__ hit_out,
+                                                                   float* __restrict__ clr_out,
+                                                                   unsigned long long* stats) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ int counters[4];
+    __shared__ float bmax;
+    unsigned char* blob = smem;
+    ObbPrep* obbs = reinterpret_cast<ObbPrep*>(smem + md.bytes_core);
+    const int nob = max(sv.n_obbs, 1);
+    int* orig = reinterpret_cast<int*>(obbs + nob);
+    LayerPrep* layers = reinterpret_cast<LayerPrep*>(orig + ((nob + 3) & ~3));
+    float* qtile = reinterpret_cast<float*>(layers + PS_MAX_LAYERS);
+
+    if (!stage_model(md, blob, &mbar)) return;
+    SceneSmem sc;
+    stage_scene(sv, obbs, orig, layers, counters, &bmax, sc);
+    const ModelSmem M = model_view(blob);
+    const int D = M.H->n_dof, NJ = M.H->n_joints;
+    const bool no_gate = (flags & PS_NO_GATE) != 0;
+    const bool want_obb_clr = (flags & PS_CLEARANCE_OBB) != 0;
+    const bool want_esdf_clr = (flags & PS_CLEARANCE_ESDF) != 0;
+    LaneStats st;
+    st.zero();
+
+    for (int base = blockIdx.x * kCfgThreads; base < n; base += gridDim.x * kCfgThreads) {
+        // Coalesced load of this block's configurations into shared memory.
+        const int cnt = min(kCfgThreads, n - base);
+        __syncthreads();
+        for (int k = threadIdx.x; k < cnt * D; k += kCfgThreads) qtile[k] = q[(size_t)base * D + k];
+        __syncthreads();
+        const int c = base + threadIdx.x;
+        const bool active = threadIdx.x < cnt;
+        const float* qc = qtile + threadIdx.x * D;
+
+        Affine s0, s1, T, a0, a1, TA;
+        affine_identity(s0);
+        affine_identity(s1);
+        affine_identity(a0);
+        affine_identity(a1);
+        bool hit = false;
+        float clr = 1000.0f;
+        if (active) {
+            st.v[ST_SAMPLES] += 1;
+            const bool shares = M.H->approx_shares_chain != 0;
+            for (int p = 0; p < NJ; ++p) {
+                const JointRec& jr = M.J[p];
+                fk_step<true>(jr, p, qc, s0, s1, T);
+                st.v[ST_JOINTS] += (p > 0);
+                if (!shares) fk_step<true>(M.JA[p], p, qc, a0, a1, TA);
+                // ---- approximate gate for this joint ----
+                bool flagged = no_gate;
+                for (int a = jr.apx_beg; a < jr.apx_end && !flagged; ++a) {
+                    const float4 sa = M.A[a];
+                    float px, py, pz;
+                    sphere_world(shares ? T : TA, sa.x, sa.y, sa.z, px, py, pz);
+                    st.v[ST_SPHERES] += 1;
+                    const float sr = __fadd_rn(sa.w, margin);
+                    const uint8_t* acm = sv.sphere_obb_acm_mask_approx
+                                             ? sv.sphere_obb_acm_mask_approx + (size_t)M.AO[a] * sv.n_obbs
+                                             : nullptr;
+                    flagged = (sc.n_obbs && sphere_obb_any(sc, nullptr, 0, px, py, pz, sr, acm, st)) ||
+                              (sc.n_layers && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
+                }
+                // ---- exact spheres of this joint ----
+                const int s_end = (kClr || (flagged && !hit)) ? jr.sph_end : jr.sph_beg;
+                for (int s_i = jr.sph_beg; s_i < s_end; ++s_i) {
+                    const float4 sp = M.S[s_i];
+                    float px, py, pz;
+                    sphere_world(T, sp.x, sp.y, sp.z, px, py, pz);
+                    st.v[ST_SPHERES] += 1;
+                    const float sr = __fadd_rn(sp.w, margin);
+                    const int so = M.SO[s_i];
+                    const uint8_t* acm =
+                        sv.sphere_obb_acm_mask ? sv.sphere_obb_acm_mask + (size_t)so * sv.n_obbs : nullptr;
+                    const uint8_t* eacm =
+                        sv.sphere_acm_mask ? sv.sphere_acm_mask + (size_t)so * sv.n_voxel_layers : nullptr;
+                    const bool decide = flagged && !hit;
+                    if (kClr) {
+                        if (sc.n_obbs && (want_obb_clr || decide)) {
+                            float min_dsq;
+                            bool any_box;
+                            float sdf = sphere_obb_min_sdf(sc, px, py, pz, acm, min_dsq, any_box, st);
+                            // sphere_obb_clearance: 1000 sentinel when no box applies
+                            if (want_obb_clr && any_box) clr = fminf(clr, __fadd_rn(sdf, -sr));
+                            if (decide && any_box) hit = decide_from_min(sc, px, py, pz, sr, min_dsq, acm, st);
+                        }
+                        if (want_esdf_clr && sc.n_layers)
+                            clr = fminf(clr, sphere_esdf_clearance(sc, sv, px, py, pz, sr, eacm, st));
+                        if (flagged && !hit && sc.n_layers) hit = sphere_esdf_any(sc, sv, px, py, pz, sr, eacm, st);
+                    } else {
+                        hit = (sc.n_obbs && sphere_obb_any(sc, nullptr, 0, px, py, pz, sr, acm, st)) ||
+                              (sc.n_layers && sphere_esdf_any(sc, sv, px, py, pz, sr, eacm, st));
+                        if (hit) break;
+                    }
+                }
+                if (!kClr && __all_sync(__activemask(), hit)) break;
+            }
+        }
+        if (active) {
+            hit_out[c] = hit ? 1 : 0;
+            if (clr_out) clr_out[c] = clr;
+        }
+    }
+    flush_stats(stats, st);
+}
+
+// Self-collision two-phase check, one configuration per lane, positions of
+// every exact and approximate sphere staged in shared memory (SoA by lane).
+constexpr int kSelfThreads = 64;
+
+__global__ void __launch_bounds__(kSelfThreads) self_check_kernel(ModelDev md, const float* __restrict__ q, int n,
+                                                                  uint8_t* __restrict__ hit_out,
+                                                                  unsigned long long* stats) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    unsigned char* blob = smem;
+    if (!stage_model(md, blob, &mbar)) return;
+    const ModelSmem M = model_view(blob);
+    const int D = M.H->n_dof, NJ = M.H->n_joints, NS = M.H->n_spheres, NA = M.H->n_approx;
+    float* pos = reinterpret_cast<float*>(smem + md.bytes_core);        // [NS*3][kSelfThreads]
+    float* apos = pos + (size_t)NS * 3 * kSelfThreads;                   // [NA*3][kSelfThreads]
+    float* qtile = apos + (size_t)NA * 3 * kSelfThreads;
+    LaneStats st;
+    st.zero();
+    const int lane = threadIdx.x;
+    for (int base = blockIdx.x * kSelfThreads; base < n; base += gridDim.x * kSelfThreads) {
+        const int cnt = min(kSelfThreads, n - base);
+        __syncthreads();
+        for (int k = threadIdx.x; k < cnt * D; k += kSelfThreads) qtile[k] = q[(size_t)base * D + k];
+        __syncthreads();
+        if (lane >= cnt) continue;
+        if (hit_out[base + lane]) continue;   // already in collision with the scene
+        const float* qc = qtile + lane * D;
+        Affine s0, s1, T;
+        affine_identity(s0);
+        affine_identity(s1);
+        for (int p = 0; p < NJ; ++p) {
+            const JointRec& jr = M.J[p];
+            fk_step<true>(jr, p, qc, s0, s1, T);
+            for (int k = jr.sph_beg; k < jr.sph_end; ++k) {
+                const float4 s = M.S[k];
+                float px, py, pz;
+                sphere_world(T, s.x, s.y, s.z, px, py, pz);
+                pos[(k * 3 + 0) * kSelfThreads + lane] = px;
+                pos[(k * 3 + 1) * kSelfThreads + lane] = py;
+                pos[(k * 3 + 2) * kSelfThreads + lane] = pz;
+            }
+            if (M.H->approx_shares_chain) {
+                for (int k = jr.apx_beg; k < jr.apx_end; ++k) {
+                    const float4 s = M.A[k];
+                    float px, py, pz;
+                    sphere_world(T, s.x, s.y, s.z, px, py, pz);
+                    apos[(k * 3 + 0) * kSelfThreads + lane] = px;
+                    apos[(k * 3 + 1) * kSelfThreads + lane] = py;
+                    apos[(k * 3 + 2) * kSelfThreads + lane] = pz;
+                }
+            }
+        }
+        if (!M.H->approx_shares_chain) {
+            affine_identity(s0);
+            affine_identity(s1);
+            for (int p = 0; p < NJ; ++p) {
+                const JointRec& jr = M.JA[p];
+                fk_step<true>(jr, p, qc, s0, s1, T);
+                for (int k = jr.apx_beg; k < jr.apx_end; ++k) {
+                    const float4 s = M.A[k];
+                    float px, py, pz;
+                    sphere_world(T, s.x, s.y, s.z, px, py, pz);
+                    apos[(k * 3 + 0) * kSelfThreads + lane] = px;
+                    apos[(k * 3 + 1) * kSelfThreads + lane] = py;
+                    apos[(k * 3 + 2) * kSelfThreads + lane] = pz;
+                }
+            }
+        }
+        bool need = false;
+        for (int k = 0; k < M.H->n_apx_self_pairs && !need; ++k) {
+            const uint32_t pr = __ldg(md.apx_self_pairs + k);
+            const int i = pr & 0xffff, j = pr >> 16;
+            st.v[ST_SELF] += 1;
+            need = ref_self_hit(apos[(i * 3) * kSelfThreads + lane], apos[(i * 3 + 1) * kSelfThreads + lane],
+                                apos[(i * 3 + 2) * kSelfThreads + lane], M.A[i].w,
+                                apos[(j * 3) * kSelfThreads + lane], apos[(j * 3 + 1) * kSelfThreads + lane],
+                                apos[(j * 3 + 2) * kSelfThreads + lane], M.A[j].w);
+        }
+        bool hit = false;
+        for (int k = 0; need && k < M.H->n_self_pairs && !hit; ++k) {
+            const uint32_t pr = __ldg(md.self_pairs + k);
+            const int i = pr & 0xffff, j = pr >> 16;
+            st.v[ST_SELF] += 1;
+            hit = ref_self_hit(pos[(i * 3) * kSelfThreads + lane], pos[(i * 3 + 1) * kSelfThreads + lane],
+                               pos[(i * 3 + 2) * kSelfThreads + lane], M.S[i].w, pos[(j * 3) * kSelfThreads + lane],
+                               pos[(j * 3 + 1) * kSelfThreads + lane], pos[(j * 3 + 2) * kSelfThreads + lane],
+                               M.S[j].w);
+        }
+        if (hit) hit_out[base + lane] = 1;
+    }
+    flush_stats(stats, st);
+}
+
+// World sphere centres in descriptor order (diagnostics / parity).
+__global__ void __launch_bounds__(kCfgThreads) fk_spheres_kernel(ModelDev md, const float* __restrict__ q, int n,
+                                                                float* __restrict__ out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    if (!stage_model(md, smem, &mbar)) return;
+    const ModelSmem M = model_view(smem);
+    const int D = M.H->n_dof, NJ = M.H->n_joints, NS = M.H->n_spheres;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        float qc[PS_MAX_DOF];
+        for (int d = 0; d < D; ++d) qc[d] = q[(size_t)c * D + d];
+        Affine s0, s1, T;
+        affine_identity(s0);
+        affine_identity(s1);
+        for (int p = 0; p < NJ; ++p) {
+            const JointRec& jr = M.J[p];
+            fk_step<true>(jr, p, qc, s0, s1, T);
+            for (int k = jr.sph_beg; k < jr.sph_end; ++k) {
+                const float4 s = M.S[k];
+                float px, py, pz;
+                sphere_world(T, s.x, s.y, s.z, px, py, pz);
+                float* o = out + ((size_t)c * NS + M.SO[k]) * 3;
+                o[0] = px;
+                o[1] = py;
+                o[2] = pz;
+            }
+        }
+    }
+}
+
+// FP32 FMA throughput probe: 8 independent FMA chains per thread.
+__global__ void __launch_bounds__(256) fma_probe_kernel(float* out, int iters, float a, float b) {
+    float x0 = threadIdx.x * 1e-7f, x1 = x0 + 1e-7f, x2 = x0 + 2e-7f, x3 = x0 + 3e-7f;
+    float x4 = x0 + 4e-7f, x5 = x0 + 5e-7f, x6 = x0 + 6e-7f, x7 = x0 + 7e-7f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            x0 = fmaf(x0, a, b); x1 = fmaf(x1, a, b); x2 = fmaf(x2, a, b); x3 = fmaf(x3, a, b);
+            x4 = fmaf(x4, a, b); x5 = fmaf(x5, a, b); x6 = fmaf(x6, a, b); x7 = fmaf(x7, a, b);
+        }
+    }
+    float s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+    if (s == 12345.678f) out[0] = s;   // keeps the chains live
+}
+
+}  // namespace
+
+unsigned long long* g_stats = nullptr;
+
+}  // namespace ps
+
+using namespace ps;
+
+extern "C" int ps_set_stats(unsigned long long* dev_counters) {
+    ps::g_stats = dev_counters;
+    return PS_OK;
+}
+
+extern "C" int ps_check_configs(const ps_model* m, const ps_scene_view* scene, const float* q, int n,
+                                float margin, unsigned flags, uint8_t* hit, float* clearance, void* stream) {
+    clear_error();
+    if (!m) return set_error(PS_EINVAL, "model is NULL");
+    if (n < 0) return set_error(PS_EINVAL, "n < 0");
+    if (n == 0) return PS_OK;
+    if (!q || !hit) return set_error(PS_EINVAL, "q / hit is NULL");
+    if (int rc = validate_scene(m, scene)) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    // Without a clearance source the output (if any) is the 1000 sentinel.
+    const bool clr = clearance != nullptr && (flags & (PS_CLEARANCE_OBB | PS_CLEARANCE_ESDF));
+    size_t smem = (size_t)m->dev.bytes_core + scene_smem_bytes(scene) + (size_t)kCfgThreads * m->info.n_dof * 4;
+    const int blocks_needed = (n + kCfgThreads - 1) / kCfgThreads;
+    const int grid = std::max(1, std::min(blocks_needed, sm_count() * 8));
+    if (clr) {
+        PS_TRY_CUDA(cudaFuncSetAttribute(check_configs_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        check_configs_kernel<true><<<grid, kCfgThreads, smem, s>>>(m->dev, *scene, q, n, margin, flags, hit, clearance,
+                                                                   g_stats);
+    } else {
+        PS_TRY_CUDA(cudaFuncSetAttribute(check_configs_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        check_configs_kernel<false><<<grid, kCfgThreads, smem, s>>>(m->dev, *scene, q, n, margin, flags, hit, clearance,
+                                                                    g_stats);
+    }
+    PS_TRY_CUDA(cudaGetLastError());
+    if (flags & PS_CHECK_SELF) {
+        size_t ss = (size_t)m->dev.bytes_core +
+                    (size_t)(m->info.n_spheres + m->info.n_approx_spheres) * 3 * kSelfThreads * 4 +
+                    (size_t)kSelfThreads * m->info.n_dof * 4;
+        PS_TRY_CUDA(cudaFuncSetAttribute(self_check_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+        const int g2 = std::max(1, std::min((n + kSelfThreads - 1) / kSelfThreads, sm_count() * 8));
+        self_check_kernel<<<g2, kSelfThreads, ss, s>>>(m->dev, q, n, hit, g_stats);
+        PS_TRY_CUDA(cudaGetLastError());
+    }
+    return PS_OK;
+}
+
+extern "C" int ps_fk_spheres(const ps_model* m, const float* q, int n, float* out, void* stream) {
+    clear_error();
+    if (!m || (n > 0 && (!q || !out))) return set_error(PS_EINVAL, "NULL argument");
+    if (n <= 0) return PS_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    size_t smem = (size_t)m->dev.bytes_core;
+    PS_TRY_CUDA(cudaFuncSetAttribute(fk_spheres_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int grid = std::max(1, std::min((n + kCfgThreads - 1) / kCfgThreads, sm_count() * 8));
+    fk_spheres_kernel<<<grid, kCfgThreads, smem, s>>>(m->dev, q, n, out);
+    PS_TRY_CUDA(cudaGetLastError());
+    return PS_OK;
+}
+
+extern "C" int ps_probe_fp32_peak(double* flops_per_s, void* stream) {
+    clear_error();
+    if (!flops_per_s) return set_error(PS_EINVAL, "NULL output");
+    cudaStream_t s = (cudaStream_t)stream;
+    float* d = nullptr;
+    PS_TRY_CUDA(cudaMalloc(&d, sizeof(float)));
+    const int blocks = sm_count() * 8, threads = 256, iters = 4096;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    fma_probe_kernel<<<blocks, threads, 0, s>>>(d, 64, 1.0000001f, 1e-7f);   // warm-up
+    cudaEventRecord(a, s);
+    fma_probe_kernel<<<blocks, threads, 0, s>>>(d, iters, 1.0000001f, 1e-7f);
+    cudaEventRecord(b, s);
+    cudaError_t e = cudaEventSynchronize(b);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_error(e, "fma probe");
+    const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+    *flops_per_s = flops / (ms * 1e-3);
+    return PS_OK;
+}

@@ -1,0 +1,309 @@
+// ps_common.cuh -- device-side building blocks of the sm_100a substrate.
+//
+// Arithmetic that decides a collision Boolean reproduces the reference's FP32
+// operation sequence exactly (paths inside code/gpu_planning/cpp/src/):
+//   * joint step columns      planning/utils.cuh:571-699 (xrot_fn/yrot_fn/zrot_fn/prism_fn)
+//   * 4x4 compose             planning/runtime_kinematics.cuh:60-70 with dot4_col (utils.cuh:709-711)
+//   * sphere emission         planning/runtime_kinematics.cuh:74-85
+//   * world -> box frame      collision/scene_collision.cuh:24-51
+//   * sphere-vs-box Boolean   collision/scene_collision.cuh:59-78
+//   * ESDF nearest lookup     collision/scene_collision.cuh:192-331
+// nvcc contracts `a*b + c*d` into fma(a, b, c*d) (the left product is fused,
+// the right one rounded). The FP32 expressions below spell that sequence out
+// with __fmaf_rn / __fmul_rn / __fadd_rn so it no longer depends on how the
+// compiler contracts this file; the GPU parity tests compare the results
+// bitwise against the reference kernels.
+//
+// Everything here is FP32 CUDA-core arithmetic: the 4x4 chains and the
+// per-pair distances are not dense contractions, so tensor cores do not apply.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/prism_b200.h"
+
+namespace ps {
+
+// ---------------------------------------------------------------------------
+// Model blob layout (device, one allocation, built by ps_model_create)
+// ---------------------------------------------------------------------------
+struct BlobHeader {          // 64 bytes
+    int n_dof, n_joints, n_spheres, n_approx;
+    int n_self_pairs, n_apx_self_pairs, approx_shares_chain, n_t_slots;
+    int off_joints, off_apx_joints, off_spheres, off_sph_orig;
+    int off_apx, off_apx_orig, bytes_core, bytes_total;
+};
+
+// One joint in DFS visit order (112 bytes).
+struct JointRec {
+    float ft[12];            // rows 0..2 of the fixed transform, row-major
+    int type, dof, parent_slot, slot;
+    int sph_beg, sph_end, apx_beg, apx_end;   // ranges into the reordered tables
+    float4 bound;            // link-frame point + radius enclosing every exact and
+                             // approximate sphere of the joint (w < 0: none)
+    int parent_pos;          // DFS position of the parent joint (root: 0)
+    int pad[3];
+};
+
+// Self pairs (global memory): packed (i | j << 16), reordered sphere indices.
+// Limits (global memory): lower[n_dof], upper[n_dof].
+struct ModelDev {
+    const unsigned char* blob;     // device
+    const uint32_t* self_pairs;    // device
+    const uint32_t* apx_self_pairs;// device
+    const float* lower;            // device
+    const float* upper;            // device
+    int* status;                   // device error latch
+    int bytes_core;
+};
+
+// ---------------------------------------------------------------------------
+// Prepared obstacle tables in shared memory
+// ---------------------------------------------------------------------------
+// Box o: l = R p + t is the world->box map of the reference's quaternion
+// formula (v + qw t + q x t, t = 2 q x v, which is linear in v), so R is that
+// map's matrix for the stored (possibly slightly non-unit) quaternion.
+struct ObbPrep {             // 80 bytes
+    float4 r0, r1, r2;       // rows of R, .w = translation (pose[0..2])
+    float4 h;                // half extents (dims * 0.5, exact), .w = |t|inf + |h|inf
+    float4 q;                // stored quaternion (qw, qx, qy, qz) for the exact path
+};
+
+struct LayerPrep {           // one ESDF layer, 64 bytes
+    float4 params;           // dx, dy, dz, voxel_size
+    float4 t;                // translation, .w = inv_vs
+    float4 q;                // qw, qx, qy, qz
+    int nx, ny, nz, enabled;
+};
+
+// Guard band of the fast sphere-vs-box path, in metres per metre of
+// coordinate magnitude: the fast map (3x3 matrix, 3 FMA per coordinate) and
+// the reference quaternion sequence differ by < 1.5e-5 m at the scales used
+// (|p|, |t| <= a few metres); the band is (S + B + 1) * PS_GUARD_K with
+// PS_GUARD_K = 2^-15 ~ 3.05e-5, leaving a 2x margin over a worst-case
+// rounding bound and >10x over typical errors. Pairs whose fast squared
+// distance lands inside the band are re-decided with the exact sequence.
+#define PS_GUARD_K 3.0517578125e-05f
+
+// ---------------------------------------------------------------------------
+// Exact reference arithmetic
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float fma_ab_cd(float a, float b, float c, float d) {
+    // a*b + c*d as nvcc contracts it: fma(a, b, rn(c*d))
+    return __fmaf_rn(a, b, __fmul_rn(c, d));
+}
+
+// transform_sphere_to_local (scene_collision.cuh:24-51), exact sequence.
+__device__ __forceinline__ void ref_to_local(float qw, float qx, float qy, float qz, float t0, float t1,
+                                             float t2, float sx, float sy, float sz, float& lx, float& ly,
+                                             float& lz) {
+    float tx = __fmul_rn(2.0f, __fmaf_rn(qy, sz, -__fmul_rn(qz, sy)));
+    float ty = __fmul_rn(2.0f, __fmaf_rn(qz, sx, -__fmul_rn(qx, sz)));
+    float tz = __fmul_rn(2.0f, __fmaf_rn(qx, sy, -__fmul_rn(qy, sx)));
+    float rx = __fadd_rn(__fmaf_rn(qw, tx, sx), __fmaf_rn(qy, tz, -__fmul_rn(qz, ty)));
+    float ry = __fadd_rn(__fmaf_rn(qw, ty, sy), __fmaf_rn(qz, tx, -__fmul_rn(qx, tz)));
+    float rz = __fadd_rn(__fmaf_rn(qw, tz, sz), __fmaf_rn(qx, ty, -__fmul_rn(qy, tx)));
+    lx = __fadd_rn(rx, t0);
+    ly = __fadd_rn(ry, t1);
+    lz = __fadd_rn(rz, t2);
+}
+
+// sphere_single_obb_collision (scene_collision.cuh:59-78), exact sequence;
+// also returns the squared outside distance it compared.
+__device__ __forceinline__ bool ref_obb_hit(const ObbPrep& o, float sx, float sy, float sz, float sr) {
+    float lx, ly, lz;
+    ref_to_local(o.q.x, o.q.y, o.q.z, o.q.w, o.r0.w, o.r1.w, o.r2.w, sx, sy, sz, lx, ly, lz);
+    float cx = fmaxf(0.0f, __fadd_rn(fabsf(lx), -o.h.x));
+    float cy = fmaxf(0.0f, __fadd_rn(fabsf(ly), -o.h.y));
+    float cz = fmaxf(0.0f, __fadd_rn(fabsf(lz), -o.h.z));
+    float dsq = __fmaf_rn(cz, cz, __fmaf_rn(cx, cx, __fmul_rn(cy, cy)));
+    return dsq < __fmul_rn(sr, sr);
+}
+
+// Sphere-sphere overlap (utils.cuh:239-267): sum - (ar+br)^2 < 0 with the
+// subtraction contracted, i.e. fma(-rs, rs, sum) < 0.
+__device__ __forceinline__ bool ref_self_hit(float ax, float ay, float az, float ar, float bx, float by,
+                                             float bz, float br) {
+    float xs = __fadd_rn(ax, -bx), ys = __fadd_rn(ay, -by), zs = __fadd_rn(az, -bz);
+    float sum = __fmaf_rn(zs, zs, __fmaf_rn(xs, xs, __fmul_rn(ys, ys)));
+    float rs = __fadd_rn(ar, br);
+    return __fmaf_rn(-rs, rs, sum) < 0.0f;
+}
+
+// ---------------------------------------------------------------------------
+// Forward kinematics: 3x4 affine per joint, held in registers.
+// ---------------------------------------------------------------------------
+struct Affine {
+    float m[12];   // row-major rows 0..2
+};
+
+__device__ __forceinline__ void affine_identity(Affine& T) {
+#pragma unroll
+    for (int k = 0; k < 12; ++k) T.m[k] = (k % 5 == 0) ? 1.0f : 0.0f;
+}
+
+// T_out = T_par * step(FT, type, q) with the reference's per-column formulas
+// and contraction (utils.cuh:571-711; runtime_kinematics.cuh:60-70). The
+// step's row 3 is (0,0,0,1) (validated at model creation), so the fourth
+// dot4 term is an exact +0 for rotation columns and +T_par[r][3] for the
+// translation column. fast_sincos selects __sinf/__cosf (reference, used by
+// every Boolean) or sincosf (accurate, used by the cost/gradient path).
+template <bool kFastSinCos>
+__device__ __forceinline__ void joint_compose(const JointRec& J, float qi, const Affine& P, Affine& O) {
+    float s[12];   // step rows 0..2
+#pragma unroll
+    for (int k = 0; k < 12; ++k) s[k] = J.ft[k];
+    const int type = J.type;
+    if (type >= PS_X_ROT) {
+        float sn, cs;
+        if (kFastSinCos) {
+            cs = __cosf(qi);
+            sn = __sinf(qi);
+        } else {
+            sincosf(qi, &sn, &cs);
+        }
+        const float nsn = -sn;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            const float f0 = J.ft[r * 4 + 0], f1 = J.ft[r * 4 + 1], f2 = J.ft[r * 4 + 2];
+            if (type == PS_Z_ROT) {
+                s[r * 4 + 0] = fma_ab_cd(f0, cs, sn, f1);
+                s[r * 4 + 1] = fma_ab_cd(f0, nsn, cs, f1);
+            } else if (type == PS_X_ROT) {
+                s[r * 4 + 1] = fma_ab_cd(f1, cs, sn, f2);
+                s[r * 4 + 2] = fma_ab_cd(f1, nsn, cs, f2);
+            } else {   // PS_Y_ROT
+                s[r * 4 + 0] = fma_ab_cd(f0, cs, nsn, f2);
+                s[r * 4 + 2] = fma_ab_cd(f0, sn, cs, f2);
+            }
+        }
+    } else if (type >= PS_X_PRISM) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r) s[r * 4 + 3] = __fmaf_rn(J.ft[r * 4 + type], qi, J.ft[r * 4 + 3]);
+    }
+    // PS_FIXED: step = FT
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const float p0 = P.m[r * 4 + 0], p1 = P.m[r * 4 + 1], p2 = P.m[r * 4 + 2], p3 = P.m[r * 4 + 3];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            float v = __fmaf_rn(p2, s[8 + c], __fmaf_rn(p0, s[c], __fmul_rn(p1, s[4 + c])));
+            O.m[r * 4 + c] = (c == 3) ? __fadd_rn(v, p3) : v;
+        }
+    }
+}
+
+// World position of a link-frame point (runtime_kinematics.cuh:79-83).
+__device__ __forceinline__ void sphere_world(const Affine& T, float x, float y, float z, float& px, float& py,
+                                             float& pz) {
+    px = __fadd_rn(__fmaf_rn(T.m[2], z, __fmaf_rn(T.m[0], x, __fmul_rn(T.m[1], y))), T.m[3]);
+    py = __fadd_rn(__fmaf_rn(T.m[6], z, __fmaf_rn(T.m[4], x, __fmul_rn(T.m[5], y))), T.m[7]);
+    pz = __fadd_rn(__fmaf_rn(T.m[10], z, __fmaf_rn(T.m[8], x, __fmul_rn(T.m[9], y))), T.m[11]);
+}
+
+// ---------------------------------------------------------------------------
+// Fast sphere-vs-box terms (free contraction; used for decisions only through
+// the guard band, and directly for clearance / cost values)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float fast_box_dsq(const ObbPrep& o, float px, float py, float pz, float& qx,
+                                              float& qy, float& qz) {
+    float lx = fmaf(o.r0.z, pz, fmaf(o.r0.y, py, fmaf(o.r0.x, px, o.r0.w)));
+    float ly = fmaf(o.r1.z, pz, fmaf(o.r1.y, py, fmaf(o.r1.x, px, o.r1.w)));
+    float lz = fmaf(o.r2.z, pz, fmaf(o.r2.y, py, fmaf(o.r2.x, px, o.r2.w)));
+    qx = fabsf(lx) - o.h.x;
+    qy = fabsf(ly) - o.h.y;
+    qz = fabsf(lz) - o.h.z;
+    float cx = fmaxf(qx, 0.0f), cy = fmaxf(qy, 0.0f), cz = fmaxf(qz, 0.0f);
+    return fmaf(cz, cz, fmaf(cy, cy, cx * cx));
+}
+
+// Decision thresholds for one sphere: definite hit if dsq < lo, definite
+// miss if dsq >= hi, else re-decide exactly. Bmax: max over boxes of
+// |t|inf + |h|inf.
+__device__ __forceinline__ void guard_thresholds(float px, float py, float pz, float sr, float Bmax, float& lo,
+                                                 float& hi) {
+    float S = fmaxf(fabsf(px), fmaxf(fabsf(py), fabsf(pz)));
+    float g = (S + Bmax + 1.0f) * PS_GUARD_K;
+    float a = fmaxf(sr - g, 0.0f), b = sr + g;
+    lo = a * a * (1.0f - 1.0e-6f);
+    hi = b * b * (1.0f + 1.0e-6f);
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory scene staging
+// ---------------------------------------------------------------------------
+struct SceneSmem {
+    const ObbPrep* obbs;       // compacted enabled boxes
+    const int* obb_orig;       // original index (ACM masks)
+    const LayerPrep* layers;
+    int n_obbs;                // enabled count
+    int n_layers;
+    float Bmax;
+};
+
+// stage_scene / stage_model live in ps_stage.cuh.
+
+// ---------------------------------------------------------------------------
+// ESDF lookup (nearest: exact reference sequence; trilinear: new mode)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int robust_floor_dev(float x) {
+    // robust_floor_scalar (scene_collision.cuh:192-200)
+    float nearest = roundf(x);
+    float diff = __fadd_rn(x, -nearest);
+    if (diff >= 1e-4f) return __float2int_rd(x);
+    return __float2int_rn(nearest);
+}
+
+// Returns true and the layer's distance ("positive = inside") if the sphere
+// centre maps to an observed voxel inside the 2-voxel guard.
+__device__ __forceinline__ bool esdf_sample(const LayerPrep& L, const float* feat, int max_vox, float px,
+                                            float py, float pz, int mode, float& dist) {
+    if (!L.enabled) return false;
+    float lx, ly, lz;
+    ref_to_local(L.q.x, L.q.y, L.q.z, L.q.w, L.t.x, L.t.y, L.t.z, px, py, pz, lx, ly, lz);
+    const float inv_vs = L.t.w;
+    const int B = 2;
+    if (mode == PS_ESDF_NEAREST) {
+        int ix = (int)__fmul_rn(__fmaf_rn(L.params.x, 0.5f, lx), inv_vs);
+        int iy = (int)__fmul_rn(__fmaf_rn(L.params.y, 0.5f, ly), inv_vs);
+        int iz = (int)__fmul_rn(__fmaf_rn(L.params.z, 0.5f, lz), inv_vs);
+        if (ix >= L.nx - B || iy >= L.ny - B || iz >= L.nz - B || ix <= B || iy <= B || iz <= B) return false;
+        long long li = (long long)ix * L.ny * L.nz + (long long)iy * L.nz + iz;
+        if (li >= max_vox) return false;
+        float d = __ldg(feat + li);
+        if (d <= -999.0f) return false;
+        dist = d;
+        return true;
+    }
+    float gx = (lx + L.params.x * 0.5f) * inv_vs;
+    float gy = (ly + L.params.y * 0.5f) * inv_vs;
+    float gz = (lz + L.params.z * 0.5f) * inv_vs;
+    float fx0 = floorf(gx), fy0 = floorf(gy), fz0 = floorf(gz);
+    if (!(fx0 > (float)B && fy0 > (float)B && fz0 > (float)B && fx0 + 1.0f < (float)(L.nx - B) &&
+          fy0 + 1.0f < (float)(L.ny - B) && fz0 + 1.0f < (float)(L.nz - B)))
+        return false;
+    int ix = (int)fx0, iy = (int)fy0, iz = (int)fz0;
+    long long base = (long long)ix * L.ny * L.nz + (long long)iy * L.nz + iz;
+    long long sx = (long long)L.ny * L.nz, sy = L.nz;
+    if (base + sx + sy + 1 >= max_vox) return false;
+    float v[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        v[c] = __ldg(feat + base + ((c & 1) ? sx : 0) + ((c & 2) ? sy : 0) + ((c & 4) ? 1 : 0));
+        if (v[c] <= -999.0f) return false;
+    }
+    float fx = gx - fx0, fy = gy - fy0, fz = gz - fz0;
+    float x00 = v[0] + fx * (v[1] - v[0]), x10 = v[2] + fx * (v[3] - v[2]);
+    float x01 = v[4] + fx * (v[5] - v[4]), x11 = v[6] + fx * (v[7] - v[6]);
+    float y0 = x00 + fy * (x10 - x00), y1 = x01 + fy * (x11 - x01);
+    dist = y0 + fz * (y1 - y0);
+    return true;
+}
+
+// Latch an error code into the model's status word (first error wins).
+__device__ __forceinline__ void latch_status(int* status, int code) {
+    if (status) atomicCAS(status, 0, code);
+}
+
+}  // namespace ps

@@ -1,0 +1,43 @@
+// ps_internal.h -- host-side internals shared by the C-ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "ps_common.cuh"
+
+// Host handle behind the opaque ps_model*.
+struct ps_model {
+    ps::ModelDev dev{};
+    void* alloc = nullptr;      // single device allocation
+    size_t alloc_bytes = 0;
+    ps_model_info info{};
+    int max_joint_spheres = 0;  // most exact spheres on one joint
+    int max_joint_approx = 0;
+    std::vector<int> sph_orig;  // reordered -> descriptor index (host copy)
+};
+
+namespace ps {
+
+int set_error(int code, const std::string& msg);
+int cuda_error(cudaError_t e, const char* where);
+void clear_error();
+
+// Validate a scene view against a model; returns PS_OK or sets the error.
+int validate_scene(const ps_model* m, const ps_scene_view* s);
+
+// Dynamic shared memory needed to stage model core + scene tables.
+size_t scene_smem_bytes(const ps_scene_view* s);
+
+// Number of SMs of the current device (cached).
+int sm_count();
+
+}  // namespace ps
+
+#define PS_TRY_CUDA(expr)                                        \
+    do {                                                         \
+        cudaError_t _e = (expr);                                 \
+        if (_e != cudaSuccess) return ps::cuda_error(_e, #expr); \
+    } while (0)

@@ -1,0 +1,98 @@
+// ps_stage.cuh -- shared-memory staging of the model core and the scene.
+#pragma once
+
+#include "ps_common.cuh"
+
+namespace ps {
+
+// Builds the prepared box table (compacted enabled boxes, 3x3 maps, exact
+// half extents) and the ESDF layer headers from the caller's
+// SceneCollisionData arrays. Call with all threads; ends with __syncthreads().
+__device__ __forceinline__ void stage_scene(const ps_scene_view& sv, ObbPrep* obbs, int* orig, LayerPrep* layers, int* counters,
+                            float* bmax_slot, SceneSmem& out) {
+    if (threadIdx.x == 0) {
+        counters[0] = 0;
+        *bmax_slot = 0.0f;
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < sv.n_obbs; o += blockDim.x) {
+        if (sv.obb_enable[o] == 0) continue;
+        const float4 dm = reinterpret_cast<const float4*>(sv.obb_dims)[o];
+        const float4 pa = reinterpret_cast<const float4*>(sv.obb_pose)[2 * o];      // tx ty tz qw
+        const float4 pb = reinterpret_cast<const float4*>(sv.obb_pose)[2 * o + 1];  // qx qy qz pad
+        const float qw = pa.w, qx = pb.x, qy = pb.y, qz = pb.z;
+        ObbPrep p;
+        // Matrix of v -> v + qw t + q x t, t = 2 q x v.
+        p.r0 = make_float4(1.0f - 2.0f * (qy * qy + qz * qz), 2.0f * (qx * qy - qw * qz), 2.0f * (qx * qz + qw * qy), pa.x);
+        p.r1 = make_float4(2.0f * (qx * qy + qw * qz), 1.0f - 2.0f * (qx * qx + qz * qz), 2.0f * (qy * qz - qw * qx), pa.y);
+        p.r2 = make_float4(2.0f * (qx * qz - qw * qy), 2.0f * (qy * qz + qw * qx), 1.0f - 2.0f * (qx * qx + qy * qy), pa.z);
+        const float hx = dm.x * 0.5f, hy = dm.y * 0.5f, hz = dm.z * 0.5f;
+        const float B = fmaxf(fmaxf(fabsf(pa.x), fmaxf(fabsf(pa.y), fabsf(pa.z))), fmaxf(hx, fmaxf(hy, hz)));
+        p.h = make_float4(hx, hy, hz, B);
+        p.q = make_float4(qw, qx, qy, qz);
+        int slot = atomicAdd(&counters[0], 1);
+        obbs[slot] = p;
+        orig[slot] = o;
+        atomicMax(reinterpret_cast<int*>(bmax_slot), __float_as_int(B));   // B >= 0: int order == float order
+    }
+    for (int l = threadIdx.x; l < sv.n_voxel_layers; l += blockDim.x) {
+        LayerPrep L;
+        const float4 pr = reinterpret_cast<const float4*>(sv.voxel_params)[l];
+        const float4 pa = reinterpret_cast<const float4*>(sv.voxel_pose)[2 * l];
+        const float4 pb = reinterpret_cast<const float4*>(sv.voxel_pose)[2 * l + 1];
+        L.params = pr;
+        L.enabled = (sv.voxel_enable[l] != 0) && (pr.w > 0.0f);
+        const float inv_vs = pr.w > 0.0f ? __fdiv_rn(1.0f, pr.w) : 0.0f;
+        L.t = make_float4(pa.x, pa.y, pa.z, inv_vs);
+        L.q = make_float4(pa.w, pb.x, pb.y, pb.z);
+        L.nx = robust_floor_dev(__fmul_rn(pr.x, inv_vs)) + 1;
+        L.ny = robust_floor_dev(__fmul_rn(pr.y, inv_vs)) + 1;
+        L.nz = robust_floor_dev(__fmul_rn(pr.z, inv_vs)) + 1;
+        layers[l] = L;
+    }
+    __syncthreads();
+    out.obbs = obbs;
+    out.obb_orig = orig;
+    out.layers = layers;
+    out.n_obbs = counters[0];
+    out.n_layers = sv.n_voxel_layers;
+    out.Bmax = *bmax_slot;
+    __syncthreads();
+}
+
+// Copies the model core (header + joint and sphere tables) into shared memory
+// with one bulk async copy (cp.async.bulk, completion on an mbarrier, bounded
+// wait). Returns false on timeout (status latched). Call with all threads.
+__device__ __forceinline__ bool stage_model(const ModelDev& md, unsigned char* smem_blob, uint64_t* mbar) {
+    const uint32_t bytes = (uint32_t)md.bytes_core;
+    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(mbar);
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(smem_blob);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+            "l"(md.blob), "r"(bytes), "r"(bar)
+            : "memory");
+    }
+    // Bounded wait on phase 0: ~2^22 polls, each try_wait may suspend for a
+    // hardware-defined interval. On expiry latch PS_ETIMEOUT and give up.
+    uint32_t done = 0;
+    for (int it = 0; it < (1 << 22) && !done; ++it) {
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(bar)
+            : "memory");
+    }
+    int ok = __syncthreads_and((int)done);
+    if (!ok && threadIdx.x == 0) latch_status(md.status, PS_ETIMEOUT);
+    return ok != 0;
+}
+
+}  // namespace ps

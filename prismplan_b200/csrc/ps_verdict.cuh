@@ -1,0 +1,222 @@
+// ps_verdict.cuh -- per-lane collision verdicts (one configuration per lane).
+//
+// Semantics are two_phase_cc's (code/gpu_planning/cpp/src/collision/
+// two_phase_cc.cuh:57-138) for one configuration: the approximate spheres of
+// joint j are tested against the scene (OBBs + ESDF, radius + margin,
+// scene_collision.cuh:584-631); if any hits, joint j is flagged and its exact
+// spheres are tested (scene_collision.cuh:519-567). The configuration
+// collides iff some exact sphere of a flagged joint hits. The order of the
+// tests does not change that OR, so the kernels test joint by joint during the
+// FK walk and stop at the first confirmed hit.
+#pragma once
+
+#include "ps_common.cuh"
+#include "ps_stage.cuh"
+
+namespace ps {
+
+// Diagnostic counters (device, optional): executed work for the roofline.
+enum StatSlot {
+    ST_PAIRS = 0,        // sphere-vs-box pair tests (fast path)
+    ST_EXACT = 1,        // pairs re-decided with the exact reference sequence
+    ST_SAMPLES = 2,      // configurations / samples evaluated
+    ST_JOINTS = 3,       // FK joint steps
+    ST_SPHERES = 4,      // sphere transforms
+    ST_SELF = 5,         // self pair tests
+    ST_ESDF = 6,         // ESDF lookups
+    ST_CULL = 7,         // broad-phase box tests
+    ST_COUNT = 8
+};
+
+struct LaneStats {
+    unsigned int v[ST_COUNT];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int k = 0; k < ST_COUNT; ++k) v[k] = 0;
+    }
+};
+
+// Block-reduce the lane counters and add them with one atomic per slot.
+__device__ __forceinline__ void flush_stats(unsigned long long* stats, LaneStats& ls) {
+    if (!stats) return;
+#pragma unroll
+    for (int k = 0; k < ST_COUNT; ++k) {
+        unsigned int x = ls.v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0 && x) atomicAdd(stats + k, (unsigned long long)x);
+    }
+}
+
+// Shared-memory view of the staged model core.
+struct ModelSmem {
+    const BlobHeader* H;
+    const JointRec* J;      // full chain, DFS order
+    const JointRec* JA;     // approx chain (== J when shared)
+    const float4* S;        // exact spheres, reordered
+    const int* SO;          // reordered -> descriptor index
+    const float4* A;        // approx spheres, reordered
+    const int* AO;
+};
+
+__device__ __forceinline__ ModelSmem model_view(const unsigned char* blob) {
+    ModelSmem m;
+    m.H = reinterpret_cast<const BlobHeader*>(blob);
+    m.J = reinterpret_cast<const JointRec*>(blob + m.H->off_joints);
+    m.JA = m.H->approx_shares_chain ? m.J : reinterpret_cast<const JointRec*>(blob + m.H->off_apx_joints);
+    m.S = reinterpret_cast<const float4*>(blob + m.H->off_spheres);
+    m.SO = reinterpret_cast<const int*>(blob + m.H->off_sph_orig);
+    m.A = reinterpret_cast<const float4*>(blob + m.H->off_apx);
+    m.AO = reinterpret_cast<const int*>(blob + m.H->off_apx_orig);
+    return m;
+}
+
+// Any box hit for one sphere with bit-exact decisions. `cand`/`ncand`
+// optionally restrict the boxes (a conservative broad phase); acm_row is the
+// sphere's row of an OBB ACM mask (global memory) or NULL.
+__device__ __forceinline__ bool sphere_obb_any(const SceneSmem& sc, const uint16_t* cand, int ncand, float px,
+                                               float py, float pz, float sr, const uint8_t* acm_row,
+                                               LaneStats& st) {
+    float lo, hi;
+    guard_thresholds(px, py, pz, sr, sc.Bmax, lo, hi);
+    const int n = cand ? ncand : sc.n_obbs;
+    float mn = 3.0e38f;
+    for (int k = 0; k < n; ++k) {
+        const int o = cand ? (int)cand[k] : k;
+        if (acm_row && acm_row[sc.obb_orig[o]] == 0) continue;
+        float qx, qy, qz;
+        float d = fast_box_dsq(sc.obbs[o], px, py, pz, qx, qy, qz);
+        mn = fminf(mn, d);
+    }
+    st.v[ST_PAIRS] += n;
+    if (mn < lo) return true;
+    if (mn >= hi) return false;
+    // Some box sits inside the guard band: re-decide those exactly.
+    for (int k = 0; k < n; ++k) {
+        const int o = cand ? (int)cand[k] : k;
+        if (acm_row && acm_row[sc.obb_orig[o]] == 0) continue;
+        float qx, qy, qz;
+        float d = fast_box_dsq(sc.obbs[o], px, py, pz, qx, qy, qz);
+        if (d < lo) return true;
+        if (d < hi) {
+            st.v[ST_EXACT] += 1;
+            if (ref_obb_hit(sc.obbs[o], px, py, pz, sr)) return true;
+        }
+    }
+    return false;
+}
+
+// Min over boxes of the box SDF of a point (world), no radius. The square
+// root and the inside term are taken once per sphere, not per pair:
+// SDF = sqrt(min outside d^2) when the centre is outside every box, else the
+// most negative max(q) over the boxes that contain it. Also returns min d^2.
+__device__ __forceinline__ float sphere_obb_min_sdf(const SceneSmem& sc, float px, float py, float pz,
+                                                    const uint8_t* acm_row, float& min_dsq, bool& any_box,
+                                                    LaneStats& st) {
+    float mn = 3.0e38f;
+    any_box = false;
+    for (int o = 0; o < sc.n_obbs; ++o) {
+        if (acm_row && acm_row[sc.obb_orig[o]] == 0) continue;
+        float qx, qy, qz;
+        mn = fminf(mn, fast_box_dsq(sc.obbs[o], px, py, pz, qx, qy, qz));
+        any_box = true;
+    }
+    st.v[ST_PAIRS] += sc.n_obbs;
+    min_dsq = mn;
+    if (!any_box) return 1000.0f;
+    if (mn > 0.0f) return sqrtf(mn);
+    float inside = 0.0f;
+    for (int o = 0; o < sc.n_obbs; ++o) {
+        if (acm_row && acm_row[sc.obb_orig[o]] == 0) continue;
+        float qx, qy, qz;
+        float d = fast_box_dsq(sc.obbs[o], px, py, pz, qx, qy, qz);
+        if (d == 0.0f) inside = fminf(inside, fmaxf(qx, fmaxf(qy, qz)));
+    }
+    return inside;
+}
+
+// Decision from a precomputed min d^2 (clearance path): exact rescan only
+// inside the guard band.
+__device__ __forceinline__ bool decide_from_min(const SceneSmem& sc, float px, float py, float pz, float sr,
+                                                float min_dsq, const uint8_t* acm_row, LaneStats& st) {
+    float lo, hi;
+    guard_thresholds(px, py, pz, sr, sc.Bmax, lo, hi);
+    if (min_dsq < lo) return true;
+    if (min_dsq >= hi) return false;
+    for (int o = 0; o < sc.n_obbs; ++o) {
+        if (acm_row && acm_row[sc.obb_orig[o]] == 0) continue;
+        float qx, qy, qz;
+        float d = fast_box_dsq(sc.obbs[o], px, py, pz, qx, qy, qz);
+        if (d < lo) return true;
+        if (d < hi) {
+            st.v[ST_EXACT] += 1;
+            if (ref_obb_hit(sc.obbs[o], px, py, pz, sr)) return true;
+        }
+    }
+    return false;
+}
+
+// ESDF any-collision / clearance for one sphere over all layers
+// (scene_collision.cuh:202-331). acm: sphere_acm_mask row or NULL.
+__device__ __forceinline__ bool sphere_esdf_any(const SceneSmem& sc, const ps_scene_view& sv, float px, float py,
+                                                float pz, float sr, const uint8_t* acm_row, LaneStats& st) {
+    for (int l = 0; l < sc.n_layers; ++l) {
+        if (acm_row && acm_row[l] == 0) continue;
+        float d;
+        st.v[ST_ESDF] += 1;
+        if (!esdf_sample(sc.layers[l], sv.voxel_features + (size_t)l * sv.max_voxels_per_layer,
+                         sv.max_voxels_per_layer, px, py, pz, sv.esdf_mode, d))
+            continue;
+        if (d > -sr) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ float sphere_esdf_clearance(const SceneSmem& sc, const ps_scene_view& sv, float px,
+                                                       float py, float pz, float sr, const uint8_t* acm_row,
+                                                       LaneStats& st) {
+    float best = 1000.0f;
+    for (int l = 0; l < sc.n_layers; ++l) {
+        if (acm_row && acm_row[l] == 0) continue;
+        float d;
+        st.v[ST_ESDF] += 1;
+        if (!esdf_sample(sc.layers[l], sv.voxel_features + (size_t)l * sv.max_voxels_per_layer,
+                         sv.max_voxels_per_layer, px, py, pz, sv.esdf_mode, d))
+            continue;
+        best = fminf(best, __fadd_rn(-d, -sr));
+    }
+    return best;
+}
+
+// Select a slot by uniform index.
+__device__ __forceinline__ void select_slot(const Affine& s0, const Affine& s1, int k, Affine& out) {
+#pragma unroll
+    for (int i = 0; i < 12; ++i) out.m[i] = k ? s1.m[i] : s0.m[i];
+}
+
+__device__ __forceinline__ void store_slot(Affine& s0, Affine& s1, int k, const Affine& v) {
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        if (k) s1.m[i] = v.m[i];
+        else s0.m[i] = v.m[i];
+    }
+}
+
+// Frame of DFS position p given the parent slots (the reference FK walk).
+template <bool kFast>
+__device__ __forceinline__ void fk_step(const JointRec& jr, int p, const float* q, Affine& s0, Affine& s1,
+                                        Affine& T) {
+    if (p == 0) {
+        // Both slots start as the identity (runtime_kinematics.cuh:31-37);
+        // the first visited joint keeps it.
+        affine_identity(T);
+    } else {
+        Affine P;
+        select_slot(s0, s1, jr.parent_slot, P);
+        const float qi = jr.dof >= 0 ? q[jr.dof] : 0.0f;
+        joint_compose<kFast>(jr, qi, P, T);
+    }
+    store_slot(s0, s1, jr.slot, T);
+}
+
+}  // namespace ps
