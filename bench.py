@@ -1,0 +1,482 @@
+"""Benchmark: checked configurations/s on the batched uneven-edge workload.
+
+Workload (one "step"): 65,536 edges of a 7-revolute Panda-like chain (59
+spheres) against 64 OBBs, each discretised at an L-inf joint step of 0.01 rad
+(1..600 samples, t = j/G, j = 1..G), any-collision per edge with early exit,
+evaluated by the persistent chunk-major work-queue kernel replayed from a
+CUDA graph. Metric: checked configurations/s = sum over edges of G (the
+samples each edge verdict covers) per second, whole job, max over ranks.
+
+Arms:
+  python bench.py [--gpus N --steps K --warmup W]      this implementation
+  python bench.py --impl reference ...                 the reference path's
+      FP32 host restatement (oracle/, the reference has no CPU path of its
+      own) on all host cores, same workload and metric.
+Under torchrun (N > 1) every rank runs its own seeded copy of the workload
+(weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "checked configs/s (batched uneven edge checks, persistent graph-captured)"
+UNIT = "configs/s"
+WORKLOAD = "edges_panda7_obb64_e65536_linf0.01"
+STEP_RAD = 0.01
+MAX_SAMPLES = 600
+
+# Algorithmic flop model (FMA = 2, compare / max / abs-add = 1):
+FLOP_JOINT = 90      # FT*motion(q) 18 + 3x4 affine compose 72
+FLOP_SPHERE = 18     # sphere centre transform
+FLOP_PAIR = 30       # sphere-vs-box: rotate+translate 18, |l|-h 3, max 3, d^2 5, cmp 1
+FLOP_CULL = 30       # broad-phase box test (same arithmetic as a pair)
+FLOP_SELF = 10
+
+
+def flops_from_stats(st):
+    """st: [pairs, exact, samples, joints, spheres, self, esdf, cull]."""
+    return (st[0] * FLOP_PAIR + st[1] * FLOP_PAIR + st[3] * FLOP_JOINT + st[4] * FLOP_SPHERE
+            + st[5] * FLOP_SELF + st[7] * FLOP_CULL)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, device: int):
+        import torch
+
+        p = torch.cuda.get_device_properties(device)
+        self.index = f"GPU-{p.uuid}"
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_edge_case(rank: int):
+    from prismplan_b200 import workloads
+    from prismplan_b200.robot import RobotModelBuilder
+    from prismplan_b200.scene import SceneTensors
+
+    wl = workloads.workload(2)
+    if rank:
+        rng = np.random.default_rng(1002 + 7919 * rank)
+        frm, to, G = workloads.edge_batch(rng, wl["asset"], len(wl["from"]))
+        wl.update({"from": frm, "to": to, "G": G})
+    b = RobotModelBuilder.from_asset(wl["asset"]).build()
+    sc = SceneTensors(*wl["obbs"])
+    return wl, b, sc
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from prismplan_b200 import _lib, api
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    wl, b, sc = build_edge_case(rank)
+    E = len(wl["from"])
+    total_samples = int(wl["G"].sum())
+    dev = torch.device("cuda", local)
+    frm = torch.from_numpy(wl["from"]).to(dev)
+    to = torch.from_numpy(wl["to"]).to(dev)
+    params = api.EdgeEvalParams(max_joint_step=STEP_RAD, max_samples=MAX_SAMPLES)
+    wsb = api.edges_workspace(E, dev)
+    out = (torch.empty(E, dtype=torch.uint8, device=dev), torch.empty(E, device=dev), torch.empty(E, device=dev))
+    stream = torch.cuda.Stream(device=dev)
+    lib = _lib.load()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)   # > 126 MB L2
+
+    with torch.cuda.stream(stream):
+        api.check_edges(b, sc, frm, to, params=params, workspace=wsb, out=out, stream=stream)
+    stream.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    ev_k0 = torch.cuda.Event(enable_timing=True)
+    ev_k1 = torch.cuda.Event(enable_timing=True)
+    ev_k0.record(stream)   # torch creates the underlying events lazily
+    ev_k1.record(stream)
+    stream.synchronize()
+    lib.ps_set_timing_events(ev_k0.cuda_event, ev_k1.cuda_event)
+    with torch.cuda.graph(graph, stream=stream):
+        api.check_edges(b, sc, frm, to, params=params, workspace=wsb, out=out, stream=stream)
+    lib.ps_set_timing_events(None, None)
+
+    for _ in range(args.warmup):
+        graph.replay()
+    torch.cuda.synchronize()
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    kern_ms = []
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(k & 0xff)                 # evict L2 between steps (outside the events)
+                ev0[k].record(stream)
+                graph.replay()
+                ev1[k].record(stream)
+            ev1[k].synchronize()
+            kern_ms.append(ev_k0.elapsed_time(ev_k1))
+        torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(c) for a, c in zip(ev0, ev1)]
+    t_total = sum(step_ms)
+    job_samples = total_samples
+    if ws > 1:
+        tt = torch.tensor([t_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_total = float(tt.item())
+        ns = torch.tensor([total_samples], device=dev, dtype=torch.float64)
+        dist.all_reduce(ns, op=dist.ReduceOp.SUM)
+        job_samples = int(ns.item())
+        dist.barrier()
+    valid_frac = float(out[0].float().mean().item())
+    del graph
+
+    result = None
+    if rank == 0:
+        value = job_samples * args.steps / (t_total * 1e-3)
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "edges": E, "samples_per_step": total_samples,
+                       "samples_rule": f"G=clamp(ceil(Linf/{STEP_RAD}),1,{MAX_SAMPLES})",
+                       "robot": "panda-like 7R, 59 spheres", "obbs": 64, "valid_fraction": valid_frac,
+                       "l2": "flushed between steps (256 MiB write)", "parallelism": f"shard{ws}"},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clk.summary(),
+            "edges_per_s": ws * E * args.steps / (t_total * 1e-3),
+        }
+        if args.headline_only:
+            result["roofline"] = {"kernel": "edges_queue_kernel", "kernel_ms": statistics.median(kern_ms)}
+        else:
+            result.update(secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev))
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev):
+    """Roofline, e2e, CPU baseline and the comparison paths (rank 0, N=1 data)."""
+    import ctypes
+
+    import torch
+
+    from prismplan_b200 import _lib, api
+
+    lib = _lib.load()
+    E = len(wl["from"])
+    total_samples = int(wl["G"].sum())
+    res = {}
+    # ---- executed work of one launch (counters) ----
+    st = torch.zeros(8, dtype=torch.int64, device=dev)
+    lib.ps_set_stats(ctypes.c_void_p(st.data_ptr()))
+    api.check_edges(b, sc, frm, to, params=params)
+    torch.cuda.synchronize()
+    lib.ps_set_stats(None)
+    stats = [int(x) for x in st.cpu().tolist()]
+    flops = flops_from_stats(stats)
+    peak = probe_peak()
+    k_ms = statistics.median(kern_ms) if kern_ms else None
+    achieved = flops / (k_ms * 1e-3) / 1e12 if k_ms else None
+    res["roofline"] = {
+        "bound": "fp32", "achieved": achieved, "peak": peak["tflops"], "unit": "TFLOP/s",
+        "frac": (achieved / peak["tflops"]) if achieved and peak["tflops"] else None,
+        "traffic": traffic_from_profiles("edges_queue_kernel"),
+        "kernel": "edges_queue_kernel", "kernel_ms": k_ms,
+        "peak_source": peak["source"], "flops_per_launch": flops,
+        "work_per_launch": dict(zip(["pairs", "exact", "samples", "joints", "spheres", "self", "esdf", "cull"], stats)),
+    }
+    # ---- e2e through the reference-facing bridge (host buffers) ----
+    ev = api.EdgeEvalGpu(7, E, sc, b)
+    ff = wl["from"].reshape(-1)
+    tt = wl["to"].reshape(-1)
+    for _ in range(3):
+        ev.evaluate(ff, tt, E, params)
+    t0 = time.perf_counter()
+    n_e2e = max(3, args.steps // 2)
+    for _ in range(n_e2e):
+        ev.evaluate(ff, tt, E, params)
+    dt = (time.perf_counter() - t0) / n_e2e
+    res["e2e"] = {"value": total_samples / dt, "unit": UNIT, "h2d_bytes_per_step": 2 * E * 7 * 4,
+                  "d2h_bytes_per_step": E * (1 + 4), "ms_per_step": dt * 1e3,
+                  "api": "prismplan_b200.EdgeEvalGpu.evaluate (pinned H2D + kernels + D2H + sync)"}
+    # ---- plain per-call path (one warp per edge, no queue, no graph) ----
+    v_pl = None
+    for _ in range(2):
+        api.check_edges(b, sc, frm, to, params=params, persistent=False)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        v_pl, _, _ = api.check_edges(b, sc, frm, to, params=params, persistent=False)
+    e1.record()
+    torch.cuda.synchronize()
+    pl_ms = e0.elapsed_time(e1) / 5
+    res["plain"] = {"value": total_samples / (pl_ms * 1e-3), "unit": UNIT, "ms_per_step": pl_ms,
+                    "path": "ps_check_edges_plain (one warp per edge, direct launch)"}
+    # ---- the reference's own kernels (plain GPU path), same inputs ----
+    res["reference_gpu"] = reference_gpu_edges(b, wl)
+    # ---- CPU baseline (oracle port, FP32, all host threads, bounded sample) ----
+    res["cpu_baseline"] = cpu_baseline(b, wl)
+    # ---- other workloads: configs (1) and CHOMP cost+gradient (3) ----
+    res["configs"] = bench_configs(dev)
+    res["chomp"] = bench_chomp(dev)
+    return res
+
+
+def probe_peak():
+    import ctypes
+
+    from prismplan_b200 import _lib
+
+    v = ctypes.c_double(0)
+    best = 0.0
+    for _ in range(3):
+        _lib.check(_lib.load().ps_probe_fp32_peak(ctypes.byref(v), None))
+        best = max(best, v.value)
+    return {"tflops": best / 1e12,
+            "source": "measured live: FP32 FMA probe (ps_probe_fp32_peak); MEASURED_PEAKS.json has no FP32 figure"}
+
+
+def traffic_from_profiles(kernel):
+    p = ROOT / "profiles" / f"{kernel}.traffic.json"
+    if p.is_file():
+        try:
+            return json.loads(p.read_text()).get("bytes_per_launch")
+        except Exception:
+            return None
+    return None
+
+
+def reference_gpu_edges(b, wl):
+    try:
+        import oracle
+
+        ref = oracle.RefKernels(b, *wl["obbs"])
+        n = len(wl["from"])
+        v, c, ms = ref.check_edges(wl["from"], wl["to"], wl["G"], reps=1)
+        return {"value": int(wl["G"].sum()) / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+                "path": "evaluate_edges_batch<<<E_G,64>>> per distinct G (reference kernels, sm_100a)",
+                "valid_fraction": float(v.mean())}
+    except Exception as e:   # harness absent
+        return {"unavailable": str(e)[:200]}
+
+
+def cpu_baseline(b, wl, target_s=8.0):
+    import oracle
+
+    om = oracle.OracleModel(b, *wl["obbs"])
+    threads = oracle.default_threads()
+    n = 2048
+    frm, to, G = wl["from"], wl["to"], wl["G"]
+    t0 = time.perf_counter()
+    om.check_edges(frm[:n], to[:n], G[:n], prec=32, threads=threads)
+    dt = time.perf_counter() - t0
+    n2 = int(min(len(frm), max(n, n * target_s / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    om.check_edges(frm[:n2], to[:n2], G[:n2], prec=32, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": float(G[:n2].sum()) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {n2} of {len(frm)} edges, FP32 restatement with early exit, {dt:.1f} s"}
+
+
+def bench_configs(dev):
+    import torch
+
+    from prismplan_b200 import api, workloads
+    from prismplan_b200.robot import RobotModelBuilder
+    from prismplan_b200.scene import SceneTensors
+
+    wl = workloads.workload(1)
+    b = RobotModelBuilder.from_asset(wl["asset"]).build()
+    sc = SceneTensors(*wl["obbs"])
+    q = torch.from_numpy(np.tile(wl["q"], (256, 1))).to(dev)   # 1M configurations: steady state
+    for _ in range(3):
+        api.check_configs(b, sc, q, clearance="obb")
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        api.check_configs(b, sc, q, clearance="obb")
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 5
+    out = {"workload": "configs_panda7_obb16 (4096 tiled to 1,048,576)", "value": q.shape[0] / (ms * 1e-3),
+           "unit": "configs/s", "ms_per_step": ms, "outputs": "hit + OBB min-clearance"}
+    try:
+        import oracle
+
+        ref = oracle.RefKernels(b, *wl["obbs"])
+        ref.check_configs(wl["q"][:256])
+        _, rms = ref.check_configs(wl["q"])
+        out["reference_gpu"] = {"value": len(wl["q"]) / (rms * 1e-3), "unit": "configs/s",
+                                "path": "pRRTC::check_collision_scene (malloc+copy+<<<N,4>>>+sync)"}
+    except Exception as e:
+        out["reference_gpu"] = {"unavailable": str(e)[:200]}
+    return out
+
+
+def bench_chomp(dev):
+    import torch
+
+    from prismplan_b200 import api, workloads
+    from prismplan_b200.robot import RobotModelBuilder
+    from prismplan_b200.scene import SceneTensors
+
+    wl = workloads.workload(3)
+    b = RobotModelBuilder.from_asset(wl["asset"]).build()
+    sc = SceneTensors(*wl["obbs"])
+    q = torch.from_numpy(wl["q"]).to(dev)
+    p = api.CostParams(collision_cost_weight=wl["w"], world_collision_margin=wl["eps"],
+                       self_collision_margin=wl["self_margin"], smoothness_weight=1.0, delta_t=wl["delta_t"])
+    for _ in range(3):
+        api.traj_cost(b, sc, q, p)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        api.traj_cost(b, sc, q, p)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 10
+    B = q.shape[0]
+    out = {"workload": "chomp_panda7_obb64_b256_t64", "value": B / (ms * 1e-3), "unit": "traj/s",
+           "ms_per_step": ms, "path": "fused FK + hinge + adjoint + smoothness (ps_traj_cost)"}
+    try:
+        import oracle
+
+        ref = oracle.RefKernels(b, *wl["obbs"])
+        th = wl["q"].transpose(0, 2, 1)
+        ref.chomp(th[:4], wl["w"], wl["eps"], wl["self_margin"])
+        _, _, rms = ref.chomp(th, wl["w"], wl["eps"], wl["self_margin"], reps=1)
+        out["reference_gpu"] = {"value": B / (rms * 1e-3), "unit": "traj/s", "ms_per_step": rms,
+                                "path": "chomp_state_cost_kernel + chomp_obs_grad_kernel per trajectory"}
+        out["speedup_vs_reference"] = rms / ms
+    except Exception as e:
+        out["reference_gpu"] = {"unavailable": str(e)[:200]}
+    return out
+
+
+def run_reference(args):
+    """Reference arm: the FP32 host restatement of the reference path on all
+    host cores, same workload/metric; rank 0 only."""
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return None
+    import oracle
+
+    from prismplan_b200 import workloads
+    from prismplan_b200.robot import RobotModelBuilder
+
+    wl = workloads.workload(2)
+    b = RobotModelBuilder.from_asset(wl["asset"])
+    om = oracle.OracleModel(b, *wl["obbs"])
+    threads = oracle.default_threads()
+    n = 4096
+    frm, to, G = wl["from"][:n], wl["to"][:n], wl["G"][:n]
+    for _ in range(max(0, min(args.warmup, 1))):
+        om.check_edges(frm, to, G, prec=32, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        om.check_edges(frm, to, G, prec=32, threads=threads)
+        times.append(time.perf_counter() - t0)
+    t = sum(times)
+    value = float(G.sum()) * args.steps / t
+    sample = f"first {n} of 65536 edges per step (FP32 restatement, early exit)"
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "edges_per_step": n, "parallelism": "host threads"},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="time the headline path only (profiling runs); skips roofline/e2e/baselines")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    res = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -278,6 +278,13 @@ int ps_probe_fp32_peak(double* flops_per_s, void* stream);
    (the default) disables counting. No reference counterpart. */
 int ps_set_stats(unsigned long long* dev_counters);
 
+/* Kernel timing hook: when both are non-NULL (cudaEvent_t as void*), each
+   ps_check_configs / ps_check_edges / ps_check_edges_plain / ps_traj_cost /
+   ps_rollout_costs call records `start` immediately before and `stop`
+   immediately after its main kernel, on the call's stream (also inside a
+   captured graph). Process-wide, not thread-safe; NULL disables. */
+int ps_set_timing_events(void* start, void* stop);
+
 #ifdef __cplusplus
 }
 #endif

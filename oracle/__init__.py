@@ -180,3 +180,155 @@ def control_cost_R(T: int, dt: float) -> np.ndarray:
     R = np.zeros((T, T))
     load().orc_control_cost_R(T, dt, _ptr(R, _dp))
     return R
+
+
+# ---------------------------------------------------------------------------
+# Reference kernels (oracle/_ref/libref_oracle.so, built from the reference
+# sources by oracle/Makefile). GPU only.
+# ---------------------------------------------------------------------------
+_ref = None
+
+
+def load_ref():
+    global _ref
+    if _ref is None:
+        if not REF_LIB.is_file():
+            raise ImportError(f"reference harness missing: {REF_LIB} (make -C oracle ref)")
+        lib = C.CDLL(str(REF_LIB))
+        lib.ref_model_create.restype = C.c_void_p
+        lib.ref_model_create.argtypes = [C.c_void_p]
+        lib.ref_model_destroy.argtypes = [C.c_void_p]
+        lib.ref_scene_create.restype = C.c_void_p
+        lib.ref_scene_create.argtypes = [_fp, _fp, _u8p, C.c_int, _fp, _fp, _u8p, _fp, C.c_int, C.c_int,
+                                         _u8p, C.c_int, _u8p, C.c_int, _u8p, C.c_int]
+        lib.ref_scene_destroy.argtypes = [C.c_void_p]
+        lib.ref_check_configs.argtypes = [C.c_void_p, C.c_void_p, _fp, C.c_int, C.c_float, _u8p, _fp]
+        lib.ref_fk_spheres.argtypes = [C.c_void_p, _fp, C.c_int, _fp]
+        lib.ref_obb_min_clearance.argtypes = [C.c_void_p, C.c_void_p, _fp, C.c_int, C.c_float, _fp]
+        lib.ref_transform_to_local.argtypes = [_fp, _fp, C.c_int, _fp]
+        lib.ref_obb_pairs.argtypes = [_fp, _fp, _fp, C.c_int, _u8p]
+        lib.ref_check_edges.argtypes = [C.c_void_p, C.c_void_p, _fp, _fp, _ip, C.c_int, C.c_float, C.c_int,
+                                        _u8p, _fp, _fp, C.c_int]
+        lib.ref_chomp.argtypes = [C.c_void_p, C.c_void_p, _fp, C.c_int, C.c_int, C.c_float, C.c_float,
+                                  C.c_float, C.c_float, _fp, _fp, _fp, C.c_int]
+        lib.ref_stomp_state_cost.argtypes = [C.c_void_p, C.c_void_p, _fp, C.c_int, C.c_int, C.c_float,
+                                             C.c_float, C.c_float, _fp, _fp, C.c_int]
+        _ref = lib
+    return _ref
+
+
+def _chk(rc, what):
+    if rc != 0:
+        raise RuntimeError(f"reference harness {what} failed ({rc})")
+
+
+class RefKernels:
+    """PrismPlan's own CUDA kernels on given host inputs (host in, host out)."""
+
+    def __init__(self, builder, obb_dims, obb_pose, obb_enable=None, esdf=None, masks=None):
+        lib = load_ref()
+        desc, self._keep = builder.descriptor()
+        self.n_dof = builder.n_dof
+        self.n_spheres = len(builder.sphere_to_joint)
+        self.m = lib.ref_model_create(C.byref(desc))
+        d = _f32(obb_dims).reshape(-1, 4)
+        p = _f32(obb_pose).reshape(-1, 8)
+        en = (np.ones(len(d), np.uint8) if obb_enable is None else np.ascontiguousarray(obb_enable, np.uint8))
+        keep = [d, p, en]
+        vp = vpose = ven = vfeat = None
+        nl = mv = 0
+        if esdf is not None:
+            vp, vpose, ven, vfeat = (np.ascontiguousarray(x) for x in esdf)
+            vp, vpose, vfeat = _f32(vp), _f32(vpose), _f32(vfeat)
+            ven = np.ascontiguousarray(ven, np.uint8)
+            nl = vp.reshape(-1, 4).shape[0]
+            mv = vfeat.reshape(nl, -1).shape[1]
+            keep += [vp, vpose, ven, vfeat]
+        m = masks or {}
+        mk = [None if m.get(k) is None else np.ascontiguousarray(m[k], np.uint8).reshape(-1)
+              for k in ("acm", "obb_acm", "obb_acm_apx")]
+        keep += mk
+        self._scene_keep = keep
+        self.s = lib.ref_scene_create(_ptr(d, _fp), _ptr(p, _fp), _ptr(en, _u8p), len(d), _ptr(vp, _fp),
+                                      _ptr(vpose, _fp), _ptr(ven, _u8p), _ptr(vfeat, _fp), nl, mv,
+                                      _ptr(mk[0], _u8p), 0 if mk[0] is None else mk[0].size,
+                                      _ptr(mk[1], _u8p), 0 if mk[1] is None else mk[1].size,
+                                      _ptr(mk[2], _u8p), 0 if mk[2] is None else mk[2].size)
+
+    def __del__(self):
+        try:
+            lib = load_ref()
+            lib.ref_scene_destroy(self.s)
+            lib.ref_model_destroy(self.m)
+        except Exception:
+            pass
+
+    def check_configs(self, q, margin=0.0):
+        q = _f32(q).reshape(-1, self.n_dof)
+        hit = np.zeros(len(q), np.uint8)
+        ms = C.c_float(0)
+        _chk(load_ref().ref_check_configs(self.m, self.s, _ptr(q, _fp), len(q), margin, _ptr(hit, _u8p),
+                                          C.byref(ms)), "check_configs")
+        return hit, ms.value
+
+    def fk_spheres(self, q):
+        q = _f32(q).reshape(-1, self.n_dof)
+        out = np.zeros((len(q), self.n_spheres, 3), np.float32)
+        _chk(load_ref().ref_fk_spheres(self.m, _ptr(q, _fp), len(q), _ptr(out, _fp)), "fk")
+        return out
+
+    def obb_min_clearance(self, q, margin=0.0):
+        q = _f32(q).reshape(-1, self.n_dof)
+        out = np.zeros(len(q), np.float32)
+        _chk(load_ref().ref_obb_min_clearance(self.m, self.s, _ptr(q, _fp), len(q), margin, _ptr(out, _fp)),
+             "obb_min_clearance")
+        return out
+
+    def check_edges(self, frm, to, G, margin=0.0, check_self=False, reps=1):
+        frm = _f32(frm).reshape(-1, self.n_dof)
+        to = _f32(to).reshape(-1, self.n_dof)
+        G = np.ascontiguousarray(G, np.int32)
+        valid = np.zeros(len(frm), np.uint8)
+        cost = np.zeros(len(frm), np.float32)
+        ms = C.c_float(0)
+        _chk(load_ref().ref_check_edges(self.m, self.s, _ptr(frm, _fp), _ptr(to, _fp), _ptr(G, _ip), len(frm),
+                                        margin, int(check_self), _ptr(valid, _u8p), _ptr(cost, _fp), C.byref(ms),
+                                        reps), "edges")
+        return valid, cost, ms.value
+
+    def chomp(self, theta_bdt, w, world_margin, self_margin, fd_eps=1e-3, state=True, grad=True, reps=1):
+        th = _f32(theta_bdt)
+        B, D, T = th.shape
+        sc = np.zeros_like(th) if state else None
+        g = np.zeros_like(th) if grad else None
+        ms = C.c_float(0)
+        _chk(load_ref().ref_chomp(self.m, self.s, _ptr(th, _fp), B, T, w, world_margin, self_margin, fd_eps,
+                                  _ptr(sc, _fp), _ptr(g, _fp), C.byref(ms), reps), "chomp")
+        return sc, g, ms.value
+
+    def stomp(self, rollouts_bdt, w, world_margin, self_margin, reps=1):
+        r = _f32(rollouts_bdt)
+        R, D, T = r.shape
+        out = np.zeros_like(r)
+        ms = C.c_float(0)
+        _chk(load_ref().ref_stomp_state_cost(self.m, self.s, _ptr(r, _fp), R, T, w, world_margin, self_margin,
+                                             _ptr(out, _fp), C.byref(ms), reps), "stomp")
+        return out, ms.value
+
+
+def ref_transform_to_local(pose, pts):
+    pose = _f32(pose).reshape(-1, 8)
+    pts = _f32(pts).reshape(-1, 3)
+    out = np.zeros_like(pts)
+    _chk(load_ref().ref_transform_to_local(_ptr(pose, _fp), _ptr(pts, _fp), len(pts), _ptr(out, _fp)), "to_local")
+    return out
+
+
+def ref_obb_pairs(dims, pose, spheres):
+    dims = _f32(dims).reshape(-1, 4)
+    pose = _f32(pose).reshape(-1, 8)
+    spheres = _f32(spheres).reshape(-1, 4)
+    out = np.zeros(len(spheres), np.uint8)
+    _chk(load_ref().ref_obb_pairs(_ptr(dims, _fp), _ptr(pose, _fp), _ptr(spheres, _fp), len(spheres),
+                                  _ptr(out, _u8p)), "obb_pairs")
+    return out

@@ -569,8 +569,12 @@ extern "C" int orc_check_edges(const orc_model* m, const orc_scene* s, const flo
         bool bad = false;
         double egap = 1e30, eclr = (double)FLT_MAX;
         long long cnt = 0;
-        for (int j = 1; j <= g; ++j) {
-            float t = (float)j / (float)g;
+        // Samples j = 1..G (t = j/G); slots past G in the last block of 16 take
+        // t = 0, the start configuration, and their verdict counts
+        // (edge_eval.cuh:110-130): it is evaluated last, as j = G + 1.
+        const int extra = (g > 0 && g % 16 != 0) ? 1 : 0;
+        for (int j = 1; j <= g + extra; ++j) {
+            float t = (j <= g) ? (float)j / (float)g : 0.0f;
             float qs[PS_MAX_DOF];
             for (int i = 0; i < D; ++i) qs[i] = std::fma(t, b[i] - a[i], a[i]);
             ++cnt;
@@ -586,7 +590,7 @@ extern "C" int orc_check_edges(const orc_model* m, const orc_scene* s, const flo
                 h = r.hit; cl = r.clearance; gp = r.gap;
             }
             egap = std::min(egap, gp);
-            if (compute_clearance) eclr = std::min(eclr, cl);
+            if (compute_clearance && j <= g) eclr = std::min(eclr, cl);
             if (h) {
                 bad = true;
                 if (early_exit) break;

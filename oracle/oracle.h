@@ -66,7 +66,9 @@ int orc_check_configs(const orc_model* m, const orc_scene* s, const float* q, in
                       uint8_t* hit, double* clearance, double* gap);
 
 /* Edge checks: samples j=1..G at t=(float)j/(float)G, interpolated in FP32 as
-   from + t*(to-from) with one rounding of the product-sum (edge_eval.cuh:115-121).
+   from + t*(to-from) with one rounding of the product-sum (edge_eval.cuh:115-121);
+   when G % 16 != 0 the start configuration (the reference's padding slots,
+   t = 0) is part of the verdict too.
    G[n_edges] given explicitly. valid[e], cost[e] (FLT_MAX if invalid),
    clearance[e] (NULL to skip; ESDF min like edge_eval.cuh:133-154),
    gap[e] (NULL to skip; min over samples of the sample gap).

@@ -134,6 +134,7 @@ _SIGNATURES = [
      [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     ("ps_probe_fp32_peak", C.c_int, [C.POINTER(C.c_double), C.c_void_p]),
     ("ps_set_stats", C.c_int, [C.c_void_p]),
+    ("ps_set_timing_events", C.c_int, [C.c_void_p, C.c_void_p]),
 ]
 
 EXPORTED_SYMBOLS = [name for name, _, _ in _SIGNATURES]

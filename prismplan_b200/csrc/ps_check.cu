@@ -271,6 +271,7 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(float* out, int iters, f
 }  // namespace
 
 unsigned long long* g_stats = nullptr;
+cudaEvent_t g_ev_start = nullptr, g_ev_stop = nullptr;
 
 }  // namespace ps
 
@@ -278,6 +279,12 @@ using namespace ps;
 
 extern "C" int ps_set_stats(unsigned long long* dev_counters) {
     ps::g_stats = dev_counters;
+    return PS_OK;
+}
+
+extern "C" int ps_set_timing_events(void* start, void* stop) {
+    ps::g_ev_start = (cudaEvent_t)start;
+    ps::g_ev_stop = (cudaEvent_t)stop;
     return PS_OK;
 }
 
@@ -297,13 +304,16 @@ extern "C" int ps_check_configs(const ps_model* m, const ps_scene_view* scene, c
     const int grid = std::max(1, std::min(blocks_needed, sm_count() * 8));
     if (clr) {
         PS_TRY_CUDA(cudaFuncSetAttribute(check_configs_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        mark_start(s);
         check_configs_kernel<true><<<grid, kCfgThreads, smem, s>>>(m->dev, *scene, q, n, margin, flags, hit, clearance,
                                                                    g_stats);
     } else {
         PS_TRY_CUDA(cudaFuncSetAttribute(check_configs_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        mark_start(s);
         check_configs_kernel<false><<<grid, kCfgThreads, smem, s>>>(m->dev, *scene, q, n, margin, flags, hit, clearance,
                                                                     g_stats);
     }
+    mark_stop(s);
     PS_TRY_CUDA(cudaGetLastError());
     if (flags & PS_CHECK_SELF) {
         size_t ss = (size_t)m->dev.bytes_core +

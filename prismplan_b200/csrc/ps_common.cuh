@@ -10,9 +10,10 @@
 //   * ESDF nearest lookup     collision/scene_collision.cuh:192-331
 // nvcc contracts `a*b + c*d` into fma(a, b, c*d) (the left product is fused,
 // the right one rounded). The FP32 expressions below spell that sequence out
-// with __fmaf_rn / __fmul_rn / __fadd_rn so it no longer depends on how the
-// compiler contracts this file; the GPU parity tests compare the results
-// bitwise against the reference kernels.
+// with __fmaf_rn / __fmul_rn / __fadd_rn (through fma_ab_cd for every
+// two-product sum) so it no longer depends on how the compiler contracts this
+// file; the GPU parity tests compare the results bitwise against the
+// reference kernels.
 //
 // Everything here is FP32 CUDA-core arithmetic: the 4x4 chains and the
 // per-pair distances are not dense contractions, so tensor cores do not apply.
@@ -89,8 +90,39 @@ struct LayerPrep {           // one ESDF layer, 64 bytes
 // ---------------------------------------------------------------------------
 // Exact reference arithmetic
 // ---------------------------------------------------------------------------
+// a*b + c*d as nvcc contracts it: the left product is fused, the right one
+// rounded. PS_FUSE_LEFT=0 builds the other order (diagnostic builds only).
+#ifndef PS_FUSE_LEFT
+#define PS_FUSE_LEFT 1
+#endif
 __device__ __forceinline__ float fma_ab_cd(float a, float b, float c, float d) {
-    // a*b + c*d as nvcc contracts it: fma(a, b, rn(c*d))
+#if PS_FUSE_LEFT
+    return __fmaf_rn(a, b, __fmul_rn(c, d));
+#else
+    return __fmaf_rn(c, d, __fmul_rn(a, b));
+#endif
+}
+
+// The 4x4 compose (dot4_col, utils.cuh:709-711): first two products, per
+// row r of the result. PS_COMPOSE_RIGHT_ROWS is a bitmask of rows whose right
+// product is fused (diagnostic builds only).
+#ifndef PS_COMPOSE_RIGHT_ROWS
+#define PS_COMPOSE_RIGHT_ROWS 0
+#endif
+template <int kRow>
+__device__ __forceinline__ float compose_sum(float a, float b, float c, float d) {
+    if ((PS_COMPOSE_RIGHT_ROWS >> kRow) & 1) return __fmaf_rn(c, d, __fmul_rn(a, b));
+    return __fmaf_rn(a, b, __fmul_rn(c, d));
+}
+
+// The joint-step columns (utils.cuh:571-699, `ft[x] * f1 + f2 * ft[y]` per
+// row r of the step) come out of nvcc with a row-dependent contraction,
+// measured on B200 against the reference kernels for every joint type and
+// column: row 0 fuses the right product, fma(f2, ft[y], rn(ft[x]*f1)); rows 1
+// and 2 fuse the left one, fma(ft[x], f1, rn(f2*ft[y])).
+template <int kRow>
+__device__ __forceinline__ float step_sum(float a, float b, float c, float d) {
+    if (kRow == 0) return __fmaf_rn(c, d, __fmul_rn(a, b));
     return __fmaf_rn(a, b, __fmul_rn(c, d));
 }
 
@@ -98,12 +130,12 @@ __device__ __forceinline__ float fma_ab_cd(float a, float b, float c, float d) {
 __device__ __forceinline__ void ref_to_local(float qw, float qx, float qy, float qz, float t0, float t1,
                                              float t2, float sx, float sy, float sz, float& lx, float& ly,
                                              float& lz) {
-    float tx = __fmul_rn(2.0f, __fmaf_rn(qy, sz, -__fmul_rn(qz, sy)));
-    float ty = __fmul_rn(2.0f, __fmaf_rn(qz, sx, -__fmul_rn(qx, sz)));
-    float tz = __fmul_rn(2.0f, __fmaf_rn(qx, sy, -__fmul_rn(qy, sx)));
-    float rx = __fadd_rn(__fmaf_rn(qw, tx, sx), __fmaf_rn(qy, tz, -__fmul_rn(qz, ty)));
-    float ry = __fadd_rn(__fmaf_rn(qw, ty, sy), __fmaf_rn(qz, tx, -__fmul_rn(qx, tz)));
-    float rz = __fadd_rn(__fmaf_rn(qw, tz, sz), __fmaf_rn(qx, ty, -__fmul_rn(qy, tx)));
+    float tx = __fmul_rn(2.0f, fma_ab_cd(qy, sz, -qz, sy));
+    float ty = __fmul_rn(2.0f, fma_ab_cd(qz, sx, -qx, sz));
+    float tz = __fmul_rn(2.0f, fma_ab_cd(qx, sy, -qy, sx));
+    float rx = __fadd_rn(__fmaf_rn(qw, tx, sx), fma_ab_cd(qy, tz, -qz, ty));
+    float ry = __fadd_rn(__fmaf_rn(qw, ty, sy), fma_ab_cd(qz, tx, -qx, tz));
+    float rz = __fadd_rn(__fmaf_rn(qw, tz, sz), fma_ab_cd(qx, ty, -qy, tx));
     lx = __fadd_rn(rx, t0);
     ly = __fadd_rn(ry, t1);
     lz = __fadd_rn(rz, t2);
@@ -117,7 +149,7 @@ __device__ __forceinline__ bool ref_obb_hit(const ObbPrep& o, float sx, float sy
     float cx = fmaxf(0.0f, __fadd_rn(fabsf(lx), -o.h.x));
     float cy = fmaxf(0.0f, __fadd_rn(fabsf(ly), -o.h.y));
     float cz = fmaxf(0.0f, __fadd_rn(fabsf(lz), -o.h.z));
-    float dsq = __fmaf_rn(cz, cz, __fmaf_rn(cx, cx, __fmul_rn(cy, cy)));
+    float dsq = __fmaf_rn(cz, cz, fma_ab_cd(cx, cx, cy, cy));
     return dsq < __fmul_rn(sr, sr);
 }
 
@@ -126,7 +158,7 @@ __device__ __forceinline__ bool ref_obb_hit(const ObbPrep& o, float sx, float sy
 __device__ __forceinline__ bool ref_self_hit(float ax, float ay, float az, float ar, float bx, float by,
                                              float bz, float br) {
     float xs = __fadd_rn(ax, -bx), ys = __fadd_rn(ay, -by), zs = __fadd_rn(az, -bz);
-    float sum = __fmaf_rn(zs, zs, __fmaf_rn(xs, xs, __fmul_rn(ys, ys)));
+    float sum = __fmaf_rn(zs, zs, fma_ab_cd(xs, xs, ys, ys));
     float rs = __fadd_rn(ar, br);
     return __fmaf_rn(-rs, rs, sum) < 0.0f;
 }
@@ -141,6 +173,34 @@ struct Affine {
 __device__ __forceinline__ void affine_identity(Affine& T) {
 #pragma unroll
     for (int k = 0; k < 12; ++k) T.m[k] = (k % 5 == 0) ? 1.0f : 0.0f;
+}
+
+// Rotation columns of step row kRow (utils.cuh:571-659).
+template <int kRow>
+__device__ __forceinline__ void step_rot_row(const JointRec& J, int type, float cs, float sn, float nsn, float* s) {
+    const float f0 = J.ft[kRow * 4 + 0], f1 = J.ft[kRow * 4 + 1], f2 = J.ft[kRow * 4 + 2];
+    if (type == PS_Z_ROT) {
+        s[kRow * 4 + 0] = step_sum<kRow>(f0, cs, sn, f1);
+        s[kRow * 4 + 1] = step_sum<kRow>(f0, nsn, cs, f1);
+    } else if (type == PS_X_ROT) {
+        s[kRow * 4 + 1] = step_sum<kRow>(f1, cs, sn, f2);
+        s[kRow * 4 + 2] = step_sum<kRow>(f1, nsn, cs, f2);
+    } else {   // PS_Y_ROT
+        s[kRow * 4 + 0] = step_sum<kRow>(f0, cs, nsn, f2);
+        s[kRow * 4 + 2] = step_sum<kRow>(f0, sn, cs, f2);
+    }
+}
+
+// Row kRow of P * step (dot4_col); reads the whole parent row first, so the
+// output may alias the parent.
+template <int kRow>
+__device__ __forceinline__ void compose_row(const Affine& P, const float* s, Affine& O) {
+    const float p0 = P.m[kRow * 4 + 0], p1 = P.m[kRow * 4 + 1], p2 = P.m[kRow * 4 + 2], p3 = P.m[kRow * 4 + 3];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        float v = __fmaf_rn(p2, s[8 + c], compose_sum<kRow>(p0, s[c], p1, s[4 + c]));
+        O.m[kRow * 4 + c] = (c == 3) ? __fadd_rn(v, p3) : v;
+    }
 }
 
 // T_out = T_par * step(FT, type, q) with the reference's per-column formulas
@@ -164,42 +224,25 @@ __device__ __forceinline__ void joint_compose(const JointRec& J, float qi, const
             sincosf(qi, &sn, &cs);
         }
         const float nsn = -sn;
-#pragma unroll
-        for (int r = 0; r < 3; ++r) {
-            const float f0 = J.ft[r * 4 + 0], f1 = J.ft[r * 4 + 1], f2 = J.ft[r * 4 + 2];
-            if (type == PS_Z_ROT) {
-                s[r * 4 + 0] = fma_ab_cd(f0, cs, sn, f1);
-                s[r * 4 + 1] = fma_ab_cd(f0, nsn, cs, f1);
-            } else if (type == PS_X_ROT) {
-                s[r * 4 + 1] = fma_ab_cd(f1, cs, sn, f2);
-                s[r * 4 + 2] = fma_ab_cd(f1, nsn, cs, f2);
-            } else {   // PS_Y_ROT
-                s[r * 4 + 0] = fma_ab_cd(f0, cs, nsn, f2);
-                s[r * 4 + 2] = fma_ab_cd(f0, sn, cs, f2);
-            }
-        }
+        step_rot_row<0>(J, type, cs, sn, nsn, s);
+        step_rot_row<1>(J, type, cs, sn, nsn, s);
+        step_rot_row<2>(J, type, cs, sn, nsn, s);
     } else if (type >= PS_X_PRISM) {
 #pragma unroll
         for (int r = 0; r < 3; ++r) s[r * 4 + 3] = __fmaf_rn(J.ft[r * 4 + type], qi, J.ft[r * 4 + 3]);
     }
     // PS_FIXED: step = FT
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-        const float p0 = P.m[r * 4 + 0], p1 = P.m[r * 4 + 1], p2 = P.m[r * 4 + 2], p3 = P.m[r * 4 + 3];
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            float v = __fmaf_rn(p2, s[8 + c], __fmaf_rn(p0, s[c], __fmul_rn(p1, s[4 + c])));
-            O.m[r * 4 + c] = (c == 3) ? __fadd_rn(v, p3) : v;
-        }
-    }
+    compose_row<0>(P, s, O);
+    compose_row<1>(P, s, O);
+    compose_row<2>(P, s, O);
 }
 
 // World position of a link-frame point (runtime_kinematics.cuh:79-83).
 __device__ __forceinline__ void sphere_world(const Affine& T, float x, float y, float z, float& px, float& py,
                                              float& pz) {
-    px = __fadd_rn(__fmaf_rn(T.m[2], z, __fmaf_rn(T.m[0], x, __fmul_rn(T.m[1], y))), T.m[3]);
-    py = __fadd_rn(__fmaf_rn(T.m[6], z, __fmaf_rn(T.m[4], x, __fmul_rn(T.m[5], y))), T.m[7]);
-    pz = __fadd_rn(__fmaf_rn(T.m[10], z, __fmaf_rn(T.m[8], x, __fmul_rn(T.m[9], y))), T.m[11]);
+    px = __fadd_rn(__fmaf_rn(T.m[2], z, fma_ab_cd(T.m[0], x, T.m[1], y)), T.m[3]);
+    py = __fadd_rn(__fmaf_rn(T.m[6], z, fma_ab_cd(T.m[4], x, T.m[5], y)), T.m[7]);
+    pz = __fadd_rn(__fmaf_rn(T.m[10], z, fma_ab_cd(T.m[8], x, T.m[9], y)), T.m[11]);
 }
 
 // ---------------------------------------------------------------------------

@@ -26,8 +26,6 @@
 
 namespace ps {
 
-extern unsigned long long* g_stats;
-
 namespace {
 
 constexpr int kCostThreads = 64;
@@ -398,12 +396,16 @@ extern "C" int ps_traj_cost(const ps_model* m, const ps_scene_view* scene, const
     if (grad) {
         PS_TRY_CUDA(cudaMemsetAsync(grad, 0, sizeof(float) * (size_t)total * m->info.n_dof, s));
         PS_TRY_CUDA(cudaFuncSetAttribute(waypoint_cost_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        mark_start(s);
         waypoint_cost_kernel<true><<<grid, kCostThreads, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
                                                                     atomic_traj ? traj_cost : nullptr, grad, g_stats);
+        mark_stop(s);
     } else {
         PS_TRY_CUDA(cudaFuncSetAttribute(waypoint_cost_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        mark_start(s);
         waypoint_cost_kernel<false><<<grid, kCostThreads, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
                                                                      atomic_traj ? traj_cost : nullptr, nullptr, g_stats);
+        mark_stop(s);
     }
     PS_TRY_CUDA(cudaGetLastError());
     if (traj_cost || (grad && P->smoothness_weight != 0.0f)) {
@@ -427,8 +429,10 @@ extern "C" int ps_rollout_costs(const ps_model* m, const ps_scene_view* scene, c
     const long long total = (long long)n_rows * T;
     const int grid = (int)std::max<long long>(1, std::min<long long>((total + kCostThreads - 1) / kCostThreads, 1 << 20));
     PS_TRY_CUDA(cudaFuncSetAttribute(waypoint_cost_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    mark_start(s);
     waypoint_cost_kernel<false><<<grid, kCostThreads, smem, s>>>(m->dev, *scene, rollouts, n_rows, T, *P, state_cost,
                                                                  broadcast_d, nullptr, nullptr, g_stats);
+    mark_stop(s);
     PS_TRY_CUDA(cudaGetLastError());
     return PS_OK;
 }

@@ -23,8 +23,6 @@
 
 namespace ps {
 
-extern unsigned long long* g_stats;
-
 namespace {
 
 constexpr int kWarps = 4;               // warps per block
@@ -86,9 +84,17 @@ __device__ bool process_chunk(const ModelSmem& M, const SceneSmem& sc, const ps_
     LaneStats st;   // padding lanes repeat a sample: their work is not credited
     st.zero();
     const int D = M.H->n_dof, NJ = M.H->n_joints;
+    // Reference sampling (edge_eval.cuh:110-121): t = j/G for j = 1..G in
+    // slots of 16; slots past G take t = 0, i.e. the start configuration,
+    // and their verdict counts. So the start configuration belongs to the
+    // edge verdict exactly when G % 16 != 0; a padding lane of the last chunk
+    // carries it (such a lane exists whenever G % 16 != 0), the remaining
+    // padding lanes repeat sample G and are not counted.
     const int j_raw = chunk * 32 + lane + 1;
-    const bool real = j_raw <= G;
-    const int j = real ? j_raw : G;    // padding lanes repeat the last sample
+    const bool in_range = j_raw <= G;
+    const bool start_lane = !in_range && (G % 16) != 0 && j_raw == G + 1;
+    const bool real = in_range || start_lane;
+    const int j = in_range ? j_raw : (start_lane ? 0 : G);
     const float t = __fdiv_rn((float)j, (float)G);
     const float* a = from + (size_t)e * D;
     const float* b = to + (size_t)e * D;
@@ -200,10 +206,184 @@ __device__ bool process_chunk(const ModelSmem& M, const SceneSmem& sc, const ps_
         if (!want_clr && __any_sync(kFull, hit && real)) break;   // warp-uniform early exit
     }
     if (want_clr) {
-        float c = real ? clr : 3.0e38f;
+        float c = in_range ? clr : 3.0e38f;   // clearance covers j = 1..G only (edge_eval.cuh:146-151)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) c = fminf(c, __shfl_xor_sync(kFull, c, o));
         *clr_min = c;
+    }
+    if (real)
+        for (int k = 0; k < ST_COUNT; ++k) st_out.v[k] += st.v[k];
+    return __any_sync(kFull, hit && real);
+}
+
+// Fast path of process_chunk for the common scene: the approximate chain is
+// the full chain, no ACM masks, no ESDF layers, no clearance. Same verdict;
+// fewer live registers and a per-joint guard band. Exact spheres of a flagged
+// joint are tested 8 at a time against each surviving box (one box load per
+// 8 spheres), then decided from their min d^2 with the exact re-decision
+// inside the guard band.
+constexpr int kBatch = 8;
+
+__device__ __forceinline__ bool batch_hits(const SceneSmem& sc, const uint16_t* cand, int ncand, const float* px,
+                                           const float* py, const float* pz, const float* sr, int nb, float g,
+                                           LaneStats& st) {
+    float mn[kBatch];
+#pragma unroll
+    for (int i = 0; i < kBatch; ++i) mn[i] = 3.0e38f;
+    for (int k = 0; k < ncand; ++k) {
+        const ObbPrep& o = sc.obbs[cand[k]];
+        const float4 r0 = o.r0, r1 = o.r1, r2 = o.r2, h = o.h;
+#pragma unroll
+        for (int i = 0; i < kBatch; ++i) {
+            if (i < nb) {
+                float lx = fmaf(r0.z, pz[i], fmaf(r0.y, py[i], fmaf(r0.x, px[i], r0.w)));
+                float ly = fmaf(r1.z, pz[i], fmaf(r1.y, py[i], fmaf(r1.x, px[i], r1.w)));
+                float lz = fmaf(r2.z, pz[i], fmaf(r2.y, py[i], fmaf(r2.x, px[i], r2.w)));
+                float cx = fmaxf(fabsf(lx) - h.x, 0.0f), cy = fmaxf(fabsf(ly) - h.y, 0.0f),
+                      cz = fmaxf(fabsf(lz) - h.z, 0.0f);
+                mn[i] = fminf(mn[i], fmaf(cz, cz, fmaf(cy, cy, cx * cx)));
+            }
+        }
+    }
+    st.v[ST_PAIRS] += ncand * nb;
+    bool hit = false;
+#pragma unroll
+    for (int i = 0; i < kBatch; ++i) {
+        if (i < nb && !hit) {
+            const float a = fmaxf(sr[i] - g, 0.0f), b = sr[i] + g;
+            const float lo = a * a * (1.0f - 1.0e-6f), hi = b * b * (1.0f + 1.0e-6f);
+            if (mn[i] < lo) {
+                hit = true;
+            } else if (mn[i] < hi) {
+                for (int k = 0; k < ncand && !hit; ++k) {
+                    const ObbPrep& o = sc.obbs[cand[k]];
+                    float qx, qy, qz;
+                    const float d = fast_box_dsq(o, px[i], py[i], pz[i], qx, qy, qz);
+                    if (d < lo) hit = true;
+                    else if (d < hi) {
+                        st.v[ST_EXACT] += 1;
+                        hit = ref_obb_hit(o, px[i], py[i], pz[i], sr[i]);
+                    }
+                }
+            }
+        }
+    }
+    return hit;
+}
+
+__device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, const ps_edge_params& P,
+                                   const float* __restrict__ from, const float* __restrict__ to, int e, int G,
+                                   int chunk, WarpScratch ws, LaneStats& st_out) {
+    const int lane = threadIdx.x & 31;
+    LaneStats st;
+    st.zero();
+    const int D = M.H->n_dof, NJ = M.H->n_joints;
+    // sampling rule as in process_chunk (edge_eval.cuh:110-121)
+    const int j_raw = chunk * 32 + lane + 1;
+    const bool in_range = j_raw <= G;
+    const bool start_lane = !in_range && (G % 16) != 0 && j_raw == G + 1;
+    const bool real = in_range || start_lane;
+    const int j = in_range ? j_raw : (start_lane ? 0 : G);
+    const float t = __fdiv_rn((float)j, (float)G);
+    const float* a = from + (size_t)e * D;
+    const float* b = to + (size_t)e * D;
+    float* qc = ws.q + lane * D;
+    for (int i = 0; i < D; ++i) {
+        const float ai = __ldg(a + i), bi = __ldg(b + i);
+        qc[i] = __fmaf_rn(t, __fadd_rn(bi, -ai), ai);
+    }
+    __syncwarp();
+    if (real) st.v[ST_SAMPLES] += 1;
+    const float margin = P.collision_margin;
+    // Slot 0 holds only the root's identity frame (checked on the host), so a
+    // joint's parent frame is the identity or the current frame: one 3x4
+    // frame in registers. Composing with the identity reproduces the step
+    // exactly, as the reference's slot walk does.
+    Affine T;
+    affine_identity(T);
+    bool hit = false;
+    for (int p = 0; p < NJ; ++p) {
+        const JointRec& jr = M.J[p];
+        if (p > 0) {
+            const float qi = jr.dof >= 0 ? qc[jr.dof] : 0.0f;
+            if (jr.parent_slot == 0) {
+                Affine I;
+                affine_identity(I);
+                joint_compose<true>(jr, qi, I, T);
+            } else {
+                joint_compose<true>(jr, qi, T, T);   // rows are read before they are written
+            }
+            st.v[ST_JOINTS] += 1;
+        }
+        if (jr.bound.w < 0.0f || sc.n_obbs == 0) continue;   // no spheres on this joint (uniform)
+        // ---- warp broad phase ----
+        float cx, cy, cz;
+        sphere_world(T, jr.bound.x, jr.bound.y, jr.bound.z, cx, cy, cz);
+        float mx = cx, my = cy, mz = cz;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mx += __shfl_xor_sync(kFull, mx, o);
+            my += __shfl_xor_sync(kFull, my, o);
+            mz += __shfl_xor_sync(kFull, mz, o);
+        }
+        mx *= (1.0f / 32.0f);
+        my *= (1.0f / 32.0f);
+        mz *= (1.0f / 32.0f);
+        const float dx = cx - mx, dy = cy - my, dz = cz - mz;
+        float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r2 = fmaxf(r2, __shfl_xor_sync(kFull, r2, o));
+        const float Sm = fmaxf(fabsf(mx), fmaxf(fabsf(my), fabsf(mz)));
+        float Rc = sqrtf(r2) + jr.bound.w + fmaxf(margin, 0.0f);
+        Rc += 4.0f * (Sm + Rc + sc.Bmax + 1.0f) * PS_GUARD_K;
+        const float Rc2 = Rc * Rc;
+        int ncand = 0;
+        __syncwarp();
+        for (int base = 0; base < sc.n_obbs; base += 32) {
+            const int o = base + lane;
+            bool keep = false;
+            if (o < sc.n_obbs) {
+                float qx, qy, qz;
+                keep = fast_box_dsq(sc.obbs[o], mx, my, mz, qx, qy, qz) < Rc2;
+                st.v[ST_CULL] += 1;
+            }
+            const unsigned bal = __ballot_sync(kFull, keep);
+            if (keep) ws.cand[ncand + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)o;
+            ncand += __popc(bal);
+        }
+        __syncwarp();
+        if (ncand == 0) continue;   // nothing reachable from any lane (uniform)
+        // Per-joint guard: every sphere of the joint lies within bound.w of c.
+        const float S = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))) + jr.bound.w;
+        const float g = (S + sc.Bmax + 1.0f) * PS_GUARD_K;
+        // ---- approximate gate ----
+        bool flagged = false;
+        for (int k = jr.apx_beg; k < jr.apx_end && !flagged; ++k) {
+            const float4 sa = M.A[k];
+            float px[kBatch], py[kBatch], pz[kBatch], sr[kBatch];
+            sphere_world(T, sa.x, sa.y, sa.z, px[0], py[0], pz[0]);
+            sr[0] = __fadd_rn(sa.w, margin);
+            st.v[ST_SPHERES] += 1;
+            flagged = batch_hits(sc, ws.cand, ncand, px, py, pz, sr, 1, g, st);
+        }
+        // ---- exact spheres of a flagged joint, 8 at a time ----
+        if (flagged && !hit) {
+            for (int k0 = jr.sph_beg; k0 < jr.sph_end && !hit; k0 += kBatch) {
+                const int nb = min(kBatch, jr.sph_end - k0);
+                float px[kBatch], py[kBatch], pz[kBatch], sr[kBatch];
+#pragma unroll
+                for (int i = 0; i < kBatch; ++i) {
+                    if (i < nb) {
+                        const float4 sp = M.S[k0 + i];
+                        sphere_world(T, sp.x, sp.y, sp.z, px[i], py[i], pz[i]);
+                        sr[i] = __fadd_rn(sp.w, margin);
+                    }
+                }
+                st.v[ST_SPHERES] += nb;
+                hit = batch_hits(sc, ws.cand, ncand, px, py, pz, sr, nb, g, st);
+            }
+        }
+        if (__any_sync(kFull, hit && real)) break;   // warp-uniform early exit
     }
     if (real)
         for (int k = 0; k < ST_COUNT; ++k) st_out.v[k] += st.v[k];
@@ -241,6 +421,7 @@ size_t edge_smem_bytes(const ps_model* m, const ps_scene_view* sv) {
 // ---------------------------------------------------------------------------
 // Plain path: one warp per edge, chunks in order.
 // ---------------------------------------------------------------------------
+template <bool kFast>
 __global__ void __launch_bounds__(kEdgeThreads) edges_plain_kernel(ModelDev md, ps_scene_view sv, ps_edge_params P,
                                                                   const float* __restrict__ from,
                                                                   const float* __restrict__ to,
@@ -273,7 +454,8 @@ __global__ void __launch_bounds__(kEdgeThreads) edges_plain_kernel(ModelDev md, 
         const int chunks = G > 0 ? (G + 31) / 32 : 0;
         for (int c = 0; c < chunks; ++c) {
             float cm = FLT_MAX;
-            bad |= process_chunk(M, sc, sv, P, from, to, e, G, c, ws, P.compute_clearance ? &cm : nullptr, st);
+            if (kFast) bad |= process_chunk_fast(M, sc, P, from, to, e, G, c, ws, st);
+            else bad |= process_chunk(M, sc, sv, P, from, to, e, G, c, ws, P.compute_clearance ? &cm : nullptr, st);
             emin = fminf(emin, cm);
             if (bad && !P.compute_clearance) break;
         }
@@ -309,7 +491,8 @@ __global__ void edges_prep_kernel(ps_edge_params P, const float* __restrict__ fr
     if ((threadIdx.x & 31) == 0 && local_max > 0) atomicMax(&hdr->max_G, local_max);
 }
 
-__global__ void __launch_bounds__(kEdgeThreads) edges_queue_kernel(ModelDev md, ps_scene_view sv, ps_edge_params P,
+template <bool kFast>
+__global__ void __launch_bounds__(kEdgeThreads, 4) edges_queue_kernel(ModelDev md, ps_scene_view sv, ps_edge_params P,
                                                                   const float* __restrict__ from,
                                                                   const float* __restrict__ to, int n_edges,
                                                                   EdgeWs* hdr, const int* __restrict__ Gs, int* bad,
@@ -360,7 +543,9 @@ __global__ void __launch_bounds__(kEdgeThreads) edges_queue_kernel(ModelDev md, 
             retired = __shfl_sync(kFull, retired, 0);
             if (!P.compute_clearance && retired) continue;   // retired meanwhile
             float cm = FLT_MAX;
-            const bool h = process_chunk(M, sc, sv, P, from, to, ee, GG, kk, ws, P.compute_clearance ? &cm : nullptr, st);
+            const bool h = kFast ? process_chunk_fast(M, sc, P, from, to, ee, GG, kk, ws, st)
+                                 : process_chunk(M, sc, sv, P, from, to, ee, GG, kk, ws,
+                                                 P.compute_clearance ? &cm : nullptr, st);
             if (lane == 0) {
                 if (h) vbad[ee] = 1;
                 if (P.compute_clearance) atomicMin(clr + ee, ordered_float(cm));
@@ -391,6 +576,11 @@ using namespace ps;
 
 namespace {
 
+bool fast_path(const ps_model* m, const ps_scene_view* sv, const ps_edge_params* P) {
+    return m->info.approx_shares_chain && m->root_slot_only && !P->compute_clearance && !P->check_self && sv->n_voxel_layers == 0 &&
+           !sv->sphere_obb_acm_mask && !sv->sphere_obb_acm_mask_approx && !sv->sphere_acm_mask;
+}
+
 int check_edge_args(const ps_model* m, const ps_scene_view* scene, const float* from, const float* to, int n,
                     const ps_edge_params* P, uint8_t* valid, float* cost) {
     if (!m) return set_error(PS_EINVAL, "model is NULL");
@@ -413,10 +603,13 @@ extern "C" int ps_check_edges_plain(const ps_model* m, const ps_scene_view* scen
     if (n_edges == 0) return PS_OK;
     cudaStream_t s = (cudaStream_t)stream;
     const size_t smem = edge_smem_bytes(m, scene);
-    PS_TRY_CUDA(cudaFuncSetAttribute(edges_plain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int grid = (n_edges + kWarps - 1) / kWarps;
-    edges_plain_kernel<<<grid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, samples_per_edge, n_edges, valid,
-                                                        cost, clearance, g_stats);
+    auto kern = fast_path(m, scene, P) ? edges_plain_kernel<true> : edges_plain_kernel<false>;
+    PS_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    mark_start(s);
+    kern<<<grid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, samples_per_edge, n_edges, valid, cost,
+                                          clearance, g_stats);
+    mark_stop(s);
     PS_TRY_CUDA(cudaGetLastError());
     return PS_OK;
 }
@@ -451,12 +644,14 @@ extern "C" int ps_check_edges(const ps_model* m, const ps_scene_view* scene, con
     PS_TRY_CUDA(cudaGetLastError());
 
     const size_t smem = edge_smem_bytes(m, scene);
-    PS_TRY_CUDA(cudaFuncSetAttribute(edges_queue_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    auto qk = fast_path(m, scene, P) ? edges_queue_kernel<true> : edges_queue_kernel<false>;
+    PS_TRY_CUDA(cudaFuncSetAttribute(qk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edges_queue_kernel, kEdgeThreads, smem));
+    PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qk, kEdgeThreads, smem));
     const int qgrid = std::max(1, sm_count() * std::max(per_sm, 1));
-    edges_queue_kernel<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, hdr, G, bad, clr,
-                                                         g_stats);
+    mark_start(s);
+    qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, hdr, G, bad, clr, g_stats);
+    mark_stop(s);
     PS_TRY_CUDA(cudaGetLastError());
     const int fgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
     edges_finalize_kernel<<<fgrid, 256, 0, s>>>(n_edges, *P, bad, len, clr, valid, cost, clearance);

@@ -15,6 +15,7 @@ struct ps_model {
     size_t alloc_bytes = 0;
     ps_model_info info{};
     int max_joint_spheres = 0;  // most exact spheres on one joint
+    bool root_slot_only = false; // slot 0 holds only the root (identity) frame
     int max_joint_approx = 0;
     std::vector<int> sph_orig;  // reordered -> descriptor index (host copy)
 };
@@ -33,6 +34,25 @@ size_t scene_smem_bytes(const ps_scene_view* s);
 
 // Number of SMs of the current device (cached).
 int sm_count();
+
+// Diagnostics shared by every launcher (set through ps_set_stats /
+// ps_set_timing_events).
+extern unsigned long long* g_stats;
+extern cudaEvent_t g_ev_start, g_ev_stop;
+// Inside a stream capture a plain cudaEventRecord only expresses a
+// dependency; an external record node is what re-records on every replay.
+inline void mark_event(cudaEvent_t e, cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &st);
+    if (st == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+    else cudaEventRecord(e, s);
+}
+inline void mark_start(cudaStream_t s) {
+    if (g_ev_start && g_ev_stop) mark_event(g_ev_start, s);
+}
+inline void mark_stop(cudaStream_t s) {
+    if (g_ev_start && g_ev_stop) mark_event(g_ev_stop, s);
+}
 
 }  // namespace ps
 

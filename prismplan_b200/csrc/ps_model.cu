@@ -320,6 +320,8 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
     m->dev.status = reinterpret_cast<int*>(base + off_status);
     m->dev.bytes_core = (int)core;
     m->max_joint_spheres = max_js;
+    m->root_slot_only = tmem[dfs[0]] == 0;
+    for (int p = 1; p < nj; ++p) m->root_slot_only = m->root_slot_only && tmem[dfs[p]] == 1;
     m->max_joint_approx = max_ja;
     m->sph_orig = sorder;
     int dev = 0;

@@ -190,6 +190,43 @@ def baxter_like(seed: int = 1005) -> Dict:
     return _finish(asset)
 
 
+def generic_chain(seed: int = 1006, n_links: int = 7, spheres_per_link: int = 6) -> Dict:
+    """Serial chain whose fixed transforms carry generic rotations (uniform
+    SO(3)) and mixed joint types (X/Y/Z revolute, one prismatic), so that every
+    joint-step column combines two nonzero products."""
+    rng = np.random.default_rng(seed)
+    types = [X_ROT] + [int(t) for t in rng.choice([X_ROT, Y_ROT, Z_ROT], n_links)]
+    types[3] = int(rng.choice([X_PRISM, Y_PRISM, Z_PRISM]))
+    fts = [_ft(np.eye(3), (0, 0, 0))]
+    sph, s2j = [], []
+    for k in range(n_links):
+        qv = rng.normal(size=4)
+        qv /= np.linalg.norm(qv)
+        w, x, y, z = qv
+        R = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                      [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                      [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+        t = rng.uniform(-0.25, 0.25, 3) + np.array([0.0, 0.0, 0.12])
+        fts.append(_ft(R, t))
+        for c in range(spheres_per_link):
+            p = rng.uniform(-0.12, 0.12, 3)
+            sph.extend([float(p[0]), float(p[1]), float(p[2]), float(rng.uniform(0.03, 0.08))])
+            s2j.append(k + 1)
+    parents = [0] + list(range(n_links))
+    lo = [-2.9] * n_links
+    hi = [2.9] * n_links
+    lo[2], hi[2] = -0.3, 0.3     # the prismatic joint (types[3] drives dof 2)
+    asset = {
+        "name": "generic_chain", "n_dof": n_links, "n_joints": n_links + 1, "joint_types": types,
+        "fixed_transforms": [float(np.float32(v)) for f in fts for v in f],
+        "spheres_flat": sph, "sphere_to_joint": s2j, "joint_lower": lo, "joint_upper": hi,
+        "joint_parents": parents, "joint_id_to_dof": [-1] + list(range(n_links)),
+        "t_memory_idx": [0] + [1] * n_links, "dfs_order": list(range(n_links + 1)),
+    }
+    asset["self_cc_ranges_flat"] = _self_ranges(s2j, parents)
+    return _finish(asset)
+
+
 # ---------------------------------------------------------------------------
 # scenes
 # ---------------------------------------------------------------------------

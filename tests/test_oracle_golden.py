@@ -83,7 +83,8 @@ def test_control_cost_matrix():
 
 
 def test_edge_oracle_samples_are_configs():
-    """An edge is invalid iff one of its samples t=j/G (FP32 product-sum) is."""
+    """An edge is invalid iff one of its samples t=j/G (FP32 product-sum) is,
+    or, when G % 16 != 0, its start configuration (edge_eval.cuh:110-130)."""
     wl = workloads.workload(2, scale=0.002)
     b = RobotModelBuilder.from_asset(wl["asset"])
     om = oracle.OracleModel(b, *wl["obbs"])
@@ -91,6 +92,8 @@ def test_edge_oracle_samples_are_configs():
     valid, cost, _, _, _ = om.check_edges(frm, to, G, early_exit=False)
     for e in range(len(frm)):
         t = (np.arange(1, G[e] + 1, dtype=np.float32) / np.float32(G[e])).astype(np.float32)
+        if G[e] % 16:   # the reference's padding slots evaluate the start configuration
+            t = np.append(t, np.float32(0.0))
         q = (frm[e][None] + t[:, None] * (to[e] - frm[e])[None]).astype(np.float32)
         hit, _, _ = om.check_configs(q, prec=64, want_gap=False)
         assert bool(valid[e]) == (not hit.any())
