@@ -60,22 +60,23 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi samples during the timed region."""
+    """nvidia-smi samples of this GPU during the timed region (all GPUs are
+    queried; the row whose UUID matches the torch device is kept)."""
+
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device: int):
         import torch
 
-        p = torch.cuda.get_device_properties(device)
-        self.index = f"GPU-{p.uuid}"
+        self.uuid = str(torch.cuda.get_device_properties(device).uuid).lower().replace("gpu-", "")
         self.proc = None
         self.lines = []
 
     def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
@@ -99,10 +100,20 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
+        rows = [[x.strip() for x in ln.split(",")] for ln in self.lines]
+        rows = [f for f in rows if len(f) >= 9]
+        mine = [f for f in rows if f[0].lower().replace("gpu-", "") == self.uuid]
+        if not mine and rows:   # UUID formats differ: take the GPU with the highest median SM clock
+            groups = {}
+            for f in rows:
+                groups.setdefault(f[0], []).append(f)
+
+            def med(g):
+                v = [float(x[1]) for x in g if x[1].replace(".", "", 1).isdigit()]
+                return statistics.median(v) if v else 0.0
+
+            mine = max(groups.values(), key=med)
+        for f in mine:
             try:
                 sm.append(float(f[1]))
                 mx = float(f[2])
@@ -112,7 +123,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "uuid_matched": bool(sm) and len(mine) < len(rows)}
 
 
 def build_edge_case(rank: int):
