@@ -211,6 +211,31 @@ int ps_check_edges(const ps_model* model, const ps_scene_view* scene,
                    uint8_t* valid, float* cost, float* clearance,
                    void* workspace, size_t workspace_bytes, void* stream);
 
+/* Persistent edge checks with the workspace built into the library, for
+   callers that cannot allocate device memory: a planner evaluating an edge
+   batch per search expansion cannot afford cudaMalloc/cudaFree inside its
+   latency budget (both can synchronise the device), and some host processes
+   have no CUDA allocator of their own to provide a workspace from. No
+   counterpart in the reference (its EdgeEvalGpu owns cudaMalloc'd buffers).
+   Same arguments, verdicts and outputs as ps_check_edges minus the
+   workspace. Limits and sharing:
+     - n_edges <= PS_EDGES_STATIC_MAX (65536); larger batches return PS_EINVAL.
+       The scratch array (about 1 MiB) is a file-scope __device__ array, held
+       by every GPU that loads the library until the process exits.
+     - The first call on each device looks up the array's device address
+       (cudaGetSymbolAddress) with that device current; make that first call
+       before any stream capture on the device.
+     - Every call on a device shares the one array and resets it as it starts,
+       so calls whose work overlaps on the GPU (other streams or threads) race.
+   Allocates nothing: no cudaMalloc, cudaFree or allocating library call. */
+#define PS_EDGES_STATIC_MAX 65536
+int ps_check_edges_static(const ps_model* model, const ps_scene_view* scene,
+                          const float* from, const float* to,
+                          const int* samples_per_edge, int n_edges,
+                          const ps_edge_params* params,
+                          uint8_t* valid, float* cost, float* clearance,
+                          void* stream);
+
 /* =========================================================================
  * Trajectory cost: summed hinge + self hinge + smoothness, with its exact
  * gradient from a hand-written adjoint.

@@ -124,6 +124,9 @@ _SIGNATURES = [
      [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
       C.POINTER(EdgeParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
       C.c_size_t, C.c_void_p]),
+    ("ps_check_edges_static", C.c_int,
+     [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+      C.POINTER(EdgeParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("ps_traj_cost", C.c_int,
      [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_int, C.c_int,
       C.POINTER(CostParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

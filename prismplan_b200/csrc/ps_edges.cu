@@ -17,6 +17,8 @@
 // edge) at the first confirmed hit.
 #include <algorithm>
 #include <cfloat>
+#include <mutex>
+#include <string>
 
 #include "ps_internal.h"
 #include "ps_verdict.cuh"
@@ -652,6 +654,94 @@ extern "C" int ps_check_edges(const ps_model* m, const ps_scene_view* scene, con
     mark_start(s);
     qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, hdr, G, bad, clr, g_stats);
     mark_stop(s);
+    PS_TRY_CUDA(cudaGetLastError());
+    const int fgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
+    edges_finalize_kernel<<<fgrid, 256, 0, s>>>(n_edges, *P, bad, len, clr, valid, cost, clearance);
+    PS_TRY_CUDA(cudaGetLastError());
+    return PS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Edge checks without a caller-provided workspace.
+//
+// Some callers cannot hand the library a device allocation: a planner that
+// evaluates an edge batch per search expansion inside a latency budget cannot
+// afford cudaMalloc / cudaFree (they can synchronise the whole device), and
+// some host processes have no CUDA allocator of their own to draw from (a
+// plugin loaded into a framework that owns all device memory, or a
+// fixed-memory real-time process). For them the persistent path's workspace
+// lives in the library itself: a file-scope device array sized for
+// PS_EDGES_STATIC_MAX edges, which every GPU that loads the library holds
+// until the process exits. Nothing here allocates.
+//
+// The array is shared by every call: a call resets what must start at zero
+// (queue head and max G) and its prep kernel rewrites the per-edge state, so
+// back-to-back calls are fine, but calls whose kernels overlap on the GPU
+// (other streams, other host threads) race on it.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kStaticWsBytes =
+    ((sizeof(EdgeWs) + 255) & ~size_t(255)) + 4 * (((size_t)PS_EDGES_STATIC_MAX * 4 + 255) & ~size_t(255));
+
+static __device__ __align__(256) unsigned char g_edges_static_ws[kStaticWsBytes];
+
+// Device address of g_edges_static_ws per device ordinal (host code must not
+// use the symbol itself: on the host it only names a stand-in).
+std::mutex g_static_ws_mutex;
+void* g_static_ws_ptr[128] = {nullptr};
+
+int static_workspace(void** out) {
+    int dev = 0;
+    PS_TRY_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 128) return set_error(PS_EINVAL, "device ordinal above 127");
+    std::lock_guard<std::mutex> lock(g_static_ws_mutex);
+    if (!g_static_ws_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_edges_static_ws);
+        if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(g_edges_static_ws)");
+        g_static_ws_ptr[dev] = p;
+    }
+    *out = g_static_ws_ptr[dev];
+    return PS_OK;
+}
+
+}  // namespace
+
+extern "C" int ps_check_edges_static(const ps_model* m, const ps_scene_view* scene, const float* from,
+                                     const float* to, const int* samples_per_edge, int n_edges,
+                                     const ps_edge_params* P, uint8_t* valid, float* cost, float* clearance,
+                                     void* stream) {
+    clear_error();
+    if (int rc = check_edge_args(m, scene, from, to, n_edges, P, valid, cost)) return rc;
+    if (n_edges > PS_EDGES_STATIC_MAX)
+        return set_error(PS_EINVAL, "n_edges " + std::to_string(n_edges) + " exceeds the built-in workspace (" +
+                                        std::to_string(PS_EDGES_STATIC_MAX) +
+                                        " edges); split the batch or use ps_check_edges with a workspace");
+    if (n_edges == 0) return PS_OK;
+    void* ws = nullptr;
+    if (int rc = static_workspace(&ws)) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char* w = reinterpret_cast<unsigned char*>(ws);
+    const size_t seg = align256((size_t)n_edges * 4);
+    EdgeWs* hdr = reinterpret_cast<EdgeWs*>(w);
+    int* G = reinterpret_cast<int*>(w + align256(sizeof(EdgeWs)));
+    float* len = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(G) + seg);
+    int* bad = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(len) + seg);
+    int* clr = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(bad) + seg);
+    const int D = m->info.n_dof;
+
+    PS_TRY_CUDA(cudaMemsetAsync(hdr, 0, sizeof(EdgeWs), s));   // queue head, max G
+    const int pgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
+    edges_prep_kernel<<<pgrid, 256, 0, s>>>(*P, from, to, samples_per_edge, n_edges, D, hdr, G, len, bad, clr);
+    PS_TRY_CUDA(cudaGetLastError());
+    const size_t smem = edge_smem_bytes(m, scene);
+    auto qk = fast_path(m, scene, P) ? edges_queue_kernel<true> : edges_queue_kernel<false>;
+    PS_TRY_CUDA(cudaFuncSetAttribute(qk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qk, kEdgeThreads, smem));
+    const int qgrid = std::max(1, sm_count() * std::max(per_sm, 1));
+    qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, hdr, G, bad, clr, g_stats);
     PS_TRY_CUDA(cudaGetLastError());
     const int fgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
     edges_finalize_kernel<<<fgrid, 256, 0, s>>>(n_edges, *P, bad, len, clr, valid, cost, clearance);
