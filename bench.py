@@ -60,70 +60,70 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi samples of this GPU during the timed region (all GPUs are
-    queried; the row whose UUID matches the torch device is kept)."""
+    """Clocks and throttle reasons of this GPU during the timed region.
 
-    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    The timed region of a step is well under a millisecond, far below
+    nvidia-smi's sampling interval, so a background thread polls NVML (the
+    library nvidia-smi reads) as fast as it answers, for the GPU whose UUID
+    matches the torch device. Read-only queries; nothing is set."""
+
+    REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20), ("hw_thermal_slowdown", 0x40),
+               ("hw_power_brake", 0x80), ("sw_power_cap", 0x4))
 
     def __init__(self, device: int):
         import torch
 
         self.uuid = str(torch.cuda.get_device_properties(device).uuid).lower().replace("gpu-", "")
-        self.proc = None
-        self.lines = []
+        self.samples = []
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self.handle = None
+        self.error = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except Exception:
-            self.proc = None
+            import pynvml as nv
+
+            nv.nvmlInit()
+            for i in range(nv.nvmlDeviceGetCount()):
+                h = nv.nvmlDeviceGetHandleByIndex(i)
+                u = nv.nvmlDeviceGetUUID(h)
+                u = (u.decode() if isinstance(u, bytes) else u).lower().replace("gpu-", "")
+                if u == self.uuid:
+                    self.handle = h
+            if self.handle is not None:
+                self.nv = nv
+                self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(self.handle, nv.NVML_CLOCK_SM)
+                self.t = threading.Thread(target=self._poll, daemon=True)
+                self.t.start()
+        except Exception as e:   # no NVML: report no samples rather than fail the bench
+            self.error = str(e)[:120]
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _poll(self):
+        nv, h = self.nv, self.handle
+        while not self._stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((mhz, rs))
+            except Exception as e:
+                self.error = str(e)[:120]
+                return
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        self._stop.set()
+        if self.handle is not None:
+            self.t.join(timeout=5)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        rows = [[x.strip() for x in ln.split(",")] for ln in self.lines]
-        rows = [f for f in rows if len(f) >= 9]
-        mine = [f for f in rows if f[0].lower().replace("gpu-", "") == self.uuid]
-        if not mine and rows:   # UUID formats differ: take the GPU with the highest median SM clock
-            groups = {}
-            for f in rows:
-                groups.setdefault(f[0], []).append(f)
-
-            def med(g):
-                v = [float(x[1]) for x in g if x[1].replace(".", "", 1).isdigit()]
-                return statistics.median(v) if v else 0.0
-
-            mine = max(groups.values(), key=med)
-        for f in mine:
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm), "uuid_matched": bool(sm) and len(mine) < len(rows)}
+        sm = [m for m, _ in self.samples]
+        reasons = sorted({n for _, rs in self.samples for n, bit in self.REASONS if rs & bit})
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+               "reasons": reasons, "samples": len(sm), "source": "NVML polled during the timed region"}
+        if self.error:
+            out["error"] = self.error
+        return out
 
 
 def build_edge_case(rank: int):

@@ -224,55 +224,58 @@ __device__ bool process_chunk(const ModelSmem& M, const SceneSmem& sc, const ps_
 // joint are tested 8 at a time against each surviving box (one box load per
 // 8 spheres), then decided from their min d^2 with the exact re-decision
 // inside the guard band.
-constexpr int kBatch = 8;
+// Decide one sphere from its min d^2 over the candidate boxes: definite
+// outside the guard band, exact re-decision of the band's boxes otherwise.
+__device__ __forceinline__ bool decide_band(const SceneSmem& sc, const uint16_t* cand, int ncand, float px, float py,
+                                            float pz, float sr, float g, float mn, LaneStats& st) {
+    const float a = fmaxf(sr - g, 0.0f), b = sr + g;
+    const float lo = a * a * (1.0f - 1.0e-6f), hi = b * b * (1.0f + 1.0e-6f);
+    if (mn < lo) return true;
+    if (mn >= hi) return false;
+    for (int k = 0; k < ncand; ++k) {
+        const ObbPrep& o = sc.obbs[cand[k]];
+        float qx, qy, qz;
+        const float d = fast_box_dsq(o, px, py, pz, qx, qy, qz);
+        if (d < lo) return true;
+        if (d < hi) {
+            st.v[ST_EXACT] += 1;
+            if (ref_obb_hit(o, px, py, pz, sr)) return true;
+        }
+    }
+    return false;
+}
 
-__device__ __forceinline__ bool batch_hits(const SceneSmem& sc, const uint16_t* cand, int ncand, const float* px,
-                                           const float* py, const float* pz, const float* sr, int nb, float g,
-                                           LaneStats& st) {
-    float mn[kBatch];
+// kN spheres (positions in registers) against every candidate box: one box
+// load per kN pair tests. Returns whether any of them hits.
+template <int kN, bool kStats>
+__device__ __forceinline__ bool spheres_hit(const SceneSmem& sc, const uint16_t* cand, int ncand, const float* px,
+                                            const float* py, const float* pz, const float* sr, float g,
+                                            LaneStats& st) {
+    float mn[kN];
 #pragma unroll
-    for (int i = 0; i < kBatch; ++i) mn[i] = 3.0e38f;
+    for (int i = 0; i < kN; ++i) mn[i] = 3.0e38f;
     for (int k = 0; k < ncand; ++k) {
         const ObbPrep& o = sc.obbs[cand[k]];
         const float4 r0 = o.r0, r1 = o.r1, r2 = o.r2, h = o.h;
 #pragma unroll
-        for (int i = 0; i < kBatch; ++i) {
-            if (i < nb) {
-                float lx = fmaf(r0.z, pz[i], fmaf(r0.y, py[i], fmaf(r0.x, px[i], r0.w)));
-                float ly = fmaf(r1.z, pz[i], fmaf(r1.y, py[i], fmaf(r1.x, px[i], r1.w)));
-                float lz = fmaf(r2.z, pz[i], fmaf(r2.y, py[i], fmaf(r2.x, px[i], r2.w)));
-                float cx = fmaxf(fabsf(lx) - h.x, 0.0f), cy = fmaxf(fabsf(ly) - h.y, 0.0f),
-                      cz = fmaxf(fabsf(lz) - h.z, 0.0f);
-                mn[i] = fminf(mn[i], fmaf(cz, cz, fmaf(cy, cy, cx * cx)));
-            }
+        for (int i = 0; i < kN; ++i) {
+            const float lx = fmaf(r0.z, pz[i], fmaf(r0.y, py[i], fmaf(r0.x, px[i], r0.w)));
+            const float ly = fmaf(r1.z, pz[i], fmaf(r1.y, py[i], fmaf(r1.x, px[i], r1.w)));
+            const float lz = fmaf(r2.z, pz[i], fmaf(r2.y, py[i], fmaf(r2.x, px[i], r2.w)));
+            const float cx = fmaxf(fabsf(lx) - h.x, 0.0f), cy = fmaxf(fabsf(ly) - h.y, 0.0f),
+                        cz = fmaxf(fabsf(lz) - h.z, 0.0f);
+            mn[i] = fminf(mn[i], fmaf(cz, cz, fmaf(cy, cy, cx * cx)));
         }
     }
-    st.v[ST_PAIRS] += ncand * nb;
+    if (kStats) st.v[ST_PAIRS] += ncand * kN;
     bool hit = false;
 #pragma unroll
-    for (int i = 0; i < kBatch; ++i) {
-        if (i < nb && !hit) {
-            const float a = fmaxf(sr[i] - g, 0.0f), b = sr[i] + g;
-            const float lo = a * a * (1.0f - 1.0e-6f), hi = b * b * (1.0f + 1.0e-6f);
-            if (mn[i] < lo) {
-                hit = true;
-            } else if (mn[i] < hi) {
-                for (int k = 0; k < ncand && !hit; ++k) {
-                    const ObbPrep& o = sc.obbs[cand[k]];
-                    float qx, qy, qz;
-                    const float d = fast_box_dsq(o, px[i], py[i], pz[i], qx, qy, qz);
-                    if (d < lo) hit = true;
-                    else if (d < hi) {
-                        st.v[ST_EXACT] += 1;
-                        hit = ref_obb_hit(o, px[i], py[i], pz[i], sr[i]);
-                    }
-                }
-            }
-        }
-    }
+    for (int i = 0; i < kN; ++i)
+        if (!hit) hit = decide_band(sc, cand, ncand, px[i], py[i], pz[i], sr[i], g, mn[i], st);
     return hit;
 }
 
+template <bool kStats>
 __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, const ps_edge_params& P,
                                    const float* __restrict__ from, const float* __restrict__ to, int e, int G,
                                    int chunk, WarpScratch ws, LaneStats& st_out) {
@@ -295,7 +298,7 @@ __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, cons
         qc[i] = __fmaf_rn(t, __fadd_rn(bi, -ai), ai);
     }
     __syncwarp();
-    if (real) st.v[ST_SAMPLES] += 1;
+    if (kStats && real) st.v[ST_SAMPLES] += 1;
     const float margin = P.collision_margin;
     // Slot 0 holds only the root's identity frame (checked on the host), so a
     // joint's parent frame is the identity or the current frame: one 3x4
@@ -315,7 +318,7 @@ __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, cons
             } else {
                 joint_compose<true>(jr, qi, T, T);   // rows are read before they are written
             }
-            st.v[ST_JOINTS] += 1;
+            if (kStats) st.v[ST_JOINTS] += 1;
         }
         if (jr.bound.w < 0.0f || sc.n_obbs == 0) continue;   // no spheres on this joint (uniform)
         // ---- warp broad phase ----
@@ -347,7 +350,7 @@ __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, cons
             if (o < sc.n_obbs) {
                 float qx, qy, qz;
                 keep = fast_box_dsq(sc.obbs[o], mx, my, mz, qx, qy, qz) < Rc2;
-                st.v[ST_CULL] += 1;
+                if (kStats) st.v[ST_CULL] += 1;
             }
             const unsigned bal = __ballot_sync(kFull, keep);
             if (keep) ws.cand[ncand + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)o;
@@ -362,32 +365,38 @@ __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, cons
         bool flagged = false;
         for (int k = jr.apx_beg; k < jr.apx_end && !flagged; ++k) {
             const float4 sa = M.A[k];
-            float px[kBatch], py[kBatch], pz[kBatch], sr[kBatch];
-            sphere_world(T, sa.x, sa.y, sa.z, px[0], py[0], pz[0]);
-            sr[0] = __fadd_rn(sa.w, margin);
-            st.v[ST_SPHERES] += 1;
-            flagged = batch_hits(sc, ws.cand, ncand, px, py, pz, sr, 1, g, st);
+            float px, py, pz;
+            sphere_world(T, sa.x, sa.y, sa.z, px, py, pz);
+            const float sr = __fadd_rn(sa.w, margin);
+            if (kStats) st.v[ST_SPHERES] += 1;
+            flagged = spheres_hit<1, kStats>(sc, ws.cand, ncand, &px, &py, &pz, &sr, g, st);
         }
-        // ---- exact spheres of a flagged joint, 8 at a time ----
+        // ---- exact spheres of a flagged joint: 4 at a time, then singles ----
         if (flagged && !hit) {
-            for (int k0 = jr.sph_beg; k0 < jr.sph_end && !hit; k0 += kBatch) {
-                const int nb = min(kBatch, jr.sph_end - k0);
-                float px[kBatch], py[kBatch], pz[kBatch], sr[kBatch];
+            int k = jr.sph_beg;
+            for (; k + 4 <= jr.sph_end && !hit; k += 4) {
+                float px[4], py[4], pz[4], sr[4];
 #pragma unroll
-                for (int i = 0; i < kBatch; ++i) {
-                    if (i < nb) {
-                        const float4 sp = M.S[k0 + i];
-                        sphere_world(T, sp.x, sp.y, sp.z, px[i], py[i], pz[i]);
-                        sr[i] = __fadd_rn(sp.w, margin);
-                    }
+                for (int i = 0; i < 4; ++i) {
+                    const float4 sp = M.S[k + i];
+                    sphere_world(T, sp.x, sp.y, sp.z, px[i], py[i], pz[i]);
+                    sr[i] = __fadd_rn(sp.w, margin);
                 }
-                st.v[ST_SPHERES] += nb;
-                hit = batch_hits(sc, ws.cand, ncand, px, py, pz, sr, nb, g, st);
+                if (kStats) st.v[ST_SPHERES] += 4;
+                hit = spheres_hit<4, kStats>(sc, ws.cand, ncand, px, py, pz, sr, g, st);
+            }
+            for (; k < jr.sph_end && !hit; ++k) {
+                const float4 sp = M.S[k];
+                float px, py, pz;
+                sphere_world(T, sp.x, sp.y, sp.z, px, py, pz);
+                const float sr = __fadd_rn(sp.w, margin);
+                if (kStats) st.v[ST_SPHERES] += 1;
+                hit = spheres_hit<1, kStats>(sc, ws.cand, ncand, &px, &py, &pz, &sr, g, st);
             }
         }
         if (__any_sync(kFull, hit && real)) break;   // warp-uniform early exit
     }
-    if (real)
+    if (kStats && real)
         for (int k = 0; k < ST_COUNT; ++k) st_out.v[k] += st.v[k];
     return __any_sync(kFull, hit && real);
 }
@@ -423,8 +432,8 @@ size_t edge_smem_bytes(const ps_model* m, const ps_scene_view* sv) {
 // ---------------------------------------------------------------------------
 // Plain path: one warp per edge, chunks in order.
 // ---------------------------------------------------------------------------
-template <bool kFast>
-__global__ void __launch_bounds__(kEdgeThreads) edges_plain_kernel(ModelDev md, ps_scene_view sv, ps_edge_params P,
+template <bool kFast, bool kStats>
+__global__ void __launch_bounds__(kEdgeThreads, kFast ? 6 : 3) edges_plain_kernel(ModelDev md, ps_scene_view sv, ps_edge_params P,
                                                                   const float* __restrict__ from,
                                                                   const float* __restrict__ to,
                                                                   const int* __restrict__ given, int n_edges,
@@ -456,7 +465,7 @@ __global__ void __launch_bounds__(kEdgeThreads) edges_plain_kernel(ModelDev md, 
         const int chunks = G > 0 ? (G + 31) / 32 : 0;
         for (int c = 0; c < chunks; ++c) {
             float cm = FLT_MAX;
-            if (kFast) bad |= process_chunk_fast(M, sc, P, from, to, e, G, c, ws, st);
+            if (kFast) bad |= process_chunk_fast<kStats>(M, sc, P, from, to, e, G, c, ws, st);
             else bad |= process_chunk(M, sc, sv, P, from, to, e, G, c, ws, P.compute_clearance ? &cm : nullptr, st);
             emin = fminf(emin, cm);
             if (bad && !P.compute_clearance) break;
@@ -493,8 +502,8 @@ __global__ void edges_prep_kernel(ps_edge_params P, const float* __restrict__ fr
     if ((threadIdx.x & 31) == 0 && local_max > 0) atomicMax(&hdr->max_G, local_max);
 }
 
-template <bool kFast>
-__global__ void __launch_bounds__(kEdgeThreads, 4) edges_queue_kernel(ModelDev md, ps_scene_view sv, ps_edge_params P,
+template <bool kFast, bool kStats>
+__global__ void __launch_bounds__(kEdgeThreads, kFast ? 6 : 3) edges_queue_kernel(ModelDev md, ps_scene_view sv, ps_edge_params P,
                                                                   const float* __restrict__ from,
                                                                   const float* __restrict__ to, int n_edges,
                                                                   EdgeWs* hdr, const int* __restrict__ Gs, int* bad,
@@ -528,8 +537,13 @@ __global__ void __launch_bounds__(kEdgeThreads, 4) edges_queue_kernel(ModelDev m
         int e = -1, k = 0, G = 0;
         bool live = false;
         if (item < total) {
-            k = (int)(item / n_edges);
-            e = (int)(item - (long long)k * n_edges);
+            if (total < (1ll << 31)) {   // 32-bit division in the common case
+                k = (int)((unsigned)item / (unsigned)n_edges);
+                e = (int)((unsigned)item - (unsigned)k * (unsigned)n_edges);
+            } else {
+                k = (int)(item / n_edges);
+                e = (int)(item - (long long)k * n_edges);
+            }
             G = __ldg(Gs + e);
             live = (k * 32 < G) && vbad[e] == 0;
         }
@@ -545,7 +559,7 @@ __global__ void __launch_bounds__(kEdgeThreads, 4) edges_queue_kernel(ModelDev m
             retired = __shfl_sync(kFull, retired, 0);
             if (!P.compute_clearance && retired) continue;   // retired meanwhile
             float cm = FLT_MAX;
-            const bool h = kFast ? process_chunk_fast(M, sc, P, from, to, ee, GG, kk, ws, st)
+            const bool h = kFast ? process_chunk_fast<kStats>(M, sc, P, from, to, ee, GG, kk, ws, st)
                                  : process_chunk(M, sc, sv, P, from, to, ee, GG, kk, ws,
                                                  P.compute_clearance ? &cm : nullptr, st);
             if (lane == 0) {
@@ -606,7 +620,9 @@ extern "C" int ps_check_edges_plain(const ps_model* m, const ps_scene_view* scen
     cudaStream_t s = (cudaStream_t)stream;
     const size_t smem = edge_smem_bytes(m, scene);
     const int grid = (n_edges + kWarps - 1) / kWarps;
-    auto kern = fast_path(m, scene, P) ? edges_plain_kernel<true> : edges_plain_kernel<false>;
+    const bool fp = fast_path(m, scene, P), stt = g_stats != nullptr;
+    auto kern = fp ? (stt ? edges_plain_kernel<true, true> : edges_plain_kernel<true, false>)
+                   : (stt ? edges_plain_kernel<false, true> : edges_plain_kernel<false, false>);
     PS_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     mark_start(s);
     kern<<<grid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, samples_per_edge, n_edges, valid, cost,
@@ -646,7 +662,9 @@ extern "C" int ps_check_edges(const ps_model* m, const ps_scene_view* scene, con
     PS_TRY_CUDA(cudaGetLastError());
 
     const size_t smem = edge_smem_bytes(m, scene);
-    auto qk = fast_path(m, scene, P) ? edges_queue_kernel<true> : edges_queue_kernel<false>;
+    const bool fp = fast_path(m, scene, P), stt = g_stats != nullptr;
+    auto qk = fp ? (stt ? edges_queue_kernel<true, true> : edges_queue_kernel<true, false>)
+                 : (stt ? edges_queue_kernel<false, true> : edges_queue_kernel<false, false>);
     PS_TRY_CUDA(cudaFuncSetAttribute(qk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qk, kEdgeThreads, smem));
@@ -736,7 +754,9 @@ extern "C" int ps_check_edges_static(const ps_model* m, const ps_scene_view* sce
     edges_prep_kernel<<<pgrid, 256, 0, s>>>(*P, from, to, samples_per_edge, n_edges, D, hdr, G, len, bad, clr);
     PS_TRY_CUDA(cudaGetLastError());
     const size_t smem = edge_smem_bytes(m, scene);
-    auto qk = fast_path(m, scene, P) ? edges_queue_kernel<true> : edges_queue_kernel<false>;
+    const bool fp = fast_path(m, scene, P), stt = g_stats != nullptr;
+    auto qk = fp ? (stt ? edges_queue_kernel<true, true> : edges_queue_kernel<true, false>)
+                 : (stt ? edges_queue_kernel<false, true> : edges_queue_kernel<false, false>);
     PS_TRY_CUDA(cudaFuncSetAttribute(qk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qk, kEdgeThreads, smem));
