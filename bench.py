@@ -302,6 +302,7 @@ def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev):
     # ---- other workloads: configs (1) and CHOMP cost+gradient (3) ----
     res["configs"] = bench_configs(dev)
     res["chomp"] = bench_chomp(dev)
+    res["mixed"] = bench_mixed(dev)
     return res
 
 
@@ -436,6 +437,82 @@ def bench_chomp(dev):
     except Exception as e:
         out["reference_gpu"] = {"unavailable": str(e)[:200]}
     return out
+
+
+def bench_mixed(dev, reps: int = 10):
+    """Mixed-size batch on the 14-DoF composite (128 OBBs + 128^3 ESDF): 65
+    edge requests of 16..256 edges (8192 edges, 1..600 samples each) and 64
+    CHOMP trajectories of 32..128 waypoints with cost + gradient. Plain =
+    one per-request call each (ps_check_edges_plain, ps_traj_cost), batched =
+    one replay of the mixed graph. Checked configurations = sum of edge
+    samples + waypoints."""
+    import torch
+
+    from prismplan_b200 import api, workloads
+    from prismplan_b200.robot import RobotModelBuilder
+    from prismplan_b200.scene import SceneTensors
+
+    wl = workloads.workload(5)
+    b = RobotModelBuilder.from_asset(wl["asset"]).build()
+    sc = SceneTensors(*wl["obbs"], *wl["esdf"])
+    frm = torch.from_numpy(wl["from"]).to(dev)
+    to = torch.from_numpy(wl["to"]).to(dev)
+    trajs = [torch.from_numpy(q).to(dev) for q in wl["trajectories"]]
+    ep = api.EdgeEvalParams(max_joint_step=STEP_RAD, max_samples=MAX_SAMPLES)
+    cp = api.CostParams(collision_cost_weight=wl["w"], world_collision_margin=wl["eps"],
+                        self_collision_margin=wl["self_margin"], smoothness_weight=1.0, delta_t=0.1)
+    splits = wl["edge_splits"]
+    n_wp = sum(len(q) for q in trajs)
+    checked = int(wl["G"].sum()) + n_wp
+    slices, off = [], 0
+    for k in splits:
+        slices.append(slice(off, off + k))
+        off += k
+
+    def plain():
+        for sl in slices:
+            api.check_edges(b, sc, frm[sl], to[sl], params=ep, persistent=False)
+        for q in trajs:
+            api.traj_cost(b, sc, q[None], cp)
+
+    for _ in range(2):
+        plain()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        plain()
+    torch.cuda.synchronize()
+    plain_ms = (time.perf_counter() - t0) * 1e3 / reps
+
+    batch = api.MixedBatch(b, len(splits), len(wl["from"]), len(trajs), n_wp, 128)
+    for sl in slices:
+        batch.add_edges(frm[sl], to[sl])
+    for q in trajs:
+        batch.add_trajectory(q)
+    tune = batch.tune(sc, ep, cp)
+    stream = torch.cuda.Stream(device=dev)
+    for _ in range(3):
+        batch.launch(sc, ep, cp, stream=stream)
+    stream.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(reps):
+            batch.launch(sc, ep, cp, stream=stream)
+        e1.record(stream)
+    stream.synchronize()
+    wall_ms = (time.perf_counter() - t0) * 1e3 / reps
+    dev_ms = e0.elapsed_time(e1) / reps
+    batch.close()
+    return {"workload": wl["name"], "requests": {"edge": len(splits), "edges": len(wl["from"]),
+                                                  "trajectories": len(trajs), "waypoints": n_wp},
+            "checked_configs_per_step": checked, "unit": "configs/s",
+            "plain": {"value": checked / (plain_ms * 1e-3), "ms_per_step": plain_ms,
+                      "path": "per-request ps_check_edges_plain + ps_traj_cost calls, one sync per step"},
+            "batched": {"value": checked / (wall_ms * 1e-3), "ms_per_step": wall_ms, "device_ms": dev_ms,
+                        "path": "ps_batch_launch (one graph replay: edge + trajectory branches)"},
+            "speedup": plain_ms / wall_ms, "tuning": tune}
 
 
 def run_reference(args):

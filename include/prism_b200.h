@@ -249,6 +249,7 @@ int ps_check_edges_static(const ps_model* model, const ps_scene_view* scene,
  * (cpp/src/planning/chomp.cu:196-210) with R from
  * cpp/src/planning/chomp_precompute.cpp:20-37 applied as a banded stencil.
  * ========================================================================= */
+#define PS_MAX_TRAJ_LEN 16384  /* longest trajectory with a smoothness term */
 #define PS_LAYOUT_BTD  0   /* q[b][t][d]  (torch-natural)                        */
 #define PS_LAYOUT_BDT  1   /* q[b][d][t]  (reference theta[d*T+t], rollouts[(r*D+d)*T+t]) */
 
@@ -282,6 +283,72 @@ int ps_rollout_costs(const ps_model* model, const ps_scene_view* scene,
                      const float* rollouts, int n_rows, int T,
                      const ps_cost_params* params, int broadcast_d,
                      float* state_cost, void* stream);
+
+/* =========================================================================
+ * Mixed-request batches: many edge-check requests of uneven length and many
+ * trajectory cost+gradient requests evaluated by one CUDA-graph launch.
+ * Replaces the reference's one-launch-and-sync-per-request pattern
+ * (EdgeEvalGpu::evaluate, cpp/src/planning/edge_batch_bridge.hh:60-96; the
+ * CHOMP iteration loop, cpp/src/planning/chomp.cu:508-555; the STOMP rollout
+ * cost launch, cpp/src/planning/stomp.cu:206-245). No reference counterpart
+ * for the batching itself.
+ *
+ * Requests hold caller device pointers; nothing is copied until launch. The
+ * first launch (and any launch whose scene/params/tuning differ from the
+ * last) captures the graph; later launches replay it with the new request
+ * table, so a planner can re-fill and launch every iteration without
+ * re-capture. Results equal the per-request calls bit for bit:
+ *   edges        == ps_check_edges / ps_check_edges_plain (valid, cost);
+ *   trajectories == ps_traj_cost(B=1, PS_LAYOUT_BTD) (waypoint_cost,
+ *                   traj_cost, grad).
+ * ps_batch_create allocates the packed device buffers and pinned host
+ * tables; ps_batch_launch allocates nothing. A launch waits (host) for the
+ * previous launch of the same batch before it rewrites the request table.
+ * ========================================================================= */
+typedef struct ps_batch ps_batch;
+
+typedef struct ps_batch_limits {
+    int max_edge_requests;   /* requests of edge checks                       */
+    int max_edges;           /* total edges over all edge requests            */
+    int max_traj_requests;   /* trajectory requests                           */
+    int max_waypoints;       /* total waypoints over all trajectory requests  */
+    int max_traj_len;        /* longest trajectory, <= PS_MAX_TRAJ_LEN        */
+} ps_batch_limits;
+
+typedef struct ps_batch_tuning {
+    float edge_share;        /* fraction of the edge kernel's resident-block
+                                slots its persistent grid takes              */
+    float traj_share;        /* same for the trajectory kernel's grid         */
+    int   traj_threads;      /* waypoints per block of the trajectory kernel  */
+    float best_ms;           /* measured time of one launch at this choice    */
+} ps_batch_tuning;
+
+int ps_batch_create(const ps_model* model, const ps_batch_limits* limits,
+                    ps_batch** out);
+int ps_batch_destroy(ps_batch* batch);
+/* Forget every request (buffers stay allocated). */
+int ps_batch_clear(ps_batch* batch);
+/* n edges from[n*D] -> to[n*D] (device). samples: device [n] or NULL (the
+   launch's ps_edge_params rule). Outputs valid[n], cost[n] (device). */
+int ps_batch_add_edges(ps_batch* batch, const float* from, const float* to,
+                       const int* samples, int n, uint8_t* valid, float* cost);
+/* One trajectory q[T*D] (device, waypoint-major). Outputs (device, each may
+   be NULL): waypoint_cost[T], traj_cost[1], grad[T*D]. A request with only
+   waypoint_cost is a STOMP rollout. */
+int ps_batch_add_trajectory(ps_batch* batch, const float* q, int T,
+                            float* waypoint_cost, float* traj_cost, float* grad);
+/* Evaluates every request. params->compute_clearance must be 0 and
+   cost->layout PS_LAYOUT_BTD. */
+int ps_batch_launch(ps_batch* batch, const ps_scene_view* scene,
+                    const ps_edge_params* params, const ps_cost_params* cost,
+                    void* stream);
+/* Autotuner: times every candidate split of the SMs between the edge and the
+   trajectory branch and every trajectory tile width on the batch's current
+   requests, keeps the fastest for later launches and reports it (out may be
+   NULL). Synchronous; launches the batch several times. */
+int ps_batch_tune(ps_batch* batch, const ps_scene_view* scene,
+                  const ps_edge_params* params, const ps_cost_params* cost,
+                  ps_batch_tuning* out);
 
 /* =========================================================================
  * Diagnostics

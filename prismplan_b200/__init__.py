@@ -14,6 +14,7 @@ from .api import (  # noqa: F401
     CostParams,
     EdgeEvalGpu,
     EdgeEvalParams,
+    MixedBatch,
     check_collision_scene,
     check_configs,
     check_edges,

@@ -104,6 +104,21 @@ class CostParams(C.Structure):
     ]
 
 
+class BatchLimits(C.Structure):
+    _fields_ = [
+        ("max_edge_requests", C.c_int), ("max_edges", C.c_int),
+        ("max_traj_requests", C.c_int), ("max_waypoints", C.c_int),
+        ("max_traj_len", C.c_int),
+    ]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [
+        ("edge_share", C.c_float), ("traj_share", C.c_float),
+        ("traj_threads", C.c_int), ("best_ms", C.c_float),
+    ]
+
+
 # (name, restype, argtypes)
 _SIGNATURES = [
     ("ps_last_error", C.c_char_p, []),
@@ -133,6 +148,18 @@ _SIGNATURES = [
     ("ps_rollout_costs", C.c_int,
      [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_int, C.c_int,
       C.POINTER(CostParams), C.c_int, C.c_void_p, C.c_void_p]),
+    ("ps_batch_create", C.c_int, [C.c_void_p, C.POINTER(BatchLimits), C.POINTER(C.c_void_p)]),
+    ("ps_batch_destroy", C.c_int, [C.c_void_p]),
+    ("ps_batch_clear", C.c_int, [C.c_void_p]),
+    ("ps_batch_add_edges", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    ("ps_batch_add_trajectory", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("ps_batch_launch", C.c_int,
+     [C.c_void_p, C.POINTER(SceneView), C.POINTER(EdgeParams), C.POINTER(CostParams), C.c_void_p]),
+    ("ps_batch_tune", C.c_int,
+     [C.c_void_p, C.POINTER(SceneView), C.POINTER(EdgeParams), C.POINTER(CostParams),
+      C.POINTER(BatchTuning)]),
     ("ps_fk_spheres", C.c_int,
      [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     ("ps_probe_fp32_peak", C.c_int, [C.POINTER(C.c_double), C.c_void_p]),

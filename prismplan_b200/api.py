@@ -320,6 +320,104 @@ def rollout_costs(robot: RobotModelBuilder, scene, rollouts, params: Optional[Co
     return out
 
 
+# ---------------------------------------------------------------------------
+# mixed-request batches
+# ---------------------------------------------------------------------------
+class MixedBatch:
+    """Many edge-check requests and trajectory cost/gradient requests in one
+    CUDA-graph launch (ps_batch_*). Results equal ``check_edges`` and
+    ``traj_cost`` per request bit for bit. Requests keep references to their
+    tensors until ``clear``; ``launch`` is asynchronous on the stream."""
+
+    def __init__(self, robot: RobotModelBuilder, max_edge_requests: int = 0, max_edges: int = 0,
+                 max_traj_requests: int = 0, max_waypoints: int = 0, max_traj_len: int = 0):
+        self.robot = robot
+        lim = _lib.BatchLimits(int(max_edge_requests), int(max_edges), int(max_traj_requests),
+                               int(max_waypoints), int(max_traj_len))
+        h = C.c_void_p()
+        _lib.check(_lib.load().ps_batch_create(_model(robot), C.byref(lim), C.byref(h)))
+        self._h = h
+        self._keep = []
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise RuntimeError("batch is closed")
+        return self._h
+
+    def clear(self):
+        _lib.check(_lib.load().ps_batch_clear(self.handle))
+        self._keep = []
+
+    def add_edges(self, frm, to, samples=None):
+        """Queue edges frm/to [n, n_dof]; returns (valid uint8 [n], cost f32 [n])
+        filled by the next launch."""
+        torch = _torch()
+        frm = _dev_f32(frm, self.robot.n_dof)
+        to = _dev_f32(to, self.robot.n_dof)
+        n = frm.shape[0]
+        if to.shape[0] != n:
+            raise ValueError("from/to row counts differ")
+        if samples is not None:
+            samples = torch.as_tensor(samples).to(device=frm.device, dtype=torch.int32).contiguous()
+            if samples.shape[0] != n:
+                raise ValueError("samples must have one entry per edge")
+        valid = torch.empty(n, dtype=torch.uint8, device=frm.device)
+        cost = torch.empty(n, dtype=torch.float32, device=frm.device)
+        _lib.check(_lib.load().ps_batch_add_edges(self.handle, frm.data_ptr(), to.data_ptr(),
+                                                  samples.data_ptr() if samples is not None else None, n,
+                                                  valid.data_ptr(), cost.data_ptr()))
+        self._keep += [frm, to, samples, valid, cost]
+        return valid, cost
+
+    def add_trajectory(self, q, want_waypoint: bool = True, want_traj: bool = True, want_grad: bool = True):
+        """Queue one trajectory q [T, n_dof]; returns (waypoint_cost [T] | None,
+        traj_cost [1] | None, grad [T, n_dof] | None) filled by the next launch."""
+        torch = _torch()
+        q = _dev_f32(q, self.robot.n_dof)
+        if q.dim() != 2:
+            raise ValueError("q must be [T, n_dof]")
+        T = q.shape[0]
+        wp = torch.empty(T, dtype=torch.float32, device=q.device) if want_waypoint else None
+        tc = torch.empty(1, dtype=torch.float32, device=q.device) if want_traj else None
+        g = torch.empty_like(q) if want_grad else None
+        ptr = lambda t: t.data_ptr() if t is not None else None  # noqa: E731
+        _lib.check(_lib.load().ps_batch_add_trajectory(self.handle, q.data_ptr(), T, ptr(wp), ptr(tc), ptr(g)))
+        self._keep += [q, wp, tc, g]
+        return wp, tc, g
+
+    def launch(self, scene, edge_params: Optional[EdgeEvalParams] = None,
+               cost_params: Optional[CostParams] = None, stream=None):
+        ep = (edge_params or EdgeEvalParams()).to_c()
+        cp = (cost_params or CostParams()).to_c(_lib.PS_LAYOUT_BTD)
+        v = _view(scene)
+        _lib.check(_lib.load().ps_batch_launch(self.handle, C.byref(v), C.byref(ep), C.byref(cp),
+                                               _stream(stream)))
+
+    def tune(self, scene, edge_params: Optional[EdgeEvalParams] = None,
+             cost_params: Optional[CostParams] = None) -> dict:
+        """Autotune the SM split and trajectory tile width on the queued requests."""
+        ep = (edge_params or EdgeEvalParams()).to_c()
+        cp = (cost_params or CostParams()).to_c(_lib.PS_LAYOUT_BTD)
+        v = _view(scene)
+        t = _lib.BatchTuning()
+        _lib.check(_lib.load().ps_batch_tune(self.handle, C.byref(v), C.byref(ep), C.byref(cp), C.byref(t)))
+        return {"edge_share": t.edge_share, "traj_share": t.traj_share, "traj_threads": t.traj_threads,
+                "best_ms": t.best_ms}
+
+    def close(self):
+        if self._h is not None:
+            _lib.check(_lib.load().ps_batch_destroy(self._h))
+            self._h = None
+            self._keep = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def _make_autograd():
     torch = _torch()
 

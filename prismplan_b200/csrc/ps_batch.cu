@@ -1,0 +1,572 @@
+// ps_batch.cu -- mixed-request batches: many edge-check requests of uneven
+// length and many trajectory cost+gradient requests in one CUDA-graph launch.
+//
+// The reference evaluates each request with its own launches and a host sync
+// (EdgeEvalGpu::evaluate, edge_batch_bridge.hh:60-96; the CHOMP loop,
+// chomp.cu:508-555; STOMP's state cost launch, stomp.cu:206-245). Here a batch
+// keeps its request table in pinned host memory and one captured graph
+//   1. copies the table and the live counts to the device,
+//   2. forks two branches that run concurrently on disjoint SM shares:
+//      edges:        gather rows + resolve G -> prep -> persistent chunk-major
+//                    queue kernel -> finalize -> scatter to each request;
+//      trajectories: gather waypoints -> one cost+adjoint kernel over every
+//                    waypoint -> one block per request adds the smoothness
+//                    term and writes the request's outputs,
+//   3. joins.
+// Every kernel reads the counts from device memory, so the graph captured
+// once is replayed for any request mix within the capacities. ps_batch_tune
+// times candidate SM splits and trajectory tile widths on the current
+// requests and keeps the fastest.
+#include <algorithm>
+#include <cfloat>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ps_costlane.cuh"
+#include "ps_edgekern.cuh"
+
+namespace ps {
+namespace {
+
+struct EdgeReq {           // one edge request as the device reads it
+    const float* from;     // [n][D]
+    const float* to;       // [n][D]
+    const int* samples;    // [n] or NULL: the params rule
+    uint8_t* valid;        // [n]
+    float* cost;           // [n]
+    int n, offset;         // rows, first packed row
+};
+
+struct TrajReq {
+    const float* q;        // [T][D]
+    float* wp_cost;        // [T] or NULL
+    float* traj_cost;      // [1] or NULL
+    float* grad;           // [T][D] or NULL
+    int T, offset;         // waypoints, first packed waypoint
+};
+
+struct Counts {
+    int n_edge_req, n_traj_req, n_edges, n_wp;
+};
+
+constexpr int kFinishThreads = 128;   // same block width as ps_traj_cost's smoothness pass
+
+// Packs every edge request's rows and resolves each edge's sample count.
+__global__ void batch_gather_edges(const EdgeReq* __restrict__ req, const Counts* __restrict__ cnt,
+                                   ps_edge_params P, int D, float* __restrict__ from, float* __restrict__ to,
+                                   int* __restrict__ G) {
+    const int nreq = cnt->n_edge_req;
+    for (int r = blockIdx.x; r < nreq; r += gridDim.x) {
+        const EdgeReq q = req[r];
+        const size_t base = (size_t)q.offset * D;
+        for (int i = threadIdx.x; i < q.n * D; i += blockDim.x) {
+            from[base + i] = q.from[i];
+            to[base + i] = q.to[i];
+        }
+        for (int i = threadIdx.x; i < q.n; i += blockDim.x) {
+            const float* a = q.from + (size_t)i * D;
+            const float* b = q.to + (size_t)i * D;
+            G[q.offset + i] = edge_samples(P, q.samples, i, a, b, D, edge_length(a, b, D));
+        }
+    }
+}
+
+__global__ void batch_scatter_edges(const EdgeReq* __restrict__ req, const Counts* __restrict__ cnt,
+                                    const uint8_t* __restrict__ valid, const float* __restrict__ cost) {
+    const int nreq = cnt->n_edge_req;
+    for (int r = blockIdx.x; r < nreq; r += gridDim.x) {
+        const EdgeReq q = req[r];
+        for (int i = threadIdx.x; i < q.n; i += blockDim.x) {
+            q.valid[i] = valid[q.offset + i];
+            q.cost[i] = cost[q.offset + i];
+        }
+    }
+}
+
+// Packs every trajectory's waypoints and zeroes their packed gradient rows.
+__global__ void batch_gather_traj(const TrajReq* __restrict__ req, const Counts* __restrict__ cnt, int D,
+                                  float* __restrict__ q, float* __restrict__ grad) {
+    const int nreq = cnt->n_traj_req;
+    for (int r = blockIdx.x; r < nreq; r += gridDim.x) {
+        const TrajReq t = req[r];
+        const size_t base = (size_t)t.offset * D;
+        for (int i = threadIdx.x; i < t.T * D; i += blockDim.x) {
+            q[base + i] = t.q[i];
+            grad[base + i] = 0.0f;
+        }
+    }
+}
+
+size_t waypoint_smem_bytes(const ps_model* m, const ps_scene_view* sv, int threads) {
+    return (size_t)m->dev.bytes_core + scene_smem_bytes(sv) +
+           (size_t)(m->info.n_spheres * 3 + m->info.n_joints * 12) * threads * 4 + (size_t)m->info.n_spheres + 16;
+}
+
+// Cost and adjoint of every packed waypoint (lane = waypoint), grid-stride.
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads) batch_waypoint_kernel(ModelDev md, ps_scene_view sv, ps_cost_params P,
+                                                                  const Counts* __restrict__ cnt,
+                                                                  const float* __restrict__ q,
+                                                                  float* __restrict__ wp_cost,
+                                                                  float* __restrict__ grad) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ int counters[4];
+    __shared__ float bmax;
+    const int n_wp = cnt->n_wp;
+    if ((long long)blockIdx.x * kThreads >= n_wp) return;   // nothing for this block: skip staging
+    if (!stage_model(md, smem, &mbar)) return;
+    const ModelSmem M = model_view(smem);
+    const int D = M.H->n_dof, NJ = M.H->n_joints, NS = M.H->n_spheres;
+    ObbPrep* obbs = reinterpret_cast<ObbPrep*>(smem + md.bytes_core);
+    const int nob = max(sv.n_obbs, 1);
+    int* orig = reinterpret_cast<int*>(obbs + nob);
+    LayerPrep* layers = reinterpret_cast<LayerPrep*>(orig + ((nob + 3) & ~3));
+    float* pos = reinterpret_cast<float*>(layers + PS_MAX_LAYERS);
+    float* jf = pos + (size_t)NS * 3 * kThreads;
+    unsigned char* sph_joint = reinterpret_cast<unsigned char*>(jf + (size_t)NJ * 12 * kThreads);
+    SceneSmem sc;
+    stage_scene(sv, obbs, orig, layers, counters, &bmax, sc);
+    for (int p = 0; p < NJ; ++p)
+        for (int k = M.J[p].sph_beg + threadIdx.x; k < M.J[p].sph_end; k += blockDim.x) sph_joint[k] = (unsigned char)p;
+    __syncthreads();
+    const int lane = threadIdx.x;
+    LaneStats st;
+    st.zero();
+    for (int k = blockIdx.x * kThreads + lane; k - lane < n_wp; k += gridDim.x * kThreads) {
+        if (k >= n_wp) continue;
+        wp_cost[k] = waypoint_cost_lane<true>(M, md, sc, sv, P, q + (size_t)k * D, pos + lane, jf + lane, sph_joint,
+                                              kThreads, grad + (size_t)k * D, 1, st);
+    }
+}
+
+// One block per trajectory request: outputs waypoint costs, the gradient
+// (adjoint + smoothness) and the total, exactly as ps_traj_cost computes them.
+__global__ void __launch_bounds__(kFinishThreads) batch_traj_finish(const TrajReq* __restrict__ req,
+                                                                    const Counts* __restrict__ cnt, int D,
+                                                                    ps_cost_params P, const float* __restrict__ q,
+                                                                    const float* __restrict__ wp_cost,
+                                                                    const float* __restrict__ grad) {
+    extern __shared__ float sh[];
+    const int nreq = cnt->n_traj_req;
+    for (int r = blockIdx.x; r < nreq; r += gridDim.x) {
+        const TrajReq t = req[r];
+        const float* qr = q + (size_t)t.offset * D;
+        const float* wr = wp_cost + t.offset;
+        if (t.wp_cost)
+            for (int i = threadIdx.x; i < t.T; i += blockDim.x) t.wp_cost[i] = wr[i];
+        if (t.grad)
+            for (int i = threadIdx.x; i < t.T * D; i += blockDim.x) t.grad[i] = grad[(size_t)t.offset * D + i];
+        __syncthreads();   // the copied rows are read back by other threads below
+        if (!t.traj_cost && !(t.grad && P.smoothness_weight != 0.0f)) continue;
+        float* g = t.grad;
+        const float tot = traj_smooth_block([&](int tt, int d) { return qr[(size_t)tt * D + d]; },
+                                            [&](int tt, int d, float v) { g[(size_t)tt * D + d] += v; },
+                                            [&](int tt) { return wr[tt]; }, t.T, D, P, g != nullptr, sh);
+        if (threadIdx.x == 0 && t.traj_cost) *t.traj_cost = tot;
+    }
+}
+
+size_t align256b(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+}  // namespace ps
+
+using namespace ps;
+
+struct ps_batch {
+    const ps_model* model = nullptr;
+    ps_batch_limits lim{};
+    std::vector<EdgeReq> ereq;
+    std::vector<TrajReq> treq;
+    int n_edges = 0, n_wp = 0;
+    // pinned mirrors read by every replay
+    EdgeReq* h_ereq = nullptr;
+    TrajReq* h_treq = nullptr;
+    Counts* h_cnt = nullptr;
+    // one device allocation holds every packed buffer
+    void* dmem = nullptr;
+    EdgeReq* d_ereq = nullptr;
+    TrajReq* d_treq = nullptr;
+    Counts* d_cnt = nullptr;
+    float *d_from = nullptr, *d_to = nullptr, *d_len = nullptr, *d_cost = nullptr;
+    int *d_given = nullptr, *d_G = nullptr, *d_bad = nullptr, *d_clr = nullptr;
+    uint8_t* d_valid = nullptr;
+    EdgeWs* d_hdr = nullptr;
+    float *d_q = nullptr, *d_wp_cost = nullptr, *d_grad = nullptr;
+    // captured graph and the configuration it was captured for
+    cudaGraphExec_t exec = nullptr;
+    std::vector<unsigned char> key;
+    cudaStream_t cap0 = nullptr, cap1 = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, done = nullptr;
+    bool launched = false;
+    // tuning state
+    float edge_share = 1.0f;   // of the edge kernel's full-occupancy grid
+    float traj_share = 0.5f;   // of the trajectory kernel's full-occupancy grid
+    int traj_threads = 32;
+};
+
+namespace {
+
+struct LaunchPlan {
+    int mode = 0;
+    void (*qk)(ModelDev, ps_scene_view, ps_edge_params, const float*, const float*, int, EdgeWs*, const int*, int*,
+               int*, unsigned long long*, const int*) = nullptr;
+    size_t qsmem = 0, wsmem = 0, fsmem = 0;
+    int qgrid = 1, wgrid = 1, req_grid_e = 1, req_grid_t = 1, pgrid = 1;
+};
+
+// Everything that is not a stream operation happens before the capture.
+int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, LaunchPlan& L) {
+    const ps_model* m = b->model;
+    const int sms = sm_count();
+    if (b->lim.max_edges > 0) {
+        L.mode = fast_path(m, sv, ep);
+        L.qk = pick(L.mode, false, edges_queue_kernel<0, false>, edges_queue_kernel<0, true>,
+                    edges_queue_kernel<1, false>, edges_queue_kernel<1, true>, edges_queue_kernel<2, false>,
+                    edges_queue_kernel<2, true>);
+        L.qsmem = edge_smem_bytes(m, sv);
+        PS_TRY_CUDA(cudaFuncSetAttribute(L.qk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.qsmem));
+        int per_sm = 0;
+        PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L.qk, kEdgeThreads, L.qsmem));
+        if (per_sm < 1) return set_error(PS_EINVAL, "edge kernel does not fit on an SM with this scene");
+        L.qgrid = std::max(1, (int)(b->edge_share * sms * per_sm + 0.5f));
+        L.pgrid = std::max(1, std::min((b->lim.max_edges + 255) / 256, sms * 4));
+        L.req_grid_e = std::max(1, std::min(b->lim.max_edge_requests, sms * 8));
+    }
+    if (b->lim.max_waypoints > 0) {
+        const int tt = b->traj_threads;
+        L.wsmem = waypoint_smem_bytes(m, sv, tt);
+        int per_sm = 0;
+        if (tt == 32) {
+            PS_TRY_CUDA(cudaFuncSetAttribute(batch_waypoint_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)L.wsmem));
+            PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_waypoint_kernel<32>, 32, L.wsmem));
+        } else {
+            PS_TRY_CUDA(cudaFuncSetAttribute(batch_waypoint_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)L.wsmem));
+            PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_waypoint_kernel<64>, 64, L.wsmem));
+        }
+        if (per_sm < 1) return set_error(PS_EINVAL, "trajectory kernel does not fit on an SM with this model/scene");
+        const int cap_blocks = (b->lim.max_waypoints + tt - 1) / tt;
+        L.wgrid = std::max(1, std::min(cap_blocks, (int)(b->traj_share * sms * per_sm + 0.5f)));
+        L.fsmem = (size_t)(2 * (b->lim.max_traj_len + 12) + kFinishThreads) * sizeof(float);
+        if (L.fsmem > 48 * 1024)
+            PS_TRY_CUDA(cudaFuncSetAttribute(batch_traj_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.fsmem));
+        L.req_grid_t = std::max(1, std::min(b->lim.max_traj_requests, sms * 8));
+    }
+    return PS_OK;
+}
+
+void record_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, const ps_cost_params* cp,
+                  const LaunchPlan& L) {
+    const ps_model* m = b->model;
+    const int D = m->info.n_dof;
+    cudaStream_t s0 = b->cap0, s1 = b->cap1;
+    cudaMemcpyAsync(b->d_ereq, b->h_ereq, sizeof(EdgeReq) * std::max(b->lim.max_edge_requests, 1),
+                    cudaMemcpyHostToDevice, s0);
+    cudaMemcpyAsync(b->d_treq, b->h_treq, sizeof(TrajReq) * std::max(b->lim.max_traj_requests, 1),
+                    cudaMemcpyHostToDevice, s0);
+    cudaMemcpyAsync(b->d_cnt, b->h_cnt, sizeof(Counts), cudaMemcpyHostToDevice, s0);
+    cudaEventRecord(b->fork, s0);
+    cudaStreamWaitEvent(s1, b->fork, 0);
+    if (b->lim.max_edges > 0) {   // edge branch on s0
+        const int* n_dev = &b->d_cnt->n_edges;
+        cudaMemsetAsync(b->d_hdr, 0, sizeof(EdgeWs), s0);
+        batch_gather_edges<<<L.req_grid_e, 128, 0, s0>>>(b->d_ereq, b->d_cnt, *ep, D, b->d_from, b->d_to, b->d_given);
+        edges_prep_kernel<<<L.pgrid, 256, 0, s0>>>(*ep, b->d_from, b->d_to, b->d_given, b->lim.max_edges, D, b->d_hdr,
+                                                   b->d_G, b->d_len, b->d_bad, b->d_clr, n_dev);
+        L.qk<<<L.qgrid, kEdgeThreads, L.qsmem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to, b->lim.max_edges, b->d_hdr,
+                                                    b->d_G, b->d_bad, b->d_clr, nullptr, n_dev);
+        edges_finalize_kernel<<<L.pgrid, 256, 0, s0>>>(b->lim.max_edges, *ep, b->d_bad, b->d_len, b->d_clr,
+                                                       b->d_valid, b->d_cost, nullptr, n_dev);
+        batch_scatter_edges<<<L.req_grid_e, 128, 0, s0>>>(b->d_ereq, b->d_cnt, b->d_valid, b->d_cost);
+    }
+    if (b->lim.max_waypoints > 0) {   // trajectory branch on s1
+        batch_gather_traj<<<L.req_grid_t, 128, 0, s1>>>(b->d_treq, b->d_cnt, D, b->d_q, b->d_grad);
+        if (b->traj_threads == 32)
+            batch_waypoint_kernel<32><<<L.wgrid, 32, L.wsmem, s1>>>(m->dev, *sv, *cp, b->d_cnt, b->d_q, b->d_wp_cost,
+                                                                    b->d_grad);
+        else
+            batch_waypoint_kernel<64><<<L.wgrid, 64, L.wsmem, s1>>>(m->dev, *sv, *cp, b->d_cnt, b->d_q, b->d_wp_cost,
+                                                                    b->d_grad);
+        batch_traj_finish<<<L.req_grid_t, kFinishThreads, L.fsmem, s1>>>(b->d_treq, b->d_cnt, D, *cp, b->d_q,
+                                                                         b->d_wp_cost, b->d_grad);
+    }
+    cudaEventRecord(b->join, s1);
+    cudaStreamWaitEvent(s0, b->join, 0);
+}
+
+int batch_capture(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, const ps_cost_params* cp) {
+    LaunchPlan L;
+    if (int rc = plan_launch(b, sv, ep, L)) return rc;
+    PS_TRY_CUDA(cudaStreamBeginCapture(b->cap0, cudaStreamCaptureModeThreadLocal));
+    record_graph(b, sv, ep, cp, L);
+    cudaGraph_t g = nullptr;
+    const cudaError_t le = cudaGetLastError();
+    cudaError_t e = cudaStreamEndCapture(b->cap0, &g);
+    if (le != cudaSuccess || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return cuda_error(le != cudaSuccess ? le : e, "capture of the batch graph");
+    }
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+    e = cudaGraphInstantiate(&b->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_error(e, "instantiate the batch graph");
+    return PS_OK;
+}
+
+std::vector<unsigned char> make_key(const ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep,
+                                    const ps_cost_params* cp) {
+    std::vector<unsigned char> k(sizeof(*sv) + sizeof(*ep) + sizeof(*cp) + 2 * sizeof(float) + sizeof(int));
+    unsigned char* p = k.data();
+    auto put = [&](const void* src, size_t n) {
+        std::memcpy(p, src, n);
+        p += n;
+    };
+    put(sv, sizeof(*sv));
+    put(ep, sizeof(*ep));
+    put(cp, sizeof(*cp));
+    put(&b->edge_share, sizeof(float));
+    put(&b->traj_share, sizeof(float));
+    put(&b->traj_threads, sizeof(int));
+    return k;
+}
+
+void release(ps_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->cap0) cudaStreamDestroy(b->cap0);
+    if (b->cap1) cudaStreamDestroy(b->cap1);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->join) cudaEventDestroy(b->join);
+    if (b->done) cudaEventDestroy(b->done);
+    if (b->h_ereq) cudaFreeHost(b->h_ereq);
+    if (b->h_treq) cudaFreeHost(b->h_treq);
+    if (b->h_cnt) cudaFreeHost(b->h_cnt);
+    if (b->dmem) cudaFree(b->dmem);
+    delete b;
+}
+
+}  // namespace
+
+extern "C" int ps_batch_create(const ps_model* m, const ps_batch_limits* lim, ps_batch** out) {
+    clear_error();
+    if (!m || !lim || !out) return set_error(PS_EINVAL, "NULL argument");
+    *out = nullptr;
+    if (lim->max_edge_requests < 0 || lim->max_edges < 0 || lim->max_traj_requests < 0 || lim->max_waypoints < 0 ||
+        lim->max_traj_len < 0)
+        return set_error(PS_EINVAL, "negative capacity");
+    if (lim->max_edges > 0 && lim->max_edge_requests <= 0)
+        return set_error(PS_EINVAL, "max_edge_requests must be > 0 when max_edges > 0");
+    if (lim->max_waypoints > 0 && (lim->max_traj_requests <= 0 || lim->max_traj_len <= 0))
+        return set_error(PS_EINVAL, "max_traj_requests and max_traj_len must be > 0 when max_waypoints > 0");
+    if (lim->max_traj_len > PS_MAX_TRAJ_LEN) return set_error(PS_EINVAL, "max_traj_len exceeds PS_MAX_TRAJ_LEN");
+    if (m->info.n_joints > 255) return set_error(PS_EINVAL, "too many joints");
+    ps_batch* b = new ps_batch();
+    b->model = m;
+    b->lim = *lim;
+    const int D = m->info.n_dof;
+    const size_t E = (size_t)std::max(lim->max_edges, 1), W = (size_t)std::max(lim->max_waypoints, 1);
+    const size_t RE = (size_t)std::max(lim->max_edge_requests, 1), RT = (size_t)std::max(lim->max_traj_requests, 1);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off += align256b(bytes);
+        return o;
+    };
+    const size_t o_ereq = take(sizeof(EdgeReq) * RE), o_treq = take(sizeof(TrajReq) * RT), o_cnt = take(sizeof(Counts));
+    const size_t o_from = take(4 * E * D), o_to = take(4 * E * D), o_len = take(4 * E), o_cost = take(4 * E);
+    const size_t o_given = take(4 * E), o_G = take(4 * E), o_bad = take(4 * E), o_clr = take(4 * E);
+    const size_t o_valid = take(E), o_hdr = take(sizeof(EdgeWs));
+    const size_t o_q = take(4 * W * D), o_wpc = take(4 * W), o_grad = take(4 * W * D);
+    cudaError_t e = cudaMalloc(&b->dmem, off);
+    if (e != cudaSuccess) {
+        b->dmem = nullptr;
+        release(b);
+        return set_error(PS_ENOMEM, std::string("batch buffers: ") + cudaGetErrorString(e));
+    }
+    unsigned char* base = (unsigned char*)b->dmem;
+    b->d_ereq = (EdgeReq*)(base + o_ereq);
+    b->d_treq = (TrajReq*)(base + o_treq);
+    b->d_cnt = (Counts*)(base + o_cnt);
+    b->d_from = (float*)(base + o_from);
+    b->d_to = (float*)(base + o_to);
+    b->d_len = (float*)(base + o_len);
+    b->d_cost = (float*)(base + o_cost);
+    b->d_given = (int*)(base + o_given);
+    b->d_G = (int*)(base + o_G);
+    b->d_bad = (int*)(base + o_bad);
+    b->d_clr = (int*)(base + o_clr);
+    b->d_valid = base + o_valid;
+    b->d_hdr = (EdgeWs*)(base + o_hdr);
+    b->d_q = (float*)(base + o_q);
+    b->d_wp_cost = (float*)(base + o_wpc);
+    b->d_grad = (float*)(base + o_grad);
+    if (cudaHostAlloc((void**)&b->h_ereq, sizeof(EdgeReq) * RE, cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc((void**)&b->h_treq, sizeof(TrajReq) * RT, cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc((void**)&b->h_cnt, sizeof(Counts), cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        release(b);
+        return set_error(PS_ENOMEM, "pinned request tables");
+    }
+    std::memset(b->h_ereq, 0, sizeof(EdgeReq) * RE);
+    std::memset(b->h_treq, 0, sizeof(TrajReq) * RT);
+    std::memset(b->h_cnt, 0, sizeof(Counts));
+    if (cudaStreamCreateWithFlags(&b->cap0, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->cap1, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess) {
+        const cudaError_t le = cudaGetLastError();
+        release(b);
+        return cuda_error(le, "batch streams/events");
+    }
+    *out = b;
+    return PS_OK;
+}
+
+extern "C" int ps_batch_destroy(ps_batch* b) {
+    clear_error();
+    if (!b) return PS_OK;
+    if (b->launched) cudaEventSynchronize(b->done);
+    release(b);
+    return PS_OK;
+}
+
+extern "C" int ps_batch_clear(ps_batch* b) {
+    clear_error();
+    if (!b) return set_error(PS_EINVAL, "NULL batch");
+    b->ereq.clear();
+    b->treq.clear();
+    b->n_edges = b->n_wp = 0;
+    return PS_OK;
+}
+
+extern "C" int ps_batch_add_edges(ps_batch* b, const float* from, const float* to, const int* samples, int n,
+                                  uint8_t* valid, float* cost) {
+    clear_error();
+    if (!b) return set_error(PS_EINVAL, "NULL batch");
+    if (n < 0) return set_error(PS_EINVAL, "negative edge count");
+    if (n > 0 && (!from || !to || !valid || !cost)) return set_error(PS_EINVAL, "NULL edge buffer");
+    if ((int)b->ereq.size() >= b->lim.max_edge_requests) return set_error(PS_EINVAL, "too many edge requests");
+    if ((long long)b->n_edges + n > b->lim.max_edges) return set_error(PS_EINVAL, "edge capacity exceeded");
+    b->ereq.push_back(EdgeReq{from, to, samples, valid, cost, n, b->n_edges});
+    b->n_edges += n;
+    return PS_OK;
+}
+
+extern "C" int ps_batch_add_trajectory(ps_batch* b, const float* q, int T, float* waypoint_cost, float* traj_cost,
+                                       float* grad) {
+    clear_error();
+    if (!b) return set_error(PS_EINVAL, "NULL batch");
+    if (T <= 0 || !q) return set_error(PS_EINVAL, "empty trajectory or NULL q");
+    if (T > b->lim.max_traj_len) return set_error(PS_EINVAL, "trajectory longer than max_traj_len");
+    if ((int)b->treq.size() >= b->lim.max_traj_requests) return set_error(PS_EINVAL, "too many trajectory requests");
+    if ((long long)b->n_wp + T > b->lim.max_waypoints) return set_error(PS_EINVAL, "waypoint capacity exceeded");
+    b->treq.push_back(TrajReq{q, waypoint_cost, traj_cost, grad, T, b->n_wp});
+    b->n_wp += T;
+    return PS_OK;
+}
+
+extern "C" int ps_batch_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep,
+                               const ps_cost_params* cp, void* stream) {
+    clear_error();
+    if (!b || !ep || !cp) return set_error(PS_EINVAL, "NULL argument");
+    if (int rc = validate_scene(b->model, sv)) return rc;
+    if (ep->compute_clearance) return set_error(PS_EINVAL, "batched edge checks do not compute clearance");
+    if (cp->layout != PS_LAYOUT_BTD) return set_error(PS_EINVAL, "batched trajectories use PS_LAYOUT_BTD");
+    cudaStream_t s = (cudaStream_t)stream;
+    // the previous replay reads the pinned tables until it is done
+    if (b->launched) PS_TRY_CUDA(cudaEventSynchronize(b->done));
+    if (!b->ereq.empty()) std::memcpy(b->h_ereq, b->ereq.data(), sizeof(EdgeReq) * b->ereq.size());
+    if (!b->treq.empty()) std::memcpy(b->h_treq, b->treq.data(), sizeof(TrajReq) * b->treq.size());
+    *b->h_cnt = Counts{(int)b->ereq.size(), (int)b->treq.size(), b->n_edges, b->n_wp};
+    std::vector<unsigned char> key = make_key(b, sv, ep, cp);
+    if (!b->exec || key != b->key) {
+        b->key.clear();
+        if (int rc = batch_capture(b, sv, ep, cp)) return rc;
+        b->key = key;
+    }
+    PS_TRY_CUDA(cudaGraphLaunch(b->exec, s));
+    PS_TRY_CUDA(cudaEventRecord(b->done, s));
+    b->launched = true;
+    return PS_OK;
+}
+
+extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep,
+                             const ps_cost_params* cp, ps_batch_tuning* out) {
+    clear_error();
+    if (!b) return set_error(PS_EINVAL, "NULL batch");
+    const float edge_shares[] = {0.5f, 0.75f, 1.0f};
+    const float traj_shares[] = {0.25f, 0.5f, 1.0f};
+    const int widths[] = {32, 64};
+    cudaStream_t s = nullptr;
+    cudaEvent_t a = nullptr, z = nullptr;
+    PS_TRY_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&z) != cudaSuccess) {
+        const cudaError_t le = cudaGetLastError();
+        if (a) cudaEventDestroy(a);
+        cudaStreamDestroy(s);
+        return cuda_error(le, "tuning events");
+    }
+    const float keep_e = b->edge_share, keep_t = b->traj_share;
+    const int keep_w = b->traj_threads;
+    float best = 3.0e38f, best_e = keep_e, best_t = keep_t;
+    int best_w = keep_w;
+    int rc = PS_OK;
+    const bool edges = b->lim.max_edges > 0, trajs = b->lim.max_waypoints > 0;
+    for (float es : edge_shares) {
+        if (!edges && es != 1.0f) continue;
+        for (float ts : traj_shares) {
+            for (int w : widths) {
+                if (!trajs && (ts != 0.5f || w != 32)) continue;
+                b->edge_share = es;
+                b->traj_share = ts;
+                b->traj_threads = w;
+                rc = ps_batch_launch(b, sv, ep, cp, s);   // capture + warm-up
+                if (rc) break;
+                float ms_min = 3.0e38f;
+                for (int r = 0; r < 3 && rc == PS_OK; ++r) {
+                    cudaEventRecord(a, s);
+                    rc = ps_batch_launch(b, sv, ep, cp, s);
+                    cudaEventRecord(z, s);
+                    if (cudaEventSynchronize(z) != cudaSuccess) rc = cuda_error(cudaGetLastError(), "tuning run");
+                    float ms = 0.0f;
+                    cudaEventElapsedTime(&ms, a, z);
+                    ms_min = std::min(ms_min, ms);
+                }
+                if (rc) break;
+                if (ms_min < best) {
+                    best = ms_min;
+                    best_e = es;
+                    best_t = ts;
+                    best_w = w;
+                }
+            }
+            if (rc) break;
+        }
+        if (rc) break;
+    }
+    cudaStreamSynchronize(s);
+    cudaEventDestroy(a);
+    cudaEventDestroy(z);
+    cudaStreamDestroy(s);
+    if (rc) {
+        b->edge_share = keep_e;
+        b->traj_share = keep_t;
+        b->traj_threads = keep_w;
+        return rc;
+    }
+    b->edge_share = best_e;
+    b->traj_share = best_t;
+    b->traj_threads = best_w;
+    if (out) {
+        out->edge_share = best_e;
+        out->traj_share = best_t;
+        out->traj_threads = best_w;
+        out->best_ms = best;
+    }
+    return PS_OK;
+}

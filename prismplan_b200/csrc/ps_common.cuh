@@ -344,6 +344,54 @@ __device__ __forceinline__ bool esdf_sample(const LayerPrep& L, const float* fea
     return true;
 }
 
+// Trilinear sample with its world-frame gradient d(dist)/dp (the interpolant
+// is linear in each cell, so this is the exact derivative inside a cell).
+// Same lookup, guard and sentinel rules as esdf_sample in trilinear mode.
+__device__ __forceinline__ bool esdf_sample_trilinear_grad(const LayerPrep& L, const float* feat, int max_vox, float px,
+                                                           float py, float pz, float& dist, float& gx, float& gy,
+                                                           float& gz) {
+    if (!L.enabled) return false;
+    float lx, ly, lz;
+    ref_to_local(L.q.x, L.q.y, L.q.z, L.q.w, L.t.x, L.t.y, L.t.z, px, py, pz, lx, ly, lz);
+    const float inv_vs = L.t.w;
+    const int B = 2;
+    const float ux = (lx + L.params.x * 0.5f) * inv_vs, uy = (ly + L.params.y * 0.5f) * inv_vs,
+                uz = (lz + L.params.z * 0.5f) * inv_vs;
+    const float fx0 = floorf(ux), fy0 = floorf(uy), fz0 = floorf(uz);
+    if (!(fx0 > (float)B && fy0 > (float)B && fz0 > (float)B && fx0 + 1.0f < (float)(L.nx - B) &&
+          fy0 + 1.0f < (float)(L.ny - B) && fz0 + 1.0f < (float)(L.nz - B)))
+        return false;
+    const long long base = (long long)(int)fx0 * L.ny * L.nz + (long long)(int)fy0 * L.nz + (int)fz0;
+    const long long sx = (long long)L.ny * L.nz, sy = L.nz;
+    if (base + sx + sy + 1 >= max_vox) return false;
+    float v[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        v[c] = __ldg(feat + base + ((c & 1) ? sx : 0) + ((c & 2) ? sy : 0) + ((c & 4) ? 1 : 0));
+        if (v[c] <= -999.0f) return false;
+    }
+    const float fx = ux - fx0, fy = uy - fy0, fz = uz - fz0;
+    const float x00 = v[0] + fx * (v[1] - v[0]), x10 = v[2] + fx * (v[3] - v[2]);
+    const float x01 = v[4] + fx * (v[5] - v[4]), x11 = v[6] + fx * (v[7] - v[6]);
+    const float y0 = x00 + fy * (x10 - x00), y1 = x01 + fy * (x11 - x01);
+    dist = y0 + fz * (y1 - y0);
+    // d/d(fx, fy, fz) of the interpolant, then d/d(local) = * inv_vs
+    const float d00 = v[1] - v[0], d10 = v[3] - v[2], d01 = v[5] - v[4], d11 = v[7] - v[6];
+    const float dx0 = d00 + fy * (d10 - d00), dx1 = d01 + fy * (d11 - d01);
+    const float dlx = (dx0 + fz * (dx1 - dx0)) * inv_vs;
+    const float dly = ((x10 - x00) + fz * ((x11 - x01) - (x10 - x00))) * inv_vs;
+    const float dlz = (y1 - y0) * inv_vs;
+    // l = R p + t  =>  grad_p = R^T grad_l, R the matrix of the stored quaternion map
+    const float qw = L.q.x, qx = L.q.y, qy = L.q.z, qz = L.q.w;
+    const float r00 = 1.0f - 2.0f * (qy * qy + qz * qz), r01 = 2.0f * (qx * qy - qw * qz), r02 = 2.0f * (qx * qz + qw * qy);
+    const float r10 = 2.0f * (qx * qy + qw * qz), r11 = 1.0f - 2.0f * (qx * qx + qz * qz), r12 = 2.0f * (qy * qz - qw * qx);
+    const float r20 = 2.0f * (qx * qz - qw * qy), r21 = 2.0f * (qy * qz + qw * qx), r22 = 1.0f - 2.0f * (qx * qx + qy * qy);
+    gx = r00 * dlx + r10 * dly + r20 * dlz;
+    gy = r01 * dlx + r11 * dly + r21 * dlz;
+    gz = r02 * dlx + r12 * dly + r22 * dlz;
+    return true;
+}
+
 // Latch an error code into the model's status word (first error wins).
 __device__ __forceinline__ void latch_status(int* status, int code) {
     if (status) atomicCAS(status, 0, code);

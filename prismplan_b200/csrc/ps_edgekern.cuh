@@ -1,0 +1,604 @@
+// ps_edgekern.cuh -- edge-check kernels shared by the edge entry points
+// (ps_edges.cu) and the mixed-request batch (ps_batch.cu). Each translation
+// unit that includes this header gets its own private copy of the kernels.
+#pragma once
+
+#include <algorithm>
+#include <cfloat>
+
+#include "ps_internal.h"
+#include "ps_verdict.cuh"
+
+namespace ps {
+
+namespace {
+
+constexpr int kWarps = 4;               // warps per block
+constexpr int kEdgeThreads = 32 * kWarps;
+constexpr unsigned kFull = 0xffffffffu;
+
+struct EdgeWs {                         // header of the persistent workspace (64 B)
+    unsigned long long head;            // next chunk-major item
+    int max_G;
+    int pad[13];
+};
+
+__device__ __forceinline__ int ordered_float(float f) {
+    int i = __float_as_int(f);
+    return i >= 0 ? i : (i ^ 0x7fffffff);
+}
+__device__ __forceinline__ float unordered_float(int i) { return __int_as_float(i >= 0 ? i : (i ^ 0x7fffffff)); }
+
+// Sample count of an edge (edge_eval.cuh:54-60 plus the L-inf rule).
+__device__ __forceinline__ int edge_samples(const ps_edge_params& P, const int* given, int e, const float* a,
+                                            const float* b, int D, float len) {
+    if (given) return given[e];
+    if (P.resolution > 0.0f) {
+        int g = (int)ceilf(__fdiv_rn(len, P.resolution));
+        return min(max(g, 2), 1024);
+    }
+    if (P.max_joint_step > 0.0f) {
+        float m = 0.0f;
+        for (int i = 0; i < D; ++i) m = fmaxf(m, fabsf(__fadd_rn(b[i], -a[i])));
+        int g = (int)ceilf(__fdiv_rn(m, P.max_joint_step));
+        const int cap = P.max_samples > 0 ? P.max_samples : 1024;
+        return min(max(g, 1), cap);
+    }
+    return P.granularity;
+}
+
+__device__ __forceinline__ float edge_length(const float* a, const float* b, int D) {
+    float len2 = 0.0f;   // edge_eval.cuh:104-106
+    for (int i = 0; i < D; ++i) {
+        float d = __fadd_rn(b[i], -a[i]);
+        len2 = __fmaf_rn(d, d, len2);
+    }
+    return sqrtf(len2);
+}
+
+struct WarpScratch {
+    float* q;          // [32 * D]
+    uint16_t* cand;    // [n_obbs]
+};
+
+// One chunk of one edge. Returns true if any sample of the chunk collides.
+// Every lane of the warp must call it. clr_min (may be NULL) receives the
+// min ESDF clearance over the chunk's samples when compute_clearance.
+__device__ bool process_chunk(const ModelSmem& M, const SceneSmem& sc, const ps_scene_view& sv,
+                              const ps_edge_params& P, const float* __restrict__ from,
+                              const float* __restrict__ to, int e, int G, int chunk, WarpScratch ws,
+                              float* clr_min, LaneStats& st_out) {
+    const int lane = threadIdx.x & 31;
+    LaneStats st;   // padding lanes repeat a sample: their work is not credited
+    st.zero();
+    const int D = M.H->n_dof, NJ = M.H->n_joints;
+    // Reference sampling (edge_eval.cuh:110-121): t = j/G for j = 1..G in
+    // slots of 16; slots past G take t = 0, i.e. the start configuration,
+    // and their verdict counts. So the start configuration belongs to the
+    // edge verdict exactly when G % 16 != 0; a padding lane of the last chunk
+    // carries it (such a lane exists whenever G % 16 != 0), the remaining
+    // padding lanes repeat sample G and are not counted.
+    const int j_raw = chunk * 32 + lane + 1;
+    const bool in_range = j_raw <= G;
+    const bool start_lane = !in_range && (G % 16) != 0 && j_raw == G + 1;
+    const bool real = in_range || start_lane;
+    const int j = in_range ? j_raw : (start_lane ? 0 : G);
+    const float t = __fdiv_rn((float)j, (float)G);
+    const float* a = from + (size_t)e * D;
+    const float* b = to + (size_t)e * D;
+    float* qc = ws.q + lane * D;
+    for (int i = 0; i < D; ++i) {
+        const float ai = __ldg(a + i), bi = __ldg(b + i);
+        qc[i] = __fmaf_rn(t, __fadd_rn(bi, -ai), ai);
+    }
+    __syncwarp();
+    if (real) st.v[ST_SAMPLES] += 1;
+    const float margin = P.collision_margin;
+    const bool shares = M.H->approx_shares_chain != 0;
+    const bool want_clr = P.compute_clearance != 0 && clr_min != nullptr;
+
+    Affine s0, s1, T, a0, a1, TA;
+    affine_identity(s0);
+    affine_identity(s1);
+    affine_identity(a0);
+    affine_identity(a1);
+    bool hit = false;
+    float clr = 1000.0f;
+    for (int p = 0; p < NJ; ++p) {
+        const JointRec& jr = M.J[p];
+        fk_step<true>(jr, p, qc, s0, s1, T);
+        if (!shares) fk_step<true>(M.JA[p], p, qc, a0, a1, TA);
+        st.v[ST_JOINTS] += (p > 0 && real);
+        const bool has_spheres = jr.sph_end > jr.sph_beg || jr.apx_end > jr.apx_beg;
+        if (!has_spheres) continue;   // uniform across the warp
+
+        // ---- warp broad phase over boxes ----
+        const uint16_t* cand = nullptr;
+        int ncand = sc.n_obbs;
+        if (shares && sc.n_obbs > 0 && jr.bound.w >= 0.0f) {
+            float cx, cy, cz;
+            sphere_world(T, jr.bound.x, jr.bound.y, jr.bound.z, cx, cy, cz);
+            float mx = cx, my = cy, mz = cz;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                mx += __shfl_xor_sync(kFull, mx, o);
+                my += __shfl_xor_sync(kFull, my, o);
+                mz += __shfl_xor_sync(kFull, mz, o);
+            }
+            mx *= (1.0f / 32.0f);
+            my *= (1.0f / 32.0f);
+            mz *= (1.0f / 32.0f);
+            const float dx = cx - mx, dy = cy - my, dz = cz - mz;
+            float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) r2 = fmaxf(r2, __shfl_xor_sync(kFull, r2, o));
+            const float S = fmaxf(fabsf(mx), fmaxf(fabsf(my), fabsf(mz)));
+            float Rc = sqrtf(r2) + jr.bound.w + fmaxf(margin, 0.0f);
+            Rc += 4.0f * (S + Rc + sc.Bmax + 1.0f) * PS_GUARD_K;
+            const float Rc2 = Rc * Rc;
+            int count = 0;
+            __syncwarp();   // previous joint's readers of ws.cand are done
+            for (int base = 0; base < sc.n_obbs; base += 32) {
+                const int o = base + lane;
+                bool keep = false;
+                if (o < sc.n_obbs) {
+                    float qx, qy, qz;
+                    keep = fast_box_dsq(sc.obbs[o], mx, my, mz, qx, qy, qz) < Rc2;
+                    st.v[ST_CULL] += 1;
+                }
+                const unsigned bal = __ballot_sync(kFull, keep);
+                if (keep) ws.cand[count + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)o;
+                count += __popc(bal);
+            }
+            __syncwarp();
+            cand = ws.cand;
+            ncand = count;
+            if (count == 0 && sc.n_layers == 0 && !want_clr) continue;   // nothing reachable
+        }
+
+        // ---- approximate gate ----
+        bool flagged = false;
+        for (int k = jr.apx_beg; k < jr.apx_end && !flagged; ++k) {
+            const float4 sa = M.A[k];
+            float px, py, pz;
+            sphere_world(shares ? T : TA, sa.x, sa.y, sa.z, px, py, pz);
+            if (real) st.v[ST_SPHERES] += 1;
+            const float sr = __fadd_rn(sa.w, margin);
+            const uint8_t* acm =
+                sv.sphere_obb_acm_mask_approx ? sv.sphere_obb_acm_mask_approx + (size_t)M.AO[k] * sv.n_obbs : nullptr;
+            flagged = (ncand > 0 && sphere_obb_any(sc, cand, ncand, px, py, pz, sr, acm, st)) ||
+                      (sc.n_layers && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
+        }
+        // ---- exact spheres of a flagged joint (and ESDF clearance) ----
+        const bool decide = flagged && !hit;
+        if (decide || want_clr) {
+            for (int k = jr.sph_beg; k < jr.sph_end; ++k) {
+                const float4 sp = M.S[k];
+                float px, py, pz;
+                sphere_world(T, sp.x, sp.y, sp.z, px, py, pz);
+                if (real) st.v[ST_SPHERES] += 1;
+                const float sr = __fadd_rn(sp.w, margin);
+                const int so = M.SO[k];
+                const uint8_t* eacm =
+                    sv.sphere_acm_mask ? sv.sphere_acm_mask + (size_t)so * sv.n_voxel_layers : nullptr;
+                if (want_clr && sc.n_layers) clr = fminf(clr, sphere_esdf_clearance(sc, sv, px, py, pz, sr, eacm, st));
+                if (decide && !hit) {
+                    const uint8_t* acm =
+                        sv.sphere_obb_acm_mask ? sv.sphere_obb_acm_mask + (size_t)so * sv.n_obbs : nullptr;
+                    hit = (ncand > 0 && sphere_obb_any(sc, cand, ncand, px, py, pz, sr, acm, st)) ||
+                          (sc.n_layers && sphere_esdf_any(sc, sv, px, py, pz, sr, eacm, st));
+                    if (hit && !want_clr) break;
+                }
+            }
+        }
+        if (!want_clr && __any_sync(kFull, hit && real)) break;   // warp-uniform early exit
+    }
+    if (want_clr) {
+        float c = in_range ? clr : 3.0e38f;   // clearance covers j = 1..G only (edge_eval.cuh:146-151)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c = fminf(c, __shfl_xor_sync(kFull, c, o));
+        *clr_min = c;
+    }
+    if (real)
+        for (int k = 0; k < ST_COUNT; ++k) st_out.v[k] += st.v[k];
+    return __any_sync(kFull, hit && real);
+}
+
+// Fast path of process_chunk for the common scene: the approximate chain is
+// the full chain, no ACM masks, no ESDF layers, no clearance. Same verdict;
+// fewer live registers and a per-joint guard band. Exact spheres of a flagged
+// joint are tested 8 at a time against each surviving box (one box load per
+// 8 spheres), then decided from their min d^2 with the exact re-decision
+// inside the guard band.
+// Decide one sphere from its min d^2 over the candidate boxes: definite
+// outside the guard band, exact re-decision of the band's boxes otherwise.
+__device__ __forceinline__ bool decide_band(const SceneSmem& sc, const uint16_t* cand, int ncand, float px, float py,
+                                            float pz, float sr, float g, float mn, LaneStats& st) {
+    const float a = fmaxf(sr - g, 0.0f), b = sr + g;
+    const float lo = a * a * (1.0f - 1.0e-6f), hi = b * b * (1.0f + 1.0e-6f);
+    if (mn < lo) return true;
+    if (mn >= hi) return false;
+    for (int k = 0; k < ncand; ++k) {
+        const ObbPrep& o = sc.obbs[cand[k]];
+        float qx, qy, qz;
+        const float d = fast_box_dsq(o, px, py, pz, qx, qy, qz);
+        if (d < lo) return true;
+        if (d < hi) {
+            st.v[ST_EXACT] += 1;
+            if (ref_obb_hit(o, px, py, pz, sr)) return true;
+        }
+    }
+    return false;
+}
+
+// kN spheres (positions in registers) against every candidate box: one box
+// load per kN pair tests. Returns whether any of them hits.
+template <int kN, bool kStats>
+__device__ __forceinline__ bool spheres_hit(const SceneSmem& sc, const uint16_t* cand, int ncand, const float* px,
+                                            const float* py, const float* pz, const float* sr, float g,
+                                            LaneStats& st) {
+    float mn[kN];
+#pragma unroll
+    for (int i = 0; i < kN; ++i) mn[i] = 3.0e38f;
+    for (int k = 0; k < ncand; ++k) {
+        const ObbPrep& o = sc.obbs[cand[k]];
+        const float4 r0 = o.r0, r1 = o.r1, r2 = o.r2, h = o.h;
+#pragma unroll
+        for (int i = 0; i < kN; ++i) {
+            const float lx = fmaf(r0.z, pz[i], fmaf(r0.y, py[i], fmaf(r0.x, px[i], r0.w)));
+            const float ly = fmaf(r1.z, pz[i], fmaf(r1.y, py[i], fmaf(r1.x, px[i], r1.w)));
+            const float lz = fmaf(r2.z, pz[i], fmaf(r2.y, py[i], fmaf(r2.x, px[i], r2.w)));
+            const float cx = fmaxf(fabsf(lx) - h.x, 0.0f), cy = fmaxf(fabsf(ly) - h.y, 0.0f),
+                        cz = fmaxf(fabsf(lz) - h.z, 0.0f);
+            mn[i] = fminf(mn[i], fmaf(cz, cz, fmaf(cy, cy, cx * cx)));
+        }
+    }
+    if (kStats) st.v[ST_PAIRS] += ncand * kN;
+    bool hit = false;
+#pragma unroll
+    for (int i = 0; i < kN; ++i)
+        if (!hit) hit = decide_band(sc, cand, ncand, px[i], py[i], pz[i], sr[i], g, mn[i], st);
+    return hit;
+}
+
+template <bool kStats, bool kEsdf>
+__device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, const ps_scene_view& sv,
+                                   const ps_edge_params& P,
+                                   const float* __restrict__ from, const float* __restrict__ to, int e, int G,
+                                   int chunk, WarpScratch ws, LaneStats& st_out) {
+    const int lane = threadIdx.x & 31;
+    LaneStats st;
+    st.zero();
+    const int D = M.H->n_dof, NJ = M.H->n_joints;
+    // sampling rule as in process_chunk (edge_eval.cuh:110-121)
+    const int j_raw = chunk * 32 + lane + 1;
+    const bool in_range = j_raw <= G;
+    const bool start_lane = !in_range && (G % 16) != 0 && j_raw == G + 1;
+    const bool real = in_range || start_lane;
+    const int j = in_range ? j_raw : (start_lane ? 0 : G);
+    const float t = __fdiv_rn((float)j, (float)G);
+    const float* a = from + (size_t)e * D;
+    const float* b = to + (size_t)e * D;
+    float* qc = ws.q + lane * D;
+    for (int i = 0; i < D; ++i) {
+        const float ai = __ldg(a + i), bi = __ldg(b + i);
+        qc[i] = __fmaf_rn(t, __fadd_rn(bi, -ai), ai);
+    }
+    __syncwarp();
+    if (kStats && real) st.v[ST_SAMPLES] += 1;
+    const float margin = P.collision_margin;
+    // Slot 0 holds only the root's identity frame (checked on the host), so a
+    // joint's parent frame is the identity or the current frame: one 3x4
+    // frame in registers. Composing with the identity reproduces the step
+    // exactly, as the reference's slot walk does.
+    Affine T;
+    affine_identity(T);
+    bool hit = false;
+    for (int p = 0; p < NJ; ++p) {
+        const JointRec& jr = M.J[p];
+        if (p > 0) {
+            const float qi = jr.dof >= 0 ? qc[jr.dof] : 0.0f;
+            if (jr.parent_slot == 0) {
+                Affine I;
+                affine_identity(I);
+                joint_compose<true>(jr, qi, I, T);
+            } else {
+                joint_compose<true>(jr, qi, T, T);   // rows are read before they are written
+            }
+            if (kStats) st.v[ST_JOINTS] += 1;
+        }
+        if (jr.bound.w < 0.0f || (sc.n_obbs == 0 && !kEsdf)) continue;   // nothing to test (uniform)
+        // ---- warp broad phase ----
+        float cx, cy, cz;
+        sphere_world(T, jr.bound.x, jr.bound.y, jr.bound.z, cx, cy, cz);
+        float mx = cx, my = cy, mz = cz;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mx += __shfl_xor_sync(kFull, mx, o);
+            my += __shfl_xor_sync(kFull, my, o);
+            mz += __shfl_xor_sync(kFull, mz, o);
+        }
+        mx *= (1.0f / 32.0f);
+        my *= (1.0f / 32.0f);
+        mz *= (1.0f / 32.0f);
+        const float dx = cx - mx, dy = cy - my, dz = cz - mz;
+        float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r2 = fmaxf(r2, __shfl_xor_sync(kFull, r2, o));
+        const float Sm = fmaxf(fabsf(mx), fmaxf(fabsf(my), fabsf(mz)));
+        float Rc = sqrtf(r2) + jr.bound.w + fmaxf(margin, 0.0f);
+        Rc += 4.0f * (Sm + Rc + sc.Bmax + 1.0f) * PS_GUARD_K;
+        const float Rc2 = Rc * Rc;
+        int ncand = 0;
+        __syncwarp();
+        for (int base = 0; base < sc.n_obbs; base += 32) {
+            const int o = base + lane;
+            bool keep = false;
+            if (o < sc.n_obbs) {
+                float qx, qy, qz;
+                keep = fast_box_dsq(sc.obbs[o], mx, my, mz, qx, qy, qz) < Rc2;
+                if (kStats) st.v[ST_CULL] += 1;
+            }
+            const unsigned bal = __ballot_sync(kFull, keep);
+            if (keep) ws.cand[ncand + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)o;
+            ncand += __popc(bal);
+        }
+        __syncwarp();
+        if (ncand == 0 && !kEsdf) continue;   // nothing reachable from any lane (uniform)
+        // Per-joint guard: every sphere of the joint lies within bound.w of c.
+        const float S = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))) + jr.bound.w;
+        const float g = (S + sc.Bmax + 1.0f) * PS_GUARD_K;
+        // ---- approximate gate ----
+        bool flagged = false;
+        for (int k = jr.apx_beg; k < jr.apx_end && !flagged; ++k) {
+            const float4 sa = M.A[k];
+            float px, py, pz;
+            sphere_world(T, sa.x, sa.y, sa.z, px, py, pz);
+            const float sr = __fadd_rn(sa.w, margin);
+            if (kStats) st.v[ST_SPHERES] += 1;
+            flagged = spheres_hit<1, kStats>(sc, ws.cand, ncand, &px, &py, &pz, &sr, g, st) ||
+                      (kEsdf && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
+        }
+        // ---- exact spheres of a flagged joint: 4 at a time, then singles ----
+        if (flagged && !hit) {
+            int k = jr.sph_beg;
+            for (; k + 4 <= jr.sph_end && !hit; k += 4) {
+                float px[4], py[4], pz[4], sr[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const float4 sp = M.S[k + i];
+                    sphere_world(T, sp.x, sp.y, sp.z, px[i], py[i], pz[i]);
+                    sr[i] = __fadd_rn(sp.w, margin);
+                }
+                if (kStats) st.v[ST_SPHERES] += 4;
+                hit = spheres_hit<4, kStats>(sc, ws.cand, ncand, px, py, pz, sr, g, st);
+                if (kEsdf)
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        if (!hit) hit = sphere_esdf_any(sc, sv, px[i], py[i], pz[i], sr[i], nullptr, st);
+            }
+            for (; k < jr.sph_end && !hit; ++k) {
+                const float4 sp = M.S[k];
+                float px, py, pz;
+                sphere_world(T, sp.x, sp.y, sp.z, px, py, pz);
+                const float sr = __fadd_rn(sp.w, margin);
+                if (kStats) st.v[ST_SPHERES] += 1;
+                hit = spheres_hit<1, kStats>(sc, ws.cand, ncand, &px, &py, &pz, &sr, g, st) ||
+                      (kEsdf && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
+            }
+        }
+        if (__any_sync(kFull, hit && real)) break;   // warp-uniform early exit
+    }
+    if (kStats && real)
+        for (int k = 0; k < ST_COUNT; ++k) st_out.v[k] += st.v[k];
+    return __any_sync(kFull, hit && real);
+}
+
+// Shared-memory carve-up common to both edge kernels.
+struct EdgeSmem {
+    unsigned char* blob;
+    ObbPrep* obbs;
+    int* orig;
+    LayerPrep* layers;
+    float* q;          // [kWarps][32*D]
+    uint16_t* cand;    // [kWarps][n_obbs_pad]
+};
+
+__device__ __forceinline__ EdgeSmem carve(unsigned char* smem, const ModelDev& md, const ps_scene_view& sv, int D) {
+    EdgeSmem s;
+    s.blob = smem;
+    s.obbs = reinterpret_cast<ObbPrep*>(smem + md.bytes_core);
+    const int nob = max(sv.n_obbs, 1);
+    s.orig = reinterpret_cast<int*>(s.obbs + nob);
+    s.layers = reinterpret_cast<LayerPrep*>(s.orig + ((nob + 3) & ~3));
+    s.q = reinterpret_cast<float*>(s.layers + PS_MAX_LAYERS);
+    s.cand = reinterpret_cast<uint16_t*>(s.q + kWarps * 32 * D);
+    return s;
+}
+
+size_t edge_smem_bytes(const ps_model* m, const ps_scene_view* sv) {
+    const int nob_pad = (std::max(sv->n_obbs, 1) + 7) & ~7;
+    return (size_t)m->dev.bytes_core + scene_smem_bytes(sv) + (size_t)kWarps * 32 * m->info.n_dof * 4 +
+           (size_t)kWarps * nob_pad * 2 + 64;
+}
+
+// ---------------------------------------------------------------------------
+// Plain path: one warp per edge, chunks in order.
+// ---------------------------------------------------------------------------
+template <int kMode, bool kStats>
+__global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_plain_kernel(ModelDev md, ps_scene_view sv, ps_edge_params P,
+                                                                  const float* __restrict__ from,
+                                                                  const float* __restrict__ to,
+                                                                  const int* __restrict__ given, int n_edges,
+                                                                  uint8_t* __restrict__ valid, float* __restrict__ cost,
+                                                                  float* __restrict__ clearance,
+                                                                  unsigned long long* stats) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ int counters[4];
+    __shared__ float bmax;
+    if (!stage_model(md, smem, &mbar)) return;
+    const ModelSmem M = model_view(smem);
+    const int D = M.H->n_dof;
+    EdgeSmem es = carve(smem, md, sv, D);
+    SceneSmem sc;
+    stage_scene(sv, es.obbs, es.orig, es.layers, counters, &bmax, sc);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nob_pad = (max(sv.n_obbs, 1) + 7) & ~7;
+    WarpScratch ws{es.q + warp * 32 * D, es.cand + warp * nob_pad};
+    LaneStats st;
+    st.zero();
+    for (int e = blockIdx.x * kWarps + warp; e < n_edges; e += gridDim.x * kWarps) {
+        const float* a = from + (size_t)e * D;
+        const float* b = to + (size_t)e * D;
+        const float len = edge_length(a, b, D);
+        const int G = edge_samples(P, given, e, a, b, D, len);
+        bool bad = false;
+        float emin = FLT_MAX;
+        const int chunks = G > 0 ? (G + 31) / 32 : 0;
+        for (int c = 0; c < chunks; ++c) {
+            float cm = FLT_MAX;
+            if (kMode) bad |= process_chunk_fast<kStats, kMode == 2>(M, sc, sv, P, from, to, e, G, c, ws, st);
+            else bad |= process_chunk(M, sc, sv, P, from, to, e, G, c, ws, P.compute_clearance ? &cm : nullptr, st);
+            emin = fminf(emin, cm);
+            if (bad && !P.compute_clearance) break;
+        }
+        if (lane == 0) {
+            valid[e] = bad ? 0 : 1;
+            cost[e] = bad ? FLT_MAX : len;
+            if (clearance) clearance[e] = P.compute_clearance ? emin : FLT_MAX;
+        }
+    }
+    flush_stats(stats, st);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent path
+// ---------------------------------------------------------------------------
+// n_dev (optional): device-resident edge count overriding n_edges, so a
+// captured graph can be replayed with a different number of edges.
+__global__ void edges_prep_kernel(ps_edge_params P, const float* __restrict__ from, const float* __restrict__ to,
+                                  const int* __restrict__ given, int n_edges, int D, EdgeWs* hdr, int* G_out,
+                                  float* len_out, int* bad, int* clr, const int* n_dev = nullptr) {
+    if (n_dev) n_edges = *n_dev;
+    int local_max = 0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_edges; e += gridDim.x * blockDim.x) {
+        const float* a = from + (size_t)e * D;
+        const float* b = to + (size_t)e * D;
+        const float len = edge_length(a, b, D);
+        const int G = edge_samples(P, given, e, a, b, D, len);
+        G_out[e] = G;
+        len_out[e] = len;
+        bad[e] = 0;
+        clr[e] = ordered_float(FLT_MAX);
+        local_max = max(local_max, G);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) local_max = max(local_max, __shfl_xor_sync(kFull, local_max, o));
+    if ((threadIdx.x & 31) == 0 && local_max > 0) atomicMax(&hdr->max_G, local_max);
+}
+
+template <int kMode, bool kStats>
+__global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_queue_kernel(ModelDev md, ps_scene_view sv, ps_edge_params P,
+                                                                  const float* __restrict__ from,
+                                                                  const float* __restrict__ to, int n_edges,
+                                                                  EdgeWs* hdr, const int* __restrict__ Gs, int* bad,
+                                                                  int* clr, unsigned long long* stats,
+                                                                  const int* n_dev = nullptr) {
+    if (n_dev) n_edges = *n_dev;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ int counters[4];
+    __shared__ float bmax;
+    if (!stage_model(md, smem, &mbar)) return;
+    const ModelSmem M = model_view(smem);
+    const int D = M.H->n_dof;
+    EdgeSmem es = carve(smem, md, sv, D);
+    SceneSmem sc;
+    stage_scene(sv, es.obbs, es.orig, es.layers, counters, &bmax, sc);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nob_pad = (max(sv.n_obbs, 1) + 7) & ~7;
+    WarpScratch ws{es.q + warp * 32 * D, es.cand + warp * nob_pad};
+    LaneStats st;
+    st.zero();
+    const int max_G = *((volatile int*)&hdr->max_G);
+    const long long rounds = (max_G + 31) / 32;
+    const long long total = rounds * (long long)n_edges;   // chunk-major item space
+    volatile int* vbad = bad;
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(&hdr->head, 32ull);
+        base = __shfl_sync(kFull, base, 0);
+        if ((long long)base >= total) break;
+        // Each lane inspects one item; live items are processed by the whole warp.
+        const long long item = (long long)base + lane;
+        int e = -1, k = 0, G = 0;
+        bool live = false;
+        if (item < total) {
+            if (total < (1ll << 31)) {   // 32-bit division in the common case
+                k = (int)((unsigned)item / (unsigned)n_edges);
+                e = (int)((unsigned)item - (unsigned)k * (unsigned)n_edges);
+            } else {
+                k = (int)(item / n_edges);
+                e = (int)(item - (long long)k * n_edges);
+            }
+            G = __ldg(Gs + e);
+            live = (k * 32 < G) && vbad[e] == 0;
+        }
+        unsigned todo = __ballot_sync(kFull, live);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int ee = __shfl_sync(kFull, e, src);
+            const int kk = __shfl_sync(kFull, k, src);
+            const int GG = __shfl_sync(kFull, G, src);
+            int retired = 0;
+            if (lane == 0) retired = vbad[ee];
+            retired = __shfl_sync(kFull, retired, 0);
+            if (!P.compute_clearance && retired) continue;   // retired meanwhile
+            float cm = FLT_MAX;
+            const bool h = kMode ? process_chunk_fast<kStats, kMode == 2>(M, sc, sv, P, from, to, ee, GG, kk, ws, st)
+                                 : process_chunk(M, sc, sv, P, from, to, ee, GG, kk, ws,
+                                                 P.compute_clearance ? &cm : nullptr, st);
+            if (lane == 0) {
+                if (h) vbad[ee] = 1;
+                if (P.compute_clearance) atomicMin(clr + ee, ordered_float(cm));
+            }
+        }
+    }
+    flush_stats(stats, st);
+}
+
+__global__ void edges_finalize_kernel(int n_edges, const ps_edge_params P, const int* __restrict__ bad,
+                                      const float* __restrict__ len, const int* __restrict__ clr,
+                                      uint8_t* __restrict__ valid, float* __restrict__ cost,
+                                      float* __restrict__ clearance, const int* n_dev = nullptr) {
+    if (n_dev) n_edges = *n_dev;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_edges; e += gridDim.x * blockDim.x) {
+        const bool b = bad[e] != 0;
+        valid[e] = b ? 0 : 1;
+        cost[e] = b ? FLT_MAX : len[e];
+        if (clearance) clearance[e] = P.compute_clearance ? unordered_float(clr[e]) : FLT_MAX;
+    }
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+
+
+// Kernel variant: 0 generic, 1 fast (boxes only), 2 fast with ESDF layers.
+int fast_path(const ps_model* m, const ps_scene_view* sv, const ps_edge_params* P) {
+    const bool fast = m->info.approx_shares_chain && m->root_slot_only && !P->compute_clearance && !P->check_self &&
+                      !sv->sphere_obb_acm_mask && !sv->sphere_obb_acm_mask_approx && !sv->sphere_acm_mask;
+    return fast ? (sv->n_voxel_layers > 0 ? 2 : 1) : 0;
+}
+
+template <typename K>
+K pick(int mode, bool stats, K g0, K g1, K f0, K f1, K e0, K e1) {
+    if (mode == 2) return stats ? e1 : e0;
+    if (mode == 1) return stats ? f1 : f0;
+    return stats ? g1 : g0;
+}
+
+}  // namespace
+}  // namespace ps

@@ -380,13 +380,23 @@ def workload(index: int, scale: float = 1.0) -> Dict:
                 "self_margin": 0.01, "name": "stomp_fetch8_obb96_32x128x100"}
     if index == 5:
         asset = baxter_like()
-        obbs = random_obbs(rng, 128)
+        # 128 boxes in a wider, sparser field than workloads 1-4 (centres
+        # U([-1.5,1.5]^3), half-extents U(0.02,0.1)): with 110 spheres on two
+        # arms the denser field leaves no collision-free edge at all.
+        obbs = random_obbs(rng, 128, -1.5, 1.5, 0.02, 0.1)
         esdf = random_esdf(rng)
         n_e = max(2, int(8192 * scale))
         frm, to, G = edge_batch(rng, asset, n_e)
         Ts = rng.integers(32, 129, max(1, int(64 * scale)))
         trajs = [straight_trajectories(rng, asset, 1, int(t))[0] for t in Ts]
+        # edge requests of uneven size (16..256 edges), as many planners' batches
+        splits = []
+        left = n_e
+        while left > 0:
+            k = min(left, int(rng.integers(16, 257)))
+            splits.append(k)
+            left -= k
         return {"asset": asset, "obbs": obbs, "esdf": esdf, "from": frm, "to": to, "G": G,
-                "trajectories": trajs, "w": 20.0, "eps": 0.05, "self_margin": 0.01,
-                "name": "mixed_baxter14_obb128_esdf128"}
+                "edge_splits": splits, "trajectories": trajs, "w": 20.0, "eps": 0.05,
+                "self_margin": 0.01, "name": "mixed_baxter14_obb128_esdf128"}
     raise ValueError(f"unknown workload {index}")
