@@ -421,9 +421,43 @@ def bench_chomp(dev):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / 10
-    B = q.shape[0]
+    B, T, D = q.shape
     out = {"workload": "chomp_panda7_obb64_b256_t64", "value": B / (ms * 1e-3), "unit": "traj/s",
            "ms_per_step": ms, "path": "fused FK + hinge + adjoint + smoothness (ps_traj_cost)"}
+    # Plain forward + separate gradient on the same kernels: one forward launch
+    # for the cost, then the collision gradient by central differences (2*D
+    # perturbed evaluations per waypoint, as the reference's obs-grad kernel
+    # does) in a second launch, plus the smoothness gradient 2*lambda*R*theta.
+    eps = 1e-3
+    R = torch.from_numpy(workloads.control_cost_R(T, wl["delta_t"]).astype(np.float32)).to(dev)
+    p0 = api.CostParams(collision_cost_weight=wl["w"], world_collision_margin=wl["eps"],
+                        self_collision_margin=wl["self_margin"], smoothness_weight=0.0, delta_t=wl["delta_t"])
+    idx = torch.arange(D, device=dev)
+    lam = p.smoothness_weight
+
+    def plain_step():
+        _, tc, _ = api.traj_cost(b, sc, q, p, want_grad=False, want_waypoint=False)
+        qp = q.unsqueeze(0).repeat(2 * D, 1, 1, 1)
+        qp[idx, :, :, idx] += eps
+        qp[D + idx, :, :, idx] -= eps
+        wp, _, _ = api.traj_cost(b, sc, qp.view(2 * D * B, T, D), p0, want_grad=False)
+        wp = wp.view(2, D, B, T)
+        g = ((wp[0] - wp[1]) / (2 * eps)).permute(1, 2, 0) + 2.0 * lam * torch.einsum("ts,bsd->btd", R, q)
+        return tc, g
+
+    for _ in range(3):
+        plain_step()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(10):
+        plain_step()
+    e1.record()
+    torch.cuda.synchronize()
+    pms = e0.elapsed_time(e1) / 10
+    out["plain_fd"] = {"value": B / (pms * 1e-3), "unit": "traj/s", "ms_per_step": pms,
+                       "path": "forward ps_traj_cost + central-difference gradient (2*D forward evaluations per "
+                               "waypoint, one launch) + 2*lambda*R*theta"}
+    out["speedup_vs_plain_fd"] = pms / ms
     try:
         import oracle
 

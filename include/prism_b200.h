@@ -319,7 +319,8 @@ typedef struct ps_batch_tuning {
     float edge_share;        /* fraction of the edge kernel's resident-block
                                 slots its persistent grid takes              */
     float traj_share;        /* same for the trajectory kernel's grid         */
-    int   traj_threads;      /* waypoints per block of the trajectory kernel  */
+    int   traj_threads;      /* threads per block of the trajectory kernel
+                                (one waypoint per warp)                      */
     float best_ms;           /* measured time of one launch at this choice    */
 } ps_batch_tuning;
 

@@ -23,7 +23,7 @@
 #include <string>
 #include <vector>
 
-#include "ps_costlane.cuh"
+#include "ps_costwarp.cuh"
 #include "ps_edgekern.cuh"
 
 namespace ps {
@@ -84,38 +84,35 @@ __global__ void batch_scatter_edges(const EdgeReq* __restrict__ req, const Count
     }
 }
 
-// Packs every trajectory's waypoints and zeroes their packed gradient rows.
+// Packs every trajectory's waypoints.
 __global__ void batch_gather_traj(const TrajReq* __restrict__ req, const Counts* __restrict__ cnt, int D,
-                                  float* __restrict__ q, float* __restrict__ grad) {
+                                  float* __restrict__ q) {
     const int nreq = cnt->n_traj_req;
     for (int r = blockIdx.x; r < nreq; r += gridDim.x) {
         const TrajReq t = req[r];
         const size_t base = (size_t)t.offset * D;
-        for (int i = threadIdx.x; i < t.T * D; i += blockDim.x) {
-            q[base + i] = t.q[i];
-            grad[base + i] = 0.0f;
-        }
+        for (int i = threadIdx.x; i < t.T * D; i += blockDim.x) q[base + i] = t.q[i];
     }
 }
 
-size_t waypoint_smem_bytes(const ps_model* m, const ps_scene_view* sv, int threads) {
-    return (size_t)m->dev.bytes_core + scene_smem_bytes(sv) +
-           (size_t)(m->info.n_spheres * 3 + m->info.n_joints * 12) * threads * 4 + (size_t)m->info.n_spheres + 16;
+size_t waypoint_smem_bytes(const ps_model* m, const ps_scene_view* sv, int warps) {
+    return (size_t)m->dev.bytes_core + scene_smem_bytes(sv) + (((size_t)m->info.n_spheres + 15) & ~size_t(15)) +
+           (size_t)warps * cost_warp_floats(m->info.n_joints, m->info.n_spheres, sv->n_obbs, true) * 4;
 }
 
-// Cost and adjoint of every packed waypoint (lane = waypoint), grid-stride.
-template <int kThreads>
-__global__ void __launch_bounds__(kThreads) batch_waypoint_kernel(ModelDev md, ps_scene_view sv, ps_cost_params P,
-                                                                  const Counts* __restrict__ cnt,
-                                                                  const float* __restrict__ q,
-                                                                  float* __restrict__ wp_cost,
-                                                                  float* __restrict__ grad) {
+// Cost and adjoint of every packed waypoint, one warp per waypoint.
+template <int kWarps>
+__global__ void __launch_bounds__(kWarps * 32, 24 / kWarps) batch_waypoint_kernel(ModelDev md, ps_scene_view sv, ps_cost_params P,
+                                                                     const Counts* __restrict__ cnt,
+                                                                     const float* __restrict__ q,
+                                                                     float* __restrict__ wp_cost,
+                                                                     float* __restrict__ grad) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ int counters[4];
     __shared__ float bmax;
     const int n_wp = cnt->n_wp;
-    if ((long long)blockIdx.x * kThreads >= n_wp) return;   // nothing for this block: skip staging
+    if ((long long)blockIdx.x * kWarps >= n_wp) return;   // nothing for this block: skip staging
     if (!stage_model(md, smem, &mbar)) return;
     const ModelSmem M = model_view(smem);
     const int D = M.H->n_dof, NJ = M.H->n_joints, NS = M.H->n_spheres;
@@ -123,21 +120,24 @@ __global__ void __launch_bounds__(kThreads) batch_waypoint_kernel(ModelDev md, p
     const int nob = max(sv.n_obbs, 1);
     int* orig = reinterpret_cast<int*>(obbs + nob);
     LayerPrep* layers = reinterpret_cast<LayerPrep*>(orig + ((nob + 3) & ~3));
-    float* pos = reinterpret_cast<float*>(layers + PS_MAX_LAYERS);
-    float* jf = pos + (size_t)NS * 3 * kThreads;
-    unsigned char* sph_joint = reinterpret_cast<unsigned char*>(jf + (size_t)NJ * 12 * kThreads);
+    unsigned char* sph_joint = reinterpret_cast<unsigned char*>(layers + PS_MAX_LAYERS);
+    float* wbase = reinterpret_cast<float*>(sph_joint + ((NS + 15) & ~15));
     SceneSmem sc;
     stage_scene(sv, obbs, orig, layers, counters, &bmax, sc);
     for (int p = 0; p < NJ; ++p)
         for (int k = M.J[p].sph_beg + threadIdx.x; k < M.J[p].sph_end; k += blockDim.x) sph_joint[k] = (unsigned char)p;
     __syncthreads();
-    const int lane = threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const CostWarpScratch ws =
+        cost_carve(wbase + (size_t)warp * cost_warp_floats(NJ, NS, sv.n_obbs, true), NJ, NS, sc.n_obbs, true);
     LaneStats st;
     st.zero();
-    for (int k = blockIdx.x * kThreads + lane; k - lane < n_wp; k += gridDim.x * kThreads) {
-        if (k >= n_wp) continue;
-        wp_cost[k] = waypoint_cost_lane<true>(M, md, sc, sv, P, q + (size_t)k * D, pos + lane, jf + lane, sph_joint,
-                                              kThreads, grad + (size_t)k * D, 1, st);
+    for (int k = blockIdx.x * kWarps + warp; k < n_wp; k += gridDim.x * kWarps) {
+        if (lane < D) ws.q[lane] = q[(size_t)k * D + lane];
+        __syncwarp();
+        const float c = waypoint_cost_warp<true>(M, md, sc, sv, P, sph_joint, ws, grad + (size_t)k * D, 1, st);
+        if (lane == 0) wp_cost[k] = c;
+        __syncwarp();
     }
 }
 
@@ -204,7 +204,7 @@ struct ps_batch {
     // tuning state
     float edge_share = 1.0f;   // of the edge kernel's full-occupancy grid
     float traj_share = 0.5f;   // of the trajectory kernel's full-occupancy grid
-    int traj_threads = 32;
+    int traj_threads = 256;   // threads per block of the trajectory kernel (one waypoint per warp)
 };
 
 namespace {
@@ -237,19 +237,19 @@ int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, 
     }
     if (b->lim.max_waypoints > 0) {
         const int tt = b->traj_threads;
-        L.wsmem = waypoint_smem_bytes(m, sv, tt);
+        L.wsmem = waypoint_smem_bytes(m, sv, tt / 32);
         int per_sm = 0;
-        if (tt == 32) {
-            PS_TRY_CUDA(cudaFuncSetAttribute(batch_waypoint_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (tt == 128) {
+            PS_TRY_CUDA(cudaFuncSetAttribute(batch_waypoint_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)L.wsmem));
-            PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_waypoint_kernel<32>, 32, L.wsmem));
+            PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_waypoint_kernel<4>, 128, L.wsmem));
         } else {
-            PS_TRY_CUDA(cudaFuncSetAttribute(batch_waypoint_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            PS_TRY_CUDA(cudaFuncSetAttribute(batch_waypoint_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)L.wsmem));
-            PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_waypoint_kernel<64>, 64, L.wsmem));
+            PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_waypoint_kernel<8>, 256, L.wsmem));
         }
         if (per_sm < 1) return set_error(PS_EINVAL, "trajectory kernel does not fit on an SM with this model/scene");
-        const int cap_blocks = (b->lim.max_waypoints + tt - 1) / tt;
+        const int cap_blocks = (b->lim.max_waypoints + tt / 32 - 1) / (tt / 32);
         L.wgrid = std::max(1, std::min(cap_blocks, (int)(b->traj_share * sms * per_sm + 0.5f)));
         L.fsmem = (size_t)(2 * (b->lim.max_traj_len + 12) + kFinishThreads) * sizeof(float);
         if (L.fsmem > 48 * 1024)
@@ -284,12 +284,12 @@ void record_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep
         batch_scatter_edges<<<L.req_grid_e, 128, 0, s0>>>(b->d_ereq, b->d_cnt, b->d_valid, b->d_cost);
     }
     if (b->lim.max_waypoints > 0) {   // trajectory branch on s1
-        batch_gather_traj<<<L.req_grid_t, 128, 0, s1>>>(b->d_treq, b->d_cnt, D, b->d_q, b->d_grad);
-        if (b->traj_threads == 32)
-            batch_waypoint_kernel<32><<<L.wgrid, 32, L.wsmem, s1>>>(m->dev, *sv, *cp, b->d_cnt, b->d_q, b->d_wp_cost,
+        batch_gather_traj<<<L.req_grid_t, 128, 0, s1>>>(b->d_treq, b->d_cnt, D, b->d_q);
+        if (b->traj_threads == 128)
+            batch_waypoint_kernel<4><<<L.wgrid, 128, L.wsmem, s1>>>(m->dev, *sv, *cp, b->d_cnt, b->d_q, b->d_wp_cost,
                                                                     b->d_grad);
         else
-            batch_waypoint_kernel<64><<<L.wgrid, 64, L.wsmem, s1>>>(m->dev, *sv, *cp, b->d_cnt, b->d_q, b->d_wp_cost,
+            batch_waypoint_kernel<8><<<L.wgrid, 256, L.wsmem, s1>>>(m->dev, *sv, *cp, b->d_cnt, b->d_q, b->d_wp_cost,
                                                                     b->d_grad);
         batch_traj_finish<<<L.req_grid_t, kFinishThreads, L.fsmem, s1>>>(b->d_treq, b->d_cnt, D, *cp, b->d_q,
                                                                          b->d_wp_cost, b->d_grad);
@@ -501,7 +501,7 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
     if (!b) return set_error(PS_EINVAL, "NULL batch");
     const float edge_shares[] = {0.5f, 0.75f, 1.0f};
     const float traj_shares[] = {0.25f, 0.5f, 1.0f};
-    const int widths[] = {32, 64};
+    const int widths[] = {128, 256};
     cudaStream_t s = nullptr;
     cudaEvent_t a = nullptr, z = nullptr;
     PS_TRY_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -521,7 +521,7 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
         if (!edges && es != 1.0f) continue;
         for (float ts : traj_shares) {
             for (int w : widths) {
-                if (!trajs && (ts != 0.5f || w != 32)) continue;
+                if (!trajs && (ts != 0.5f || w != 256)) continue;
                 b->edge_share = es;
                 b->traj_share = ts;
                 b->traj_threads = w;

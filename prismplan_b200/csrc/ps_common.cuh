@@ -48,11 +48,16 @@ struct JointRec {
 };
 
 // Self pairs (global memory): packed (i | j << 16), reordered sphere indices.
+// gpairs holds the same pairs grouped by the DFS positions of their two
+// joints; jpairs[g] = (joint of i, joint of j, first, end) indexes gpairs.
 // Limits (global memory): lower[n_dof], upper[n_dof].
 struct ModelDev {
     const unsigned char* blob;     // device
     const uint32_t* self_pairs;    // device
     const uint32_t* apx_self_pairs;// device
+    const uint32_t* gpairs;        // device, grouped self pairs
+    const int4* jpairs;            // device, joint-pair groups
+    int n_jpairs;
     const float* lower;            // device
     const float* upper;            // device
     int* status;                   // device error latch

@@ -21,24 +21,23 @@
 // zero-padded trajectory instead of a dense T x T product.
 #include <algorithm>
 
-#include "ps_costlane.cuh"
+#include "ps_costwarp.cuh"
 
 namespace ps {
 
 namespace {
 
-constexpr int kCostThreads = 64;
+constexpr int kCostWarps = 8;   // waypoints in flight per block (one per warp)
 
-struct CostSmem {
-    float* pos;    // [NS*3][kCostThreads]
-    float* jf;     // [NJ*12][kCostThreads]: axis(3) origin(3) F(3) M(3)
-    float* q;      // [kCostThreads*D]
-    unsigned char* sph_joint;   // [NS] DFS position of each reordered sphere
-};
+size_t cost_block_smem(const ps_model* m, const ps_scene_view* sv, bool grad) {
+    return (size_t)m->dev.bytes_core + scene_smem_bytes(sv) + (((size_t)m->info.n_spheres + 15) & ~size_t(15)) +
+           (size_t)kCostWarps * cost_warp_floats(m->info.n_joints, m->info.n_spheres, sv->n_obbs, grad) * 4;
+}
 
-// kGrad: also produce the adjoint. Output layouts follow ps_cost_params.layout.
+// One warp per waypoint (see ps_costwarp.cuh). kGrad: also the adjoint.
+// Output layouts follow ps_cost_params.layout.
 template <bool kGrad>
-__global__ void __launch_bounds__(kCostThreads) waypoint_cost_kernel(
+__global__ void __launch_bounds__(kCostWarps * 32, 3) waypoint_cost_kernel(
     ModelDev md, ps_scene_view sv, const float* __restrict__ q, int n_rows, int T, ps_cost_params P,
     float* __restrict__ wp_cost, int broadcast_d, float* __restrict__ traj_acc, float* __restrict__ grad,
     unsigned long long* stats) {
@@ -53,48 +52,45 @@ __global__ void __launch_bounds__(kCostThreads) waypoint_cost_kernel(
     const int nob = max(sv.n_obbs, 1);
     int* orig = reinterpret_cast<int*>(obbs + nob);
     LayerPrep* layers = reinterpret_cast<LayerPrep*>(orig + ((nob + 3) & ~3));
-    CostSmem cs;
-    cs.pos = reinterpret_cast<float*>(layers + PS_MAX_LAYERS);
-    cs.jf = cs.pos + (size_t)NS * 3 * kCostThreads;
-    cs.q = cs.jf + (size_t)NJ * 12 * kCostThreads;
-    cs.sph_joint = reinterpret_cast<unsigned char*>(cs.q + kCostThreads * D);
+    unsigned char* sph_joint = reinterpret_cast<unsigned char*>(layers + PS_MAX_LAYERS);
+    float* wbase = reinterpret_cast<float*>(sph_joint + ((NS + 15) & ~15));
     SceneSmem sc;
     stage_scene(sv, obbs, orig, layers, counters, &bmax, sc);
     for (int p = 0; p < NJ; ++p)
-        for (int k = M.J[p].sph_beg + threadIdx.x; k < M.J[p].sph_end; k += blockDim.x) cs.sph_joint[k] = (unsigned char)p;
+        for (int k = M.J[p].sph_beg + threadIdx.x; k < M.J[p].sph_end; k += blockDim.x) sph_joint[k] = (unsigned char)p;
     __syncthreads();
 
-    const int lane = threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const CostWarpScratch ws =
+        cost_carve(wbase + (size_t)warp * cost_warp_floats(NJ, NS, sv.n_obbs, kGrad), NJ, NS, sc.n_obbs, kGrad);
     const bool bdt = P.layout == PS_LAYOUT_BDT;
     const long long total = (long long)n_rows * T;
     LaneStats st;
     st.zero();
-    for (long long base = (long long)blockIdx.x * kCostThreads; base < total; base += (long long)gridDim.x * kCostThreads) {
-        const long long idx = base + lane;
-        const bool active = idx < total;
-        const int b = active ? (int)(idx / T) : 0;
-        const int t = active ? (int)(idx - (long long)b * T) : 0;
-        float* qc = cs.q + lane * D;
-        if (active)
-            for (int d = 0; d < D; ++d) qc[d] = bdt ? q[((size_t)b * D + d) * T + t] : q[((size_t)b * T + t) * D + d];
-        if (!active) continue;
-        st.v[ST_SAMPLES] += 1;
-
+    for (long long idx = (long long)blockIdx.x * kCostWarps + warp; idx < total;
+         idx += (long long)gridDim.x * kCostWarps) {
+        const int b = (int)(idx / T);
+        const int t = (int)(idx - (long long)b * T);
+        if (lane < D) ws.q[lane] = bdt ? q[((size_t)b * D + lane) * T + t] : q[((size_t)b * T + t) * D + lane];
+        __syncwarp();
         float* grow = nullptr;
         int gstride = 1;
         if (kGrad) {
             grow = bdt ? grad + ((size_t)b * D) * T + t : grad + ((size_t)b * T + t) * D;
             gstride = bdt ? T : 1;
         }
-        const float cost = waypoint_cost_lane<kGrad>(M, md, sc, sv, P, qc, cs.pos + lane, cs.jf + lane,
-                                                     cs.sph_joint, kCostThreads, grow, gstride, st);
-        if (wp_cost) {
-            if (broadcast_d)
-                for (int d = 0; d < D; ++d) wp_cost[((size_t)b * D + d) * T + t] = cost;
-            else
-                wp_cost[idx] = cost;
+        const float cost = waypoint_cost_warp<kGrad>(M, md, sc, sv, P, sph_joint, ws, grow, gstride, st);
+        if (lane == 0) {
+            st.v[ST_SAMPLES] += 1;
+            if (wp_cost) {
+                if (broadcast_d)
+                    for (int d = 0; d < D; ++d) wp_cost[((size_t)b * D + d) * T + t] = cost;
+                else
+                    wp_cost[idx] = cost;
+            }
+            if (traj_acc) atomicAdd(traj_acc + b, cost);
         }
-        if (traj_acc) atomicAdd(traj_acc + b, cost);
+        __syncwarp();
     }
     flush_stats(stats, st);
 }
@@ -119,10 +115,19 @@ __global__ void smoothness_kernel(const float* __restrict__ q, int B, int T, int
     }
 }
 
-size_t cost_smem(const ps_model* m, const ps_scene_view* sv) {
-    return (size_t)m->dev.bytes_core + scene_smem_bytes(sv) +
-           (size_t)m->info.n_spheres * 3 * kCostThreads * 4 + (size_t)m->info.n_joints * 12 * kCostThreads * 4 +
-           (size_t)kCostThreads * m->info.n_dof * 4 + (size_t)m->info.n_spheres + 16;
+// Grid of a persistent-style launch: every block resident at once, capped by
+// the waypoint count. Returns -1 (error set) if a block does not fit.
+template <class K>
+int cost_grid(K kernel, size_t smem, long long total) {
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(PS_EINVAL, "cost kernel shared memory exceeds the device limit"), -1;
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kCostWarps * 32, smem);
+    if (per_sm < 1) return set_error(PS_EINVAL, "cost kernel does not fit on an SM with this model/scene"), -1;
+    const long long need = (total + kCostWarps - 1) / kCostWarps;
+    return (int)std::max<long long>(1, std::min<long long>(need, (long long)per_sm * sm_count()));
 }
 
 int check_cost_params(const ps_model* m, const ps_scene_view* scene, const float* q, int rows, int T,
@@ -150,22 +155,23 @@ extern "C" int ps_traj_cost(const ps_model* m, const ps_scene_view* scene, const
     if (T > PS_MAX_TRAJ_LEN && (traj_cost || (grad && P->smoothness_weight != 0.0f)))
         return set_error(PS_EINVAL, "T exceeds PS_MAX_TRAJ_LEN for the smoothness term");
     cudaStream_t s = (cudaStream_t)stream;
-    const size_t smem = cost_smem(m, scene);
     const long long total = (long long)B * T;
-    const int grid = (int)std::max<long long>(1, std::min<long long>((total + kCostThreads - 1) / kCostThreads, 1 << 20));
     const bool atomic_traj = traj_cost && !waypoint_cost;
     if (atomic_traj) PS_TRY_CUDA(cudaMemsetAsync(traj_cost, 0, sizeof(float) * B, s));
     if (grad) {
-        PS_TRY_CUDA(cudaMemsetAsync(grad, 0, sizeof(float) * (size_t)total * m->info.n_dof, s));
-        PS_TRY_CUDA(cudaFuncSetAttribute(waypoint_cost_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const size_t smem = cost_block_smem(m, scene, true);
+        const int grid = cost_grid(waypoint_cost_kernel<true>, smem, total);
+        if (grid < 0) return PS_EINVAL;
         mark_start(s);
-        waypoint_cost_kernel<true><<<grid, kCostThreads, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
+        waypoint_cost_kernel<true><<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
                                                                     atomic_traj ? traj_cost : nullptr, grad, g_stats);
         mark_stop(s);
     } else {
-        PS_TRY_CUDA(cudaFuncSetAttribute(waypoint_cost_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const size_t smem = cost_block_smem(m, scene, false);
+        const int grid = cost_grid(waypoint_cost_kernel<false>, smem, total);
+        if (grid < 0) return PS_EINVAL;
         mark_start(s);
-        waypoint_cost_kernel<false><<<grid, kCostThreads, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
+        waypoint_cost_kernel<false><<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
                                                                      atomic_traj ? traj_cost : nullptr, nullptr, g_stats);
         mark_stop(s);
     }
@@ -189,12 +195,12 @@ extern "C" int ps_rollout_costs(const ps_model* m, const ps_scene_view* scene, c
     if (broadcast_d && P->layout != PS_LAYOUT_BDT) return set_error(PS_EINVAL, "broadcast_d needs PS_LAYOUT_BDT");
     if (n_rows == 0 || T == 0) return PS_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    const size_t smem = cost_smem(m, scene);
     const long long total = (long long)n_rows * T;
-    const int grid = (int)std::max<long long>(1, std::min<long long>((total + kCostThreads - 1) / kCostThreads, 1 << 20));
-    PS_TRY_CUDA(cudaFuncSetAttribute(waypoint_cost_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t smem = cost_block_smem(m, scene, false);
+    const int grid = cost_grid(waypoint_cost_kernel<false>, smem, total);
+    if (grid < 0) return PS_EINVAL;
     mark_start(s);
-    waypoint_cost_kernel<false><<<grid, kCostThreads, smem, s>>>(m->dev, *scene, rollouts, n_rows, T, *P, state_cost,
+    waypoint_cost_kernel<false><<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, rollouts, n_rows, T, *P, state_cost,
                                                                  broadcast_d, nullptr, nullptr, g_stats);
     mark_stop(s);
     PS_TRY_CUDA(cudaGetLastError());

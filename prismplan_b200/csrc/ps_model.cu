@@ -192,6 +192,26 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
         if (rc) return rc;
     }
 
+    // Self pairs grouped by joint pair (for the bound-sphere prefilter of the
+    // cost kernels); stable within a group.
+    std::vector<int> sph_pos(std::max(ns, 1), 0);
+    for (int p = 0; p < nj; ++p)
+        for (int k = sbeg[p]; k < send[p]; ++k) sph_pos[k] = p;
+    std::vector<uint32_t> gpairs(pairs);
+    auto jkey = [&](uint32_t pr) {
+        const int a = sph_pos[pr & 0xffff], b = sph_pos[pr >> 16];
+        return std::make_pair(std::min(a, b), std::max(a, b));
+    };
+    std::stable_sort(gpairs.begin(), gpairs.end(), [&](uint32_t x, uint32_t y) { return jkey(x) < jkey(y); });
+    std::vector<int> jpairs;   // 4 ints per group
+    for (size_t k = 0; k < gpairs.size();) {
+        size_t e = k;
+        while (e < gpairs.size() && jkey(gpairs[e]) == jkey(gpairs[k])) ++e;
+        const auto jk = jkey(gpairs[k]);
+        jpairs.insert(jpairs.end(), {jk.first, jk.second, (int)k, (int)e});
+        k = e;
+    }
+
     bool shares = std::memcmp(aft, d->fixed_transforms, sizeof(float) * 16 * nj) == 0;
     for (int i = 0; i < nj && shares; ++i) shares = atypes[i] == d->joint_types[i];
 
@@ -215,6 +235,10 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
     off += align16(sizeof(uint32_t) * std::max<size_t>(pairs.size(), 1));
     const size_t off_apairs = off;
     off += align16(sizeof(uint32_t) * std::max<size_t>(apairs.size(), 1));
+    const size_t off_gpairs = off;
+    off += align16(sizeof(uint32_t) * std::max<size_t>(gpairs.size(), 1));
+    const size_t off_jpairs = off;
+    off += align16(sizeof(int) * std::max<size_t>(jpairs.size(), 4));
     const size_t off_lower = off;
     off += align16(sizeof(float) * nd);
     const size_t off_upper = off;
@@ -295,6 +319,8 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
     }
     if (!pairs.empty()) std::memcpy(host.data() + off_pairs, pairs.data(), pairs.size() * 4);
     if (!apairs.empty()) std::memcpy(host.data() + off_apairs, apairs.data(), apairs.size() * 4);
+    if (!gpairs.empty()) std::memcpy(host.data() + off_gpairs, gpairs.data(), gpairs.size() * 4);
+    if (!jpairs.empty()) std::memcpy(host.data() + off_jpairs, jpairs.data(), jpairs.size() * 4);
     std::memcpy(host.data() + off_lower, d->joint_lower, sizeof(float) * nd);
     std::memcpy(host.data() + off_upper, d->joint_upper, sizeof(float) * nd);
 
@@ -315,6 +341,9 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
     m->dev.blob = base;
     m->dev.self_pairs = reinterpret_cast<const uint32_t*>(base + off_pairs);
     m->dev.apx_self_pairs = reinterpret_cast<const uint32_t*>(base + off_apairs);
+    m->dev.gpairs = reinterpret_cast<const uint32_t*>(base + off_gpairs);
+    m->dev.jpairs = reinterpret_cast<const int4*>(base + off_jpairs);
+    m->dev.n_jpairs = (int)(jpairs.size() / 4);
     m->dev.lower = reinterpret_cast<const float*>(base + off_lower);
     m->dev.upper = reinterpret_cast<const float*>(base + off_upper);
     m->dev.status = reinterpret_cast<int*>(base + off_status);

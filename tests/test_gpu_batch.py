@@ -161,7 +161,7 @@ def test_batch_tune_keeps_results(w5):
     ep = api.EdgeEvalParams(max_joint_step=0.01, max_samples=600)
     cp = _cost_params(wl)
     t = batch.tune(sc, ep, cp)
-    assert t["traj_threads"] in (32, 64) and 0.0 < t["edge_share"] <= 1.0 and t["best_ms"] > 0.0
+    assert t["traj_threads"] in (128, 256) and 0.0 < t["edge_share"] <= 1.0 and t["best_ms"] > 0.0
     batch.launch(sc, ep, cp)
     torch.cuda.synchronize()
     _check_against_calls(b, sc, frm, to, reqs, trajs, ep, cp)
