@@ -43,13 +43,43 @@ FLOP_JOINT = 90      # FT*motion(q) 18 + 3x4 affine compose 72
 FLOP_SPHERE = 18     # sphere centre transform
 FLOP_PAIR = 30       # sphere-vs-box: rotate+translate 18, |l|-h 3, max 3, d^2 5, cmp 1
 FLOP_CULL = 30       # broad-phase box test (same arithmetic as a pair)
-FLOP_SELF = 10
+FLOP_SELF = 10       # self pair (or joint-pair bound) test: 3 sub, 3 FMA, sub, cmp
+FLOP_ESDF = 24       # ESDF lookup: quaternion rotate into the grid frame + index math
 
 
 def flops_from_stats(st):
     """st: [pairs, exact, samples, joints, spheres, self, esdf, cull]."""
     return (st[0] * FLOP_PAIR + st[1] * FLOP_PAIR + st[3] * FLOP_JOINT + st[4] * FLOP_SPHERE
-            + st[5] * FLOP_SELF + st[7] * FLOP_CULL)
+            + st[5] * FLOP_SELF + st[6] * FLOP_ESDF + st[7] * FLOP_CULL)
+
+
+def kernel_roofline(lib, dev, fn, reps=10):
+    """Executed-work FLOPs of one call of `fn` (device counters) and the median
+    duration of its main kernel (CUDA events recorded by the library around
+    it, on the call's stream)."""
+    import ctypes
+
+    import torch
+
+    st = torch.zeros(8, dtype=torch.int64, device=dev)
+    lib.ps_set_stats(ctypes.c_void_p(st.data_ptr()))
+    fn()
+    torch.cuda.synchronize()
+    lib.ps_set_stats(None)
+    stats = [int(x) for x in st.cpu().tolist()]
+    k0 = torch.cuda.Event(enable_timing=True)
+    k1 = torch.cuda.Event(enable_timing=True)
+    k0.record()
+    k1.record()
+    torch.cuda.synchronize()
+    lib.ps_set_timing_events(k0.cuda_event, k1.cuda_event)
+    ms = []
+    for _ in range(reps):
+        fn()
+        torch.cuda.synchronize()
+        ms.append(k0.elapsed_time(k1))
+    lib.ps_set_timing_events(None, None)
+    return stats, statistics.median(ms)
 
 
 def dist_env():
@@ -362,7 +392,7 @@ def cpu_baseline(b, wl, target_s=8.0):
             "sample": f"first {n2} of {len(frm)} edges, FP32 restatement with early exit, {dt:.1f} s"}
 
 
-def bench_configs(dev):
+def bench_configs(dev, with_ref=True):
     import torch
 
     from prismplan_b200 import api, workloads
@@ -385,6 +415,8 @@ def bench_configs(dev):
     ms = e0.elapsed_time(e1) / 5
     out = {"workload": "configs_panda7_obb16 (4096 tiled to 1,048,576)", "value": q.shape[0] / (ms * 1e-3),
            "unit": "configs/s", "ms_per_step": ms, "outputs": "hit + OBB min-clearance"}
+    if not with_ref:
+        return out
     try:
         import oracle
 
@@ -398,7 +430,7 @@ def bench_configs(dev):
     return out
 
 
-def bench_chomp(dev):
+def bench_chomp(dev, with_ref=True):
     import torch
 
     from prismplan_b200 import api, workloads
@@ -458,6 +490,18 @@ def bench_chomp(dev):
                        "path": "forward ps_traj_cost + central-difference gradient (2*D forward evaluations per "
                                "waypoint, one launch) + 2*lambda*R*theta"}
     out["speedup_vs_plain_fd"] = pms / ms
+    from prismplan_b200 import _lib
+
+    stats, kms = kernel_roofline(_lib.load(), dev, lambda: api.traj_cost(b, sc, q, p))
+    peak = probe_peak()
+    ach = flops_from_stats(stats) / (kms * 1e-3) / 1e12
+    out["roofline"] = {"bound": "fp32", "kernel": "waypoint_cost_kernel<grad>", "kernel_ms": kms,
+                       "achieved": ach, "peak": peak["tflops"], "unit": "TFLOP/s", "frac": ach / peak["tflops"],
+                       "flops_per_launch": flops_from_stats(stats),
+                       "work_per_launch": dict(zip(["pairs", "exact", "samples", "joints", "spheres", "self",
+                                                    "esdf", "cull"], stats))}
+    if not with_ref:
+        return out
     try:
         import oracle
 
@@ -473,7 +517,7 @@ def bench_chomp(dev):
     return out
 
 
-def bench_mixed(dev, reps: int = 10):
+def bench_mixed(dev, reps: int = 10, with_ref=True):
     """Mixed-size batch on the 14-DoF composite (128 OBBs + 128^3 ESDF): 65
     edge requests of 16..256 edges (8192 edges, 1..600 samples each) and 64
     CHOMP trajectories of 32..128 waypoints with cost + gradient. Plain =
@@ -593,8 +637,17 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--headline-only", action="store_true",
                     help="time the headline path only (profiling runs); skips roofline/e2e/baselines")
+    ap.add_argument("--case", choices=["configs", "chomp", "mixed"],
+                    help="run one secondary workload alone on cuda:0 and print its line (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.case:
+        import torch
+
+        dev = torch.device("cuda", 0)
+        fn = {"configs": bench_configs, "chomp": bench_chomp, "mixed": bench_mixed}[args.case]
+        print(json.dumps({"case": args.case, **fn(dev, with_ref=False)}), flush=True)
+        return
     res = run_reference(args) if args.impl == "reference" else run_ours(args)
     if res is not None:
         print(json.dumps(res), flush=True)
