@@ -332,6 +332,7 @@ def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev):
     # ---- other workloads: configs (1) and CHOMP cost+gradient (3) ----
     res["configs"] = bench_configs(dev)
     res["chomp"] = bench_chomp(dev)
+    res["stomp"] = bench_stomp(dev)
     res["mixed"] = bench_mixed(dev)
     return res
 
@@ -415,6 +416,16 @@ def bench_configs(dev, with_ref=True):
     ms = e0.elapsed_time(e1) / 5
     out = {"workload": "configs_panda7_obb16 (4096 tiled to 1,048,576)", "value": q.shape[0] / (ms * 1e-3),
            "unit": "configs/s", "ms_per_step": ms, "outputs": "hit + OBB min-clearance"}
+    from prismplan_b200 import _lib
+
+    stats, kms = kernel_roofline(_lib.load(), dev, lambda: api.check_configs(b, sc, q, clearance="obb"))
+    peak = probe_peak()
+    ach = flops_from_stats(stats) / (kms * 1e-3) / 1e12
+    out["roofline"] = {"bound": "fp32", "kernel": "check_configs_kernel<clearance>", "kernel_ms": kms,
+                       "achieved": ach, "peak": peak["tflops"], "unit": "TFLOP/s", "frac": ach / peak["tflops"],
+                       "flops_per_launch": flops_from_stats(stats),
+                       "work_per_launch": dict(zip(["pairs", "exact", "samples", "joints", "spheres", "self",
+                                                    "esdf", "cull"], stats))}
     if not with_ref:
         return out
     try:
@@ -515,6 +526,71 @@ def bench_chomp(dev, with_ref=True):
     except Exception as e:
         out["reference_gpu"] = {"unavailable": str(e)[:200]}
     return out
+
+
+def bench_stomp(dev, with_ref=True):
+    """STOMP rollout state costs: 32 trajectories x 128 noisy rollouts x 100
+    waypoints of an 8-DoF Fetch-like chain (70 spheres) against 96 OBBs, in
+    the reference layout [(r*D + d)*T + t], cost broadcast over d as
+    stomp_state_cost_kernel writes it."""
+    import ctypes
+
+    import torch
+
+    from prismplan_b200 import _lib, api, workloads
+    from prismplan_b200.robot import RobotModelBuilder
+    from prismplan_b200.scene import SceneTensors
+
+    wl = workloads.workload(4)
+    b = RobotModelBuilder.from_asset(wl["asset"]).build()
+    sc = SceneTensors(*wl["obbs"])
+    r = torch.from_numpy(wl["rollouts"]).to(dev)
+    R, D, T = r.shape
+    p = api.CostParams(collision_cost_weight=wl["w"], world_collision_margin=wl["eps"],
+                       self_collision_margin=wl["self_margin"])
+    out = torch.empty((R, D, T), device=dev)
+    v = sc.view()
+    pc = p.to_c(_lib.PS_LAYOUT_BDT)
+    lib = _lib.load()
+
+    def run():
+        _lib.check(lib.ps_rollout_costs(b.handle, ctypes.byref(v), r.data_ptr(), R, T, ctypes.byref(pc), 1,
+                                        out.data_ptr(), None))
+
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 10
+    stats, kms = kernel_roofline(lib, dev, run)
+    peak = probe_peak()
+    ach = flops_from_stats(stats) / (kms * 1e-3) / 1e12
+    res = {"workload": wl["name"], "value": R * T / (ms * 1e-3), "unit": "rollout waypoints/s", "ms_per_step": ms,
+           "rollouts_per_s": R / (ms * 1e-3), "path": "ps_rollout_costs (one launch, cost broadcast over D)",
+           "roofline": {"bound": "fp32", "kernel": "waypoint_cost_kernel<no grad>", "kernel_ms": kms,
+                        "achieved": ach, "peak": peak["tflops"], "unit": "TFLOP/s", "frac": ach / peak["tflops"],
+                        "flops_per_launch": flops_from_stats(stats),
+                        "work_per_launch": dict(zip(["pairs", "exact", "samples", "joints", "spheres", "self",
+                                                     "esdf", "cull"], stats))}}
+    if not with_ref:
+        return res
+    try:
+        import oracle
+
+        ref = oracle.RefKernels(b, *wl["obbs"])
+        ref.stomp(wl["rollouts"][:64], wl["w"], wl["eps"], wl["self_margin"])
+        _, rms = ref.stomp(wl["rollouts"], wl["w"], wl["eps"], wl["self_margin"])
+        res["reference_gpu"] = {"value": R * T / (rms * 1e-3), "unit": "rollout waypoints/s", "ms_per_step": rms,
+                                "path": "stomp_state_cost_kernel<<<R*T, 4>>> (one launch)"}
+        res["speedup_vs_reference"] = rms / ms
+    except Exception as e:
+        res["reference_gpu"] = {"unavailable": str(e)[:200]}
+    return res
 
 
 def bench_mixed(dev, reps: int = 10, with_ref=True):
@@ -637,7 +713,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--headline-only", action="store_true",
                     help="time the headline path only (profiling runs); skips roofline/e2e/baselines")
-    ap.add_argument("--case", choices=["configs", "chomp", "mixed"],
+    ap.add_argument("--case", choices=["configs", "chomp", "stomp", "mixed"],
                     help="run one secondary workload alone on cuda:0 and print its line (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -645,7 +721,7 @@ def main():
         import torch
 
         dev = torch.device("cuda", 0)
-        fn = {"configs": bench_configs, "chomp": bench_chomp, "mixed": bench_mixed}[args.case]
+        fn = {"configs": bench_configs, "chomp": bench_chomp, "stomp": bench_stomp, "mixed": bench_mixed}[args.case]
         print(json.dumps({"case": args.case, **fn(dev, with_ref=False)}), flush=True)
         return
     res = run_reference(args) if args.impl == "reference" else run_ours(args)

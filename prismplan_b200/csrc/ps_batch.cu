@@ -96,8 +96,7 @@ __global__ void batch_gather_traj(const TrajReq* __restrict__ req, const Counts*
 }
 
 size_t waypoint_smem_bytes(const ps_model* m, const ps_scene_view* sv, int warps) {
-    return (size_t)m->dev.bytes_core + scene_smem_bytes(sv) + (((size_t)m->info.n_spheres + 15) & ~size_t(15)) +
-           (size_t)warps * cost_warp_floats(m->info.n_joints, m->info.n_spheres, sv->n_obbs, true) * 4;
+    return cost_block_bytes(m, sv, warps, true);
 }
 
 // Cost and adjoint of every packed waypoint, one warp per waypoint.
@@ -120,22 +119,19 @@ __global__ void __launch_bounds__(kWarps * 32, 24 / kWarps) batch_waypoint_kerne
     const int nob = max(sv.n_obbs, 1);
     int* orig = reinterpret_cast<int*>(obbs + nob);
     LayerPrep* layers = reinterpret_cast<LayerPrep*>(orig + ((nob + 3) & ~3));
-    unsigned char* sph_joint = reinterpret_cast<unsigned char*>(layers + PS_MAX_LAYERS);
-    float* wbase = reinterpret_cast<float*>(sph_joint + ((NS + 15) & ~15));
     SceneSmem sc;
     stage_scene(sv, obbs, orig, layers, counters, &bmax, sc);
-    for (int p = 0; p < NJ; ++p)
-        for (int k = M.J[p].sph_beg + threadIdx.x; k < M.J[p].sph_end; k += blockDim.x) sph_joint[k] = (unsigned char)p;
+    const CostBlock cb = cost_block_setup(reinterpret_cast<unsigned char*>(layers + PS_MAX_LAYERS), M, sc, sv.n_obbs);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const CostWarpScratch ws =
-        cost_carve(wbase + (size_t)warp * cost_warp_floats(NJ, NS, sv.n_obbs, true), NJ, NS, sc.n_obbs, true);
+        cost_carve(cb.wbase + (size_t)warp * cost_warp_floats(NJ, NS, sv.n_obbs, true), NJ, NS, sc.n_obbs, true);
     LaneStats st;
     st.zero();
     for (int k = blockIdx.x * kWarps + warp; k < n_wp; k += gridDim.x * kWarps) {
         if (lane < D) ws.q[lane] = q[(size_t)k * D + lane];
         __syncwarp();
-        const float c = waypoint_cost_warp<true>(M, md, sc, sv, P, sph_joint, ws, grad + (size_t)k * D, 1, st);
+        const float c = waypoint_cost_warp<true>(M, md, sc, sv, P, cb, ws, grad + (size_t)k * D, 1, st);
         if (lane == 0) wp_cost[k] = c;
         __syncwarp();
     }

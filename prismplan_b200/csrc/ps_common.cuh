@@ -49,7 +49,8 @@ struct JointRec {
 
 // Self pairs (global memory): packed (i | j << 16), reordered sphere indices.
 // gpairs holds the same pairs grouped by the DFS positions of their two
-// joints; jpairs[g] = (joint of i, joint of j, first, end) indexes gpairs.
+// joints, packed (i | j << 9 | g << 18); jpairs[g] = (joint of i, joint of j,
+// first, end) indexes gpairs.
 // Limits (global memory): lower[n_dof], upper[n_dof].
 struct ModelDev {
     const unsigned char* blob;     // device
@@ -212,22 +213,15 @@ __device__ __forceinline__ void compose_row(const Affine& P, const float* s, Aff
 // and contraction (utils.cuh:571-711; runtime_kinematics.cuh:60-70). The
 // step's row 3 is (0,0,0,1) (validated at model creation), so the fourth
 // dot4 term is an exact +0 for rotation columns and +T_par[r][3] for the
-// translation column. fast_sincos selects __sinf/__cosf (reference, used by
-// every Boolean) or sincosf (accurate, used by the cost/gradient path).
-template <bool kFastSinCos>
-__device__ __forceinline__ void joint_compose(const JointRec& J, float qi, const Affine& P, Affine& O) {
+// translation column. sn/cs are the joint angle's sine and cosine (read by
+// rotation joints only).
+__device__ __forceinline__ void joint_compose_sc(const JointRec& J, float qi, float sn, float cs, const Affine& P,
+                                                 Affine& O) {
     float s[12];   // step rows 0..2
 #pragma unroll
     for (int k = 0; k < 12; ++k) s[k] = J.ft[k];
     const int type = J.type;
     if (type >= PS_X_ROT) {
-        float sn, cs;
-        if (kFastSinCos) {
-            cs = __cosf(qi);
-            sn = __sinf(qi);
-        } else {
-            sincosf(qi, &sn, &cs);
-        }
         const float nsn = -sn;
         step_rot_row<0>(J, type, cs, sn, nsn, s);
         step_rot_row<1>(J, type, cs, sn, nsn, s);
@@ -240,6 +234,23 @@ __device__ __forceinline__ void joint_compose(const JointRec& J, float qi, const
     compose_row<0>(P, s, O);
     compose_row<1>(P, s, O);
     compose_row<2>(P, s, O);
+}
+
+// The same step with its sine/cosine evaluated here: kFastSinCos selects
+// __sinf/__cosf (reference, used by every Boolean) or sincosf (accurate, used
+// by the cost/gradient path).
+template <bool kFastSinCos>
+__device__ __forceinline__ void joint_compose(const JointRec& J, float qi, const Affine& P, Affine& O) {
+    float sn = 0.0f, cs = 1.0f;
+    if (J.type >= PS_X_ROT) {
+        if (kFastSinCos) {
+            cs = __cosf(qi);
+            sn = __sinf(qi);
+        } else {
+            sincosf(qi, &sn, &cs);
+        }
+    }
+    joint_compose_sc(J, qi, sn, cs, P, O);
 }
 
 // World position of a link-frame point (runtime_kinematics.cuh:79-83).

@@ -30,8 +30,7 @@ namespace {
 constexpr int kCostWarps = 8;   // waypoints in flight per block (one per warp)
 
 size_t cost_block_smem(const ps_model* m, const ps_scene_view* sv, bool grad) {
-    return (size_t)m->dev.bytes_core + scene_smem_bytes(sv) + (((size_t)m->info.n_spheres + 15) & ~size_t(15)) +
-           (size_t)kCostWarps * cost_warp_floats(m->info.n_joints, m->info.n_spheres, sv->n_obbs, grad) * 4;
+    return cost_block_bytes(m, sv, kCostWarps, grad);
 }
 
 // One warp per waypoint (see ps_costwarp.cuh). kGrad: also the adjoint.
@@ -52,17 +51,14 @@ __global__ void __launch_bounds__(kCostWarps * 32, 3) waypoint_cost_kernel(
     const int nob = max(sv.n_obbs, 1);
     int* orig = reinterpret_cast<int*>(obbs + nob);
     LayerPrep* layers = reinterpret_cast<LayerPrep*>(orig + ((nob + 3) & ~3));
-    unsigned char* sph_joint = reinterpret_cast<unsigned char*>(layers + PS_MAX_LAYERS);
-    float* wbase = reinterpret_cast<float*>(sph_joint + ((NS + 15) & ~15));
     SceneSmem sc;
     stage_scene(sv, obbs, orig, layers, counters, &bmax, sc);
-    for (int p = 0; p < NJ; ++p)
-        for (int k = M.J[p].sph_beg + threadIdx.x; k < M.J[p].sph_end; k += blockDim.x) sph_joint[k] = (unsigned char)p;
+    const CostBlock cb = cost_block_setup(reinterpret_cast<unsigned char*>(layers + PS_MAX_LAYERS), M, sc, sv.n_obbs);
     __syncthreads();
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const CostWarpScratch ws =
-        cost_carve(wbase + (size_t)warp * cost_warp_floats(NJ, NS, sv.n_obbs, kGrad), NJ, NS, sc.n_obbs, kGrad);
+        cost_carve(cb.wbase + (size_t)warp * cost_warp_floats(NJ, NS, sv.n_obbs, kGrad), NJ, NS, sc.n_obbs, kGrad);
     const bool bdt = P.layout == PS_LAYOUT_BDT;
     const long long total = (long long)n_rows * T;
     LaneStats st;
@@ -79,7 +75,7 @@ __global__ void __launch_bounds__(kCostWarps * 32, 3) waypoint_cost_kernel(
             grow = bdt ? grad + ((size_t)b * D) * T + t : grad + ((size_t)b * T + t) * D;
             gstride = bdt ? T : 1;
         }
-        const float cost = waypoint_cost_warp<kGrad>(M, md, sc, sv, P, sph_joint, ws, grow, gstride, st);
+        const float cost = waypoint_cost_warp<kGrad>(M, md, sc, sv, P, cb, ws, grow, gstride, st);
         if (lane == 0) {
             st.v[ST_SAMPLES] += 1;
             if (wp_cost) {

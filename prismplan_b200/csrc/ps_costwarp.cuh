@@ -8,21 +8,28 @@
 //         + relu(m_self - min_(i,j) (|p_i - p_j| - r_i - r_j)) ).
 // The reference evaluates every sphere against every box and every self pair
 // in one thread. Here the 32 lanes of a warp share one waypoint:
-//   1. FK (every lane walks the chain; lane p keeps frame p in shared memory);
+//   1. FK: lane p evaluates joint p's sine/cosine, every lane walks the chain
+//      with them, lane p keeps frame p in shared memory;
 //   2. per joint, the boxes that can reach any of its spheres within the
 //      hinge band are found from the joint's bound sphere (lanes over boxes,
 //      one ballot word per 32 boxes): a box farther than R_p + max(m, 0)
 //      from the bound centre has sdf > m + r for every sphere of the joint
-//      and contributes nothing;
+//      and contributes nothing. A circumscribed-sphere test of the box comes
+//      first, the box distance only for the boxes it keeps;
 //   3. lanes over spheres: closest candidate box, ESDF, hinge and d/dp;
 //   4. self hinge: joint pairs whose bound spheres are within m_self of each
-//      other expand their sphere pairs across the lanes; warp argmin;
+//      other expand their sphere pairs across the lanes; a pair whose squared
+//      distance is outside (r_i + r_j + m_self)^2 cannot set the hinge and
+//      skips the square root; warp argmin;
 //   5. adjoint: per joint F = sum g, M = sum p x g (lane per joint), subtree
 //      accumulation from the leaves, dC/dq = a . (M - o x F) (revolute) or
 //      a . F (prismatic), a/o the joint axis/origin in the world.
 // Sums run in a fixed order (lane-strided partials, xor-tree reduction), so a
 // waypoint gives the same bits wherever it is evaluated.
 #pragma once
+
+#include <algorithm>
+#include <cstdint>
 
 #include "ps_internal.h"
 #include "ps_verdict.cuh"
@@ -32,22 +39,25 @@ namespace {
 
 constexpr unsigned kCostFull = 0xffffffffu;
 
-// Per-warp scratch in shared memory (floats unless noted).
+// Per-warp scratch in shared memory (floats unless noted; 16-byte aligned).
 struct CostWarpScratch {
     float* q;        // [16]
     float* frame;    // [NJ][12]
-    float* bnd;      // [NJ][4]: bound centre (world), radius
-    float* pos;      // [NS][3]
+    float4* bnd;     // [NJ][2]: (bound centre (world), radius), (box cull threshold, its square, |centre|inf, -)
+    float4* pos;     // [NS]: centre (world), radius
     float* g;        // [NS][3]   (gradient only)
     float* jfm;      // [NJ][8]: F, M, dC/dq   (gradient only)
+    unsigned* jact;  // [8]       active joint-pair groups (one bit each)
     unsigned* mask;  // [NJ][nw]  candidate boxes per joint
 };
 
 __host__ __device__ inline int cost_mask_words(int n_obbs) { return (n_obbs + 31) / 32; }
 
 __host__ __device__ inline size_t cost_warp_floats(int NJ, int NS, int n_obbs, bool grad) {
-    size_t f = 16 + (size_t)NJ * 12 + (size_t)NJ * 4 + (size_t)NS * 3 + (size_t)NJ * cost_mask_words(n_obbs);
+    size_t f = 16 + (size_t)NJ * 12 + (size_t)NJ * 8 + (size_t)NS * 4;
     if (grad) f += (size_t)NS * 3 + (size_t)NJ * 8;
+    f = (f + 3) & ~size_t(3);
+    f += 8 + (size_t)NJ * cost_mask_words(n_obbs);
     return (f + 3) & ~size_t(3);   // keep every warp's slice 16-byte aligned
 }
 
@@ -55,9 +65,9 @@ __device__ __forceinline__ CostWarpScratch cost_carve(float* base, int NJ, int N
     CostWarpScratch w;
     w.q = base;
     w.frame = w.q + 16;
-    w.bnd = w.frame + NJ * 12;
-    w.pos = w.bnd + NJ * 4;
-    float* p = w.pos + NS * 3;
+    w.bnd = reinterpret_cast<float4*>(w.frame + NJ * 12);
+    w.pos = w.bnd + NJ * 2;
+    float* p = reinterpret_cast<float*>(w.pos + NS);
     if (grad) {
         w.g = p;
         w.jfm = w.g + NS * 3;
@@ -66,8 +76,87 @@ __device__ __forceinline__ CostWarpScratch cost_carve(float* base, int NJ, int N
         w.g = nullptr;
         w.jfm = nullptr;
     }
-    w.mask = reinterpret_cast<unsigned*>(p);
+    p = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
+    w.jact = reinterpret_cast<unsigned*>(p);
+    w.mask = w.jact + 8;
     return w;
+}
+
+// Block-wide tables of the cost kernels, placed after the staged scene:
+//   sph_joint[NS]  DFS position of each reordered sphere
+//   dof_joint[16]  per DoF: the one joint it drives, -1 none, -2 several
+//   jlist[32], njs the joints that carry exact spheres
+//   obs[n_obbs]    world centre and circumscribed radius of each box
+struct CostBlock {
+    const unsigned char* sph_joint;
+    const signed char* dof_joint;
+    const unsigned char* jlist;
+    const int* njs;
+    const float4* obs;
+    float* wbase;    // first warp's scratch
+};
+
+inline size_t cost_block_bytes(const ps_model* m, const ps_scene_view* sv, int warps, bool grad) {
+    return (size_t)m->dev.bytes_core + scene_smem_bytes(sv) + (((size_t)m->info.n_spheres + 15) & ~size_t(15)) + 64 +
+           (size_t)16 * std::max(sv->n_obbs, 1) +
+           (size_t)warps * cost_warp_floats(m->info.n_joints, m->info.n_spheres, sv->n_obbs, grad) * 4;
+}
+
+// Fills the block tables (every thread calls it; the caller syncs after).
+__device__ __forceinline__ CostBlock cost_block_setup(unsigned char* at, const ModelSmem& M, const SceneSmem& sc,
+                                                      int n_obbs_alloc) {
+    const int NJ = M.H->n_joints, NS = M.H->n_spheres, D = M.H->n_dof;
+    CostBlock cb;
+    unsigned char* sj = at;
+    signed char* dj = reinterpret_cast<signed char*>(sj + ((NS + 15) & ~15));
+    unsigned char* jl = reinterpret_cast<unsigned char*>(dj + 16);
+    int* njs = reinterpret_cast<int*>(dj + 48);
+    float4* obs = reinterpret_cast<float4*>(dj + 64);
+    cb.sph_joint = sj;
+    cb.dof_joint = dj;
+    cb.jlist = jl;
+    cb.njs = njs;
+    cb.obs = obs;
+    if (threadIdx.x == 0) {
+        int n = 0;
+        for (int p = 0; p < NJ; ++p)
+            if (M.J[p].sph_end > M.J[p].sph_beg) jl[n++] = (unsigned char)p;
+        *njs = n;
+    }
+    cb.wbase = reinterpret_cast<float*>(obs + max(n_obbs_alloc, 1));
+    for (int p = 0; p < NJ; ++p)
+        for (int k = M.J[p].sph_beg + threadIdx.x; k < M.J[p].sph_end; k += blockDim.x) sj[k] = (unsigned char)p;
+    for (int d = threadIdx.x; d < D; d += blockDim.x) {
+        int who = -1;
+        for (int p = 1; p < NJ; ++p)
+            if (M.J[p].dof == d && M.J[p].type != PS_FIXED) who = who == -1 ? p : -2;
+        dj[d] = (signed char)who;
+    }
+    for (int o = threadIdx.x; o < sc.n_obbs; o += blockDim.x) {
+        const ObbPrep& b = sc.obbs[o];
+        // local = R p + t  =>  centre p = -R^T t
+        const float cx = -(b.r0.x * b.r0.w + b.r1.x * b.r1.w + b.r2.x * b.r2.w);
+        const float cy = -(b.r0.y * b.r0.w + b.r1.y * b.r1.w + b.r2.y * b.r2.w);
+        const float cz = -(b.r0.z * b.r0.w + b.r1.z * b.r1.w + b.r2.z * b.r2.w);
+        const float r = sqrtf(b.h.x * b.h.x + b.h.y * b.h.y + b.h.z * b.h.z);
+        obs[o] = make_float4(cx, cy, cz, r);
+    }
+    return cb;
+}
+
+__device__ __forceinline__ void load_frame(const float* f, Affine& T) {
+    const float4* v = reinterpret_cast<const float4*>(f);
+    const float4 a = v[0], b = v[1], c = v[2];
+    T.m[0] = a.x; T.m[1] = a.y; T.m[2] = a.z; T.m[3] = a.w;
+    T.m[4] = b.x; T.m[5] = b.y; T.m[6] = b.z; T.m[7] = b.w;
+    T.m[8] = c.x; T.m[9] = c.y; T.m[10] = c.z; T.m[11] = c.w;
+}
+
+__device__ __forceinline__ void store_frame(float* f, const Affine& T) {
+    float4* v = reinterpret_cast<float4*>(f);
+    v[0] = make_float4(T.m[0], T.m[1], T.m[2], T.m[3]);
+    v[1] = make_float4(T.m[4], T.m[5], T.m[6], T.m[7]);
+    v[2] = make_float4(T.m[8], T.m[9], T.m[10], T.m[11]);
 }
 
 // World gradient of the SDF of box o at p.
@@ -158,63 +247,94 @@ __device__ __forceinline__ float warp_sum(float v) {
 // configuration is ws.q[0..D).
 template <bool kGrad>
 __device__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, const SceneSmem& sc,
-                                    const ps_scene_view& sv, const ps_cost_params& P,
-                                    const unsigned char* sph_joint, const CostWarpScratch& ws, float* grad_row,
-                                    int gstride, LaneStats& st) {
+                                    const ps_scene_view& sv, const ps_cost_params& P, const CostBlock& cb,
+                                    const CostWarpScratch& ws, float* grad_row, int gstride, LaneStats& st) {
     const int lane = threadIdx.x & 31;
     const int D = M.H->n_dof, NJ = M.H->n_joints, NS = M.H->n_spheres;
     const float w = P.collision_cost_weight, wm = P.world_margin, smg = P.self_margin;
     const int nob = sc.n_obbs, nw = cost_mask_words(nob);
 
-    // ---- 1. FK: every lane walks the chain, lane p stores frame p ----
+    // ---- 1. FK by pointer jumping: lane p < NJ forms joint p's local step
+    //      S_p = FT_p * motion(q) and holds A_p, the transform from its
+    //      current ancestor anc_p to p; each round composes A_anc * A_p and
+    //      jumps anc_p to anc_anc, so depth d takes ceil(log2 d) rounds. ----
     {
-        Affine s0, s1, Tf;
-        affine_identity(s0);
-        affine_identity(s1);
-        for (int p = 0; p < NJ; ++p) {
-            fk_step<false>(M.J[p], p, ws.q, s0, s1, Tf);
-            if (lane == (p & 31)) {
+        Affine A;
+        affine_identity(A);
+        int anc = -1;
+        if (lane > 0 && lane < NJ) {
+            const JointRec& jr = M.J[lane];
+            const float qi = jr.dof >= 0 ? ws.q[jr.dof] : 0.0f;
+            float sn = 0.0f, cs = 1.0f;
+            if (jr.type >= PS_X_ROT) sincosf(qi, &sn, &cs);
+            Affine I;
+            affine_identity(I);
+            joint_compose_sc(jr, qi, sn, cs, I, A);
+            anc = jr.parent_pos;
+        }
+        while (__ballot_sync(kCostFull, anc >= 0)) {
+            const int src = anc >= 0 ? anc : lane;
+            Affine B;
 #pragma unroll
-                for (int i = 0; i < 12; ++i) ws.frame[p * 12 + i] = Tf.m[i];
+            for (int i = 0; i < 12; ++i) B.m[i] = __shfl_sync(kCostFull, A.m[i], src);
+            const int anc2 = __shfl_sync(kCostFull, anc, src);
+            if (anc >= 0) {
+                Affine C;
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        float v = fmaf(B.m[r * 4 + 2], A.m[8 + c], fmaf(B.m[r * 4 + 1], A.m[4 + c], B.m[r * 4] * A.m[c]));
+                        C.m[r * 4 + c] = c == 3 ? v + B.m[r * 4 + 3] : v;
+                    }
+                }
+                A = C;
+                anc = anc2;
             }
+        }
+        if (lane < NJ) {
+            const JointRec& jr = M.J[lane];
+            store_frame(ws.frame + lane * 12, A);
+            const float4 b = jr.bound;
+            float cx = 0.f, cy = 0.f, cz = 0.f, thr = -1.0f;
+            if (b.w >= 0.0f) {
+                sphere_world(A, b.x, b.y, b.z, cx, cy, cz);
+                // a box farther than R + max(m, 0) from the centre reaches no
+                // sphere of the joint inside the hinge band; slack for FP32
+                const float S = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz)));
+                thr = b.w + fmaxf(wm, 0.0f);
+                thr += 4.0f * (S + thr + sc.Bmax + 1.0f) * PS_GUARD_K;
+            }
+            ws.bnd[lane * 2] = make_float4(cx, cy, cz, b.w);
+            ws.bnd[lane * 2 + 1] = make_float4(thr, thr * thr, fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))), 0.0f);
         }
         if (lane == 0) st.v[ST_JOINTS] += NJ;
     }
     __syncwarp();
-    // bound sphere of each joint in the world
-    for (int p = lane; p < NJ; p += 32) {
-        const float4 b = M.J[p].bound;
-        Affine T;
-#pragma unroll
-        for (int i = 0; i < 12; ++i) T.m[i] = ws.frame[p * 12 + i];
-        float cx = 0.f, cy = 0.f, cz = 0.f;
-        if (b.w >= 0.0f) sphere_world(T, b.x, b.y, b.z, cx, cy, cz);
-        ws.bnd[p * 4 + 0] = cx;
-        ws.bnd[p * 4 + 1] = cy;
-        ws.bnd[p * 4 + 2] = cz;
-        ws.bnd[p * 4 + 3] = b.w;
-    }
-    __syncwarp();
 
-    // ---- 2. candidate boxes per joint (lanes over boxes) ----
+    // ---- 2. candidate boxes per joint (lanes over boxes): circumscribed-
+    //      sphere prefilter, then the box distance of the bound centre ----
     if (nob > 0) {
-        const float mpos = fmaxf(wm, 0.0f);
         for (int base = 0; base < nob; base += 32) {
             const int o = base + lane;
             const bool ok = o < nob;
-            ObbPrep box;
-            if (ok) box = sc.obbs[o];
-            for (int p = 0; p < NJ; ++p) {
-                const float R = ws.bnd[p * 4 + 3];
+            float4 ob = make_float4(0.f, 0.f, 0.f, -1.0f);
+            if (ok) ob = cb.obs[o];
+            const float So = fmaxf(fabsf(ob.x), fmaxf(fabsf(ob.y), fabsf(ob.z))) + ob.w;
+            const int njs = *cb.njs;
+            for (int pi = 0; pi < njs; ++pi) {
+                const int p = cb.jlist[pi];
+                const float4 bc = ws.bnd[p * 2];
+                const float4 th = ws.bnd[p * 2 + 1];
                 bool keep = false;
-                if (R >= 0.0f && ok) {
-                    const float cx = ws.bnd[p * 4 + 0], cy = ws.bnd[p * 4 + 1], cz = ws.bnd[p * 4 + 2];
-                    // slack for the FP32 rounding of the transforms and the test
-                    const float S = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz)));
-                    float thr = R + mpos;
-                    thr += 4.0f * (S + thr + sc.Bmax + 1.0f) * PS_GUARD_K;
-                    float qx, qy, qz;
-                    keep = fast_box_dsq(box, cx, cy, cz, qx, qy, qz) < thr * thr;
+                if (ok && bc.w >= 0.0f) {
+                    const float dx = bc.x - ob.x, dy = bc.y - ob.y, dz = bc.z - ob.z;
+                    float lim = th.x + ob.w;
+                    lim += 4.0f * (So + th.z + lim + 1.0f) * PS_GUARD_K;
+                    if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) < lim * lim) {
+                        float qx, qy, qz;
+                        keep = fast_box_dsq(sc.obbs[o], bc.x, bc.y, bc.z, qx, qy, qz) < th.y;
+                    }
                     st.v[ST_CULL] += 1;
                 }
                 const unsigned bal = __ballot_sync(kCostFull, keep);
@@ -227,16 +347,13 @@ __device__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, cons
     // ---- 3. spheres (lanes over spheres) ----
     float obb_part = 0.0f, esdf_part = 0.0f;
     for (int k = lane; k < NS; k += 32) {
-        const int p = sph_joint[k];
+        const int p = cb.sph_joint[k];
         const float4 sp = M.S[k];
         Affine T;
-#pragma unroll
-        for (int i = 0; i < 12; ++i) T.m[i] = ws.frame[p * 12 + i];
+        load_frame(ws.frame + p * 12, T);
         float px, py, pz;
         sphere_world(T, sp.x, sp.y, sp.z, px, py, pz);
-        ws.pos[k * 3 + 0] = px;
-        ws.pos[k * 3 + 1] = py;
-        ws.pos[k * 3 + 2] = pz;
+        ws.pos[k] = make_float4(px, py, pz, sp.w);
         st.v[ST_SPHERES] += 1;
         const int so = M.SO[k];
         float gx = 0.f, gy = 0.f, gz = 0.f;
@@ -303,44 +420,49 @@ __device__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, cons
     }
     __syncwarp();
 
-    // ---- 4. self hinge: joint-pair prefilter, then sphere pairs ----
+    // ---- 4. self hinge: joint-pair prefilter, then sphere pairs whose
+    //      squared distance is inside (r_i + r_j + m_self)^2 ----
     float self_h = 0.0f;
     int self_arg = -1;
     if (P.include_self && md.n_jpairs > 0) {
         float bv = 3.0e38f;
         int bk = 0x7fffffff;
+        const float smp = fmaxf(smg, 0.0f);
         for (int base = 0; base < md.n_jpairs; base += 32) {
             const int gi = base + lane;
             bool act = false;
-            int4 jp = make_int4(0, 0, 0, 0);
             if (gi < md.n_jpairs) {
-                jp = __ldg(md.jpairs + gi);
-                const float* A = ws.bnd + jp.x * 4;
-                const float* B = ws.bnd + jp.y * 4;
-                const float dx = A[0] - B[0], dy = A[1] - B[1], dz = A[2] - B[2];
-                const float S = fmaxf(fmaxf(fabsf(A[0]), fabsf(A[1])), fmaxf(fabsf(A[2]), fmaxf(fabsf(B[0]),
-                                fmaxf(fabsf(B[1]), fabsf(B[2])))));
-                float thr = A[3] + B[3] + fmaxf(smg, 0.0f);
+                const int4 jp = __ldg(md.jpairs + gi);
+                const float4 A = ws.bnd[jp.x * 2], B = ws.bnd[jp.y * 2];
+                const float dx = A.x - B.x, dy = A.y - B.y, dz = A.z - B.z;
+                const float S = fmaxf(fmaxf(fabsf(A.x), fabsf(A.y)), fmaxf(fabsf(A.z), fmaxf(fabsf(B.x),
+                                fmaxf(fabsf(B.y), fabsf(B.z)))));
+                float thr = A.w + B.w + smp;
                 thr += 4.0f * (S + thr + 1.0f) * PS_GUARD_K;
                 act = fmaf(dz, dz, fmaf(dy, dy, dx * dx)) < thr * thr;
                 st.v[ST_SELF] += 1;
             }
-            unsigned todo = __ballot_sync(kCostFull, act);
-            while (todo) {
-                const int src = __ffs(todo) - 1;
-                todo &= todo - 1;
-                const int beg = __shfl_sync(kCostFull, jp.z, src), end = __shfl_sync(kCostFull, jp.w, src);
-                for (int k = beg + lane; k < end; k += 32) {
-                    const uint32_t pr = __ldg(md.gpairs + k);
-                    const int i = pr & 0xffff, j = pr >> 16;
-                    const float dx = ws.pos[i * 3] - ws.pos[j * 3], dy = ws.pos[i * 3 + 1] - ws.pos[j * 3 + 1],
-                                dz = ws.pos[i * 3 + 2] - ws.pos[j * 3 + 2];
-                    const float c = sqrtf(fmaf(dz, dz, fmaf(dy, dy, dx * dx))) - (M.S[i].w + M.S[j].w);
-                    if (c < bv || (c == bv && k < bk)) {
-                        bv = c;
-                        bk = k;
-                    }
-                    st.v[ST_SELF] += 1;
+            const unsigned bal = __ballot_sync(kCostFull, act);
+            if (lane == 0) ws.jact[base >> 5] = bal;
+        }
+        __syncwarp();
+        // every pair, in gpairs order; pairs of inactive groups are skipped
+        const int n_pairs = M.H->n_self_pairs;
+        for (int k = lane; k < n_pairs; k += 32) {
+            const uint32_t pr = __ldg(md.gpairs + k);
+            const uint32_t g = pr >> 18;
+            if (!((ws.jact[g >> 5] >> (g & 31)) & 1u)) continue;
+            const float4 a = ws.pos[pr & 0x1ffu], b = ws.pos[(pr >> 9) & 0x1ffu];
+            const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+            const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            const float rs = a.w + b.w;
+            const float lim = (rs + smp) * (1.0f + 1.0e-5f) + 1.0e-6f;
+            st.v[ST_SELF] += 1;
+            if (d2 < lim * lim) {
+                const float c = sqrtf(d2) - rs;
+                if (c < bv || (c == bv && k < bk)) {
+                    bv = c;
+                    bk = k;
                 }
             }
         }
@@ -362,9 +484,9 @@ __device__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, cons
     // ---- 5. adjoint ----
     if (self_arg >= 0 && lane == 0) {
         const uint32_t pr = __ldg(md.gpairs + self_arg);
-        const int i = pr & 0xffff, j = pr >> 16;
-        const float dx = ws.pos[i * 3] - ws.pos[j * 3], dy = ws.pos[i * 3 + 1] - ws.pos[j * 3 + 1],
-                    dz = ws.pos[i * 3 + 2] - ws.pos[j * 3 + 2];
+        const int i = pr & 0x1ffu, j = (pr >> 9) & 0x1ffu;
+        const float4 a = ws.pos[i], b = ws.pos[j];
+        const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
         const float dd = sqrtf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
         if (dd > 0.0f) {
             // d cost / d p_i = -w (p_i - p_j)/d ; d cost / d p_j = +w (p_i - p_j)/d
@@ -383,11 +505,11 @@ __device__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, cons
         float Fx = 0.f, Fy = 0.f, Fz = 0.f, Mx = 0.f, My = 0.f, Mz = 0.f;
         for (int k = M.J[p].sph_beg; k < M.J[p].sph_end; ++k) {
             const float gx = ws.g[k * 3], gy = ws.g[k * 3 + 1], gz = ws.g[k * 3 + 2];
-            const float px = ws.pos[k * 3], py = ws.pos[k * 3 + 1], pz = ws.pos[k * 3 + 2];
+            const float4 pk = ws.pos[k];
             Fx += gx; Fy += gy; Fz += gz;
-            Mx += py * gz - pz * gy;
-            My += pz * gx - px * gz;
-            Mz += px * gy - py * gx;
+            Mx += pk.y * gz - pk.z * gy;
+            My += pk.z * gx - pk.x * gz;
+            Mz += pk.x * gy - pk.y * gx;
         }
         float* f = ws.jfm + p * 8;
         f[0] = Fx; f[1] = Fy; f[2] = Fz; f[3] = Mx; f[4] = My; f[5] = Mz;
@@ -420,11 +542,17 @@ __device__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, cons
         ws.jfm[p * 8 + 6] = gq;
     }
     __syncwarp();
-    // a DoF may drive several joints: lane d sums its joints in DFS order
+    // lane d writes DoF d: its joint's term, or, for a DoF that drives several
+    // joints, their sum in DFS order
     for (int d = lane; d < D; d += 32) {
+        const int who = cb.dof_joint[d];
         float acc = 0.0f;
-        for (int p = 1; p < NJ; ++p)
-            if (M.J[p].dof == d && M.J[p].type != PS_FIXED) acc += ws.jfm[p * 8 + 6];
+        if (who >= 0) {
+            acc = ws.jfm[who * 8 + 6];
+        } else if (who == -2) {
+            for (int p = 1; p < NJ; ++p)
+                if (M.J[p].dof == d && M.J[p].type != PS_FIXED) acc += ws.jfm[p * 8 + 6];
+        }
         grad_row[(size_t)d * gstride] = acc;
     }
     __syncwarp();

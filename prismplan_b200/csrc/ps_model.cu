@@ -211,6 +211,12 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
         jpairs.insert(jpairs.end(), {jk.first, jk.second, (int)k, (int)e});
         k = e;
     }
+    // repack as i | j << 9 | group << 18 (spheres < 512, groups < 16384)
+    for (size_t g = 0; g < jpairs.size() / 4; ++g)
+        for (int k = jpairs[4 * g + 2]; k < jpairs[4 * g + 3]; ++k) {
+            const uint32_t pr = gpairs[k];
+            gpairs[k] = (pr & 0x1ffu) | ((pr >> 16) & 0x1ffu) << 9 | (uint32_t)g << 18;
+        }
 
     bool shares = std::memcmp(aft, d->fixed_transforms, sizeof(float) * 16 * nj) == 0;
     for (int i = 0; i < nj && shares; ++i) shares = atypes[i] == d->joint_types[i];
