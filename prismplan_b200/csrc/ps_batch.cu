@@ -125,13 +125,13 @@ __global__ void __launch_bounds__(kWarps * 32, 24 / kWarps) batch_waypoint_kerne
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const CostWarpScratch ws =
-        cost_carve(cb.wbase + (size_t)warp * cost_warp_floats(NJ, NS, sv.n_obbs, true), NJ, NS, sc.n_obbs, true);
+        cost_carve(cb.wbase + (size_t)warp * cost_warp_floats(NJ, NS, sv.n_obbs, md.n_sruns, true), NJ, NS, sc.n_obbs, true);
     LaneStats st;
     st.zero();
     for (int k = blockIdx.x * kWarps + warp; k < n_wp; k += gridDim.x * kWarps) {
         if (lane < D) ws.q[lane] = q[(size_t)k * D + lane];
         __syncwarp();
-        const float c = waypoint_cost_warp<true>(M, md, sc, sv, P, cb, ws, grad + (size_t)k * D, 1, st);
+        const float c = waypoint_cost_warp<true, false>(M, md, sc, sv, P, cb, ws, grad + (size_t)k * D, 1, st);
         if (lane == 0) wp_cost[k] = c;
         __syncwarp();
     }

@@ -48,17 +48,17 @@ struct JointRec {
 };
 
 // Self pairs (global memory): packed (i | j << 16), reordered sphere indices.
-// gpairs holds the same pairs grouped by the DFS positions of their two
-// joints, packed (i | j << 9 | g << 18); jpairs[g] = (joint of i, joint of j,
-// first, end) indexes gpairs.
+// The same pairs as runs: sruns[r] = (i | q << 9 | len << 14, first) is
+// sphere i against the len spheres spairs[first..first+len) of joint q (DFS
+// position).
 // Limits (global memory): lower[n_dof], upper[n_dof].
 struct ModelDev {
     const unsigned char* blob;     // device
     const uint32_t* self_pairs;    // device
     const uint32_t* apx_self_pairs;// device
-    const uint32_t* gpairs;        // device, grouped self pairs
-    const int4* jpairs;            // device, joint-pair groups
-    int n_jpairs;
+    const uint2* sruns;            // device, self-pair runs
+    const uint16_t* spairs;        // device, second sphere of each run pair
+    int n_sruns;
     const float* lower;            // device
     const float* upper;            // device
     int* status;                   // device error latch

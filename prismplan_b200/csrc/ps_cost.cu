@@ -33,9 +33,9 @@ size_t cost_block_smem(const ps_model* m, const ps_scene_view* sv, bool grad) {
     return cost_block_bytes(m, sv, kCostWarps, grad);
 }
 
-// One warp per waypoint (see ps_costwarp.cuh). kGrad: also the adjoint.
-// Output layouts follow ps_cost_params.layout.
-template <bool kGrad>
+// One warp per waypoint (see ps_costwarp.cuh). kGrad: also the adjoint;
+// kStats: count executed work. Output layouts follow ps_cost_params.layout.
+template <bool kGrad, bool kStats>
 __global__ void __launch_bounds__(kCostWarps * 32, 3) waypoint_cost_kernel(
     ModelDev md, ps_scene_view sv, const float* __restrict__ q, int n_rows, int T, ps_cost_params P,
     float* __restrict__ wp_cost, int broadcast_d, float* __restrict__ traj_acc, float* __restrict__ grad,
@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(kCostWarps * 32, 3) waypoint_cost_kernel(
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const CostWarpScratch ws =
-        cost_carve(cb.wbase + (size_t)warp * cost_warp_floats(NJ, NS, sv.n_obbs, kGrad), NJ, NS, sc.n_obbs, kGrad);
+        cost_carve(cb.wbase + (size_t)warp * cost_warp_floats(NJ, NS, sv.n_obbs, md.n_sruns, kGrad), NJ, NS, sc.n_obbs, kGrad);
     const bool bdt = P.layout == PS_LAYOUT_BDT;
     const long long total = (long long)n_rows * T;
     LaneStats st;
@@ -75,9 +75,9 @@ __global__ void __launch_bounds__(kCostWarps * 32, 3) waypoint_cost_kernel(
             grow = bdt ? grad + ((size_t)b * D) * T + t : grad + ((size_t)b * T + t) * D;
             gstride = bdt ? T : 1;
         }
-        const float cost = waypoint_cost_warp<kGrad>(M, md, sc, sv, P, cb, ws, grow, gstride, st);
+        const float cost = waypoint_cost_warp<kGrad, kStats>(M, md, sc, sv, P, cb, ws, grow, gstride, st);
         if (lane == 0) {
-            st.v[ST_SAMPLES] += 1;
+            if (kStats) st.v[ST_SAMPLES] += 1;
             if (wp_cost) {
                 if (broadcast_d)
                     for (int d = 0; d < D; ++d) wp_cost[((size_t)b * D + d) * T + t] = cost;
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(kCostWarps * 32, 3) waypoint_cost_kernel(
         }
         __syncwarp();
     }
-    flush_stats(stats, st);
+    if (kStats) flush_stats(stats, st);
 }
 
 // Per trajectory: smoothness cost and its gradient added to grad (see
@@ -156,18 +156,20 @@ extern "C" int ps_traj_cost(const ps_model* m, const ps_scene_view* scene, const
     if (atomic_traj) PS_TRY_CUDA(cudaMemsetAsync(traj_cost, 0, sizeof(float) * B, s));
     if (grad) {
         const size_t smem = cost_block_smem(m, scene, true);
-        const int grid = cost_grid(waypoint_cost_kernel<true>, smem, total);
+        auto k = g_stats ? waypoint_cost_kernel<true, true> : waypoint_cost_kernel<true, false>;
+        const int grid = cost_grid(k, smem, total);
         if (grid < 0) return PS_EINVAL;
         mark_start(s);
-        waypoint_cost_kernel<true><<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
+        k<<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
                                                                     atomic_traj ? traj_cost : nullptr, grad, g_stats);
         mark_stop(s);
     } else {
         const size_t smem = cost_block_smem(m, scene, false);
-        const int grid = cost_grid(waypoint_cost_kernel<false>, smem, total);
+        auto k = g_stats ? waypoint_cost_kernel<false, true> : waypoint_cost_kernel<false, false>;
+        const int grid = cost_grid(k, smem, total);
         if (grid < 0) return PS_EINVAL;
         mark_start(s);
-        waypoint_cost_kernel<false><<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
+        k<<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
                                                                      atomic_traj ? traj_cost : nullptr, nullptr, g_stats);
         mark_stop(s);
     }
@@ -193,10 +195,11 @@ extern "C" int ps_rollout_costs(const ps_model* m, const ps_scene_view* scene, c
     cudaStream_t s = (cudaStream_t)stream;
     const long long total = (long long)n_rows * T;
     const size_t smem = cost_block_smem(m, scene, false);
-    const int grid = cost_grid(waypoint_cost_kernel<false>, smem, total);
+    auto k = g_stats ? waypoint_cost_kernel<false, true> : waypoint_cost_kernel<false, false>;
+    const int grid = cost_grid(k, smem, total);
     if (grid < 0) return PS_EINVAL;
     mark_start(s);
-    waypoint_cost_kernel<false><<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, rollouts, n_rows, T, *P, state_cost,
+    k<<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, rollouts, n_rows, T, *P, state_cost,
                                                                  broadcast_d, nullptr, nullptr, g_stats);
     mark_stop(s);
     PS_TRY_CUDA(cudaGetLastError());

@@ -47,17 +47,17 @@ struct CostWarpScratch {
     float4* pos;     // [NS]: centre (world), radius
     float* g;        // [NS][3]   (gradient only)
     float* jfm;      // [NJ][8]: F, M, dC/dq   (gradient only)
-    unsigned* jact;  // [8]       active joint-pair groups (one bit each)
     unsigned* mask;  // [NJ][nw]  candidate boxes per joint
+    uint16_t* alist; // [n_sruns] active self-pair runs
 };
 
 __host__ __device__ inline int cost_mask_words(int n_obbs) { return (n_obbs + 31) / 32; }
 
-__host__ __device__ inline size_t cost_warp_floats(int NJ, int NS, int n_obbs, bool grad) {
+__host__ __device__ inline size_t cost_warp_floats(int NJ, int NS, int n_obbs, int n_sruns, bool grad) {
     size_t f = 16 + (size_t)NJ * 12 + (size_t)NJ * 8 + (size_t)NS * 4;
     if (grad) f += (size_t)NS * 3 + (size_t)NJ * 8;
     f = (f + 3) & ~size_t(3);
-    f += 8 + (size_t)NJ * cost_mask_words(n_obbs);
+    f += (size_t)NJ * cost_mask_words(n_obbs) + ((size_t)n_sruns + 1) / 2;
     return (f + 3) & ~size_t(3);   // keep every warp's slice 16-byte aligned
 }
 
@@ -77,8 +77,8 @@ __device__ __forceinline__ CostWarpScratch cost_carve(float* base, int NJ, int N
         w.jfm = nullptr;
     }
     p = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
-    w.jact = reinterpret_cast<unsigned*>(p);
-    w.mask = w.jact + 8;
+    w.mask = reinterpret_cast<unsigned*>(p);
+    w.alist = reinterpret_cast<uint16_t*>(w.mask + NJ * cost_mask_words(n_obbs));
     return w;
 }
 
@@ -99,7 +99,7 @@ struct CostBlock {
 inline size_t cost_block_bytes(const ps_model* m, const ps_scene_view* sv, int warps, bool grad) {
     return (size_t)m->dev.bytes_core + scene_smem_bytes(sv) + (((size_t)m->info.n_spheres + 15) & ~size_t(15)) + 64 +
            (size_t)16 * std::max(sv->n_obbs, 1) +
-           (size_t)warps * cost_warp_floats(m->info.n_joints, m->info.n_spheres, sv->n_obbs, grad) * 4;
+           (size_t)warps * cost_warp_floats(m->info.n_joints, m->info.n_spheres, sv->n_obbs, m->dev.n_sruns, grad) * 4;
 }
 
 // Fills the block tables (every thread calls it; the caller syncs after).
@@ -244,9 +244,9 @@ __device__ __forceinline__ float warp_sum(float v) {
 
 // Cost (returned on every lane) and, with kGrad, d cost / d q written by
 // lanes d < n_dof to grad_row[d * gstride]. The whole warp calls it; the
-// configuration is ws.q[0..D).
-template <bool kGrad>
-__device__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, const SceneSmem& sc,
+// configuration is ws.q[0..D). kStats: count the executed work into st.
+template <bool kGrad, bool kStats>
+__device__ __forceinline__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, const SceneSmem& sc,
                                     const ps_scene_view& sv, const ps_cost_params& P, const CostBlock& cb,
                                     const CostWarpScratch& ws, float* grad_row, int gstride, LaneStats& st) {
     const int lane = threadIdx.x & 31;
@@ -308,7 +308,7 @@ __device__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, cons
             ws.bnd[lane * 2] = make_float4(cx, cy, cz, b.w);
             ws.bnd[lane * 2 + 1] = make_float4(thr, thr * thr, fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))), 0.0f);
         }
-        if (lane == 0) st.v[ST_JOINTS] += NJ;
+        if (kStats && lane == 0) st.v[ST_JOINTS] += NJ;
     }
     __syncwarp();
 
@@ -335,7 +335,7 @@ __device__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, cons
                         float qx, qy, qz;
                         keep = fast_box_dsq(sc.obbs[o], bc.x, bc.y, bc.z, qx, qy, qz) < th.y;
                     }
-                    st.v[ST_CULL] += 1;
+                    if (kStats) st.v[ST_CULL] += 1;
                 }
                 const unsigned bal = __ballot_sync(kCostFull, keep);
                 if (lane == 0) ws.mask[p * nw + (base >> 5)] = bal;
@@ -354,7 +354,7 @@ __device__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, cons
         float px, py, pz;
         sphere_world(T, sp.x, sp.y, sp.z, px, py, pz);
         ws.pos[k] = make_float4(px, py, pz, sp.w);
-        st.v[ST_SPHERES] += 1;
+        if (kStats) st.v[ST_SPHERES] += 1;
         const int so = M.SO[k];
         float gx = 0.f, gy = 0.f, gz = 0.f;
         if (nob > 0) {
@@ -375,7 +375,7 @@ __device__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, cons
                     }
                 }
             }
-            st.v[ST_PAIRS] += tests;
+            if (kStats) st.v[ST_PAIRS] += tests;
         }
         if (sc.n_layers) {
             const uint8_t* eacm = sv.sphere_acm_mask ? sv.sphere_acm_mask + (size_t)so * sv.n_voxel_layers : nullptr;
@@ -385,7 +385,7 @@ __device__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, cons
                 for (int l = 0; l < sc.n_layers; ++l) {
                     if (eacm && eacm[l] == 0) continue;
                     float d, dgx, dgy, dgz;
-                    st.v[ST_ESDF] += 1;
+                    if (kStats) st.v[ST_ESDF] += 1;
                     if (!esdf_sample_trilinear_grad(sc.layers[l], sv.voxel_features + (size_t)l * sv.max_voxels_per_layer,
                                                     sv.max_voxels_per_layer, px, py, pz, d, dgx, dgy, dgz))
                         continue;
@@ -407,7 +407,10 @@ __device__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, cons
                     }
                 }
             } else {
-                const float clr = sphere_esdf_clearance(sc, sv, px, py, pz, sp.w, eacm, st);
+                LaneStats est;
+                est.zero();
+                const float clr = sphere_esdf_clearance(sc, sv, px, py, pz, sp.w, eacm, est);
+                if (kStats) st.v[ST_ESDF] += est.v[ST_ESDF];
                 esdf_part += fmaxf(0.0f, wm - clr);
                 // the nearest-voxel lookup is piecewise constant: zero gradient
             }
@@ -420,49 +423,54 @@ __device__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, cons
     }
     __syncwarp();
 
-    // ---- 4. self hinge: joint-pair prefilter, then sphere pairs whose
-    //      squared distance is inside (r_i + r_j + m_self)^2 ----
+    // ---- 4. self hinge. A run (sphere i against the spheres of joint q) can
+    //      hold a pair with |p_i - p_j| - r_i - r_j < m_self only if
+    //      |p_i - c_q| < r_i + R_q + m_self: lanes test the runs, ballot-
+    //      compact the active ones, then each lane walks whole active runs. ----
     float self_h = 0.0f;
-    int self_arg = -1;
-    if (P.include_self && md.n_jpairs > 0) {
-        float bv = 3.0e38f;
-        int bk = 0x7fffffff;
+    int self_i = -1, self_j = -1;
+    if (P.include_self && md.n_sruns > 0) {
         const float smp = fmaxf(smg, 0.0f);
-        for (int base = 0; base < md.n_jpairs; base += 32) {
-            const int gi = base + lane;
+        int n_act = 0;
+        for (int base = 0; base < md.n_sruns; base += 32) {
+            const int r = base + lane;
             bool act = false;
-            if (gi < md.n_jpairs) {
-                const int4 jp = __ldg(md.jpairs + gi);
-                const float4 A = ws.bnd[jp.x * 2], B = ws.bnd[jp.y * 2];
-                const float dx = A.x - B.x, dy = A.y - B.y, dz = A.z - B.z;
-                const float S = fmaxf(fmaxf(fabsf(A.x), fabsf(A.y)), fmaxf(fabsf(A.z), fmaxf(fabsf(B.x),
-                                fmaxf(fabsf(B.y), fabsf(B.z)))));
-                float thr = A.w + B.w + smp;
+            if (r < md.n_sruns) {
+                const uint2 run = __ldg(md.sruns + r);
+                const float4 a = ws.pos[run.x & 0x1ffu];
+                const float4 c = ws.bnd[((run.x >> 9) & 31u) * 2];
+                const float dx = a.x - c.x, dy = a.y - c.y, dz = a.z - c.z;
+                const float S = fmaxf(fmaxf(fabsf(a.x), fabsf(a.y)), fmaxf(fabsf(a.z), fmaxf(fabsf(c.x),
+                                fmaxf(fabsf(c.y), fabsf(c.z)))));
+                float thr = a.w + c.w + smp;
                 thr += 4.0f * (S + thr + 1.0f) * PS_GUARD_K;
                 act = fmaf(dz, dz, fmaf(dy, dy, dx * dx)) < thr * thr;
-                st.v[ST_SELF] += 1;
+                if (kStats) st.v[ST_SELF] += 1;
             }
             const unsigned bal = __ballot_sync(kCostFull, act);
-            if (lane == 0) ws.jact[base >> 5] = bal;
+            if (act) ws.alist[n_act + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)r;
+            n_act += __popc(bal);
         }
         __syncwarp();
-        // every pair, in gpairs order; pairs of inactive groups are skipped
-        const int n_pairs = M.H->n_self_pairs;
-        for (int k = lane; k < n_pairs; k += 32) {
-            const uint32_t pr = __ldg(md.gpairs + k);
-            const uint32_t g = pr >> 18;
-            if (!((ws.jact[g >> 5] >> (g & 31)) & 1u)) continue;
-            const float4 a = ws.pos[pr & 0x1ffu], b = ws.pos[(pr >> 9) & 0x1ffu];
-            const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
-            const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-            const float rs = a.w + b.w;
-            const float lim = (rs + smp) * (1.0f + 1.0e-5f) + 1.0e-6f;
-            st.v[ST_SELF] += 1;
-            if (d2 < lim * lim) {
-                const float c = sqrtf(d2) - rs;
-                if (c < bv || (c == bv && k < bk)) {
+        float bv = 3.0e38f;
+        int bk = 0x7fffffff, bi = -1, bj = -1;
+        for (int t = lane; t < n_act; t += 32) {
+            const uint2 run = __ldg(md.sruns + ws.alist[t]);
+            const int i = run.x & 0x1ffu, len = (run.x >> 14) & 0x1ffu;
+            const float4 a = ws.pos[i];
+            for (int u = 0; u < len; ++u) {
+                const int k = (int)run.y + u;
+                const int j = __ldg(md.spairs + k);
+                const float4 b = ws.pos[j];
+                const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+                const float d2 = fmaxf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)), 1.0e-30f);
+                const float c = d2 * rsqrtf(d2) - (a.w + b.w);
+                if (kStats) st.v[ST_SELF] += 1;
+                if (c < bv) {   // k increases along a lane: the first minimum wins ties
                     bv = c;
                     bk = k;
+                    bi = i;
+                    bj = j;
                 }
             }
         }
@@ -470,21 +478,27 @@ __device__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, cons
         for (int o = 16; o > 0; o >>= 1) {
             const float ov = __shfl_xor_sync(kCostFull, bv, o);
             const int ok = __shfl_xor_sync(kCostFull, bk, o);
+            const int oi = __shfl_xor_sync(kCostFull, bi, o);
+            const int oj = __shfl_xor_sync(kCostFull, bj, o);
             if (ov < bv || (ov == bv && ok < bk)) {
                 bv = ov;
                 bk = ok;
+                bi = oi;
+                bj = oj;
             }
         }
         self_h = fmaxf(0.0f, smg - bv);
-        self_arg = self_h > 0.0f ? bk : -1;
+        if (self_h > 0.0f) {
+            self_i = bi;
+            self_j = bj;
+        }
     }
     const float cost = w * (warp_sum(esdf_part) + warp_sum(obb_part) + self_h);
     if (!kGrad) return cost;
 
     // ---- 5. adjoint ----
-    if (self_arg >= 0 && lane == 0) {
-        const uint32_t pr = __ldg(md.gpairs + self_arg);
-        const int i = pr & 0x1ffu, j = (pr >> 9) & 0x1ffu;
+    if (self_i >= 0 && lane == 0) {
+        const int i = self_i, j = self_j;
         const float4 a = ws.pos[i], b = ws.pos[j];
         const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
         const float dd = sqrtf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)));

@@ -192,31 +192,33 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
         if (rc) return rc;
     }
 
-    // Self pairs grouped by joint pair (for the bound-sphere prefilter of the
-    // cost kernels); stable within a group.
+    // Self pairs as runs for the cost kernels' prefilter: a run is one sphere
+    // i against the spheres of one joint q, pairs sorted by (i, q, j).
+    // sruns[r] = (i | q << 9 | len << 14, first); spairs[k] = j.
     std::vector<int> sph_pos(std::max(ns, 1), 0);
     for (int p = 0; p < nj; ++p)
         for (int k = sbeg[p]; k < send[p]; ++k) sph_pos[k] = p;
-    std::vector<uint32_t> gpairs(pairs);
-    auto jkey = [&](uint32_t pr) {
-        const int a = sph_pos[pr & 0xffff], b = sph_pos[pr >> 16];
-        return std::make_pair(std::min(a, b), std::max(a, b));
-    };
-    std::stable_sort(gpairs.begin(), gpairs.end(), [&](uint32_t x, uint32_t y) { return jkey(x) < jkey(y); });
-    std::vector<int> jpairs;   // 4 ints per group
-    for (size_t k = 0; k < gpairs.size();) {
+    std::vector<uint32_t> opairs(pairs);
+    std::stable_sort(opairs.begin(), opairs.end(), [&](uint32_t x, uint32_t y) {
+        const int xi = x & 0xffff, xj = x >> 16, yi = y & 0xffff, yj = y >> 16;
+        if (xi != yi) return xi < yi;
+        if (sph_pos[xj] != sph_pos[yj]) return sph_pos[xj] < sph_pos[yj];
+        return xj < yj;
+    });
+    std::vector<uint32_t> sruns;   // 2 words per run
+    std::vector<uint16_t> spairs(opairs.size());
+    for (size_t k = 0; k < opairs.size();) {
+        const int i = opairs[k] & 0xffff, q = sph_pos[opairs[k] >> 16];
         size_t e = k;
-        while (e < gpairs.size() && jkey(gpairs[e]) == jkey(gpairs[k])) ++e;
-        const auto jk = jkey(gpairs[k]);
-        jpairs.insert(jpairs.end(), {jk.first, jk.second, (int)k, (int)e});
+        while (e < opairs.size() && (int)(opairs[e] & 0xffff) == i && sph_pos[opairs[e] >> 16] == q && e - k < 511) {
+            spairs[e] = (uint16_t)(opairs[e] >> 16);
+            ++e;
+        }
+        sruns.push_back((uint32_t)i | (uint32_t)q << 9 | (uint32_t)(e - k) << 14);
+        sruns.push_back((uint32_t)k);
         k = e;
     }
-    // repack as i | j << 9 | group << 18 (spheres < 512, groups < 16384)
-    for (size_t g = 0; g < jpairs.size() / 4; ++g)
-        for (int k = jpairs[4 * g + 2]; k < jpairs[4 * g + 3]; ++k) {
-            const uint32_t pr = gpairs[k];
-            gpairs[k] = (pr & 0x1ffu) | ((pr >> 16) & 0x1ffu) << 9 | (uint32_t)g << 18;
-        }
+    if (sruns.size() / 2 > 65535) return set_error(PS_EINVAL, "too many self-pair runs");
 
     bool shares = std::memcmp(aft, d->fixed_transforms, sizeof(float) * 16 * nj) == 0;
     for (int i = 0; i < nj && shares; ++i) shares = atypes[i] == d->joint_types[i];
@@ -241,10 +243,10 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
     off += align16(sizeof(uint32_t) * std::max<size_t>(pairs.size(), 1));
     const size_t off_apairs = off;
     off += align16(sizeof(uint32_t) * std::max<size_t>(apairs.size(), 1));
-    const size_t off_gpairs = off;
-    off += align16(sizeof(uint32_t) * std::max<size_t>(gpairs.size(), 1));
-    const size_t off_jpairs = off;
-    off += align16(sizeof(int) * std::max<size_t>(jpairs.size(), 4));
+    const size_t off_sruns = off;
+    off += align16(sizeof(uint32_t) * std::max<size_t>(sruns.size(), 2));
+    const size_t off_spairs = off;
+    off += align16(sizeof(uint16_t) * std::max<size_t>(spairs.size(), 1));
     const size_t off_lower = off;
     off += align16(sizeof(float) * nd);
     const size_t off_upper = off;
@@ -325,8 +327,8 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
     }
     if (!pairs.empty()) std::memcpy(host.data() + off_pairs, pairs.data(), pairs.size() * 4);
     if (!apairs.empty()) std::memcpy(host.data() + off_apairs, apairs.data(), apairs.size() * 4);
-    if (!gpairs.empty()) std::memcpy(host.data() + off_gpairs, gpairs.data(), gpairs.size() * 4);
-    if (!jpairs.empty()) std::memcpy(host.data() + off_jpairs, jpairs.data(), jpairs.size() * 4);
+    if (!sruns.empty()) std::memcpy(host.data() + off_sruns, sruns.data(), sruns.size() * 4);
+    if (!spairs.empty()) std::memcpy(host.data() + off_spairs, spairs.data(), spairs.size() * 2);
     std::memcpy(host.data() + off_lower, d->joint_lower, sizeof(float) * nd);
     std::memcpy(host.data() + off_upper, d->joint_upper, sizeof(float) * nd);
 
@@ -347,9 +349,9 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
     m->dev.blob = base;
     m->dev.self_pairs = reinterpret_cast<const uint32_t*>(base + off_pairs);
     m->dev.apx_self_pairs = reinterpret_cast<const uint32_t*>(base + off_apairs);
-    m->dev.gpairs = reinterpret_cast<const uint32_t*>(base + off_gpairs);
-    m->dev.jpairs = reinterpret_cast<const int4*>(base + off_jpairs);
-    m->dev.n_jpairs = (int)(jpairs.size() / 4);
+    m->dev.sruns = reinterpret_cast<const uint2*>(base + off_sruns);
+    m->dev.spairs = reinterpret_cast<const uint16_t*>(base + off_spairs);
+    m->dev.n_sruns = (int)(sruns.size() / 2);
     m->dev.lower = reinterpret_cast<const float*>(base + off_lower);
     m->dev.upper = reinterpret_cast<const float*>(base + off_upper);
     m->dev.status = reinterpret_cast<int*>(base + off_status);
