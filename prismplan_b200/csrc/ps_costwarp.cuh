@@ -132,15 +132,7 @@ __device__ __forceinline__ CostBlock cost_block_setup(unsigned char* at, const M
             if (M.J[p].dof == d && M.J[p].type != PS_FIXED) who = who == -1 ? p : -2;
         dj[d] = (signed char)who;
     }
-    for (int o = threadIdx.x; o < sc.n_obbs; o += blockDim.x) {
-        const ObbPrep& b = sc.obbs[o];
-        // local = R p + t  =>  centre p = -R^T t
-        const float cx = -(b.r0.x * b.r0.w + b.r1.x * b.r1.w + b.r2.x * b.r2.w);
-        const float cy = -(b.r0.y * b.r0.w + b.r1.y * b.r1.w + b.r2.y * b.r2.w);
-        const float cz = -(b.r0.z * b.r0.w + b.r1.z * b.r1.w + b.r2.z * b.r2.w);
-        const float r = sqrtf(b.h.x * b.h.x + b.h.y * b.h.y + b.h.z * b.h.z);
-        obs[o] = make_float4(cx, cy, cz, r);
-    }
+    box_spheres(sc, obs);
     return cb;
 }
 

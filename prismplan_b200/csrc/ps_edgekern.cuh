@@ -19,8 +19,27 @@ constexpr unsigned kFull = 0xffffffffu;
 
 struct EdgeWs {                         // header of the persistent workspace (64 B)
     unsigned long long head;            // next chunk-major item
-    int max_G;
+    int max_rounds;                     // most chunk rounds of any edge
     int pad[13];
+};
+
+// Chunk visiting order of an edge with nc chunks of 32 samples: with
+// s = ceil(sqrt(nc)) and m = ceil(nc / s), round k visits chunk
+// (k % m) * s + k / m, so the first rounds spread over the whole edge and a
+// colliding stretch is found, and the edge retired, after fewer chunks than
+// in order. Rounds whose chunk is >= nc are empty. The verdict is the OR over
+// all samples, so the order changes only the work, never the result.
+struct ChunkOrder {
+    int nc, s, m;
+    __device__ __forceinline__ explicit ChunkOrder(int G) {
+        nc = G > 0 ? (G + 31) / 32 : 0;
+        s = nc > 0 ? (int)ceilf(sqrtf((float)nc)) : 1;
+        while (s > 1 && (s - 1) * (s - 1) >= nc) --s;   // exact integer ceil(sqrt)
+        while (s * s < nc) ++s;
+        m = nc > 0 ? (nc + s - 1) / s : 0;
+    }
+    __device__ __forceinline__ int rounds() const { return m * s; }
+    __device__ __forceinline__ int chunk(int k) const { return (k % m) * s + k / m; }
 };
 
 __device__ __forceinline__ int ordered_float(float f) {
@@ -59,6 +78,7 @@ __device__ __forceinline__ float edge_length(const float* a, const float* b, int
 struct WarpScratch {
     float* q;          // [32 * D]
     uint16_t* cand;    // [n_obbs]
+    const float4* obs; // [n_obbs] box centre and circumscribed radius (block-wide)
 };
 
 // One chunk of one edge. Returns true if any sample of the chunk collides.
@@ -308,23 +328,15 @@ __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, cons
             if (kStats) st.v[ST_JOINTS] += 1;
         }
         if (jr.bound.w < 0.0f || (sc.n_obbs == 0 && !kEsdf)) continue;   // nothing to test (uniform)
-        // ---- warp broad phase ----
+        // ---- warp broad phase: one sphere around the joint's bound spheres of
+        //      all 32 samples, centred on the middle sample's ----
         float cx, cy, cz;
         sphere_world(T, jr.bound.x, jr.bound.y, jr.bound.z, cx, cy, cz);
-        float mx = cx, my = cy, mz = cz;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            mx += __shfl_xor_sync(kFull, mx, o);
-            my += __shfl_xor_sync(kFull, my, o);
-            mz += __shfl_xor_sync(kFull, mz, o);
-        }
-        mx *= (1.0f / 32.0f);
-        my *= (1.0f / 32.0f);
-        mz *= (1.0f / 32.0f);
+        const float mx = __shfl_sync(kFull, cx, 16), my = __shfl_sync(kFull, cy, 16),
+                    mz = __shfl_sync(kFull, cz, 16);
         const float dx = cx - mx, dy = cy - my, dz = cz - mz;
-        float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) r2 = fmaxf(r2, __shfl_xor_sync(kFull, r2, o));
+        // max over lanes in one warp reduction: non-negative floats order as their bits
+        const float r2 = __uint_as_float(__reduce_max_sync(kFull, __float_as_uint(fmaf(dz, dz, fmaf(dy, dy, dx * dx)))));
         const float Sm = fmaxf(fabsf(mx), fmaxf(fabsf(my), fabsf(mz)));
         float Rc = sqrtf(r2) + jr.bound.w + fmaxf(margin, 0.0f);
         Rc += 4.0f * (Sm + Rc + sc.Bmax + 1.0f) * PS_GUARD_K;
@@ -335,8 +347,15 @@ __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, cons
             const int o = base + lane;
             bool keep = false;
             if (o < sc.n_obbs) {
-                float qx, qy, qz;
-                keep = fast_box_dsq(sc.obbs[o], mx, my, mz, qx, qy, qz) < Rc2;
+                // circumscribed-sphere test first, the box distance only if it passes
+                const float4 ob = ws.obs[o];
+                const float ex = ob.x - mx, ey = ob.y - my, ez = ob.z - mz;
+                float lim = Rc + ob.w;
+                lim += 4.0f * (Sm + fmaxf(fabsf(ob.x), fmaxf(fabsf(ob.y), fabsf(ob.z))) + lim + 1.0f) * PS_GUARD_K;
+                if (fmaf(ez, ez, fmaf(ey, ey, ex * ex)) < lim * lim) {
+                    float qx, qy, qz;
+                    keep = fast_box_dsq(sc.obbs[o], mx, my, mz, qx, qy, qz) < Rc2;
+                }
                 if (kStats) st.v[ST_CULL] += 1;
             }
             const unsigned bal = __ballot_sync(kFull, keep);
@@ -348,21 +367,14 @@ __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, cons
         // Per-joint guard: every sphere of the joint lies within bound.w of c.
         const float S = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))) + jr.bound.w;
         const float g = (S + sc.Bmax + 1.0f) * PS_GUARD_K;
-        // ---- approximate gate ----
-        bool flagged = false;
-        for (int k = jr.apx_beg; k < jr.apx_end && !flagged; ++k) {
-            const float4 sa = M.A[k];
-            float px, py, pz;
-            sphere_world(T, sa.x, sa.y, sa.z, px, py, pz);
-            const float sr = __fadd_rn(sa.w, margin);
-            if (kStats) st.v[ST_SPHERES] += 1;
-            flagged = spheres_hit<1, kStats>(sc, ws.cand, ncand, &px, &py, &pz, &sr, g, st) ||
-                      (kEsdf && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
-        }
-        // ---- exact spheres of a flagged joint: 4 at a time, then singles ----
-        if (flagged && !hit) {
+        // ---- exact spheres (4 at a time, then singles), then the approximate
+        //      gate of a lane whose exact spheres hit: the verdict of the joint
+        //      is gate && exact (two_phase_cc.cuh:57-138), evaluated in the
+        //      order that skips the gate for every lane without an exact hit ----
+        if (!hit) {
+            bool ex = false;
             int k = jr.sph_beg;
-            for (; k + 4 <= jr.sph_end && !hit; k += 4) {
+            for (; k + 4 <= jr.sph_end && !ex; k += 4) {
                 float px[4], py[4], pz[4], sr[4];
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
@@ -371,21 +383,32 @@ __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, cons
                     sr[i] = __fadd_rn(sp.w, margin);
                 }
                 if (kStats) st.v[ST_SPHERES] += 4;
-                hit = spheres_hit<4, kStats>(sc, ws.cand, ncand, px, py, pz, sr, g, st);
+                ex = spheres_hit<4, kStats>(sc, ws.cand, ncand, px, py, pz, sr, g, st);
                 if (kEsdf)
 #pragma unroll
                     for (int i = 0; i < 4; ++i)
-                        if (!hit) hit = sphere_esdf_any(sc, sv, px[i], py[i], pz[i], sr[i], nullptr, st);
+                        if (!ex) ex = sphere_esdf_any(sc, sv, px[i], py[i], pz[i], sr[i], nullptr, st);
             }
-            for (; k < jr.sph_end && !hit; ++k) {
+            for (; k < jr.sph_end && !ex; ++k) {
                 const float4 sp = M.S[k];
                 float px, py, pz;
                 sphere_world(T, sp.x, sp.y, sp.z, px, py, pz);
                 const float sr = __fadd_rn(sp.w, margin);
                 if (kStats) st.v[ST_SPHERES] += 1;
-                hit = spheres_hit<1, kStats>(sc, ws.cand, ncand, &px, &py, &pz, &sr, g, st) ||
-                      (kEsdf && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
+                ex = spheres_hit<1, kStats>(sc, ws.cand, ncand, &px, &py, &pz, &sr, g, st) ||
+                     (kEsdf && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
             }
+            bool flagged = false;
+            for (int a = jr.apx_beg; ex && a < jr.apx_end && !flagged; ++a) {
+                const float4 sa = M.A[a];
+                float px, py, pz;
+                sphere_world(T, sa.x, sa.y, sa.z, px, py, pz);
+                const float sr = __fadd_rn(sa.w, margin);
+                if (kStats) st.v[ST_SPHERES] += 1;
+                flagged = spheres_hit<1, kStats>(sc, ws.cand, ncand, &px, &py, &pz, &sr, g, st) ||
+                          (kEsdf && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
+            }
+            hit = ex && flagged;
         }
         if (__any_sync(kFull, hit && real)) break;   // warp-uniform early exit
     }
@@ -402,6 +425,7 @@ struct EdgeSmem {
     LayerPrep* layers;
     float* q;          // [kWarps][32*D]
     uint16_t* cand;    // [kWarps][n_obbs_pad]
+    float4* obs;       // [n_obbs]
 };
 
 __device__ __forceinline__ EdgeSmem carve(unsigned char* smem, const ModelDev& md, const ps_scene_view& sv, int D) {
@@ -413,13 +437,15 @@ __device__ __forceinline__ EdgeSmem carve(unsigned char* smem, const ModelDev& m
     s.layers = reinterpret_cast<LayerPrep*>(s.orig + ((nob + 3) & ~3));
     s.q = reinterpret_cast<float*>(s.layers + PS_MAX_LAYERS);
     s.cand = reinterpret_cast<uint16_t*>(s.q + kWarps * 32 * D);
+    const int nob_pad = (nob + 7) & ~7;
+    s.obs = reinterpret_cast<float4*>(s.cand + kWarps * nob_pad);
     return s;
 }
 
 size_t edge_smem_bytes(const ps_model* m, const ps_scene_view* sv) {
     const int nob_pad = (std::max(sv->n_obbs, 1) + 7) & ~7;
     return (size_t)m->dev.bytes_core + scene_smem_bytes(sv) + (size_t)kWarps * 32 * m->info.n_dof * 4 +
-           (size_t)kWarps * nob_pad * 2 + 64;
+           (size_t)kWarps * nob_pad * 2 + (size_t)16 * std::max(sv->n_obbs, 1) + 64;
 }
 
 // ---------------------------------------------------------------------------
@@ -443,9 +469,11 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_plain_kerne
     EdgeSmem es = carve(smem, md, sv, D);
     SceneSmem sc;
     stage_scene(sv, es.obbs, es.orig, es.layers, counters, &bmax, sc);
+    box_spheres(sc, es.obs);
+    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nob_pad = (max(sv.n_obbs, 1) + 7) & ~7;
-    WarpScratch ws{es.q + warp * 32 * D, es.cand + warp * nob_pad};
+    WarpScratch ws{es.q + warp * 32 * D, es.cand + warp * nob_pad, es.obs};
     LaneStats st;
     st.zero();
     for (int e = blockIdx.x * kWarps + warp; e < n_edges; e += gridDim.x * kWarps) {
@@ -455,8 +483,10 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_plain_kerne
         const int G = edge_samples(P, given, e, a, b, D, len);
         bool bad = false;
         float emin = FLT_MAX;
-        const int chunks = G > 0 ? (G + 31) / 32 : 0;
-        for (int c = 0; c < chunks; ++c) {
+        const ChunkOrder ord(G);
+        for (int r = 0; r < ord.rounds(); ++r) {
+            const int c = ord.chunk(r);
+            if (c >= ord.nc) continue;
             float cm = FLT_MAX;
             if (kMode) bad |= process_chunk_fast<kStats, kMode == 2>(M, sc, sv, P, from, to, e, G, c, ws, st);
             else bad |= process_chunk(M, sc, sv, P, from, to, e, G, c, ws, P.compute_clearance ? &cm : nullptr, st);
@@ -491,11 +521,11 @@ __global__ void edges_prep_kernel(ps_edge_params P, const float* __restrict__ fr
         len_out[e] = len;
         bad[e] = 0;
         clr[e] = ordered_float(FLT_MAX);
-        local_max = max(local_max, G);
+        local_max = max(local_max, ChunkOrder(G).rounds());
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) local_max = max(local_max, __shfl_xor_sync(kFull, local_max, o));
-    if ((threadIdx.x & 31) == 0 && local_max > 0) atomicMax(&hdr->max_G, local_max);
+    if ((threadIdx.x & 31) == 0 && local_max > 0) atomicMax(&hdr->max_rounds, local_max);
 }
 
 template <int kMode, bool kStats>
@@ -516,13 +546,14 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_queue_kerne
     EdgeSmem es = carve(smem, md, sv, D);
     SceneSmem sc;
     stage_scene(sv, es.obbs, es.orig, es.layers, counters, &bmax, sc);
+    box_spheres(sc, es.obs);
+    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nob_pad = (max(sv.n_obbs, 1) + 7) & ~7;
-    WarpScratch ws{es.q + warp * 32 * D, es.cand + warp * nob_pad};
+    WarpScratch ws{es.q + warp * 32 * D, es.cand + warp * nob_pad, es.obs};
     LaneStats st;
     st.zero();
-    const int max_G = *((volatile int*)&hdr->max_G);
-    const long long rounds = (max_G + 31) / 32;
+    const long long rounds = *((volatile int*)&hdr->max_rounds);
     const long long total = rounds * (long long)n_edges;   // chunk-major item space
     volatile int* vbad = bad;
     for (;;) {
@@ -543,7 +574,11 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_queue_kerne
                 e = (int)(item - (long long)k * n_edges);
             }
             G = __ldg(Gs + e);
-            live = (k * 32 < G) && vbad[e] == 0;
+            const ChunkOrder ord(G);
+            if (k < ord.rounds()) {
+                k = ord.chunk(k);   // round -> chunk index
+                live = k < ord.nc && vbad[e] == 0;
+            }
         }
         unsigned todo = __ballot_sync(kFull, live);
         while (todo) {

@@ -48,6 +48,18 @@ __device__ __forceinline__ void flush_stats(unsigned long long* stats, LaneStats
     }
 }
 
+// World centre and circumscribed radius of each staged box (local = R p + t,
+// so the centre is -R^T t). Every thread of the block calls it.
+__device__ __forceinline__ void box_spheres(const SceneSmem& sc, float4* obs) {
+    for (int o = threadIdx.x; o < sc.n_obbs; o += blockDim.x) {
+        const ObbPrep& b = sc.obbs[o];
+        const float cx = -(b.r0.x * b.r0.w + b.r1.x * b.r1.w + b.r2.x * b.r2.w);
+        const float cy = -(b.r0.y * b.r0.w + b.r1.y * b.r1.w + b.r2.y * b.r2.w);
+        const float cz = -(b.r0.z * b.r0.w + b.r1.z * b.r1.w + b.r2.z * b.r2.w);
+        obs[o] = make_float4(cx, cy, cz, sqrtf(b.h.x * b.h.x + b.h.y * b.h.y + b.h.z * b.h.z));
+    }
+}
+
 // Shared-memory view of the staged model core.
 struct ModelSmem {
     const BlobHeader* H;
