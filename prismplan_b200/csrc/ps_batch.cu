@@ -208,7 +208,7 @@ namespace {
 struct LaunchPlan {
     int mode = 0;
     void (*qk)(ModelDev, ps_scene_view, ps_edge_params, const float*, const float*, int, EdgeWs*, const int*, int*,
-               int*, unsigned long long*, const int*) = nullptr;
+               int*, unsigned long long*, int, const int*) = nullptr;
     size_t qsmem = 0, wsmem = 0, fsmem = 0;
     int qgrid = 1, wgrid = 1, req_grid_e = 1, req_grid_t = 1, pgrid = 1;
 };
@@ -274,7 +274,9 @@ void record_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep
         edges_prep_kernel<<<L.pgrid, 256, 0, s0>>>(*ep, b->d_from, b->d_to, b->d_given, b->lim.max_edges, D, b->d_hdr,
                                                    b->d_G, b->d_len, b->d_bad, b->d_clr, n_dev);
         L.qk<<<L.qgrid, kEdgeThreads, L.qsmem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to, b->lim.max_edges, b->d_hdr,
-                                                    b->d_G, b->d_bad, b->d_clr, nullptr, n_dev);
+                                                    b->d_G, b->d_bad, b->d_clr, nullptr, 0, n_dev);
+        L.qk<<<L.qgrid, kEdgeThreads, L.qsmem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to, b->lim.max_edges, b->d_hdr,
+                                                    b->d_G, b->d_bad, b->d_clr, nullptr, 1, n_dev);
         edges_finalize_kernel<<<L.pgrid, 256, 0, s0>>>(b->lim.max_edges, *ep, b->d_bad, b->d_len, b->d_clr,
                                                        b->d_valid, b->d_cost, nullptr, n_dev);
         batch_scatter_edges<<<L.req_grid_e, 128, 0, s0>>>(b->d_ereq, b->d_cnt, b->d_valid, b->d_cost);

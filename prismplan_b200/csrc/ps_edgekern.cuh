@@ -18,9 +18,9 @@ constexpr int kEdgeThreads = 32 * kWarps;
 constexpr unsigned kFull = 0xffffffffu;
 
 struct EdgeWs {                         // header of the persistent workspace (64 B)
-    unsigned long long head;            // next chunk-major item
+    unsigned long long head[2];         // next chunk-major item of each pass
     int max_rounds;                     // most chunk rounds of any edge
-    int pad[13];
+    int pad[11];
 };
 
 // Chunk visiting order of an edge with nc chunks of 32 samples: with
@@ -281,6 +281,25 @@ __device__ __forceinline__ bool spheres_hit(const SceneSmem& sc, const uint16_t*
     return hit;
 }
 
+// Approximate gate of one joint for this lane: any approximate sphere hits a
+// candidate box (or an ESDF layer).
+template <bool kStats, bool kEsdf>
+__device__ __forceinline__ bool joint_gate(const ModelSmem& M, const SceneSmem& sc, const ps_scene_view& sv,
+                                           const JointRec& jr, const Affine& T, float margin, const WarpScratch& ws,
+                                           int ncand, float g, LaneStats& st) {
+    bool flagged = false;
+    for (int a = jr.apx_beg; a < jr.apx_end && !flagged; ++a) {
+        const float4 sa = M.A[a];
+        float px, py, pz;
+        sphere_world(T, sa.x, sa.y, sa.z, px, py, pz);
+        const float sr = __fadd_rn(sa.w, margin);
+        if (kStats) st.v[ST_SPHERES] += 1;
+        flagged = spheres_hit<1, kStats>(sc, ws.cand, ncand, &px, &py, &pz, &sr, g, st) ||
+                  (kEsdf && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
+    }
+    return flagged;
+}
+
 template <bool kStats, bool kEsdf>
 __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, const ps_scene_view& sv,
                                    const ps_edge_params& P,
@@ -363,51 +382,49 @@ __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, cons
             ncand += __popc(bal);
         }
         __syncwarp();
-        if (ncand == 0 && !kEsdf) continue;   // nothing reachable from any lane (uniform)
+        // ESDF layers within reach of any sphere of the joint over the chunk (uniform)
+        const bool esdf = kEsdf && esdf_reachable(sc, mx, my, mz, Rc);
+        if (ncand == 0 && !esdf) continue;   // nothing reachable from any lane (uniform)
         // Per-joint guard: every sphere of the joint lies within bound.w of c.
         const float S = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))) + jr.bound.w;
         const float g = (S + sc.Bmax + 1.0f) * PS_GUARD_K;
-        // ---- exact spheres (4 at a time, then singles), then the approximate
-        //      gate of a lane whose exact spheres hit: the verdict of the joint
-        //      is gate && exact (two_phase_cc.cuh:57-138), evaluated in the
-        //      order that skips the gate for every lane without an exact hit ----
+        // ---- the joint's verdict is gate && exact (two_phase_cc.cuh:57-138).
+        //      Boxes only: exact spheres first, the approximate gate only for a
+        //      lane whose exact spheres hit. With an ESDF layer in reach the
+        //      gate comes first, so unflagged joints skip the exact spheres'
+        //      ESDF lookups. ----
         if (!hit) {
-            bool ex = false;
-            int k = jr.sph_beg;
-            for (; k + 4 <= jr.sph_end && !ex; k += 4) {
-                float px[4], py[4], pz[4], sr[4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const float4 sp = M.S[k + i];
-                    sphere_world(T, sp.x, sp.y, sp.z, px[i], py[i], pz[i]);
-                    sr[i] = __fadd_rn(sp.w, margin);
-                }
-                if (kStats) st.v[ST_SPHERES] += 4;
-                ex = spheres_hit<4, kStats>(sc, ws.cand, ncand, px, py, pz, sr, g, st);
-                if (kEsdf)
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-                        if (!ex) ex = sphere_esdf_any(sc, sv, px[i], py[i], pz[i], sr[i], nullptr, st);
-            }
-            for (; k < jr.sph_end && !ex; ++k) {
-                const float4 sp = M.S[k];
-                float px, py, pz;
-                sphere_world(T, sp.x, sp.y, sp.z, px, py, pz);
-                const float sr = __fadd_rn(sp.w, margin);
-                if (kStats) st.v[ST_SPHERES] += 1;
-                ex = spheres_hit<1, kStats>(sc, ws.cand, ncand, &px, &py, &pz, &sr, g, st) ||
-                     (kEsdf && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
-            }
             bool flagged = false;
-            for (int a = jr.apx_beg; ex && a < jr.apx_end && !flagged; ++a) {
-                const float4 sa = M.A[a];
-                float px, py, pz;
-                sphere_world(T, sa.x, sa.y, sa.z, px, py, pz);
-                const float sr = __fadd_rn(sa.w, margin);
-                if (kStats) st.v[ST_SPHERES] += 1;
-                flagged = spheres_hit<1, kStats>(sc, ws.cand, ncand, &px, &py, &pz, &sr, g, st) ||
-                          (kEsdf && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
+            if (esdf) flagged = joint_gate<kStats, true>(M, sc, sv, jr, T, margin, ws, ncand, g, st);
+            bool ex = false;
+            if (!esdf || flagged) {
+                int k = jr.sph_beg;
+                for (; k + 4 <= jr.sph_end && !ex; k += 4) {
+                    float px[4], py[4], pz[4], sr[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const float4 sp = M.S[k + i];
+                        sphere_world(T, sp.x, sp.y, sp.z, px[i], py[i], pz[i]);
+                        sr[i] = __fadd_rn(sp.w, margin);
+                    }
+                    if (kStats) st.v[ST_SPHERES] += 4;
+                    ex = spheres_hit<4, kStats>(sc, ws.cand, ncand, px, py, pz, sr, g, st);
+                    if (esdf)
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+                            if (!ex) ex = sphere_esdf_any(sc, sv, px[i], py[i], pz[i], sr[i], nullptr, st);
+                }
+                for (; k < jr.sph_end && !ex; ++k) {
+                    const float4 sp = M.S[k];
+                    float px, py, pz;
+                    sphere_world(T, sp.x, sp.y, sp.z, px, py, pz);
+                    const float sr = __fadd_rn(sp.w, margin);
+                    if (kStats) st.v[ST_SPHERES] += 1;
+                    ex = spheres_hit<1, kStats>(sc, ws.cand, ncand, &px, &py, &pz, &sr, g, st) ||
+                         (esdf && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
+                }
             }
+            if (!esdf && ex) flagged = joint_gate<kStats, false>(M, sc, sv, jr, T, margin, ws, ncand, g, st);
             hit = ex && flagged;
         }
         if (__any_sync(kFull, hit && real)) break;   // warp-uniform early exit
@@ -533,9 +550,21 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_queue_kerne
                                                                   const float* __restrict__ from,
                                                                   const float* __restrict__ to, int n_edges,
                                                                   EdgeWs* hdr, const int* __restrict__ Gs, int* bad,
-                                                                  int* clr, unsigned long long* stats,
+                                                                  int* clr, unsigned long long* stats, int pass,
                                                                   const int* n_dev = nullptr) {
     if (n_dev) n_edges = *n_dev;
+    // Rounds of this launch. With many edges per resident warp (>= 8) one
+    // launch (pass 0) runs every round and pass 1 returns at once. With fewer,
+    // round 1 would start while much of round 0 is still in flight and check
+    // chunks of edges that round 0 retires, so pass 0 runs round 0 only and
+    // the second launch (pass 1) the rest.
+    const int max_rounds = *((volatile int*)&hdr->max_rounds);
+    const bool split = (long long)n_edges < 8ll * gridDim.x * kWarps;
+    const int r_lo = pass == 0 ? 0 : (split ? 1 : max_rounds);
+    const int r_hi = pass == 0 ? (split ? min(max_rounds, 1) : max_rounds) : max_rounds;
+    const long long rounds = max(r_hi - r_lo, 0);
+    const long long total = rounds * (long long)n_edges;   // chunk-major item space
+    if (total == 0) return;   // uniform over the grid: nothing staged yet
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ int counters[4];
@@ -553,19 +582,21 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_queue_kerne
     WarpScratch ws{es.q + warp * 32 * D, es.cand + warp * nob_pad, es.obs};
     LaneStats st;
     st.zero();
-    const long long rounds = *((volatile int*)&hdr->max_rounds);
-    const long long total = rounds * (long long)n_edges;   // chunk-major item space
+    unsigned long long* head = &hdr->head[pass == 0 ? 0 : 1];
+    // Items per grab: up to 32, fewer when the pass has few items, so that
+    // every resident warp gets a share.
+    const int grab = (int)max(1ll, min(32ll, total / ((long long)gridDim.x * kWarps * 2)));
     volatile int* vbad = bad;
     for (;;) {
         unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(&hdr->head, 32ull);
+        if (lane == 0) base = atomicAdd(head, (unsigned long long)grab);
         base = __shfl_sync(kFull, base, 0);
         if ((long long)base >= total) break;
         // Each lane inspects one item; live items are processed by the whole warp.
         const long long item = (long long)base + lane;
         int e = -1, k = 0, G = 0;
         bool live = false;
-        if (item < total) {
+        if (lane < grab && item < total) {
             if (total < (1ll << 31)) {   // 32-bit division in the common case
                 k = (int)((unsigned)item / (unsigned)n_edges);
                 e = (int)((unsigned)item - (unsigned)k * (unsigned)n_edges);
@@ -573,6 +604,7 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_queue_kerne
                 k = (int)(item / n_edges);
                 e = (int)(item - (long long)k * n_edges);
             }
+            k += r_lo;
             G = __ldg(Gs + e);
             const ChunkOrder ord(G);
             if (k < ord.rounds()) {

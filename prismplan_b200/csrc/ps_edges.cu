@@ -99,7 +99,10 @@ extern "C" int ps_check_edges(const ps_model* m, const ps_scene_view* scene, con
     PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qk, kEdgeThreads, smem));
     const int qgrid = std::max(1, sm_count() * std::max(per_sm, 1));
     mark_start(s);
-    qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, hdr, G, bad, clr, g_stats, nullptr);
+    qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, hdr, G, bad, clr, g_stats, 0, nullptr);
+    if ((long long)n_edges < 8ll * qgrid * kEdgeThreads / 32)   // the kernel's own split rule
+        qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, hdr, G, bad, clr, g_stats, 1,
+                                             nullptr);
     mark_stop(s);
     PS_TRY_CUDA(cudaGetLastError());
     const int fgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
@@ -190,7 +193,10 @@ extern "C" int ps_check_edges_static(const ps_model* m, const ps_scene_view* sce
     int per_sm = 0;
     PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qk, kEdgeThreads, smem));
     const int qgrid = std::max(1, sm_count() * std::max(per_sm, 1));
-    qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, hdr, G, bad, clr, g_stats, nullptr);
+    qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, hdr, G, bad, clr, g_stats, 0, nullptr);
+    if ((long long)n_edges < 8ll * qgrid * kEdgeThreads / 32)   // the kernel's own split rule
+        qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, hdr, G, bad, clr, g_stats, 1,
+                                             nullptr);
     PS_TRY_CUDA(cudaGetLastError());
     const int fgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
     edges_finalize_kernel<<<fgrid, 256, 0, s>>>(n_edges, *P, bad, len, clr, valid, cost, clearance);

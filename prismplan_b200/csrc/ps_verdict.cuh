@@ -48,6 +48,26 @@ __device__ __forceinline__ void flush_stats(unsigned long long* stats, LaneStats
     }
 }
 
+// Whether a sphere (centre c, radius R) can reach the voxel box of any
+// enabled ESDF layer: its centre, mapped into the layer frame, within R (plus
+// slack for the FP32 map) of the grid extent on every axis. A lookup outside
+// the extent never reports a distance, so a sphere set inside that bound sees
+// no layer.
+__device__ __forceinline__ bool esdf_reachable(const SceneSmem& sc, float cx, float cy, float cz, float R) {
+    for (int l = 0; l < sc.n_layers; ++l) {
+        const LayerPrep& L = sc.layers[l];
+        if (!L.enabled) continue;
+        float lx, ly, lz;
+        ref_to_local(L.q.x, L.q.y, L.q.z, L.q.w, L.t.x, L.t.y, L.t.z, cx, cy, cz, lx, ly, lz);
+        const float S = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))) + fmaxf(fabsf(L.t.x), fmaxf(fabsf(L.t.y), fabsf(L.t.z)));
+        const float slack = 1.0e-4f * (S + R + 1.0f);
+        if (fabsf(lx) <= 0.5f * L.params.x + R + slack && fabsf(ly) <= 0.5f * L.params.y + R + slack &&
+            fabsf(lz) <= 0.5f * L.params.z + R + slack)
+            return true;
+    }
+    return false;
+}
+
 // World centre and circumscribed radius of each staged box (local = R p + t,
 // so the centre is -R^T t). Every thread of the block calls it.
 __device__ __forceinline__ void box_spheres(const SceneSmem& sc, float4* obs) {
