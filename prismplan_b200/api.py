@@ -94,10 +94,13 @@ def check_configs(robot: RobotModelBuilder, scene, q, collision_margin: float = 
     return hit, clr
 
 
-def check_collision_scene(configs, scene_builder, robot: RobotModelBuilder,
+def check_collision_scene(configs, scene, robot: RobotModelBuilder,
                           collision_margin: float = 0.0) -> np.ndarray:
-    """Drop-in for prrtc.check_collision_scene: configs [N, n_dof] host array
-    -> bool [N] (True = in collision), synchronous."""
+    """Drop-in for prrtc.check_collision_scene (bindings.cpp:493-532), same
+    keywords: configs [N, n_dof] host array -> bool [N] (True = in
+    collision), synchronous. Raises RuntimeError on a column mismatch, as the
+    reference does (bindings.cpp:505-507)."""
+    scene_builder = scene
     torch = _torch()
     robot.build()
     c = np.asarray(configs, np.float32)

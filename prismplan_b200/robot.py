@@ -158,10 +158,17 @@ class RobotModelBuilder:
     the device model; ``destroy()`` or garbage collection frees it.
     """
 
+    # Mesh BVH fields of the reference builder (bindings.cpp:980-984). Mesh
+    # collision is outside this substrate: the fields are accepted so that
+    # assets and callers that set them keep working, but they are not uploaded
+    # and any request for mesh checks (EdgeEvalParams.enable_mesh) is refused.
+    MESH_FIELDS = ("mesh_bvh_nodes", "mesh_tri_vertices", "mesh_link_bvh_root", "mesh_link_tri_offset",
+                   "mesh_link_tri_count")
+
     def __init__(self):
         self.n_dof = 0
         self.n_joints = 0
-        for f in _BUILDER_FIELDS:
+        for f in _BUILDER_FIELDS + self.MESH_FIELDS:
             setattr(self, f, [])
         self._handle = None
 

@@ -1,0 +1,47 @@
+"""The substrate names of the reference's `prrtc` module (bindings.cpp:960-1037,
+used by python/gpu_planning/plugins/_substrate_planner_base.py:281-292) exist
+in prismplan_b200.prrtc with the same fields and keywords. CPU only."""
+import inspect
+
+import pytest
+
+from prismplan_b200 import prrtc
+
+ROBOT_FIELDS = (
+    "n_dof n_joints fixed_transforms joint_types spheres_flat sphere_to_joint self_cc_ranges_flat "
+    "approx_spheres_flat approx_sphere_to_joint approx_self_cc_ranges_flat approx_fixed_transforms "
+    "approx_joint_types joint_lower joint_upper joint_parents joint_id_to_dof t_memory_idx dfs_order "
+    "mesh_bvh_nodes mesh_tri_vertices mesh_link_bvh_root mesh_link_tri_offset mesh_link_tri_count").split()
+SCENE_FIELDS = (
+    "obb_dims_ptr obb_pose_ptr obb_enable_ptr n_obbs voxel_params_ptr voxel_pose_ptr voxel_enable_ptr "
+    "voxel_features_ptr n_voxel_layers max_voxels_per_layer sphere_acm_mask_ptr sphere_obb_acm_mask_ptr "
+    "sphere_obb_acm_mask_approx_ptr").split()
+
+
+def test_robot_builder_fields_and_methods():
+    r = prrtc.RobotModelBuilder()
+    for f in ROBOT_FIELDS:
+        assert hasattr(r, f), f
+        setattr(r, f, getattr(r, f))   # writable, like def_readwrite
+    for m in ("build", "update_joint_limits", "destroy"):
+        assert callable(getattr(r, m)), m
+
+
+def test_scene_builder_fields():
+    s = prrtc.SceneCollisionDataBuilder()
+    for f in SCENE_FIELDS:
+        assert hasattr(s, f), f
+        setattr(s, f, getattr(s, f))
+
+
+def test_check_collision_scene_keywords():
+    # the plugins call it with configs=, scene=, robot=, collision_margin=
+    params = inspect.signature(prrtc.check_collision_scene).parameters
+    assert list(params)[:4] == ["configs", "scene", "robot", "collision_margin"]
+    assert params["collision_margin"].default == 0.0
+
+
+def test_planner_entry_points_are_refused():
+    for name in ("solve_scene", "chomp_solve_scene", "stomp_solve_scene", "CHOMPSettings"):
+        with pytest.raises(AttributeError, match="substrate"):
+            getattr(prrtc, name)
