@@ -320,7 +320,9 @@ typedef struct ps_batch_tuning {
                                 slots its persistent grid takes              */
     float traj_share;        /* same for the trajectory kernel's grid         */
     int   traj_threads;      /* threads per block of the trajectory kernel
-                                (one waypoint per warp)                      */
+                                (one tile of waypoints per warp)             */
+    int   traj_tile;         /* waypoints per tile: 1 or 4 (one box cull per
+                                tile, against the union of their bounds)     */
     float best_ms;           /* measured time of one launch at this choice    */
 } ps_batch_tuning;
 
@@ -344,9 +346,10 @@ int ps_batch_launch(ps_batch* batch, const ps_scene_view* scene,
                     const ps_edge_params* params, const ps_cost_params* cost,
                     void* stream);
 /* Autotuner: times every candidate split of the SMs between the edge and the
-   trajectory branch and every trajectory tile width on the batch's current
-   requests, keeps the fastest for later launches and reports it (out may be
-   NULL). Synchronous; launches the batch several times. */
+   trajectory branch, every trajectory block width and tile size on the
+   batch's current requests, keeps the fastest for later launches and
+   reports it (out may be NULL). Synchronous; launches the batch several
+   times. */
 int ps_batch_tune(ps_batch* batch, const ps_scene_view* scene,
                   const ps_edge_params* params, const ps_cost_params* cost,
                   ps_batch_tuning* out);

@@ -115,7 +115,7 @@ class BatchLimits(C.Structure):
 class BatchTuning(C.Structure):
     _fields_ = [
         ("edge_share", C.c_float), ("traj_share", C.c_float),
-        ("traj_threads", C.c_int), ("best_ms", C.c_float),
+        ("traj_threads", C.c_int), ("traj_tile", C.c_int), ("best_ms", C.c_float),
     ]
 
 

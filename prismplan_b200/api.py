@@ -406,7 +406,7 @@ class MixedBatch:
         t = _lib.BatchTuning()
         _lib.check(_lib.load().ps_batch_tune(self.handle, C.byref(v), C.byref(ep), C.byref(cp), C.byref(t)))
         return {"edge_share": t.edge_share, "traj_share": t.traj_share, "traj_threads": t.traj_threads,
-                "best_ms": t.best_ms}
+                "traj_tile": t.traj_tile, "best_ms": t.best_ms}
 
     def close(self):
         if self._h is not None:

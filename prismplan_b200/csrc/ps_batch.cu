@@ -99,8 +99,9 @@ size_t waypoint_smem_bytes(const ps_model* m, const ps_scene_view* sv, int warps
     return cost_block_bytes(m, sv, warps, true);
 }
 
-// Cost and adjoint of every packed waypoint, one warp per waypoint.
-template <int kWarps>
+// Cost and adjoint of every packed waypoint, one warp per tile of kTile
+// consecutive waypoints.
+template <int kWarps, int kTile>
 __global__ void __launch_bounds__(kWarps * 32, 24 / kWarps) batch_waypoint_kernel(ModelDev md, ps_scene_view sv, ps_cost_params P,
                                                                      const Counts* __restrict__ cnt,
                                                                      const float* __restrict__ q,
@@ -111,7 +112,7 @@ __global__ void __launch_bounds__(kWarps * 32, 24 / kWarps) batch_waypoint_kerne
     __shared__ int counters[4];
     __shared__ float bmax;
     const int n_wp = cnt->n_wp;
-    if ((long long)blockIdx.x * kWarps >= n_wp) return;   // nothing for this block: skip staging
+    if ((long long)blockIdx.x * kWarps * kTile >= n_wp) return;   // nothing for this block: skip staging
     if (!stage_model(md, smem, &mbar)) return;
     const ModelSmem M = model_view(smem);
     const int D = M.H->n_dof, NJ = M.H->n_joints, NS = M.H->n_spheres;
@@ -128,12 +129,22 @@ __global__ void __launch_bounds__(kWarps * 32, 24 / kWarps) batch_waypoint_kerne
         cost_carve(cb.wbase + (size_t)warp * cost_warp_floats(NJ, NS, sv.n_obbs, md.n_sruns, true), NJ, NS, sc.n_obbs, true);
     LaneStats st;
     st.zero();
-    for (int k = blockIdx.x * kWarps + warp; k < n_wp; k += gridDim.x * kWarps) {
-        if (lane < D) ws.q[lane] = q[(size_t)k * D + lane];
+    const int n_tiles = (n_wp + kTile - 1) / kTile;
+    for (int tile = blockIdx.x * kWarps + warp; tile < n_tiles; tile += gridDim.x * kWarps) {
+        const int k0 = tile * kTile;
+        const int nt = min(kTile, n_wp - k0);
+        for (int t = 0; t < nt; ++t)
+            if (lane < D) ws.q[t * 16 + lane] = q[(size_t)(k0 + t) * D + lane];
         __syncwarp();
-        const float c = waypoint_cost_warp<true, false>(M, md, sc, sv, P, cb, ws, grad + (size_t)k * D, 1, st);
-        if (lane == 0) wp_cost[k] = c;
+        for (int t = 0; t < nt; ++t)
+            cost_fk<false>(M, ws.q + t * 16, ws.frame + t * NJ * 12, ws.bnd + t * NJ, st);
         __syncwarp();
+        cost_cull<false>(M, sc, cb, ws, nt, P.world_margin, st);
+        for (int t = 0; t < nt; ++t) {
+            const float c = cost_eval<true, false>(M, md, sc, sv, P, cb, ws, t, grad + (size_t)(k0 + t) * D, 1, st);
+            if (lane == 0) wp_cost[k0 + t] = c;
+            __syncwarp();
+        }
     }
 }
 
@@ -200,7 +211,8 @@ struct ps_batch {
     // tuning state
     float edge_share = 1.0f;   // of the edge kernel's full-occupancy grid
     float traj_share = 0.5f;   // of the trajectory kernel's full-occupancy grid
-    int traj_threads = 256;   // threads per block of the trajectory kernel (one waypoint per warp)
+    int traj_threads = 256;   // threads per block of the trajectory kernel (one tile per warp)
+    int traj_tile = 1;        // waypoints per warp tile (1 or kCostTile)
 };
 
 namespace {
@@ -209,9 +221,17 @@ struct LaunchPlan {
     int mode = 0;
     void (*qk)(ModelDev, ps_scene_view, ps_edge_params, const float*, const float*, int, EdgeWs*, const int*, int*,
                int*, unsigned long long*, int, const int*) = nullptr;
+    void (*wk)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*) = nullptr;
     size_t qsmem = 0, wsmem = 0, fsmem = 0;
     int qgrid = 1, wgrid = 1, req_grid_e = 1, req_grid_t = 1, pgrid = 1;
 };
+
+using WaypointKernel = void (*)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*);
+
+WaypointKernel pick_waypoint_kernel(int threads, int tile) {
+    if (threads == 128) return tile == 1 ? batch_waypoint_kernel<4, 1> : batch_waypoint_kernel<4, kCostTile>;
+    return tile == 1 ? batch_waypoint_kernel<8, 1> : batch_waypoint_kernel<8, kCostTile>;
+}
 
 // Everything that is not a stream operation happens before the capture.
 int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, LaunchPlan& L) {
@@ -234,18 +254,13 @@ int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, 
     if (b->lim.max_waypoints > 0) {
         const int tt = b->traj_threads;
         L.wsmem = waypoint_smem_bytes(m, sv, tt / 32);
+        L.wk = pick_waypoint_kernel(tt, b->traj_tile);
         int per_sm = 0;
-        if (tt == 128) {
-            PS_TRY_CUDA(cudaFuncSetAttribute(batch_waypoint_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)L.wsmem));
-            PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_waypoint_kernel<4>, 128, L.wsmem));
-        } else {
-            PS_TRY_CUDA(cudaFuncSetAttribute(batch_waypoint_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)L.wsmem));
-            PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_waypoint_kernel<8>, 256, L.wsmem));
-        }
+        PS_TRY_CUDA(cudaFuncSetAttribute(L.wk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.wsmem));
+        PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L.wk, tt, L.wsmem));
         if (per_sm < 1) return set_error(PS_EINVAL, "trajectory kernel does not fit on an SM with this model/scene");
-        const int cap_blocks = (b->lim.max_waypoints + tt / 32 - 1) / (tt / 32);
+        const int per_block = (tt / 32) * b->traj_tile;
+        const int cap_blocks = (b->lim.max_waypoints + per_block - 1) / per_block;
         L.wgrid = std::max(1, std::min(cap_blocks, (int)(b->traj_share * sms * per_sm + 0.5f)));
         L.fsmem = (size_t)(2 * (b->lim.max_traj_len + 12) + kFinishThreads) * sizeof(float);
         if (L.fsmem > 48 * 1024)
@@ -283,12 +298,7 @@ void record_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep
     }
     if (b->lim.max_waypoints > 0) {   // trajectory branch on s1
         batch_gather_traj<<<L.req_grid_t, 128, 0, s1>>>(b->d_treq, b->d_cnt, D, b->d_q);
-        if (b->traj_threads == 128)
-            batch_waypoint_kernel<4><<<L.wgrid, 128, L.wsmem, s1>>>(m->dev, *sv, *cp, b->d_cnt, b->d_q, b->d_wp_cost,
-                                                                    b->d_grad);
-        else
-            batch_waypoint_kernel<8><<<L.wgrid, 256, L.wsmem, s1>>>(m->dev, *sv, *cp, b->d_cnt, b->d_q, b->d_wp_cost,
-                                                                    b->d_grad);
+        L.wk<<<L.wgrid, b->traj_threads, L.wsmem, s1>>>(m->dev, *sv, *cp, b->d_cnt, b->d_q, b->d_wp_cost, b->d_grad);
         batch_traj_finish<<<L.req_grid_t, kFinishThreads, L.fsmem, s1>>>(b->d_treq, b->d_cnt, D, *cp, b->d_q,
                                                                          b->d_wp_cost, b->d_grad);
     }
@@ -318,7 +328,7 @@ int batch_capture(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep
 
 std::vector<unsigned char> make_key(const ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep,
                                     const ps_cost_params* cp) {
-    std::vector<unsigned char> k(sizeof(*sv) + sizeof(*ep) + sizeof(*cp) + 2 * sizeof(float) + sizeof(int));
+    std::vector<unsigned char> k(sizeof(*sv) + sizeof(*ep) + sizeof(*cp) + 2 * sizeof(float) + 2 * sizeof(int));
     unsigned char* p = k.data();
     auto put = [&](const void* src, size_t n) {
         std::memcpy(p, src, n);
@@ -330,6 +340,7 @@ std::vector<unsigned char> make_key(const ps_batch* b, const ps_scene_view* sv, 
     put(&b->edge_share, sizeof(float));
     put(&b->traj_share, sizeof(float));
     put(&b->traj_threads, sizeof(int));
+    put(&b->traj_tile, sizeof(int));
     return k;
 }
 
@@ -500,6 +511,7 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
     const float edge_shares[] = {0.5f, 0.75f, 1.0f};
     const float traj_shares[] = {0.25f, 0.5f, 1.0f};
     const int widths[] = {128, 256};
+    const int tiles[] = {1, kCostTile};
     cudaStream_t s = nullptr;
     cudaEvent_t a = nullptr, z = nullptr;
     PS_TRY_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -510,38 +522,43 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
         return cuda_error(le, "tuning events");
     }
     const float keep_e = b->edge_share, keep_t = b->traj_share;
-    const int keep_w = b->traj_threads;
+    const int keep_w = b->traj_threads, keep_tile = b->traj_tile;
     float best = 3.0e38f, best_e = keep_e, best_t = keep_t;
-    int best_w = keep_w;
+    int best_w = keep_w, best_tile = keep_tile;
     int rc = PS_OK;
     const bool edges = b->lim.max_edges > 0, trajs = b->lim.max_waypoints > 0;
     for (float es : edge_shares) {
         if (!edges && es != 1.0f) continue;
         for (float ts : traj_shares) {
             for (int w : widths) {
-                if (!trajs && (ts != 0.5f || w != 256)) continue;
-                b->edge_share = es;
-                b->traj_share = ts;
-                b->traj_threads = w;
-                rc = ps_batch_launch(b, sv, ep, cp, s);   // capture + warm-up
-                if (rc) break;
-                float ms_min = 3.0e38f;
-                for (int r = 0; r < 3 && rc == PS_OK; ++r) {
-                    cudaEventRecord(a, s);
-                    rc = ps_batch_launch(b, sv, ep, cp, s);
-                    cudaEventRecord(z, s);
-                    if (cudaEventSynchronize(z) != cudaSuccess) rc = cuda_error(cudaGetLastError(), "tuning run");
-                    float ms = 0.0f;
-                    cudaEventElapsedTime(&ms, a, z);
-                    ms_min = std::min(ms_min, ms);
+                for (int tl : tiles) {
+                    if (!trajs && (ts != 0.5f || w != 256 || tl != 1)) continue;
+                    b->edge_share = es;
+                    b->traj_share = ts;
+                    b->traj_threads = w;
+                    b->traj_tile = tl;
+                    rc = ps_batch_launch(b, sv, ep, cp, s);   // capture + warm-up
+                    if (rc) break;
+                    float ms_min = 3.0e38f;
+                    for (int r = 0; r < 3 && rc == PS_OK; ++r) {
+                        cudaEventRecord(a, s);
+                        rc = ps_batch_launch(b, sv, ep, cp, s);
+                        cudaEventRecord(z, s);
+                        if (cudaEventSynchronize(z) != cudaSuccess) rc = cuda_error(cudaGetLastError(), "tuning run");
+                        float ms = 0.0f;
+                        cudaEventElapsedTime(&ms, a, z);
+                        ms_min = std::min(ms_min, ms);
+                    }
+                    if (rc) break;
+                    if (ms_min < best) {
+                        best = ms_min;
+                        best_e = es;
+                        best_t = ts;
+                        best_w = w;
+                        best_tile = tl;
+                    }
                 }
                 if (rc) break;
-                if (ms_min < best) {
-                    best = ms_min;
-                    best_e = es;
-                    best_t = ts;
-                    best_w = w;
-                }
             }
             if (rc) break;
         }
@@ -555,15 +572,18 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
         b->edge_share = keep_e;
         b->traj_share = keep_t;
         b->traj_threads = keep_w;
+        b->traj_tile = keep_tile;
         return rc;
     }
     b->edge_share = best_e;
     b->traj_share = best_t;
     b->traj_threads = best_w;
+    b->traj_tile = best_tile;
     if (out) {
         out->edge_share = best_e;
         out->traj_share = best_t;
         out->traj_threads = best_w;
+        out->traj_tile = best_tile;
         out->best_ms = best;
     }
     return PS_OK;

@@ -33,9 +33,11 @@ size_t cost_block_smem(const ps_model* m, const ps_scene_view* sv, bool grad) {
     return cost_block_bytes(m, sv, kCostWarps, grad);
 }
 
-// One warp per waypoint (see ps_costwarp.cuh). kGrad: also the adjoint;
-// kStats: count executed work. Output layouts follow ps_cost_params.layout.
-template <bool kGrad, bool kStats>
+// One warp per tile of kTile consecutive waypoints (see ps_costwarp.cuh).
+// kGrad: also the adjoint; kStats: count executed work. Output layouts follow
+// ps_cost_params.layout. Gradients run tiles of 1 (the cull is cheap next to
+// the adjoint), rollouts tiles of kCostTile (smooth rollouts share boxes).
+template <bool kGrad, bool kStats, int kTile>
 __global__ void __launch_bounds__(kCostWarps * 32, 3) waypoint_cost_kernel(
     ModelDev md, ps_scene_view sv, const float* __restrict__ q, int n_rows, int T, ps_cost_params P,
     float* __restrict__ wp_cost, int broadcast_d, float* __restrict__ traj_acc, float* __restrict__ grad,
@@ -63,30 +65,46 @@ __global__ void __launch_bounds__(kCostWarps * 32, 3) waypoint_cost_kernel(
     const long long total = (long long)n_rows * T;
     LaneStats st;
     st.zero();
-    for (long long idx = (long long)blockIdx.x * kCostWarps + warp; idx < total;
-         idx += (long long)gridDim.x * kCostWarps) {
-        const int b = (int)(idx / T);
-        const int t = (int)(idx - (long long)b * T);
-        if (lane < D) ws.q[lane] = bdt ? q[((size_t)b * D + lane) * T + t] : q[((size_t)b * T + t) * D + lane];
-        __syncwarp();
-        float* grow = nullptr;
-        int gstride = 1;
-        if (kGrad) {
-            grow = bdt ? grad + ((size_t)b * D) * T + t : grad + ((size_t)b * T + t) * D;
-            gstride = bdt ? T : 1;
+    const long long n_tiles = (total + kTile - 1) / kTile;
+    for (long long tile = (long long)blockIdx.x * kCostWarps + warp; tile < n_tiles;
+         tile += (long long)gridDim.x * kCostWarps) {
+        const long long idx0 = tile * kTile;
+        const int nt = (int)min((long long)kTile, total - idx0);
+        for (int t = 0; t < nt; ++t) {
+            const long long idx = idx0 + t;
+            const int b = (int)(idx / T);
+            const int tt = (int)(idx - (long long)b * T);
+            if (lane < D)
+                ws.q[t * 16 + lane] = bdt ? q[((size_t)b * D + lane) * T + tt] : q[((size_t)b * T + tt) * D + lane];
         }
-        const float cost = waypoint_cost_warp<kGrad, kStats>(M, md, sc, sv, P, cb, ws, grow, gstride, st);
-        if (lane == 0) {
-            if (kStats) st.v[ST_SAMPLES] += 1;
-            if (wp_cost) {
-                if (broadcast_d)
-                    for (int d = 0; d < D; ++d) wp_cost[((size_t)b * D + d) * T + t] = cost;
-                else
-                    wp_cost[idx] = cost;
+        __syncwarp();
+        for (int t = 0; t < nt; ++t)
+            cost_fk<kStats>(M, ws.q + t * 16, ws.frame + t * NJ * 12, ws.bnd + t * NJ, st);
+        __syncwarp();
+        cost_cull<kStats>(M, sc, cb, ws, nt, P.world_margin, st);
+        for (int t = 0; t < nt; ++t) {
+            const long long idx = idx0 + t;
+            const int b = (int)(idx / T);
+            const int tt = (int)(idx - (long long)b * T);
+            float* grow = nullptr;
+            int gstride = 1;
+            if (kGrad) {
+                grow = bdt ? grad + ((size_t)b * D) * T + tt : grad + ((size_t)b * T + tt) * D;
+                gstride = bdt ? T : 1;
             }
-            if (traj_acc) atomicAdd(traj_acc + b, cost);
+            const float cost = cost_eval<kGrad, kStats>(M, md, sc, sv, P, cb, ws, t, grow, gstride, st);
+            if (lane == 0) {
+                if (kStats) st.v[ST_SAMPLES] += 1;
+                if (wp_cost) {
+                    if (broadcast_d)
+                        for (int d = 0; d < D; ++d) wp_cost[((size_t)b * D + d) * T + tt] = cost;
+                    else
+                        wp_cost[idx] = cost;
+                }
+                if (traj_acc) atomicAdd(traj_acc + b, cost);
+            }
+            __syncwarp();
         }
-        __syncwarp();
     }
     if (kStats) flush_stats(stats, st);
 }
@@ -156,7 +174,7 @@ extern "C" int ps_traj_cost(const ps_model* m, const ps_scene_view* scene, const
     if (atomic_traj) PS_TRY_CUDA(cudaMemsetAsync(traj_cost, 0, sizeof(float) * B, s));
     if (grad) {
         const size_t smem = cost_block_smem(m, scene, true);
-        auto k = g_stats ? waypoint_cost_kernel<true, true> : waypoint_cost_kernel<true, false>;
+        auto k = g_stats ? waypoint_cost_kernel<true, true, 1> : waypoint_cost_kernel<true, false, 1>;
         const int grid = cost_grid(k, smem, total);
         if (grid < 0) return PS_EINVAL;
         mark_start(s);
@@ -165,7 +183,7 @@ extern "C" int ps_traj_cost(const ps_model* m, const ps_scene_view* scene, const
         mark_stop(s);
     } else {
         const size_t smem = cost_block_smem(m, scene, false);
-        auto k = g_stats ? waypoint_cost_kernel<false, true> : waypoint_cost_kernel<false, false>;
+        auto k = g_stats ? waypoint_cost_kernel<false, true, kCostTile> : waypoint_cost_kernel<false, false, kCostTile>;
         const int grid = cost_grid(k, smem, total);
         if (grid < 0) return PS_EINVAL;
         mark_start(s);
@@ -195,7 +213,7 @@ extern "C" int ps_rollout_costs(const ps_model* m, const ps_scene_view* scene, c
     cudaStream_t s = (cudaStream_t)stream;
     const long long total = (long long)n_rows * T;
     const size_t smem = cost_block_smem(m, scene, false);
-    auto k = g_stats ? waypoint_cost_kernel<false, true> : waypoint_cost_kernel<false, false>;
+    auto k = g_stats ? waypoint_cost_kernel<false, true, kCostTile> : waypoint_cost_kernel<false, false, kCostTile>;
     const int grid = cost_grid(k, smem, total);
     if (grid < 0) return PS_EINVAL;
     mark_start(s);

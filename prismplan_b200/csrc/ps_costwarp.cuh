@@ -7,11 +7,14 @@
 //   w * ( sum_s relu(m - esdf_clr_s) + sum_s relu(m - min_o obb_clr_s,o)
 //         + relu(m_self - min_(i,j) (|p_i - p_j| - r_i - r_j)) ).
 // The reference evaluates every sphere against every box and every self pair
-// in one thread. Here the 32 lanes of a warp share one waypoint:
+// in one thread. Here a warp takes a tile of kCostTile consecutive waypoints;
+// steps 1 and 3-5 run per waypoint with the 32 lanes sharing it, step 2 once
+// per tile:
 //   1. FK: lane p evaluates joint p's sine/cosine, every lane walks the chain
 //      with them, lane p keeps frame p in shared memory;
 //   2. per joint, the boxes that can reach any of its spheres within the
-//      hinge band are found from the joint's bound sphere (lanes over boxes,
+//      hinge band are found from the union of the joint's bound spheres over
+//      the tile's waypoints (lanes over boxes,
 //      one ballot word per 32 boxes): a box farther than R_p + max(m, 0)
 //      from the bound centre has sdf > m + r for every sphere of the joint
 //      and contributes nothing. A circumscribed-sphere test of the box comes
@@ -39,11 +42,17 @@ namespace {
 
 constexpr unsigned kCostFull = 0xffffffffu;
 
+// Most waypoints per warp tile: the box cull of a joint is done once per
+// tile, against the union of the joint's bound spheres over the tile's
+// waypoints. Kernels run tiles of 1 or kCostTile waypoints.
+constexpr int kCostTile = 4;
+
 // Per-warp scratch in shared memory (floats unless noted; 16-byte aligned).
 struct CostWarpScratch {
-    float* q;        // [16]
-    float* frame;    // [NJ][12]
-    float4* bnd;     // [NJ][2]: (bound centre (world), radius), (box cull threshold, its square, |centre|inf, -)
+    float* q;        // [kCostTile][16]
+    float* frame;    // [kCostTile][NJ][12]
+    float4* bnd;     // [kCostTile][NJ]: bound centre (world), radius
+    float4* ubnd;    // [NJ][2]: (union centre, -), (box cull threshold, its square, |centre|inf, -)
     float4* pos;     // [NS]: centre (world), radius
     float* g;        // [NS][3]   (gradient only)
     float* jfm;      // [NJ][8]: F, M, dC/dq   (gradient only)
@@ -54,7 +63,7 @@ struct CostWarpScratch {
 __host__ __device__ inline int cost_mask_words(int n_obbs) { return (n_obbs + 31) / 32; }
 
 __host__ __device__ inline size_t cost_warp_floats(int NJ, int NS, int n_obbs, int n_sruns, bool grad) {
-    size_t f = 16 + (size_t)NJ * 12 + (size_t)NJ * 8 + (size_t)NS * 4;
+    size_t f = (size_t)kCostTile * (16 + (size_t)NJ * 12 + (size_t)NJ * 4) + (size_t)NJ * 8 + (size_t)NS * 4;
     if (grad) f += (size_t)NS * 3 + (size_t)NJ * 8;
     f = (f + 3) & ~size_t(3);
     f += (size_t)NJ * cost_mask_words(n_obbs) + ((size_t)n_sruns + 1) / 2;
@@ -64,9 +73,10 @@ __host__ __device__ inline size_t cost_warp_floats(int NJ, int NS, int n_obbs, i
 __device__ __forceinline__ CostWarpScratch cost_carve(float* base, int NJ, int NS, int n_obbs, bool grad) {
     CostWarpScratch w;
     w.q = base;
-    w.frame = w.q + 16;
-    w.bnd = reinterpret_cast<float4*>(w.frame + NJ * 12);
-    w.pos = w.bnd + NJ * 2;
+    w.frame = w.q + kCostTile * 16;
+    w.bnd = reinterpret_cast<float4*>(w.frame + kCostTile * NJ * 12);
+    w.ubnd = w.bnd + kCostTile * NJ;
+    w.pos = w.ubnd + NJ * 2;
     float* p = reinterpret_cast<float*>(w.pos + NS);
     if (grad) {
         w.g = p;
@@ -234,18 +244,13 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
-// Cost (returned on every lane) and, with kGrad, d cost / d q written by
-// lanes d < n_dof to grad_row[d * gstride]. The whole warp calls it; the
-// configuration is ws.q[0..D). kStats: count the executed work into st.
-template <bool kGrad, bool kStats>
-__device__ __forceinline__ float waypoint_cost_warp(const ModelSmem& M, const ModelDev& md, const SceneSmem& sc,
-                                    const ps_scene_view& sv, const ps_cost_params& P, const CostBlock& cb,
-                                    const CostWarpScratch& ws, float* grad_row, int gstride, LaneStats& st) {
+// FK of one waypoint (configuration q) for the whole warp: frames and the
+// world bound sphere of every joint.
+template <bool kStats>
+__device__ __forceinline__ void cost_fk(const ModelSmem& M, const float* q, float* frame, float4* bnd,
+                                        LaneStats& st) {
     const int lane = threadIdx.x & 31;
-    const int D = M.H->n_dof, NJ = M.H->n_joints, NS = M.H->n_spheres;
-    const float w = P.collision_cost_weight, wm = P.world_margin, smg = P.self_margin;
-    const int nob = sc.n_obbs, nw = cost_mask_words(nob);
-
+    const int NJ = M.H->n_joints;
     // ---- 1. FK by pointer jumping: lane p < NJ forms joint p's local step
     //      S_p = FT_p * motion(q) and holds A_p, the transform from its
     //      current ancestor anc_p to p; each round composes A_anc * A_p and
@@ -256,7 +261,7 @@ __device__ __forceinline__ float waypoint_cost_warp(const ModelSmem& M, const Mo
         int anc = -1;
         if (lane > 0 && lane < NJ) {
             const JointRec& jr = M.J[lane];
-            const float qi = jr.dof >= 0 ? ws.q[jr.dof] : 0.0f;
+            const float qi = jr.dof >= 0 ? q[jr.dof] : 0.0f;
             float sn = 0.0f, cs = 1.0f;
             if (jr.type >= PS_X_ROT) sincosf(qi, &sn, &cs);
             Affine I;
@@ -285,25 +290,46 @@ __device__ __forceinline__ float waypoint_cost_warp(const ModelSmem& M, const Mo
             }
         }
         if (lane < NJ) {
-            const JointRec& jr = M.J[lane];
-            store_frame(ws.frame + lane * 12, A);
-            const float4 b = jr.bound;
-            float cx = 0.f, cy = 0.f, cz = 0.f, thr = -1.0f;
-            if (b.w >= 0.0f) {
-                sphere_world(A, b.x, b.y, b.z, cx, cy, cz);
-                // a box farther than R + max(m, 0) from the centre reaches no
-                // sphere of the joint inside the hinge band; slack for FP32
-                const float S = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz)));
-                thr = b.w + fmaxf(wm, 0.0f);
-                thr += 4.0f * (S + thr + sc.Bmax + 1.0f) * PS_GUARD_K;
-            }
-            ws.bnd[lane * 2] = make_float4(cx, cy, cz, b.w);
-            ws.bnd[lane * 2 + 1] = make_float4(thr, thr * thr, fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))), 0.0f);
+            store_frame(frame + lane * 12, A);
+            const float4 b = M.J[lane].bound;
+            float cx = 0.f, cy = 0.f, cz = 0.f;
+            if (b.w >= 0.0f) sphere_world(A, b.x, b.y, b.z, cx, cy, cz);
+            bnd[lane] = make_float4(cx, cy, cz, b.w);
         }
         if (kStats && lane == 0) st.v[ST_JOINTS] += NJ;
     }
     __syncwarp();
 
+}
+
+// Candidate boxes per joint for a tile of nt waypoints, from the union of
+// the joint's bound spheres over the tile: a box farther than that union's
+// radius + max(m, 0) reaches no sphere of the joint inside the hinge band.
+template <bool kStats>
+__device__ __forceinline__ void cost_cull(const ModelSmem& M, const SceneSmem& sc, const CostBlock& cb,
+                                          const CostWarpScratch& ws, int nt, float wm, LaneStats& st) {
+    const int lane = threadIdx.x & 31;
+    const int NJ = M.H->n_joints;
+    const int nob = sc.n_obbs, nw = cost_mask_words(nob);
+    for (int p = lane; p < NJ; p += 32) {
+        const float4 c0 = ws.bnd[p];
+        float thr = -1.0f, S = 0.0f;
+        if (c0.w >= 0.0f) {
+            float r2 = 0.0f;
+            for (int t = 1; t < nt; ++t) {
+                const float4 c = ws.bnd[t * NJ + p];
+                const float dx = c.x - c0.x, dy = c.y - c0.y, dz = c.z - c0.z;
+                r2 = fmaxf(r2, fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
+            }
+            // slack for the FP32 rounding of the transforms and the tests
+            S = fmaxf(fabsf(c0.x), fmaxf(fabsf(c0.y), fabsf(c0.z)));
+            thr = sqrtf(r2) + c0.w + fmaxf(wm, 0.0f);
+            thr += 4.0f * (S + thr + sc.Bmax + 1.0f) * PS_GUARD_K;
+        }
+        ws.ubnd[p * 2] = make_float4(c0.x, c0.y, c0.z, c0.w);
+        ws.ubnd[p * 2 + 1] = make_float4(thr, thr * thr, S, 0.0f);
+    }
+    __syncwarp();
     // ---- 2. candidate boxes per joint (lanes over boxes): circumscribed-
     //      sphere prefilter, then the box distance of the bound centre ----
     if (nob > 0) {
@@ -316,8 +342,8 @@ __device__ __forceinline__ float waypoint_cost_warp(const ModelSmem& M, const Mo
             const int njs = *cb.njs;
             for (int pi = 0; pi < njs; ++pi) {
                 const int p = cb.jlist[pi];
-                const float4 bc = ws.bnd[p * 2];
-                const float4 th = ws.bnd[p * 2 + 1];
+                const float4 bc = ws.ubnd[p * 2];
+                const float4 th = ws.ubnd[p * 2 + 1];
                 bool keep = false;
                 if (ok && bc.w >= 0.0f) {
                     const float dx = bc.x - ob.x, dy = bc.y - ob.y, dz = bc.z - ob.z;
@@ -335,14 +361,29 @@ __device__ __forceinline__ float waypoint_cost_warp(const ModelSmem& M, const Mo
         }
         __syncwarp();
     }
+}
 
+// Cost (returned on every lane) of waypoint t of the tile and, with kGrad,
+// d cost / d q written by lanes d < n_dof to grad_row[d * gstride]. The whole
+// warp calls it after cost_fk and cost_cull. kStats: count executed work.
+template <bool kGrad, bool kStats>
+__device__ __forceinline__ float cost_eval(const ModelSmem& M, const ModelDev& md, const SceneSmem& sc,
+                                           const ps_scene_view& sv, const ps_cost_params& P, const CostBlock& cb,
+                                           const CostWarpScratch& ws, int t, float* grad_row, int gstride,
+                                           LaneStats& st) {
+    const int lane = threadIdx.x & 31;
+    const int D = M.H->n_dof, NJ = M.H->n_joints, NS = M.H->n_spheres;
+    const float w = P.collision_cost_weight, wm = P.world_margin, smg = P.self_margin;
+    const int nob = sc.n_obbs, nw = cost_mask_words(nob);
+    const float* fr = ws.frame + t * NJ * 12;
+    const float4* bw = ws.bnd + t * NJ;
     // ---- 3. spheres (lanes over spheres) ----
     float obb_part = 0.0f, esdf_part = 0.0f;
     for (int k = lane; k < NS; k += 32) {
         const int p = cb.sph_joint[k];
         const float4 sp = M.S[k];
         Affine T;
-        load_frame(ws.frame + p * 12, T);
+        load_frame(fr + p * 12, T);
         float px, py, pz;
         sphere_world(T, sp.x, sp.y, sp.z, px, py, pz);
         ws.pos[k] = make_float4(px, py, pz, sp.w);
@@ -430,7 +471,7 @@ __device__ __forceinline__ float waypoint_cost_warp(const ModelSmem& M, const Mo
             if (r < md.n_sruns) {
                 const uint2 run = __ldg(md.sruns + r);
                 const float4 a = ws.pos[run.x & 0x1ffu];
-                const float4 c = ws.bnd[((run.x >> 9) & 31u) * 2];
+                const float4 c = bw[(run.x >> 9) & 31u];
                 const float dx = a.x - c.x, dy = a.y - c.y, dz = a.z - c.z;
                 const float S = fmaxf(fmaxf(fabsf(a.x), fabsf(a.y)), fmaxf(fabsf(a.z), fmaxf(fabsf(c.x),
                                 fmaxf(fabsf(c.y), fabsf(c.z)))));
@@ -531,7 +572,7 @@ __device__ __forceinline__ float waypoint_cost_warp(const ModelSmem& M, const Mo
         float gq = 0.0f;
         if (p >= 1 && jr.dof >= 0 && jr.type != PS_FIXED) {
             const float* f = ws.jfm + p * 8;
-            const float* T = ws.frame + p * 12;
+            const float* T = fr + p * 12;
             const int ax = jr.type >= PS_X_ROT ? jr.type - PS_X_ROT : (jr.type >= PS_X_PRISM ? jr.type : 0);
             const float axx = T[0 + ax], axy = T[4 + ax], axz = T[8 + ax];
             if (jr.type >= PS_X_ROT) {
