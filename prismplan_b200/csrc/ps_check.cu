@@ -20,7 +20,42 @@ namespace {
 
 constexpr int kCfgThreads = 128;
 
-template <bool kClr>
+// Min d^2 over every box for kN sphere centres at once (one box load per kN
+// pair tests); no ACM masks.
+template <int kN>
+__device__ __forceinline__ void spheres_min_dsq(const SceneSmem& sc, const float* px, const float* py,
+                                                const float* pz, float* mn) {
+#pragma unroll
+    for (int i = 0; i < kN; ++i) mn[i] = 3.0e38f;
+    for (int o = 0; o < sc.n_obbs; ++o) {
+        const ObbPrep& b = sc.obbs[o];
+        const float4 r0 = b.r0, r1 = b.r1, r2 = b.r2, h = b.h;
+#pragma unroll
+        for (int i = 0; i < kN; ++i) {
+            const float lx = fmaf(r0.z, pz[i], fmaf(r0.y, py[i], fmaf(r0.x, px[i], r0.w)));
+            const float ly = fmaf(r1.z, pz[i], fmaf(r1.y, py[i], fmaf(r1.x, px[i], r1.w)));
+            const float lz = fmaf(r2.z, pz[i], fmaf(r2.y, py[i], fmaf(r2.x, px[i], r2.w)));
+            const float cx = fmaxf(fabsf(lx) - h.x, 0.0f), cy = fmaxf(fabsf(ly) - h.y, 0.0f),
+                        cz = fmaxf(fabsf(lz) - h.z, 0.0f);
+            mn[i] = fminf(mn[i], fmaf(cz, cz, fmaf(cy, cy, cx * cx)));
+        }
+    }
+}
+
+// SDF of a point from its min outside d^2 over the boxes (as
+// sphere_obb_min_sdf): sqrt when outside every box, else the most negative
+// max(q) over the boxes that contain it.
+__device__ __forceinline__ float sdf_from_min(const SceneSmem& sc, float px, float py, float pz, float mn) {
+    if (mn > 0.0f) return sqrtf(mn);
+    float inside = 0.0f;
+    for (int o = 0; o < sc.n_obbs; ++o) {
+        float qx, qy, qz;
+        if (fast_box_dsq(sc.obbs[o], px, py, pz, qx, qy, qz) == 0.0f) inside = fminf(inside, fmaxf(qx, fmaxf(qy, qz)));
+    }
+    return inside;
+}
+
+template <bool kClr, bool kStats>
 __global__ void __launch_bounds__(kCfgThreads) check_configs_kernel(ModelDev md, ps_scene_view sv, const float* __restrict__ q,
                                                                    int n, float margin, unsigned flags,
                                                                    uint8_t* __restrict__ hit_out,
@@ -66,12 +101,12 @@ __global__ void __launch_bounds__(kCfgThreads) check_configs_kernel(ModelDev md,
         bool hit = false;
         float clr = 1000.0f;
         if (active) {
-            st.v[ST_SAMPLES] += 1;
+            if (kStats) st.v[ST_SAMPLES] += 1;
             const bool shares = M.H->approx_shares_chain != 0;
             for (int p = 0; p < NJ; ++p) {
                 const JointRec& jr = M.J[p];
                 fk_step<true>(jr, p, qc, s0, s1, T);
-                st.v[ST_JOINTS] += (p > 0);
+                if (kStats) st.v[ST_JOINTS] += (p > 0);
                 if (!shares) fk_step<true>(M.JA[p], p, qc, a0, a1, TA);
                 // ---- approximate gate for this joint ----
                 bool flagged = no_gate;
@@ -79,7 +114,7 @@ __global__ void __launch_bounds__(kCfgThreads) check_configs_kernel(ModelDev md,
                     const float4 sa = M.A[a];
                     float px, py, pz;
                     sphere_world(shares ? T : TA, sa.x, sa.y, sa.z, px, py, pz);
-                    st.v[ST_SPHERES] += 1;
+                    if (kStats) st.v[ST_SPHERES] += 1;
                     const float sr = __fadd_rn(sa.w, margin);
                     const uint8_t* acm = sv.sphere_obb_acm_mask_approx
                                              ? sv.sphere_obb_acm_mask_approx + (size_t)M.AO[a] * sv.n_obbs
@@ -88,12 +123,13 @@ __global__ void __launch_bounds__(kCfgThreads) check_configs_kernel(ModelDev md,
                               (sc.n_layers && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
                 }
                 // ---- exact spheres of this joint ----
+                const int s_first = jr.sph_beg;
                 const int s_end = (kClr || (flagged && !hit)) ? jr.sph_end : jr.sph_beg;
-                for (int s_i = jr.sph_beg; s_i < s_end; ++s_i) {
+                for (int s_i = s_first; s_i < s_end; ++s_i) {
                     const float4 sp = M.S[s_i];
                     float px, py, pz;
                     sphere_world(T, sp.x, sp.y, sp.z, px, py, pz);
-                    st.v[ST_SPHERES] += 1;
+                    if (kStats) st.v[ST_SPHERES] += 1;
                     const float sr = __fadd_rn(sp.w, margin);
                     const int so = M.SO[s_i];
                     const uint8_t* acm =
@@ -127,7 +163,140 @@ __global__ void __launch_bounds__(kCfgThreads) check_configs_kernel(ModelDev md,
             if (clr_out) clr_out[c] = clr;
         }
     }
-    flush_stats(stats, st);
+    if (kStats) flush_stats(stats, st);
+}
+
+// Fast variant for the common model and scene: the root is the only slot-0
+// frame (one 3x4 frame in registers), the approximate chain is the full
+// chain, no ACM masks. Same decisions and clearance as check_configs_kernel;
+// in clearance mode the exact spheres of a joint are tested 4 per box load.
+// Clearance and decision of one exact sphere from its min d^2 over the boxes
+// (the per-sphere tail of the fast kernel, kept out of line so that the
+// unrolled pair loop stays small in the instruction cache).
+__device__ __noinline__ void sphere_tail(const SceneSmem& sc, const ps_scene_view& sv, float px, float py, float pz,
+                                         float sr, float mn, bool want_obb_clr, bool want_esdf_clr, bool flagged,
+                                         bool& hit, float& clr, unsigned& exact) {
+    LaneStats st;
+    st.zero();
+    if (sc.n_obbs) {
+        if (want_obb_clr) clr = fminf(clr, __fadd_rn(sdf_from_min(sc, px, py, pz, mn), -sr));
+        if (flagged && !hit) hit = decide_from_min(sc, px, py, pz, sr, mn, nullptr, st);
+    }
+    if (want_esdf_clr && sc.n_layers) clr = fminf(clr, sphere_esdf_clearance(sc, sv, px, py, pz, sr, nullptr, st));
+    if (flagged && !hit && sc.n_layers) hit = sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st);
+    exact += st.v[ST_EXACT];
+}
+
+template <bool kClr, bool kStats>
+__global__ void __launch_bounds__(kCfgThreads, 4) check_configs_fast_kernel(ModelDev md, ps_scene_view sv,
+                                                                        const float* __restrict__ q, int n,
+                                                                        float margin, unsigned flags,
+                                                                        uint8_t* __restrict__ hit_out,
+                                                                        float* __restrict__ clr_out,
+                                                                        unsigned long long* stats) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ int counters[4];
+    __shared__ float bmax;
+    unsigned char* blob = smem;
+    ObbPrep* obbs = reinterpret_cast<ObbPrep*>(smem + md.bytes_core);
+    const int nob = max(sv.n_obbs, 1);
+    int* orig = reinterpret_cast<int*>(obbs + nob);
+    LayerPrep* layers = reinterpret_cast<LayerPrep*>(orig + ((nob + 3) & ~3));
+    float* qtile = reinterpret_cast<float*>(layers + PS_MAX_LAYERS);
+
+    if (!stage_model(md, blob, &mbar)) return;
+    SceneSmem sc;
+    stage_scene(sv, obbs, orig, layers, counters, &bmax, sc);
+    const ModelSmem M = model_view(blob);
+    const int D = M.H->n_dof, NJ = M.H->n_joints;
+    const bool no_gate = (flags & PS_NO_GATE) != 0;
+    const bool want_obb_clr = kClr && (flags & PS_CLEARANCE_OBB) != 0;
+    const bool want_esdf_clr = kClr && (flags & PS_CLEARANCE_ESDF) != 0;
+    LaneStats st;
+    st.zero();
+
+    // each warp stages its own 32 configurations: no block-wide barrier
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float* wq = qtile + warp * 32 * D;
+    for (int base = (blockIdx.x * (kCfgThreads / 32) + warp) * 32; base < n; base += gridDim.x * kCfgThreads) {
+        const int cnt = min(32, n - base);
+        __syncwarp();
+        for (int k = lane; k < cnt * D; k += 32) wq[k] = q[(size_t)base * D + k];
+        __syncwarp();
+        const int c = base + lane;
+        if (lane >= cnt) continue;   // no warp-wide sync below
+        const float* qc = wq + lane * D;
+        if (kStats) st.v[ST_SAMPLES] += 1;
+        Affine T;
+        affine_identity(T);
+        bool hit = false;
+        float clr = 1000.0f;
+        for (int p = 0; p < NJ; ++p) {
+            const JointRec& jr = M.J[p];
+            if (p > 0) {
+                const float qi = jr.dof >= 0 ? qc[jr.dof] : 0.0f;
+                if (jr.parent_slot == 0) {
+                    Affine I;
+                    affine_identity(I);
+                    joint_compose<true>(jr, qi, I, T);
+                } else {
+                    joint_compose<true>(jr, qi, T, T);   // rows are read before they are written
+                }
+                if (kStats) st.v[ST_JOINTS] += 1;
+            }
+            // ---- approximate gate ----
+            bool flagged = no_gate;
+            for (int a = jr.apx_beg; a < jr.apx_end && !flagged; ++a) {
+                const float4 sa = M.A[a];
+                float px, py, pz;
+                sphere_world(T, sa.x, sa.y, sa.z, px, py, pz);
+                if (kStats) st.v[ST_SPHERES] += 1;
+                const float sr = __fadd_rn(sa.w, margin);
+                flagged = (sc.n_obbs && sphere_obb_any(sc, nullptr, 0, px, py, pz, sr, nullptr, st)) ||
+                          (sc.n_layers && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
+            }
+            if (!kClr && !(flagged && !hit)) continue;
+            // ---- exact spheres: 4 per box load, then singles ----
+            int k = jr.sph_beg;
+            for (; k + 4 <= jr.sph_end; k += 4) {
+                if (!kClr && hit) break;
+                float px[4], py[4], pz[4], mn[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const float4 sp = M.S[k + i];
+                    sphere_world(T, sp.x, sp.y, sp.z, px[i], py[i], pz[i]);
+                }
+                if (kStats) st.v[ST_SPHERES] += 4;
+                if (sc.n_obbs) {
+                    spheres_min_dsq<4>(sc, px, py, pz, mn);
+                    if (kStats) st.v[ST_PAIRS] += 4 * sc.n_obbs;
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    sphere_tail(sc, sv, px[i], py[i], pz[i], __fadd_rn(M.S[k + i].w, margin), mn[i], want_obb_clr,
+                                want_esdf_clr, flagged, hit, clr, st.v[ST_EXACT]);
+            }
+            for (; k < jr.sph_end; ++k) {
+                if (!kClr && hit) break;
+                const float4 sp = M.S[k];
+                float px, py, pz;
+                sphere_world(T, sp.x, sp.y, sp.z, px, py, pz);
+                if (kStats) st.v[ST_SPHERES] += 1;
+                const float sr = __fadd_rn(sp.w, margin);
+                float mn = 3.0e38f;
+                if (sc.n_obbs) {
+                    spheres_min_dsq<1>(sc, &px, &py, &pz, &mn);
+                    if (kStats) st.v[ST_PAIRS] += sc.n_obbs;
+                }
+                sphere_tail(sc, sv, px, py, pz, sr, mn, want_obb_clr, want_esdf_clr, flagged, hit, clr, st.v[ST_EXACT]);
+            }
+            if (!kClr && hit) break;
+        }
+        hit_out[c] = hit ? 1 : 0;
+        if (clr_out) clr_out[c] = clr;
+    }
+    if (kStats) flush_stats(stats, st);
 }
 
 // Self-collision two-phase check, one configuration per lane, positions of
@@ -302,17 +471,15 @@ extern "C" int ps_check_configs(const ps_model* m, const ps_scene_view* scene, c
     size_t smem = (size_t)m->dev.bytes_core + scene_smem_bytes(scene) + (size_t)kCfgThreads * m->info.n_dof * 4;
     const int blocks_needed = (n + kCfgThreads - 1) / kCfgThreads;
     const int grid = std::max(1, std::min(blocks_needed, sm_count() * 8));
-    if (clr) {
-        PS_TRY_CUDA(cudaFuncSetAttribute(check_configs_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        mark_start(s);
-        check_configs_kernel<true><<<grid, kCfgThreads, smem, s>>>(m->dev, *scene, q, n, margin, flags, hit, clearance,
-                                                                   g_stats);
-    } else {
-        PS_TRY_CUDA(cudaFuncSetAttribute(check_configs_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        mark_start(s);
-        check_configs_kernel<false><<<grid, kCfgThreads, smem, s>>>(m->dev, *scene, q, n, margin, flags, hit, clearance,
-                                                                    g_stats);
-    }
+    const bool fast = m->root_slot_only && m->info.approx_shares_chain && !scene->sphere_obb_acm_mask &&
+                      !scene->sphere_obb_acm_mask_approx && !scene->sphere_acm_mask;
+    auto k = fast ? (clr ? (g_stats ? check_configs_fast_kernel<true, true> : check_configs_fast_kernel<true, false>)
+                         : (g_stats ? check_configs_fast_kernel<false, true> : check_configs_fast_kernel<false, false>))
+                  : (clr ? (g_stats ? check_configs_kernel<true, true> : check_configs_kernel<true, false>)
+                         : (g_stats ? check_configs_kernel<false, true> : check_configs_kernel<false, false>));
+    PS_TRY_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    mark_start(s);
+    k<<<grid, kCfgThreads, smem, s>>>(m->dev, *scene, q, n, margin, flags, hit, clearance, g_stats);
     mark_stop(s);
     PS_TRY_CUDA(cudaGetLastError());
     if (flags & PS_CHECK_SELF) {
