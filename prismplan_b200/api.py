@@ -223,16 +223,10 @@ class EdgeEvalGpu:
         self._h_out = torch.empty((3, self.max_edges), dtype=torch.float32).pin_memory()
         self._h_valid = torch.empty(self.max_edges, dtype=torch.uint8).pin_memory()
         self._stream = torch.cuda.Stream()
+        self._graphs = {}
 
-    def evaluate(self, from_flat, to_flat, num_edges: int, params: EdgeEvalParams):
+    def _enqueue(self, n: int, params: EdgeEvalParams):
         torch = _torch()
-        n = int(num_edges)
-        if n <= 0:
-            return np.zeros(0, np.uint8), np.zeros(0, np.float32), np.zeros(0, np.float32)
-        if n > self.max_edges:
-            raise RuntimeError("EdgeEvalGpu: num_edges exceeds max_edges_")
-        self._h_from[:n].copy_(torch.from_numpy(np.asarray(from_flat, np.float32).reshape(-1, self.dim)[:n]))
-        self._h_to[:n].copy_(torch.from_numpy(np.asarray(to_flat, np.float32).reshape(-1, self.dim)[:n]))
         with torch.cuda.stream(self._stream):
             self._from[:n].copy_(self._h_from[:n], non_blocking=True)
             self._to[:n].copy_(self._h_to[:n], non_blocking=True)
@@ -242,6 +236,34 @@ class EdgeEvalGpu:
             self._h_out[0, :n].copy_(self._cost[:n], non_blocking=True)
             if params.compute_clearance:
                 self._h_out[1, :n].copy_(self._clr[:n], non_blocking=True)
+
+    def evaluate(self, from_flat, to_flat, num_edges: int, params: EdgeEvalParams):
+        """Copy in, check, copy out, synchronise. The copies and launches of
+        each (num_edges, params) seen before are replayed from a CUDA graph
+        (one launch instead of a dozen API calls); the first call of a key
+        runs eagerly and captures."""
+        torch = _torch()
+        n = int(num_edges)
+        if n <= 0:
+            return np.zeros(0, np.uint8), np.zeros(0, np.float32), np.zeros(0, np.float32)
+        if n > self.max_edges:
+            raise RuntimeError("EdgeEvalGpu: num_edges exceeds max_edges_")
+        self._h_from[:n].copy_(torch.from_numpy(np.asarray(from_flat, np.float32).reshape(-1, self.dim)[:n]))
+        self._h_to[:n].copy_(torch.from_numpy(np.asarray(to_flat, np.float32).reshape(-1, self.dim)[:n]))
+        key = (n, tuple(sorted(vars(params).items())))
+        graph = self._graphs.get(key)
+        if graph is None:
+            self._enqueue(n, params)
+            self._stream.synchronize()
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=self._stream):
+                self._enqueue(n, params)
+            if len(self._graphs) >= 8:   # small LRU of captured sizes
+                self._graphs.pop(next(iter(self._graphs)))
+            self._graphs[key] = graph
+        else:
+            self._graphs[key] = self._graphs.pop(key)
+        graph.replay()
         self._stream.synchronize()
         valid = self._h_valid[:n].numpy().copy()
         cost = self._h_out[0, :n].numpy().copy()
