@@ -186,6 +186,15 @@ typedef struct ps_edge_params {
     float collision_margin; /* added to every radius (edge_eval.cuh:39)         */
     int   check_self;       /* also run the self check (edge_eval.cuh:40)       */
     int   compute_clearance;/* ESDF min clearance over samples (edge_eval.cuh:41) */
+    float time_budget_ms;   /* > 0: persistent paths (ps_check_edges,
+                               ps_check_edges_static, ps_batch) stop pulling
+                               work once this much device time has passed
+                               since the call's first kernel began; edges left
+                               unfinished come back invalid (cost FLT_MAX)
+                               and the status query reports PS_ETIMEOUT. The
+                               planners' own device deadline is the model
+                               (pRRTC.cu:1595-1602). 0: no limit. The plain
+                               path ignores it. No reference field.          */
 } ps_edge_params;
 
 /* Plain per-call path: one warp per edge, samples in order, early exit at the
@@ -235,6 +244,11 @@ int ps_check_edges_static(const ps_model* model, const ps_scene_view* scene,
                           const ps_edge_params* params,
                           uint8_t* valid, float* cost, float* clearance,
                           void* stream);
+
+/* Status of the last persistent call that used `workspace` (NULL: the
+   built-in workspace of the current device): PS_OK, or PS_ETIMEOUT when its
+   time budget ran out. Synchronous (reads the workspace header). */
+int ps_edges_status(const void* workspace, int* status);
 
 /* =========================================================================
  * Trajectory cost: summed hinge + self hinge + smoothness, with its exact
@@ -353,6 +367,9 @@ int ps_batch_launch(ps_batch* batch, const ps_scene_view* scene,
 int ps_batch_tune(ps_batch* batch, const ps_scene_view* scene,
                   const ps_edge_params* params, const ps_cost_params* cost,
                   ps_batch_tuning* out);
+/* Status of the batch's last launch (waits for it): PS_OK, or PS_ETIMEOUT
+   when params->time_budget_ms ran out in its edge branch. */
+int ps_batch_status(ps_batch* batch, int* status);
 
 /* =========================================================================
  * Diagnostics

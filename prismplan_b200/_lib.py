@@ -91,7 +91,7 @@ class EdgeParams(C.Structure):
         ("granularity", C.c_int), ("resolution", C.c_float),
         ("max_joint_step", C.c_float), ("max_samples", C.c_int),
         ("collision_margin", C.c_float), ("check_self", C.c_int),
-        ("compute_clearance", C.c_int),
+        ("compute_clearance", C.c_int), ("time_budget_ms", C.c_float),
     ]
 
 
@@ -148,6 +148,7 @@ _SIGNATURES = [
     ("ps_rollout_costs", C.c_int,
      [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_int, C.c_int,
       C.POINTER(CostParams), C.c_int, C.c_void_p, C.c_void_p]),
+    ("ps_edges_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     ("ps_batch_create", C.c_int, [C.c_void_p, C.POINTER(BatchLimits), C.POINTER(C.c_void_p)]),
     ("ps_batch_destroy", C.c_int, [C.c_void_p]),
     ("ps_batch_clear", C.c_int, [C.c_void_p]),
@@ -157,6 +158,7 @@ _SIGNATURES = [
      [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("ps_batch_launch", C.c_int,
      [C.c_void_p, C.POINTER(SceneView), C.POINTER(EdgeParams), C.POINTER(CostParams), C.c_void_p]),
+    ("ps_batch_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     ("ps_batch_tune", C.c_int,
      [C.c_void_p, C.POINTER(SceneView), C.POINTER(EdgeParams), C.POINTER(CostParams),
       C.POINTER(BatchTuning)]),

@@ -137,6 +137,7 @@ class EdgeEvalParams:
     resolution: float = 0.0
     max_joint_step: float = 0.0
     max_samples: int = 1024
+    time_budget_ms: float = 0.0   # persistent paths: stop after this much device time (0 = none)
 
     def to_c(self) -> _lib.EdgeParams:
         if self.enable_mesh:
@@ -149,6 +150,7 @@ class EdgeEvalParams:
         p.collision_margin = float(self.collision_margin)
         p.check_self = int(bool(self.check_self))
         p.compute_clearance = int(bool(self.compute_clearance))
+        p.time_budget_ms = float(self.time_budget_ms)
         return p
 
 
@@ -156,6 +158,14 @@ def edges_workspace(n_edges: int, device="cuda"):
     torch = _torch()
     nbytes = int(_lib.load().ps_edges_workspace_bytes(int(n_edges)))
     return torch.empty(nbytes, dtype=torch.uint8, device=device)
+
+
+def edges_status(workspace=None) -> int:
+    """PS_OK or PS_ETIMEOUT for the last persistent call on ``workspace``
+    (None: the built-in workspace of the current device). Synchronous."""
+    st = C.c_int(0)
+    _lib.check(_lib.load().ps_edges_status(workspace.data_ptr() if workspace is not None else None, C.byref(st)))
+    return st.value
 
 
 def check_edges(robot: RobotModelBuilder, scene, frm, to, samples=None,
@@ -263,7 +273,8 @@ class EdgeEvalGpu:
             self._graphs[key] = graph
         else:
             self._graphs[key] = self._graphs.pop(key)
-        graph.replay()
+        with torch.cuda.stream(self._stream):   # replay on the stream synchronised below
+            graph.replay()
         self._stream.synchronize()
         valid = self._h_valid[:n].numpy().copy()
         cost = self._h_out[0, :n].numpy().copy()
@@ -418,6 +429,12 @@ class MixedBatch:
         v = _view(scene)
         _lib.check(_lib.load().ps_batch_launch(self.handle, C.byref(v), C.byref(ep), C.byref(cp),
                                                _stream(stream)))
+
+    def status(self) -> int:
+        """PS_OK or PS_ETIMEOUT for the last launch (waits for it)."""
+        st = C.c_int(0)
+        _lib.check(_lib.load().ps_batch_status(self.handle, C.byref(st)))
+        return st.value
 
     def tune(self, scene, edge_params: Optional[EdgeEvalParams] = None,
              cost_params: Optional[CostParams] = None) -> dict:

@@ -198,7 +198,7 @@ struct ps_batch {
     TrajReq* d_treq = nullptr;
     Counts* d_cnt = nullptr;
     float *d_from = nullptr, *d_to = nullptr, *d_len = nullptr, *d_cost = nullptr;
-    int *d_given = nullptr, *d_G = nullptr, *d_bad = nullptr, *d_clr = nullptr;
+    int *d_given = nullptr, *d_G = nullptr, *d_bad = nullptr, *d_clr = nullptr, *d_done = nullptr;
     uint8_t* d_valid = nullptr;
     EdgeWs* d_hdr = nullptr;
     float *d_q = nullptr, *d_wp_cost = nullptr, *d_grad = nullptr;
@@ -220,7 +220,7 @@ namespace {
 struct LaunchPlan {
     int mode = 0;
     void (*qk)(ModelDev, ps_scene_view, ps_edge_params, const float*, const float*, int, EdgeWs*, const int*, int*,
-               int*, unsigned long long*, int, const int*) = nullptr;
+               int*, int*, unsigned long long*, int, const int*) = nullptr;
     void (*wk)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*) = nullptr;
     size_t qsmem = 0, wsmem = 0, fsmem = 0;
     int qgrid = 1, wgrid = 1, req_grid_e = 1, req_grid_t = 1, pgrid = 1;
@@ -287,13 +287,13 @@ void record_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep
         cudaMemsetAsync(b->d_hdr, 0, sizeof(EdgeWs), s0);
         batch_gather_edges<<<L.req_grid_e, 128, 0, s0>>>(b->d_ereq, b->d_cnt, *ep, D, b->d_from, b->d_to, b->d_given);
         edges_prep_kernel<<<L.pgrid, 256, 0, s0>>>(*ep, b->d_from, b->d_to, b->d_given, b->lim.max_edges, D, b->d_hdr,
-                                                   b->d_G, b->d_len, b->d_bad, b->d_clr, n_dev);
+                                                   b->d_G, b->d_len, b->d_bad, b->d_clr, b->d_done, n_dev);
         L.qk<<<L.qgrid, kEdgeThreads, L.qsmem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to, b->lim.max_edges, b->d_hdr,
-                                                    b->d_G, b->d_bad, b->d_clr, nullptr, 0, n_dev);
+                                                    b->d_G, b->d_bad, b->d_clr, b->d_done, nullptr, 0, n_dev);
         L.qk<<<L.qgrid, kEdgeThreads, L.qsmem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to, b->lim.max_edges, b->d_hdr,
-                                                    b->d_G, b->d_bad, b->d_clr, nullptr, 1, n_dev);
-        edges_finalize_kernel<<<L.pgrid, 256, 0, s0>>>(b->lim.max_edges, *ep, b->d_bad, b->d_len, b->d_clr,
-                                                       b->d_valid, b->d_cost, nullptr, n_dev);
+                                                    b->d_G, b->d_bad, b->d_clr, b->d_done, nullptr, 1, n_dev);
+        edges_finalize_kernel<<<L.pgrid, 256, 0, s0>>>(b->lim.max_edges, *ep, b->d_bad, b->d_len, b->d_clr, b->d_done,
+                                                       b->d_G, b->d_hdr, b->d_valid, b->d_cost, nullptr, n_dev);
         batch_scatter_edges<<<L.req_grid_e, 128, 0, s0>>>(b->d_ereq, b->d_cnt, b->d_valid, b->d_cost);
     }
     if (b->lim.max_waypoints > 0) {   // trajectory branch on s1
@@ -387,7 +387,8 @@ extern "C" int ps_batch_create(const ps_model* m, const ps_batch_limits* lim, ps
     };
     const size_t o_ereq = take(sizeof(EdgeReq) * RE), o_treq = take(sizeof(TrajReq) * RT), o_cnt = take(sizeof(Counts));
     const size_t o_from = take(4 * E * D), o_to = take(4 * E * D), o_len = take(4 * E), o_cost = take(4 * E);
-    const size_t o_given = take(4 * E), o_G = take(4 * E), o_bad = take(4 * E), o_clr = take(4 * E);
+    const size_t o_given = take(4 * E), o_G = take(4 * E), o_bad = take(4 * E), o_clr = take(4 * E),
+                 o_done = take(4 * E);
     const size_t o_valid = take(E), o_hdr = take(sizeof(EdgeWs));
     const size_t o_q = take(4 * W * D), o_wpc = take(4 * W), o_grad = take(4 * W * D);
     cudaError_t e = cudaMalloc(&b->dmem, off);
@@ -408,6 +409,7 @@ extern "C" int ps_batch_create(const ps_model* m, const ps_batch_limits* lim, ps
     b->d_G = (int*)(base + o_G);
     b->d_bad = (int*)(base + o_bad);
     b->d_clr = (int*)(base + o_clr);
+    b->d_done = (int*)(base + o_done);
     b->d_valid = base + o_valid;
     b->d_hdr = (EdgeWs*)(base + o_hdr);
     b->d_q = (float*)(base + o_q);
@@ -501,6 +503,18 @@ extern "C" int ps_batch_launch(ps_batch* b, const ps_scene_view* sv, const ps_ed
     PS_TRY_CUDA(cudaGraphLaunch(b->exec, s));
     PS_TRY_CUDA(cudaEventRecord(b->done, s));
     b->launched = true;
+    return PS_OK;
+}
+
+extern "C" int ps_batch_status(ps_batch* b, int* status) {
+    clear_error();
+    if (!b || !status) return set_error(PS_EINVAL, "NULL argument");
+    *status = PS_OK;
+    if (!b->launched || b->lim.max_edges <= 0) return PS_OK;
+    PS_TRY_CUDA(cudaEventSynchronize(b->done));
+    EdgeWs h;
+    PS_TRY_CUDA(cudaMemcpy(&h, b->d_hdr, sizeof(EdgeWs), cudaMemcpyDeviceToHost));
+    *status = h.timed_out ? PS_ETIMEOUT : PS_OK;
     return PS_OK;
 }
 

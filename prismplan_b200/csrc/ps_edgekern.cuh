@@ -19,9 +19,17 @@ constexpr unsigned kFull = 0xffffffffu;
 
 struct EdgeWs {                         // header of the persistent workspace (64 B)
     unsigned long long head[2];         // next chunk-major item of each pass
+    unsigned long long deadline;        // %globaltimer deadline (ns), 0 = none
     int max_rounds;                     // most chunk rounds of any edge
-    int pad[11];
+    int timed_out;                      // set once a queue kernel stops at the deadline
+    int pad[8];
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 // Chunk visiting order of an edge with nc chunks of 32 samples: with
 // s = ceil(sqrt(nc)) and m = ceil(nc / s), round k visits chunk
@@ -526,8 +534,13 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_plain_kerne
 // captured graph can be replayed with a different number of edges.
 __global__ void edges_prep_kernel(ps_edge_params P, const float* __restrict__ from, const float* __restrict__ to,
                                   const int* __restrict__ given, int n_edges, int D, EdgeWs* hdr, int* G_out,
-                                  float* len_out, int* bad, int* clr, const int* n_dev = nullptr) {
+                                  float* len_out, int* bad, int* clr, int* done, const int* n_dev = nullptr) {
     if (n_dev) n_edges = *n_dev;
+    // the time budget starts when the call's first kernel runs
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        hdr->deadline = P.time_budget_ms > 0.0f
+                            ? global_ns() + (unsigned long long)((double)P.time_budget_ms * 1.0e6) + 1ull
+                            : 0ull;
     int local_max = 0;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_edges; e += gridDim.x * blockDim.x) {
         const float* a = from + (size_t)e * D;
@@ -538,6 +551,7 @@ __global__ void edges_prep_kernel(ps_edge_params P, const float* __restrict__ fr
         len_out[e] = len;
         bad[e] = 0;
         clr[e] = ordered_float(FLT_MAX);
+        done[e] = 0;
         local_max = max(local_max, ChunkOrder(G).rounds());
     }
 #pragma unroll
@@ -550,8 +564,8 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_queue_kerne
                                                                   const float* __restrict__ from,
                                                                   const float* __restrict__ to, int n_edges,
                                                                   EdgeWs* hdr, const int* __restrict__ Gs, int* bad,
-                                                                  int* clr, unsigned long long* stats, int pass,
-                                                                  const int* n_dev = nullptr) {
+                                                                  int* clr, int* done, unsigned long long* stats,
+                                                                  int pass, const int* n_dev = nullptr) {
     if (n_dev) n_edges = *n_dev;
     // Rounds of this launch. With many edges per resident warp (>= 8) one
     // launch (pass 0) runs every round and pass 1 returns at once. With fewer,
@@ -583,13 +597,22 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_queue_kerne
     LaneStats st;
     st.zero();
     unsigned long long* head = &hdr->head[pass == 0 ? 0 : 1];
+    // time budget: stop pulling items past the deadline (checked per grab)
+    const unsigned long long deadline = *((volatile unsigned long long*)&hdr->deadline);
     // Items per grab: up to 32, fewer when the pass has few items, so that
     // every resident warp gets a share.
     const int grab = (int)max(1ll, min(32ll, total / ((long long)gridDim.x * kWarps * 2)));
     volatile int* vbad = bad;
     for (;;) {
         unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(head, (unsigned long long)grab);
+        if (lane == 0) {
+            if (deadline && global_ns() > deadline) {
+                atomicExch(&hdr->timed_out, 1);
+                base = (unsigned long long)total;   // stop this warp
+            } else {
+                base = atomicAdd(head, (unsigned long long)grab);
+            }
+        }
         base = __shfl_sync(kFull, base, 0);
         if ((long long)base >= total) break;
         // Each lane inspects one item; live items are processed by the whole warp.
@@ -630,19 +653,25 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_queue_kerne
             if (lane == 0) {
                 if (h) vbad[ee] = 1;
                 if (P.compute_clearance) atomicMin(clr + ee, ordered_float(cm));
+                if (deadline) atomicAdd(done + ee, 1);   // completed chunks, read only after a timeout
             }
         }
     }
     flush_stats(stats, st);
 }
 
+// After a timeout an edge that is neither retired nor complete comes back
+// invalid (cost FLT_MAX): not shown free. Its clearance is the min over the
+// samples that were checked.
 __global__ void edges_finalize_kernel(int n_edges, const ps_edge_params P, const int* __restrict__ bad,
                                       const float* __restrict__ len, const int* __restrict__ clr,
+                                      const int* __restrict__ done, const int* __restrict__ Gs, const EdgeWs* hdr,
                                       uint8_t* __restrict__ valid, float* __restrict__ cost,
                                       float* __restrict__ clearance, const int* n_dev = nullptr) {
     if (n_dev) n_edges = *n_dev;
+    const bool timed_out = hdr->timed_out != 0;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_edges; e += gridDim.x * blockDim.x) {
-        const bool b = bad[e] != 0;
+        const bool b = bad[e] != 0 || (timed_out && done[e] < ChunkOrder(Gs[e]).nc);
         valid[e] = b ? 0 : 1;
         cost[e] = b ? FLT_MAX : len[e];
         if (clearance) clearance[e] = P.compute_clearance ? unordered_float(clr[e]) : FLT_MAX;

@@ -63,8 +63,67 @@ extern "C" int ps_check_edges_plain(const ps_model* m, const ps_scene_view* scen
 
 extern "C" size_t ps_edges_workspace_bytes(int n_edges) {
     const size_t n = (size_t)std::max(n_edges, 1);
-    return align256(sizeof(EdgeWs)) + 4 * align256(n * 4);
+    return align256(sizeof(EdgeWs)) + 5 * align256(n * 4);
 }
+
+namespace {
+
+// Workspace layout: header, then per-edge G, length, retire flag,
+// ordered-int clearance and completed-chunk count (4 B each).
+struct EdgeBufs {
+    EdgeWs* hdr;
+    int *G, *bad, *clr, *done;
+    float* len;
+};
+
+EdgeBufs carve_workspace(void* ws, int n_edges) {
+    unsigned char* w = reinterpret_cast<unsigned char*>(ws);
+    const size_t seg = align256((size_t)n_edges * 4);
+    EdgeBufs b;
+    b.hdr = reinterpret_cast<EdgeWs*>(w);
+    unsigned char* p = w + align256(sizeof(EdgeWs));
+    b.G = reinterpret_cast<int*>(p);
+    b.len = reinterpret_cast<float*>(p + seg);
+    b.bad = reinterpret_cast<int*>(p + 2 * seg);
+    b.clr = reinterpret_cast<int*>(p + 3 * seg);
+    b.done = reinterpret_cast<int*>(p + 4 * seg);
+    return b;
+}
+
+// memset header -> prep -> queue pass(es) -> finalize on stream s.
+int run_persistent(const ps_model* m, const ps_scene_view* scene, const float* from, const float* to,
+                   const int* samples_per_edge, int n_edges, const ps_edge_params* P, uint8_t* valid, float* cost,
+                   float* clearance, const EdgeBufs& b, cudaStream_t s) {
+    const int D = m->info.n_dof;
+    PS_TRY_CUDA(cudaMemsetAsync(b.hdr, 0, sizeof(EdgeWs), s));   // queue heads, deadline, max rounds, timeout
+    const int pgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
+    edges_prep_kernel<<<pgrid, 256, 0, s>>>(*P, from, to, samples_per_edge, n_edges, D, b.hdr, b.G, b.len, b.bad,
+                                            b.clr, b.done);
+    PS_TRY_CUDA(cudaGetLastError());
+    const size_t smem = edge_smem_bytes(m, scene);
+    auto qk = pick(fast_path(m, scene, P), g_stats != nullptr, edges_queue_kernel<0, false>,
+                   edges_queue_kernel<0, true>, edges_queue_kernel<1, false>, edges_queue_kernel<1, true>,
+                   edges_queue_kernel<2, false>, edges_queue_kernel<2, true>);
+    PS_TRY_CUDA(cudaFuncSetAttribute(qk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qk, kEdgeThreads, smem));
+    const int qgrid = std::max(1, sm_count() * std::max(per_sm, 1));
+    mark_start(s);
+    qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, b.hdr, b.G, b.bad, b.clr, b.done,
+                                         g_stats, 0, nullptr);
+    if ((long long)n_edges < 8ll * qgrid * kEdgeThreads / 32)   // the kernel's own split rule
+        qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, b.hdr, b.G, b.bad, b.clr, b.done,
+                                             g_stats, 1, nullptr);
+    mark_stop(s);
+    PS_TRY_CUDA(cudaGetLastError());
+    const int fgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
+    edges_finalize_kernel<<<fgrid, 256, 0, s>>>(n_edges, *P, b.bad, b.len, b.clr, b.done, b.G, b.hdr, valid, cost,
+                                                clearance);
+    PS_TRY_CUDA(cudaGetLastError());
+    return PS_OK;
+}
+
+}  // namespace
 
 extern "C" int ps_check_edges(const ps_model* m, const ps_scene_view* scene, const float* from, const float* to,
                               const int* samples_per_edge, int n_edges, const ps_edge_params* P, uint8_t* valid,
@@ -75,40 +134,8 @@ extern "C" int ps_check_edges(const ps_model* m, const ps_scene_view* scene, con
     if (!workspace || workspace_bytes < ps_edges_workspace_bytes(n_edges))
         return set_error(PS_EINVAL, "workspace missing or smaller than ps_edges_workspace_bytes(n_edges)");
     if ((reinterpret_cast<uintptr_t>(workspace) & 15) != 0) return set_error(PS_EINVAL, "workspace not 16-byte aligned");
-    cudaStream_t s = (cudaStream_t)stream;
-    unsigned char* w = reinterpret_cast<unsigned char*>(workspace);
-    const size_t seg = align256((size_t)n_edges * 4);
-    EdgeWs* hdr = reinterpret_cast<EdgeWs*>(w);
-    int* G = reinterpret_cast<int*>(w + align256(sizeof(EdgeWs)));
-    float* len = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(G) + seg);
-    int* bad = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(len) + seg);
-    int* clr = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(bad) + seg);
-    const int D = m->info.n_dof;
-
-    PS_TRY_CUDA(cudaMemsetAsync(hdr, 0, sizeof(EdgeWs), s));
-    const int pgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
-    edges_prep_kernel<<<pgrid, 256, 0, s>>>(*P, from, to, samples_per_edge, n_edges, D, hdr, G, len, bad, clr);
-    PS_TRY_CUDA(cudaGetLastError());
-
-    const size_t smem = edge_smem_bytes(m, scene);
-    auto qk = pick(fast_path(m, scene, P), g_stats != nullptr, edges_queue_kernel<0, false>,
-                   edges_queue_kernel<0, true>, edges_queue_kernel<1, false>, edges_queue_kernel<1, true>,
-                   edges_queue_kernel<2, false>, edges_queue_kernel<2, true>);
-    PS_TRY_CUDA(cudaFuncSetAttribute(qk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qk, kEdgeThreads, smem));
-    const int qgrid = std::max(1, sm_count() * std::max(per_sm, 1));
-    mark_start(s);
-    qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, hdr, G, bad, clr, g_stats, 0, nullptr);
-    if ((long long)n_edges < 8ll * qgrid * kEdgeThreads / 32)   // the kernel's own split rule
-        qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, hdr, G, bad, clr, g_stats, 1,
-                                             nullptr);
-    mark_stop(s);
-    PS_TRY_CUDA(cudaGetLastError());
-    const int fgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
-    edges_finalize_kernel<<<fgrid, 256, 0, s>>>(n_edges, *P, bad, len, clr, valid, cost, clearance);
-    PS_TRY_CUDA(cudaGetLastError());
-    return PS_OK;
+    return run_persistent(m, scene, from, to, samples_per_edge, n_edges, P, valid, cost, clearance,
+                          carve_workspace(workspace, n_edges), (cudaStream_t)stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -132,7 +159,7 @@ extern "C" int ps_check_edges(const ps_model* m, const ps_scene_view* scene, con
 namespace {
 
 constexpr size_t kStaticWsBytes =
-    ((sizeof(EdgeWs) + 255) & ~size_t(255)) + 4 * (((size_t)PS_EDGES_STATIC_MAX * 4 + 255) & ~size_t(255));
+    ((sizeof(EdgeWs) + 255) & ~size_t(255)) + 5 * (((size_t)PS_EDGES_STATIC_MAX * 4 + 255) & ~size_t(255));
 
 static __device__ __align__(256) unsigned char g_edges_static_ws[kStaticWsBytes];
 
@@ -171,35 +198,18 @@ extern "C" int ps_check_edges_static(const ps_model* m, const ps_scene_view* sce
     if (n_edges == 0) return PS_OK;
     void* ws = nullptr;
     if (int rc = static_workspace(&ws)) return rc;
-    cudaStream_t s = (cudaStream_t)stream;
-    unsigned char* w = reinterpret_cast<unsigned char*>(ws);
-    const size_t seg = align256((size_t)n_edges * 4);
-    EdgeWs* hdr = reinterpret_cast<EdgeWs*>(w);
-    int* G = reinterpret_cast<int*>(w + align256(sizeof(EdgeWs)));
-    float* len = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(G) + seg);
-    int* bad = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(len) + seg);
-    int* clr = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(bad) + seg);
-    const int D = m->info.n_dof;
+    return run_persistent(m, scene, from, to, samples_per_edge, n_edges, P, valid, cost, clearance,
+                          carve_workspace(ws, n_edges), (cudaStream_t)stream);
+}
 
-    PS_TRY_CUDA(cudaMemsetAsync(hdr, 0, sizeof(EdgeWs), s));   // queue head, max G
-    const int pgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
-    edges_prep_kernel<<<pgrid, 256, 0, s>>>(*P, from, to, samples_per_edge, n_edges, D, hdr, G, len, bad, clr);
-    PS_TRY_CUDA(cudaGetLastError());
-    const size_t smem = edge_smem_bytes(m, scene);
-    auto qk = pick(fast_path(m, scene, P), g_stats != nullptr, edges_queue_kernel<0, false>,
-                   edges_queue_kernel<0, true>, edges_queue_kernel<1, false>, edges_queue_kernel<1, true>,
-                   edges_queue_kernel<2, false>, edges_queue_kernel<2, true>);
-    PS_TRY_CUDA(cudaFuncSetAttribute(qk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qk, kEdgeThreads, smem));
-    const int qgrid = std::max(1, sm_count() * std::max(per_sm, 1));
-    qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, hdr, G, bad, clr, g_stats, 0, nullptr);
-    if ((long long)n_edges < 8ll * qgrid * kEdgeThreads / 32)   // the kernel's own split rule
-        qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, hdr, G, bad, clr, g_stats, 1,
-                                             nullptr);
-    PS_TRY_CUDA(cudaGetLastError());
-    const int fgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
-    edges_finalize_kernel<<<fgrid, 256, 0, s>>>(n_edges, *P, bad, len, clr, valid, cost, clearance);
-    PS_TRY_CUDA(cudaGetLastError());
+extern "C" int ps_edges_status(const void* workspace, int* status) {
+    clear_error();
+    if (!status) return set_error(PS_EINVAL, "status is NULL");
+    void* ws = const_cast<void*>(workspace);
+    if (!ws)
+        if (int rc = static_workspace(&ws)) return rc;
+    EdgeWs h;
+    PS_TRY_CUDA(cudaMemcpy(&h, ws, sizeof(EdgeWs), cudaMemcpyDeviceToHost));
+    *status = h.timed_out ? PS_ETIMEOUT : PS_OK;
     return PS_OK;
 }

@@ -31,7 +31,38 @@ def test_binding_loads_and_reports_version():
     assert lib.ps_edges_workspace_bytes(65536) >= 65536 * 16
 
 
-def test_struct_sizes_match_header_layout():
-    # ps_model_desc: 4 ints + 18 pointers laid out with natural alignment
-    assert ctypes.sizeof(_lib.EdgeParams) == 28
-    assert ctypes.sizeof(_lib.CostParams) == 28
+STRUCTS = {   # ctypes mirror -> C struct of include/prism_b200.h
+    "ModelDesc": "ps_model_desc", "ModelInfo": "ps_model_info", "SceneView": "ps_scene_view",
+    "EdgeParams": "ps_edge_params", "CostParams": "ps_cost_params", "BatchLimits": "ps_batch_limits",
+    "BatchTuning": "ps_batch_tuning",
+}
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """Compile a C program against the header that prints sizeof and every
+    field offset, and compare them with the ctypes mirrors."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        import pytest
+
+        pytest.skip("no C compiler")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "prism_b200.h"', "int main(void) {"]
+    for py, c in STRUCTS.items():
+        lines.append(f'printf("{py} size %zu\\n", sizeof({c}));')
+        for name, _ in getattr(_lib, py)._fields_:
+            lines.append(f'printf("{py}.{name} %zu\\n", offsetof({c}, {name}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.rsplit(" ", 1) for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                              text=True).stdout.splitlines())
+    for py in STRUCTS:
+        cls = getattr(_lib, py)
+        assert int(got[f"{py} size"]) == ctypes.sizeof(cls), py
+        for name, _ in cls._fields_:
+            assert int(got[f"{py}.{name}"]) == getattr(cls, name).offset, f"{py}.{name}"

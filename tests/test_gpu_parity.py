@@ -289,6 +289,14 @@ def test_edge_bridge_roundtrip(w2):
     np.testing.assert_array_equal(valid, rv)
     with pytest.raises(RuntimeError):
         ev.evaluate(wl["from"], wl["to"], 300, p)
+    # later calls of the same size replay a captured graph: feed different edges
+    # each time and check every answer against the reference kernels
+    for k in range(1, 4):
+        sl = slice(200 * k, 200 * (k + 1))
+        valid, cost, _ = ev.evaluate(wl["from"][sl].reshape(-1), wl["to"][sl].reshape(-1), 200, p)
+        rv, rc, _ = ref.check_edges(wl["from"][sl], wl["to"][sl], np.full(200, 40, np.int32))
+        np.testing.assert_array_equal(valid, rv)
+        assert np.array_equal(cost.view(np.uint32), rc.view(np.uint32))
 
 
 def test_edges_graph_capture_replay(w2):
