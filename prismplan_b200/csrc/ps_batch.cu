@@ -483,6 +483,7 @@ extern "C" int ps_batch_add_trajectory(ps_batch* b, const float* q, int T, float
 
 extern "C" int ps_batch_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep,
                                const ps_cost_params* cp, void* stream) {
+    PS_NVTX("ps_batch_launch");
     clear_error();
     if (!b || !ep || !cp) return set_error(PS_EINVAL, "NULL argument");
     if (int rc = validate_scene(b->model, sv)) return rc;
@@ -520,6 +521,7 @@ extern "C" int ps_batch_status(ps_batch* b, int* status) {
 
 extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep,
                              const ps_cost_params* cp, ps_batch_tuning* out) {
+    PS_NVTX("ps_batch_tune");
     clear_error();
     if (!b) return set_error(PS_EINVAL, "NULL batch");
     const float edge_shares[] = {0.5f, 0.75f, 1.0f};

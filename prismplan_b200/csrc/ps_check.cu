@@ -459,6 +459,7 @@ extern "C" int ps_set_timing_events(void* start, void* stop) {
 
 extern "C" int ps_check_configs(const ps_model* m, const ps_scene_view* scene, const float* q, int n,
                                 float margin, unsigned flags, uint8_t* hit, float* clearance, void* stream) {
+    PS_NVTX("ps_check_configs");
     clear_error();
     if (!m) return set_error(PS_EINVAL, "model is NULL");
     if (n < 0) return set_error(PS_EINVAL, "n < 0");
@@ -495,6 +496,7 @@ extern "C" int ps_check_configs(const ps_model* m, const ps_scene_view* scene, c
 }
 
 extern "C" int ps_fk_spheres(const ps_model* m, const float* q, int n, float* out, void* stream) {
+    PS_NVTX("ps_fk_spheres");
     clear_error();
     if (!m || (n > 0 && (!q || !out))) return set_error(PS_EINVAL, "NULL argument");
     if (n <= 0) return PS_OK;

@@ -163,6 +163,7 @@ using namespace ps;
 extern "C" int ps_traj_cost(const ps_model* m, const ps_scene_view* scene, const float* q, int B, int T,
                             const ps_cost_params* P, float* waypoint_cost, float* traj_cost, float* grad,
                             void* stream) {
+    PS_NVTX("ps_traj_cost");
     clear_error();
     if (int rc = check_cost_params(m, scene, q, B, T, P)) return rc;
     if (B == 0 || T == 0) return PS_OK;
@@ -205,6 +206,7 @@ extern "C" int ps_traj_cost(const ps_model* m, const ps_scene_view* scene, const
 
 extern "C" int ps_rollout_costs(const ps_model* m, const ps_scene_view* scene, const float* rollouts, int n_rows,
                                 int T, const ps_cost_params* P, int broadcast_d, float* state_cost, void* stream) {
+    PS_NVTX("ps_rollout_costs");
     clear_error();
     if (int rc = check_cost_params(m, scene, rollouts, n_rows, T, P)) return rc;
     if (!state_cost && n_rows > 0 && T > 0) return set_error(PS_EINVAL, "state_cost is NULL");

@@ -43,6 +43,7 @@ extern "C" int ps_check_edges_plain(const ps_model* m, const ps_scene_view* scen
                                     const float* to, const int* samples_per_edge, int n_edges,
                                     const ps_edge_params* P, uint8_t* valid, float* cost, float* clearance,
                                     void* stream) {
+    PS_NVTX("ps_check_edges_plain");
     clear_error();
     if (int rc = check_edge_args(m, scene, from, to, n_edges, P, valid, cost)) return rc;
     if (n_edges == 0) return PS_OK;
@@ -128,6 +129,7 @@ int run_persistent(const ps_model* m, const ps_scene_view* scene, const float* f
 extern "C" int ps_check_edges(const ps_model* m, const ps_scene_view* scene, const float* from, const float* to,
                               const int* samples_per_edge, int n_edges, const ps_edge_params* P, uint8_t* valid,
                               float* cost, float* clearance, void* workspace, size_t workspace_bytes, void* stream) {
+    PS_NVTX("ps_check_edges");
     clear_error();
     if (int rc = check_edge_args(m, scene, from, to, n_edges, P, valid, cost)) return rc;
     if (n_edges == 0) return PS_OK;
@@ -189,6 +191,7 @@ extern "C" int ps_check_edges_static(const ps_model* m, const ps_scene_view* sce
                                      const float* to, const int* samples_per_edge, int n_edges,
                                      const ps_edge_params* P, uint8_t* valid, float* cost, float* clearance,
                                      void* stream) {
+    PS_NVTX("ps_check_edges_static");
     clear_error();
     if (int rc = check_edge_args(m, scene, from, to, n_edges, P, valid, cost)) return rc;
     if (n_edges > PS_EDGES_STATIC_MAX)

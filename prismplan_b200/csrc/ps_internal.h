@@ -20,7 +20,19 @@ struct ps_model {
     std::vector<int> sph_orig;  // reordered -> descriptor index (host copy)
 };
 
+#include <nvtx3/nvToolsExt.h>
+
 namespace ps {
+
+// NVTX range around a C-ABI call (profilers show each call by name; a no-op
+// when no tool is attached).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+#define PS_NVTX(name) ::ps::NvtxRange ps_nvtx_range_(name)
 
 int set_error(int code, const std::string& msg);
 int cuda_error(cudaError_t e, const char* where);

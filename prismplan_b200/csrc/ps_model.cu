@@ -85,6 +85,7 @@ extern "C" const char* ps_last_error(void) { return g_last_error.c_str(); }
 extern "C" const char* ps_version(void) { return "prismplan_b200 0.1 (sm_100a)"; }
 
 extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
+    PS_NVTX("ps_model_create");
     using namespace ps;
     clear_error();
     if (!d || !out) return set_error(PS_EINVAL, "NULL descriptor or output");

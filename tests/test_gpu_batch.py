@@ -186,3 +186,34 @@ def test_batch_argument_errors(w5):
     batch.launch(sc, api.EdgeEvalParams(), api.CostParams())
     torch.cuda.synchronize()
     batch.close()
+
+
+def test_batch_edge_cases(w5):
+    """Empty launch, G in {0, 1, 33}, a one-waypoint trajectory, replay after
+    clear: each equals its per-request call."""
+    wl, b, sc = w5
+    batch = api.MixedBatch(b, 4, 64, 4, 256, 128)
+    ep = api.EdgeEvalParams(max_joint_step=0.01, max_samples=600)
+    cp = _cost_params(wl, smooth=0.5)
+    batch.launch(sc, ep, cp)                       # no requests at all
+    torch.cuda.synchronize()
+    frm = torch.from_numpy(wl["from"][:6]).cuda()
+    to = torch.from_numpy(wl["to"][:6]).cuda()
+    G = torch.tensor([0, 1, 33, 2, 600, 31], dtype=torch.int32, device="cuda")
+    v, c = batch.add_edges(frm, to, G)
+    q1 = torch.from_numpy(wl["trajectories"][0][:1]).cuda()   # T = 1
+    wp, tc, g = batch.add_trajectory(q1)
+    batch.launch(sc, ep, cp)
+    torch.cuda.synchronize()
+    v1, c1, _ = api.check_edges(b, sc, frm, to, samples=G, params=ep, persistent=False)
+    assert torch.equal(v, v1) and torch.equal(c.view(torch.int32), c1.view(torch.int32))
+    wp1, tc1, g1 = api.traj_cost(b, sc, q1[None], cp)
+    assert torch.equal(wp.view(torch.int32), wp1[0].view(torch.int32))
+    assert torch.equal(tc.view(torch.int32), tc1.view(torch.int32))
+    assert torch.equal(g.view(torch.int32), g1[0].view(torch.int32))
+    batch.clear()
+    batch.launch(sc, ep, cp)                       # empty again after clear
+    torch.cuda.synchronize()
+    batch.close()
+    with pytest.raises(RuntimeError):
+        batch.launch(sc, ep, cp)
