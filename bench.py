@@ -336,6 +336,7 @@ def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev):
     # ---- other workloads: configs (1) and CHOMP cost+gradient (3) ----
     res["configs"] = bench_configs(dev)
     res["chomp"] = bench_chomp(dev)
+    res["chomp_solve"] = bench_chomp_solve(dev)
     res["stomp"] = bench_stomp(dev)
     res["mixed"] = bench_mixed(dev)
     return res
@@ -532,6 +533,87 @@ def bench_chomp(dev, with_ref=True):
     return out
 
 
+def reference_asset(name: str):
+    """A robot asset of the reference (its YAML description as recorded in
+    tests/golden/reference_golden.npz)."""
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden",
+                             "reference_golden.npz"))
+    a = {k.split("/", 1)[1]: z[k] for k in z.files if k.startswith(name + "/")}
+    out = {"name": name, "n_dof": int(a["n_dof"]), "n_joints": int(a["n_joints"])}
+    for k in ("fixed_transforms", "joint_types", "spheres_flat", "sphere_to_joint", "self_cc_ranges_flat",
+              "joint_lower", "joint_upper", "joint_parents", "joint_id_to_dof", "t_memory_idx", "dfs_order",
+              "approx_spheres_flat", "approx_sphere_to_joint", "approx_self_cc_ranges_flat"):
+        out[k] = a[k].tolist()
+    return out
+
+
+def bench_chomp_solve(dev, with_ref=True, ref_sample=16):
+    """CHOMP optimisation of 256 planning requests on the reference's Panda
+    (59 spheres) among 16 random OBBs, T = 64 waypoints, the reference's
+    default settings otherwise; both endpoints of every request are
+    collision-free. One batched device loop (ps_chomp_optimize) against the
+    reference's one-request-at-a-time CHOMP::solve_runtime_scene, timed on a
+    bounded sample of the same requests."""
+    import torch
+
+    from prismplan_b200 import api, workloads
+    from prismplan_b200.robot import RobotModelBuilder
+    from prismplan_b200.scene import SceneTensors
+
+    asset = reference_asset("panda")
+    rng = np.random.default_rng(1003)
+    obbs = workloads.random_obbs(rng, 16)
+    b = RobotModelBuilder.from_asset(asset).build()
+    sc = SceneTensors(*obbs)
+
+    def is_free(q):
+        hit, _ = api.check_configs(b, sc, torch.from_numpy(q).to(dev), check_self=True)
+        return hit.cpu().numpy() == 0
+
+    B, T = 256, 64
+    starts, goals = workloads.free_pairs(rng, asset, B, is_free)
+    s = api.ChompSettings(num_timesteps=T, time_limit_ms=0.0)
+    theta0 = api.chomp_linear_init(b, starts, goals, T)
+    ws = api.chomp_workspace(b, B, T, dev)
+    res = None
+    for _ in range(2):
+        res = api.chomp_optimize(b, sc, theta0.clone(), s, workspace=ws)
+    torch.cuda.synchronize()
+    reps = 3
+    th = [theta0.clone() for _ in range(reps)]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(reps):
+        res = api.chomp_optimize(b, sc, th[i], s, workspace=ws)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    iters = res.iterations.cpu().numpy()
+    solved = res.solved.cpu().numpy()
+    out = {"workload": "chomp_solve_panda_obb16_b256_t64", "value": B / (ms * 1e-3), "unit": "requests/s",
+           "ms_per_step": ms, "solved": int(solved.sum()), "requests": B, "mean_iterations": float(iters.mean()),
+           "max_iterations": int(iters.max()),
+           "path": "ps_chomp_optimize: 256 requests per call, CUDA-graph chunks of 8 iterations"}
+    if not with_ref:
+        return out
+    try:
+        import oracle
+
+        ref = oracle.RefKernels(b, *obbs)
+        n = min(ref_sample, B)
+        ref.chomp_solve(starts[:1], goals[:1], T, s.to_c())
+        _, rsolved, riters, _, rms = ref.chomp_solve(starts[:n], goals[:n], T, s.to_c())
+        out["reference_gpu"] = {"value": n / (rms * 1e-3), "unit": "requests/s", "ms_per_request": rms / n,
+                                "sample": f"first {n} of the {B} requests, one CHOMP::solve_runtime_scene each",
+                                "solved": int(rsolved.sum()), "mean_iterations": float(riters.mean()),
+                                "device_solved_same_sample": int(solved[:n].sum()),
+                                "device_mean_iterations_same_sample": float(iters[:n].mean())}
+        out["speedup_vs_reference"] = out["value"] / out["reference_gpu"]["value"]
+    except Exception as e:
+        out["reference_gpu"] = {"unavailable": str(e)[:200]}
+    return out
+
+
 def bench_stomp(dev, with_ref=True):
     """STOMP rollout state costs: 32 trajectories x 128 noisy rollouts x 100
     waypoints of an 8-DoF Fetch-like chain (70 spheres) against 96 OBBs, in
@@ -717,7 +799,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--headline-only", action="store_true",
                     help="time the headline path only (profiling runs); skips roofline/e2e/baselines")
-    ap.add_argument("--case", choices=["configs", "chomp", "stomp", "mixed"],
+    ap.add_argument("--case", choices=["configs", "chomp", "chomp_solve", "stomp", "mixed"],
                     help="run one secondary workload alone on cuda:0 and print its line (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -725,7 +807,8 @@ def main():
         import torch
 
         dev = torch.device("cuda", 0)
-        fn = {"configs": bench_configs, "chomp": bench_chomp, "stomp": bench_stomp, "mixed": bench_mixed}[args.case]
+        fn = {"configs": bench_configs, "chomp": bench_chomp, "chomp_solve": bench_chomp_solve, "stomp": bench_stomp,
+              "mixed": bench_mixed}[args.case]
         print(json.dumps({"case": args.case, **fn(dev, with_ref=False)}), flush=True)
         return
     res = run_reference(args) if args.impl == "reference" else run_ours(args)

@@ -372,6 +372,61 @@ int ps_batch_tune(ps_batch* batch, const ps_scene_view* scene,
 int ps_batch_status(ps_batch* batch, int* status);
 
 /* =========================================================================
+ * Batched CHOMP optimisation: B trajectories advance together on the
+ * device. Replaces the per-request host loop of CHOMP::solve_runtime_scene
+ * (cpp/src/planning/chomp.cu:358-600) with the same iteration semantics:
+ *   theta <- clamp(theta - step_size (R + 1e-8 I)^-1 (obs_grad + lambda R theta))
+ *   on the interior waypoints (chomp_update_kernel, chomp.cu:259-289), where
+ *   obs_grad is the exact adjoint of the summed hinge (ps_traj_cost) instead
+ *   of the reference's central differences (chomp.cu:71-120);
+ *   total cost = sum of waypoint costs + lambda theta^T R theta
+ *   (chomp.cu:196-243);
+ *   validity = every waypoint and every segment sample theta_t + s/n_sub
+ *   (theta_t+1 - theta_t), n_sub = ceil(max segment L2 / collision_check_step),
+ *   two-phase check (chomp.cu:296-349, 459-485);
+ *   best valid snapshot, num_iterations_after_valid polishing iterations and
+ *   a two-iteration convergence streak below convergence_eps
+ *   (chomp.cu:487-537).
+ * ========================================================================= */
+typedef struct ps_chomp_params {
+    int   num_iterations;             /* CHOMP_settings.hh:26 (100)          */
+    int   num_iterations_after_valid; /* CHOMP_settings.hh:27 (5)            */
+    float step_size;                  /* CHOMP_settings.hh:33 (0.3)          */
+    float smoothness_weight;          /* lambda, CHOMP_settings.hh:34 (1.0)  */
+    float collision_cost_weight;      /* CHOMP_settings.hh:35 (20)           */
+    float world_margin;               /* CHOMP_settings.hh:42 (0.02)         */
+    float self_margin;                /* CHOMP_settings.hh:43 (0.01)         */
+    float delta_t;                    /* CHOMP_settings.hh:46 (0.1)          */
+    float convergence_eps;            /* CHOMP_settings.hh:49 (1e-4)         */
+    float collision_check_step;       /* CHOMP_settings.hh:55 (0.05)         */
+    float collision_margin;           /* validity radius margin (pRRTC_settings) */
+    int   include_self;               /* self hinge in the cost (1)          */
+    int   check_self;                 /* self check in the validity (1, as
+                                         chomp.cu:345)                       */
+    float time_limit_ms;              /* > 0: a trajectory stops iterating once
+                                         this much device time has passed
+                                         since the call began (chomp.cu:501-505
+                                         measures host wall time). 0: none.  */
+} ps_chomp_params;
+
+/* Device workspace for ps_chomp_optimize (caller allocates, 256-byte
+   aligned). 0 when the model is NULL or T < 2. */
+size_t ps_chomp_workspace_bytes(const ps_model* model, int B, int T);
+
+/* theta: device [B*T*D] (waypoint-major per trajectory), the initial
+   trajectories in, the last iterate out; waypoints 0 and T-1 stay fixed.
+   Outputs (device): best [B*T*D] = best valid iterate (the last iterate
+   when none was valid), solved [B] (1 = a valid iterate was found),
+   iterations [B] (updates applied, chomp.cu:522), best_cost [B] (total cost
+   of best). 2 <= T <= 1024. Synchronises the stream every 8 iterations to
+   stop once every trajectory has finished; not capturable. */
+int ps_chomp_optimize(const ps_model* model, const ps_scene_view* scene,
+                      float* theta, int B, int T, const ps_chomp_params* params,
+                      float* best, uint8_t* solved, int* iterations,
+                      float* best_cost, void* workspace, size_t workspace_bytes,
+                      void* stream);
+
+/* =========================================================================
  * Diagnostics
  * ========================================================================= */
 /* World-frame sphere centres for n configurations (device out [n*n_spheres*3],

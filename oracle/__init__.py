@@ -213,6 +213,8 @@ def load_ref():
                                   C.c_float, C.c_float, _fp, _fp, _fp, C.c_int]
         lib.ref_stomp_state_cost.argtypes = [C.c_void_p, C.c_void_p, _fp, C.c_int, C.c_int, C.c_float,
                                              C.c_float, C.c_float, _fp, _fp, C.c_int]
+        lib.ref_chomp_solve.argtypes = [C.c_void_p, C.c_void_p, _fp, _fp, C.c_int, C.c_int, C.c_void_p, _fp,
+                                        _u8p, _ip, _fp, C.POINTER(C.c_double)]
         _ref = lib
     return _ref
 
@@ -305,6 +307,23 @@ class RefKernels:
         _chk(load_ref().ref_chomp(self.m, self.s, _ptr(th, _fp), B, T, w, world_margin, self_margin, fd_eps,
                                   _ptr(sc, _fp), _ptr(g, _fp), C.byref(ms), reps), "chomp")
         return sc, g, ms.value
+
+    def chomp_solve(self, starts, goals, T, params):
+        """CHOMP::solve_runtime_scene per request (chomp.cu:358-600).
+        params: a ps_chomp_params ctypes structure. Returns (path [B,T,D],
+        solved [B] u8, iterations [B] i32, final_total_cost [B], wall ms)."""
+        st = _f32(starts).reshape(-1, self.n_dof)
+        gl = _f32(goals).reshape(-1, self.n_dof)
+        B = len(st)
+        path = np.zeros((B, T, self.n_dof), np.float32)
+        solved = np.zeros(B, np.uint8)
+        iters = np.zeros(B, np.int32)
+        total = np.zeros(B, np.float32)
+        ms = C.c_double(0)
+        _chk(load_ref().ref_chomp_solve(self.m, self.s, _ptr(st, _fp), _ptr(gl, _fp), B, int(T), C.byref(params),
+                                        _ptr(path, _fp), _ptr(solved, _u8p), _ptr(iters, _ip), _ptr(total, _fp),
+                                        C.byref(ms)), "chomp_solve")
+        return path, solved, iters, total, ms.value
 
     def stomp(self, rollouts_bdt, w, world_margin, self_margin, reps=1):
         r = _f32(rollouts_bdt)

@@ -12,6 +12,8 @@
 //   ppln::search::evaluate_edges_batch                           (planning/edge_eval.cuh:64-165)
 //   CHOMP chomp_state_cost_kernel / chomp_obs_grad_kernel        (planning/chomp.cu:83-188)
 //   STOMP stomp_state_cost_kernel                                (planning/stomp.cu:206-245)
+//   CHOMP::solve_runtime_scene with CHOMPBuffers                 (planning/chomp.cu:358-600,
+//                                                                 planning/chomp_buffers.cu)
 //   ppln::collision::fk_runtime, transform_sphere_to_local,
 //   sphere_single_obb_collision, sphere_obb_clearance            (device functions, through
 //                                                                 the small wrapper kernels below)
@@ -21,12 +23,14 @@
 // outside that mask (scene_collision.cuh:379 reached from a 64-thread block).
 #include "src/planning/pRRTC.cu"
 #include "src/planning/chomp.cu"
+#include "src/planning/chomp_buffers.cu"
 #include "src/planning/stomp.cu"
 #include "src/planning/edge_eval.cuh"
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <map>
@@ -418,6 +422,52 @@ int ref_chomp(void* mp, void* sp, const float* theta, int B, int T, float w, flo
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     for (void* p : own) cudaFree(p);
+    return rc;
+}
+
+// CHOMP::solve_runtime_scene once per request, with one CHOMPBuffers set
+// reused across requests as chomp_plugin.py does. starts / goals [B][D];
+// path [B][T][D], solved [B], iters [B], total [B] (final_total_cost) out,
+// all host. include_self / check_self are not settings of the reference
+// (it always includes both). *ms = host wall time of the B solves.
+int ref_chomp_solve(void* mp, void* sp, const float* starts, const float* goals, int B, int T,
+                    const ps_chomp_params* P, float* path, uint8_t* solved, int* iters, float* total,
+                    double* ms) {
+    RefModel* m = (RefModel*)mp;
+    RefScene* s = (RefScene*)sp;
+    ppln::RobotModel& mod = m->dev.model;
+    const int D = mod.n_dof;
+    CHOMP_settings st;
+    st.num_timesteps = T;
+    st.num_iterations = P->num_iterations;
+    st.num_iterations_after_valid = P->num_iterations_after_valid;
+    st.step_size = P->step_size;
+    st.smoothness_weight = P->smoothness_weight;
+    st.collision_cost_weight = P->collision_cost_weight;
+    st.world_collision_margin = P->world_margin;
+    st.self_collision_margin = P->self_margin;
+    st.delta_t = P->delta_t;
+    st.convergence_eps = P->convergence_eps;
+    st.collision_check_step = P->collision_check_step;
+    st.collision_margin = P->collision_margin;
+    st.time_limit_ms = P->time_limit_ms;
+    CHOMPBuffers bufs = CHOMPBuffers::create(D, T);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int b = 0; b < B; ++b) {
+        std::vector<float> start(starts + (size_t)b * D, starts + (size_t)(b + 1) * D);
+        std::vector<std::vector<float>> gl(1, std::vector<float>(goals + (size_t)b * D, goals + (size_t)(b + 1) * D));
+        CHOMPResult r = CHOMP::solve_runtime_scene(start, gl, s->d, st, mod, &bufs);
+        for (int t = 0; t < T && t < (int)r.path.size(); ++t)
+            for (int d = 0; d < D; ++d) path[((size_t)b * T + t) * D + d] = r.path[t][d];
+        solved[b] = r.solved ? 1 : 0;
+        iters[b] = r.iterations_run;
+        total[b] = r.final_total_cost;
+    }
+    cudaDeviceSynchronize();
+    const auto t1 = std::chrono::steady_clock::now();
+    if (ms) *ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    const int rc = last_cuda("chomp_solve");
+    bufs.destroy();
     return rc;
 }
 

@@ -119,6 +119,18 @@ class BatchTuning(C.Structure):
     ]
 
 
+class ChompParams(C.Structure):
+    _fields_ = [
+        ("num_iterations", C.c_int), ("num_iterations_after_valid", C.c_int),
+        ("step_size", C.c_float), ("smoothness_weight", C.c_float),
+        ("collision_cost_weight", C.c_float), ("world_margin", C.c_float),
+        ("self_margin", C.c_float), ("delta_t", C.c_float),
+        ("convergence_eps", C.c_float), ("collision_check_step", C.c_float),
+        ("collision_margin", C.c_float), ("include_self", C.c_int),
+        ("check_self", C.c_int), ("time_limit_ms", C.c_float),
+    ]
+
+
 # (name, restype, argtypes)
 _SIGNATURES = [
     ("ps_last_error", C.c_char_p, []),
@@ -162,6 +174,10 @@ _SIGNATURES = [
     ("ps_batch_tune", C.c_int,
      [C.c_void_p, C.POINTER(SceneView), C.POINTER(EdgeParams), C.POINTER(CostParams),
       C.POINTER(BatchTuning)]),
+    ("ps_chomp_workspace_bytes", C.c_size_t, [C.c_void_p, C.c_int, C.c_int]),
+    ("ps_chomp_optimize", C.c_int,
+     [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_int, C.c_int, C.POINTER(ChompParams),
+      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
     ("ps_fk_spheres", C.c_int,
      [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     ("ps_probe_fp32_peak", C.c_int, [C.POINTER(C.c_double), C.c_void_p]),

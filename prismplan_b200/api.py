@@ -357,6 +357,124 @@ def rollout_costs(robot: RobotModelBuilder, scene, rollouts, params: Optional[Co
 
 
 # ---------------------------------------------------------------------------
+# batched CHOMP optimisation
+# ---------------------------------------------------------------------------
+@dataclass
+class ChompSettings:
+    """CHOMP settings with the reference's names and defaults
+    (cpp/src/planning/CHOMP_settings.hh:23-55; time_limit_ms and
+    collision_margin from pRRTC_settings.hh:6,25). ``fd_epsilon`` has no
+    counterpart: the obstacle gradient is the exact adjoint."""
+
+    num_timesteps: int = 51
+    num_iterations: int = 100
+    num_iterations_after_valid: int = 5
+    step_size: float = 0.3
+    smoothness_weight: float = 1.0
+    collision_cost_weight: float = 20.0
+    world_collision_margin: float = 0.02
+    self_collision_margin: float = 0.01
+    delta_t: float = 0.1
+    convergence_eps: float = 1.0e-4
+    collision_check_step: float = 0.05
+    collision_margin: float = 0.0
+    time_limit_ms: float = 4000.0
+    include_self: bool = True
+    check_self: bool = True
+
+    def to_c(self) -> _lib.ChompParams:
+        p = _lib.ChompParams()
+        p.num_iterations = int(self.num_iterations)
+        p.num_iterations_after_valid = int(self.num_iterations_after_valid)
+        p.step_size = float(self.step_size)
+        p.smoothness_weight = float(self.smoothness_weight)
+        p.collision_cost_weight = float(self.collision_cost_weight)
+        p.world_margin = float(self.world_collision_margin)
+        p.self_margin = float(self.self_collision_margin)
+        p.delta_t = float(self.delta_t)
+        p.convergence_eps = float(self.convergence_eps)
+        p.collision_check_step = float(self.collision_check_step)
+        p.collision_margin = float(self.collision_margin)
+        p.include_self = int(bool(self.include_self))
+        p.check_self = int(bool(self.check_self))
+        p.time_limit_ms = float(self.time_limit_ms)
+        return p
+
+
+@dataclass
+class ChompResult:
+    """Per-request outcome of ``chomp_optimize`` / ``chomp_solve``, the fields
+    of CHOMPResult (Planners.hh) for B requests at once."""
+
+    path: "torch.Tensor"        # [B, T, D] best valid iterate (last iterate if none)
+    solved: "torch.Tensor"      # [B] bool
+    iterations: "torch.Tensor"  # [B] int32, updates applied
+    cost: "torch.Tensor"        # [B] total cost of ``path``
+    theta: "torch.Tensor"       # [B, T, D] last iterate
+
+
+def chomp_workspace(robot: RobotModelBuilder, B: int, T: int, device="cuda"):
+    torch = _torch()
+    nbytes = int(_lib.load().ps_chomp_workspace_bytes(_model(robot), int(B), int(T)))
+    return torch.empty(max(nbytes, 1), dtype=torch.uint8, device=device)
+
+
+def chomp_linear_init(robot: RobotModelBuilder, starts, goals, T: int):
+    """Straight-line initial trajectories [B, T, D] clamped to the joint
+    limits, as chomp_init_trajectory_kernel (chomp.cu:57-69) builds them."""
+    torch = _torch()
+    s = _dev_f32(starts, robot.n_dof).reshape(-1, robot.n_dof)
+    g = _dev_f32(goals, robot.n_dof).reshape(-1, robot.n_dof)
+    if s.shape != g.shape:
+        raise ValueError("starts and goals differ in shape")
+    t = torch.arange(T, device=s.device, dtype=torch.float32)
+    frac = t / float(T - 1) if T > 1 else torch.zeros_like(t)
+    v = s[:, None, :] * (1.0 - frac)[None, :, None] + g[:, None, :] * frac[None, :, None]
+    lo = torch.tensor(np.asarray(robot.joint_lower, np.float32), device=s.device)
+    hi = torch.tensor(np.asarray(robot.joint_upper, np.float32), device=s.device)
+    return torch.maximum(lo, torch.minimum(hi, v)).contiguous()
+
+
+def chomp_optimize(robot: RobotModelBuilder, scene, theta, settings: Optional[ChompSettings] = None,
+                   workspace=None, stream=None) -> ChompResult:
+    """Run CHOMP on B trajectories ``theta`` [B, T, D] at once (the reference
+    runs one, chomp.cu:358-600). ``theta`` is updated in place when it is a
+    contiguous float32 CUDA tensor. Synchronises the stream every 8
+    iterations."""
+    torch = _torch()
+    settings = settings or ChompSettings()
+    th = _dev_f32(theta)
+    if th.dim() != 3 or th.shape[2] != robot.n_dof:
+        raise ValueError("theta must be [B, T, n_dof]")
+    B, T, D = th.shape
+    best = torch.empty_like(th)
+    solved = torch.empty(B, dtype=torch.uint8, device=th.device)
+    iters = torch.empty(B, dtype=torch.int32, device=th.device)
+    cost = torch.empty(B, dtype=torch.float32, device=th.device)
+    ws = workspace if workspace is not None else chomp_workspace(robot, B, T, th.device)
+    p = settings.to_c()
+    v = _view(scene)
+    _lib.check(_lib.load().ps_chomp_optimize(_model(robot), C.byref(v), th.data_ptr(), B, T, C.byref(p),
+                                             best.data_ptr(), solved.data_ptr(), iters.data_ptr(),
+                                             cost.data_ptr(), ws.data_ptr(), ws.numel(), _stream(stream)))
+    return ChompResult(best, solved.bool(), iters, cost, th)
+
+
+def chomp_solve(robot: RobotModelBuilder, scene, starts, goals, settings: Optional[ChompSettings] = None,
+                stream=None) -> ChompResult:
+    """CHOMP::solve_runtime_scene for B (start, goal) pairs: straight-line
+    initialisation over num_timesteps waypoints, the optimiser loop, and the
+    path's first and last waypoints set to start and goal
+    (chomp.cu:557-567)."""
+    settings = settings or ChompSettings()
+    theta = chomp_linear_init(robot, starts, goals, settings.num_timesteps)
+    res = chomp_optimize(robot, scene, theta, settings, stream=stream)
+    res.path[:, 0, :] = _dev_f32(starts, robot.n_dof).reshape(-1, robot.n_dof)
+    res.path[:, -1, :] = _dev_f32(goals, robot.n_dof).reshape(-1, robot.n_dof)
+    return res
+
+
+# ---------------------------------------------------------------------------
 # mixed-request batches
 # ---------------------------------------------------------------------------
 class MixedBatch:

@@ -37,11 +37,13 @@ size_t cost_block_smem(const ps_model* m, const ps_scene_view* sv, bool grad) {
 // kGrad: also the adjoint; kStats: count executed work. Output layouts follow
 // ps_cost_params.layout. Gradients run tiles of 1 (the cull is cheap next to
 // the adjoint), rollouts tiles of kCostTile (smooth rollouts share boxes).
+// skip (tiles of 1 only; may be NULL): rows b with skip[b] != 0 are left
+// untouched.
 template <bool kGrad, bool kStats, int kTile>
 __global__ void __launch_bounds__(kCostWarps * 32, 3) waypoint_cost_kernel(
     ModelDev md, ps_scene_view sv, const float* __restrict__ q, int n_rows, int T, ps_cost_params P,
     float* __restrict__ wp_cost, int broadcast_d, float* __restrict__ traj_acc, float* __restrict__ grad,
-    unsigned long long* stats) {
+    unsigned long long* stats, const uint8_t* __restrict__ skip) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ int counters[4];
@@ -70,6 +72,7 @@ __global__ void __launch_bounds__(kCostWarps * 32, 3) waypoint_cost_kernel(
          tile += (long long)gridDim.x * kCostWarps) {
         const long long idx0 = tile * kTile;
         const int nt = (int)min((long long)kTile, total - idx0);
+        if (kTile == 1 && skip && skip[idx0 / T]) continue;   // uniform over the warp
         for (int t = 0; t < nt; ++t) {
             const long long idx = idx0 + t;
             const int b = (int)(idx / T);
@@ -114,10 +117,10 @@ __global__ void __launch_bounds__(kCostWarps * 32, 3) waypoint_cost_kernel(
 // waypoint costs were written, else traj_cost += smoothness.
 __global__ void smoothness_kernel(const float* __restrict__ q, int B, int T, int D, ps_cost_params P,
                                   const float* __restrict__ wp_cost, float* __restrict__ traj_cost,
-                                  float* __restrict__ grad) {
+                                  float* __restrict__ grad, const uint8_t* __restrict__ skip) {
     extern __shared__ float sh[];
     const int b = blockIdx.x;
-    if (b >= B) return;
+    if (b >= B || (skip && skip[b])) return;
     const bool bdt = P.layout == PS_LAYOUT_BDT;
     auto idx = [&](int t, int d) { return bdt ? ((size_t)b * D + d) * T + t : ((size_t)b * T + t) * D + d; };
     const float tot = traj_smooth_block(
@@ -160,16 +163,14 @@ int check_cost_params(const ps_model* m, const ps_scene_view* scene, const float
 
 using namespace ps;
 
-extern "C" int ps_traj_cost(const ps_model* m, const ps_scene_view* scene, const float* q, int B, int T,
-                            const ps_cost_params* P, float* waypoint_cost, float* traj_cost, float* grad,
-                            void* stream) {
-    PS_NVTX("ps_traj_cost");
-    clear_error();
+int ps::traj_cost_launch(const ps_model* m, const ps_scene_view* scene, const float* q, int B, int T,
+                         const ps_cost_params* P, float* waypoint_cost, float* traj_cost, float* grad,
+                         const uint8_t* skip, cudaStream_t s) {
     if (int rc = check_cost_params(m, scene, q, B, T, P)) return rc;
     if (B == 0 || T == 0) return PS_OK;
     if (T > PS_MAX_TRAJ_LEN && (traj_cost || (grad && P->smoothness_weight != 0.0f)))
         return set_error(PS_EINVAL, "T exceeds PS_MAX_TRAJ_LEN for the smoothness term");
-    cudaStream_t s = (cudaStream_t)stream;
+    if (skip && !grad) return set_error(PS_EINVAL, "row skipping needs the gradient kernel");
     const long long total = (long long)B * T;
     const bool atomic_traj = traj_cost && !waypoint_cost;
     if (atomic_traj) PS_TRY_CUDA(cudaMemsetAsync(traj_cost, 0, sizeof(float) * B, s));
@@ -180,7 +181,7 @@ extern "C" int ps_traj_cost(const ps_model* m, const ps_scene_view* scene, const
         if (grid < 0) return PS_EINVAL;
         mark_start(s);
         k<<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
-                                                                    atomic_traj ? traj_cost : nullptr, grad, g_stats);
+                                              atomic_traj ? traj_cost : nullptr, grad, g_stats, skip);
         mark_stop(s);
     } else {
         const size_t smem = cost_block_smem(m, scene, false);
@@ -189,7 +190,7 @@ extern "C" int ps_traj_cost(const ps_model* m, const ps_scene_view* scene, const
         if (grid < 0) return PS_EINVAL;
         mark_start(s);
         k<<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
-                                                                     atomic_traj ? traj_cost : nullptr, nullptr, g_stats);
+                                              atomic_traj ? traj_cost : nullptr, nullptr, g_stats, nullptr);
         mark_stop(s);
     }
     PS_TRY_CUDA(cudaGetLastError());
@@ -198,10 +199,18 @@ extern "C" int ps_traj_cost(const ps_model* m, const ps_scene_view* scene, const
         const size_t sm2 = (size_t)(2 * (T + 12) + threads) * sizeof(float);
         if (sm2 > 48 * 1024)
             PS_TRY_CUDA(cudaFuncSetAttribute(smoothness_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-        smoothness_kernel<<<B, threads, sm2, s>>>(q, B, T, m->info.n_dof, *P, waypoint_cost, traj_cost, grad);
+        smoothness_kernel<<<B, threads, sm2, s>>>(q, B, T, m->info.n_dof, *P, waypoint_cost, traj_cost, grad, skip);
         PS_TRY_CUDA(cudaGetLastError());
     }
     return PS_OK;
+}
+
+extern "C" int ps_traj_cost(const ps_model* m, const ps_scene_view* scene, const float* q, int B, int T,
+                            const ps_cost_params* P, float* waypoint_cost, float* traj_cost, float* grad,
+                            void* stream) {
+    PS_NVTX("ps_traj_cost");
+    clear_error();
+    return traj_cost_launch(m, scene, q, B, T, P, waypoint_cost, traj_cost, grad, nullptr, (cudaStream_t)stream);
 }
 
 extern "C" int ps_rollout_costs(const ps_model* m, const ps_scene_view* scene, const float* rollouts, int n_rows,
@@ -220,7 +229,7 @@ extern "C" int ps_rollout_costs(const ps_model* m, const ps_scene_view* scene, c
     if (grid < 0) return PS_EINVAL;
     mark_start(s);
     k<<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, rollouts, n_rows, T, *P, state_cost,
-                                                                 broadcast_d, nullptr, nullptr, g_stats);
+                                                                 broadcast_d, nullptr, nullptr, g_stats, nullptr);
     mark_stop(s);
     PS_TRY_CUDA(cudaGetLastError());
     return PS_OK;

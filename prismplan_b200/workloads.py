@@ -283,6 +283,18 @@ def uniform_configs(rng, asset: Dict, n: int) -> np.ndarray:
     return (lo + rng.random((n, len(lo))) * (hi - lo)).astype(np.float32)
 
 
+def free_pairs(rng, asset: Dict, n: int, is_free, oversample: int = 4):
+    """n (start, goal) pairs drawn uniformly within the limits from
+    configurations that ``is_free`` (a callable, [m, D] -> bool [m]) accepts,
+    as a planning benchmark poses them (both endpoints collision-free).
+    Raises if fewer than 2 n candidates pass."""
+    cand = uniform_configs(rng, asset, max(2 * n * oversample, 2))
+    free = cand[np.asarray(is_free(cand), bool)]
+    if len(free) < 2 * n:
+        raise ValueError(f"only {len(free)} of {len(cand)} candidates are collision-free")
+    return free[:n].copy(), free[n:2 * n].copy()
+
+
 def linf_samples(frm: np.ndarray, to: np.ndarray, step: float, max_samples: int = 600) -> np.ndarray:
     """G_e = clamp(ceil(max_i |to_i - from_i| / step), 1, max_samples), computed
     in float32 as the device does."""
