@@ -4,13 +4,16 @@ Drop-in surface (names of the reference ``prrtc`` module and substrate):
 ``RobotModelBuilder``, ``SceneCollisionDataBuilder``, ``PlanningScene``,
 ``check_collision_scene``, ``EdgeEvalGpu``, ``load_robot_asset``,
 ``build_robot_model``; device-resident torch ops ``check_configs``,
-``check_edges``, ``traj_cost``, ``rollout_costs``, ``hinge_cost``.
+``check_edges``, ``traj_cost``, ``rollout_costs``, ``hinge_cost``; the
+batched CHOMP optimiser ``chomp_solve`` / ``chomp_optimize``.
 The compute path is the CUDA library ``libprism_b200.so``; importing this
 package does not load it (so CPU-only tooling works), the first call does and
 fails loudly if it is missing.
 """
 from ._lib import PrismError  # noqa: F401
 from .api import (  # noqa: F401
+    ChompResult,
+    ChompSettings,
     CostParams,
     EdgeEvalGpu,
     EdgeEvalParams,
@@ -18,6 +21,10 @@ from .api import (  # noqa: F401
     check_collision_scene,
     check_configs,
     check_edges,
+    chomp_linear_init,
+    chomp_optimize,
+    chomp_solve,
+    chomp_workspace,
     edges_workspace,
     fk_spheres,
     hinge_cost,
