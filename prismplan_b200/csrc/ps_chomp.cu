@@ -99,13 +99,18 @@ __global__ void chomp_init_kernel(ChompState* __restrict__ st, uint8_t* __restri
 }
 
 // One block per request: its segments (theta_t -> theta_t+1) as edges with
-// n_sub samples each (0 once finished).
+// n_sub samples each; 0 samples once the request has finished or when one of
+// its waypoints already collides (wp_hit, from the configuration check of the
+// same iterate), since the trajectory is then invalid whatever its segments.
 __global__ void chomp_segments_kernel(const float* __restrict__ theta, int T, int D, float check_step,
-                                      const uint8_t* __restrict__ done, float* __restrict__ from,
-                                      float* __restrict__ to, int* __restrict__ G) {
+                                      const uint8_t* __restrict__ done, const uint8_t* __restrict__ wp_hit,
+                                      float* __restrict__ from, float* __restrict__ to, int* __restrict__ G) {
     __shared__ float red[256];
     const int b = blockIdx.x;
     const float* th = theta + (size_t)b * T * D;
+    bool any_hit = false;
+    for (int t = threadIdx.x; t < T; t += blockDim.x) any_hit |= wp_hit[(size_t)b * T + t] != 0;
+    any_hit = __syncthreads_or(any_hit) != 0;
     float mx = 0.0f;
     for (int t = threadIdx.x; t < T - 1; t += blockDim.x) {
         float d2 = 0.0f;   // in order, without contraction, as the host loop of chomp.cu:462-469
@@ -124,7 +129,7 @@ __global__ void chomp_segments_kernel(const float* __restrict__ theta, int T, in
     const float max_seg = red[0];
     int n_sub = 1;   // chomp.cu:471-474; capped so that the cast stays defined
     if (check_step > 0.0f && max_seg > check_step) n_sub = (int)fminf(ceilf(__fdiv_rn(max_seg, check_step)), 1048576.0f);
-    const int g = done[b] ? 0 : n_sub;
+    const int g = (done[b] || any_hit) ? 0 : n_sub;
     const size_t e0 = (size_t)b * (T - 1);
     for (int i = threadIdx.x; i < (T - 1) * D; i += blockDim.x) {
         from[e0 * D + i] = th[i];
@@ -212,13 +217,15 @@ __global__ void chomp_update_kernel(float* __restrict__ theta, const float* __re
                                     const double* __restrict__ L, const float* __restrict__ lower,
                                     const float* __restrict__ upper, int T, int D, float step, float lambda,
                                     float dt_f, const uint8_t* __restrict__ done) {
-    extern __shared__ double shd[];   // th [T + 12], ac [T + 12], x [T]
+    extern __shared__ double shd[];   // th [T + 12], ac [T + 12], x [T], Ls [5 T]
     const int b = blockIdx.x / D, d = blockIdx.x % D;
     if (done[b]) return;
     const int Np = T + 12;
     double* th = shd;
     double* ac = th + Np;
     double* x = ac + Np;
+    double* Ls = x + T;   // the factor, staged so that the serial solve reads shared memory
+    for (int k = threadIdx.x; k < 5 * T; k += blockDim.x) Ls[k] = L[k];
     float* col = theta + (size_t)b * T * D + d;   // stride D
     for (int k = threadIdx.x; k < Np; k += blockDim.x) {
         const int t = k - 6;
@@ -242,13 +249,13 @@ __global__ void chomp_update_kernel(float* __restrict__ theta, const float* __re
     if (threadIdx.x == 0) {
         for (int i = 0; i < T; ++i) {   // L y = g
             double s = x[i];
-            for (int j = max(0, i - kBand); j < i; ++j) s -= L[i * 5 + (i - j)] * x[j];
-            x[i] = s * L[i * 5];
+            for (int j = max(0, i - kBand); j < i; ++j) s -= Ls[i * 5 + (i - j)] * x[j];
+            x[i] = s * Ls[i * 5];
         }
         for (int i = T - 1; i >= 0; --i) {   // L^T x = y
             double s = x[i];
-            for (int j = i + 1; j <= min(T - 1, i + kBand); ++j) s -= L[j * 5 + (j - i)] * x[j];
-            x[i] = s * L[i * 5];
+            for (int j = i + 1; j <= min(T - 1, i + kBand); ++j) s -= Ls[j * 5 + (j - i)] * x[j];
+            x[i] = s * Ls[i * 5];
         }
     }
     __syncthreads();
@@ -404,19 +411,22 @@ extern "C" int ps_chomp_optimize(const ps_model* m, const ps_scene_view* scene, 
     if (bk_smem > 48 * 1024)
         PS_TRY_CUDA(cudaFuncSetAttribute(chomp_bookkeep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bk_smem));
     const int up_threads = std::min(T, 256);
-    const size_t up_smem = sizeof(double) * (3 * T + 24);
+    const size_t up_smem = sizeof(double) * (8 * T + 24);
+    if (up_smem > 48 * 1024)
+        PS_TRY_CUDA(cudaFuncSetAttribute(chomp_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)up_smem));
 
     // One iteration: evaluate the current iterate (cost, adjoint, validity,
     // bookkeeping), then step every unfinished trajectory. The step index
     // lives in the device state, so every iteration enqueues the same work.
     auto iteration = [&](cudaStream_t q) -> int {
         if (int rc = traj_cost_launch(m, scene, theta, B, T, &cp, w.wp, nullptr, w.grad, w.done, q)) return rc;
-        chomp_segments_kernel<<<B, 256, 0, q>>>(theta, T, D, P->collision_check_step, w.done, w.from, w.to, w.G);
+        if (int rc = ps_check_configs(m, scene, theta, B * T, P->collision_margin, cfg_flags, w.hit, nullptr, q))
+            return rc;
+        chomp_segments_kernel<<<B, 256, 0, q>>>(theta, T, D, P->collision_check_step, w.done, w.hit, w.from, w.to,
+                                                w.G);
         PS_TRY_CUDA(cudaGetLastError());
         if (int rc = ps_check_edges(m, scene, w.from, w.to, w.G, E, &ep, w.evalid, w.ecost, nullptr, w.ews,
                                     w.ews_bytes, q))
-            return rc;
-        if (int rc = ps_check_configs(m, scene, theta, B * T, P->collision_margin, cfg_flags, w.hit, nullptr, q))
             return rc;
         chomp_bookkeep_kernel<<<B, bk_threads, bk_smem, q>>>(theta, w.wp, w.evalid, w.hit, T, D, cp_total,
                                                              P->num_iterations, P->convergence_eps, P->time_limit_ms,
