@@ -14,7 +14,10 @@
  *     the caller. Pointers documented as "host" are plain host memory.
  *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
  *     Every compute call is asynchronous on that stream, allocates nothing and
- *     never synchronises, so it can be captured into a CUDA graph.
+ *     never synchronises, so it can be captured into a CUDA graph. The
+ *     optimiser loops (ps_chomp_optimize, ps_stomp_optimize) are the
+ *     exception: they capture and replay their own graph and synchronise the
+ *     stream between replays.
  *   - Calls on distinct streams are thread-safe: kernels use no mutable
  *     __device__ globals; all state lives in caller-owned buffers or in the
  *     immutable model object.
@@ -425,6 +428,84 @@ int ps_chomp_optimize(const ps_model* model, const ps_scene_view* scene,
                       float* best, uint8_t* solved, int* iterations,
                       float* best_cost, void* workspace, size_t workspace_bytes,
                       void* stream);
+
+/* =========================================================================
+ * Batched STOMP optimisation: B trajectories advance together on the
+ * device. Replaces the per-request host loop of STOMP::solve_runtime_scene
+ * (cpp/src/planning/stomp.cu:565-965) with its iteration semantics
+ * (stomp.cu:786-889):
+ *   rollouts: num_rollouts_new fresh noisy copies of the optimum
+ *   (theta + L z, endpoints pinned, clamped; all num_rollouts_new +
+ *   num_rollouts_old fresh on the first iteration), the num_rollouts_old
+ *   lowest-cost rollouts of the previous iteration, and the optimum itself;
+ *   per-rollout cost = state cost (the summed hinge of ps_rollout_costs) +
+ *   control_cost_weight theta_d^T R theta_d;
+ *   per (d, t) weights p_r = exp(-h (c_r - min) / (max - min)) / sum;
+ *   theta <- theta + M (sum_r p_r noise_r), endpoints pinned, unconditionally;
+ *   validity, best valid snapshot, polish budget and convergence streak as
+ *   in CHOMP.
+ * L L^T = (R + 1e-8 I)^-1 rescaled to max entry 1/T (times noise_scale) and
+ * M = (R + 1e-8 I)^-1 with columns scaled to max 1/T (stomp_precompute.cpp:
+ * 46-98) are applied as banded triangular solves with the factor of
+ * R + 1e-8 I: L = sqrt(c) J (Lb^-T) J and M x = (R + 1e-8 I)^-1 (s .* x),
+ * in FP64. The normal variates z come from Philox4x32-10 (Salmon et al.,
+ * SC 2011) keyed by `seed` with counter (t / 4, rollout * D + d, iteration),
+ * through Box-Muller: every request of a batch draws the same stream, as
+ * every reference solve draws its fixed seed (stomp.cu:707), so a request's
+ * result does not depend on the batch it is in. The reference draws from
+ * cuRAND XORWOW; the streams differ, the distribution is the same.
+ * ========================================================================= */
+typedef struct ps_stomp_params {
+    int   num_iterations;             /* STOMP_settings.hh (20)               */
+    int   num_iterations_after_valid; /* (3)                                  */
+    int   num_rollouts_new;           /* (30)                                 */
+    int   num_rollouts_old;           /* (20)                                 */
+    float delta_t;                    /* R time step (0.1)                    */
+    float control_cost_weight;        /* (0.1)                                */
+    float collision_cost_weight;      /* (20)                                 */
+    float exponentiated_cost_sensitivity; /* h (2.0)                          */
+    float world_margin;               /* world hinge band (0.02)              */
+    float self_margin;                /* self hinge band (0.01)               */
+    float convergence_eps;            /* (1e-4)                               */
+    float noise_scale;                /* factor on L (1.0)                    */
+    float collision_check_step;       /* validity densification (0.05)        */
+    float collision_margin;           /* validity radius margin (0)           */
+    int   include_self;               /* self hinge in the state cost (1)     */
+    int   check_self;                 /* self check in the validity (1)       */
+    float time_limit_ms;              /* > 0: device-time limit, 0: none      */
+    unsigned long long seed;          /* Philox key (reference seed 0x5be5)   */
+} ps_stomp_params;
+
+/* Device workspace for ps_stomp_optimize (caller allocates, 256-byte
+   aligned). 0 for invalid arguments. */
+size_t ps_stomp_workspace_bytes(const ps_model* model, int B, int T,
+                                const ps_stomp_params* params);
+
+/* Same arguments and outputs as ps_chomp_optimize: theta [B*T*D] device,
+   initial trajectories in, last iterate out (waypoints 0 and T-1 fixed);
+   best, solved, iterations, best_cost as there. 3 <= T <= 1024;
+   num_rollouts_new >= 1, num_rollouts_old >= 0, their sum + 1 <= 1024.
+   Synchronises the stream every 8 iterations; not capturable. */
+int ps_stomp_optimize(const ps_model* model, const ps_scene_view* scene,
+                      float* theta, int B, int T, const ps_stomp_params* params,
+                      float* best, uint8_t* solved, int* iterations,
+                      float* best_cost, void* workspace, size_t workspace_bytes,
+                      void* stream);
+
+/* Where the last iteration's rollouts sit inside the workspace (byte
+   offsets; diagnostics and tests). Rows are rollout-major over requests:
+   row = r * B + b, r = 0..rows-1 (new, then old, then the optimum). Each
+   iteration writes buffer (iteration & 1) of the double-buffered arrays. */
+typedef struct ps_stomp_layout {
+    int    rows;             /* num_rollouts_new + num_rollouts_old + 1      */
+    size_t rollouts[2];      /* float [rows*B][T][D]                         */
+    size_t noise;            /* float [rows*B][T][D], rollout - optimum      */
+    size_t state_cost[2];    /* float [rows*B][T]                            */
+    size_t row_total[2];     /* float [rows*B]: sum of state + control cost  */
+    size_t reuse_index;      /* int [B][num_rollouts_old]: rows reused       */
+} ps_stomp_layout;
+int ps_stomp_workspace_layout(const ps_model* model, int B, int T,
+                              const ps_stomp_params* params, ps_stomp_layout* out);
 
 /* =========================================================================
  * Diagnostics

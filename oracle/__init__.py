@@ -215,6 +215,8 @@ def load_ref():
                                              C.c_float, C.c_float, _fp, _fp, C.c_int]
         lib.ref_chomp_solve.argtypes = [C.c_void_p, C.c_void_p, _fp, _fp, C.c_int, C.c_int, C.c_void_p, _fp,
                                         _u8p, _ip, _fp, C.POINTER(C.c_double)]
+        lib.ref_stomp_solve.argtypes = [C.c_void_p, C.c_void_p, _fp, _fp, C.c_int, C.c_int, C.c_void_p, _fp,
+                                        _u8p, _ip, _fp, C.POINTER(C.c_double)]
         _ref = lib
     return _ref
 
@@ -312,6 +314,14 @@ class RefKernels:
         """CHOMP::solve_runtime_scene per request (chomp.cu:358-600).
         params: a ps_chomp_params ctypes structure. Returns (path [B,T,D],
         solved [B] u8, iterations [B] i32, final_total_cost [B], wall ms)."""
+        return self._solve(load_ref().ref_chomp_solve, starts, goals, T, params, "chomp_solve")
+
+    def stomp_solve(self, starts, goals, T, params):
+        """STOMP::solve_runtime_scene per request (stomp.cu:565-965), with a
+        ps_stomp_params structure; outputs as chomp_solve."""
+        return self._solve(load_ref().ref_stomp_solve, starts, goals, T, params, "stomp_solve")
+
+    def _solve(self, fn, starts, goals, T, params, what):
         st = _f32(starts).reshape(-1, self.n_dof)
         gl = _f32(goals).reshape(-1, self.n_dof)
         B = len(st)
@@ -320,9 +330,8 @@ class RefKernels:
         iters = np.zeros(B, np.int32)
         total = np.zeros(B, np.float32)
         ms = C.c_double(0)
-        _chk(load_ref().ref_chomp_solve(self.m, self.s, _ptr(st, _fp), _ptr(gl, _fp), B, int(T), C.byref(params),
-                                        _ptr(path, _fp), _ptr(solved, _u8p), _ptr(iters, _ip), _ptr(total, _fp),
-                                        C.byref(ms)), "chomp_solve")
+        _chk(fn(self.m, self.s, _ptr(st, _fp), _ptr(gl, _fp), B, int(T), C.byref(params), _ptr(path, _fp),
+                _ptr(solved, _u8p), _ptr(iters, _ip), _ptr(total, _fp), C.byref(ms)), what)
         return path, solved, iters, total, ms.value
 
     def stomp(self, rollouts_bdt, w, world_margin, self_margin, reps=1):

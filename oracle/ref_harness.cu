@@ -14,6 +14,8 @@
 //   STOMP stomp_state_cost_kernel                                (planning/stomp.cu:206-245)
 //   CHOMP::solve_runtime_scene with CHOMPBuffers                 (planning/chomp.cu:358-600,
 //                                                                 planning/chomp_buffers.cu)
+//   STOMP::solve_runtime_scene with STOMPBuffers                 (planning/stomp.cu:565-965,
+//                                                                 planning/stomp_buffers.cu)
 //   ppln::collision::fk_runtime, transform_sphere_to_local,
 //   sphere_single_obb_collision, sphere_obb_clearance            (device functions, through
 //                                                                 the small wrapper kernels below)
@@ -24,6 +26,7 @@
 #include "src/planning/pRRTC.cu"
 #include "src/planning/chomp.cu"
 #include "src/planning/chomp_buffers.cu"
+#include "src/planning/stomp_buffers.cu"
 #include "src/planning/stomp.cu"
 #include "src/planning/edge_eval.cuh"
 
@@ -467,6 +470,53 @@ int ref_chomp_solve(void* mp, void* sp, const float* starts, const float* goals,
     const auto t1 = std::chrono::steady_clock::now();
     if (ms) *ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     const int rc = last_cuda("chomp_solve");
+    bufs.destroy();
+    return rc;
+}
+
+// STOMP::solve_runtime_scene once per request, with one STOMPBuffers set
+// reused across requests as stomp_plugin.py does. Same outputs as
+// ref_chomp_solve. The seed is the reference's own (its RNG init is fixed).
+int ref_stomp_solve(void* mp, void* sp, const float* starts, const float* goals, int B, int T,
+                    const ps_stomp_params* P, float* path, uint8_t* solved, int* iters, float* total,
+                    double* ms) {
+    RefModel* m = (RefModel*)mp;
+    RefScene* s = (RefScene*)sp;
+    ppln::RobotModel& mod = m->dev.model;
+    const int D = mod.n_dof;
+    STOMP_settings st;
+    st.num_timesteps = T;
+    st.num_iterations = P->num_iterations;
+    st.num_iterations_after_valid = P->num_iterations_after_valid;
+    st.num_rollouts_new = P->num_rollouts_new;
+    st.num_rollouts_old = P->num_rollouts_old;
+    st.delta_t = P->delta_t;
+    st.control_cost_weight = P->control_cost_weight;
+    st.collision_cost_weight = P->collision_cost_weight;
+    st.exponentiated_cost_sensitivity = P->exponentiated_cost_sensitivity;
+    st.world_collision_margin = P->world_margin;
+    st.self_collision_margin = P->self_margin;
+    st.convergence_eps = P->convergence_eps;
+    st.noise_scale = P->noise_scale;
+    st.collision_check_step = P->collision_check_step;
+    st.collision_margin = P->collision_margin;
+    st.time_limit_ms = P->time_limit_ms;
+    STOMPBuffers bufs = STOMPBuffers::create(D, T, st.num_rollouts_new, st.num_rollouts_old, 1);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int b = 0; b < B; ++b) {
+        std::vector<float> start(starts + (size_t)b * D, starts + (size_t)(b + 1) * D);
+        std::vector<std::vector<float>> gl(1, std::vector<float>(goals + (size_t)b * D, goals + (size_t)(b + 1) * D));
+        STOMPResult r = STOMP::solve_runtime_scene(start, gl, s->d, st, mod, &bufs);
+        for (int t = 0; t < T && t < (int)r.path.size(); ++t)
+            for (int d = 0; d < D; ++d) path[((size_t)b * T + t) * D + d] = r.path[t][d];
+        solved[b] = r.solved ? 1 : 0;
+        iters[b] = r.iterations_run;
+        total[b] = r.final_total_cost;
+    }
+    cudaDeviceSynchronize();
+    const auto t1 = std::chrono::steady_clock::now();
+    if (ms) *ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    const int rc = last_cuda("stomp_solve");
     bufs.destroy();
     return rc;
 }

@@ -5,7 +5,8 @@ Drop-in surface (names of the reference ``prrtc`` module and substrate):
 ``check_collision_scene``, ``EdgeEvalGpu``, ``load_robot_asset``,
 ``build_robot_model``; device-resident torch ops ``check_configs``,
 ``check_edges``, ``traj_cost``, ``rollout_costs``, ``hinge_cost``; the
-batched CHOMP optimiser ``chomp_solve`` / ``chomp_optimize``.
+batched optimisers ``chomp_solve`` / ``chomp_optimize`` and
+``stomp_solve`` / ``stomp_optimize``.
 The compute path is the CUDA library ``libprism_b200.so``; importing this
 package does not load it (so CPU-only tooling works), the first call does and
 fails loudly if it is missing.
@@ -18,6 +19,7 @@ from .api import (  # noqa: F401
     EdgeEvalGpu,
     EdgeEvalParams,
     MixedBatch,
+    StompSettings,
     check_collision_scene,
     check_configs,
     check_edges,
@@ -29,6 +31,9 @@ from .api import (  # noqa: F401
     fk_spheres,
     hinge_cost,
     rollout_costs,
+    stomp_optimize,
+    stomp_solve,
+    stomp_workspace,
     traj_cost,
 )
 from .robot import RobotModelBuilder, build_robot_model, load_robot_asset  # noqa: F401

@@ -131,6 +131,27 @@ class ChompParams(C.Structure):
     ]
 
 
+class StompParams(C.Structure):
+    _fields_ = [
+        ("num_iterations", C.c_int), ("num_iterations_after_valid", C.c_int),
+        ("num_rollouts_new", C.c_int), ("num_rollouts_old", C.c_int),
+        ("delta_t", C.c_float), ("control_cost_weight", C.c_float),
+        ("collision_cost_weight", C.c_float), ("exponentiated_cost_sensitivity", C.c_float),
+        ("world_margin", C.c_float), ("self_margin", C.c_float),
+        ("convergence_eps", C.c_float), ("noise_scale", C.c_float),
+        ("collision_check_step", C.c_float), ("collision_margin", C.c_float),
+        ("include_self", C.c_int), ("check_self", C.c_int),
+        ("time_limit_ms", C.c_float), ("seed", C.c_ulonglong),
+    ]
+
+
+class StompLayout(C.Structure):
+    _fields_ = [
+        ("rows", C.c_int), ("rollouts", C.c_size_t * 2), ("noise", C.c_size_t),
+        ("state_cost", C.c_size_t * 2), ("row_total", C.c_size_t * 2), ("reuse_index", C.c_size_t),
+    ]
+
+
 # (name, restype, argtypes)
 _SIGNATURES = [
     ("ps_last_error", C.c_char_p, []),
@@ -177,6 +198,12 @@ _SIGNATURES = [
     ("ps_chomp_workspace_bytes", C.c_size_t, [C.c_void_p, C.c_int, C.c_int]),
     ("ps_chomp_optimize", C.c_int,
      [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_int, C.c_int, C.POINTER(ChompParams),
+      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
+    ("ps_stomp_workspace_bytes", C.c_size_t, [C.c_void_p, C.c_int, C.c_int, C.POINTER(StompParams)]),
+    ("ps_stomp_workspace_layout", C.c_int,
+     [C.c_void_p, C.c_int, C.c_int, C.POINTER(StompParams), C.POINTER(StompLayout)]),
+    ("ps_stomp_optimize", C.c_int,
+     [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_int, C.c_int, C.POINTER(StompParams),
       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
     ("ps_fk_spheres", C.c_int,
      [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),

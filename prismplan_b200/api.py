@@ -475,6 +475,121 @@ def chomp_solve(robot: RobotModelBuilder, scene, starts, goals, settings: Option
 
 
 # ---------------------------------------------------------------------------
+# batched STOMP optimisation
+# ---------------------------------------------------------------------------
+@dataclass
+class StompSettings:
+    """STOMP settings with the reference's names and defaults
+    (cpp/src/planning/STOMP_settings.hh:17-59; time_limit_ms and
+    collision_margin from pRRTC_settings.hh:6,25). ``seed`` keys the noise
+    stream (the reference's fixed seed is 0x5be5, stomp.cu:707)."""
+
+    num_timesteps: int = 51
+    num_iterations: int = 20
+    num_iterations_after_valid: int = 3
+    num_rollouts_new: int = 30
+    num_rollouts_old: int = 20
+    delta_t: float = 0.1
+    control_cost_weight: float = 0.1
+    collision_cost_weight: float = 20.0
+    exponentiated_cost_sensitivity: float = 2.0
+    world_collision_margin: float = 0.02
+    self_collision_margin: float = 0.01
+    convergence_eps: float = 1.0e-4
+    noise_scale: float = 1.0
+    collision_check_step: float = 0.05
+    collision_margin: float = 0.0
+    time_limit_ms: float = 4000.0
+    include_self: bool = True
+    check_self: bool = True
+    seed: int = 0x5BE5
+
+    def to_c(self) -> _lib.StompParams:
+        p = _lib.StompParams()
+        p.num_iterations = int(self.num_iterations)
+        p.num_iterations_after_valid = int(self.num_iterations_after_valid)
+        p.num_rollouts_new = int(self.num_rollouts_new)
+        p.num_rollouts_old = int(self.num_rollouts_old)
+        p.delta_t = float(self.delta_t)
+        p.control_cost_weight = float(self.control_cost_weight)
+        p.collision_cost_weight = float(self.collision_cost_weight)
+        p.exponentiated_cost_sensitivity = float(self.exponentiated_cost_sensitivity)
+        p.world_margin = float(self.world_collision_margin)
+        p.self_margin = float(self.self_collision_margin)
+        p.convergence_eps = float(self.convergence_eps)
+        p.noise_scale = float(self.noise_scale)
+        p.collision_check_step = float(self.collision_check_step)
+        p.collision_margin = float(self.collision_margin)
+        p.include_self = int(bool(self.include_self))
+        p.check_self = int(bool(self.check_self))
+        p.time_limit_ms = float(self.time_limit_ms)
+        p.seed = int(self.seed) & 0xFFFFFFFFFFFFFFFF
+        return p
+
+
+def stomp_workspace(robot: RobotModelBuilder, B: int, T: int, settings: Optional[StompSettings] = None,
+                    device="cuda"):
+    torch = _torch()
+    p = (settings or StompSettings()).to_c()
+    nbytes = int(_lib.load().ps_stomp_workspace_bytes(_model(robot), int(B), int(T), C.byref(p)))
+    if nbytes == 0:
+        raise ValueError("invalid STOMP sizes")
+    return torch.empty(nbytes, dtype=torch.uint8, device=device)
+
+
+def stomp_layout(robot: RobotModelBuilder, B: int, T: int, settings: Optional[StompSettings] = None):
+    """Byte offsets of the last iteration's rollouts inside the workspace
+    (ps_stomp_workspace_layout), as a dict."""
+    p = (settings or StompSettings()).to_c()
+    lay = _lib.StompLayout()
+    _lib.check(_lib.load().ps_stomp_workspace_layout(_model(robot), int(B), int(T), C.byref(p), C.byref(lay)))
+    return {"rows": lay.rows, "rollouts": tuple(lay.rollouts), "noise": lay.noise,
+            "state_cost": tuple(lay.state_cost), "row_total": tuple(lay.row_total),
+            "reuse_index": lay.reuse_index}
+
+
+def stomp_optimize(robot: RobotModelBuilder, scene, theta, settings: Optional[StompSettings] = None,
+                   workspace=None, stream=None) -> ChompResult:
+    """Run STOMP on B trajectories ``theta`` [B, T, D] at once (the reference
+    runs one, stomp.cu:565-965). ``theta`` is updated in place when it is a
+    contiguous float32 CUDA tensor. Synchronises the stream every 8
+    iterations. Returns the CHOMPResult-like fields of STOMPResult."""
+    torch = _torch()
+    settings = settings or StompSettings()
+    th = _dev_f32(theta)
+    if th.dim() != 3 or th.shape[2] != robot.n_dof:
+        raise ValueError("theta must be [B, T, n_dof]")
+    B, T, D = th.shape
+    best = torch.empty_like(th)
+    solved = torch.empty(B, dtype=torch.uint8, device=th.device)
+    iters = torch.empty(B, dtype=torch.int32, device=th.device)
+    cost = torch.empty(B, dtype=torch.float32, device=th.device)
+    p = settings.to_c()
+    if workspace is None:
+        nbytes = int(_lib.load().ps_stomp_workspace_bytes(_model(robot), B, T, C.byref(p)))
+        workspace = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=th.device)
+    v = _view(scene)
+    _lib.check(_lib.load().ps_stomp_optimize(_model(robot), C.byref(v), th.data_ptr(), B, T, C.byref(p),
+                                             best.data_ptr(), solved.data_ptr(), iters.data_ptr(),
+                                             cost.data_ptr(), workspace.data_ptr(), workspace.numel(),
+                                             _stream(stream)))
+    return ChompResult(best, solved.bool(), iters, cost, th)
+
+
+def stomp_solve(robot: RobotModelBuilder, scene, starts, goals, settings: Optional[StompSettings] = None,
+                stream=None, workspace=None) -> ChompResult:
+    """STOMP::solve_runtime_scene for B (start, goal) pairs: straight-line
+    initialisation (stomp.cu:60-74), the optimiser loop, and the path's first
+    and last waypoints set to start and goal (stomp.cu:897-904)."""
+    settings = settings or StompSettings()
+    theta = chomp_linear_init(robot, starts, goals, settings.num_timesteps)
+    res = stomp_optimize(robot, scene, theta, settings, workspace=workspace, stream=stream)
+    res.path[:, 0, :] = _dev_f32(starts, robot.n_dof).reshape(-1, robot.n_dof)
+    res.path[:, -1, :] = _dev_f32(goals, robot.n_dof).reshape(-1, robot.n_dof)
+    return res
+
+
+# ---------------------------------------------------------------------------
 # mixed-request batches
 # ---------------------------------------------------------------------------
 class MixedBatch:

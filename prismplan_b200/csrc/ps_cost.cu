@@ -37,8 +37,9 @@ size_t cost_block_smem(const ps_model* m, const ps_scene_view* sv, bool grad) {
 // kGrad: also the adjoint; kStats: count executed work. Output layouts follow
 // ps_cost_params.layout. Gradients run tiles of 1 (the cull is cheap next to
 // the adjoint), rollouts tiles of kCostTile (smooth rollouts share boxes).
-// skip (tiles of 1 only; may be NULL): rows b with skip[b] != 0 are left
-// untouched.
+// skip (may be NULL): rows b with skip[b] != 0 need no output; a tile is
+// skipped when every row it touches is, so a skipped row that shares a tile
+// with a live one is evaluated all the same (with the same bits).
 template <bool kGrad, bool kStats, int kTile>
 __global__ void __launch_bounds__(kCostWarps * 32, 3) waypoint_cost_kernel(
     ModelDev md, ps_scene_view sv, const float* __restrict__ q, int n_rows, int T, ps_cost_params P,
@@ -72,7 +73,11 @@ __global__ void __launch_bounds__(kCostWarps * 32, 3) waypoint_cost_kernel(
          tile += (long long)gridDim.x * kCostWarps) {
         const long long idx0 = tile * kTile;
         const int nt = (int)min((long long)kTile, total - idx0);
-        if (kTile == 1 && skip && skip[idx0 / T]) continue;   // uniform over the warp
+        if (skip) {   // uniform over the warp
+            bool all = true;
+            for (long long r = idx0 / T; r <= (idx0 + nt - 1) / T; ++r) all = all && skip[r] != 0;
+            if (all) continue;
+        }
         for (int t = 0; t < nt; ++t) {
             const long long idx = idx0 + t;
             const int b = (int)(idx / T);
@@ -170,7 +175,6 @@ int ps::traj_cost_launch(const ps_model* m, const ps_scene_view* scene, const fl
     if (B == 0 || T == 0) return PS_OK;
     if (T > PS_MAX_TRAJ_LEN && (traj_cost || (grad && P->smoothness_weight != 0.0f)))
         return set_error(PS_EINVAL, "T exceeds PS_MAX_TRAJ_LEN for the smoothness term");
-    if (skip && !grad) return set_error(PS_EINVAL, "row skipping needs the gradient kernel");
     const long long total = (long long)B * T;
     const bool atomic_traj = traj_cost && !waypoint_cost;
     if (atomic_traj) PS_TRY_CUDA(cudaMemsetAsync(traj_cost, 0, sizeof(float) * B, s));
@@ -190,7 +194,7 @@ int ps::traj_cost_launch(const ps_model* m, const ps_scene_view* scene, const fl
         if (grid < 0) return PS_EINVAL;
         mark_start(s);
         k<<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
-                                              atomic_traj ? traj_cost : nullptr, nullptr, g_stats, nullptr);
+                                              atomic_traj ? traj_cost : nullptr, nullptr, g_stats, skip);
         mark_stop(s);
     }
     PS_TRY_CUDA(cudaGetLastError());

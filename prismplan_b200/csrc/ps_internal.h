@@ -39,9 +39,9 @@ int cuda_error(cudaError_t e, const char* where);
 void clear_error();
 
 // Trajectory cost launcher behind ps_traj_cost (same arguments, stream
-// typed). skip (device [B] or NULL, gradient launches only): trajectories b
-// with skip[b] != 0 are left untouched, which the batched optimiser uses for
-// trajectories that have finished.
+// typed). skip (device [B] or NULL): trajectories b with skip[b] != 0 need
+// no output (the batched optimisers skip finished requests this way); their
+// outputs may still be written, with the values an unskipped launch writes.
 int traj_cost_launch(const ps_model* m, const ps_scene_view* scene, const float* q, int B, int T,
                      const ps_cost_params* P, float* waypoint_cost, float* traj_cost, float* grad,
                      const uint8_t* skip, cudaStream_t s);

@@ -34,7 +34,8 @@ def test_binding_loads_and_reports_version():
 STRUCTS = {   # ctypes mirror -> C struct of include/prism_b200.h
     "ModelDesc": "ps_model_desc", "ModelInfo": "ps_model_info", "SceneView": "ps_scene_view",
     "EdgeParams": "ps_edge_params", "CostParams": "ps_cost_params", "BatchLimits": "ps_batch_limits",
-    "BatchTuning": "ps_batch_tuning", "ChompParams": "ps_chomp_params",
+    "BatchTuning": "ps_batch_tuning", "ChompParams": "ps_chomp_params", "StompParams": "ps_stomp_params",
+    "StompLayout": "ps_stomp_layout",
 }
 
 
