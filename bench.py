@@ -337,6 +337,7 @@ def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev):
     res["configs"] = bench_configs(dev)
     res["chomp"] = bench_chomp(dev)
     res["chomp_solve"] = bench_chomp_solve(dev)
+    res["stomp_solve"] = bench_stomp_solve(dev)
     res["stomp"] = bench_stomp(dev)
     res["mixed"] = bench_mixed(dev)
     return res
@@ -547,13 +548,9 @@ def reference_asset(name: str):
     return out
 
 
-def bench_chomp_solve(dev, with_ref=True, ref_sample=16):
-    """CHOMP optimisation of 256 planning requests on the reference's Panda
-    (59 spheres) among 16 random OBBs, T = 64 waypoints, the reference's
-    default settings otherwise; both endpoints of every request are
-    collision-free. One batched device loop (ps_chomp_optimize) against the
-    reference's one-request-at-a-time CHOMP::solve_runtime_scene, timed on a
-    bounded sample of the same requests."""
+def _solve_case(dev, B, T):
+    """The optimiser workload: the reference's Panda (59 spheres) among 16
+    random OBBs, B requests whose endpoints are both collision-free."""
     import torch
 
     from prismplan_b200 import api, workloads
@@ -570,30 +567,45 @@ def bench_chomp_solve(dev, with_ref=True, ref_sample=16):
         hit, _ = api.check_configs(b, sc, torch.from_numpy(q).to(dev), check_self=True)
         return hit.cpu().numpy() == 0
 
-    B, T = 256, 64
     starts, goals = workloads.free_pairs(rng, asset, B, is_free)
-    s = api.ChompSettings(num_timesteps=T, time_limit_ms=0.0)
+    return b, sc, obbs, starts, goals
+
+
+def _bench_solver(dev, kind, with_ref, ref_sample):
+    import torch
+
+    from prismplan_b200 import api
+
+    B, T = 256, 64
+    b, sc, obbs, starts, goals = _solve_case(dev, B, T)
+    if kind == "chomp":
+        s = api.ChompSettings(num_timesteps=T, time_limit_ms=0.0)
+        ws = api.chomp_workspace(b, B, T, dev)
+        opt = api.chomp_optimize
+    else:
+        s = api.StompSettings(num_timesteps=T, time_limit_ms=0.0)
+        ws = api.stomp_workspace(b, B, T, s, dev)
+        opt = api.stomp_optimize
     theta0 = api.chomp_linear_init(b, starts, goals, T)
-    ws = api.chomp_workspace(b, B, T, dev)
     res = None
     for _ in range(2):
-        res = api.chomp_optimize(b, sc, theta0.clone(), s, workspace=ws)
+        res = opt(b, sc, theta0.clone(), s, workspace=ws)
     torch.cuda.synchronize()
     reps = 3
     th = [theta0.clone() for _ in range(reps)]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for i in range(reps):
-        res = api.chomp_optimize(b, sc, th[i], s, workspace=ws)
+        res = opt(b, sc, th[i], s, workspace=ws)
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
     iters = res.iterations.cpu().numpy()
     solved = res.solved.cpu().numpy()
-    out = {"workload": "chomp_solve_panda_obb16_b256_t64", "value": B / (ms * 1e-3), "unit": "requests/s",
+    out = {"workload": f"{kind}_solve_panda_obb16_b{B}_t{T}", "value": B / (ms * 1e-3), "unit": "requests/s",
            "ms_per_step": ms, "solved": int(solved.sum()), "requests": B, "mean_iterations": float(iters.mean()),
            "max_iterations": int(iters.max()),
-           "path": "ps_chomp_optimize: 256 requests per call, CUDA-graph chunks of 8 iterations"}
+           "path": f"ps_{kind}_optimize: {B} requests per call, CUDA-graph chunks of 8 iterations"}
     if not with_ref:
         return out
     try:
@@ -601,10 +613,12 @@ def bench_chomp_solve(dev, with_ref=True, ref_sample=16):
 
         ref = oracle.RefKernels(b, *obbs)
         n = min(ref_sample, B)
-        ref.chomp_solve(starts[:1], goals[:1], T, s.to_c())
-        _, rsolved, riters, _, rms = ref.chomp_solve(starts[:n], goals[:n], T, s.to_c())
+        fn = ref.chomp_solve if kind == "chomp" else ref.stomp_solve
+        fn(starts[:1], goals[:1], T, s.to_c())
+        _, rsolved, riters, _, rms = fn(starts[:n], goals[:n], T, s.to_c())
         out["reference_gpu"] = {"value": n / (rms * 1e-3), "unit": "requests/s", "ms_per_request": rms / n,
-                                "sample": f"first {n} of the {B} requests, one CHOMP::solve_runtime_scene each",
+                                "sample": f"first {n} of the {B} requests, one {kind.upper()}::solve_runtime_scene "
+                                          "each",
                                 "solved": int(rsolved.sum()), "mean_iterations": float(riters.mean()),
                                 "device_solved_same_sample": int(solved[:n].sum()),
                                 "device_mean_iterations_same_sample": float(iters[:n].mean())}
@@ -612,6 +626,22 @@ def bench_chomp_solve(dev, with_ref=True, ref_sample=16):
     except Exception as e:
         out["reference_gpu"] = {"unavailable": str(e)[:200]}
     return out
+
+
+def bench_chomp_solve(dev, with_ref=True, ref_sample=16):
+    """CHOMP optimisation of 256 planning requests (T = 64, the reference's
+    default settings otherwise) in one batched device loop
+    (ps_chomp_optimize), against the reference's one-request-at-a-time
+    CHOMP::solve_runtime_scene timed on a bounded sample of the same
+    requests."""
+    return _bench_solver(dev, "chomp", with_ref, ref_sample)
+
+
+def bench_stomp_solve(dev, with_ref=True, ref_sample=16):
+    """STOMP optimisation of the same 256 requests (T = 64, 30 + 20 rollouts,
+    the reference's default settings otherwise) in one batched device loop
+    (ps_stomp_optimize), against STOMP::solve_runtime_scene on a sample."""
+    return _bench_solver(dev, "stomp", with_ref, ref_sample)
 
 
 def bench_stomp(dev, with_ref=True):
@@ -799,7 +829,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--headline-only", action="store_true",
                     help="time the headline path only (profiling runs); skips roofline/e2e/baselines")
-    ap.add_argument("--case", choices=["configs", "chomp", "chomp_solve", "stomp", "mixed"],
+    ap.add_argument("--case", choices=["configs", "chomp", "chomp_solve", "stomp", "stomp_solve", "mixed"],
                     help="run one secondary workload alone on cuda:0 and print its line (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -808,7 +838,7 @@ def main():
 
         dev = torch.device("cuda", 0)
         fn = {"configs": bench_configs, "chomp": bench_chomp, "chomp_solve": bench_chomp_solve, "stomp": bench_stomp,
-              "mixed": bench_mixed}[args.case]
+              "stomp_solve": bench_stomp_solve, "mixed": bench_mixed}[args.case]
         print(json.dumps({"case": args.case, **fn(dev, with_ref=False)}), flush=True)
         return
     res = run_reference(args) if args.impl == "reference" else run_ours(args)
