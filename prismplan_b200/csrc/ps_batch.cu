@@ -222,8 +222,8 @@ struct LaunchPlan {
     void (*qk)(ModelDev, ps_scene_view, ps_edge_params, const float*, const float*, int, EdgeWs*, const int*, int*,
                int*, int*, unsigned long long*, int, const int*) = nullptr;
     void (*wk)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*) = nullptr;
-    size_t qsmem = 0, wsmem = 0, fsmem = 0;
-    int qgrid = 1, wgrid = 1, req_grid_e = 1, req_grid_t = 1, pgrid = 1;
+    size_t qsmem = 0, wsmem = 0, fsmem = 0, ssmem = 0;
+    int qgrid = 1, wgrid = 1, req_grid_e = 1, req_grid_t = 1, pgrid = 1, sgrid = 1;
 };
 
 using WaypointKernel = void (*)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*);
@@ -250,6 +250,16 @@ int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, 
         L.qgrid = std::max(1, (int)(b->edge_share * sms * per_sm + 0.5f));
         L.pgrid = std::max(1, std::min((b->lim.max_edges + 255) / 256, sms * 4));
         L.req_grid_e = std::max(1, std::min(b->lim.max_edge_requests, sms * 8));
+        if (ep->check_self) {
+            L.ssmem = self_smem_bytes(m);
+            PS_TRY_CUDA(cudaFuncSetAttribute(edges_self_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)L.ssmem));
+            int s_per_sm = 0;
+            PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s_per_sm, edges_self_kernel, kSelfThreads,
+                                                                      L.ssmem));
+            if (s_per_sm < 1) return set_error(PS_EINVAL, "self-check kernel does not fit on an SM with this model");
+            L.sgrid = std::max(1, std::min(b->lim.max_edges, (int)(b->edge_share * sms * s_per_sm + 0.5f)));
+        }
     }
     if (b->lim.max_waypoints > 0) {
         const int tt = b->traj_threads;
@@ -292,6 +302,10 @@ void record_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep
                                                     b->d_G, b->d_bad, b->d_clr, b->d_done, nullptr, 0, n_dev);
         L.qk<<<L.qgrid, kEdgeThreads, L.qsmem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to, b->lim.max_edges, b->d_hdr,
                                                     b->d_G, b->d_bad, b->d_clr, b->d_done, nullptr, 1, n_dev);
+        if (ep->check_self)
+            edges_self_kernel<<<L.sgrid, kSelfThreads, L.ssmem, s0>>>(m->dev, *ep, b->d_from, b->d_to, b->d_given,
+                                                                      b->lim.max_edges, b->d_G, b->d_bad, nullptr,
+                                                                      nullptr, b->d_hdr, nullptr, n_dev);
         edges_finalize_kernel<<<L.pgrid, 256, 0, s0>>>(b->lim.max_edges, *ep, b->d_bad, b->d_len, b->d_clr, b->d_done,
                                                        b->d_G, b->d_hdr, b->d_valid, b->d_cost, nullptr, n_dev);
         batch_scatter_edges<<<L.req_grid_e, 128, 0, s0>>>(b->d_ereq, b->d_cnt, b->d_valid, b->d_cost);

@@ -299,10 +299,8 @@ __global__ void __launch_bounds__(kCfgThreads, 4) check_configs_fast_kernel(Mode
     if (kStats) flush_stats(stats, st);
 }
 
-// Self-collision two-phase check, one configuration per lane, positions of
-// every exact and approximate sphere staged in shared memory (SoA by lane).
-constexpr int kSelfThreads = 64;
-
+// Self-collision two-phase check, one configuration per lane
+// (lane_self_hit), for the configurations without a scene hit.
 __global__ void __launch_bounds__(kSelfThreads) self_check_kernel(ModelDev md, const float* __restrict__ q, int n,
                                                                   uint8_t* __restrict__ hit_out,
                                                                   unsigned long long* stats) {
@@ -311,7 +309,7 @@ __global__ void __launch_bounds__(kSelfThreads) self_check_kernel(ModelDev md, c
     unsigned char* blob = smem;
     if (!stage_model(md, blob, &mbar)) return;
     const ModelSmem M = model_view(blob);
-    const int D = M.H->n_dof, NJ = M.H->n_joints, NS = M.H->n_spheres, NA = M.H->n_approx;
+    const int D = M.H->n_dof, NS = M.H->n_spheres, NA = M.H->n_approx;
     float* pos = reinterpret_cast<float*>(smem + md.bytes_core);        // [NS*3][kSelfThreads]
     float* apos = pos + (size_t)NS * 3 * kSelfThreads;                   // [NA*3][kSelfThreads]
     float* qtile = apos + (size_t)NA * 3 * kSelfThreads;
@@ -325,69 +323,7 @@ __global__ void __launch_bounds__(kSelfThreads) self_check_kernel(ModelDev md, c
         __syncthreads();
         if (lane >= cnt) continue;
         if (hit_out[base + lane]) continue;   // already in collision with the scene
-        const float* qc = qtile + lane * D;
-        Affine s0, s1, T;
-        affine_identity(s0);
-        affine_identity(s1);
-        for (int p = 0; p < NJ; ++p) {
-            const JointRec& jr = M.J[p];
-            fk_step<true>(jr, p, qc, s0, s1, T);
-            for (int k = jr.sph_beg; k < jr.sph_end; ++k) {
-                const float4 s = M.S[k];
-                float px, py, pz;
-                sphere_world(T, s.x, s.y, s.z, px, py, pz);
-                pos[(k * 3 + 0) * kSelfThreads + lane] = px;
-                pos[(k * 3 + 1) * kSelfThreads + lane] = py;
-                pos[(k * 3 + 2) * kSelfThreads + lane] = pz;
-            }
-            if (M.H->approx_shares_chain) {
-                for (int k = jr.apx_beg; k < jr.apx_end; ++k) {
-                    const float4 s = M.A[k];
-                    float px, py, pz;
-                    sphere_world(T, s.x, s.y, s.z, px, py, pz);
-                    apos[(k * 3 + 0) * kSelfThreads + lane] = px;
-                    apos[(k * 3 + 1) * kSelfThreads + lane] = py;
-                    apos[(k * 3 + 2) * kSelfThreads + lane] = pz;
-                }
-            }
-        }
-        if (!M.H->approx_shares_chain) {
-            affine_identity(s0);
-            affine_identity(s1);
-            for (int p = 0; p < NJ; ++p) {
-                const JointRec& jr = M.JA[p];
-                fk_step<true>(jr, p, qc, s0, s1, T);
-                for (int k = jr.apx_beg; k < jr.apx_end; ++k) {
-                    const float4 s = M.A[k];
-                    float px, py, pz;
-                    sphere_world(T, s.x, s.y, s.z, px, py, pz);
-                    apos[(k * 3 + 0) * kSelfThreads + lane] = px;
-                    apos[(k * 3 + 1) * kSelfThreads + lane] = py;
-                    apos[(k * 3 + 2) * kSelfThreads + lane] = pz;
-                }
-            }
-        }
-        bool need = false;
-        for (int k = 0; k < M.H->n_apx_self_pairs && !need; ++k) {
-            const uint32_t pr = __ldg(md.apx_self_pairs + k);
-            const int i = pr & 0xffff, j = pr >> 16;
-            st.v[ST_SELF] += 1;
-            need = ref_self_hit(apos[(i * 3) * kSelfThreads + lane], apos[(i * 3 + 1) * kSelfThreads + lane],
-                                apos[(i * 3 + 2) * kSelfThreads + lane], M.A[i].w,
-                                apos[(j * 3) * kSelfThreads + lane], apos[(j * 3 + 1) * kSelfThreads + lane],
-                                apos[(j * 3 + 2) * kSelfThreads + lane], M.A[j].w);
-        }
-        bool hit = false;
-        for (int k = 0; need && k < M.H->n_self_pairs && !hit; ++k) {
-            const uint32_t pr = __ldg(md.self_pairs + k);
-            const int i = pr & 0xffff, j = pr >> 16;
-            st.v[ST_SELF] += 1;
-            hit = ref_self_hit(pos[(i * 3) * kSelfThreads + lane], pos[(i * 3 + 1) * kSelfThreads + lane],
-                               pos[(i * 3 + 2) * kSelfThreads + lane], M.S[i].w, pos[(j * 3) * kSelfThreads + lane],
-                               pos[(j * 3 + 1) * kSelfThreads + lane], pos[(j * 3 + 2) * kSelfThreads + lane],
-                               M.S[j].w);
-        }
-        if (hit) hit_out[base + lane] = 1;
+        if (lane_self_hit<kSelfThreads>(M, md, qtile + lane * D, pos, apos, lane, st)) hit_out[base + lane] = 1;
     }
     flush_stats(stats, st);
 }
@@ -484,9 +420,7 @@ extern "C" int ps_check_configs(const ps_model* m, const ps_scene_view* scene, c
     mark_stop(s);
     PS_TRY_CUDA(cudaGetLastError());
     if (flags & PS_CHECK_SELF) {
-        size_t ss = (size_t)m->dev.bytes_core +
-                    (size_t)(m->info.n_spheres + m->info.n_approx_spheres) * 3 * kSelfThreads * 4 +
-                    (size_t)kSelfThreads * m->info.n_dof * 4;
+        const size_t ss = self_smem_bytes(m);
         PS_TRY_CUDA(cudaFuncSetAttribute(self_check_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
         const int g2 = std::max(1, std::min((n + kSelfThreads - 1) / kSelfThreads, sm_count() * 8));
         self_check_kernel<<<g2, kSelfThreads, ss, s>>>(m->dev, q, n, hit, g_stats);

@@ -660,9 +660,85 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_queue_kerne
     flush_stats(stats, st);
 }
 
+// Self-collision pass of the edge checks (check_self: edge_eval.cuh:128 runs
+// two_phase_cc with params.check_self for every sample). After the scene
+// pass, each edge without a scene hit gets the self verdict of every sample
+// of the scene pass' set (t = j/G for j = 1..G, and j = 0 when G % 16 != 0),
+// one sample per thread of a kSelfThreads block, the edge's samples in
+// blocks of kSelfThreads with an exit at the first hit (lane_self_hit).
+// Persistent mode (bad != nullptr): bad[e] goes from 0 to 1 (self hit) or 2
+// (checked, free); an edge still at 0 after a deadline comes back invalid.
+// Plain mode (valid, cost): a self hit turns a free edge invalid.
+__global__ void __launch_bounds__(kSelfThreads) edges_self_kernel(ModelDev md, ps_edge_params P,
+                                                                  const float* __restrict__ from,
+                                                                  const float* __restrict__ to,
+                                                                  const int* __restrict__ given, int n_edges,
+                                                                  const int* __restrict__ Gs, int* bad,
+                                                                  uint8_t* valid, float* cost, EdgeWs* hdr,
+                                                                  unsigned long long* stats,
+                                                                  const int* n_dev = nullptr) {
+    if (n_dev) n_edges = *n_dev;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ int s_stop;
+    if (!stage_model(md, smem, &mbar)) return;
+    const ModelSmem M = model_view(smem);
+    const int D = M.H->n_dof, NS = M.H->n_spheres, NA = M.H->n_approx;
+    float* pos = reinterpret_cast<float*>(smem + md.bytes_core);   // [NS*3][kSelfThreads]
+    float* apos = pos + (size_t)NS * 3 * kSelfThreads;              // [NA*3][kSelfThreads]
+    float* qc = apos + (size_t)NA * 3 * kSelfThreads + threadIdx.x * D;
+    const bool persistent = bad != nullptr;
+    const unsigned long long deadline = hdr ? *((volatile unsigned long long*)&hdr->deadline) : 0ull;
+    const int lane = threadIdx.x;
+    LaneStats st;
+    st.zero();
+    for (int e = blockIdx.x; e < n_edges; e += gridDim.x) {
+        if (persistent ? bad[e] != 0 : valid[e] == 0) continue;   // uniform over the block
+        if (deadline) {
+            __syncthreads();
+            if (lane == 0) s_stop = global_ns() > deadline;
+            __syncthreads();
+            if (s_stop) {
+                if (lane == 0) atomicExch(&hdr->timed_out, 1);
+                break;
+            }
+        }
+        const float* a = from + (size_t)e * D;
+        const float* b = to + (size_t)e * D;
+        const int G = persistent ? Gs[e] : edge_samples(P, given, e, a, b, D, edge_length(a, b, D));
+        const int n_s = G + ((G % 16) != 0 ? 1 : 0);
+        bool hit_any = false;
+        for (int base = 0; base < n_s && !hit_any; base += kSelfThreads) {
+            const int idx = base + lane;
+            bool hit = false;
+            if (idx < n_s) {
+                const int j = idx < G ? idx + 1 : 0;
+                const float t = __fdiv_rn((float)j, (float)G);
+                for (int i = 0; i < D; ++i) {
+                    const float ai = __ldg(a + i), bi = __ldg(b + i);
+                    qc[i] = __fmaf_rn(t, __fadd_rn(bi, -ai), ai);
+                }
+                st.v[ST_SAMPLES] += 1;
+                hit = lane_self_hit<kSelfThreads>(M, md, qc, pos, apos, lane, st);
+            }
+            hit_any = __syncthreads_or(hit) != 0;
+        }
+        if (lane == 0) {
+            if (persistent) {
+                bad[e] = hit_any ? 1 : 2;
+            } else if (hit_any) {
+                valid[e] = 0;
+                cost[e] = FLT_MAX;
+            }
+        }
+    }
+    flush_stats(stats, st);
+}
+
 // After a timeout an edge that is neither retired nor complete comes back
 // invalid (cost FLT_MAX): not shown free. Its clearance is the min over the
-// samples that were checked.
+// samples that were checked. With check_self an edge is free only when the
+// self pass marked it so (bad == 2).
 __global__ void edges_finalize_kernel(int n_edges, const ps_edge_params P, const int* __restrict__ bad,
                                       const float* __restrict__ len, const int* __restrict__ clr,
                                       const int* __restrict__ done, const int* __restrict__ Gs, const EdgeWs* hdr,
@@ -671,7 +747,8 @@ __global__ void edges_finalize_kernel(int n_edges, const ps_edge_params P, const
     if (n_dev) n_edges = *n_dev;
     const bool timed_out = hdr->timed_out != 0;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_edges; e += gridDim.x * blockDim.x) {
-        const bool b = bad[e] != 0 || (timed_out && done[e] < ChunkOrder(Gs[e]).nc);
+        const int bv = bad[e];
+        const bool b = (P.check_self ? bv != 2 : bv != 0) || (timed_out && done[e] < ChunkOrder(Gs[e]).nc);
         valid[e] = b ? 0 : 1;
         cost[e] = b ? FLT_MAX : len[e];
         if (clearance) clearance[e] = P.compute_clearance ? unordered_float(clr[e]) : FLT_MAX;
@@ -680,11 +757,31 @@ __global__ void edges_finalize_kernel(int n_edges, const ps_edge_params P, const
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Launches the self pass when params ask for it (a no-op otherwise). The grid
+// covers every SM at the kernel's occupancy; blocks stride over the edges.
+int launch_edges_self(const ps_model* m, const ps_edge_params* P, const float* from, const float* to,
+                      const int* given, int n_edges, const int* Gs, int* bad, uint8_t* valid, float* cost,
+                      EdgeWs* hdr, const int* n_dev, cudaStream_t s) {
+    if (!P->check_self || n_edges <= 0) return PS_OK;
+    const size_t smem = self_smem_bytes(m);
+    PS_TRY_CUDA(cudaFuncSetAttribute(edges_self_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edges_self_kernel, kSelfThreads, smem));
+    if (per_sm < 1) return set_error(PS_EINVAL, "self-check kernel does not fit on an SM with this model");
+    const int grid = std::max(1, std::min(n_edges, sm_count() * per_sm));
+    edges_self_kernel<<<grid, kSelfThreads, smem, s>>>(m->dev, *P, from, to, given, n_edges, Gs, bad, valid, cost,
+                                                       hdr, g_stats, n_dev);
+    PS_TRY_CUDA(cudaGetLastError());
+    return PS_OK;
+}
+
 
 
 // Kernel variant: 0 generic, 1 fast (boxes only), 2 fast with ESDF layers.
+// The self check (check_self) is a separate pass (edges_self_kernel) after
+// either variant.
 int fast_path(const ps_model* m, const ps_scene_view* sv, const ps_edge_params* P) {
-    const bool fast = m->info.approx_shares_chain && m->root_slot_only && !P->compute_clearance && !P->check_self &&
+    const bool fast = m->info.approx_shares_chain && m->root_slot_only && !P->compute_clearance &&
                       !sv->sphere_obb_acm_mask && !sv->sphere_obb_acm_mask_approx && !sv->sphere_acm_mask;
     return fast ? (sv->n_voxel_layers > 0 ? 2 : 1) : 0;
 }

@@ -59,7 +59,8 @@ extern "C" int ps_check_edges_plain(const ps_model* m, const ps_scene_view* scen
                                           clearance, g_stats);
     mark_stop(s);
     PS_TRY_CUDA(cudaGetLastError());
-    return PS_OK;
+    return launch_edges_self(m, P, from, to, samples_per_edge, n_edges, nullptr, nullptr, valid, cost, nullptr,
+                             nullptr, s);
 }
 
 extern "C" size_t ps_edges_workspace_bytes(int n_edges) {
@@ -117,6 +118,9 @@ int run_persistent(const ps_model* m, const ps_scene_view* scene, const float* f
                                              g_stats, 1, nullptr);
     mark_stop(s);
     PS_TRY_CUDA(cudaGetLastError());
+    if (int rc = launch_edges_self(m, P, from, to, samples_per_edge, n_edges, b.G, b.bad, nullptr, nullptr, b.hdr,
+                                   nullptr, s))
+        return rc;
     const int fgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
     edges_finalize_kernel<<<fgrid, 256, 0, s>>>(n_edges, *P, b.bad, b.len, b.clr, b.done, b.G, b.hdr, valid, cost,
                                                 clearance);

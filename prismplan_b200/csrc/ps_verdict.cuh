@@ -251,4 +251,87 @@ __device__ __forceinline__ void fk_step(const JointRec& jr, int p, const float* 
     store_slot(s0, s1, jr.slot, T);
 }
 
+// ---------------------------------------------------------------------------
+// Two-phase self check of one configuration per thread (two_phase_cc.cuh:
+// 108-131, runtime_kinematics.cuh:249-284 and 383-417): the approximate
+// sphere pairs first; the exact pairs only when an approximate pair
+// overlaps; the collision margin does not apply to self pairs. Positions of
+// every exact and approximate sphere are staged in shared memory, SoA by
+// thread: pos [n_spheres * 3][kLanes], apos [n_approx * 3][kLanes].
+// ---------------------------------------------------------------------------
+constexpr int kSelfThreads = 64;
+
+template <int kLanes>
+__device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const float* qc, float* pos, float* apos,
+                              int lane, LaneStats& st) {
+    const int NJ = M.H->n_joints;
+    Affine s0, s1, T;
+    affine_identity(s0);
+    affine_identity(s1);
+    for (int p = 0; p < NJ; ++p) {
+        const JointRec& jr = M.J[p];
+        fk_step<true>(jr, p, qc, s0, s1, T);
+        for (int k = jr.sph_beg; k < jr.sph_end; ++k) {
+            const float4 s = M.S[k];
+            float px, py, pz;
+            sphere_world(T, s.x, s.y, s.z, px, py, pz);
+            pos[(k * 3 + 0) * kLanes + lane] = px;
+            pos[(k * 3 + 1) * kLanes + lane] = py;
+            pos[(k * 3 + 2) * kLanes + lane] = pz;
+        }
+        if (M.H->approx_shares_chain) {
+            for (int k = jr.apx_beg; k < jr.apx_end; ++k) {
+                const float4 s = M.A[k];
+                float px, py, pz;
+                sphere_world(T, s.x, s.y, s.z, px, py, pz);
+                apos[(k * 3 + 0) * kLanes + lane] = px;
+                apos[(k * 3 + 1) * kLanes + lane] = py;
+                apos[(k * 3 + 2) * kLanes + lane] = pz;
+            }
+        }
+    }
+    if (!M.H->approx_shares_chain) {
+        affine_identity(s0);
+        affine_identity(s1);
+        for (int p = 0; p < NJ; ++p) {
+            const JointRec& jr = M.JA[p];
+            fk_step<true>(jr, p, qc, s0, s1, T);
+            for (int k = jr.apx_beg; k < jr.apx_end; ++k) {
+                const float4 s = M.A[k];
+                float px, py, pz;
+                sphere_world(T, s.x, s.y, s.z, px, py, pz);
+                apos[(k * 3 + 0) * kLanes + lane] = px;
+                apos[(k * 3 + 1) * kLanes + lane] = py;
+                apos[(k * 3 + 2) * kLanes + lane] = pz;
+            }
+        }
+    }
+    bool need = false;
+    for (int k = 0; k < M.H->n_apx_self_pairs && !need; ++k) {
+        const uint32_t pr = __ldg(md.apx_self_pairs + k);
+        const int i = pr & 0xffff, j = pr >> 16;
+        st.v[ST_SELF] += 1;
+        need = ref_self_hit(apos[(i * 3) * kLanes + lane], apos[(i * 3 + 1) * kLanes + lane],
+                            apos[(i * 3 + 2) * kLanes + lane], M.A[i].w, apos[(j * 3) * kLanes + lane],
+                            apos[(j * 3 + 1) * kLanes + lane], apos[(j * 3 + 2) * kLanes + lane], M.A[j].w);
+    }
+    bool hit = false;
+    for (int k = 0; need && k < M.H->n_self_pairs && !hit; ++k) {
+        const uint32_t pr = __ldg(md.self_pairs + k);
+        const int i = pr & 0xffff, j = pr >> 16;
+        st.v[ST_SELF] += 1;
+        hit = ref_self_hit(pos[(i * 3) * kLanes + lane], pos[(i * 3 + 1) * kLanes + lane],
+                           pos[(i * 3 + 2) * kLanes + lane], M.S[i].w, pos[(j * 3) * kLanes + lane],
+                           pos[(j * 3 + 1) * kLanes + lane], pos[(j * 3 + 2) * kLanes + lane], M.S[j].w);
+    }
+    return hit;
+}
+
+// Shared memory of a kSelfThreads-lane block running lane_self_hit: model
+// core, sphere positions and a tile of configurations.
+inline size_t self_smem_bytes(const ps_model* m) {
+    return (size_t)m->dev.bytes_core + (size_t)(m->info.n_spheres + m->info.n_approx_spheres) * 3 * kSelfThreads * 4 +
+           (size_t)kSelfThreads * m->info.n_dof * 4;
+}
+
 }  // namespace ps

@@ -1,0 +1,100 @@
+"""Edge checks with the self check (check_self, edge_eval.cuh:40 and :128):
+every edge path (persistent, plain, static, mixed batch) against the
+reference's evaluate_edges_batch run with check_self on the same inputs, bit
+for bit, on the reference's Panda where a share of the edges is free of the
+scene but not of itself."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from conftest import golden_asset
+from prismplan_b200 import _lib, api, workloads
+from prismplan_b200.robot import RobotModelBuilder
+from prismplan_b200.scene import SceneTensors
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def case(golden):
+    asset, _ = golden_asset(golden, "panda")
+    rng = np.random.default_rng(2024)
+    obbs = workloads.random_obbs(rng, 8)
+    b = RobotModelBuilder.from_asset(asset).build()
+    sc = SceneTensors(*obbs)
+    frm, to, G = workloads.edge_batch(rng, asset, 3000, step=0.02, max_samples=300)
+    G[:7] = [0, 1, 15, 16, 17, 32, 33]   # zero samples, the start-sample rule (G % 16) and chunk edges
+    ref = oracle.RefKernels(b, *obbs)
+    return asset, obbs, b, sc, frm, to, G, ref
+
+
+def _static(b, sc, frm, to, G, p):
+    E = frm.shape[0]
+    v = torch.empty(E, dtype=torch.uint8, device="cuda")
+    c = torch.empty(E, dtype=torch.float32, device="cuda")
+    k = torch.empty(E, dtype=torch.float32, device="cuda")
+    pc = p.to_c()
+    view = sc.view()
+    _lib.check(_lib.load().ps_check_edges_static(b.handle, C.byref(view), frm.data_ptr(), to.data_ptr(),
+                                                 G.data_ptr(), E, C.byref(pc), v.data_ptr(), c.data_ptr(),
+                                                 k.data_ptr(), None))
+    return v, c
+
+
+def test_edges_self_bitexact_vs_reference(case):
+    asset, obbs, b, sc, frm, to, G, ref = case
+    rv_scene, _, _ = ref.check_edges(frm, to, G, check_self=False)
+    rv, rc, _ = ref.check_edges(frm, to, G, check_self=True)
+    only_self = (rv_scene == 1) & (rv == 0)
+    print(f"edges: {len(G)}, free of the scene {rv_scene.mean():.3f}, free {rv.mean():.3f}, "
+          f"invalid by self only {only_self.sum()}")
+    assert only_self.sum() > 20 and rv.sum() > 20
+    f, t, g = (torch.from_numpy(x).cuda() for x in (frm, to, G))
+    p = api.EdgeEvalParams(check_self=True)
+    outs = {
+        "persistent": api.check_edges(b, sc, f, t, samples=g, params=p)[:2],
+        "plain": api.check_edges(b, sc, f, t, samples=g, params=p, persistent=False)[:2],
+        "static": _static(b, sc, f, t, g, p),
+    }
+    for name, (v, c) in outs.items():
+        v, c = v.cpu().numpy(), c.cpu().numpy()
+        np.testing.assert_array_equal(v, rv, err_msg=name)
+        assert np.array_equal(c.view(np.uint32), rc.view(np.uint32)), name
+    # without the self check nothing changes
+    v0, c0, _ = api.check_edges(b, sc, f, t, samples=g, params=api.EdgeEvalParams(check_self=False))
+    np.testing.assert_array_equal(v0.cpu().numpy(), rv_scene)
+
+
+def test_batch_edges_with_self(case):
+    asset, obbs, b, sc, frm, to, G, ref = case
+    p = api.EdgeEvalParams(check_self=True)
+    n = len(G)
+    batch = api.MixedBatch(b, 3, n, 0, 0, 0)
+    cuts = [0, 700, 1900, n]
+    f, t, g = (torch.from_numpy(x).cuda() for x in (frm, to, G))
+    outs = [batch.add_edges(f[cuts[i]:cuts[i + 1]], t[cuts[i]:cuts[i + 1]], g[cuts[i]:cuts[i + 1]])
+            for i in range(3)]
+    batch.launch(sc, p, api.CostParams())
+    torch.cuda.synchronize()
+    v = torch.cat([o[0] for o in outs]).cpu().numpy()
+    c = torch.cat([o[1] for o in outs]).cpu().numpy()
+    rv, rc, _ = ref.check_edges(frm, to, G, check_self=True)
+    np.testing.assert_array_equal(v, rv)
+    assert np.array_equal(c.view(np.uint32), rc.view(np.uint32))
+    batch.close()
+
+
+def test_self_pass_respects_time_budget(case):
+    asset, obbs, b, sc, frm, to, G, ref = case
+    f, t, g = (torch.from_numpy(x).cuda() for x in (frm, to, G))
+    ws = api.edges_workspace(len(G))
+    rv, _, _ = ref.check_edges(frm, to, G, check_self=True)
+    v, c, _ = api.check_edges(b, sc, f, t, samples=g, workspace=ws,
+                              params=api.EdgeEvalParams(check_self=True, time_budget_ms=1e-6))
+    torch.cuda.synchronize()
+    assert api.edges_status(ws) == _lib.PS_ETIMEOUT
+    v = v.cpu().numpy()
+    assert not np.any((v == 1) & (rv == 0))   # never free when not shown free
