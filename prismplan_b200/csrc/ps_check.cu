@@ -309,10 +309,9 @@ __global__ void __launch_bounds__(kSelfThreads) self_check_kernel(ModelDev md, c
     unsigned char* blob = smem;
     if (!stage_model(md, blob, &mbar)) return;
     const ModelSmem M = model_view(blob);
-    const int D = M.H->n_dof, NS = M.H->n_spheres, NA = M.H->n_approx;
-    float* pos = reinterpret_cast<float*>(smem + md.bytes_core);        // [NS*3][kSelfThreads]
-    float* apos = pos + (size_t)NS * 3 * kSelfThreads;                   // [NA*3][kSelfThreads]
-    float* qtile = apos + (size_t)NA * 3 * kSelfThreads;
+    const int D = M.H->n_dof, NS = M.H->n_spheres, NA = M.H->n_approx, NJ = M.H->n_joints;
+    const SelfSmem sm = carve_self<kSelfThreads>(smem + md.bytes_core, NS, NA, NJ);
+    float* qtile = sm.cpos + (size_t)NJ * 3 * kSelfThreads;
     LaneStats st;
     st.zero();
     const int lane = threadIdx.x;
@@ -323,7 +322,7 @@ __global__ void __launch_bounds__(kSelfThreads) self_check_kernel(ModelDev md, c
         __syncthreads();
         if (lane >= cnt) continue;
         if (hit_out[base + lane]) continue;   // already in collision with the scene
-        if (lane_self_hit<kSelfThreads>(M, md, qtile + lane * D, pos, apos, lane, st)) hit_out[base + lane] = 1;
+        if (lane_self_hit<kSelfThreads>(M, md, qtile + lane * D, sm, lane, st)) hit_out[base + lane] = 1;
     }
     flush_stats(stats, st);
 }

@@ -20,9 +20,12 @@ constexpr unsigned kFull = 0xffffffffu;
 struct EdgeWs {                         // header of the persistent workspace (64 B)
     unsigned long long head[2];         // next chunk-major item of each pass
     unsigned long long deadline;        // %globaltimer deadline (ns), 0 = none
+    unsigned long long self_samples;    // samples of every edge (self pass sizing)
     int max_rounds;                     // most chunk rounds of any edge
     int timed_out;                      // set once a queue kernel stops at the deadline
-    int pad[8];
+    int self_edges;                     // edges with at least one sample
+    int self_next;                      // next window of the self pass
+    int pad[4];
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -541,7 +544,8 @@ __global__ void edges_prep_kernel(ps_edge_params P, const float* __restrict__ fr
         hdr->deadline = P.time_budget_ms > 0.0f
                             ? global_ns() + (unsigned long long)((double)P.time_budget_ms * 1.0e6) + 1ull
                             : 0ull;
-    int local_max = 0;
+    int local_max = 0, local_ne = 0;
+    unsigned long long local_ns = 0;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_edges; e += gridDim.x * blockDim.x) {
         const float* a = from + (size_t)e * D;
         const float* b = to + (size_t)e * D;
@@ -553,10 +557,20 @@ __global__ void edges_prep_kernel(ps_edge_params P, const float* __restrict__ fr
         clr[e] = ordered_float(FLT_MAX);
         done[e] = 0;
         local_max = max(local_max, ChunkOrder(G).rounds());
+        local_ns += (unsigned long long)(G + ((G % 16) != 0 ? 1 : 0));
+        local_ne += G > 0;
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) local_max = max(local_max, __shfl_xor_sync(kFull, local_max, o));
+    for (int o = 16; o > 0; o >>= 1) {
+        local_max = max(local_max, __shfl_xor_sync(kFull, local_max, o));
+        local_ns += __shfl_xor_sync(kFull, local_ns, o);
+        local_ne += __shfl_xor_sync(kFull, local_ne, o);
+    }
     if ((threadIdx.x & 31) == 0 && local_max > 0) atomicMax(&hdr->max_rounds, local_max);
+    if ((threadIdx.x & 31) == 0 && P.check_self && local_ns > 0) {
+        atomicAdd(&hdr->self_samples, local_ns);
+        atomicAdd(&hdr->self_edges, local_ne);
+    }
 }
 
 template <int kMode, bool kStats>
@@ -662,10 +676,15 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_queue_kerne
 
 // Self-collision pass of the edge checks (check_self: edge_eval.cuh:128 runs
 // two_phase_cc with params.check_self for every sample). After the scene
-// pass, each edge without a scene hit gets the self verdict of every sample
-// of the scene pass' set (t = j/G for j = 1..G, and j = 0 when G % 16 != 0),
-// one sample per thread of a kSelfThreads block, the edge's samples in
-// blocks of kSelfThreads with an exit at the first hit (lane_self_hit).
+// pass, each edge without a scene hit gets the self verdict (lane_self_hit)
+// of every sample of the scene pass' set: t = j/G for j = 1..G, and j = 0
+// when G % 16 != 0. A block takes a window of W consecutive edges, lays
+// their samples end to end and checks them kSelfThreads at a time, one per
+// thread; an edge's remaining samples are skipped after its first hit. W is
+// sized from the counts the prep kernel took (about kSelfThreads samples per
+// window over the edges that have samples): short edges share a block
+// instead of leaving its threads idle, long edges get a block each so that
+// every SM has work. With a workspace, blocks take windows from a counter.
 // Persistent mode (bad != nullptr): bad[e] goes from 0 to 1 (self hit) or 2
 // (checked, free); an edge still at 0 after a deadline comes back invalid.
 // Plain mode (valid, cost): a self hit turns a free edge invalid.
@@ -677,60 +696,105 @@ __global__ void __launch_bounds__(kSelfThreads) edges_self_kernel(ModelDev md, p
                                                                   uint8_t* valid, float* cost, EdgeWs* hdr,
                                                                   unsigned long long* stats,
                                                                   const int* n_dev = nullptr) {
+    static_assert(kSelfThreads == 64, "two-warp scan below");
     if (n_dev) n_edges = *n_dev;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar;
-    __shared__ int s_stop;
+    __shared__ int s_off[kSelfThreads + 1], s_G[kSelfThreads], s_hit[kSelfThreads], s_wsum[2], s_stop;
     if (!stage_model(md, smem, &mbar)) return;
     const ModelSmem M = model_view(smem);
-    const int D = M.H->n_dof, NS = M.H->n_spheres, NA = M.H->n_approx;
-    float* pos = reinterpret_cast<float*>(smem + md.bytes_core);   // [NS*3][kSelfThreads]
-    float* apos = pos + (size_t)NS * 3 * kSelfThreads;              // [NA*3][kSelfThreads]
-    float* qc = apos + (size_t)NA * 3 * kSelfThreads + threadIdx.x * D;
+    const int D = M.H->n_dof, NS = M.H->n_spheres, NA = M.H->n_approx, NJ = M.H->n_joints;
+    const SelfSmem sm = carve_self<kSelfThreads>(smem + md.bytes_core, NS, NA, NJ);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float* qc = sm.cpos + (size_t)NJ * 3 * kSelfThreads + tid * D;
     const bool persistent = bad != nullptr;
     const unsigned long long deadline = hdr ? *((volatile unsigned long long*)&hdr->deadline) : 0ull;
-    const int lane = threadIdx.x;
     LaneStats st;
     st.zero();
-    for (int e = blockIdx.x; e < n_edges; e += gridDim.x) {
-        if (persistent ? bad[e] != 0 : valid[e] == 0) continue;   // uniform over the block
-        if (deadline) {
+    bool stopped = false;
+    int W = 8;   // plain path: no sample count
+    if (hdr) {
+        const unsigned long long tot = *((volatile unsigned long long*)&hdr->self_samples);
+        const unsigned long long ne = (unsigned long long)*((volatile int*)&hdr->self_edges);
+        W = tot > 0 ? (int)min(64ull, max(1ull, (64ull * ne + tot - 1) / tot)) : 64;
+    }
+    __shared__ int s_win;
+    for (int wi = blockIdx.x;; wi += gridDim.x) {
+        if (hdr) {   // dynamic: the next window from the counter
             __syncthreads();
-            if (lane == 0) s_stop = global_ns() > deadline;
+            if (tid == 0) s_win = atomicAdd(&hdr->self_next, 1);
             __syncthreads();
-            if (s_stop) {
-                if (lane == 0) atomicExch(&hdr->timed_out, 1);
-                break;
-            }
+            wi = s_win;
         }
-        const float* a = from + (size_t)e * D;
-        const float* b = to + (size_t)e * D;
-        const int G = persistent ? Gs[e] : edge_samples(P, given, e, a, b, D, edge_length(a, b, D));
-        const int n_s = G + ((G % 16) != 0 ? 1 : 0);
-        bool hit_any = false;
-        for (int base = 0; base < n_s && !hit_any; base += kSelfThreads) {
-            const int idx = base + lane;
-            bool hit = false;
-            if (idx < n_s) {
-                const int j = idx < G ? idx + 1 : 0;
-                const float t = __fdiv_rn((float)j, (float)G);
-                for (int i = 0; i < D; ++i) {
-                    const float ai = __ldg(a + i), bi = __ldg(b + i);
-                    qc[i] = __fmaf_rn(t, __fadd_rn(bi, -ai), ai);
+        const long long w0l = (long long)wi * W;
+        if (w0l >= n_edges || stopped) break;
+        const int w0 = (int)w0l;
+        const int e = w0 + tid;
+        const bool active = tid < W && e < n_edges && (persistent ? bad[e] == 0 : valid[e] != 0);
+        int G = 0;
+        if (active) {
+            const float* a = from + (size_t)e * D;
+            const float* b = to + (size_t)e * D;
+            G = persistent ? Gs[e] : edge_samples(P, given, e, a, b, D, edge_length(a, b, D));
+        }
+        const int ns = active ? G + ((G % 16) != 0 ? 1 : 0) : 0;
+        int v = ns;   // inclusive scan over the block's 64 edges
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, v, o);
+            if (lane >= o) v += y;
+        }
+        if (lane == 31) s_wsum[warp] = v;
+        s_G[tid] = G;
+        s_hit[tid] = 0;
+        __syncthreads();
+        s_off[tid + 1] = v + (warp == 1 ? s_wsum[0] : 0);
+        if (tid == 0) s_off[0] = 0;
+        __syncthreads();
+        const int total = s_off[kSelfThreads];
+        for (int base = 0; base < total; base += kSelfThreads) {
+            if (deadline) {
+                if (tid == 0) s_stop = global_ns() > deadline;
+                __syncthreads();
+                if (s_stop) {
+                    if (tid == 0) atomicExch(&hdr->timed_out, 1);
+                    stopped = true;
+                    break;
                 }
-                st.v[ST_SAMPLES] += 1;
-                hit = lane_self_hit<kSelfThreads>(M, md, qc, pos, apos, lane, st);
             }
-            hit_any = __syncthreads_or(hit) != 0;
+            const int idx = base + tid;
+            if (idx < total) {
+                int lo = 0, hi = kSelfThreads;   // s_off[lo] <= idx < s_off[hi]
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (s_off[mid] <= idx) lo = mid;
+                    else hi = mid;
+                }
+                if (!*((volatile int*)&s_hit[lo])) {
+                    const int k = idx - s_off[lo], Gl = s_G[lo], el = w0 + lo;
+                    const int j = k < Gl ? k + 1 : 0;
+                    const float t = __fdiv_rn((float)j, (float)Gl);
+                    const float* a = from + (size_t)el * D;
+                    const float* b = to + (size_t)el * D;
+                    for (int i = 0; i < D; ++i) {
+                        const float ai = __ldg(a + i), bi = __ldg(b + i);
+                        qc[i] = __fmaf_rn(t, __fadd_rn(bi, -ai), ai);
+                    }
+                    st.v[ST_SAMPLES] += 1;
+                    if (lane_self_hit<kSelfThreads>(M, md, qc, sm, tid, st)) s_hit[lo] = 1;
+                }
+            }
+            __syncthreads();
         }
-        if (lane == 0) {
+        if (active && !stopped) {
             if (persistent) {
-                bad[e] = hit_any ? 1 : 2;
-            } else if (hit_any) {
+                bad[e] = s_hit[tid] ? 1 : 2;
+            } else if (s_hit[tid]) {
                 valid[e] = 0;
                 cost[e] = FLT_MAX;
             }
         }
+        __syncthreads();   // the next window rewrites the block's tables
     }
     flush_stats(stats, st);
 }

@@ -256,15 +256,44 @@ __device__ __forceinline__ void fk_step(const JointRec& jr, int p, const float* 
 // 108-131, runtime_kinematics.cuh:249-284 and 383-417): the approximate
 // sphere pairs first; the exact pairs only when an approximate pair
 // overlaps; the collision margin does not apply to self pairs. Positions of
-// every exact and approximate sphere are staged in shared memory, SoA by
-// thread: pos [n_spheres * 3][kLanes], apos [n_approx * 3][kLanes].
+// every exact and approximate sphere and every joint's bound centre are
+// staged in shared memory, SoA by thread (stride kLanes).
+//
+// The exact pairs run as the model's runs (sphere i against the spheres of
+// one joint q): a run is skipped when |p_i - c_q| >= r_i + R_q plus the
+// guard band, R_q bounding |p_j - c_q| + r_j for every sphere j of q, so no
+// pair of the run can pass the float test; the others are tested pair by
+// pair with the reference's float test. The verdict is an OR over pairs, so
+// the order and the skipped runs change the work, not the result.
 // ---------------------------------------------------------------------------
 constexpr int kSelfThreads = 64;
 
+struct SelfSmem {
+    float *pos, *apos, *cpos;   // [n_spheres*3][L], [n_approx*3][L], [n_joints*3][L]
+};
+
 template <int kLanes>
-__device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const float* qc, float* pos, float* apos,
-                              int lane, LaneStats& st) {
+__device__ __forceinline__ SelfSmem carve_self(unsigned char* base, int NS, int NA, int NJ) {
+    SelfSmem s;
+    s.pos = reinterpret_cast<float*>(base);
+    s.apos = s.pos + (size_t)NS * 3 * kLanes;
+    s.cpos = s.apos + (size_t)NA * 3 * kLanes;
+    return s;
+}
+
+__device__ __forceinline__ void put3(float* a, int k, int L, int lane, float x, float y, float z) {
+    a[(k * 3 + 0) * L + lane] = x;
+    a[(k * 3 + 1) * L + lane] = y;
+    a[(k * 3 + 2) * L + lane] = z;
+}
+
+template <int kLanes>
+__device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const float* qc, const SelfSmem& sm, int lane,
+                              LaneStats& st) {
     const int NJ = M.H->n_joints;
+    float* pos = sm.pos;
+    float* apos = sm.apos;
+    float* cpos = sm.cpos;
     Affine s0, s1, T;
     affine_identity(s0);
     affine_identity(s1);
@@ -275,18 +304,19 @@ __device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const floa
             const float4 s = M.S[k];
             float px, py, pz;
             sphere_world(T, s.x, s.y, s.z, px, py, pz);
-            pos[(k * 3 + 0) * kLanes + lane] = px;
-            pos[(k * 3 + 1) * kLanes + lane] = py;
-            pos[(k * 3 + 2) * kLanes + lane] = pz;
+            put3(pos, k, kLanes, lane, px, py, pz);
+        }
+        if (jr.bound.w >= 0.0f) {
+            float px, py, pz;
+            sphere_world(T, jr.bound.x, jr.bound.y, jr.bound.z, px, py, pz);
+            put3(cpos, p, kLanes, lane, px, py, pz);
         }
         if (M.H->approx_shares_chain) {
             for (int k = jr.apx_beg; k < jr.apx_end; ++k) {
                 const float4 s = M.A[k];
                 float px, py, pz;
                 sphere_world(T, s.x, s.y, s.z, px, py, pz);
-                apos[(k * 3 + 0) * kLanes + lane] = px;
-                apos[(k * 3 + 1) * kLanes + lane] = py;
-                apos[(k * 3 + 2) * kLanes + lane] = pz;
+                put3(apos, k, kLanes, lane, px, py, pz);
             }
         }
     }
@@ -300,37 +330,46 @@ __device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const floa
                 const float4 s = M.A[k];
                 float px, py, pz;
                 sphere_world(T, s.x, s.y, s.z, px, py, pz);
-                apos[(k * 3 + 0) * kLanes + lane] = px;
-                apos[(k * 3 + 1) * kLanes + lane] = py;
-                apos[(k * 3 + 2) * kLanes + lane] = pz;
+                put3(apos, k, kLanes, lane, px, py, pz);
             }
         }
     }
+    auto at = [&](const float* a, int k, int c) { return a[(k * 3 + c) * kLanes + lane]; };
     bool need = false;
     for (int k = 0; k < M.H->n_apx_self_pairs && !need; ++k) {
         const uint32_t pr = __ldg(md.apx_self_pairs + k);
         const int i = pr & 0xffff, j = pr >> 16;
         st.v[ST_SELF] += 1;
-        need = ref_self_hit(apos[(i * 3) * kLanes + lane], apos[(i * 3 + 1) * kLanes + lane],
-                            apos[(i * 3 + 2) * kLanes + lane], M.A[i].w, apos[(j * 3) * kLanes + lane],
-                            apos[(j * 3 + 1) * kLanes + lane], apos[(j * 3 + 2) * kLanes + lane], M.A[j].w);
+        need = ref_self_hit(at(apos, i, 0), at(apos, i, 1), at(apos, i, 2), M.A[i].w, at(apos, j, 0), at(apos, j, 1),
+                            at(apos, j, 2), M.A[j].w);
     }
-    bool hit = false;
-    for (int k = 0; need && k < M.H->n_self_pairs && !hit; ++k) {
-        const uint32_t pr = __ldg(md.self_pairs + k);
-        const int i = pr & 0xffff, j = pr >> 16;
+    if (!need) return false;
+    for (int r = 0; r < md.n_sruns; ++r) {
+        const uint2 run = __ldg(md.sruns + r);
+        const int i = run.x & 0x1ff, q = (run.x >> 9) & 0x1f, len = run.x >> 14;
+        const float px = at(pos, i, 0), py = at(pos, i, 1), pz = at(pos, i, 2), ri = M.S[i].w;
+        const float4 bq = M.J[q].bound;
+        const float cx = at(cpos, q, 0), cy = at(cpos, q, 1), cz = at(cpos, q, 2);
+        const float dx = px - cx, dy = py - cy, dz = pz - cz;
+        const float S = fmaxf(fmaxf(fabsf(px), fmaxf(fabsf(py), fabsf(pz))), fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))));
+        float lim = ri + bq.w;
+        lim += 4.0f * (S + lim + 1.0f) * PS_GUARD_K;
         st.v[ST_SELF] += 1;
-        hit = ref_self_hit(pos[(i * 3) * kLanes + lane], pos[(i * 3 + 1) * kLanes + lane],
-                           pos[(i * 3 + 2) * kLanes + lane], M.S[i].w, pos[(j * 3) * kLanes + lane],
-                           pos[(j * 3 + 1) * kLanes + lane], pos[(j * 3 + 2) * kLanes + lane], M.S[j].w);
+        if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) >= lim * lim * (1.0f + 1.0e-6f)) continue;   // no pair can hit
+        for (int k = 0; k < len; ++k) {
+            const int j = __ldg(md.spairs + run.y + k);
+            st.v[ST_SELF] += 1;
+            if (ref_self_hit(px, py, pz, ri, at(pos, j, 0), at(pos, j, 1), at(pos, j, 2), M.S[j].w)) return true;
+        }
     }
-    return hit;
+    return false;
 }
 
 // Shared memory of a kSelfThreads-lane block running lane_self_hit: model
-// core, sphere positions and a tile of configurations.
+// core, sphere and bound positions and a tile of configurations.
 inline size_t self_smem_bytes(const ps_model* m) {
-    return (size_t)m->dev.bytes_core + (size_t)(m->info.n_spheres + m->info.n_approx_spheres) * 3 * kSelfThreads * 4 +
+    return (size_t)m->dev.bytes_core +
+           (size_t)(m->info.n_spheres + m->info.n_approx_spheres + m->info.n_joints) * 3 * kSelfThreads * 4 +
            (size_t)kSelfThreads * m->info.n_dof * 4;
 }
 
