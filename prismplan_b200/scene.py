@@ -161,6 +161,36 @@ class PlanningScene:
         self._dirty = True
         self._tensors: Optional[SceneTensors] = None
 
+    @classmethod
+    def from_robot_asset(cls, asset_path, device: str = "cuda") -> "PlanningScene":
+        """A scene sized to a robot YAML asset: its name and n_dof
+        (planning_scene.py:92-100)."""
+        from .robot import load_robot_asset
+
+        asset = load_robot_asset(asset_path)
+        return cls(num_joints=asset["n_dof"], robot_id=asset["name"], device=device)
+
+    @property
+    def num_joints(self) -> int:
+        return self._num_joints
+
+    @property
+    def robot_id(self) -> str:
+        return self._robot_id
+
+    @property
+    def n_obbs(self) -> int:
+        """Boxes in the last built collision data (planning_scene.py:111-113,
+        set when the tensors are rebuilt)."""
+        return 0 if self._tensors is None else self._tensors.n_obbs
+
+    @property
+    def current_obstacles(self) -> List[Dict[str, Any]]:
+        """The cuboids as update_world takes them (planning_scene.py:115-128):
+        name, type, dims, position, quaternion (w, x, y, z)."""
+        return [{"name": name, "type": "cuboid", "dims": d.tolist(), "position": p.tolist(),
+                 "quaternion": q.tolist()} for name, (d, p, q) in self._cuboids.items()]
+
     def add_cuboid(self, name: str, dims: Sequence[float], position: Sequence[float],
                    quaternion=(1.0, 0.0, 0.0, 0.0)) -> None:
         q = np.asarray(quaternion, np.float64).reshape(4)

@@ -45,3 +45,33 @@ def test_planner_entry_points_are_refused():
     for name in ("solve_scene", "chomp_solve_scene", "stomp_solve_scene", "CHOMPSettings"):
         with pytest.raises(AttributeError, match="substrate"):
             getattr(prrtc, name)
+
+
+def test_planning_scene_surface(tmp_path):
+    # the members the planner plugins read (planning_scene.py:92-128), host side only
+    from prismplan_b200.scene import PlanningScene
+
+    yaml_text = "\n".join([
+        "name: two_link", "n_dof: 2", "n_joints: 3",
+        "joint_types: [-1, 5, 5]",
+        "fixed_transforms:",
+        "  - [1,0,0,0, 0,1,0,0, 0,0,1,0, 0,0,0,1]",
+        "  - [1,0,0,0, 0,1,0,0, 0,0,1,0.1, 0,0,0,1]",
+        "  - [1,0,0,0.3, 0,1,0,0, 0,0,1,0, 0,0,0,1]",
+        "spheres: [[0,0,0,0.05], [0.1,0,0,0.05], [0.1,0,0,0.04]]",
+        "sphere_to_joint: [1, 1, 2]",
+        "self_cc_ranges: []",
+        "joint_lower: [-1, -1]", "joint_upper: [1, 1]",
+    ])
+    path = tmp_path / "two_link.yaml"
+    path.write_text(yaml_text)
+    scene = PlanningScene.from_robot_asset(str(path), device="cpu")
+    assert scene.num_joints == 2 and scene.robot_id == "two_link" and scene.n_obbs == 0
+    scene.add_cuboid("a", [0.1, 0.2, 0.3], [1.0, 0.0, 0.5])
+    scene.add_cuboid("b", [0.2, 0.2, 0.2], [0.0, 1.0, 0.5], [0.0, 1.0, 0.0, 0.0])
+    obs = scene.current_obstacles
+    assert [o["name"] for o in obs] == ["a", "b"] and obs[1]["quaternion"] == [0.0, 1.0, 0.0, 0.0]
+    assert obs[0]["type"] == "cuboid" and obs[0]["dims"] == [0.1, 0.2, 0.3]
+    clone = PlanningScene(2)
+    clone.update_world(obs)
+    assert clone.current_obstacles == obs
