@@ -237,18 +237,19 @@ __device__ bool process_chunk(const ModelSmem& M, const SceneSmem& sc, const ps_
 
 // Fast path of process_chunk for the common scene: the approximate chain is
 // the full chain, no ACM masks, no ESDF layers, no clearance. Same verdict;
-// fewer live registers and a per-joint guard band. Exact spheres of a flagged
-// joint are tested 8 at a time against each surviving box (one box load per
-// 8 spheres), then decided from their min d^2 with the exact re-decision
-// inside the guard band.
-// Decide one sphere from its min d^2 over the candidate boxes: definite
-// outside the guard band, exact re-decision of the band's boxes otherwise.
-__device__ __forceinline__ bool decide_band(const SceneSmem& sc, const uint16_t* cand, int ncand, float px, float py,
-                                            float pz, float sr, float g, float mn, LaneStats& st) {
-    const float a = fmaxf(sr - g, 0.0f), b = sr + g;
-    const float lo = a * a * (1.0f - 1.0e-6f), hi = b * b * (1.0f + 1.0e-6f);
-    if (mn < lo) return true;
-    if (mn >= hi) return false;
+// fewer live registers and a per-joint guard band. Exact spheres are tested 4
+// at a time against each surviving box (one box load per 4 spheres), then
+// decided from their min d^2 with the exact re-decision inside the guard band.
+//
+// Code size matters here: the kernel issues about 3 of every 4 cycles, and
+// instruction fetch stalls were the third largest stall reason. The box loops
+// are kept rolled and the rare band re-decision is out of line, which took
+// 7 % (boxes only) and 15 % (boxes and ESDF) off the kernel time.
+
+// Exact re-decision of one sphere whose min d^2 fell inside the guard band
+// (lo, hi): the band's boxes are decided one by one with the reference test.
+__device__ __noinline__ bool band_redecide(const SceneSmem& sc, const uint16_t* cand, int ncand, float px, float py,
+                                           float pz, float sr, float lo, float hi, LaneStats& st) {
     for (int k = 0; k < ncand; ++k) {
         const ObbPrep& o = sc.obbs[cand[k]];
         float qx, qy, qz;
@@ -262,6 +263,17 @@ __device__ __forceinline__ bool decide_band(const SceneSmem& sc, const uint16_t*
     return false;
 }
 
+// Decide one sphere from its min d^2 over the candidate boxes: definite
+// outside the guard band, exact re-decision of the band's boxes otherwise.
+__device__ __forceinline__ bool decide_band(const SceneSmem& sc, const uint16_t* cand, int ncand, float px, float py,
+                                            float pz, float sr, float g, float mn, LaneStats& st) {
+    const float a = fmaxf(sr - g, 0.0f), b = sr + g;
+    const float lo = a * a * (1.0f - 1.0e-6f), hi = b * b * (1.0f + 1.0e-6f);
+    if (mn < lo) return true;
+    if (mn >= hi) return false;
+    return band_redecide(sc, cand, ncand, px, py, pz, sr, lo, hi, st);
+}
+
 // kN spheres (positions in registers) against every candidate box: one box
 // load per kN pair tests. Returns whether any of them hits.
 template <int kN, bool kStats>
@@ -271,6 +283,7 @@ __device__ __forceinline__ bool spheres_hit(const SceneSmem& sc, const uint16_t*
     float mn[kN];
 #pragma unroll
     for (int i = 0; i < kN; ++i) mn[i] = 3.0e38f;
+#pragma unroll 1
     for (int k = 0; k < ncand; ++k) {
         const ObbPrep& o = sc.obbs[cand[k]];
         const float4 r0 = o.r0, r1 = o.r1, r2 = o.r2, h = o.h;
@@ -373,6 +386,7 @@ __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, cons
         const float Rc2 = Rc * Rc;
         int ncand = 0;
         __syncwarp();
+#pragma unroll 1
         for (int base = 0; base < sc.n_obbs; base += 32) {
             const int o = base + lane;
             bool keep = false;
