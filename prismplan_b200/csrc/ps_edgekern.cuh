@@ -238,8 +238,9 @@ __device__ bool process_chunk(const ModelSmem& M, const SceneSmem& sc, const ps_
 // Fast path of process_chunk for the common scene: the approximate chain is
 // the full chain, no ACM masks, no ESDF layers, no clearance. Same verdict;
 // fewer live registers and a per-joint guard band. Exact spheres are tested 4
-// at a time against each surviving box (one box load per 4 spheres), then
-// decided from their min d^2 with the exact re-decision inside the guard band.
+// at a time (2 with ESDF layers) against each surviving box (one box load per
+// group), then decided from their min d^2 with the exact re-decision inside
+// the guard band.
 //
 // Code size matters here: the kernel issues about 3 of every 4 cycles, and
 // instruction fetch stalls were the third largest stall reason. The box loops
@@ -424,19 +425,22 @@ __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, cons
             bool ex = false;
             if (!esdf || flagged) {
                 int k = jr.sph_beg;
-                for (; k + 4 <= jr.sph_end && !ex; k += 4) {
-                    float px[4], py[4], pz[4], sr[4];
+                // spheres per box load: 4 with boxes only, 2 when the ESDF
+                // lookups share the registers (measured best for each)
+                constexpr int kG = kEsdf ? 2 : 4;
+                for (; k + kG <= jr.sph_end && !ex; k += kG) {
+                    float px[kG], py[kG], pz[kG], sr[kG];
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) {
+                    for (int i = 0; i < kG; ++i) {
                         const float4 sp = M.S[k + i];
                         sphere_world(T, sp.x, sp.y, sp.z, px[i], py[i], pz[i]);
                         sr[i] = __fadd_rn(sp.w, margin);
                     }
-                    if (kStats) st.v[ST_SPHERES] += 4;
-                    ex = spheres_hit<4, kStats>(sc, ws.cand, ncand, px, py, pz, sr, g, st);
+                    if (kStats) st.v[ST_SPHERES] += kG;
+                    ex = spheres_hit<kG, kStats>(sc, ws.cand, ncand, px, py, pz, sr, g, st);
                     if (esdf)
 #pragma unroll
-                        for (int i = 0; i < 4; ++i)
+                        for (int i = 0; i < kG; ++i)
                             if (!ex) ex = sphere_esdf_any(sc, sv, px[i], py[i], pz[i], sr[i], nullptr, st);
                 }
                 for (; k < jr.sph_end && !ex; ++k) {
@@ -587,8 +591,10 @@ __global__ void edges_prep_kernel(ps_edge_params P, const float* __restrict__ fr
     }
 }
 
+// Residency per variant, measured: the boxes-only fast path runs fastest
+// with 5 blocks per SM (room for 96 registers), the ESDF variant with 6.
 template <int kMode, bool kStats>
-__global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_queue_kernel(ModelDev md, ps_scene_view sv, ps_edge_params P,
+__global__ void __launch_bounds__(kEdgeThreads, kMode == 1 ? 5 : (kMode ? 6 : 3)) edges_queue_kernel(ModelDev md, ps_scene_view sv, ps_edge_params P,
                                                                   const float* __restrict__ from,
                                                                   const float* __restrict__ to, int n_edges,
                                                                   EdgeWs* hdr, const int* __restrict__ Gs, int* bad,
