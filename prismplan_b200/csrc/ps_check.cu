@@ -187,8 +187,10 @@ __device__ __noinline__ void sphere_tail(const SceneSmem& sc, const ps_scene_vie
     exact += st.v[ST_EXACT];
 }
 
+// Residency, measured: 6 blocks per SM with clearance (short per-sphere work,
+// latency-bound), 4 without (the early-exit loop wants its registers).
 template <bool kClr, bool kStats>
-__global__ void __launch_bounds__(kCfgThreads, 4) check_configs_fast_kernel(ModelDev md, ps_scene_view sv,
+__global__ void __launch_bounds__(kCfgThreads, kClr ? 6 : 4) check_configs_fast_kernel(ModelDev md, ps_scene_view sv,
                                                                         const float* __restrict__ q, int n,
                                                                         float margin, unsigned flags,
                                                                         uint8_t* __restrict__ hit_out,

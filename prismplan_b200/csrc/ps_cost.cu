@@ -40,8 +40,10 @@ size_t cost_block_smem(const ps_model* m, const ps_scene_view* sv, bool grad) {
 // skip (may be NULL): rows b with skip[b] != 0 need no output; a tile is
 // skipped when every row it touches is, so a skipped row that shares a tile
 // with a live one is evaluated all the same (with the same bits).
+// Residency, measured: 4 blocks per SM for the gradient kernel, 3 for the
+// rollout kernel (its tiles keep more live state).
 template <bool kGrad, bool kStats, int kTile>
-__global__ void __launch_bounds__(kCostWarps * 32, 3) waypoint_cost_kernel(
+__global__ void __launch_bounds__(kCostWarps * 32, kGrad ? 4 : 3) waypoint_cost_kernel(
     ModelDev md, ps_scene_view sv, const float* __restrict__ q, int n_rows, int T, ps_cost_params P,
     float* __restrict__ wp_cost, int broadcast_d, float* __restrict__ traj_acc, float* __restrict__ grad,
     unsigned long long* stats, const uint8_t* __restrict__ skip) {
