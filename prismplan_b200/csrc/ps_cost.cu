@@ -88,8 +88,7 @@ __global__ void __launch_bounds__(kCostWarps * 32, kGrad ? 4 : 3) waypoint_cost_
                 ws.q[t * 16 + lane] = bdt ? q[((size_t)b * D + lane) * T + tt] : q[((size_t)b * T + tt) * D + lane];
         }
         __syncwarp();
-        for (int t = 0; t < nt; ++t)
-            cost_fk<kStats>(M, ws.q + t * 16, ws.frame + t * NJ * 12, ws.bnd + t * NJ, st);
+        cost_fk_tile<kStats>(M, ws.q, nt, ws.frame, ws.bnd, st);
         __syncwarp();
         cost_cull<kStats>(M, sc, cb, ws, nt, P.world_margin, st);
         for (int t = 0; t < nt; ++t) {

@@ -302,6 +302,67 @@ __device__ __forceinline__ void cost_fk(const ModelSmem& M, const float* q, floa
 
 }
 
+// FK of the nt waypoints of a tile at once: the warp splits into groups of
+// n_joints lanes, one group per waypoint (32 / n_joints waypoints per pass),
+// each running the pointer-jumping FK of cost_fk on its own waypoint. Every
+// (waypoint, joint) frame is composed from the same factors in the same
+// order as cost_fk, so the frames and bounds are the same bits; only the
+// idle lanes of a one-waypoint pass are put to work.
+template <bool kStats>
+__device__ __forceinline__ void cost_fk_tile(const ModelSmem& M, const float* q, int nt, float* frame, float4* bnd,
+                                             LaneStats& st) {
+    const int lane = threadIdx.x & 31;
+    const int NJ = M.H->n_joints;
+    const int per = max(1, 32 / NJ);
+    const int grp = lane / NJ, p = lane - grp * NJ, base = grp * NJ;
+    for (int t0 = 0; t0 < nt; t0 += per) {
+        const int t = t0 + grp;
+        const bool act = grp < per && t < nt;
+        Affine A;
+        affine_identity(A);
+        int anc = -1;
+        if (act && p > 0) {
+            const JointRec& jr = M.J[p];
+            const float qi = jr.dof >= 0 ? q[t * 16 + jr.dof] : 0.0f;
+            float sn = 0.0f, cs = 1.0f;
+            if (jr.type >= PS_X_ROT) sincosf(qi, &sn, &cs);
+            Affine I;
+            affine_identity(I);
+            joint_compose_sc(jr, qi, sn, cs, I, A);
+            anc = jr.parent_pos;
+        }
+        while (__ballot_sync(kCostFull, anc >= 0)) {
+            const int src = anc >= 0 ? base + anc : lane;
+            Affine B;
+#pragma unroll
+            for (int i = 0; i < 12; ++i) B.m[i] = __shfl_sync(kCostFull, A.m[i], src);
+            const int anc2 = __shfl_sync(kCostFull, anc, src);
+            if (anc >= 0) {
+                Affine C;
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        float v = fmaf(B.m[r * 4 + 2], A.m[8 + c], fmaf(B.m[r * 4 + 1], A.m[4 + c], B.m[r * 4] * A.m[c]));
+                        C.m[r * 4 + c] = c == 3 ? v + B.m[r * 4 + 3] : v;
+                    }
+                }
+                A = C;
+                anc = anc2;
+            }
+        }
+        if (act) {
+            store_frame(frame + ((size_t)t * NJ + p) * 12, A);
+            const float4 b = M.J[p].bound;
+            float cx = 0.f, cy = 0.f, cz = 0.f;
+            if (b.w >= 0.0f) sphere_world(A, b.x, b.y, b.z, cx, cy, cz);
+            bnd[t * NJ + p] = make_float4(cx, cy, cz, b.w);
+        }
+    }
+    if (kStats && lane == 0) st.v[ST_JOINTS] += NJ * nt;
+    __syncwarp();
+}
+
 // Candidate boxes per joint for a tile of nt waypoints, from the union of
 // the joint's bound spheres over the tile: a box farther than that union's
 // radius + max(m, 0) reaches no sphere of the joint inside the hinge band.
