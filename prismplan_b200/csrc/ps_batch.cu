@@ -136,8 +136,7 @@ __global__ void __launch_bounds__(kWarps * 32, 24 / kWarps) batch_waypoint_kerne
         for (int t = 0; t < nt; ++t)
             if (lane < D) ws.q[t * 16 + lane] = q[(size_t)(k0 + t) * D + lane];
         __syncwarp();
-        for (int t = 0; t < nt; ++t)
-            cost_fk<false>(M, ws.q + t * 16, ws.frame + t * NJ * 12, ws.bnd + t * NJ, st);
+        cost_fk_tile<false>(M, ws.q, nt, ws.frame, ws.bnd, st);
         __syncwarp();
         cost_cull<false>(M, sc, cb, ws, nt, P.world_margin, st);
         for (int t = 0; t < nt; ++t) {

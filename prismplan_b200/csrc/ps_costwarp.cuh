@@ -244,70 +244,14 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
-// FK of one waypoint (configuration q) for the whole warp: frames and the
-// world bound sphere of every joint.
-template <bool kStats>
-__device__ __forceinline__ void cost_fk(const ModelSmem& M, const float* q, float* frame, float4* bnd,
-                                        LaneStats& st) {
-    const int lane = threadIdx.x & 31;
-    const int NJ = M.H->n_joints;
-    // ---- 1. FK by pointer jumping: lane p < NJ forms joint p's local step
-    //      S_p = FT_p * motion(q) and holds A_p, the transform from its
-    //      current ancestor anc_p to p; each round composes A_anc * A_p and
-    //      jumps anc_p to anc_anc, so depth d takes ceil(log2 d) rounds. ----
-    {
-        Affine A;
-        affine_identity(A);
-        int anc = -1;
-        if (lane > 0 && lane < NJ) {
-            const JointRec& jr = M.J[lane];
-            const float qi = jr.dof >= 0 ? q[jr.dof] : 0.0f;
-            float sn = 0.0f, cs = 1.0f;
-            if (jr.type >= PS_X_ROT) sincosf(qi, &sn, &cs);
-            Affine I;
-            affine_identity(I);
-            joint_compose_sc(jr, qi, sn, cs, I, A);
-            anc = jr.parent_pos;
-        }
-        while (__ballot_sync(kCostFull, anc >= 0)) {
-            const int src = anc >= 0 ? anc : lane;
-            Affine B;
-#pragma unroll
-            for (int i = 0; i < 12; ++i) B.m[i] = __shfl_sync(kCostFull, A.m[i], src);
-            const int anc2 = __shfl_sync(kCostFull, anc, src);
-            if (anc >= 0) {
-                Affine C;
-#pragma unroll
-                for (int r = 0; r < 3; ++r) {
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        float v = fmaf(B.m[r * 4 + 2], A.m[8 + c], fmaf(B.m[r * 4 + 1], A.m[4 + c], B.m[r * 4] * A.m[c]));
-                        C.m[r * 4 + c] = c == 3 ? v + B.m[r * 4 + 3] : v;
-                    }
-                }
-                A = C;
-                anc = anc2;
-            }
-        }
-        if (lane < NJ) {
-            store_frame(frame + lane * 12, A);
-            const float4 b = M.J[lane].bound;
-            float cx = 0.f, cy = 0.f, cz = 0.f;
-            if (b.w >= 0.0f) sphere_world(A, b.x, b.y, b.z, cx, cy, cz);
-            bnd[lane] = make_float4(cx, cy, cz, b.w);
-        }
-        if (kStats && lane == 0) st.v[ST_JOINTS] += NJ;
-    }
-    __syncwarp();
-
-}
-
-// FK of the nt waypoints of a tile at once: the warp splits into groups of
-// n_joints lanes, one group per waypoint (32 / n_joints waypoints per pass),
-// each running the pointer-jumping FK of cost_fk on its own waypoint. Every
-// (waypoint, joint) frame is composed from the same factors in the same
-// order as cost_fk, so the frames and bounds are the same bits; only the
-// idle lanes of a one-waypoint pass are put to work.
+// FK of the nt waypoints of a tile: frames and world bound spheres of every
+// joint. The warp splits into groups of n_joints lanes, one group per
+// waypoint (32 / n_joints waypoints per pass). In a group, lane p forms joint
+// p's local step S_p = FT_p * motion(q) with accurate sincosf and holds A_p,
+// the transform from its current ancestor anc_p to p; each round composes
+// A_anc * A_p and jumps anc_p to anc_anc, so depth d takes ceil(log2 d)
+// rounds. A frame's factors and their order depend only on the tree, so a
+// waypoint gets the same bits in any group and tile.
 template <bool kStats>
 __device__ __forceinline__ void cost_fk_tile(const ModelSmem& M, const float* q, int nt, float* frame, float4* bnd,
                                              LaneStats& st) {
@@ -426,7 +370,7 @@ __device__ __forceinline__ void cost_cull(const ModelSmem& M, const SceneSmem& s
 
 // Cost (returned on every lane) of waypoint t of the tile and, with kGrad,
 // d cost / d q written by lanes d < n_dof to grad_row[d * gstride]. The whole
-// warp calls it after cost_fk and cost_cull. kStats: count executed work.
+// warp calls it after cost_fk_tile and cost_cull. kStats: count executed work.
 template <bool kGrad, bool kStats>
 __device__ __forceinline__ float cost_eval(const ModelSmem& M, const ModelDev& md, const SceneSmem& sc,
                                            const ps_scene_view& sv, const ps_cost_params& P, const CostBlock& cb,
