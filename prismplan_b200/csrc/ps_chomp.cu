@@ -124,7 +124,7 @@ size_t chomp_layout(int B, int T, int D, ChompBufs* out, void* base) {
 using namespace ps;
 
 extern "C" size_t ps_chomp_workspace_bytes(const ps_model* m, int B, int T) {
-    if (!m || B < 0 || T < 2) return 0;
+    if (!m || B < 0 || T < 2 || (long long)B * T >= (1ll << 31)) return 0;
     return chomp_layout(B, T, m->info.n_dof, nullptr, nullptr);
 }
 
@@ -136,6 +136,7 @@ extern "C" int ps_chomp_optimize(const ps_model* m, const ps_scene_view* scene, 
     if (!m || !P) return set_error(PS_EINVAL, "model / params is NULL");
     if (B < 0) return set_error(PS_EINVAL, "B < 0");
     if (T < 2 || T > kOptMaxT) return set_error(PS_EINVAL, "T must be in [2, 1024]");
+    if ((long long)B * T >= (1ll << 31)) return set_error(PS_EINVAL, "B * T exceeds 2^31");
     if (int rc = validate_scene(m, scene)) return rc;
     if (B == 0) return PS_OK;
     if (!theta || !best || !solved || !iterations || !best_cost) return set_error(PS_EINVAL, "NULL output buffer");
