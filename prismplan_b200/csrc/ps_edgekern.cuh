@@ -89,7 +89,7 @@ __device__ __forceinline__ float edge_length(const float* a, const float* b, int
 struct WarpScratch {
     float* q;          // [32 * D]
     uint16_t* cand;    // [n_obbs]
-    const float4* obs; // [n_obbs] box centre and circumscribed radius (block-wide)
+    const float4* obs; // [n_obbs] box centre, .w its part of the broad-phase limit (block-wide)
 };
 
 // One chunk of one edge. Returns true if any sample of the chunk collides.
@@ -382,9 +382,13 @@ __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, cons
         // max over lanes in one warp reduction: non-negative floats order as their bits
         const float r2 = __uint_as_float(__reduce_max_sync(kFull, __float_as_uint(fmaf(dz, dz, fmaf(dy, dy, dx * dx)))));
         const float Sm = fmaxf(fabsf(mx), fmaxf(fabsf(my), fabsf(mz)));
-        float Rc = sqrtf(r2) + jr.bound.w + fmaxf(margin, 0.0f);
+        // the square root only widens a conservative bound: the approximate
+        // one, raised by 1e-6 relative (far above its error), is enough
+        const float r2c = fmaxf(r2, 1.0e-30f);
+        float Rc = r2c * rsqrtf(r2c) * (1.0f + 1.0e-6f) + jr.bound.w + fmaxf(margin, 0.0f);
         Rc += 4.0f * (Sm + Rc + sc.Bmax + 1.0f) * PS_GUARD_K;
         const float Rc2 = Rc * Rc;
+        const float Rj = (Rc * (1.0f + 4.0f * PS_GUARD_K) + 4.0f * PS_GUARD_K * (Sm + 1.0f)) * (1.0f + 1.0e-6f);
         int ncand = 0;
         __syncwarp();
 #pragma unroll 1
@@ -395,8 +399,7 @@ __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, cons
                 // circumscribed-sphere test first, the box distance only if it passes
                 const float4 ob = ws.obs[o];
                 const float ex = ob.x - mx, ey = ob.y - my, ez = ob.z - mz;
-                float lim = Rc + ob.w;
-                lim += 4.0f * (Sm + fmaxf(fabsf(ob.x), fmaxf(fabsf(ob.y), fabsf(ob.z))) + lim + 1.0f) * PS_GUARD_K;
+                const float lim = Rj + ob.w;   // see box_limits
                 if (fmaf(ez, ez, fmaf(ey, ey, ex * ex)) < lim * lim) {
                     float qx, qy, qz;
                     keep = fast_box_dsq(sc.obbs[o], mx, my, mz, qx, qy, qz) < Rc2;
@@ -463,6 +466,24 @@ __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, cons
     return __any_sync(kFull, hit && real);
 }
 
+// Circumscribed-sphere prefilter of the fast path's broad phase. With
+// Rc the joint's cull radius around the chunk centre m (Sm = |m|inf), box o's
+// centre c_o (M_o = |c_o|inf) and circumscribed radius w_o, the guarded limit
+//   Rc + w_o + 4K (Sm + M_o + Rc + w_o + 1)
+// splits into a joint part Rj = Rc (1 + 4K) + 4K (Sm + 1) and a box part
+//   B_o = w_o (1 + 4K) + 4K M_o,
+// each raised by 1e-6 relative to cover their roundings, so the test stays
+// at least as wide as the unsplit one. B_o replaces obs[o].w (every thread
+// calls it after box_spheres and a block barrier).
+__device__ __forceinline__ void box_limits(const SceneSmem& sc, float4* obs) {
+    for (int o = threadIdx.x; o < sc.n_obbs; o += blockDim.x) {
+        float4 ob = obs[o];
+        const float M = fmaxf(fabsf(ob.x), fmaxf(fabsf(ob.y), fabsf(ob.z)));
+        ob.w = (ob.w * (1.0f + 4.0f * PS_GUARD_K) + 4.0f * PS_GUARD_K * M) * (1.0f + 1.0e-6f);
+        obs[o] = ob;
+    }
+}
+
 // Shared-memory carve-up common to both edge kernels.
 struct EdgeSmem {
     unsigned char* blob;
@@ -516,6 +537,8 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_plain_kerne
     SceneSmem sc;
     stage_scene(sv, es.obbs, es.orig, es.layers, counters, &bmax, sc);
     box_spheres(sc, es.obs);
+    __syncthreads();
+    box_limits(sc, es.obs);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nob_pad = (max(sv.n_obbs, 1) + 7) & ~7;
@@ -624,6 +647,8 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode == 1 ? 5 : (kMode ? 6 : 3)
     SceneSmem sc;
     stage_scene(sv, es.obbs, es.orig, es.layers, counters, &bmax, sc);
     box_spheres(sc, es.obs);
+    __syncthreads();
+    box_limits(sc, es.obs);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nob_pad = (max(sv.n_obbs, 1) + 7) & ~7;
