@@ -145,7 +145,9 @@ typedef struct ps_scene_view {
     int            max_voxels_per_layer;
     const uint8_t* sphere_acm_mask;             /* device [n_spheres*L] or NULL */
     const uint8_t* sphere_obb_acm_mask;         /* device [n_spheres*n_obbs] or NULL */
-    const uint8_t* sphere_obb_acm_mask_approx;  /* device [n_approx*n_obbs] or NULL */
+    const uint8_t* sphere_obb_acm_mask_approx;  /* device [n_approx*n_obbs] or NULL. Read by nothing: the
+                                                   reference's approximate pass passes sphere index -1 and so
+                                                   applies no mask (scene_collision.cuh:584-606) */
     int            esdf_mode;       /* PS_ESDF_NEAREST or PS_ESDF_TRILINEAR */
 } ps_scene_view;
 

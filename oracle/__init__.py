@@ -209,6 +209,7 @@ def load_ref():
         lib.ref_obb_pairs.argtypes = [_fp, _fp, _fp, C.c_int, _u8p]
         lib.ref_check_edges.argtypes = [C.c_void_p, C.c_void_p, _fp, _fp, _ip, C.c_int, C.c_float, C.c_int,
                                         _u8p, _fp, _fp, C.c_int]
+        lib.ref_esdf_min_clearance.argtypes = [C.c_void_p, C.c_void_p, _fp, C.c_int, C.c_float, _fp]
         lib.ref_chomp.argtypes = [C.c_void_p, C.c_void_p, _fp, C.c_int, C.c_int, C.c_float, C.c_float,
                                   C.c_float, C.c_float, _fp, _fp, _fp, C.c_int]
         lib.ref_stomp_state_cost.argtypes = [C.c_void_p, C.c_void_p, _fp, C.c_int, C.c_int, C.c_float,
@@ -286,6 +287,14 @@ class RefKernels:
         out = np.zeros(len(q), np.float32)
         _chk(load_ref().ref_obb_min_clearance(self.m, self.s, _ptr(q, _fp), len(q), margin, _ptr(out, _fp)),
              "obb_min_clearance")
+        return out
+
+    def esdf_min_clearance(self, q, margin=0.0):
+        """scene_min_clearance_runtime per configuration (4-thread blocks)."""
+        q = _f32(q).reshape(-1, self.n_dof)
+        out = np.zeros(len(q), np.float32)
+        _chk(load_ref().ref_esdf_min_clearance(self.m, self.s, _ptr(q, _fp), len(q), margin, _ptr(out, _fp)),
+             "esdf_min_clearance")
         return out
 
     def check_edges(self, frm, to, G, margin=0.0, check_self=False, reps=1):

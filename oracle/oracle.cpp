@@ -500,6 +500,10 @@ void orc_scene_destroy(orc_scene* s) { delete s; }
 extern "C" void orc_scene_set_masks(orc_scene* s, const uint8_t* acm, int n_acm,
                                     const uint8_t* obb_acm, int n_obb_acm,
                                     const uint8_t* obb_acm_apx, int n_obb_acm_apx) {
+    // each call replaces all three masks; NULL (or empty) means none
+    s->acm.clear();
+    s->obb_acm.clear();
+    s->obb_acm_apx.clear();
     if (acm && n_acm > 0) s->acm.assign(acm, acm + n_acm);
     if (obb_acm && n_obb_acm > 0) s->obb_acm.assign(obb_acm, obb_acm + n_obb_acm);
     if (obb_acm_apx && n_obb_acm_apx > 0) s->obb_acm_apx.assign(obb_acm_apx, obb_acm_apx + n_obb_acm_apx);

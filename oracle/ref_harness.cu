@@ -120,6 +120,28 @@ __global__ void harness_obb_clearance_kernel(const float* q_all, int n, ppln::Ro
     if (tid == 0) out[idx] = fminf(fminf(part[0], part[1]), fminf(part[2], part[3]));
 }
 
+// scene_min_clearance_runtime (scene_collision.cuh:339-384) of one
+// configuration per block. The block has 4 threads, one lane group, so the
+// function's __shfl_xor_sync(0xf, ...) names every lane that calls it.
+__global__ void harness_esdf_clearance_kernel(const float* q_all, int n, ppln::RobotModel model,
+                                              ppln::collision::SceneCollisionData scene, float margin,
+                                              float* out) {
+    int idx = blockIdx.x;
+    if (idx >= n) return;
+    int tid = threadIdx.x;
+    extern __shared__ float smem[];
+    float* sphere_pos = smem;
+    float* T = sphere_pos + model.n_spheres * BATCH_SIZE * 3;
+    float* q = T + BATCH_SIZE * ppln::FK_T_SLOTS * 16;
+    if (tid == 0)
+        for (int d = 0; d < model.n_dof; ++d) q[d] = q_all[idx * model.n_dof + d];
+    __syncthreads();
+    ppln::collision::fk_runtime(model, q, sphere_pos, T, tid);
+    __syncthreads();
+    const float m = ppln::collision::scene_min_clearance_runtime(model, sphere_pos, scene, tid, margin);
+    if (tid == 0) out[idx] = m;
+}
+
 __global__ void harness_to_local_kernel(const float* pose, const float* pts, int n, float* out) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -264,6 +286,22 @@ int ref_obb_min_clearance(void* mp, void* sp, const float* q, int n, float margi
     cudaMalloc(&dout, (size_t)n * sizeof(float));
     harness_obb_clearance_kernel<<<n, 4, state_smem(mod)>>>(dq, n, mod, s->d, margin, dout);
     int rc = last_cuda("obb_clearance");
+    cudaMemcpy(out, dout, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(dout);
+    for (void* p : own) cudaFree(p);
+    return rc;
+}
+
+int ref_esdf_min_clearance(void* mp, void* sp, const float* q, int n, float margin, float* out) {
+    RefModel* m = (RefModel*)mp;
+    RefScene* s = (RefScene*)sp;
+    const auto& mod = m->dev.model;
+    std::vector<void*> own;
+    float* dq = upload(q, (size_t)n * mod.n_dof, own);
+    float* dout = nullptr;
+    cudaMalloc(&dout, (size_t)n * sizeof(float));
+    harness_esdf_clearance_kernel<<<n, 4, state_smem(mod)>>>(dq, n, mod, s->d, margin, dout);
+    int rc = last_cuda("esdf_clearance");
     cudaMemcpy(out, dout, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
     cudaFree(dout);
     for (void* p : own) cudaFree(p);

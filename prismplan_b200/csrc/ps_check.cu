@@ -116,10 +116,10 @@ __global__ void __launch_bounds__(kCfgThreads) check_configs_kernel(ModelDev md,
                     sphere_world(shares ? T : TA, sa.x, sa.y, sa.z, px, py, pz);
                     if (kStats) st.v[ST_SPHERES] += 1;
                     const float sr = __fadd_rn(sa.w, margin);
-                    const uint8_t* acm = sv.sphere_obb_acm_mask_approx
-                                             ? sv.sphere_obb_acm_mask_approx + (size_t)M.AO[a] * sv.n_obbs
-                                             : nullptr;
-                    flagged = (sc.n_obbs && sphere_obb_any(sc, nullptr, 0, px, py, pz, sr, acm, st)) ||
+                    // no mask in the approximate pass: the reference passes
+                    // sphere index -1 (scene_collision.cuh:584-606), which
+                    // turns both the OBB and the ESDF mask lookups off
+                    flagged = (sc.n_obbs && sphere_obb_any(sc, nullptr, 0, px, py, pz, sr, nullptr, st)) ||
                               (sc.n_layers && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
                 }
                 // ---- exact spheres of this joint ----
@@ -409,8 +409,9 @@ extern "C" int ps_check_configs(const ps_model* m, const ps_scene_view* scene, c
     size_t smem = (size_t)m->dev.bytes_core + scene_smem_bytes(scene) + (size_t)kCfgThreads * m->info.n_dof * 4;
     const int blocks_needed = (n + kCfgThreads - 1) / kCfgThreads;
     const int grid = std::max(1, std::min(blocks_needed, sm_count() * 8));
+    // (sphere_obb_acm_mask_approx changes no result: see the approximate gate)
     const bool fast = m->root_slot_only && m->info.approx_shares_chain && !scene->sphere_obb_acm_mask &&
-                      !scene->sphere_obb_acm_mask_approx && !scene->sphere_acm_mask;
+                      !scene->sphere_acm_mask;
     auto k = fast ? (clr ? (g_stats ? check_configs_fast_kernel<true, true> : check_configs_fast_kernel<true, false>)
                          : (g_stats ? check_configs_fast_kernel<false, true> : check_configs_fast_kernel<false, false>))
                   : (clr ? (g_stats ? check_configs_kernel<true, true> : check_configs_kernel<true, false>)

@@ -195,9 +195,9 @@ __device__ bool process_chunk(const ModelSmem& M, const SceneSmem& sc, const ps_
             sphere_world(shares ? T : TA, sa.x, sa.y, sa.z, px, py, pz);
             if (real) st.v[ST_SPHERES] += 1;
             const float sr = __fadd_rn(sa.w, margin);
-            const uint8_t* acm =
-                sv.sphere_obb_acm_mask_approx ? sv.sphere_obb_acm_mask_approx + (size_t)M.AO[k] * sv.n_obbs : nullptr;
-            flagged = (ncand > 0 && sphere_obb_any(sc, cand, ncand, px, py, pz, sr, acm, st)) ||
+            // no mask in the approximate pass (sphere index -1 in the
+            // reference, scene_collision.cuh:584-606)
+            flagged = (ncand > 0 && sphere_obb_any(sc, cand, ncand, px, py, pz, sr, nullptr, st)) ||
                       (sc.n_layers && sphere_esdf_any(sc, sv, px, py, pz, sr, nullptr, st));
         }
         // ---- exact spheres of a flagged joint (and ESDF clearance) ----
@@ -691,7 +691,9 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode == 1 ? 5 : (kMode ? 6 : 3)
             const ChunkOrder ord(G);
             if (k < ord.rounds()) {
                 k = ord.chunk(k);   // round -> chunk index
-                live = k < ord.nc && vbad[e] == 0;
+                // a retired edge's remaining chunks still count toward the
+                // clearance, which covers every sample (edge_eval.cuh:133-153)
+                live = k < ord.nc && (P.compute_clearance || vbad[e] == 0);
             }
         }
         unsigned todo = __ballot_sync(kFull, live);
@@ -890,8 +892,9 @@ int launch_edges_self(const ps_model* m, const ps_edge_params* P, const float* f
 // The self check (check_self) is a separate pass (edges_self_kernel) after
 // either variant.
 int fast_path(const ps_model* m, const ps_scene_view* sv, const ps_edge_params* P) {
+    // (sphere_obb_acm_mask_approx changes no result: the approximate gate applies no mask)
     const bool fast = m->info.approx_shares_chain && m->root_slot_only && !P->compute_clearance &&
-                      !sv->sphere_obb_acm_mask && !sv->sphere_obb_acm_mask_approx && !sv->sphere_acm_mask;
+                      !sv->sphere_obb_acm_mask && !sv->sphere_acm_mask;
     return fast ? (sv->n_voxel_layers > 0 ? 2 : 1) : 0;
 }
 

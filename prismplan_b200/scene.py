@@ -100,11 +100,22 @@ class SceneCollisionDataBuilder:
 class SceneTensors:
     """Device tensors of one scene plus the builder that points at them.
 
-    ``host`` keeps the float32 host arrays (what the oracle consumes)."""
+    ``host`` keeps the float32 host arrays (what the oracle consumes).
+
+    Optional allowed-collision masks, uint8 with 0 = pair ignored, indexed by
+    the robot descriptor's sphere order (scene_collision_data.hh):
+    ``sphere_acm_mask`` [n_spheres, n_voxel_layers], ``sphere_obb_acm_mask``
+    [n_spheres, n_obbs] and ``sphere_obb_acm_mask_approx`` [n_approx_spheres,
+    n_obbs]. The reference's approximate pass looks neither mask up
+    (scene_collision.cuh:584-606 passes sphere index -1), so the approximate
+    one is carried for layout parity and changes no result."""
+
+    _MASKS = ("sphere_acm_mask", "sphere_obb_acm_mask", "sphere_obb_acm_mask_approx")
 
     def __init__(self, obb_dims, obb_pose, obb_enable, voxel_params=None, voxel_pose=None,
                  voxel_enable=None, voxel_features=None, esdf_mode=_lib.PS_ESDF_NEAREST,
-                 device="cuda"):
+                 device="cuda", sphere_acm_mask=None, sphere_obb_acm_mask=None,
+                 sphere_obb_acm_mask_approx=None):
         import torch
 
         self.host = {
@@ -119,6 +130,15 @@ class SceneTensors:
             self.host["voxel_enable"] = (np.ones(n_layers, np.uint8) if voxel_enable is None
                                          else np.ascontiguousarray(voxel_enable, np.uint8).reshape(-1))
             self.host["voxel_features"] = np.ascontiguousarray(voxel_features, np.float32).reshape(n_layers, -1)
+        n_obbs = self.host["obb_dims"].shape[0]
+        for name, m, cols in zip(self._MASKS, (sphere_acm_mask, sphere_obb_acm_mask, sphere_obb_acm_mask_approx),
+                                 (n_layers, n_obbs, n_obbs)):
+            if m is None:
+                continue
+            m = np.ascontiguousarray(m, np.uint8)
+            if cols == 0 or m.size % cols:
+                raise ValueError(f"{name}: {m.size} entries is not a whole number of rows of {cols}")
+            self.host[name] = m.reshape(-1, cols)
         self.esdf_mode = esdf_mode
         self.device = device
         dev = torch.device(device)
@@ -137,8 +157,17 @@ class SceneTensors:
             b.voxel_features_ptr = t["voxel_features"].data_ptr()
             b.n_voxel_layers = n_layers
             b.max_voxels_per_layer = self.host["voxel_features"].shape[1]
+        for name in self._MASKS:
+            if name in t:
+                setattr(b, name + "_ptr", t[name].data_ptr())
         b.esdf_mode = esdf_mode
         self.builder = b
+
+    @property
+    def masks(self) -> Dict[str, np.ndarray]:
+        """The host masks by the oracle's names (acm, obb_acm, obb_acm_apx)."""
+        keys = dict(zip(self._MASKS, ("acm", "obb_acm", "obb_acm_apx")))
+        return {keys[k]: self.host[k] for k in self._MASKS if k in self.host}
 
     @property
     def n_obbs(self) -> int:

@@ -61,6 +61,28 @@ def test_oracle_verdicts_match_reference_numpy(golden, name, gate):
         assert len(bad) == 0 or np.abs(gap[bad]).max() < 1e-6, (s, bad, gap[bad])
 
 
+def test_oracle_masks_follow_reference_rules(golden):
+    """Allowed-collision masks in the oracle, by the reference's rules
+    (scene_collision.cuh:118-135 skips a box whose mask entry is 0 for the
+    sphere's index; :584-606 gives the approximate pass sphere index -1, so it
+    applies no mask): all-ones masks change nothing, an all-zero exact mask
+    frees every configuration of a box-only scene, and the approximate mask
+    changes nothing whatever it holds."""
+    asset, raw = golden_asset(golden, "panda")
+    b = RobotModelBuilder.from_asset(asset)
+    d, p, en = pack_obbs(raw["obb_dims"][0], raw["obb_pos"][0], raw["obb_quat"][0])
+    ns, na, no = len(b.sphere_to_joint), len(np.asarray(asset["approx_spheres_flat"])) // 4, len(d)
+    om = oracle.OracleModel(b, d, p, en)
+    base, _, _ = om.check_configs(raw["q"], prec=64)
+    assert 0 < base.sum() < len(base)
+    om.set_masks(None, np.ones((ns, no), np.uint8), np.ones((na, no), np.uint8))
+    np.testing.assert_array_equal(om.check_configs(raw["q"], prec=64)[0], base)
+    om.set_masks(None, None, np.zeros((na, no), np.uint8))
+    np.testing.assert_array_equal(om.check_configs(raw["q"], prec=64)[0], base)
+    om.set_masks(None, np.zeros((ns, no), np.uint8), None)
+    assert om.check_configs(raw["q"], prec=64)[0].sum() == 0
+
+
 def test_oracle_fp32_baseline_agrees_with_fp64():
     wl = workloads.workload(1, scale=0.25)
     b = RobotModelBuilder.from_asset(wl["asset"])
