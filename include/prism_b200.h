@@ -113,8 +113,9 @@ typedef struct ps_model_info {
 int ps_model_create(const ps_model_desc* desc, ps_model** out);
 /* Frees the device blob. Safe on NULL. */
 int ps_model_destroy(ps_model* model);
-/* Re-uploads joint limits (and the derived range) without a rebuild
-   (bindings.cpp:175-205). Host arrays of n_dof floats. Synchronous. */
+/* Re-uploads joint limits without a rebuild (bindings.cpp:181-205). Host
+   arrays of n_dof floats. Synchronous. The reference also re-derives
+   joint_range = upper - lower; no kernel here reads a range, so none is kept. */
 int ps_model_set_limits(ps_model* model, const float* lower, const float* upper);
 int ps_model_get_info(const ps_model* model, ps_model_info* info);
 /* Reads and clears the model's device error latch (synchronous): *code is

@@ -260,3 +260,30 @@ def test_time_limit_and_edge_cases(solve_case):
     ws = torch.empty(256, dtype=torch.uint8, device="cuda")
     with pytest.raises(_lib.PrismError):
         api.chomp_optimize(b, sc, torch.from_numpy(th0).cuda(), _settings(wl), workspace=ws)
+
+
+def test_update_joint_limits_equals_rebuild(solve_case):
+    """update_joint_limits (bindings.cpp:181-205) reaches the device: CHOMP
+    clamps its updates to the model's limits (chomp.cu:259-289), and a model
+    whose limits were narrowed in place gives the same bits as one built with
+    the narrowed limits, inside those limits."""
+    wl, _, sc, starts, goals = solve_case
+    asset = wl["asset"]
+    lo = np.asarray(asset["joint_lower"], np.float32)
+    hi = np.asarray(asset["joint_upper"], np.float32)
+    mid, half = (lo + hi) * 0.5, (hi - lo) * 0.25
+    lo2, hi2 = (mid - half).astype(np.float32), (mid + half).astype(np.float32)
+    st, gl = np.clip(starts[:8], lo2, hi2), np.clip(goals[:8], lo2, hi2)
+    s = _free_run(wl, num_iterations=40)
+    moved = RobotModelBuilder.from_asset(asset).build()
+    wide = api.chomp_solve(moved, sc, st, gl, s).path.cpu().numpy()
+    moved.joint_lower, moved.joint_upper = lo2.tolist(), hi2.tolist()
+    moved.update_joint_limits()
+    fresh = RobotModelBuilder.from_asset(dict(asset, joint_lower=lo2.tolist(), joint_upper=hi2.tolist())).build()
+    a = api.chomp_solve(moved, sc, st, gl, s).path.cpu().numpy()
+    f = api.chomp_solve(fresh, sc, st, gl, s).path.cpu().numpy()
+    outside = ((wide < lo2) | (wide > hi2)).mean()
+    print(f"share of waypoint values outside the narrowed limits with the original ones: {outside:.3f}")
+    assert np.array_equal(a.view(np.uint32), f.view(np.uint32))
+    assert (a >= lo2).all() and (a <= hi2).all()
+    assert outside > 0

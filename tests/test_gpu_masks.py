@@ -22,10 +22,15 @@ from prismplan_b200.scene import SceneTensors
 pytestmark = pytest.mark.gpu
 
 
-def two_layer_esdf(rng):
+def three_layer_esdf(rng):
+    """Three ESDF layers, the middle one disabled: mask columns follow the
+    layers' own indices."""
     a = workloads.random_esdf(rng, n_vox=48, voxel=0.02, centre=(0.45, 0.0, 0.45))
-    b = workloads.random_esdf(rng, n_vox=48, voxel=0.02, centre=(0.2, 0.35, 0.6))
-    return tuple(np.concatenate([x, y]) for x, y in zip(a, b))
+    c = workloads.random_esdf(rng, n_vox=48, voxel=0.02, centre=(0.2, 0.35, 0.6))
+    off = workloads.random_esdf(np.random.default_rng(5), n_vox=48, voxel=0.02, centre=(0.2, 0.35, 0.6))
+    out = tuple(np.concatenate(x) for x in zip(a, off, c))
+    out[2][1] = 0
+    return out
 
 
 @pytest.fixture(scope="module")
@@ -33,13 +38,14 @@ def case(golden):
     asset, _ = golden_asset(golden, "panda")
     rng = np.random.default_rng(77)
     obbs = workloads.random_obbs(rng, 16)
-    esdf = two_layer_esdf(rng)
+    obbs[2][[3, 9]] = 0        # disabled boxes: the masks index the boxes as given
+    esdf = three_layer_esdf(rng)
     b = RobotModelBuilder.from_asset(asset).build()
     ns = len(b.sphere_to_joint)
     na = len(np.asarray(asset["approx_spheres_flat"]).reshape(-1, 4))
     masks = {
-        "sphere_acm_mask": (rng.random((ns, 2)) > 0.3).astype(np.uint8),
-        "sphere_obb_acm_mask": (rng.random((ns, 16)) > 0.3).astype(np.uint8),
+        "sphere_acm_mask": (rng.random((ns, 3)) > 0.5).astype(np.uint8),
+        "sphere_obb_acm_mask": (rng.random((ns, 16)) > 0.5).astype(np.uint8),
         "sphere_obb_acm_mask_approx": np.zeros((na, 16), np.uint8),
     }
     sc = SceneTensors(*obbs, *esdf, **masks)
