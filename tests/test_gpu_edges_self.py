@@ -68,6 +68,22 @@ def test_edges_self_bitexact_vs_reference(case):
     np.testing.assert_array_equal(v0.cpu().numpy(), rv_scene)
 
 
+def test_edges_self_with_margin(case):
+    """A collision margin widens the scene spheres only: the self pairs of
+    two_phase_cc take none (two_phase_cc.cuh:109-131)."""
+    asset, obbs, b, sc, frm, to, G, ref = case
+    n = 1200
+    rv, rc, _ = ref.check_edges(frm[:n], to[:n], G[:n], margin=0.01, check_self=True)
+    rv0, _, _ = ref.check_edges(frm[:n], to[:n], G[:n], margin=0.0, check_self=True)
+    assert (rv != rv0).any()
+    f, t, g = (torch.from_numpy(x[:n]).cuda() for x in (frm, to, G))
+    p = api.EdgeEvalParams(check_self=True, collision_margin=0.01)
+    for persistent in (True, False):
+        v, c, _ = api.check_edges(b, sc, f, t, samples=g, params=p, persistent=persistent)
+        np.testing.assert_array_equal(v.cpu().numpy(), rv, err_msg=f"persistent={persistent}")
+        assert np.array_equal(c.cpu().numpy().view(np.uint32), rc.view(np.uint32))
+
+
 def test_batch_edges_with_self(case):
     asset, obbs, b, sc, frm, to, G, ref = case
     p = api.EdgeEvalParams(check_self=True)

@@ -166,6 +166,17 @@ def test_costs_with_masks(case):
     relr = np.abs(rc - theirs) / np.maximum(np.abs(theirs), 1.0)
     print(f"masked rollout cost: max rel diff vs reference stomp kernel {relr.max():.2e}")
     assert relr.max() < 1e-3
+    # the mixed batch's trajectory branch reads the same masks: bitwise equal
+    batch = api.MixedBatch(b, 0, 0, 2, 2 * T, T)
+    qt = [torch.from_numpy(q[i]).cuda() for i in (0, 7)]
+    outs = [batch.add_trajectory(x) for x in qt]
+    batch.launch(sc, api.EdgeEvalParams(), p)
+    torch.cuda.synchronize()
+    for x, (bw, bt, bg) in zip(qt, outs):
+        w1, t1, g1 = api.traj_cost(b, sc, x[None], p)
+        assert torch.equal(bw.view(torch.int32), w1[0].view(torch.int32))
+        assert torch.equal(bg.view(torch.int32), g1[0].view(torch.int32))
+    batch.close()
 
 
 def test_cost_gradient_with_obb_masks(case):
