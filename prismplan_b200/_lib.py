@@ -28,6 +28,16 @@ PS_LAYOUT_BDT = 1
 
 PS_MAX_DOF = 14
 PS_MAX_JOINTS = 20
+PS_MAX_SPHERES = 512
+PS_MAX_OBBS = 1024
+PS_MAX_LAYERS = 8
+PS_EDGES_STATIC_MAX = 65536
+PS_MAX_TRAJ_LEN = 16384
+
+# joint types (utils.cuh:20-26)
+PS_FIXED = -1
+PS_X_PRISM, PS_Y_PRISM, PS_Z_PRISM = 0, 1, 2
+PS_X_ROT, PS_Y_ROT, PS_Z_ROT = 3, 4, 5
 
 
 class PrismError(RuntimeError):

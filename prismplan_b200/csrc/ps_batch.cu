@@ -250,6 +250,7 @@ int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, 
         L.pgrid = std::max(1, std::min((b->lim.max_edges + 255) / 256, sms * 4));
         L.req_grid_e = std::max(1, std::min(b->lim.max_edge_requests, sms * 8));
         if (ep->check_self) {
+            if (int rc = check_self_fits(m)) return rc;
             L.ssmem = self_smem_bytes(m);
             PS_TRY_CUDA(cudaFuncSetAttribute(edges_self_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)L.ssmem));

@@ -422,6 +422,7 @@ extern "C" int ps_check_configs(const ps_model* m, const ps_scene_view* scene, c
     mark_stop(s);
     PS_TRY_CUDA(cudaGetLastError());
     if (flags & PS_CHECK_SELF) {
+        if (int rc = check_self_fits(m)) return rc;
         const size_t ss = self_smem_bytes(m);
         PS_TRY_CUDA(cudaFuncSetAttribute(self_check_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
         const int g2 = std::max(1, std::min((n + kSelfThreads - 1) / kSelfThreads, sm_count() * 8));

@@ -874,6 +874,7 @@ int launch_edges_self(const ps_model* m, const ps_edge_params* P, const float* f
                       const int* given, int n_edges, const int* Gs, int* bad, uint8_t* valid, float* cost,
                       EdgeWs* hdr, const int* n_dev, cudaStream_t s) {
     if (!P->check_self || n_edges <= 0) return PS_OK;
+    if (int rc = check_self_fits(m)) return rc;
     const size_t smem = self_smem_bytes(m);
     PS_TRY_CUDA(cudaFuncSetAttribute(edges_self_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;

@@ -54,6 +54,8 @@ size_t scene_smem_bytes(const ps_scene_view* s);
 
 // Number of SMs of the current device (cached).
 int sm_count();
+// Largest dynamic shared memory one block may opt into on the current device.
+size_t smem_optin();
 
 // Diagnostics shared by every launcher (set through ps_set_stats /
 // ps_set_timing_events).

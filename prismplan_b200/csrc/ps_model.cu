@@ -36,6 +36,18 @@ int cuda_error(cudaError_t e, const char* where) {
 
 void clear_error() { g_last_error.clear(); }
 
+size_t smem_optin() {
+    static thread_local int dev_cached = -1;
+    static thread_local int bytes = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != dev_cached) {
+        cudaDeviceGetAttribute(&bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        dev_cached = dev;
+    }
+    return (size_t)bytes;
+}
+
 int sm_count() {
     static thread_local int dev_cached = -1, sms = 0;
     int dev = 0;

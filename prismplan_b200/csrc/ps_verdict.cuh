@@ -373,4 +373,17 @@ inline size_t self_smem_bytes(const ps_model* m) {
            (size_t)kSelfThreads * m->info.n_dof * 4;
 }
 
+// PS_EINVAL with the sizes when the self check's block does not fit in shared
+// memory: about 280 spheres, approximate spheres and joints together on a
+// B200 (the reference's edge kernel stages at most 125 spheres, 52
+// approximate ones: edge_eval.cuh:83-84).
+inline int check_self_fits(const ps_model* m) {
+    const size_t need = self_smem_bytes(m), have = smem_optin();
+    if (need <= have) return PS_OK;
+    return set_error(PS_EINVAL, "check_self: n_spheres + n_approx_spheres + n_joints = " +
+                                    std::to_string(m->info.n_spheres + m->info.n_approx_spheres + m->info.n_joints) +
+                                    " needs " + std::to_string(need) + " bytes of shared memory per block, above the "
+                                    "device's " + std::to_string(have));
+}
+
 }  // namespace ps

@@ -25,6 +25,16 @@ def test_python_binding_covers_header():
     assert sorted(header_symbols()) == sorted(_lib.EXPORTED_SYMBOLS)
 
 
+def test_binding_constants_match_header():
+    text = (ROOT / "include" / "prism_b200.h").read_text()
+    defines = {k: int(v, 0) for k, v in
+               re.findall(r"#define\s+(PS_[A-Z0-9_]+)\s+\(?(-?(?:0x[0-9a-fA-F]+|\d+))u?\)?", text)}
+    assert len(defines) > 20
+    missing = [k for k in defines if not hasattr(_lib, k)]
+    assert not missing, missing
+    assert {k: getattr(_lib, k) for k in defines} == defines
+
+
 def test_binding_loads_and_reports_version():
     lib = _lib.load()
     assert lib.ps_version().startswith(b"prismplan_b200")
