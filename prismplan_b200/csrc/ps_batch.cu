@@ -223,6 +223,7 @@ struct LaunchPlan {
     void (*wk)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*) = nullptr;
     size_t qsmem = 0, wsmem = 0, fsmem = 0, ssmem = 0;
     int qgrid = 1, wgrid = 1, req_grid_e = 1, req_grid_t = 1, pgrid = 1, sgrid = 1;
+    ProbePlan probe;
 };
 
 using WaypointKernel = void (*)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*);
@@ -247,6 +248,7 @@ int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, 
         PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L.qk, kEdgeThreads, L.qsmem));
         if (per_sm < 1) return set_error(PS_EINVAL, "edge kernel does not fit on an SM with this scene");
         L.qgrid = std::max(1, (int)(b->edge_share * sms * per_sm + 0.5f));
+        if (int rc = plan_probe(m, sv, L.mode, false, b->edge_share, b->lim.max_edges, L.probe)) return rc;
         L.pgrid = std::max(1, std::min((b->lim.max_edges + 255) / 256, sms * 4));
         L.req_grid_e = std::max(1, std::min(b->lim.max_edge_requests, sms * 8));
         if (ep->check_self) {
@@ -298,6 +300,10 @@ void record_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep
         batch_gather_edges<<<L.req_grid_e, 128, 0, s0>>>(b->d_ereq, b->d_cnt, *ep, D, b->d_from, b->d_to, b->d_given);
         edges_prep_kernel<<<L.pgrid, 256, 0, s0>>>(*ep, b->d_from, b->d_to, b->d_given, b->lim.max_edges, D, b->d_hdr,
                                                    b->d_G, b->d_len, b->d_bad, b->d_clr, b->d_done, n_dev);
+        if (L.probe.k)
+            L.probe.k<<<L.probe.grid, kProbeThreads, L.probe.smem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to,
+                                                                          b->lim.max_edges, b->d_hdr, b->d_G,
+                                                                          b->d_bad, nullptr, n_dev);
         L.qk<<<L.qgrid, kEdgeThreads, L.qsmem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to, b->lim.max_edges, b->d_hdr,
                                                     b->d_G, b->d_bad, b->d_clr, b->d_done, nullptr, 0, n_dev);
         L.qk<<<L.qgrid, kEdgeThreads, L.qsmem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to, b->lim.max_edges, b->d_hdr,

@@ -20,28 +20,6 @@ namespace {
 
 constexpr int kCfgThreads = 128;
 
-// Min d^2 over every box for kN sphere centres at once (one box load per kN
-// pair tests); no ACM masks.
-template <int kN>
-__device__ __forceinline__ void spheres_min_dsq(const SceneSmem& sc, const float* px, const float* py,
-                                                const float* pz, float* mn) {
-#pragma unroll
-    for (int i = 0; i < kN; ++i) mn[i] = 3.0e38f;
-    for (int o = 0; o < sc.n_obbs; ++o) {
-        const ObbPrep& b = sc.obbs[o];
-        const float4 r0 = b.r0, r1 = b.r1, r2 = b.r2, h = b.h;
-#pragma unroll
-        for (int i = 0; i < kN; ++i) {
-            const float lx = fmaf(r0.z, pz[i], fmaf(r0.y, py[i], fmaf(r0.x, px[i], r0.w)));
-            const float ly = fmaf(r1.z, pz[i], fmaf(r1.y, py[i], fmaf(r1.x, px[i], r1.w)));
-            const float lz = fmaf(r2.z, pz[i], fmaf(r2.y, py[i], fmaf(r2.x, px[i], r2.w)));
-            const float cx = fmaxf(fabsf(lx) - h.x, 0.0f), cy = fmaxf(fabsf(ly) - h.y, 0.0f),
-                        cz = fmaxf(fabsf(lz) - h.z, 0.0f);
-            mn[i] = fminf(mn[i], fmaf(cz, cz, fmaf(cy, cy, cx * cx)));
-        }
-    }
-}
-
 // SDF of a point from its min outside d^2 over the boxes (as
 // sphere_obb_min_sdf): sqrt when outside every box, else the most negative
 // max(q) over the boxes that contain it.

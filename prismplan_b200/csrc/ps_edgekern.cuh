@@ -614,6 +614,188 @@ __global__ void edges_prep_kernel(ps_edge_params P, const float* __restrict__ fr
     }
 }
 
+// ---------------------------------------------------------------------------
+// End-sample probe (persistent path, boxes-only fast variant)
+// ---------------------------------------------------------------------------
+// Before the chunk queue starts, one thread per edge checks the edge's last
+// sample (j = G, t = 1, formed as the chunk path forms it) and retires the
+// edge on a hit (bad[e] = 1). The verdict is the OR over the samples, so
+// checking one of them first changes no result; the queue skips retired
+// edges. A warp chunk costs 32 lanes for an edge that collides at its end
+// sample, the probe one lane: on uniformly drawn edges about 85 % of the
+// colliding ones collide there. The probe is best effort: a lane whose joint
+// reaches more than kProbeCand boxes stops and leaves its edge to the queue.
+constexpr int kProbeThreads = 128;
+constexpr int kProbeCand = 32;                 // candidate boxes a lane keeps for one joint
+constexpr int kProbeStride = kProbeCand + 2;   // 17 words per lane: lanes hit distinct banks
+
+// The fast chunk verdict (process_chunk_fast) for one configuration held by
+// one thread: per joint, the boxes within reach of the joint's bound sphere
+// (same guarded limits, radius of one sample), the exact spheres 4 per box
+// load against them, the approximate gate only after an exact hit. Returns
+// true on a confirmed hit, false when none was found or the lane gave up.
+template <bool kStats>
+__device__ bool lane_probe_hit(const ModelSmem& M, const SceneSmem& sc, const float4* __restrict__ obs,
+                               uint16_t* cand, const float* qc, float margin, LaneStats& st) {
+    const int NJ = M.H->n_joints;
+    Affine T;
+    affine_identity(T);
+    for (int p = 0; p < NJ; ++p) {
+        const JointRec& jr = M.J[p];
+        if (p > 0) {
+            const float qi = jr.dof >= 0 ? qc[jr.dof] : 0.0f;
+            if (jr.parent_slot == 0) {
+                Affine I;
+                affine_identity(I);
+                joint_compose<true>(jr, qi, I, T);
+            } else {
+                joint_compose<true>(jr, qi, T, T);   // rows are read before they are written
+            }
+            if (kStats) st.v[ST_JOINTS] += 1;
+        }
+        if (jr.bound.w < 0.0f) continue;
+        float cx, cy, cz;
+        sphere_world(T, jr.bound.x, jr.bound.y, jr.bound.z, cx, cy, cz);
+        const float Sm = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz)));
+        float Rc = jr.bound.w + fmaxf(margin, 0.0f);
+        Rc += 4.0f * (Sm + Rc + sc.Bmax + 1.0f) * PS_GUARD_K;
+        const float Rc2 = Rc * Rc;
+        const float Rj = (Rc * (1.0f + 4.0f * PS_GUARD_K) + 4.0f * PS_GUARD_K * (Sm + 1.0f)) * (1.0f + 1.0e-6f);
+        int ncand = 0;
+#pragma unroll 1
+        for (int o = 0; o < sc.n_obbs; ++o) {
+            const float4 ob = obs[o];
+            const float ex = ob.x - cx, ey = ob.y - cy, ez = ob.z - cz;
+            const float lim = Rj + ob.w;   // see box_limits
+            if (kStats) st.v[ST_CULL] += 1;
+            if (fmaf(ez, ez, fmaf(ey, ey, ex * ex)) >= lim * lim) continue;
+            float qx, qy, qz;
+            if (fast_box_dsq(sc.obbs[o], cx, cy, cz, qx, qy, qz) >= Rc2) continue;
+            if (ncand == kProbeCand) return false;   // too many: the queue takes this edge
+            cand[ncand++] = (uint16_t)o;
+        }
+        if (ncand == 0) continue;
+        const float g = (Sm + jr.bound.w + sc.Bmax + 1.0f) * PS_GUARD_K;
+        bool ex = false;
+        int k = jr.sph_beg;
+        for (; k + 4 <= jr.sph_end && !ex; k += 4) {
+            float px[4], py[4], pz[4], sr[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const float4 sp = M.S[k + i];
+                sphere_world(T, sp.x, sp.y, sp.z, px[i], py[i], pz[i]);
+                sr[i] = __fadd_rn(sp.w, margin);
+            }
+            if (kStats) st.v[ST_SPHERES] += 4;
+            ex = spheres_hit<4, kStats>(sc, cand, ncand, px, py, pz, sr, g, st);
+        }
+        for (; k < jr.sph_end && !ex; ++k) {
+            const float4 sp = M.S[k];
+            float px, py, pz;
+            sphere_world(T, sp.x, sp.y, sp.z, px, py, pz);
+            const float sr = __fadd_rn(sp.w, margin);
+            if (kStats) st.v[ST_SPHERES] += 1;
+            ex = spheres_hit<1, kStats>(sc, cand, ncand, &px, &py, &pz, &sr, g, st);
+        }
+        if (!ex) continue;
+        bool flagged = false;
+        for (int a = jr.apx_beg; a < jr.apx_end && !flagged; ++a) {
+            const float4 sa = M.A[a];
+            float px, py, pz;
+            sphere_world(T, sa.x, sa.y, sa.z, px, py, pz);
+            const float sr = __fadd_rn(sa.w, margin);
+            if (kStats) st.v[ST_SPHERES] += 1;
+            flagged = spheres_hit<1, kStats>(sc, cand, ncand, &px, &py, &pz, &sr, g, st);
+        }
+        if (flagged) return true;
+    }
+    return false;
+}
+
+// Shared memory: model core, staged scene, one configuration per thread, box
+// spheres, per-thread candidate lists.
+size_t probe_smem_bytes(const ps_model* m, const ps_scene_view* sv) {
+    return (size_t)m->dev.bytes_core + scene_smem_bytes(sv) + (size_t)kProbeThreads * m->info.n_dof * 4 +
+           (size_t)16 * std::max(sv->n_obbs, 1) + (size_t)kProbeThreads * kProbeStride * 2;
+}
+
+template <bool kStats>
+__global__ void __launch_bounds__(kProbeThreads, 4) edges_probe_kernel(ModelDev md, ps_scene_view sv,
+                                                                        ps_edge_params P,
+                                                                        const float* __restrict__ from,
+                                                                        const float* __restrict__ to, int n_edges,
+                                                                        EdgeWs* hdr, const int* __restrict__ Gs,
+                                                                        int* bad, unsigned long long* stats,
+                                                                        const int* n_dev = nullptr) {
+    if (n_dev) n_edges = *n_dev;
+    if (n_edges <= 0) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ int counters[4];
+    __shared__ float bmax;
+    if (!stage_model(md, smem, &mbar)) return;
+    ObbPrep* obbs = reinterpret_cast<ObbPrep*>(smem + md.bytes_core);
+    const int nob = max(sv.n_obbs, 1);
+    int* orig = reinterpret_cast<int*>(obbs + nob);
+    LayerPrep* layers = reinterpret_cast<LayerPrep*>(orig + ((nob + 3) & ~3));
+    SceneSmem sc;
+    stage_scene(sv, obbs, orig, layers, counters, &bmax, sc);
+    const ModelSmem M = model_view(smem);
+    const int D = M.H->n_dof;
+    float* qtile = reinterpret_cast<float*>(layers + PS_MAX_LAYERS);
+    float4* obs = reinterpret_cast<float4*>(qtile + kProbeThreads * D);
+    uint16_t* cand = reinterpret_cast<uint16_t*>(obs + nob) + threadIdx.x * kProbeStride;
+    box_spheres(sc, obs);
+    __syncthreads();
+    box_limits(sc, obs);
+    __syncthreads();
+    float* qc = qtile + threadIdx.x * D;
+    const unsigned long long deadline = *((volatile unsigned long long*)&hdr->deadline);
+    LaneStats st;
+    st.zero();
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_edges; e += gridDim.x * blockDim.x) {
+        const int G = Gs[e];
+        if (G <= 0) continue;
+        if (deadline && global_ns() > deadline) break;   // the queue reports the timeout
+        const float t = __fdiv_rn((float)G, (float)G);   // sample j = G, as process_chunk forms it
+        const float* a = from + (size_t)e * D;
+        const float* b = to + (size_t)e * D;
+        for (int i = 0; i < D; ++i) {
+            const float ai = __ldg(a + i), bi = __ldg(b + i);
+            qc[i] = __fmaf_rn(t, __fadd_rn(bi, -ai), ai);
+        }
+        if (kStats) st.v[ST_SAMPLES] += 1;
+        if (lane_probe_hit<kStats>(M, sc, obs, cand, qc, P.collision_margin, st)) bad[e] = 1;
+    }
+    flush_stats(stats, st);
+}
+
+// Kernel, shared memory and grid of the probe for edge variant `mode`: the
+// boxes-only fast variant only (the generic one serves clearance, which
+// wants every sample, and masks; the ESDF lookups do not pay off one lane at
+// a time). `share` scales the grid (mixed batch).
+struct ProbePlan {
+    void (*k)(ModelDev, ps_scene_view, ps_edge_params, const float*, const float*, int, EdgeWs*, const int*, int*,
+              unsigned long long*, const int*) = nullptr;
+    size_t smem = 0;
+    int grid = 1;
+};
+
+int plan_probe(const ps_model* m, const ps_scene_view* sv, int mode, bool stats, float share, int max_edges,
+               ProbePlan& out) {
+    out = ProbePlan{};
+    if (mode != 1 || max_edges <= 0 || sv->n_obbs == 0) return PS_OK;
+    out.k = stats ? edges_probe_kernel<true> : edges_probe_kernel<false>;
+    out.smem = probe_smem_bytes(m, sv);
+    PS_TRY_CUDA(cudaFuncSetAttribute(out.k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)out.smem));
+    int per_sm = 0;
+    PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, out.k, kProbeThreads, out.smem));
+    if (per_sm < 1) return set_error(PS_EINVAL, "edge probe kernel does not fit on an SM with this scene");
+    const int cap = (max_edges + kProbeThreads - 1) / kProbeThreads;
+    out.grid = std::max(1, std::min(cap, (int)(share * sm_count() * per_sm + 0.5f)));
+    return PS_OK;
+}
+
 // Residency per variant, measured: the boxes-only fast path runs fastest
 // with 5 blocks per SM (room for 96 registers), the ESDF variant with 6.
 template <int kMode, bool kStats>

@@ -92,7 +92,8 @@ EdgeBufs carve_workspace(void* ws, int n_edges) {
     return b;
 }
 
-// memset header -> prep -> queue pass(es) -> finalize on stream s.
+// memset header -> prep -> end-sample probe -> queue pass(es) -> self pass ->
+// finalize on stream s.
 int run_persistent(const ps_model* m, const ps_scene_view* scene, const float* from, const float* to,
                    const int* samples_per_edge, int n_edges, const ps_edge_params* P, uint8_t* valid, float* cost,
                    float* clearance, const EdgeBufs& b, cudaStream_t s) {
@@ -103,14 +104,20 @@ int run_persistent(const ps_model* m, const ps_scene_view* scene, const float* f
                                             b.clr, b.done);
     PS_TRY_CUDA(cudaGetLastError());
     const size_t smem = edge_smem_bytes(m, scene);
-    auto qk = pick(fast_path(m, scene, P), g_stats != nullptr, edges_queue_kernel<0, false>,
-                   edges_queue_kernel<0, true>, edges_queue_kernel<1, false>, edges_queue_kernel<1, true>,
-                   edges_queue_kernel<2, false>, edges_queue_kernel<2, true>);
+    const int mode = fast_path(m, scene, P);
+    auto qk = pick(mode, g_stats != nullptr, edges_queue_kernel<0, false>, edges_queue_kernel<0, true>,
+                   edges_queue_kernel<1, false>, edges_queue_kernel<1, true>, edges_queue_kernel<2, false>,
+                   edges_queue_kernel<2, true>);
     PS_TRY_CUDA(cudaFuncSetAttribute(qk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qk, kEdgeThreads, smem));
     const int qgrid = std::max(1, sm_count() * std::max(per_sm, 1));
+    ProbePlan probe;
+    if (int rc = plan_probe(m, scene, mode, g_stats != nullptr, 1.0f, n_edges, probe)) return rc;
     mark_start(s);
+    if (probe.k)
+        probe.k<<<probe.grid, kProbeThreads, probe.smem, s>>>(m->dev, *scene, *P, from, to, n_edges, b.hdr, b.G,
+                                                               b.bad, g_stats, nullptr);
     qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, b.hdr, b.G, b.bad, b.clr, b.done,
                                          g_stats, 0, nullptr);
     if ((long long)n_edges < 8ll * qgrid * kEdgeThreads / 32)   // the kernel's own split rule
