@@ -662,16 +662,39 @@ __device__ bool lane_probe_hit(const ModelSmem& M, const SceneSmem& sc, const fl
         const float Rc2 = Rc * Rc;
         const float Rj = (Rc * (1.0f + 4.0f * PS_GUARD_K) + 4.0f * PS_GUARD_K * (Sm + 1.0f)) * (1.0f + 1.0e-6f);
         int ncand = 0;
+        int o = 0;
+        // circumscribed-sphere tests 4 boxes at a time (independent, so they
+        // overlap), the box distance for the ones that pass
 #pragma unroll 1
-        for (int o = 0; o < sc.n_obbs; ++o) {
+        for (; o + 4 <= sc.n_obbs; o += 4) {
+            unsigned pass = 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const float4 ob = obs[o + i];
+                const float ex = ob.x - cx, ey = ob.y - cy, ez = ob.z - cz;
+                const float lim = Rj + ob.w;   // see box_limits
+                pass |= (fmaf(ez, ez, fmaf(ey, ey, ex * ex)) < lim * lim ? 1u : 0u) << i;
+            }
+            if (kStats) st.v[ST_CULL] += 4;
+            while (pass) {
+                const int oo = o + __ffs(pass) - 1;
+                pass &= pass - 1;
+                float qx, qy, qz;
+                if (fast_box_dsq(sc.obbs[oo], cx, cy, cz, qx, qy, qz) >= Rc2) continue;
+                if (ncand == kProbeCand) return false;   // too many: the queue takes this edge
+                cand[ncand++] = (uint16_t)oo;
+            }
+        }
+#pragma unroll 1
+        for (; o < sc.n_obbs; ++o) {
             const float4 ob = obs[o];
             const float ex = ob.x - cx, ey = ob.y - cy, ez = ob.z - cz;
-            const float lim = Rj + ob.w;   // see box_limits
+            const float lim = Rj + ob.w;
             if (kStats) st.v[ST_CULL] += 1;
             if (fmaf(ez, ez, fmaf(ey, ey, ex * ex)) >= lim * lim) continue;
             float qx, qy, qz;
             if (fast_box_dsq(sc.obbs[o], cx, cy, cz, qx, qy, qz) >= Rc2) continue;
-            if (ncand == kProbeCand) return false;   // too many: the queue takes this edge
+            if (ncand == kProbeCand) return false;
             cand[ncand++] = (uint16_t)o;
         }
         if (ncand == 0) continue;
