@@ -793,10 +793,11 @@ __global__ void __launch_bounds__(kProbeThreads, 4) edges_probe_kernel(ModelDev 
     flush_stats(stats, st);
 }
 
-// Kernel, shared memory and grid of the probe for edge variant `mode`: the
-// boxes-only fast variant only (the generic one serves clearance, which
-// wants every sample, and masks; the ESDF lookups do not pay off one lane at
-// a time). `share` scales the grid (mixed batch).
+// Kernel, shared memory and grid of the probe for edge variant `mode`, or
+// none: the probe serves the boxes-only fast variant (the generic one serves
+// clearance, which wants every sample, and masks; the ESDF lookups do not pay
+// off one lane at a time) with enough edges to fill the GPU. `share` scales
+// the grid (mixed batch).
 struct ProbePlan {
     void (*k)(ModelDev, ps_scene_view, ps_edge_params, const float*, const float*, int, EdgeWs*, const int*, int*,
               unsigned long long*, const int*) = nullptr;
@@ -808,6 +809,10 @@ int plan_probe(const ps_model* m, const ps_scene_view* sv, int mode, bool stats,
                ProbePlan& out) {
     out = ProbePlan{};
     if (mode != 1 || max_edges <= 0 || sv->n_obbs == 0) return PS_OK;
+    // One thread per edge: below 8 warps per SM the probe runs latency-bound
+    // and costs more than it retires (measured: the 16 K segment edges of a
+    // 256-request CHOMP iteration ran 3 % slower with it).
+    if ((long long)max_edges < 8ll * 32 * sm_count()) return PS_OK;
     out.k = stats ? edges_probe_kernel<true> : edges_probe_kernel<false>;
     out.smem = probe_smem_bytes(m, sv);
     PS_TRY_CUDA(cudaFuncSetAttribute(out.k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)out.smem));

@@ -445,3 +445,21 @@ def test_rollout_costs_vs_reference_stomp():
     rel64 = np.abs(ours[:, 0, :].reshape(-1) - c64) / np.maximum(np.abs(c64), 1.0)
     print(f"rollout cost: max rel err vs fp64 = {rel64.max():.2e}")
     assert rel64.max() < 1e-4
+
+
+def test_edges_probe_path_bitexact():
+    """The end-sample probe runs in front of the persistent queue when there
+    are at least 8 edges per SM lane group (38 K on a B200): at 0.6 of
+    workload 2 (39,321 edges) the persistent path, with the probe, equals the
+    reference kernels and the probe-free plain path bit for bit."""
+    wl = workloads.workload(2, scale=0.6)
+    b, sc, om, ref = make(wl["asset"], wl["obbs"])
+    n_sm = torch.cuda.get_device_properties(0).multi_processor_count
+    assert len(wl["G"]) >= 8 * 32 * n_sm
+    f, t, g = (torch.from_numpy(x).cuda() for x in (wl["from"], wl["to"], wl["G"]))
+    v, c, _ = api.check_edges(b, sc, f, t, samples=g)
+    vp, cp, _ = api.check_edges(b, sc, f, t, samples=g, persistent=False)
+    assert torch.equal(v, vp) and torch.equal(c.view(torch.int32), cp.view(torch.int32))
+    rv, rc, _ = ref.check_edges(wl["from"], wl["to"], wl["G"])
+    np.testing.assert_array_equal(v.cpu().numpy(), rv)
+    assert np.array_equal(c.cpu().numpy().view(np.uint32), rc.view(np.uint32))
