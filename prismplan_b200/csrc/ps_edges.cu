@@ -14,7 +14,9 @@
 // the boxes it cannot reach (a conservative broad phase with the same guard
 // band as the pair path), then runs the gate and exact tests against the
 // survivors only; an __any_sync after every joint retires the chunk (and the
-// edge) at the first confirmed hit.
+// edge) at the first confirmed hit. With enough edges to fill the GPU, an
+// end-sample probe (one thread per edge, sample j = G) runs first and retires
+// the edges that collide there before the queue starts.
 #include <algorithm>
 #include <cfloat>
 #include <mutex>
