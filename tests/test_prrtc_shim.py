@@ -75,3 +75,27 @@ def test_planning_scene_surface(tmp_path):
     clone = PlanningScene(2)
     clone.update_world(obs)
     assert clone.current_obstacles == obs
+
+
+def test_scene_tensors_masks_host_side():
+    """Allowed-collision masks on SceneTensors (host side, CPU tensors): rows
+    of the right width are kept and pointed at, a ragged mask is refused, and
+    `masks` hands them to the oracle under its names."""
+    import numpy as np
+
+    from prismplan_b200 import workloads
+    from prismplan_b200.scene import SceneTensors
+
+    rng = np.random.default_rng(3)
+    obbs = workloads.random_obbs(rng, 5)
+    m_obb = (rng.random((7, 5)) > 0.5).astype(np.uint8)
+    m_apx = np.zeros((3, 5), np.uint8)
+    sc = SceneTensors(*obbs, device="cpu", sphere_obb_acm_mask=m_obb, sphere_obb_acm_mask_approx=m_apx.ravel())
+    v = sc.view()
+    assert v.sphere_obb_acm_mask and v.sphere_obb_acm_mask_approx and not v.sphere_acm_mask
+    np.testing.assert_array_equal(sc.tensors["sphere_obb_acm_mask"].numpy(), m_obb)
+    assert set(sc.masks) == {"obb_acm", "obb_acm_apx"} and sc.masks["obb_acm_apx"].shape == (3, 5)
+    with pytest.raises(ValueError):
+        SceneTensors(*obbs, device="cpu", sphere_obb_acm_mask=np.ones(11, np.uint8))
+    with pytest.raises(ValueError):   # no ESDF layers: an ESDF mask has no columns
+        SceneTensors(*obbs, device="cpu", sphere_acm_mask=np.ones(4, np.uint8))
