@@ -240,10 +240,12 @@ def run_ours(args):
         dist.barrier()
     valid_frac = float(out[0].float().mean().item())
     del graph
-    # prep, queue pass 0, finalize; a second queue pass when the edges are fewer
-    # than 8 per resident warp (6 blocks of 4 warps per SM for this kernel)
+    # prep, queue pass 0, finalize; the end-sample probe when there are at
+    # least 8 warps of edges per SM; a second queue pass when the edges are
+    # fewer than 8 per resident warp (5 blocks of 4 warps per SM for this
+    # kernel variant)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
-    launches_per_step = 3 + (1 if E < 8 * sms * 6 * 4 else 0)
+    launches_per_step = 3 + (1 if E >= 8 * 32 * sms else 0) + (1 if E < 8 * sms * 5 * 4 else 0)
 
     result = None
     if rank == 0:
