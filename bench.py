@@ -239,6 +239,7 @@ def run_ours(args):
         job_samples = int(ns.item())
         dist.barrier()
     valid_frac = float(out[0].float().mean().item())
+    timed_out = (out[0].cpu().numpy().copy(), out[1].cpu().numpy().copy())   # the timed step's verdicts and costs
     del graph
     # prep, queue pass 0, finalize; the end-sample probe when there are at
     # least 8 warps of edges per SM; a second queue pass when the edges are
@@ -265,15 +266,16 @@ def run_ours(args):
         if args.headline_only:
             result["roofline"] = {"kernel": "edges_probe_kernel + edges_queue_kernel", "kernel_ms": statistics.median(kern_ms)}
         else:
-            result.update(secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev))
+            result.update(secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev, timed_out))
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
     return result
 
 
-def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev):
-    """Roofline, e2e, CPU baseline and the comparison paths (rank 0, N=1 data)."""
+def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev, timed_out):
+    """Roofline, e2e, parity, CPU baseline and the comparison paths (rank 0,
+    N=1 data). timed_out: (valid, cost) of the timed graph replay."""
     import ctypes
 
     import torch
@@ -311,8 +313,9 @@ def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev):
         ev.evaluate(ff, tt, E, params)
     t0 = time.perf_counter()
     n_e2e = max(50, 2 * args.steps)   # sub-millisecond host-timed steps: average over many
+    e2e_out = None
     for _ in range(n_e2e):
-        ev.evaluate(ff, tt, E, params)
+        e2e_out = ev.evaluate(ff, tt, E, params)
     dt = (time.perf_counter() - t0) / n_e2e
     res["e2e"] = {"value": total_samples / dt, "unit": UNIT, "h2d_bytes_per_step": 2 * E * 7 * 4,
                   "d2h_bytes_per_step": E * (1 + 4), "ms_per_step": dt * 1e3, "iterations": n_e2e,
@@ -331,8 +334,10 @@ def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev):
     pl_ms = e0.elapsed_time(e1) / 5
     res["plain"] = {"value": total_samples / (pl_ms * 1e-3), "unit": UNIT, "ms_per_step": pl_ms,
                     "path": "ps_check_edges_plain (one warp per edge, direct launch)"}
-    # ---- the reference's own kernels (plain GPU path), same inputs ----
-    res["reference_gpu"] = reference_gpu_edges(b, wl)
+    # ---- the reference's own kernels (plain GPU path), same inputs, and the
+    #      parity of the timed step (and of the e2e bridge) against them ----
+    res["reference_gpu"], ref_out = reference_gpu_edges(b, wl)
+    res["parity"] = edge_parity(timed_out, e2e_out, ref_out)
     # ---- CPU baseline (oracle port, FP32, all host threads, bounded sample) ----
     res["cpu_baseline"] = cpu_baseline(b, wl)
     # ---- other workloads: configs (1) and CHOMP cost+gradient (3) ----
@@ -370,17 +375,39 @@ def traffic_from_profiles(kernel):
 
 
 def reference_gpu_edges(b, wl):
+    """Times the reference's evaluate_edges_batch on the headline inputs;
+    returns (summary, (valid, cost) or None)."""
     try:
         import oracle
 
         ref = oracle.RefKernels(b, *wl["obbs"])
-        n = len(wl["from"])
         v, c, ms = ref.check_edges(wl["from"], wl["to"], wl["G"], reps=1)
-        return {"value": int(wl["G"].sum()) / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
-                "path": "evaluate_edges_batch<<<E_G,64>>> per distinct G (reference kernels, sm_100a)",
-                "valid_fraction": float(v.mean())}
+        return ({"value": int(wl["G"].sum()) / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+                 "path": "evaluate_edges_batch<<<E_G,64>>> per distinct G (reference kernels, sm_100a)",
+                 "valid_fraction": float(v.mean())}, (np.asarray(v), np.asarray(c)))
     except Exception as e:   # harness absent
-        return {"unavailable": str(e)[:200]}
+        return {"unavailable": str(e)[:200]}, None
+
+
+def edge_parity(timed, e2e, ref):
+    """Verdict flips and cost bit-equality of the timed headline step and of
+    the e2e bridge's last call against the reference kernels' outputs on the
+    identical 65,536 edges."""
+    if ref is None:
+        return {"unavailable": "reference kernels not built (oracle/_ref)"}
+    rv, rc = ref
+    out = {"against": "evaluate_edges_batch (reference kernels, sm_100a), same inputs", "edges": int(len(rv))}
+    for name, got in (("timed_step", timed), ("e2e", e2e)):
+        if got is None:
+            continue
+        v = np.asarray(got[0]).reshape(-1).astype(np.uint8)
+        c = np.asarray(got[1]).reshape(-1).astype(np.float32)
+        flips = np.nonzero(v != rv.astype(np.uint8))[0]
+        out[name] = {"flips": int(len(flips)),
+                     "cost_bitwise": bool(np.array_equal(c.view(np.uint32), rc.astype(np.float32).view(np.uint32))),
+                     "first_flips": flips[:8].tolist()}
+    out["ok"] = all(out[k]["flips"] == 0 and out[k]["cost_bitwise"] for k in ("timed_step", "e2e") if k in out)
+    return out
 
 
 def cpu_baseline(b, wl, target_s=8.0):
@@ -846,6 +873,10 @@ def main():
     res = run_reference(args) if args.impl == "reference" else run_ours(args)
     if res is not None:
         print(json.dumps(res), flush=True)
+        par = res.get("parity") or {}
+        if par.get("ok") is False:   # a fast step whose verdicts differ from the reference's is not a result
+            print(f"bench: headline parity FAILED against the reference kernels: {par}", file=sys.stderr)
+            sys.exit(1)
 
 
 if __name__ == "__main__":

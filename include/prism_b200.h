@@ -123,6 +123,17 @@ int ps_model_get_info(const ps_model* model, ps_model_info* info);
    wait since the last poll (its outputs for that launch are incomplete).
    Replaces the reference's cudaCheckError -> exit() (utils.cuh:433-439). */
 int ps_model_poll_status(ps_model* model, int* code);
+/* Polls of the bounded wait with which each kernel stages this model into
+   shared memory (default 2^22, far beyond a real copy; < 0 restores it).
+   Takes effect for later launches (a captured graph keeps the value it was
+   captured with). When a wait gives up, the kernel latches PS_ETIMEOUT
+   (ps_model_poll_status) and writes fail-closed outputs: configurations in
+   collision, edges invalid (cost FLT_MAX, and PS_ETIMEOUT from
+   ps_edges_status / ps_batch_status on the persistent paths), costs,
+   clearances and gradients NaN. With 0 every wait gives up at once, which
+   is how the failure paths are tested without a fault. No reference
+   counterpart (its waits are unbounded, utils.cuh:433-439). */
+int ps_model_set_wait_limit(ps_model* model, int polls);
 
 /* =========================================================================
  * Scene view: non-owning device pointers in the exact layout of
@@ -239,7 +250,10 @@ int ps_check_edges(const ps_model* model, const ps_scene_view* scene,
        by every GPU that loads the library until the process exits.
      - The first call on each device looks up the array's device address
        (cudaGetSymbolAddress) with that device current; make that first call
-       before any stream capture on the device.
+       before any stream capture on the device. The address is kept for the
+       life of the process: after cudaDeviceReset on a device, this entry
+       point must not be called again on it (the kept address belongs to
+       the destroyed context).
      - Every call on a device shares the one array and resets it as it starts,
        so calls whose work overlaps on the GPU (other streams or threads) race.
    Allocates nothing: no cudaMalloc, cudaFree or allocating library call. */
@@ -517,6 +531,18 @@ int ps_stomp_workspace_layout(const ps_model* model, int B, int T,
    sphere order as in the descriptor). Same arithmetic as the checks. */
 int ps_fk_spheres(const ps_model* model, const float* q, int n,
                   float* sphere_xyz, void* stream);
+
+/* Sphere-vs-box pairs decided exactly as the kernels decide them (3x3 fast
+   path, guard band, the reference sequence of sphere_single_obb_collision,
+   scene_collision.cuh:24-78, inside the band), one pair per index i:
+   obb_dims [n*4], obb_pose [n*8] (SceneCollisionData layout), spheres
+   [n*4] (x, y, z, radius incl. margin), all device and 16-byte aligned.
+   decision [n] (device): bit 0 = hit, bit 1 = the pair fell inside the
+   guard band and was re-decided with the reference sequence. local_xyz
+   [n*3] (device, may be NULL): the reference sequence's box-frame
+   coordinates (transform_sphere_to_local). Diagnostics and parity tests. */
+int ps_debug_obb_pairs(const float* obb_dims, const float* obb_pose, const float* spheres, int n,
+                       uint8_t* decision, float* local_xyz, void* stream);
 
 /* FP32 FMA throughput probe used as the roofline denominator: 8 independent
    FMA chains per thread on every SM; returns FLOP/s (host). Synchronous; the

@@ -338,26 +338,36 @@ void eval_config(const orc_model& m, const orc_scene& s, const float* qf, F marg
         if (flags & PS_CLEARANCE_OBB) clr = std::min(clr, (double)obb_clearance<F>(s, p, sr, i, acm));
         if (flags & PS_CLEARANCE_ESDF) clr = std::min(clr, (double)esdf_clearance<F>(s, p, sr, i));
     }
-    // self (runtime_kinematics.cuh:248-284, 382-416; two_phase_cc.cuh:109-130)
+    // self (runtime_kinematics.cuh:248-284, 382-416; two_phase_cc.cuh:109-130).
+    // With want_gap every pair is visited and gap also takes the distance to
+    // contact |d - (r_i + r_j)| of each approximate and exact pair, so that a
+    // self verdict flip can be reported with its distance to contact.
     if ((flags & PS_CHECK_SELF) && !hit) {
         bool need = gate_off;
         for (const Pair& pr : m.apx_self_pairs) {
-            if (need) break;
+            if (need && !want_gap) break;
             F dx = apos[pr.i * 3] - apos[pr.j * 3], dy = apos[pr.i * 3 + 1] - apos[pr.j * 3 + 1],
               dz = apos[pr.i * 3 + 2] - apos[pr.j * 3 + 2];
             F rs = (F)m.apx[pr.i * 4 + 3] + (F)m.apx[pr.j * 4 + 3];
             if (sizeof(F) == 4) rs = m.apx32[pr.i * 4 + 3] + m.apx32[pr.j * 4 + 3];
             if (dx * dx + dy * dy + dz * dz - rs * rs < F(0)) need = true;
+            if (want_gap) gap = std::min(gap, std::fabs(std::sqrt((double)(dx * dx + dy * dy + dz * dz)) - (double)rs));
         }
-        if (need) {
+        if (need || want_gap) {
+            bool self_hit = false;
             for (const Pair& pr : m.self_pairs) {
                 F dx = pos[pr.i * 3] - pos[pr.j * 3], dy = pos[pr.i * 3 + 1] - pos[pr.j * 3 + 1],
                   dz = pos[pr.i * 3 + 2] - pos[pr.j * 3 + 2];
                 F rs = (F)m.sph[pr.i * 4 + 3] + (F)m.sph[pr.j * 4 + 3];
                 if (sizeof(F) == 4) rs = m.sph32[pr.i * 4 + 3] + m.sph32[pr.j * 4 + 3];
                 F sum = dx * dx + dy * dy + dz * dz;
-                if (sum - rs * rs < F(0)) { hit = true; break; }
+                if (want_gap) gap = std::min(gap, std::fabs(std::sqrt((double)sum) - (double)rs));
+                if (sum - rs * rs < F(0)) {
+                    self_hit = true;
+                    if (!want_gap) break;
+                }
             }
+            hit = need && self_hit;
         }
     }
     res.hit = hit;
@@ -631,6 +641,24 @@ extern "C" double orc_state_cost_d(const orc_model* m, const orc_scene* s, const
     return state_cost<double>(*m, *s, q, w, wm, sm, include_self);
 }
 
+// Distance (metres) from p to the nearest face of layer l's voxel lattice:
+// where the nearest lookup's voxel, or the trilinear lookup's cell, changes
+// (the guard band's edges lie on the same lattice).
+static double esdf_face_distance(const orc_scene& s, int layer, const double* p) {
+    const float* prm = &s.vparams[layer * 4];
+    const double vs = prm[3];
+    if (vs <= 0.0) return 1e30;
+    double l[3];
+    to_local<double>(&s.vpose[layer * 8], p[0], p[1], p[2], l[0], l[1], l[2]);
+    double best = 1e30;
+    for (int k = 0; k < 3; ++k) {
+        const double g = (l[k] + prm[k] * 0.5) / vs;
+        const double f = g - std::floor(g);
+        best = std::min(best, std::min(f, 1.0 - f) * vs);
+    }
+    return best;
+}
+
 extern "C" double orc_state_cost_kink_distance(const orc_model* m, const orc_scene* s, const double* q,
                                                double wm, double sm, int include_self) {
     std::vector<Affine<double>> T;
@@ -661,6 +689,27 @@ extern "C" double orc_state_cost_kink_distance(const orc_model* m, const orc_sce
                 }
             } else if (c < second) {
                 second = c;
+            }
+        }
+        // ESDF: hinge activation of the min over layers, ties between layers,
+        // and the voxel faces of the minimising layer
+        if (s->n_layers > 0) {
+            double eb = 1000.0, e2 = 1000.0;
+            int el = -1;
+            for (int l = 0; l < s->n_layers; ++l) {
+                if (s->v_en[l] == 0) continue;
+                if (!s->acm.empty() && s->acm[(size_t)i * s->n_layers + l] == 0) continue;
+                double d;
+                if (!esdf_lookup<double>(*s, l, p, d)) continue;
+                const double c = -d - r;
+                if (c < eb) { e2 = eb; eb = c; el = l; } else if (c < e2) { e2 = c; }
+            }
+            if (el >= 0) {
+                kd = std::min(kd, std::fabs(wm - eb));
+                if (eb < wm) {   // active: the value (nearest) or the gradient (trilinear) jumps across faces
+                    kd = std::min(kd, e2 - eb);
+                    kd = std::min(kd, esdf_face_distance(*s, el, p));
+                }
             }
         }
         if (best_o < 0) continue;

@@ -171,6 +171,9 @@ _SIGNATURES = [
     ("ps_model_set_limits", C.c_int, [C.c_void_p, _fp, _fp]),
     ("ps_model_get_info", C.c_int, [C.c_void_p, C.POINTER(ModelInfo)]),
     ("ps_model_poll_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    ("ps_model_set_wait_limit", C.c_int, [C.c_void_p, C.c_int]),
+    ("ps_debug_obb_pairs", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]),
     ("ps_check_configs", C.c_int,
      [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_int, C.c_float, C.c_uint,
       C.c_void_p, C.c_void_p, C.c_void_p]),

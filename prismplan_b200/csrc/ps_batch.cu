@@ -113,7 +113,14 @@ __global__ void __launch_bounds__(kWarps * 32, 24 / kWarps) batch_waypoint_kerne
     __shared__ float bmax;
     const int n_wp = cnt->n_wp;
     if ((long long)blockIdx.x * kWarps * kTile >= n_wp) return;   // nothing for this block: skip staging
-    if (!stage_model(md, smem, &mbar)) return;
+    if (!stage_model(md, smem, &mbar)) {   // fail closed: NaN costs and gradient rows
+        const float nan = __int_as_float(0x7fc00000);
+        cost_fail_closed(md, n_wp, kWarps * kTile, [&](long long k, int D) {
+            wp_cost[k] = nan;
+            for (int d = 0; d < D; ++d) grad[(size_t)k * D + d] = nan;
+        });
+        return;
+    }
     const ModelSmem M = model_view(smem);
     const int D = M.H->n_dof, NJ = M.H->n_joints, NS = M.H->n_spheres;
     ObbPrep* obbs = reinterpret_cast<ObbPrep*>(smem + md.bytes_core);
@@ -348,7 +355,7 @@ int batch_capture(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep
 
 std::vector<unsigned char> make_key(const ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep,
                                     const ps_cost_params* cp) {
-    std::vector<unsigned char> k(sizeof(*sv) + sizeof(*ep) + sizeof(*cp) + 2 * sizeof(float) + 2 * sizeof(int));
+    std::vector<unsigned char> k(sizeof(*sv) + sizeof(*ep) + sizeof(*cp) + 2 * sizeof(float) + 3 * sizeof(int));
     unsigned char* p = k.data();
     auto put = [&](const void* src, size_t n) {
         std::memcpy(p, src, n);
@@ -361,6 +368,7 @@ std::vector<unsigned char> make_key(const ps_batch* b, const ps_scene_view* sv, 
     put(&b->traj_share, sizeof(float));
     put(&b->traj_threads, sizeof(int));
     put(&b->traj_tile, sizeof(int));
+    put(&b->model->dev.stage_polls, sizeof(int));   // kernels get the model by value at capture
     return k;
 }
 
@@ -383,6 +391,7 @@ void release(ps_batch* b) {
 extern "C" int ps_batch_create(const ps_model* m, const ps_batch_limits* lim, ps_batch** out) {
     clear_error();
     if (!m || !lim || !out) return set_error(PS_EINVAL, "NULL argument");
+    if (int rc = check_model_device(m)) return rc;
     *out = nullptr;
     if (lim->max_edge_requests < 0 || lim->max_edges < 0 || lim->max_traj_requests < 0 || lim->max_waypoints < 0 ||
         lim->max_traj_len < 0)

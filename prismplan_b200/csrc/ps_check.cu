@@ -33,6 +33,16 @@ __device__ __forceinline__ float sdf_from_min(const SceneSmem& sc, float px, flo
     return inside;
 }
 
+// Fail-closed outputs of a configuration kernel whose model staging gave up:
+// this block's configurations (c = block * threads + thread, grid-strided)
+// are reported in collision with a NaN clearance.
+__device__ __forceinline__ void configs_fail_closed(int n, int threads, uint8_t* hit_out, float* clr_out) {
+    for (long long c = (long long)blockIdx.x * threads + threadIdx.x; c < n; c += (long long)gridDim.x * threads) {
+        hit_out[c] = 1;
+        if (clr_out) clr_out[c] = __int_as_float(0x7fc00000);
+    }
+}
+
 template <bool kClr, bool kStats>
 __global__ void __launch_bounds__(kCfgThreads) check_configs_kernel(ModelDev md, ps_scene_view sv, const float* __restrict__ q,
                                                                    int n, float margin, unsigned flags,
@@ -50,7 +60,7 @@ __global__ void __launch_bounds__(kCfgThreads) check_configs_kernel(ModelDev md,
     LayerPrep* layers = reinterpret_cast<LayerPrep*>(orig + ((nob + 3) & ~3));
     float* qtile = reinterpret_cast<float*>(layers + PS_MAX_LAYERS);
 
-    if (!stage_model(md, blob, &mbar)) return;
+    if (!stage_model(md, blob, &mbar)) return configs_fail_closed(n, kCfgThreads, hit_out, clr_out);
     SceneSmem sc;
     stage_scene(sv, obbs, orig, layers, counters, &bmax, sc);
     const ModelSmem M = model_view(blob);
@@ -185,7 +195,7 @@ __global__ void __launch_bounds__(kCfgThreads, kClr ? 6 : 4) check_configs_fast_
     LayerPrep* layers = reinterpret_cast<LayerPrep*>(orig + ((nob + 3) & ~3));
     float* qtile = reinterpret_cast<float*>(layers + PS_MAX_LAYERS);
 
-    if (!stage_model(md, blob, &mbar)) return;
+    if (!stage_model(md, blob, &mbar)) return configs_fail_closed(n, kCfgThreads, hit_out, clr_out);
     SceneSmem sc;
     stage_scene(sv, obbs, orig, layers, counters, &bmax, sc);
     const ModelSmem M = model_view(blob);
@@ -287,7 +297,7 @@ __global__ void __launch_bounds__(kSelfThreads) self_check_kernel(ModelDev md, c
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar;
     unsigned char* blob = smem;
-    if (!stage_model(md, blob, &mbar)) return;
+    if (!stage_model(md, blob, &mbar)) return configs_fail_closed(n, kSelfThreads, hit_out, nullptr);
     const ModelSmem M = model_view(blob);
     const int D = M.H->n_dof, NS = M.H->n_spheres, NA = M.H->n_approx, NJ = M.H->n_joints;
     const SelfSmem sm = carve_self<kSelfThreads>(smem + md.bytes_core, NS, NA, NJ);
@@ -312,7 +322,13 @@ __global__ void __launch_bounds__(kCfgThreads) fk_spheres_kernel(ModelDev md, co
                                                                 float* __restrict__ out) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar;
-    if (!stage_model(md, smem, &mbar)) return;
+    if (!stage_model(md, smem, &mbar)) {   // fail closed: NaN centres (sizes from the blob in global memory)
+        const long long total = (long long)n * reinterpret_cast<const BlobHeader*>(md.blob)->n_spheres * 3;
+        for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+             k += (long long)gridDim.x * blockDim.x)
+            out[k] = __int_as_float(0x7fc00000);
+        return;
+    }
     const ModelSmem M = model_view(smem);
     const int D = M.H->n_dof, NJ = M.H->n_joints, NS = M.H->n_spheres;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
@@ -333,6 +349,34 @@ __global__ void __launch_bounds__(kCfgThreads) fk_spheres_kernel(ModelDev md, co
                 o[1] = py;
                 o[2] = pz;
             }
+        }
+    }
+}
+
+// One sphere-vs-box pair per thread, decided as every kernel decides it:
+// prepared box (prep_box), 3x3 fast squared distance, definite outside the
+// guard band of this pair (the narrowest any kernel uses: S = |p|inf and
+// B = this box's |t|inf + |h|inf), the reference sequence inside it. Also the
+// exact-sequence local coordinates (ref_to_local). Diagnostics.
+__global__ void obb_pairs_kernel(const float4* __restrict__ dims, const float4* __restrict__ pose,
+                                 const float4* __restrict__ sph, int n, uint8_t* __restrict__ decision,
+                                 float* __restrict__ local) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const ObbPrep o = prep_box(dims[i], pose[2 * i], pose[2 * i + 1]);
+        const float4 sp = sph[i];
+        float lo, hi;
+        guard_thresholds(sp.x, sp.y, sp.z, sp.w, o.h.w, lo, hi);
+        float qx, qy, qz;
+        const float d = fast_box_dsq(o, sp.x, sp.y, sp.z, qx, qy, qz);
+        const bool band = d >= lo && d < hi;
+        const bool hit = d < lo ? true : (d >= hi ? false : ref_obb_hit(o, sp.x, sp.y, sp.z, sp.w));
+        decision[i] = (uint8_t)((hit ? 1 : 0) | (band ? 2 : 0));
+        if (local) {
+            float lx, ly, lz;
+            ref_to_local(o.q.x, o.q.y, o.q.z, o.q.w, o.r0.w, o.r1.w, o.r2.w, sp.x, sp.y, sp.z, lx, ly, lz);
+            local[3 * i] = lx;
+            local[3 * i + 1] = ly;
+            local[3 * i + 2] = lz;
         }
     }
 }
@@ -414,12 +458,31 @@ extern "C" int ps_fk_spheres(const ps_model* m, const float* q, int n, float* ou
     PS_NVTX("ps_fk_spheres");
     clear_error();
     if (!m || (n > 0 && (!q || !out))) return set_error(PS_EINVAL, "NULL argument");
+    if (int rc = check_model_device(m)) return rc;
     if (n <= 0) return PS_OK;
     cudaStream_t s = (cudaStream_t)stream;
     size_t smem = (size_t)m->dev.bytes_core;
     PS_TRY_CUDA(cudaFuncSetAttribute(fk_spheres_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int grid = std::max(1, std::min((n + kCfgThreads - 1) / kCfgThreads, sm_count() * 8));
     fk_spheres_kernel<<<grid, kCfgThreads, smem, s>>>(m->dev, q, n, out);
+    PS_TRY_CUDA(cudaGetLastError());
+    return PS_OK;
+}
+
+extern "C" int ps_debug_obb_pairs(const float* obb_dims, const float* obb_pose, const float* spheres, int n,
+                                  uint8_t* decision, float* local_xyz, void* stream) {
+    PS_NVTX("ps_debug_obb_pairs");
+    clear_error();
+    if (n < 0) return set_error(PS_EINVAL, "n < 0");
+    if (n == 0) return PS_OK;
+    if (!obb_dims || !obb_pose || !spheres || !decision) return set_error(PS_EINVAL, "NULL argument");
+    if (((reinterpret_cast<uintptr_t>(obb_dims) | reinterpret_cast<uintptr_t>(obb_pose) |
+          reinterpret_cast<uintptr_t>(spheres)) & 15) != 0)
+        return set_error(PS_EINVAL, "inputs must be 16-byte aligned");
+    const int grid = std::max(1, std::min((n + 255) / 256, sm_count() * 8));
+    obb_pairs_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(
+        reinterpret_cast<const float4*>(obb_dims), reinterpret_cast<const float4*>(obb_pose),
+        reinterpret_cast<const float4*>(spheres), n, decision, local_xyz);
     PS_TRY_CUDA(cudaGetLastError());
     return PS_OK;
 }

@@ -63,7 +63,12 @@ struct ModelDev {
     const float* upper;            // device
     int* status;                   // device error latch
     int bytes_core;
+    int stage_polls;               // polls of the staging wait before a kernel gives up
 };
+
+// Default staging wait: ~2^22 polls, each try_wait may suspend for a
+// hardware-defined interval (far beyond any real copy of a few KB).
+#define PS_STAGE_POLLS (1 << 22)
 
 // ---------------------------------------------------------------------------
 // Prepared obstacle tables in shared memory

@@ -51,7 +51,23 @@ __global__ void __launch_bounds__(kCostWarps * 32, kGrad ? 4 : 3) waypoint_cost_
     __shared__ __align__(8) uint64_t mbar;
     __shared__ int counters[4];
     __shared__ float bmax;
-    if (!stage_model(md, smem, &mbar)) return;
+    const bool bdt = P.layout == PS_LAYOUT_BDT;
+    if (!stage_model(md, smem, &mbar)) {
+        const float nan = __int_as_float(0x7fc00000);
+        cost_fail_closed(md, (long long)n_rows * T, kCostWarps * kTile, [&](long long idx, int D) {
+            const int b = (int)(idx / T), tt = (int)(idx - (long long)b * T);
+            if (wp_cost) {
+                if (broadcast_d)
+                    for (int d = 0; d < D; ++d) wp_cost[((size_t)b * D + d) * T + tt] = nan;
+                else
+                    wp_cost[idx] = nan;
+            }
+            if (traj_acc) atomicAdd(traj_acc + b, nan);
+            if (kGrad)
+                for (int d = 0; d < D; ++d) grad[bdt ? ((size_t)b * D + d) * T + tt : ((size_t)b * T + tt) * D + d] = nan;
+        });
+        return;
+    }
     const ModelSmem M = model_view(smem);
     const int D = M.H->n_dof, NJ = M.H->n_joints, NS = M.H->n_spheres;
     ObbPrep* obbs = reinterpret_cast<ObbPrep*>(smem + md.bytes_core);
@@ -66,7 +82,6 @@ __global__ void __launch_bounds__(kCostWarps * 32, kGrad ? 4 : 3) waypoint_cost_
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const CostWarpScratch ws =
         cost_carve(cb.wbase + (size_t)warp * cost_warp_floats(NJ, NS, sv.n_obbs, md.n_sruns, kGrad), NJ, NS, sc.n_obbs, kGrad);
-    const bool bdt = P.layout == PS_LAYOUT_BDT;
     const long long total = (long long)n_rows * T;
     LaneStats st;
     st.zero();

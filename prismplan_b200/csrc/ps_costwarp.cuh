@@ -146,6 +146,18 @@ __device__ __forceinline__ CostBlock cost_block_setup(unsigned char* at, const M
     return cb;
 }
 
+// Fail-closed outputs of a cost kernel whose model staging gave up: NaN
+// waypoint costs and gradient rows for the waypoints idx this block owns
+// (ranges of per_block waypoints, grid-strided). The row writer gets the
+// waypoint index and D (read from the blob header in global memory).
+template <class RowNaN>
+__device__ __forceinline__ void cost_fail_closed(const ModelDev& md, long long total, int per_block, RowNaN row_nan) {
+    const int D = reinterpret_cast<const BlobHeader*>(md.blob)->n_dof;
+    for (long long r0 = (long long)blockIdx.x * per_block; r0 < total; r0 += (long long)gridDim.x * per_block)
+        for (int i = threadIdx.x; i < per_block; i += blockDim.x)
+            if (r0 + i < total) row_nan(r0 + i, D);
+}
+
 __device__ __forceinline__ void load_frame(const float* f, Affine& T) {
     const float4* v = reinterpret_cast<const float4*>(f);
     const float4 a = v[0], b = v[1], c = v[2];

@@ -530,7 +530,16 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_plain_kerne
     __shared__ __align__(8) uint64_t mbar;
     __shared__ int counters[4];
     __shared__ float bmax;
-    if (!stage_model(md, smem, &mbar)) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (!stage_model(md, smem, &mbar)) {   // fail closed: this block's edges come back invalid
+        for (int e = blockIdx.x * kWarps + warp; e < n_edges; e += gridDim.x * kWarps)
+            if (lane == 0) {
+                valid[e] = 0;
+                cost[e] = FLT_MAX;
+                if (clearance) clearance[e] = __int_as_float(0x7fc00000);
+            }
+        return;
+    }
     const ModelSmem M = model_view(smem);
     const int D = M.H->n_dof;
     EdgeSmem es = carve(smem, md, sv, D);
@@ -540,7 +549,6 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_plain_kerne
     __syncthreads();
     box_limits(sc, es.obs);
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nob_pad = (max(sv.n_obbs, 1) + 7) & ~7;
     WarpScratch ws{es.q + warp * 32 * D, es.cand + warp * nob_pad, es.obs};
     LaneStats st;
@@ -756,7 +764,7 @@ __global__ void __launch_bounds__(kProbeThreads, 4) edges_probe_kernel(ModelDev 
     __shared__ __align__(8) uint64_t mbar;
     __shared__ int counters[4];
     __shared__ float bmax;
-    if (!stage_model(md, smem, &mbar)) return;
+    if (!stage_model(md, smem, &mbar)) return;   // best effort: the queue still checks every edge
     ObbPrep* obbs = reinterpret_cast<ObbPrep*>(smem + md.bytes_core);
     const int nob = max(sv.n_obbs, 1);
     int* orig = reinterpret_cast<int*>(obbs + nob);
@@ -850,7 +858,12 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode == 1 ? 5 : (kMode ? 6 : 3)
     __shared__ __align__(8) uint64_t mbar;
     __shared__ int counters[4];
     __shared__ float bmax;
-    if (!stage_model(md, smem, &mbar)) return;
+    if (!stage_model(md, smem, &mbar)) {
+        // fail closed: finalize reports every edge that is neither retired
+        // nor complete as invalid, and the status query PS_ETIMEOUT
+        if (threadIdx.x == 0) atomicExch(&hdr->timed_out, 1);
+        return;
+    }
     const ModelSmem M = model_view(smem);
     const int D = M.H->n_dof;
     EdgeSmem es = carve(smem, md, sv, D);
@@ -958,7 +971,21 @@ __global__ void __launch_bounds__(kSelfThreads) edges_self_kernel(ModelDev md, p
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ int s_off[kSelfThreads + 1], s_G[kSelfThreads], s_hit[kSelfThreads], s_wsum[2], s_stop;
-    if (!stage_model(md, smem, &mbar)) return;
+    if (!stage_model(md, smem, &mbar)) {
+        // fail closed. Persistent: bad[] stays 0 for the edges no block
+        // checked, and finalize reports them invalid once timed_out is set.
+        // Plain: this block's windows (8 edges each) come back invalid.
+        if (hdr) {
+            if (threadIdx.x == 0) atomicExch(&hdr->timed_out, 1);
+        } else if (!bad) {
+            for (long long e0 = (long long)blockIdx.x * 8; e0 < n_edges; e0 += (long long)gridDim.x * 8)
+                if (threadIdx.x < 8 && e0 + threadIdx.x < n_edges) {
+                    valid[e0 + threadIdx.x] = 0;
+                    cost[e0 + threadIdx.x] = FLT_MAX;
+                }
+        }
+        return;
+    }
     const ModelSmem M = model_view(smem);
     const int D = M.H->n_dof, NS = M.H->n_spheres, NA = M.H->n_approx, NJ = M.H->n_joints;
     const SelfSmem sm = carve_self<kSelfThreads>(smem + md.bytes_core, NS, NA, NJ);

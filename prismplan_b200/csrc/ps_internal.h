@@ -46,8 +46,14 @@ int traj_cost_launch(const ps_model* m, const ps_scene_view* scene, const float*
                      const ps_cost_params* P, float* waypoint_cost, float* traj_cost, float* grad,
                      const uint8_t* skip, cudaStream_t s);
 
-// Validate a scene view against a model; returns PS_OK or sets the error.
+// Validate a scene view against a model (and the model's device, below);
+// returns PS_OK or sets the error.
 int validate_scene(const ps_model* m, const ps_scene_view* s);
+// The model's blob lives on the device it was created on: PS_EINVAL (with a
+// message) unless that device is the current one. Every kernel reads the
+// blob, so running with another device current would read another GPU's
+// memory.
+int check_model_device(const ps_model* m);
 
 // Dynamic shared memory needed to stage model core + scene tables.
 size_t scene_smem_bytes(const ps_scene_view* s);

@@ -72,7 +72,18 @@ int validate_scene(const ps_model* m, const ps_scene_view* s) {
         return set_error(PS_EINVAL, "n_voxel_layers > 0 but a voxel array is NULL or max_voxels_per_layer <= 0");
     if (s->esdf_mode != PS_ESDF_NEAREST && s->esdf_mode != PS_ESDF_TRILINEAR)
         return set_error(PS_EINVAL, "esdf_mode must be PS_ESDF_NEAREST or PS_ESDF_TRILINEAR");
-    (void)m;
+    return check_model_device(m);
+}
+
+int check_model_device(const ps_model* m) {
+    if (!m) return set_error(PS_EINVAL, "model is NULL");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetDevice");
+    if (dev != m->info.device)
+        return set_error(PS_EINVAL, "model was created on device " + std::to_string(m->info.device) + " but device " +
+                                        std::to_string(dev) +
+                                        " is current; make the model's device current (or build one per device)");
     return PS_OK;
 }
 
@@ -369,6 +380,7 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
     m->dev.upper = reinterpret_cast<const float*>(base + off_upper);
     m->dev.status = reinterpret_cast<int*>(base + off_status);
     m->dev.bytes_core = (int)core;
+    m->dev.stage_polls = PS_STAGE_POLLS;
     m->max_joint_spheres = max_js;
     m->root_slot_only = tmem[dfs[0]] == 0;
     for (int p = 1; p < nj; ++p) m->root_slot_only = m->root_slot_only && tmem[dfs[p]] == 1;
@@ -408,6 +420,13 @@ extern "C" int ps_model_set_limits(ps_model* m, const float* lower, const float*
 extern "C" int ps_model_get_info(const ps_model* m, ps_model_info* info) {
     if (!m || !info) return ps::set_error(PS_EINVAL, "NULL argument");
     *info = m->info;
+    return PS_OK;
+}
+
+extern "C" int ps_model_set_wait_limit(ps_model* m, int polls) {
+    ps::clear_error();
+    if (!m) return ps::set_error(PS_EINVAL, "model is NULL");
+    m->dev.stage_polls = polls < 0 ? PS_STAGE_POLLS : polls;
     return PS_OK;
 }
 

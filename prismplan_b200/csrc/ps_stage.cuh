@@ -5,6 +5,23 @@
 
 namespace ps {
 
+// Prepared record of one box from its SceneCollisionData entries: dims
+// (dx, dy, dz, pad: full extents) and the inverse pose (tx, ty, tz, qw) +
+// (qx, qy, qz, pad).
+__device__ __forceinline__ ObbPrep prep_box(float4 dm, float4 pa, float4 pb) {
+    const float qw = pa.w, qx = pb.x, qy = pb.y, qz = pb.z;
+    ObbPrep p;
+    // Matrix of v -> v + qw t + q x t, t = 2 q x v.
+    p.r0 = make_float4(1.0f - 2.0f * (qy * qy + qz * qz), 2.0f * (qx * qy - qw * qz), 2.0f * (qx * qz + qw * qy), pa.x);
+    p.r1 = make_float4(2.0f * (qx * qy + qw * qz), 1.0f - 2.0f * (qx * qx + qz * qz), 2.0f * (qy * qz - qw * qx), pa.y);
+    p.r2 = make_float4(2.0f * (qx * qz - qw * qy), 2.0f * (qy * qz + qw * qx), 1.0f - 2.0f * (qx * qx + qy * qy), pa.z);
+    const float hx = dm.x * 0.5f, hy = dm.y * 0.5f, hz = dm.z * 0.5f;
+    const float B = fmaxf(fmaxf(fabsf(pa.x), fmaxf(fabsf(pa.y), fabsf(pa.z))), fmaxf(hx, fmaxf(hy, hz)));
+    p.h = make_float4(hx, hy, hz, B);
+    p.q = make_float4(qw, qx, qy, qz);
+    return p;
+}
+
 // Builds the prepared box table (compacted enabled boxes, 3x3 maps, exact
 // half extents) and the ESDF layer headers from the caller's
 // SceneCollisionData arrays. Call with all threads; ends with __syncthreads().
@@ -17,19 +34,10 @@ __device__ __forceinline__ void stage_scene(const ps_scene_view& sv, ObbPrep* ob
     __syncthreads();
     for (int o = threadIdx.x; o < sv.n_obbs; o += blockDim.x) {
         if (sv.obb_enable[o] == 0) continue;
-        const float4 dm = reinterpret_cast<const float4*>(sv.obb_dims)[o];
-        const float4 pa = reinterpret_cast<const float4*>(sv.obb_pose)[2 * o];      // tx ty tz qw
-        const float4 pb = reinterpret_cast<const float4*>(sv.obb_pose)[2 * o + 1];  // qx qy qz pad
-        const float qw = pa.w, qx = pb.x, qy = pb.y, qz = pb.z;
-        ObbPrep p;
-        // Matrix of v -> v + qw t + q x t, t = 2 q x v.
-        p.r0 = make_float4(1.0f - 2.0f * (qy * qy + qz * qz), 2.0f * (qx * qy - qw * qz), 2.0f * (qx * qz + qw * qy), pa.x);
-        p.r1 = make_float4(2.0f * (qx * qy + qw * qz), 1.0f - 2.0f * (qx * qx + qz * qz), 2.0f * (qy * qz - qw * qx), pa.y);
-        p.r2 = make_float4(2.0f * (qx * qz - qw * qy), 2.0f * (qy * qz + qw * qx), 1.0f - 2.0f * (qx * qx + qy * qy), pa.z);
-        const float hx = dm.x * 0.5f, hy = dm.y * 0.5f, hz = dm.z * 0.5f;
-        const float B = fmaxf(fmaxf(fabsf(pa.x), fmaxf(fabsf(pa.y), fabsf(pa.z))), fmaxf(hx, fmaxf(hy, hz)));
-        p.h = make_float4(hx, hy, hz, B);
-        p.q = make_float4(qw, qx, qy, qz);
+        const ObbPrep p = prep_box(reinterpret_cast<const float4*>(sv.obb_dims)[o],
+                                   reinterpret_cast<const float4*>(sv.obb_pose)[2 * o],       // tx ty tz qw
+                                   reinterpret_cast<const float4*>(sv.obb_pose)[2 * o + 1]);  // qx qy qz pad
+        const float B = p.h.w;
         int slot = atomicAdd(&counters[0], 1);
         obbs[slot] = p;
         orig[slot] = o;
@@ -60,9 +68,23 @@ __device__ __forceinline__ void stage_scene(const ps_scene_view& sv, ObbPrep* ob
     __syncthreads();
 }
 
+__device__ __forceinline__ uint32_t mbar_try_phase0(uint32_t bar) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar)
+        : "memory");
+    return done;
+}
+
 // Copies the model core (header + joint and sphere tables) into shared memory
 // with one bulk async copy (cp.async.bulk, completion on an mbarrier, bounded
-// wait). Returns false on timeout (status latched). Call with all threads.
+// wait of md.stage_polls polls). Returns false on timeout: the status is
+// latched, and the copy still in flight is waited for (again bounded) so that
+// it cannot land in shared memory after the block has exited. A kernel that
+// gets false must write its fail-closed outputs (in collision, invalid, NaN)
+// and return. Call with all threads.
 __device__ __forceinline__ bool stage_model(const ModelDev& md, unsigned char* smem_blob, uint64_t* mbar) {
     const uint32_t bytes = (uint32_t)md.bytes_core;
     const uint32_t bar = (uint32_t)__cvta_generic_to_shared(mbar);
@@ -80,18 +102,17 @@ __device__ __forceinline__ bool stage_model(const ModelDev& md, unsigned char* s
             "l"(md.blob), "r"(bytes), "r"(bar)
             : "memory");
     }
-    // Bounded wait on phase 0: ~2^22 polls, each try_wait may suspend for a
-    // hardware-defined interval. On expiry latch PS_ETIMEOUT and give up.
+    // Bounded wait on phase 0. On expiry latch PS_ETIMEOUT and give up.
     uint32_t done = 0;
-    for (int it = 0; it < (1 << 22) && !done; ++it) {
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(done)
-            : "r"(bar)
-            : "memory");
-    }
+    for (int it = 0; it < md.stage_polls && !done; ++it) done = mbar_try_phase0(bar);
     int ok = __syncthreads_and((int)done);
-    if (!ok && threadIdx.x == 0) latch_status(md.status, PS_ETIMEOUT);
+    if (!ok) {
+        if (threadIdx.x == 0) latch_status(md.status, PS_ETIMEOUT);
+        // drain: the copy may still be in flight (bounded as well)
+        uint32_t landed = done;
+        for (int it = 0; it < PS_STAGE_POLLS && !landed; ++it) landed = mbar_try_phase0(bar);
+        __syncthreads();
+    }
     return ok != 0;
 }
 

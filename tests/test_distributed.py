@@ -1,8 +1,9 @@
 """CPU: the multi-rank sharding logic with gloo ranks (world size 2).
 
-Each rank evaluates its contiguous shard of an edge batch (with the CPU
-oracle standing in for the GPU kernel, which the ranks would call on their own
-devices) and the gathered result must equal the unsharded one, in order.
+Each rank runs the product's check_edges_sharded on its contiguous shard of
+an edge batch, with the CPU oracle as the per-shard checker in place of the
+GPU kernel that the ranks would call on their own devices, and the gathered
+result must equal the unsharded one, in order.
 """
 import os
 import socket
@@ -11,7 +12,7 @@ import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
-from prismplan_b200.distributed import shard_range
+from prismplan_b200.distributed import require_same_device, shard_range
 
 
 def test_shard_range_covers_exactly():
@@ -22,6 +23,12 @@ def test_shard_range_covers_exactly():
             assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
             sizes = [hi - lo for lo, hi in spans]
             assert max(sizes) - min(sizes) <= 1
+
+
+def test_model_device_mismatch_is_refused():
+    require_same_device(0, 0)
+    with pytest.raises(ValueError, match="built on cuda:1 but cuda:0"):
+        require_same_device(1, 0)
 
 
 def _free_port():
@@ -37,7 +44,7 @@ def _worker(rank, world, port, q):
 
     import oracle
     from prismplan_b200 import workloads
-    from prismplan_b200.distributed import run_sharded
+    from prismplan_b200.distributed import check_edges_sharded
     from prismplan_b200.robot import RobotModelBuilder
 
     os.environ["MASTER_ADDR"] = "127.0.0.1"
@@ -48,11 +55,15 @@ def _worker(rank, world, port, q):
         om = oracle.OracleModel(RobotModelBuilder.from_asset(wl["asset"]), *wl["obbs"])
         frm, to, G = wl["from"], wl["to"], np.minimum(wl["G"], 40)
 
-        def evaluate(lo, hi):
-            v, c, _, _, _ = om.check_edges(frm[lo:hi], to[lo:hi], G[lo:hi], threads=1)
+        seen = []
+
+        def checker(f, t, g):
+            seen.append(len(f))
+            v, c, _, _, _ = om.check_edges(f, t, g, threads=1)
             return v, c
 
-        valid, cost = run_sharded(len(frm), evaluate)
+        valid, cost = check_edges_sharded(None, None, frm, to, samples=G, checker=checker)
+        assert seen == [128], seen   # this rank's half only
         if rank == 0:
             v_all, c_all, _, _, _ = om.check_edges(frm, to, G, threads=1)
             q.put((bool(np.array_equal(valid, v_all)), bool(np.array_equal(cost, c_all)), len(valid)))

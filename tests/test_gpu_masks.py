@@ -11,6 +11,7 @@ sphere_scene_in_collision), so a gate that applied it would pass every
 configuration the scene's boxes collide with."""
 import numpy as np
 import pytest
+from conftest import COST_REL_TOL, assert_gradient_vs_fd
 import torch
 
 import oracle
@@ -159,7 +160,7 @@ def test_costs_with_masks(case):
     print(f"masked waypoint cost: max rel diff vs reference {rel.max():.2e}, vs fp64 {rel64.max():.2e}, "
           f"active {(c64 > 0).mean():.2f}")
     assert (c64 > 0).mean() > 0.2
-    assert rel.max() < 1e-3 and rel64.max() < 1e-4
+    assert rel.max() < 1e-3 and rel64.max() < COST_REL_TOL
     r = q.transpose(0, 2, 1).copy()    # the same waypoints as rollouts [R, D, T]
     rc = api.rollout_costs(b, sc, torch.from_numpy(r).cuda(), p, broadcast_d=True).cpu().numpy()
     theirs, _ = ref.stomp(r, w, wm, sm)
@@ -192,8 +193,4 @@ def test_cost_gradient_with_obb_masks(case):
     om.set_masks(None, masks["sphere_obb_acm_mask"], None)
     flat = q.reshape(-1, q.shape[2])
     fd = om.state_cost_fd_grad(flat, w, wm, sm, h=1e-6)
-    ok = om.kink_distance(flat, wm, sm) > 1e-4
-    num = np.linalg.norm((ours - fd)[ok])
-    den = max(np.linalg.norm(fd[ok]), 1e-12)
-    print(f"masked gradient: rel L2 err vs FP64 FD = {num / den:.2e} over {ok.sum()} of {len(ok)} waypoints")
-    assert np.linalg.norm(fd[ok]) > 0 and num / den < 1e-4
+    assert_gradient_vs_fd(ours, fd, om.kink_distance(flat, wm, sm), "masked gradient")

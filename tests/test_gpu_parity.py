@@ -11,7 +11,7 @@ import pytest
 import torch
 
 import oracle
-from conftest import golden_asset
+from conftest import COST_REL_TOL, assert_gradient_vs_fd, golden_asset
 from prismplan_b200 import api, workloads
 from prismplan_b200 import _lib
 from prismplan_b200.robot import RobotModelBuilder
@@ -198,8 +198,11 @@ def test_self_check_vs_oracle(w1):
     q = wl["q"][:1024]
     h, _ = api.check_configs(b, None, torch.from_numpy(q).cuda(), check_self=True)
     om0 = oracle.OracleModel(b, np.zeros((0, 4)), np.zeros((0, 8)))
-    h64, _, _ = om0.check_configs(q, flags=_lib.PS_CHECK_SELF, want_gap=False)
-    assert (h.cpu().numpy() != h64).sum() <= 1
+    h64, _, gap = om0.check_configs(q, flags=_lib.PS_CHECK_SELF, want_gap=True)
+    flips = np.nonzero(h.cpu().numpy() != h64)[0]
+    print(f"self check vs FP64: {len(flips)} flips of {len(q)}; FP64 distance to contact (m) of each: "
+          f"{gap[flips].tolist()}")
+    assert np.all(gap[flips] < 1e-5), "a self-check flip away from contact"
     assert h64.mean() > 0.0
 
 
@@ -356,7 +359,7 @@ def test_waypoint_cost_vs_fp64_and_reference(w3):
     c64 = om.state_cost(q.reshape(-1, D), wl["w"], wl["eps"], wl["self_margin"])
     rel = np.abs(ours - c64) / np.maximum(np.abs(c64), 1.0)
     print(f"waypoint cost: max rel err vs fp64 = {rel.max():.2e}, active = {(c64 > 0).mean():.2f}")
-    assert rel.max() < 1e-4
+    assert rel.max() < COST_REL_TOL
     rsc, _, _ = ref.chomp(q.transpose(0, 2, 1), wl["w"], wl["eps"], wl["self_margin"], grad=False)
     rref = rsc[:, 0, :].reshape(-1)
     relr = np.abs(ours - rref) / np.maximum(np.abs(rref), 1.0)
@@ -374,13 +377,7 @@ def test_gradient_vs_fp64_central_difference(w3):
     flat = q.reshape(-1, D)
     fd = om.state_cost_fd_grad(flat, wl["w"], wl["eps"], wl["self_margin"], h=1e-6)
     kink = om.kink_distance(flat, wl["eps"], wl["self_margin"])
-    ok = kink > 1e-4
-    num = np.linalg.norm((ours - fd)[ok])
-    den = max(np.linalg.norm(fd[ok]), 1e-12)
-    per = np.linalg.norm(ours - fd, axis=1) / np.maximum(np.linalg.norm(fd, axis=1), 1e-3)
-    print(f"gradient: rel L2 err vs FP64 FD (h=1e-6) = {num / den:.2e} over {ok.sum()} of {len(ok)} "
-          f"waypoints (kink-excluded {len(ok) - ok.sum()}); worst waypoint {per[ok].max():.2e}")
-    assert num / den < 1e-4
+    assert_gradient_vs_fd(ours, fd, kink, "gradient")
 
 
 def test_gradient_vs_reference_fd_kernel(w3):
@@ -444,7 +441,7 @@ def test_rollout_costs_vs_reference_stomp():
     c64 = om.state_cost(r.transpose(0, 2, 1).reshape(-1, D), wl["w"], wl["eps"], wl["self_margin"])
     rel64 = np.abs(ours[:, 0, :].reshape(-1) - c64) / np.maximum(np.abs(c64), 1.0)
     print(f"rollout cost: max rel err vs fp64 = {rel64.max():.2e}")
-    assert rel64.max() < 1e-4
+    assert rel64.max() < COST_REL_TOL
 
 
 def test_edges_probe_path_bitexact():

@@ -54,6 +54,35 @@ def test_static_workspace_matches_caller_workspace(use_given_samples):
     assert 0.02 < float(v_ref.float().mean()) < 0.98
 
 
+def test_static_workspace_at_full_capacity():
+    """65,536 edges, the array's limit: the per-edge segments fill it exactly
+    and the end-sample probe runs in front of the queue (it starts at 8 warps
+    of edges per SM), as on the persistent path."""
+    wl = workloads.workload(2)                          # 65,536 edges, 1..600 samples each
+    E = len(wl["from"])
+    assert E == _lib.PS_EDGES_STATIC_MAX
+    b = RobotModelBuilder.from_asset(wl["asset"]).build()
+    sc = SceneTensors(*wl["obbs"])
+    frm = torch.from_numpy(wl["from"]).cuda()
+    to = torch.from_numpy(wl["to"]).cuda()
+    G = torch.from_numpy(wl["G"]).cuda()
+    p = api.EdgeEvalParams(max_joint_step=0.01, max_samples=600)
+    v_ref, c_ref, _ = api.check_edges(b, sc, frm, to, samples=G, params=p)
+    torch.cuda.synchronize()
+    lib = _lib.load()
+    view, cp = sc.view(), p.to_c()
+    for call in range(2):
+        out = (torch.full((E,), 7, dtype=torch.uint8, device="cuda"), torch.full((E,), -1.0, device="cuda"),
+               torch.full((E,), -1.0, device="cuda"))
+        _lib.check(_call_static(lib, b, view, frm, to, G, cp, out))
+        torch.cuda.synchronize()
+        assert torch.equal(out[0], v_ref), f"call {call}: verdicts differ"
+        assert np.array_equal(out[1].cpu().numpy().view(np.uint32), c_ref.cpu().numpy().view(np.uint32))
+    st = C.c_int(-1)
+    _lib.check(lib.ps_edges_status(None, C.byref(st)))
+    assert st.value == _lib.PS_OK
+
+
 def test_static_workspace_rejects_oversized_batch():
     wl = workloads.workload(2, scale=1.0 / 16)
     b = RobotModelBuilder.from_asset(wl["asset"]).build()
