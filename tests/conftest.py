@@ -51,23 +51,29 @@ def golden_asset(z, name):
 # Contract bars for floating-point results against the FP64 oracle.
 COST_REL_TOL = 1e-5       # cost / clearance: |ours - fp64| / max(|fp64|, 1)
 GRAD_REL_TOL = 1e-5       # gradient: relative L2 over the compared waypoints
-KINK_M = 1e-4             # waypoints this close (m) to a kink of the cost are not FD-comparable
 MAX_KINK_EXCLUDED = 0.05  # at most this fraction of waypoints may be excluded
 
 
-def assert_gradient_vs_fd(ours, fd, kink, label):
+def kink_threshold(h):
+    """A central difference with step h (rad) moves a sphere by at most about
+    h times the longest lever arm (< 2 m on these robots); a waypoint closer
+    than 10x that to a kink of the cost is not FD-comparable."""
+    return 20.0 * h
+
+
+def assert_gradient_vs_fd(ours, fd, kink, label, h=1e-6):
     """Relative L2 error of the adjoint gradient against FP64 central
-    differences over the waypoints at least KINK_M from a kink of the state
-    cost (hinge activation, min ties, box regions, ESDF voxel faces), with the
-    excluded count bounded and each excluded waypoint's kink distance
-    printed."""
-    ok = kink > KINK_M
+    differences (step h) over the waypoints at least kink_threshold(h) from a
+    kink of the state cost (hinge activation, min ties, box regions, ESDF
+    voxel faces), with the excluded count bounded and each excluded
+    waypoint's kink distance printed."""
+    ok = kink > kink_threshold(h)
     excluded = np.nonzero(~ok)[0]
     num = np.linalg.norm((ours - fd)[ok])
     den = max(np.linalg.norm(fd[ok]), 1e-12)
     err = num / den
-    print(f"{label}: rel L2 err vs FP64 FD (h=1e-6) = {err:.2e} over {ok.sum()} of {len(ok)} waypoints; "
-          f"excluded {len(excluded)} with kink distances (m) "
+    print(f"{label}: rel L2 err vs FP64 FD (h={h:g}) = {err:.2e} over {ok.sum()} of {len(ok)} waypoints; "
+          f"excluded {len(excluded)} (kink closer than {kink_threshold(h):g} m) with kink distances (m) "
           f"{np.array2string(np.sort(kink[excluded]), precision=1, max_line_width=400)}")
     assert len(excluded) <= MAX_KINK_EXCLUDED * len(ok), f"{len(excluded)} of {len(ok)} waypoints excluded"
     assert np.linalg.norm(fd[ok]) > 0
