@@ -695,24 +695,32 @@ class MixedBatch:
 
 def _make_autograd():
     torch = _torch()
+    from torch.autograd.function import once_differentiable
 
     class _TrajCost(torch.autograd.Function):
         """traj_cost[b] = sum_t w*hinge(q[b,t]) + lambda*sum_d q_d^T R q_d.
 
-        Forward runs the fused FK + hinge + adjoint kernel once and keeps the
-        gradient; backward scales it by grad_output (no second pass)."""
+        Forward evaluates the cost only (the kernel without the adjoint).
+        Backward runs the fused FK + hinge + adjoint kernel on the saved
+        configurations: the link transforms are recomputed there rather than
+        kept from the forward pass, so nothing per link or per sphere is stored
+        between the passes. The scene's device arrays must stay alive until
+        backward. First order only: the adjoint is not itself differentiable
+        (double backward raises)."""
 
         @staticmethod
         def forward(ctx, q, robot, scene, params):
-            need = q.requires_grad
-            _, tc, g = traj_cost(robot, scene, q.detach(), params, want_grad=need, want_waypoint=False)
-            ctx.save_for_backward(g if need else torch.empty(0, device=q.device))
+            _, tc, _ = traj_cost(robot, scene, q.detach(), params, want_grad=False, want_waypoint=False)
+            ctx.save_for_backward(q)
+            ctx.robot, ctx.scene, ctx.params = robot, scene, params
             return tc
 
         @staticmethod
+        @once_differentiable
         def backward(ctx, grad_out):
-            (g,) = ctx.saved_tensors
-            return grad_out.view(-1, 1, 1) * g, None, None, None
+            (q,) = ctx.saved_tensors
+            _, _, g = traj_cost(ctx.robot, ctx.scene, q.detach(), ctx.params, want_grad=True, want_waypoint=False)
+            return grad_out.reshape(-1, 1, 1) * g, None, None, None
 
     return _TrajCost
 

@@ -23,7 +23,7 @@
 #include <string>
 #include <vector>
 
-#include "ps_costwarp.cuh"
+#include "ps_costlane.cuh"
 #include "ps_edgekern.cuh"
 
 namespace ps {
@@ -96,33 +96,34 @@ __global__ void batch_gather_traj(const TrajReq* __restrict__ req, const Counts*
 }
 
 size_t waypoint_smem_bytes(const ps_model* m, const ps_scene_view* sv, int warps) {
-    return cost_block_bytes(m, sv, warps, true);
+    return lane_block_bytes(m, sv, warps, true);
 }
 
-// Cost and adjoint of every packed waypoint, one warp per tile of kTile
-// consecutive waypoints.
-template <int kWarps, int kTile>
-__global__ void __launch_bounds__(kWarps * 32, 24 / kWarps) batch_waypoint_kernel(ModelDev md, ps_scene_view sv, ps_cost_params P,
-                                                                     const Counts* __restrict__ cnt,
-                                                                     const float* __restrict__ q,
-                                                                     float* __restrict__ wp_cost,
-                                                                     float* __restrict__ grad) {
+// Cost and adjoint of every packed waypoint, one lane per waypoint (32
+// consecutive packed waypoints per warp, ps_costlane.cuh).
+template <int kWarps>
+__global__ void __launch_bounds__(kWarps * 32, 8 / kWarps) batch_waypoint_kernel(ModelDev md, ps_scene_view sv,
+                                                                                 ps_cost_params P,
+                                                                                 const Counts* __restrict__ cnt,
+                                                                                 const float* __restrict__ q,
+                                                                                 float* __restrict__ wp_cost,
+                                                                                 float* __restrict__ grad) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ int counters[4];
     __shared__ float bmax;
     const int n_wp = cnt->n_wp;
-    if ((long long)blockIdx.x * kWarps * kTile >= n_wp) return;   // nothing for this block: skip staging
+    if ((long long)blockIdx.x * kWarps * 32 >= n_wp) return;   // nothing for this block: skip staging
     if (!stage_model(md, smem, &mbar)) {   // fail closed: NaN costs and gradient rows
         const float nan = __int_as_float(0x7fc00000);
-        cost_fail_closed(md, n_wp, kWarps * kTile, [&](long long k, int D) {
+        cost_fail_closed(md, n_wp, kWarps * 32, [&](long long k, int D) {
             wp_cost[k] = nan;
             for (int d = 0; d < D; ++d) grad[(size_t)k * D + d] = nan;
         });
         return;
     }
     const ModelSmem M = model_view(smem);
-    const int D = M.H->n_dof, NJ = M.H->n_joints, NS = M.H->n_spheres;
+    const int D = M.H->n_dof, NJ = M.H->n_joints;
     ObbPrep* obbs = reinterpret_cast<ObbPrep*>(smem + md.bytes_core);
     const int nob = max(sv.n_obbs, 1);
     int* orig = reinterpret_cast<int*>(obbs + nob);
@@ -131,25 +132,22 @@ __global__ void __launch_bounds__(kWarps * 32, 24 / kWarps) batch_waypoint_kerne
     stage_scene(sv, obbs, orig, layers, counters, &bmax, sc);
     const CostBlock cb = cost_block_setup(reinterpret_cast<unsigned char*>(layers + PS_MAX_LAYERS), M, sc, sv.n_obbs);
     __syncthreads();
+    box_limits(sc, const_cast<float4*>(cb.obs));
+    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const CostWarpScratch ws =
-        cost_carve(cb.wbase + (size_t)warp * cost_warp_floats(NJ, NS, sv.n_obbs, md.n_sruns, true), NJ, NS, sc.n_obbs, true);
+    const LaneScratch ws =
+        lane_carve(reinterpret_cast<unsigned char*>(cb.wbase) + (size_t)warp * lane_warp_bytes(NJ, D, sv.n_obbs, true),
+                   NJ, D, true);
     LaneStats st;
-    st.zero();
-    const int n_tiles = (n_wp + kTile - 1) / kTile;
-    for (int tile = blockIdx.x * kWarps + warp; tile < n_tiles; tile += gridDim.x * kWarps) {
-        const int k0 = tile * kTile;
-        const int nt = min(kTile, n_wp - k0);
-        for (int t = 0; t < nt; ++t)
-            if (lane < D) ws.q[t * 16 + lane] = q[(size_t)(k0 + t) * D + lane];
-        __syncwarp();
-        cost_fk_tile<false>(M, ws.q, nt, ws.frame, ws.bnd, st);
-        __syncwarp();
-        cost_cull<false>(M, sc, cb, ws, nt, P.world_margin, st);
-        for (int t = 0; t < nt; ++t) {
-            const float c = cost_eval<true, false>(M, md, sc, sv, P, cb, ws, t, grad + (size_t)(k0 + t) * D, 1, st);
-            if (lane == 0) wp_cost[k0 + t] = c;
-            __syncwarp();
+    for (int base = (blockIdx.x * kWarps + warp) * 32; base < n_wp; base += gridDim.x * kWarps * 32) {
+        const int k = base + lane;
+        const int kc = k < n_wp ? k : n_wp - 1;   // past the end: repeat the last waypoint
+        for (int d = 0; d < D; ++d) ws.q[d * 32 + lane] = q[(size_t)kc * D + d];
+        st.zero();
+        const float c = lane_cost<true, false>(M, md, sc, sv, P, cb, ws, st);
+        if (k < n_wp) {
+            wp_cost[k] = c;
+            lane_write_grad(M, cb, ws, grad + (size_t)k * D, 1);
         }
     }
 }
@@ -217,8 +215,8 @@ struct ps_batch {
     // tuning state
     float edge_share = 1.0f;   // of the edge kernel's full-occupancy grid
     float traj_share = 0.5f;   // of the trajectory kernel's full-occupancy grid
-    int traj_threads = 256;   // threads per block of the trajectory kernel (one tile per warp)
-    int traj_tile = 1;        // waypoints per warp tile (1 or kCostTile)
+    int traj_threads = 128;   // threads per block of the trajectory kernel (one waypoint per thread)
+    int traj_tile = 1;        // waypoints per thread (always 1)
 };
 
 namespace {
@@ -235,9 +233,8 @@ struct LaunchPlan {
 
 using WaypointKernel = void (*)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*);
 
-WaypointKernel pick_waypoint_kernel(int threads, int tile) {
-    if (threads == 128) return tile == 1 ? batch_waypoint_kernel<4, 1> : batch_waypoint_kernel<4, kCostTile>;
-    return tile == 1 ? batch_waypoint_kernel<8, 1> : batch_waypoint_kernel<8, kCostTile>;
+WaypointKernel pick_waypoint_kernel(int threads) {
+    return threads == 64 ? batch_waypoint_kernel<2> : batch_waypoint_kernel<4>;
 }
 
 // Everything that is not a stream operation happens before the capture.
@@ -273,12 +270,12 @@ int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, 
     if (b->lim.max_waypoints > 0) {
         const int tt = b->traj_threads;
         L.wsmem = waypoint_smem_bytes(m, sv, tt / 32);
-        L.wk = pick_waypoint_kernel(tt, b->traj_tile);
+        L.wk = pick_waypoint_kernel(tt);
         int per_sm = 0;
         PS_TRY_CUDA(cudaFuncSetAttribute(L.wk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.wsmem));
         PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L.wk, tt, L.wsmem));
         if (per_sm < 1) return set_error(PS_EINVAL, "trajectory kernel does not fit on an SM with this model/scene");
-        const int per_block = (tt / 32) * b->traj_tile;
+        const int per_block = tt;   // one waypoint per thread
         const int cap_blocks = (b->lim.max_waypoints + per_block - 1) / per_block;
         L.wgrid = std::max(1, std::min(cap_blocks, (int)(b->traj_share * sms * per_sm + 0.5f)));
         L.fsmem = (size_t)(2 * (b->lim.max_traj_len + 12) + kFinishThreads) * sizeof(float);
@@ -555,8 +552,8 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
     if (!b) return set_error(PS_EINVAL, "NULL batch");
     const float edge_shares[] = {0.5f, 0.75f, 1.0f};
     const float traj_shares[] = {0.25f, 0.5f, 1.0f};
-    const int widths[] = {128, 256};
-    const int tiles[] = {1, kCostTile};
+    const int widths[] = {64, 128};
+    const int tiles[] = {1};
     cudaStream_t s = nullptr;
     cudaEvent_t a = nullptr, z = nullptr;
     PS_TRY_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -577,7 +574,7 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
         for (float ts : traj_shares) {
             for (int w : widths) {
                 for (int tl : tiles) {
-                    if (!trajs && (ts != 0.5f || w != 256 || tl != 1)) continue;
+                    if (!trajs && (ts != 0.5f || w != 128 || tl != 1)) continue;
                     b->edge_share = es;
                     b->traj_share = ts;
                     b->traj_threads = w;

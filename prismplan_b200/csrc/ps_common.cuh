@@ -50,7 +50,8 @@ struct JointRec {
 // Self pairs (global memory): packed (i | j << 16), reordered sphere indices.
 // The same pairs as runs: sruns[r] = (i | q << 9 | len << 14, first) is
 // sphere i against the len spheres spairs[first..first+len) of joint q (DFS
-// position).
+// position). Runs are ordered by joint pair (joint of i, q), then i;
+// sjp[k] = (a | q << 16, first run, end run, 0) lists the joint pairs.
 // Limits (global memory): lower[n_dof], upper[n_dof].
 struct ModelDev {
     const unsigned char* blob;     // device
@@ -59,6 +60,8 @@ struct ModelDev {
     const uint2* sruns;            // device, self-pair runs
     const uint16_t* spairs;        // device, second sphere of each run pair
     int n_sruns;
+    const uint4* sjp;              // device, joint pairs: (a | q << 16, first run, end run, 0)
+    int n_sjp;
     const float* lower;            // device
     const float* upper;            // device
     int* status;                   // device error latch

@@ -21,29 +21,24 @@
 // zero-padded trajectory instead of a dense T x T product.
 #include <algorithm>
 
-#include "ps_costwarp.cuh"
+#include "ps_costlane.cuh"
 
 namespace ps {
 
 namespace {
 
-constexpr int kCostWarps = 8;   // waypoints in flight per block (one per warp)
-
 size_t cost_block_smem(const ps_model* m, const ps_scene_view* sv, bool grad) {
-    return cost_block_bytes(m, sv, kCostWarps, grad);
+    return lane_block_bytes(m, sv, kLaneCostWarps, grad);
 }
 
-// One warp per tile of kTile consecutive waypoints (see ps_costwarp.cuh).
-// kGrad: also the adjoint; kStats: count executed work. Output layouts follow
-// ps_cost_params.layout. Gradients run tiles of 1 (the cull is cheap next to
-// the adjoint), rollouts tiles of kCostTile (smooth rollouts share boxes).
-// skip (may be NULL): rows b with skip[b] != 0 need no output; a tile is
-// skipped when every row it touches is, so a skipped row that shares a tile
-// with a live one is evaluated all the same (with the same bits).
-// Residency, measured: 4 blocks per SM for the gradient kernel, 3 for the
-// rollout kernel (its tiles keep more live state).
-template <bool kGrad, bool kStats, int kTile>
-__global__ void __launch_bounds__(kCostWarps * 32, kGrad ? 4 : 3) waypoint_cost_kernel(
+// One lane per waypoint, 32 consecutive waypoints per warp (see
+// ps_costlane.cuh). kGrad: also the adjoint; kStats: count executed work.
+// Output layouts follow ps_cost_params.layout. skip (may be NULL): rows b
+// with skip[b] != 0 need no output and get none; a warp whose rows are all
+// skipped does nothing. Other waypoints of a warp are evaluated with the same
+// bits whichever rows share it.
+template <bool kGrad, bool kStats>
+__global__ void __launch_bounds__(kLaneCostWarps * 32, 2) waypoint_cost_kernel(
     ModelDev md, ps_scene_view sv, const float* __restrict__ q, int n_rows, int T, ps_cost_params P,
     float* __restrict__ wp_cost, int broadcast_d, float* __restrict__ traj_acc, float* __restrict__ grad,
     unsigned long long* stats, const uint8_t* __restrict__ skip) {
@@ -54,7 +49,7 @@ __global__ void __launch_bounds__(kCostWarps * 32, kGrad ? 4 : 3) waypoint_cost_
     const bool bdt = P.layout == PS_LAYOUT_BDT;
     if (!stage_model(md, smem, &mbar)) {
         const float nan = __int_as_float(0x7fc00000);
-        cost_fail_closed(md, (long long)n_rows * T, kCostWarps * kTile, [&](long long idx, int D) {
+        cost_fail_closed(md, (long long)n_rows * T, kLaneCostWarps * 32, [&](long long idx, int D) {
             const int b = (int)(idx / T), tt = (int)(idx - (long long)b * T);
             if (wp_cost) {
                 if (broadcast_d)
@@ -69,7 +64,7 @@ __global__ void __launch_bounds__(kCostWarps * 32, kGrad ? 4 : 3) waypoint_cost_
         return;
     }
     const ModelSmem M = model_view(smem);
-    const int D = M.H->n_dof, NJ = M.H->n_joints, NS = M.H->n_spheres;
+    const int D = M.H->n_dof, NJ = M.H->n_joints;
     ObbPrep* obbs = reinterpret_cast<ObbPrep*>(smem + md.bytes_core);
     const int nob = max(sv.n_obbs, 1);
     int* orig = reinterpret_cast<int*>(obbs + nob);
@@ -78,57 +73,43 @@ __global__ void __launch_bounds__(kCostWarps * 32, kGrad ? 4 : 3) waypoint_cost_
     stage_scene(sv, obbs, orig, layers, counters, &bmax, sc);
     const CostBlock cb = cost_block_setup(reinterpret_cast<unsigned char*>(layers + PS_MAX_LAYERS), M, sc, sv.n_obbs);
     __syncthreads();
+    box_limits(sc, const_cast<float4*>(cb.obs));
+    __syncthreads();
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const CostWarpScratch ws =
-        cost_carve(cb.wbase + (size_t)warp * cost_warp_floats(NJ, NS, sv.n_obbs, md.n_sruns, kGrad), NJ, NS, sc.n_obbs, kGrad);
+    const LaneScratch ws = lane_carve(reinterpret_cast<unsigned char*>(cb.wbase) +
+                                          (size_t)warp * lane_warp_bytes(NJ, D, sv.n_obbs, kGrad),
+                                      NJ, D, kGrad);
     const long long total = (long long)n_rows * T;
     LaneStats st;
     st.zero();
-    const long long n_tiles = (total + kTile - 1) / kTile;
-    for (long long tile = (long long)blockIdx.x * kCostWarps + warp; tile < n_tiles;
-         tile += (long long)gridDim.x * kCostWarps) {
-        const long long idx0 = tile * kTile;
-        const int nt = (int)min((long long)kTile, total - idx0);
-        if (skip) {   // uniform over the warp
-            bool all = true;
-            for (long long r = idx0 / T; r <= (idx0 + nt - 1) / T; ++r) all = all && skip[r] != 0;
-            if (all) continue;
+    for (long long base = ((long long)blockIdx.x * kLaneCostWarps + warp) * 32; base < total;
+         base += (long long)gridDim.x * kLaneCostWarps * 32) {
+        const long long idx = base + lane;
+        const long long ic = idx < total ? idx : total - 1;   // past the end: repeat the last waypoint
+        const int b = (int)(ic / T), tt = (int)(ic - (long long)b * T);
+        const bool live = idx < total && !(skip && skip[b]);
+        if (!__any_sync(kCostFull, live)) continue;   // uniform
+        for (int d = 0; d < D; ++d)
+            ws.q[d * 32 + lane] = bdt ? q[((size_t)b * D + d) * T + tt] : q[((size_t)b * T + tt) * D + d];
+        LaneStats ls;
+        ls.zero();
+        const float cost = lane_cost<kGrad, kStats>(M, md, sc, sv, P, cb, ws, ls);
+        if (!live) continue;
+        if (kStats) {
+            ls.v[ST_SAMPLES] += 1;
+            for (int k = 0; k < ST_COUNT; ++k) st.v[k] += ls.v[k];
         }
-        for (int t = 0; t < nt; ++t) {
-            const long long idx = idx0 + t;
-            const int b = (int)(idx / T);
-            const int tt = (int)(idx - (long long)b * T);
-            if (lane < D)
-                ws.q[t * 16 + lane] = bdt ? q[((size_t)b * D + lane) * T + tt] : q[((size_t)b * T + tt) * D + lane];
+        if (wp_cost) {
+            if (broadcast_d)
+                for (int d = 0; d < D; ++d) wp_cost[((size_t)b * D + d) * T + tt] = cost;
+            else
+                wp_cost[idx] = cost;
         }
-        __syncwarp();
-        cost_fk_tile<kStats>(M, ws.q, nt, ws.frame, ws.bnd, st);
-        __syncwarp();
-        cost_cull<kStats>(M, sc, cb, ws, nt, P.world_margin, st);
-        for (int t = 0; t < nt; ++t) {
-            const long long idx = idx0 + t;
-            const int b = (int)(idx / T);
-            const int tt = (int)(idx - (long long)b * T);
-            float* grow = nullptr;
-            int gstride = 1;
-            if (kGrad) {
-                grow = bdt ? grad + ((size_t)b * D) * T + tt : grad + ((size_t)b * T + tt) * D;
-                gstride = bdt ? T : 1;
-            }
-            const float cost = cost_eval<kGrad, kStats>(M, md, sc, sv, P, cb, ws, t, grow, gstride, st);
-            if (lane == 0) {
-                if (kStats) st.v[ST_SAMPLES] += 1;
-                if (wp_cost) {
-                    if (broadcast_d)
-                        for (int d = 0; d < D; ++d) wp_cost[((size_t)b * D + d) * T + tt] = cost;
-                    else
-                        wp_cost[idx] = cost;
-                }
-                if (traj_acc) atomicAdd(traj_acc + b, cost);
-            }
-            __syncwarp();
-        }
+        if (traj_acc) atomicAdd(traj_acc + b, cost);
+        if (kGrad)
+            lane_write_grad(M, cb, ws, bdt ? grad + ((size_t)b * D) * T + tt : grad + ((size_t)b * T + tt) * D,
+                            bdt ? T : 1);
     }
     if (kStats) flush_stats(stats, st);
 }
@@ -162,9 +143,9 @@ int cost_grid(K kernel, size_t smem, long long total) {
         return set_error(PS_EINVAL, "cost kernel shared memory exceeds the device limit"), -1;
     }
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kCostWarps * 32, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kLaneCostWarps * 32, smem);
     if (per_sm < 1) return set_error(PS_EINVAL, "cost kernel does not fit on an SM with this model/scene"), -1;
-    const long long need = (total + kCostWarps - 1) / kCostWarps;
+    const long long need = (total + kLaneCostWarps * 32 - 1) / (kLaneCostWarps * 32);
     return (int)std::max<long long>(1, std::min<long long>(need, (long long)per_sm * sm_count()));
 }
 
@@ -196,21 +177,21 @@ int ps::traj_cost_launch(const ps_model* m, const ps_scene_view* scene, const fl
     if (atomic_traj) PS_TRY_CUDA(cudaMemsetAsync(traj_cost, 0, sizeof(float) * B, s));
     if (grad) {
         const size_t smem = cost_block_smem(m, scene, true);
-        auto k = g_stats ? waypoint_cost_kernel<true, true, 1> : waypoint_cost_kernel<true, false, 1>;
+        auto k = g_stats ? waypoint_cost_kernel<true, true> : waypoint_cost_kernel<true, false>;
         const int grid = cost_grid(k, smem, total);
         if (grid < 0) return PS_EINVAL;
         mark_start(s);
-        k<<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
-                                              atomic_traj ? traj_cost : nullptr, grad, g_stats, skip);
+        k<<<grid, kLaneCostWarps * 32, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
+                                                  atomic_traj ? traj_cost : nullptr, grad, g_stats, skip);
         mark_stop(s);
     } else {
         const size_t smem = cost_block_smem(m, scene, false);
-        auto k = g_stats ? waypoint_cost_kernel<false, true, kCostTile> : waypoint_cost_kernel<false, false, kCostTile>;
+        auto k = g_stats ? waypoint_cost_kernel<false, true> : waypoint_cost_kernel<false, false>;
         const int grid = cost_grid(k, smem, total);
         if (grid < 0) return PS_EINVAL;
         mark_start(s);
-        k<<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
-                                              atomic_traj ? traj_cost : nullptr, nullptr, g_stats, skip);
+        k<<<grid, kLaneCostWarps * 32, smem, s>>>(m->dev, *scene, q, B, T, *P, waypoint_cost, 0,
+                                                  atomic_traj ? traj_cost : nullptr, nullptr, g_stats, skip);
         mark_stop(s);
     }
     PS_TRY_CUDA(cudaGetLastError());
@@ -244,12 +225,12 @@ extern "C" int ps_rollout_costs(const ps_model* m, const ps_scene_view* scene, c
     cudaStream_t s = (cudaStream_t)stream;
     const long long total = (long long)n_rows * T;
     const size_t smem = cost_block_smem(m, scene, false);
-    auto k = g_stats ? waypoint_cost_kernel<false, true, kCostTile> : waypoint_cost_kernel<false, false, kCostTile>;
+    auto k = g_stats ? waypoint_cost_kernel<false, true> : waypoint_cost_kernel<false, false>;
     const int grid = cost_grid(k, smem, total);
     if (grid < 0) return PS_EINVAL;
     mark_start(s);
-    k<<<grid, kCostWarps * 32, smem, s>>>(m->dev, *scene, rollouts, n_rows, T, *P, state_cost,
-                                                                 broadcast_d, nullptr, nullptr, g_stats, nullptr);
+    k<<<grid, kLaneCostWarps * 32, smem, s>>>(m->dev, *scene, rollouts, n_rows, T, *P, state_cost, broadcast_d,
+                                              nullptr, nullptr, g_stats, nullptr);
     mark_stop(s);
     PS_TRY_CUDA(cudaGetLastError());
     return PS_OK;

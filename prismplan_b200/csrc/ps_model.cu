@@ -229,7 +229,11 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
         if (sph_pos[xj] != sph_pos[yj]) return sph_pos[xj] < sph_pos[yj];
         return xj < yj;
     });
-    std::vector<uint32_t> sruns;   // 2 words per run
+    struct Run {
+        int a, q, i;
+        uint32_t w0, w1;
+    };
+    std::vector<Run> runs;
     std::vector<uint16_t> spairs(opairs.size());
     for (size_t k = 0; k < opairs.size();) {
         const int i = opairs[k] & 0xffff, q = sph_pos[opairs[k] >> 16];
@@ -238,11 +242,32 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
             spairs[e] = (uint16_t)(opairs[e] >> 16);
             ++e;
         }
-        sruns.push_back((uint32_t)i | (uint32_t)q << 9 | (uint32_t)(e - k) << 14);
-        sruns.push_back((uint32_t)k);
+        runs.push_back({sph_pos[i], q, i, (uint32_t)i | (uint32_t)q << 9 | (uint32_t)(e - k) << 14, (uint32_t)k});
         k = e;
     }
-    if (sruns.size() / 2 > 65535) return set_error(PS_EINVAL, "too many self-pair runs");
+    if (runs.size() > 65535) return set_error(PS_EINVAL, "too many self-pair runs");
+    // Runs ordered by joint pair (joint of i, joint q), then i; the joint-pair
+    // table sjp[k] = (a | q << 16, first run, end run, 0) lets the cost
+    // kernels cull whole joint pairs by their bound spheres.
+    std::stable_sort(runs.begin(), runs.end(), [](const Run& x, const Run& y) {
+        if (x.a != y.a) return x.a < y.a;
+        if (x.q != y.q) return x.q < y.q;
+        return x.i < y.i;
+    });
+    std::vector<uint32_t> sruns;   // 2 words per run
+    std::vector<uint32_t> sjp;     // 4 words per joint pair
+    for (size_t r = 0; r < runs.size(); ++r) {
+        if (r == 0 || runs[r].a != runs[r - 1].a || runs[r].q != runs[r - 1].q) {
+            if (!sjp.empty()) sjp[sjp.size() - 2] = (uint32_t)r;
+            sjp.push_back((uint32_t)runs[r].a | (uint32_t)runs[r].q << 16);
+            sjp.push_back((uint32_t)r);
+            sjp.push_back(0);
+            sjp.push_back(0);
+        }
+        sruns.push_back(runs[r].w0);
+        sruns.push_back(runs[r].w1);
+    }
+    if (!sjp.empty()) sjp[sjp.size() - 2] = (uint32_t)runs.size();
 
     bool shares = std::memcmp(aft, d->fixed_transforms, sizeof(float) * 16 * nj) == 0;
     for (int i = 0; i < nj && shares; ++i) shares = atypes[i] == d->joint_types[i];
@@ -271,6 +296,8 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
     off += align16(sizeof(uint32_t) * std::max<size_t>(sruns.size(), 2));
     const size_t off_spairs = off;
     off += align16(sizeof(uint16_t) * std::max<size_t>(spairs.size(), 1));
+    const size_t off_sjp = off;
+    off += align16(sizeof(uint32_t) * std::max<size_t>(sjp.size(), 4));
     const size_t off_lower = off;
     off += align16(sizeof(float) * nd);
     const size_t off_upper = off;
@@ -353,6 +380,7 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
     if (!apairs.empty()) std::memcpy(host.data() + off_apairs, apairs.data(), apairs.size() * 4);
     if (!sruns.empty()) std::memcpy(host.data() + off_sruns, sruns.data(), sruns.size() * 4);
     if (!spairs.empty()) std::memcpy(host.data() + off_spairs, spairs.data(), spairs.size() * 2);
+    if (!sjp.empty()) std::memcpy(host.data() + off_sjp, sjp.data(), sjp.size() * 4);
     std::memcpy(host.data() + off_lower, d->joint_lower, sizeof(float) * nd);
     std::memcpy(host.data() + off_upper, d->joint_upper, sizeof(float) * nd);
 
@@ -376,6 +404,8 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
     m->dev.sruns = reinterpret_cast<const uint2*>(base + off_sruns);
     m->dev.spairs = reinterpret_cast<const uint16_t*>(base + off_spairs);
     m->dev.n_sruns = (int)(sruns.size() / 2);
+    m->dev.sjp = reinterpret_cast<const uint4*>(base + off_sjp);
+    m->dev.n_sjp = (int)(sjp.size() / 4);
     m->dev.lower = reinterpret_cast<const float*>(base + off_lower);
     m->dev.upper = reinterpret_cast<const float*>(base + off_upper);
     m->dev.status = reinterpret_cast<int*>(base + off_status);

@@ -80,6 +80,25 @@ __device__ __forceinline__ void box_spheres(const SceneSmem& sc, float4* obs) {
     }
 }
 
+// Circumscribed-sphere prefilter of the fast path's broad phase. With
+// Rc the joint's cull radius around the chunk centre m (Sm = |m|inf), box o's
+// centre c_o (M_o = |c_o|inf) and circumscribed radius w_o, the guarded limit
+//   Rc + w_o + 4K (Sm + M_o + Rc + w_o + 1)
+// splits into a joint part Rj = Rc (1 + 4K) + 4K (Sm + 1) and a box part
+//   B_o = w_o (1 + 4K) + 4K M_o,
+// each raised by 1e-6 relative to cover their roundings, so the test stays
+// at least as wide as the unsplit one. B_o replaces obs[o].w (every thread
+// calls it after box_spheres and a block barrier).
+__device__ __forceinline__ void box_limits(const SceneSmem& sc, float4* obs) {
+    for (int o = threadIdx.x; o < sc.n_obbs; o += blockDim.x) {
+        float4 ob = obs[o];
+        const float M = fmaxf(fabsf(ob.x), fmaxf(fabsf(ob.y), fabsf(ob.z)));
+        ob.w = (ob.w * (1.0f + 4.0f * PS_GUARD_K) + 4.0f * PS_GUARD_K * M) * (1.0f + 1.0e-6f);
+        obs[o] = ob;
+    }
+}
+
+
 // Shared-memory view of the staged model core.
 struct ModelSmem {
     const BlobHeader* H;

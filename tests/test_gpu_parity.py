@@ -409,12 +409,20 @@ def test_smoothness_term_matches_dense_R(w3):
 
 
 def test_autograd_function(w3):
+    """Forward is the cost kernel alone; backward recomputes FK and runs the
+    adjoint kernel; the result is the fused call's gradient scaled by
+    grad_output. Double backward is refused."""
     wl, b, sc, om, ref = w3
     q = torch.from_numpy(wl["q"][:4]).cuda().requires_grad_(True)
     cost = api.hinge_cost(q, b, sc, _params(wl, 0.5))
+    _, tc, g = api.traj_cost(b, sc, q.detach(), _params(wl, 0.5))
+    torch.testing.assert_close(cost.detach(), tc, rtol=1e-6, atol=1e-5)
     (cost * torch.arange(1, 5, device="cuda")).sum().backward()
-    _, _, g = api.traj_cost(b, sc, q.detach(), _params(wl, 0.5))
-    torch.testing.assert_close(q.grad, g * torch.arange(1, 5, device="cuda").view(-1, 1, 1))
+    assert torch.equal(q.grad, g * torch.arange(1, 5, device="cuda", dtype=torch.float32).view(-1, 1, 1))
+    q2 = torch.from_numpy(wl["q"][:2]).cuda().requires_grad_(True)
+    (gq,) = torch.autograd.grad(api.hinge_cost(q2, b, sc, _params(wl, 0.5)).sum(), q2, create_graph=True)
+    with pytest.raises(RuntimeError):
+        gq.sum().backward()
 
 
 def test_bdt_layout_equals_btd(w3):

@@ -99,3 +99,22 @@ def test_scene_tensors_masks_host_side():
         SceneTensors(*obbs, device="cpu", sphere_obb_acm_mask=np.ones(11, np.uint8))
     with pytest.raises(ValueError):   # no ESDF layers: an ESDF mask has no columns
         SceneTensors(*obbs, device="cpu", sphere_acm_mask=np.ones(4, np.uint8))
+
+
+def test_reference_call_shapes_set_only_known_fields():
+    """Every field the reference's build_robot_model and
+    PlanningScene.build_scene_collision_data set on the prrtc builders
+    (recorded in tests/golden/mbm_sample_fixtures.npz) exists on this
+    module's builders."""
+    from pathlib import Path
+
+    import numpy as np
+
+    z = np.load(Path(__file__).resolve().parent / "golden" / "mbm_sample_fixtures.npz")
+    robot_fields = z["robot_fields"].tolist()
+    assert set(robot_fields) <= set(ROBOT_FIELDS)
+    assert {"n_dof", "fixed_transforms", "spheres_flat", "joint_parents"} <= set(robot_fields)
+    for n in range(int(z["n_problems"])):
+        fields = z[f"p{n}/scene_fields"].tolist()
+        assert set(fields) <= set(SCENE_FIELDS), fields
+        assert int(z[f"p{n}/n_obbs"]) == len(z[f"p{n}/obb_dims"]) > 0
