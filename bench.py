@@ -340,6 +340,10 @@ def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev, timed_out)
     res["parity"] = edge_parity(timed_out, e2e_out, ref_out)
     # ---- CPU baseline (oracle port, FP32, all host threads, bounded sample) ----
     res["cpu_baseline"] = cpu_baseline(b, wl)
+    # evaluated samples per second of the headline step (early exit skips the rest)
+    res["evaluated_samples_per_s"] = stats[2] / (k_ms * 1e-3) if k_ms else None
+    # ---- the same chain and edges among sparser boxes (most edges free) ----
+    res["edges_sparse"] = bench_edges_sparse(dev, wl, b, frm, to, params)
     # ---- other workloads: configs (1) and CHOMP cost+gradient (3) ----
     res["configs"] = bench_configs(dev)
     res["chomp"] = bench_chomp(dev)
@@ -347,6 +351,91 @@ def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev, timed_out)
     res["stomp_solve"] = bench_stomp_solve(dev)
     res["stomp"] = bench_stomp(dev)
     res["mixed"] = bench_mixed(dev)
+    return res
+
+
+def bench_edges_sparse(dev, wl, b, frm, to, params, steps=20, with_ref=True):
+    """The headline's chain and 65,536 edges among 64 sparser boxes (centres
+    U([-1,1]^3), half-extents U(0.02, 0.1) instead of 0.3): about two thirds
+    of the edges are free, so most samples are evaluated rather than skipped
+    by early exit. Same graph-replayed persistent path; reports checked and
+    evaluated samples per second, the kernels' roofline fraction and the
+    verdict flips against the reference kernels on the same inputs."""
+    import ctypes
+
+    import torch
+
+    from prismplan_b200 import _lib, api, workloads
+    from prismplan_b200.scene import SceneTensors
+
+    lib = _lib.load()
+    obbs = workloads.random_obbs(np.random.default_rng(1012), 64, lo=-1.0, hi=1.0, half_lo=0.02, half_hi=0.1)
+    sc = SceneTensors(*obbs)
+    E = len(wl["from"])
+    total_samples = int(wl["G"].sum())
+    wsb = api.edges_workspace(E, dev)
+    out = (torch.empty(E, dtype=torch.uint8, device=dev), torch.empty(E, device=dev), torch.empty(E, device=dev))
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    with torch.cuda.stream(stream):
+        api.check_edges(b, sc, frm, to, params=params, workspace=wsb, out=out, stream=stream)
+    stream.synchronize()
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k0.record(stream)
+    k1.record(stream)
+    stream.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    lib.ps_set_timing_events(k0.cuda_event, k1.cuda_event)
+    with torch.cuda.graph(graph, stream=stream):
+        api.check_edges(b, sc, frm, to, params=params, workspace=wsb, out=out, stream=stream)
+    lib.ps_set_timing_events(None, None)
+    for _ in range(3):
+        graph.replay()
+    torch.cuda.synchronize()
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    kms = []
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 0xff)
+            e0[k].record(stream)
+            graph.replay()
+            e1[k].record(stream)
+        e1[k].synchronize()
+        kms.append(k0.elapsed_time(k1))
+    ms = statistics.median([a.elapsed_time(c) for a, c in zip(e0, e1)])
+    kmed = statistics.median(kms)
+    v_ours, c_ours = out[0].cpu().numpy().copy(), out[1].cpu().numpy().copy()
+    del graph
+    st = torch.zeros(8, dtype=torch.int64, device=dev)
+    lib.ps_set_stats(ctypes.c_void_p(st.data_ptr()))
+    api.check_edges(b, sc, frm, to, params=params)
+    torch.cuda.synchronize()
+    lib.ps_set_stats(None)
+    stats = [int(x) for x in st.cpu().tolist()]
+    peak = probe_peak()
+    ach = flops_from_stats(stats) / (kmed * 1e-3) / 1e12
+    res = {"workload": "edges_panda7_obb64sparse_e65536_linf0.01", "value": total_samples / (ms * 1e-3),
+           "unit": UNIT, "ms_per_step": ms, "valid_fraction": float(v_ours.mean()),
+           "evaluated_samples_per_s": stats[2] / (kmed * 1e-3), "evaluated_samples_per_step": stats[2],
+           "roofline": {"bound": "fp32", "kernel": "edges_probe_kernel + edges_queue_kernel", "kernel_ms": kmed,
+                        "achieved": ach, "peak": peak["tflops"], "unit": "TFLOP/s", "frac": ach / peak["tflops"],
+                        "flops_per_launch": flops_from_stats(stats),
+                        "work_per_launch": dict(zip(["pairs", "exact", "samples", "joints", "spheres", "self",
+                                                     "esdf", "cull"], stats))},
+           "scene": "64 OBBs, centres U([-1,1]^3), half-extents U(0.02,0.1), seed 1012"}
+    if with_ref:
+        try:
+            import oracle
+
+            ref = oracle.RefKernels(b, *obbs)
+            rv, rc, rms = ref.check_edges(wl["from"], wl["to"], wl["G"], reps=1)
+            flips = np.nonzero(v_ours != rv)[0]
+            res["reference_gpu"] = {"value": total_samples / (rms * 1e-3), "unit": UNIT, "ms_per_step": rms}
+            res["parity"] = {"flips": int(len(flips)),
+                             "cost_bitwise": bool(np.array_equal(c_ours.view(np.uint32), rc.view(np.uint32)))}
+        except Exception as e:
+            res["reference_gpu"] = {"unavailable": str(e)[:200]}
     return res
 
 
@@ -648,6 +737,9 @@ def _bench_solver(dev, kind, with_ref, ref_sample):
         out["reference_gpu"] = {"value": n / (rms * 1e-3), "unit": "requests/s", "ms_per_request": rms / n,
                                 "sample": f"first {n} of the {B} requests, one {kind.upper()}::solve_runtime_scene "
                                           "each",
+                                "precompute": "the reference solver's R / inverse / Cholesky come from an FP32 "
+                                              "restatement of its Eigen calls (partial-pivot LU inverse, LLT); "
+                                              "Eigen itself is absent here",
                                 "solved": int(rsolved.sum()), "mean_iterations": float(riters.mean()),
                                 "device_solved_same_sample": int(solved[:n].sum()),
                                 "device_mean_iterations_same_sample": float(iters[:n].mean())}
@@ -740,11 +832,12 @@ def bench_stomp(dev, with_ref=True):
 
 def bench_mixed(dev, reps: int = 10, with_ref=True):
     """Mixed-size batch on the 14-DoF composite (128 OBBs + 128^3 ESDF): 65
-    edge requests of 16..256 edges (8192 edges, 1..600 samples each) and 64
-    CHOMP trajectories of 32..128 waypoints with cost + gradient. Plain =
-    one per-request call each (ps_check_edges_plain, ps_traj_cost), batched =
-    one replay of the mixed graph. Checked configurations = sum of edge
-    samples + waypoints."""
+    edge requests of 16..256 edges (8192 edges, 1..600 samples each), 64
+    CHOMP trajectories of 32..128 waypoints with cost + gradient and 16 STOMP
+    rollout requests of 8 rollouts. Plain = one per-request call each
+    (ps_check_edges_plain, ps_traj_cost, ps_rollout_costs), batched = one
+    replay of the mixed graph. Checked configurations = sum of edge samples +
+    trajectory waypoints + rollout waypoints."""
     import torch
 
     from prismplan_b200 import api, workloads
@@ -761,8 +854,16 @@ def bench_mixed(dev, reps: int = 10, with_ref=True):
     cp = api.CostParams(collision_cost_weight=wl["w"], world_collision_margin=wl["eps"],
                         self_collision_margin=wl["self_margin"], smoothness_weight=1.0, delta_t=0.1)
     splits = wl["edge_splits"]
+    # STOMP rollout requests: 16 requests of 8 noisy copies (N(0, 0.05) rad) of
+    # the first 16 trajectories, in the reference layout [R, D, T]
+    rng = np.random.default_rng(1105)
+    rolls = []
+    for q in wl["trajectories"][:16]:
+        r = q.T[None] + rng.normal(0.0, 0.05, (8,) + q.T.shape)
+        rolls.append(torch.from_numpy(np.ascontiguousarray(r, np.float32)).to(dev))
     n_wp = sum(len(q) for q in trajs)
-    checked = int(wl["G"].sum()) + n_wp
+    n_roll = sum(r.shape[0] * r.shape[2] for r in rolls)
+    checked = int(wl["G"].sum()) + n_wp + n_roll
     slices, off = [], 0
     for k in splits:
         slices.append(slice(off, off + k))
@@ -773,21 +874,53 @@ def bench_mixed(dev, reps: int = 10, with_ref=True):
             api.check_edges(b, sc, frm[sl], to[sl], params=ep, persistent=False)
         for q in trajs:
             api.traj_cost(b, sc, q[None], cp)
+        for r in rolls:
+            api.rollout_costs(b, sc, r, cp)
 
     for _ in range(2):
         plain()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pe0.record()
     for _ in range(reps):
         plain()
+    pe1.record()
     torch.cuda.synchronize()
     plain_ms = (time.perf_counter() - t0) * 1e3 / reps
+    plain_dev_ms = pe0.elapsed_time(pe1) / reps
+    # the plain arm's kernels alone: each call's main kernel timed by the
+    # library's events, summed over the requests (no launch gaps, no host)
+    from prismplan_b200 import _lib
 
-    batch = api.MixedBatch(b, len(splits), len(wl["from"]), len(trajs), n_wp, 128)
+    lib = _lib.load()
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k0.record()
+    k1.record()
+    torch.cuda.synchronize()
+    lib.ps_set_timing_events(k0.cuda_event, k1.cuda_event)
+    plain_kernel_ms = 0.0
+    for sl in slices:
+        api.check_edges(b, sc, frm[sl], to[sl], params=ep, persistent=False)
+        torch.cuda.synchronize()
+        plain_kernel_ms += k0.elapsed_time(k1)
+    for q in trajs:
+        api.traj_cost(b, sc, q[None], cp)
+        torch.cuda.synchronize()
+        plain_kernel_ms += k0.elapsed_time(k1)
+    for r in rolls:
+        api.rollout_costs(b, sc, r, cp)
+        torch.cuda.synchronize()
+        plain_kernel_ms += k0.elapsed_time(k1)
+    lib.ps_set_timing_events(None, None)
+
+    batch = api.MixedBatch(b, len(splits), len(wl["from"]), len(trajs) + len(rolls), n_wp + n_roll, 128)
     for sl in slices:
         batch.add_edges(frm[sl], to[sl])
     for q in trajs:
         batch.add_trajectory(q)
+    for r in rolls:
+        batch.add_rollouts(r)
     tune = batch.tune(sc, ep, cp)
     stream = torch.cuda.Stream(device=dev)
     for _ in range(3):
@@ -805,13 +938,18 @@ def bench_mixed(dev, reps: int = 10, with_ref=True):
     dev_ms = e0.elapsed_time(e1) / reps
     batch.close()
     return {"workload": wl["name"], "requests": {"edge": len(splits), "edges": len(wl["from"]),
-                                                  "trajectories": len(trajs), "waypoints": n_wp},
+                                                  "trajectories": len(trajs), "waypoints": n_wp,
+                                                  "rollout_requests": len(rolls), "rollout_waypoints": n_roll},
             "checked_configs_per_step": checked, "unit": "configs/s",
-            "plain": {"value": checked / (plain_ms * 1e-3), "ms_per_step": plain_ms,
-                      "path": "per-request ps_check_edges_plain + ps_traj_cost calls, one sync per step"},
+            "plain": {"value": checked / (plain_ms * 1e-3), "ms_per_step": plain_ms, "device_ms": plain_dev_ms,
+                      "kernel_ms_sum": plain_kernel_ms,
+                      "path": "per-request ps_check_edges_plain + ps_traj_cost calls, one sync per step; "
+                              "device_ms = CUDA events around the step (launch gaps included), kernel_ms_sum = "
+                              "each call's main kernel alone, summed"},
             "batched": {"value": checked / (wall_ms * 1e-3), "ms_per_step": wall_ms, "device_ms": dev_ms,
                         "path": "ps_batch_launch (one graph replay: edge + trajectory branches)"},
-            "speedup": plain_ms / wall_ms, "tuning": tune}
+            "speedup": plain_ms / wall_ms, "speedup_device": plain_dev_ms / dev_ms,
+            "speedup_kernels_only": plain_kernel_ms / dev_ms, "tuning": tune}
 
 
 def run_reference(args):

@@ -319,8 +319,9 @@ int ps_rollout_costs(const ps_model* model, const ps_scene_view* scene,
                      float* state_cost, void* stream);
 
 /* =========================================================================
- * Mixed-request batches: many edge-check requests of uneven length and many
- * trajectory cost+gradient requests evaluated by one CUDA-graph launch.
+ * Mixed-request batches: many edge-check requests of uneven length, many
+ * trajectory cost+gradient requests and STOMP rollout-cost requests
+ * evaluated by one CUDA-graph launch.
  * Replaces the reference's one-launch-and-sync-per-request pattern
  * (EdgeEvalGpu::evaluate, cpp/src/planning/edge_batch_bridge.hh:60-96; the
  * CHOMP iteration loop, cpp/src/planning/chomp.cu:508-555; the STOMP rollout
@@ -354,9 +355,9 @@ typedef struct ps_batch_tuning {
                                 slots its persistent grid takes              */
     float traj_share;        /* same for the trajectory kernel's grid         */
     int   traj_threads;      /* threads per block of the trajectory kernel
-                                (one tile of waypoints per warp)             */
-    int   traj_tile;         /* waypoints per tile: 1 or 4 (one box cull per
-                                tile, against the union of their bounds)     */
+                                (64 or 128, one waypoint per thread)         */
+    int   traj_tile;         /* waypoints per thread of the trajectory kernel:
+                                always 1 (one waypoint per lane)             */
     float best_ms;           /* measured time of one launch at this choice    */
 } ps_batch_tuning;
 
@@ -374,6 +375,14 @@ int ps_batch_add_edges(ps_batch* batch, const float* from, const float* to,
    waypoint_cost is a STOMP rollout. */
 int ps_batch_add_trajectory(ps_batch* batch, const float* q, int T,
                             float* waypoint_cost, float* traj_cost, float* grad);
+/* n_rows STOMP rollouts of T waypoints (device, the reference layout
+   rollouts[(r*D + d)*T + t], stomp.cu:206-245). Output (device): state_cost
+   [n_rows*T], or [n_rows*D*T] with each value repeated over d when
+   broadcast_d != 0, as stomp_state_cost_kernel writes it. Equal to
+   ps_rollout_costs bit for bit; no gradient is computed. Counts one
+   trajectory request and n_rows*T waypoints of the capacity. */
+int ps_batch_add_rollouts(ps_batch* batch, const float* rollouts, int n_rows, int T,
+                          int broadcast_d, float* state_cost);
 /* Evaluates every request. params->compute_clearance must be 0 and
    cost->layout PS_LAYOUT_BTD. */
 int ps_batch_launch(ps_batch* batch, const ps_scene_view* scene,

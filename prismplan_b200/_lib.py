@@ -202,6 +202,7 @@ _SIGNATURES = [
      [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     ("ps_batch_add_trajectory", C.c_int,
      [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("ps_batch_add_rollouts", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     ("ps_batch_launch", C.c_int,
      [C.c_void_p, C.POINTER(SceneView), C.POINTER(EdgeParams), C.POINTER(CostParams), C.c_void_p]),
     ("ps_batch_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),

@@ -655,6 +655,21 @@ class MixedBatch:
         self._keep += [q, wp, tc, g]
         return wp, tc, g
 
+    def add_rollouts(self, rollouts, broadcast_d: bool = False):
+        """Queue STOMP rollouts [R, n_dof, T] (the reference layout); returns
+        their state costs, [R, T] or [R, n_dof, T] when broadcast_d, filled by
+        the next launch (equal to ``rollout_costs`` bit for bit)."""
+        torch = _torch()
+        r = _dev_f32(rollouts)
+        if r.dim() != 3 or r.shape[1] != self.robot.n_dof:
+            raise ValueError("rollouts must be [R, n_dof, T]")
+        R, D, T = r.shape
+        out = torch.empty((R, D, T) if broadcast_d else (R, T), dtype=torch.float32, device=r.device)
+        _lib.check(_lib.load().ps_batch_add_rollouts(self.handle, r.data_ptr(), R, T, 1 if broadcast_d else 0,
+                                                     out.data_ptr()))
+        self._keep += [r, out]
+        return out
+
     def launch(self, scene, edge_params: Optional[EdgeEvalParams] = None,
                cost_params: Optional[CostParams] = None, stream=None):
         ep = (edge_params or EdgeEvalParams()).to_c()

@@ -39,15 +39,19 @@ struct EdgeReq {           // one edge request as the device reads it
 };
 
 struct TrajReq {
-    const float* q;        // [T][D]
-    float* wp_cost;        // [T] or NULL
-    float* traj_cost;      // [1] or NULL
-    float* grad;           // [T][D] or NULL
-    int T, offset;         // waypoints, first packed waypoint
+    const float* q;        // trajectory [T][D]; rollouts [rows][D][T]
+    float* wp_cost;        // trajectory: [T] or NULL; rollouts: [rows*T] or [rows*D*T] (broadcast)
+    float* traj_cost;      // [1] or NULL (trajectories only)
+    float* grad;           // [T][D] or NULL (trajectories only)
+    int T, offset;         // waypoints per row, first packed waypoint
+    int rows;              // 1 for a trajectory, the rollout count otherwise
+    int rollouts;          // 1: STOMP rollouts (reference layout, no gradient)
+    int broadcast_d;       // rollouts: repeat each state cost over d
+    int pad;
 };
 
 struct Counts {
-    int n_edge_req, n_traj_req, n_edges, n_wp;
+    int n_edge_req, n_traj_req, n_edges, n_wp, n_roll;
 };
 
 constexpr int kFinishThreads = 128;   // same block width as ps_traj_cost's smoothness pass
@@ -84,14 +88,25 @@ __global__ void batch_scatter_edges(const EdgeReq* __restrict__ req, const Count
     }
 }
 
-// Packs every trajectory's waypoints.
+// Packs every trajectory's waypoints (waypoint-major); rollouts go from the
+// reference layout [rows][D][T] to waypoint-major rows.
 __global__ void batch_gather_traj(const TrajReq* __restrict__ req, const Counts* __restrict__ cnt, int D,
                                   float* __restrict__ q) {
     const int nreq = cnt->n_traj_req;
     for (int r = blockIdx.x; r < nreq; r += gridDim.x) {
         const TrajReq t = req[r];
         const size_t base = (size_t)t.offset * D;
-        for (int i = threadIdx.x; i < t.T * D; i += blockDim.x) q[base + i] = t.q[i];
+        if (!t.rollouts) {
+            for (int i = threadIdx.x; i < t.T * D; i += blockDim.x) q[base + i] = t.q[i];
+        } else {
+            const long long n = (long long)t.rows * t.T * D;
+            for (long long i = threadIdx.x; i < n; i += blockDim.x) {   // i over the packed rows
+                const int d = (int)(i % D);
+                const long long w = i / D;
+                const int row = (int)(w / t.T), tt = (int)(w - (long long)row * t.T);
+                q[base + i] = t.q[((size_t)row * D + d) * t.T + tt];
+            }
+        }
     }
 }
 
@@ -99,27 +114,33 @@ size_t waypoint_smem_bytes(const ps_model* m, const ps_scene_view* sv, int warps
     return lane_block_bytes(m, sv, warps, true);
 }
 
-// Cost and adjoint of every packed waypoint, one lane per waypoint (32
-// consecutive packed waypoints per warp, ps_costlane.cuh).
+// Cost and adjoint of every packed trajectory waypoint, and the cost alone of
+// every packed rollout waypoint, kCostSub lanes per waypoint (kCostSlots
+// consecutive packed waypoints per warp, ps_costlane.cuh). Trajectory
+// waypoints fill [0, n_wp) of the packed rows, rollout waypoints
+// [cap - n_roll, cap); a warp takes its waypoints from one range, so rollout
+// warps run without the adjoint.
 template <int kWarps>
-__global__ void __launch_bounds__(kWarps * 32, 8 / kWarps) batch_waypoint_kernel(ModelDev md, ps_scene_view sv,
+__global__ void __launch_bounds__(kWarps * 32, 16 / kWarps) batch_waypoint_kernel(ModelDev md, ps_scene_view sv,
                                                                                  ps_cost_params P,
                                                                                  const Counts* __restrict__ cnt,
                                                                                  const float* __restrict__ q,
                                                                                  float* __restrict__ wp_cost,
-                                                                                 float* __restrict__ grad) {
+                                                                                 float* __restrict__ grad, int cap) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ int counters[4];
     __shared__ float bmax;
-    const int n_wp = cnt->n_wp;
-    if ((long long)blockIdx.x * kWarps * 32 >= n_wp) return;   // nothing for this block: skip staging
+    const int n_wp = cnt->n_wp, n_roll = cnt->n_roll;
+    const int chunks_a = (n_wp + kCostSlots - 1) / kCostSlots, chunks = chunks_a + (n_roll + kCostSlots - 1) / kCostSlots;
+    if (blockIdx.x * kWarps >= chunks) return;   // nothing for this block: skip staging
     if (!stage_model(md, smem, &mbar)) {   // fail closed: NaN costs and gradient rows
         const float nan = __int_as_float(0x7fc00000);
-        cost_fail_closed(md, n_wp, kWarps * 32, [&](long long k, int D) {
+        cost_fail_closed(md, n_wp, kWarps * kCostSlots, [&](long long k, int D) {
             wp_cost[k] = nan;
             for (int d = 0; d < D; ++d) grad[(size_t)k * D + d] = nan;
         });
+        cost_fail_closed(md, n_roll, kWarps * kCostSlots, [&](long long k, int D) { wp_cost[cap - n_roll + k] = nan; });
         return;
     }
     const ModelSmem M = model_view(smem);
@@ -135,19 +156,28 @@ __global__ void __launch_bounds__(kWarps * 32, 8 / kWarps) batch_waypoint_kernel
     box_limits(sc, const_cast<float4*>(cb.obs));
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int slot = lane / kCostSub, u = lane % kCostSub;
     const LaneScratch ws =
         lane_carve(reinterpret_cast<unsigned char*>(cb.wbase) + (size_t)warp * lane_warp_bytes(NJ, D, sv.n_obbs, true),
                    NJ, D, true);
     LaneStats st;
-    for (int base = (blockIdx.x * kWarps + warp) * 32; base < n_wp; base += gridDim.x * kWarps * 32) {
-        const int k = base + lane;
-        const int kc = k < n_wp ? k : n_wp - 1;   // past the end: repeat the last waypoint
-        for (int d = 0; d < D; ++d) ws.q[d * 32 + lane] = q[(size_t)kc * D + d];
+    for (int c = blockIdx.x * kWarps + warp; c < chunks; c += gridDim.x * kWarps) {
+        const bool traj = c < chunks_a;   // uniform over the warp
+        const int lo = traj ? 0 : cap - n_roll, hi = traj ? n_wp : cap;
+        const int k = lo + (traj ? c : c - chunks_a) * kCostSlots + slot;
+        const int kc = k < hi ? k : hi - 1;   // past the end: repeat the last waypoint
+        for (int d = u; d < D; d += kCostSub) ws.q[d * kCostSlots + slot] = q[(size_t)kc * D + d];
+        __syncwarp();
         st.zero();
-        const float c = lane_cost<true, false>(M, md, sc, sv, P, cb, ws, st);
-        if (k < n_wp) {
-            wp_cost[k] = c;
-            lane_write_grad(M, cb, ws, grad + (size_t)k * D, 1);
+        if (traj) {
+            const float v = lane_cost<true, false>(M, md, sc, sv, P, cb, ws, st);
+            if (k < hi) {
+                if (u == 0) wp_cost[k] = v;
+                lane_write_grad(M, cb, ws, grad + (size_t)k * D, 1);
+            }
+        } else {
+            const float v = lane_cost<false, false>(M, md, sc, sv, P, cb, ws, st);
+            if (k < hi && u == 0) wp_cost[k] = v;
         }
     }
 }
@@ -165,6 +195,18 @@ __global__ void __launch_bounds__(kFinishThreads) batch_traj_finish(const TrajRe
         const TrajReq t = req[r];
         const float* qr = q + (size_t)t.offset * D;
         const float* wr = wp_cost + t.offset;
+        if (t.rollouts) {   // state costs only, in the reference layout
+            const long long n = (long long)t.rows * t.T;
+            for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+                if (t.broadcast_d) {
+                    const long long row = i / t.T, tt = i - row * t.T;
+                    for (int d = 0; d < D; ++d) t.wp_cost[((size_t)row * D + d) * t.T + tt] = wr[i];
+                } else {
+                    t.wp_cost[i] = wr[i];
+                }
+            }
+            continue;   // uniform over the block
+        }
         if (t.wp_cost)
             for (int i = threadIdx.x; i < t.T; i += blockDim.x) t.wp_cost[i] = wr[i];
         if (t.grad)
@@ -191,7 +233,7 @@ struct ps_batch {
     ps_batch_limits lim{};
     std::vector<EdgeReq> ereq;
     std::vector<TrajReq> treq;
-    int n_edges = 0, n_wp = 0;
+    int n_edges = 0, n_wp = 0, n_roll = 0;   // trajectory waypoints from 0 up, rollout waypoints from the top
     // pinned mirrors read by every replay
     EdgeReq* h_ereq = nullptr;
     TrajReq* h_treq = nullptr;
@@ -215,8 +257,8 @@ struct ps_batch {
     // tuning state
     float edge_share = 1.0f;   // of the edge kernel's full-occupancy grid
     float traj_share = 0.5f;   // of the trajectory kernel's full-occupancy grid
-    int traj_threads = 128;   // threads per block of the trajectory kernel (one waypoint per thread)
-    int traj_tile = 1;        // waypoints per thread (always 1)
+    int traj_threads = 128;   // threads per block of the trajectory kernel (kCostSub per waypoint)
+    int traj_tile = 1;        // kept for the tuning record: always 1
 };
 
 namespace {
@@ -225,13 +267,14 @@ struct LaunchPlan {
     int mode = 0;
     void (*qk)(ModelDev, ps_scene_view, ps_edge_params, const float*, const float*, int, EdgeWs*, const int*, int*,
                int*, int*, unsigned long long*, int, const int*) = nullptr;
-    void (*wk)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*) = nullptr;
+    void (*wk)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*, int) = nullptr;
     size_t qsmem = 0, wsmem = 0, fsmem = 0, ssmem = 0;
     int qgrid = 1, wgrid = 1, req_grid_e = 1, req_grid_t = 1, pgrid = 1, sgrid = 1;
     ProbePlan probe;
 };
 
-using WaypointKernel = void (*)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*);
+using WaypointKernel = void (*)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*,
+                                int);
 
 WaypointKernel pick_waypoint_kernel(int threads) {
     return threads == 64 ? batch_waypoint_kernel<2> : batch_waypoint_kernel<4>;
@@ -247,7 +290,7 @@ int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, 
                     edges_queue_kernel<1, false>, edges_queue_kernel<1, true>, edges_queue_kernel<2, false>,
                     edges_queue_kernel<2, true>);
         L.qsmem = edge_smem_bytes(m, sv);
-        PS_TRY_CUDA(cudaFuncSetAttribute(L.qk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.qsmem));
+        PS_TRY_CUDA(allow_smem((const void*)L.qk, L.qsmem));
         int per_sm = 0;
         PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L.qk, kEdgeThreads, L.qsmem));
         if (per_sm < 1) return set_error(PS_EINVAL, "edge kernel does not fit on an SM with this scene");
@@ -258,8 +301,7 @@ int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, 
         if (ep->check_self) {
             if (int rc = check_self_fits(m)) return rc;
             L.ssmem = self_smem_bytes(m);
-            PS_TRY_CUDA(cudaFuncSetAttribute(edges_self_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)L.ssmem));
+            PS_TRY_CUDA(allow_smem((const void*)edges_self_kernel, L.ssmem));
             int s_per_sm = 0;
             PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s_per_sm, edges_self_kernel, kSelfThreads,
                                                                       L.ssmem));
@@ -272,15 +314,15 @@ int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, 
         L.wsmem = waypoint_smem_bytes(m, sv, tt / 32);
         L.wk = pick_waypoint_kernel(tt);
         int per_sm = 0;
-        PS_TRY_CUDA(cudaFuncSetAttribute(L.wk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.wsmem));
+        PS_TRY_CUDA(allow_smem((const void*)L.wk, L.wsmem));
         PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L.wk, tt, L.wsmem));
         if (per_sm < 1) return set_error(PS_EINVAL, "trajectory kernel does not fit on an SM with this model/scene");
-        const int per_block = tt;   // one waypoint per thread
+        const int per_block = tt / kCostSub;   // waypoints per block
         const int cap_blocks = (b->lim.max_waypoints + per_block - 1) / per_block;
         L.wgrid = std::max(1, std::min(cap_blocks, (int)(b->traj_share * sms * per_sm + 0.5f)));
         L.fsmem = (size_t)(2 * (b->lim.max_traj_len + 12) + kFinishThreads) * sizeof(float);
         if (L.fsmem > 48 * 1024)
-            PS_TRY_CUDA(cudaFuncSetAttribute(batch_traj_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.fsmem));
+            PS_TRY_CUDA(allow_smem((const void*)batch_traj_finish, L.fsmem));
         L.req_grid_t = std::max(1, std::min(b->lim.max_traj_requests, sms * 8));
     }
     return PS_OK;
@@ -322,7 +364,8 @@ void record_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep
     }
     if (b->lim.max_waypoints > 0) {   // trajectory branch on s1
         batch_gather_traj<<<L.req_grid_t, 128, 0, s1>>>(b->d_treq, b->d_cnt, D, b->d_q);
-        L.wk<<<L.wgrid, b->traj_threads, L.wsmem, s1>>>(m->dev, *sv, *cp, b->d_cnt, b->d_q, b->d_wp_cost, b->d_grad);
+        L.wk<<<L.wgrid, b->traj_threads, L.wsmem, s1>>>(m->dev, *sv, *cp, b->d_cnt, b->d_q, b->d_wp_cost, b->d_grad,
+                                                        b->lim.max_waypoints);
         batch_traj_finish<<<L.req_grid_t, kFinishThreads, L.fsmem, s1>>>(b->d_treq, b->d_cnt, D, *cp, b->d_q,
                                                                          b->d_wp_cost, b->d_grad);
     }
@@ -477,7 +520,7 @@ extern "C" int ps_batch_clear(ps_batch* b) {
     if (!b) return set_error(PS_EINVAL, "NULL batch");
     b->ereq.clear();
     b->treq.clear();
-    b->n_edges = b->n_wp = 0;
+    b->n_edges = b->n_wp = b->n_roll = 0;
     return PS_OK;
 }
 
@@ -501,9 +544,25 @@ extern "C" int ps_batch_add_trajectory(ps_batch* b, const float* q, int T, float
     if (T <= 0 || !q) return set_error(PS_EINVAL, "empty trajectory or NULL q");
     if (T > b->lim.max_traj_len) return set_error(PS_EINVAL, "trajectory longer than max_traj_len");
     if ((int)b->treq.size() >= b->lim.max_traj_requests) return set_error(PS_EINVAL, "too many trajectory requests");
-    if ((long long)b->n_wp + T > b->lim.max_waypoints) return set_error(PS_EINVAL, "waypoint capacity exceeded");
-    b->treq.push_back(TrajReq{q, waypoint_cost, traj_cost, grad, T, b->n_wp});
+    if ((long long)b->n_wp + b->n_roll + T > b->lim.max_waypoints)
+        return set_error(PS_EINVAL, "waypoint capacity exceeded");
+    b->treq.push_back(TrajReq{q, waypoint_cost, traj_cost, grad, T, b->n_wp, 1, 0, 0, 0});
     b->n_wp += T;
+    return PS_OK;
+}
+
+extern "C" int ps_batch_add_rollouts(ps_batch* b, const float* rollouts, int n_rows, int T, int broadcast_d,
+                                     float* state_cost) {
+    clear_error();
+    if (!b) return set_error(PS_EINVAL, "NULL batch");
+    if (n_rows <= 0 || T <= 0 || !rollouts || !state_cost) return set_error(PS_EINVAL, "empty rollouts or NULL buffer");
+    if ((int)b->treq.size() >= b->lim.max_traj_requests) return set_error(PS_EINVAL, "too many trajectory requests");
+    const long long n = (long long)n_rows * T;
+    if ((long long)b->n_wp + b->n_roll + n > b->lim.max_waypoints)
+        return set_error(PS_EINVAL, "waypoint capacity exceeded");
+    b->n_roll += (int)n;
+    b->treq.push_back(TrajReq{rollouts, state_cost, nullptr, nullptr, T, b->lim.max_waypoints - b->n_roll, n_rows, 1,
+                              broadcast_d ? 1 : 0, 0});
     return PS_OK;
 }
 
@@ -520,7 +579,7 @@ extern "C" int ps_batch_launch(ps_batch* b, const ps_scene_view* sv, const ps_ed
     if (b->launched) PS_TRY_CUDA(cudaEventSynchronize(b->done));
     if (!b->ereq.empty()) std::memcpy(b->h_ereq, b->ereq.data(), sizeof(EdgeReq) * b->ereq.size());
     if (!b->treq.empty()) std::memcpy(b->h_treq, b->treq.data(), sizeof(TrajReq) * b->treq.size());
-    *b->h_cnt = Counts{(int)b->ereq.size(), (int)b->treq.size(), b->n_edges, b->n_wp};
+    *b->h_cnt = Counts{(int)b->ereq.size(), (int)b->treq.size(), b->n_edges, b->n_wp, b->n_roll};
     std::vector<unsigned char> key = make_key(b, sv, ep, cp);
     if (!b->exec || key != b->key) {
         b->key.clear();

@@ -438,7 +438,7 @@ extern "C" int ps_check_configs(const ps_model* m, const ps_scene_view* scene, c
                          : (g_stats ? check_configs_fast_kernel<false, true> : check_configs_fast_kernel<false, false>))
                   : (clr ? (g_stats ? check_configs_kernel<true, true> : check_configs_kernel<true, false>)
                          : (g_stats ? check_configs_kernel<false, true> : check_configs_kernel<false, false>));
-    PS_TRY_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PS_TRY_CUDA(allow_smem((const void*)k, smem));
     mark_start(s);
     k<<<grid, kCfgThreads, smem, s>>>(m->dev, *scene, q, n, margin, flags, hit, clearance, g_stats);
     mark_stop(s);
@@ -446,7 +446,7 @@ extern "C" int ps_check_configs(const ps_model* m, const ps_scene_view* scene, c
     if (flags & PS_CHECK_SELF) {
         if (int rc = check_self_fits(m)) return rc;
         const size_t ss = self_smem_bytes(m);
-        PS_TRY_CUDA(cudaFuncSetAttribute(self_check_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+        PS_TRY_CUDA(allow_smem((const void*)self_check_kernel, ss));
         const int g2 = std::max(1, std::min((n + kSelfThreads - 1) / kSelfThreads, sm_count() * 8));
         self_check_kernel<<<g2, kSelfThreads, ss, s>>>(m->dev, q, n, hit, g_stats);
         PS_TRY_CUDA(cudaGetLastError());
@@ -462,7 +462,7 @@ extern "C" int ps_fk_spheres(const ps_model* m, const float* q, int n, float* ou
     if (n <= 0) return PS_OK;
     cudaStream_t s = (cudaStream_t)stream;
     size_t smem = (size_t)m->dev.bytes_core;
-    PS_TRY_CUDA(cudaFuncSetAttribute(fk_spheres_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PS_TRY_CUDA(allow_smem((const void*)fk_spheres_kernel, smem));
     const int grid = std::max(1, std::min((n + kCfgThreads - 1) / kCfgThreads, sm_count() * 8));
     fk_spheres_kernel<<<grid, kCfgThreads, smem, s>>>(m->dev, q, n, out);
     PS_TRY_CUDA(cudaGetLastError());

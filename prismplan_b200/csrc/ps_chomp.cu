@@ -172,11 +172,11 @@ extern "C" int ps_chomp_optimize(const ps_model* m, const ps_scene_view* scene, 
     const int bk_threads = 128;
     const size_t bk_smem = (size_t)(2 * (T + 12) + bk_threads) * sizeof(float);
     if (bk_smem > 48 * 1024)
-        PS_TRY_CUDA(cudaFuncSetAttribute(chomp_bookkeep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bk_smem));
+        PS_TRY_CUDA(allow_smem((const void*)chomp_bookkeep_kernel, bk_smem));
     const int up_threads = std::min(T, 256);
     const size_t up_smem = sizeof(double) * (8 * T + 24);
     if (up_smem > 48 * 1024)
-        PS_TRY_CUDA(cudaFuncSetAttribute(chomp_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)up_smem));
+        PS_TRY_CUDA(allow_smem((const void*)chomp_update_kernel, up_smem));
 
     // One iteration: evaluate the current iterate (cost, adjoint, validity,
     // bookkeeping), then step every unfinished trajectory. The step index

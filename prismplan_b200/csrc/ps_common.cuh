@@ -48,9 +48,9 @@ struct JointRec {
 };
 
 // Self pairs (global memory): packed (i | j << 16), reordered sphere indices.
-// The same pairs as runs: sruns[r] = (i | q << 9 | len << 14, first) is
-// sphere i against the len spheres spairs[first..first+len) of joint q (DFS
-// position). Runs are ordered by joint pair (joint of i, q), then i;
+// The same pairs as runs: sruns[r] = (i | q << 9 | len << 14, j0) is sphere i
+// against the len consecutive spheres j0..j0+len-1 of joint q (DFS position).
+// Runs are ordered by joint pair (joint of i, q), then i, then j0;
 // sjp[k] = (a | q << 16, first run, end run, 0) lists the joint pairs.
 // Limits (global memory): lower[n_dof], upper[n_dof].
 struct ModelDev {
@@ -58,7 +58,6 @@ struct ModelDev {
     const uint32_t* self_pairs;    // device
     const uint32_t* apx_self_pairs;// device
     const uint2* sruns;            // device, self-pair runs
-    const uint16_t* spairs;        // device, second sphere of each run pair
     int n_sruns;
     const uint4* sjp;              // device, joint pairs: (a | q << 16, first run, end run, 0)
     int n_sjp;
@@ -307,7 +306,19 @@ struct SceneSmem {
     int n_obbs;                // enabled count
     int n_layers;
     float Bmax;
+    float Mscale;              // bound on |M v| / |v| over the boxes' and layers' world -> local maps
 };
+
+// A stored quaternion q with s = |q|^2 != 1 makes the reference's world ->
+// local map M = (1 - s) I + s R(q / |q|) instead of a rotation. M is normal
+// with singular values 1 and |(1 - s) + s e^{+-i theta}|, so with e = s - 1:
+//   |M v| <= (1 + 2|e|) |v|,  |M^-1 v| <= |v| / sqrt(1 - 4|e|(1 + |e|)).
+// The broad phases, which bound world distances, widen by these factors; a
+// box whose inverse bound does not hold (|e| >= 0.16) is never culled.
+__device__ __forceinline__ float quat_norm_err(float qw, float qx, float qy, float qz) {
+    return fabsf(fmaf(qw, qw, fmaf(qx, qx, fmaf(qy, qy, qz * qz))) - 1.0f) + 1.0e-6f;   // + its own rounding
+}
+__device__ __forceinline__ float map_stretch(float e) { return (1.0f + 2.0f * e) * (1.0f + 1.0e-6f); }
 
 // stage_scene / stage_model live in ps_stage.cuh.
 

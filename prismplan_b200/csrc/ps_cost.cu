@@ -31,14 +31,14 @@ size_t cost_block_smem(const ps_model* m, const ps_scene_view* sv, bool grad) {
     return lane_block_bytes(m, sv, kLaneCostWarps, grad);
 }
 
-// One lane per waypoint, 32 consecutive waypoints per warp (see
-// ps_costlane.cuh). kGrad: also the adjoint; kStats: count executed work.
-// Output layouts follow ps_cost_params.layout. skip (may be NULL): rows b
-// with skip[b] != 0 need no output and get none; a warp whose rows are all
-// skipped does nothing. Other waypoints of a warp are evaluated with the same
-// bits whichever rows share it.
+// A group of kCostSub lanes per waypoint, kCostSlots consecutive waypoints
+// per warp (see ps_costlane.cuh). kGrad: also the adjoint; kStats: count
+// executed work. Output layouts follow ps_cost_params.layout. skip (may be
+// NULL): rows b with skip[b] != 0 need no output and get none; a warp whose
+// rows are all skipped does nothing. A waypoint gets the same bits whichever
+// rows share its warp.
 template <bool kGrad, bool kStats>
-__global__ void __launch_bounds__(kLaneCostWarps * 32, 2) waypoint_cost_kernel(
+__global__ void __launch_bounds__(kLaneCostWarps * 32, 4) waypoint_cost_kernel(
     ModelDev md, ps_scene_view sv, const float* __restrict__ q, int n_rows, int T, ps_cost_params P,
     float* __restrict__ wp_cost, int broadcast_d, float* __restrict__ traj_acc, float* __restrict__ grad,
     unsigned long long* stats, const uint8_t* __restrict__ skip) {
@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(kLaneCostWarps * 32, 2) waypoint_cost_kernel(
     const bool bdt = P.layout == PS_LAYOUT_BDT;
     if (!stage_model(md, smem, &mbar)) {
         const float nan = __int_as_float(0x7fc00000);
-        cost_fail_closed(md, (long long)n_rows * T, kLaneCostWarps * 32, [&](long long idx, int D) {
+        cost_fail_closed(md, (long long)n_rows * T, kLaneCostWarps * kCostSlots, [&](long long idx, int D) {
             const int b = (int)(idx / T), tt = (int)(idx - (long long)b * T);
             if (wp_cost) {
                 if (broadcast_d)
@@ -77,36 +77,40 @@ __global__ void __launch_bounds__(kLaneCostWarps * 32, 2) waypoint_cost_kernel(
     __syncthreads();
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int slot = lane / kCostSub, u = lane % kCostSub;
     const LaneScratch ws = lane_carve(reinterpret_cast<unsigned char*>(cb.wbase) +
                                           (size_t)warp * lane_warp_bytes(NJ, D, sv.n_obbs, kGrad),
                                       NJ, D, kGrad);
     const long long total = (long long)n_rows * T;
     LaneStats st;
     st.zero();
-    for (long long base = ((long long)blockIdx.x * kLaneCostWarps + warp) * 32; base < total;
-         base += (long long)gridDim.x * kLaneCostWarps * 32) {
-        const long long idx = base + lane;
+    for (long long base = ((long long)blockIdx.x * kLaneCostWarps + warp) * kCostSlots; base < total;
+         base += (long long)gridDim.x * kLaneCostWarps * kCostSlots) {
+        const long long idx = base + slot;
         const long long ic = idx < total ? idx : total - 1;   // past the end: repeat the last waypoint
         const int b = (int)(ic / T), tt = (int)(ic - (long long)b * T);
         const bool live = idx < total && !(skip && skip[b]);
         if (!__any_sync(kCostFull, live)) continue;   // uniform
-        for (int d = 0; d < D; ++d)
-            ws.q[d * 32 + lane] = bdt ? q[((size_t)b * D + d) * T + tt] : q[((size_t)b * T + tt) * D + d];
+        for (int d = u; d < D; d += kCostSub)
+            ws.q[d * kCostSlots + slot] = bdt ? q[((size_t)b * D + d) * T + tt] : q[((size_t)b * T + tt) * D + d];
+        __syncwarp();
         LaneStats ls;
         ls.zero();
         const float cost = lane_cost<kGrad, kStats>(M, md, sc, sv, P, cb, ws, ls);
         if (!live) continue;
         if (kStats) {
-            ls.v[ST_SAMPLES] += 1;
+            if (u == 0) ls.v[ST_SAMPLES] += 1;
             for (int k = 0; k < ST_COUNT; ++k) st.v[k] += ls.v[k];
         }
-        if (wp_cost) {
-            if (broadcast_d)
-                for (int d = 0; d < D; ++d) wp_cost[((size_t)b * D + d) * T + tt] = cost;
-            else
-                wp_cost[idx] = cost;
+        if (u == 0) {
+            if (wp_cost) {
+                if (broadcast_d)
+                    for (int d = 0; d < D; ++d) wp_cost[((size_t)b * D + d) * T + tt] = cost;
+                else
+                    wp_cost[idx] = cost;
+            }
+            if (traj_acc) atomicAdd(traj_acc + b, cost);
         }
-        if (traj_acc) atomicAdd(traj_acc + b, cost);
         if (kGrad)
             lane_write_grad(M, cb, ws, bdt ? grad + ((size_t)b * D) * T + tt : grad + ((size_t)b * T + tt) * D,
                             bdt ? T : 1);
@@ -138,14 +142,14 @@ __global__ void smoothness_kernel(const float* __restrict__ q, int B, int T, int
 // the waypoint count. Returns -1 (error set) if a block does not fit.
 template <class K>
 int cost_grid(K kernel, size_t smem, long long total) {
-    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    if (allow_smem((const void*)kernel, smem) != cudaSuccess) {
         cudaGetLastError();
         return set_error(PS_EINVAL, "cost kernel shared memory exceeds the device limit"), -1;
     }
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kLaneCostWarps * 32, smem);
     if (per_sm < 1) return set_error(PS_EINVAL, "cost kernel does not fit on an SM with this model/scene"), -1;
-    const long long need = (total + kLaneCostWarps * 32 - 1) / (kLaneCostWarps * 32);
+    const long long need = (total + kLaneCostWarps * kCostSlots - 1) / (kLaneCostWarps * kCostSlots);
     return (int)std::max<long long>(1, std::min<long long>(need, (long long)per_sm * sm_count()));
 }
 
@@ -199,7 +203,7 @@ int ps::traj_cost_launch(const ps_model* m, const ps_scene_view* scene, const fl
         const int threads = 128;
         const size_t sm2 = (size_t)(2 * (T + 12) + threads) * sizeof(float);
         if (sm2 > 48 * 1024)
-            PS_TRY_CUDA(cudaFuncSetAttribute(smoothness_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+            PS_TRY_CUDA(allow_smem((const void*)smoothness_kernel, sm2));
         smoothness_kernel<<<B, threads, sm2, s>>>(q, B, T, m->info.n_dof, *P, waypoint_cost, traj_cost, grad, skip);
         PS_TRY_CUDA(cudaGetLastError());
     }

@@ -1,41 +1,47 @@
-// ps_costlane.cuh -- per-waypoint summed-hinge cost and its adjoint, one lane
-// per waypoint. Shared by the trajectory kernels (ps_cost.cu) and the
-// mixed-request batch (ps_batch.cu).
+// ps_costlane.cuh -- per-waypoint summed-hinge cost and its adjoint, a group
+// of kCostSub lanes per waypoint. Shared by the trajectory kernels
+// (ps_cost.cu) and the mixed-request batch (ps_batch.cu).
 //
 // Cost of one configuration (chomp.cu:151-188 / stomp.cu:206-245 over
 // scene_collision.cuh:394-495 and runtime_kinematics.cuh:295-330):
 //   w * ( sum_s relu(m - esdf_clr_s) + sum_s relu(m - min_o obb_clr_s,o)
 //         + relu(m_self - min_(i,j) (|p_i - p_j| - r_i - r_j)) ).
-// A warp holds 32 waypoints, one per lane; every loop below is uniform over
-// the warp, so lanes never diverge on the candidate lists:
-//   1. FK walk in DFS order with accurate sincosf; each lane keeps its frames
-//      (and each joint's world bound centre) in shared memory, SoA by lane;
-//   2. per joint, one warp broad phase: the joint's bound spheres of the 32
-//      waypoints are enclosed by one sphere (centre = lane 16's, radius = a
-//      one-instruction warp max), and lanes over boxes keep the boxes within
-//      that radius + max(m, 0) (a circumscribed-sphere test first, the box
-//      distance second). A box outside it has sdf > m + r for every sphere of
-//      the joint at every lane, so it changes no hinge;
-//   3. the joint's spheres, 4 per box load, against the kept boxes: the
-//      closest box by one key per pair (d^2 outside, the most negative
-//      max(q) inside), then sdf, hinge and, with the gradient, the force
-//      g = -w grad(sdf) summed into the joint's F = sum g, M = sum p x g;
-//   4. F and M are folded into the joint's ancestors right away:
-//      dC/dq_p += a_p . (M - o_p x F) (revolute) or a_p . F (prismatic), a_p
-//      and o_p the joint axis and origin from the stored frames;
-//   5. self hinge: joint pairs whose bound spheres can come within m_self
-//      (any lane) expand their runs (sphere i of joint a against the spheres
-//      of joint q); sphere i is mapped into q's link frame once per run, so a
-//      pair costs one difference against the link-frame centre; a run whose
-//      bound test fails on every lane is skipped. Only pairs within
-//      r_i + r_j + m_self can set the hinge, and a square root is taken only
-//      for those; the argmin pair's force goes to both joints' ancestors.
-// Every candidate set is a superset of what the waypoint itself needs, so a
-// waypoint gives the same bits whatever other waypoints share its warp; the
-// batch relies on that. Sums run in sphere order per lane.
+// A warp holds kCostSlots waypoints, kCostSub lanes each; every loop below is
+// uniform over the warp (candidate lists, runs, joint pairs), so lanes do not
+// diverge on them:
+//   1. FK walk in DFS order with accurate sincosf (each lane of a group
+//      repeats it; the group's frames and each joint's world bound centre go
+//      to shared memory, SoA by waypoint slot);
+//   2. per joint, one warp broad phase: the joint's bound spheres of the
+//      warp's waypoints are enclosed by one sphere (centre = lane 16's, radius
+//      = a one-instruction warp max), and lanes over boxes keep the boxes
+//      within that radius + max(m, 0) (a circumscribed-sphere test first, the
+//      box distance second). A box outside it has sdf > m + r for every sphere
+//      of the joint at every waypoint of the warp, so it changes no hinge;
+//   3. the joint's spheres, split over the group's lanes, up to 4 per box load,
+//      against the kept boxes: the closest box by one key per pair (d^2
+//      outside, the most negative max(q) inside), then sdf, hinge and, with the
+//      gradient, the force g = -w grad(sdf) summed into the joint's
+//      F = sum g, M = sum p x g;
+//   4. F and M are summed over the group and folded into the joint's
+//      ancestors: dC/dq_p += a_p . (M - o_p x F) (revolute) or a_p . F
+//      (prismatic), a_p and o_p the joint axis and origin from the frames;
+//   5. self hinge: joint pairs whose bound spheres can come within m_self (on
+//      any waypoint of the warp) expand their runs (sphere i of joint a against
+//      consecutive spheres j of joint q), a run whose bound test fails
+//      everywhere is skipped; sphere i is mapped into q's link frame once per
+//      run, so a pair costs one difference against a link-frame centre, split
+//      over the group's lanes. Only pairs within r_i + r_j + m_self can set the
+//      hinge, and a square root is taken only for those; the minimum over the
+//      group is taken by (value, pair order), and the argmin pair's force goes
+//      to both joints' ancestors.
+// Every candidate set is a superset of what the waypoint itself needs, and
+// the group size is fixed, so a waypoint gives the same bits whatever other
+// waypoints share its warp; the batch relies on that.
 #pragma once
 
 #include <algorithm>
+#include <climits>
 #include <cstdint>
 
 #include "ps_costwarp.cuh"
@@ -43,23 +49,25 @@
 namespace ps {
 namespace {
 
-constexpr int kLaneCostWarps = 4;   // warps per block of the lane cost kernels
+constexpr int kCostSub = 4;                  // lanes per waypoint
+constexpr int kCostSlots = 32 / kCostSub;    // waypoints per warp
+constexpr int kLaneCostWarps = 4;            // warps per block of the cost kernels
 
-// Per-warp scratch floats, SoA over the 32 lanes: frames of joints 1..NJ-1
-// (joint 0 is the identity), world bound centres, per-joint gradient
-// (gradient only), the lane's configuration.
+// Per-warp scratch floats, SoA over the warp's waypoint slots: frames of
+// joints 1..NJ-1 (joint 0 is the identity), world bound centres, per-joint
+// gradient (gradient only), the waypoint's configuration.
 __host__ __device__ inline int lane_cost_floats(int NJ, int D, bool grad) {
-    return 32 * (12 * (NJ - 1) + 3 * NJ + (grad ? NJ : 0) + D);
+    return kCostSlots * (12 * (NJ - 1) + 3 * NJ + (grad ? NJ : 0) + D);
 }
 __host__ __device__ inline size_t lane_warp_bytes(int NJ, int D, int n_obbs, bool grad) {
     return (size_t)lane_cost_floats(NJ, D, grad) * 4 + ((((size_t)(n_obbs > 0 ? n_obbs : 1)) * 2 + 15) & ~size_t(15));
 }
 
 struct LaneScratch {
-    float* fr;        // [(NJ-1)*12][32]
-    float* bc;        // [NJ*3][32]
-    float* dq;        // [NJ][32] (gradient only)
-    float* q;         // [D][32]
+    float* fr;        // [(NJ-1)*12][slots]
+    float* bc;        // [NJ*3][slots]
+    float* dq;        // [NJ][slots] (gradient only)
+    float* q;         // [D][slots]
     uint16_t* cand;   // [n_obbs]: boxes kept by the current joint's broad phase (warp-uniform)
 };
 
@@ -67,13 +75,13 @@ __device__ __forceinline__ LaneScratch lane_carve(unsigned char* base, int NJ, i
     LaneScratch s;
     float* f = reinterpret_cast<float*>(base);
     s.fr = f;
-    f += 32 * 12 * (NJ - 1);
+    f += kCostSlots * 12 * (NJ - 1);
     s.bc = f;
-    f += 32 * 3 * NJ;
+    f += kCostSlots * 3 * NJ;
     s.dq = grad ? f : nullptr;
-    if (grad) f += 32 * NJ;
+    if (grad) f += kCostSlots * NJ;
     s.q = f;
-    f += 32 * D;
+    f += kCostSlots * D;
     s.cand = reinterpret_cast<uint16_t*>(f);
     return s;
 }
@@ -86,29 +94,29 @@ inline size_t lane_block_bytes(const ps_model* m, const ps_scene_view* sv, int w
            (size_t)warps * lane_warp_bytes(m->info.n_joints, m->info.n_dof, sv->n_obbs, grad);
 }
 
-__device__ __forceinline__ void lane_frame(const float* fr, int p, int lane, Affine& T) {
+__device__ __forceinline__ void lane_frame(const float* fr, int p, int slot, Affine& T) {
     if (p == 0) {
         affine_identity(T);
         return;
     }
-    const float* b = fr + (size_t)(p - 1) * 12 * 32 + lane;
+    const float* b = fr + (size_t)(p - 1) * 12 * kCostSlots + slot;
 #pragma unroll
-    for (int k = 0; k < 12; ++k) T.m[k] = b[k * 32];
+    for (int k = 0; k < 12; ++k) T.m[k] = b[k * kCostSlots];
 }
 
-// dC/dq_p of a joint's summed force F and moment M (about the world origin),
-// added to every movable ancestor p of joint j (j included).
-__device__ __forceinline__ void lane_fold(const ModelSmem& M, const LaneScratch& ws, int lane, int j, float Fx,
+// dC/dq_p of a summed force F and moment M (about the world origin) applied
+// through joint j, added to every movable ancestor p of j (j included).
+__device__ __forceinline__ void lane_fold(const ModelSmem& M, const LaneScratch& ws, int slot, int j, float Fx,
                                           float Fy, float Fz, float Mx, float My, float Mz) {
     for (int p = j; p >= 1; p = M.J[p].parent_pos) {
         const JointRec& jr = M.J[p];
         if (jr.dof < 0 || jr.type == PS_FIXED) continue;
-        const float* b = ws.fr + (size_t)(p - 1) * 12 * 32 + lane;
+        const float* b = ws.fr + (size_t)(p - 1) * 12 * kCostSlots + slot;
         const int ax = jr.type >= PS_X_ROT ? jr.type - PS_X_ROT : jr.type;
-        const float axx = b[ax * 32], axy = b[(4 + ax) * 32], axz = b[(8 + ax) * 32];
+        const float axx = b[ax * kCostSlots], axy = b[(4 + ax) * kCostSlots], axz = b[(8 + ax) * kCostSlots];
         float v;
         if (jr.type >= PS_X_ROT) {
-            const float ox = b[3 * 32], oy = b[7 * 32], oz = b[11 * 32];
+            const float ox = b[3 * kCostSlots], oy = b[7 * kCostSlots], oz = b[11 * kCostSlots];
             const float tx = Mx - (oy * Fz - oz * Fy);
             const float ty = My - (oz * Fx - ox * Fz);
             const float tz = Mz - (ox * Fy - oy * Fx);
@@ -116,8 +124,15 @@ __device__ __forceinline__ void lane_fold(const ModelSmem& M, const LaneScratch&
         } else {
             v = axx * Fx + axy * Fy + axz * Fz;
         }
-        ws.dq[p * 32 + lane] += v;
+        ws.dq[p * kCostSlots + slot] += v;
     }
+}
+
+// Sum over the kCostSub lanes of a waypoint's group (fixed xor order).
+__device__ __forceinline__ float group_sum(float v) {
+#pragma unroll
+    for (int o = 1; o < kCostSub; o <<= 1) v += __shfl_xor_sync(kCostFull, v, o);
+    return v;
 }
 
 // Closest-box key of kG spheres over the candidate boxes: d^2 outside, the
@@ -157,7 +172,6 @@ __device__ __forceinline__ void lane_keys(const SceneSmem& sc, const uint16_t* c
 }
 
 // Same for one sphere with its ACM row (global memory): masked boxes skipped.
-template <bool kGrad>
 __device__ __forceinline__ void lane_key_masked(const SceneSmem& sc, const uint16_t* cand, int ncand, float px,
                                                 float py, float pz, const uint8_t* acm_row, float& key, int& arg) {
     key = 3.0e38f;
@@ -165,7 +179,7 @@ __device__ __forceinline__ void lane_key_masked(const SceneSmem& sc, const uint1
 #pragma unroll 1
     for (int c = 0; c < ncand; ++c) {
         const int o = cand[c];
-        if (acm_row[sc.obb_orig[o]] == 0) continue;   // uniform: same sphere on every lane
+        if (acm_row[sc.obb_orig[o]] == 0) continue;
         float qx, qy, qz;
         const float d2 = fast_box_dsq(sc.obbs[o], px, py, pz, qx, qy, qz);
         const float k = d2 + fminf(fmaxf(qx, fmaxf(qy, qz)), 0.0f);
@@ -176,19 +190,85 @@ __device__ __forceinline__ void lane_key_masked(const SceneSmem& sc, const uint1
     }
 }
 
-// Cost of this lane's waypoint (its configuration in ws.q) and, with kGrad,
-// the per-joint gradient in ws.dq. Every lane of the warp calls it.
+// Hinge terms of one sphere (box key already found): adds the OBB and ESDF
+// hinges to the lane's partial sums and, with kGrad, returns the force on the
+// sphere in (gx, gy, gz).
+template <bool kGrad, bool kStats>
+__device__ __forceinline__ void lane_sphere_terms(const ModelSmem& M, const SceneSmem& sc, const ps_scene_view& sv,
+                                                  const ps_cost_params& P, int k, float px, float py, float pz,
+                                                  float r, bool have_key, float key, int arg, float& obb_part,
+                                                  float& esdf_part, float& gx, float& gy, float& gz, LaneStats& st) {
+    const float w = P.collision_cost_weight, wm = P.world_margin;
+    gx = gy = gz = 0.0f;
+    if (have_key && key < 3.0e38f) {
+        const float sdf = key > 0.0f ? sqrtf(key) : key;
+        const float hinge = wm - (sdf - r);
+        if (hinge > 0.0f) {
+            obb_part += hinge;
+            if (kGrad) {
+                float ux, uy, uz;
+                box_sdf_grad(sc.obbs[arg], px, py, pz, ux, uy, uz);
+                gx -= w * ux;
+                gy -= w * uy;
+                gz -= w * uz;
+            }
+        }
+    }
+    if (sc.n_layers) {
+        const int so = M.SO[k];
+        const uint8_t* eacm = sv.sphere_acm_mask ? sv.sphere_acm_mask + (size_t)so * sv.n_voxel_layers : nullptr;
+        if (sv.esdf_mode == PS_ESDF_TRILINEAR) {
+            // min over layers of -d - r; d(cost)/dp = w * grad d of the minimising layer
+            float best = 1000.0f, bgx = 0.f, bgy = 0.f, bgz = 0.f;
+            for (int l = 0; l < sc.n_layers; ++l) {
+                if (eacm && eacm[l] == 0) continue;
+                float d, dgx, dgy, dgz;
+                if (kStats) st.v[ST_ESDF] += 1;
+                if (!esdf_sample_trilinear_grad(sc.layers[l], sv.voxel_features + (size_t)l * sv.max_voxels_per_layer,
+                                                sv.max_voxels_per_layer, px, py, pz, d, dgx, dgy, dgz))
+                    continue;
+                const float c = -d - r;
+                if (c < best) {
+                    best = c;
+                    bgx = dgx;
+                    bgy = dgy;
+                    bgz = dgz;
+                }
+            }
+            const float hinge = wm - best;
+            if (hinge > 0.0f) {
+                esdf_part += hinge;
+                if (kGrad) {
+                    gx += w * bgx;
+                    gy += w * bgy;
+                    gz += w * bgz;
+                }
+            }
+        } else {
+            LaneStats est;
+            est.zero();
+            const float clr = sphere_esdf_clearance(sc, sv, px, py, pz, r, eacm, est);
+            if (kStats) st.v[ST_ESDF] += est.v[ST_ESDF];
+            esdf_part += fmaxf(0.0f, wm - clr);
+            // the nearest-voxel lookup is piecewise constant: zero gradient
+        }
+    }
+}
+
+// Cost of the lane group's waypoint (its configuration in ws.q) and, with
+// kGrad, the per-joint gradient in ws.dq. Every lane of the warp calls it; the
+// result is the same on the kCostSub lanes of a group.
 template <bool kGrad, bool kStats>
 __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSmem& sc, const ps_scene_view& sv,
                            const ps_cost_params& P, const CostBlock& cb, const LaneScratch& ws, LaneStats& st) {
     const float4* __restrict__ obs = cb.obs;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, slot = lane / kCostSub, u = lane % kCostSub;
     const int NJ = M.H->n_joints;
-    const float w = P.collision_cost_weight, wm = P.world_margin;
-    const float wmp = fmaxf(wm, 0.0f);
+    const float w = P.collision_cost_weight, wmp = fmaxf(P.world_margin, 0.0f);
     float obb_part = 0.0f, esdf_part = 0.0f;
-    if (kGrad)
-        for (int p = 0; p < NJ; ++p) ws.dq[p * 32 + lane] = 0.0f;
+    if (kGrad && u == 0)
+        for (int p = 0; p < NJ; ++p) ws.dq[p * kCostSlots + slot] = 0.0f;
+    const bool masked = sv.sphere_obb_acm_mask != nullptr;
     Affine T;
     for (int p = 0; p < NJ; ++p) {
         const JointRec& jr = M.J[p];
@@ -196,21 +276,27 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
             affine_identity(T);
         } else {
             Affine Pf;
-            lane_frame(ws.fr, jr.parent_pos, lane, Pf);
-            const float qi = jr.dof >= 0 ? ws.q[jr.dof * 32 + lane] : 0.0f;
+            lane_frame(ws.fr, jr.parent_pos, slot, Pf);
+            const float qi = jr.dof >= 0 ? ws.q[jr.dof * kCostSlots + slot] : 0.0f;
             joint_compose<false>(jr, qi, Pf, T);
-            float* b = ws.fr + (size_t)(p - 1) * 12 * 32 + lane;
+            if (u == 0) {
+                float* b = ws.fr + (size_t)(p - 1) * 12 * kCostSlots + slot;
 #pragma unroll
-            for (int k = 0; k < 12; ++k) b[k * 32] = T.m[k];
-            if (kStats) st.v[ST_JOINTS] += 1;
+                for (int k = 0; k < 12; ++k) b[k * kCostSlots] = T.m[k];
+            }
+            if (kStats && u == 0) st.v[ST_JOINTS] += 1;
         }
+        __syncwarp();
         if (jr.bound.w < 0.0f) continue;   // no spheres on this joint (uniform)
         float cx, cy, cz;
         sphere_world(T, jr.bound.x, jr.bound.y, jr.bound.z, cx, cy, cz);
-        ws.bc[(p * 3 + 0) * 32 + lane] = cx;
-        ws.bc[(p * 3 + 1) * 32 + lane] = cy;
-        ws.bc[(p * 3 + 2) * 32 + lane] = cz;
-        if (jr.sph_end == jr.sph_beg) continue;   // approximate spheres only: no cost term
+        if (u == 0) {
+            ws.bc[(p * 3 + 0) * kCostSlots + slot] = cx;
+            ws.bc[(p * 3 + 1) * kCostSlots + slot] = cy;
+            ws.bc[(p * 3 + 2) * kCostSlots + slot] = cz;
+        }
+        const int n = jr.sph_end - jr.sph_beg;
+        if (n == 0) continue;   // approximate spheres only: no cost term
         // ---- warp broad phase over boxes ----
         int ncand = 0;
         if (sc.n_obbs > 0) {
@@ -223,7 +309,8 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
             const float r2c = fmaxf(r2, 1.0e-30f);
             float Rc = r2c * rsqrtf(r2c) * (1.0f + 1.0e-6f) + jr.bound.w + wmp;
             Rc += 4.0f * (Sm + Rc + sc.Bmax + 1.0f) * PS_GUARD_K;
-            const float Rc2 = Rc * Rc;
+            const float Rcl = Rc * sc.Mscale;   // world radius -> box-frame radius (map stretch)
+            const float Rc2 = Rcl * Rcl;
             const float Rj = (Rc * (1.0f + 4.0f * PS_GUARD_K) + 4.0f * PS_GUARD_K * (Sm + 1.0f)) * (1.0f + 1.0e-6f);
             __syncwarp();   // the previous joint's readers of ws.cand are done
 #pragma unroll 1
@@ -246,93 +333,48 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
             }
             __syncwarp();
         }
-        // ---- the joint's spheres ----
+        // ---- the joint's spheres: lane u of the group takes spheres
+        //      sph_beg + u, + kCostSub, ... (up to 4 per box load) ----
         float Fx = 0.f, Fy = 0.f, Fz = 0.f, Mx = 0.f, My = 0.f, Mz = 0.f;
-        const bool masked = sv.sphere_obb_acm_mask != nullptr;
-        int k = jr.sph_beg;
-        while (k < jr.sph_end) {
-            constexpr int kG = 4;
-            const int ng = (!masked && k + kG <= jr.sph_end) ? kG : 1;   // uniform
-            float px[kG], py[kG], pz[kG], rr[kG], key[kG];
-            int arg[kG];
+        const int nm = (n + kCostSub - 1) / kCostSub;   // spheres per lane, uniform
+        for (int m0 = 0; m0 < nm;) {
+            const int ng = masked ? 1 : min(4, nm - m0);   // uniform
+            float px[4], py[4], pz[4], rr[4], key[4];
+            int arg[4], kk[4];
+            bool val[4];
 #pragma unroll
-            for (int i = 0; i < kG; ++i) {
-                const float4 sp = M.S[i < ng ? k + i : k];
+            for (int i = 0; i < 4; ++i) {
+                const int k = jr.sph_beg + u + kCostSub * (m0 + i);
+                val[i] = i < ng && k < jr.sph_end;
+                kk[i] = val[i] ? k : jr.sph_beg;
+                const float4 sp = M.S[kk[i]];
                 sphere_world(T, sp.x, sp.y, sp.z, px[i], py[i], pz[i]);
                 rr[i] = sp.w;
+                key[i] = 3.0e38f;
+                arg[i] = -1;
+                if (kStats && val[i]) st.v[ST_SPHERES] += 1;
             }
-            if (kStats) st.v[ST_SPHERES] += ng;
             if (ncand > 0) {
-                if (masked) {
-                    lane_key_masked<kGrad>(sc, ws.cand, ncand, px[0], py[0], pz[0],
-                                           sv.sphere_obb_acm_mask + (size_t)M.SO[k] * sv.n_obbs, key[0], arg[0]);
-                } else if (ng == kG) {
-                    lane_keys<kG, kGrad>(sc, ws.cand, ncand, px, py, pz, key, arg);
-                } else {
+                if (masked)
+                    lane_key_masked(sc, ws.cand, ncand, px[0], py[0], pz[0],
+                                    sv.sphere_obb_acm_mask + (size_t)M.SO[kk[0]] * sv.n_obbs, key[0], arg[0]);
+                else if (ng == 4)
+                    lane_keys<4, kGrad>(sc, ws.cand, ncand, px, py, pz, key, arg);
+                else if (ng == 3)
+                    lane_keys<3, kGrad>(sc, ws.cand, ncand, px, py, pz, key, arg);
+                else if (ng == 2)
+                    lane_keys<2, kGrad>(sc, ws.cand, ncand, px, py, pz, key, arg);
+                else
                     lane_keys<1, kGrad>(sc, ws.cand, ncand, px, py, pz, key, arg);
-                }
-                if (kStats) st.v[ST_PAIRS] += ncand * ng;
+                if (kStats)
+                    for (int i = 0; i < 4; ++i) st.v[ST_PAIRS] += val[i] ? ncand : 0;
             }
 #pragma unroll
-            for (int i = 0; i < kG; ++i) {
-                if (i >= ng) break;
-                float gx = 0.f, gy = 0.f, gz = 0.f;
-                if (ncand > 0 && key[i] < 3.0e38f) {
-                    const float sdf = key[i] > 0.0f ? sqrtf(key[i]) : key[i];
-                    const float hinge = wm - (sdf - rr[i]);
-                    if (hinge > 0.0f) {
-                        obb_part += hinge;
-                        if (kGrad) {
-                            float ux, uy, uz;
-                            box_sdf_grad(sc.obbs[arg[i]], px[i], py[i], pz[i], ux, uy, uz);
-                            gx -= w * ux;
-                            gy -= w * uy;
-                            gz -= w * uz;
-                        }
-                    }
-                }
-                if (sc.n_layers) {
-                    const int so = M.SO[k + i];
-                    const uint8_t* eacm =
-                        sv.sphere_acm_mask ? sv.sphere_acm_mask + (size_t)so * sv.n_voxel_layers : nullptr;
-                    if (sv.esdf_mode == PS_ESDF_TRILINEAR) {
-                        // min over layers of -d - r; d(cost)/dp = w * grad d of the minimising layer
-                        float best = 1000.0f, bgx = 0.f, bgy = 0.f, bgz = 0.f;
-                        for (int l = 0; l < sc.n_layers; ++l) {
-                            if (eacm && eacm[l] == 0) continue;
-                            float d, dgx, dgy, dgz;
-                            if (kStats) st.v[ST_ESDF] += 1;
-                            if (!esdf_sample_trilinear_grad(sc.layers[l],
-                                                            sv.voxel_features + (size_t)l * sv.max_voxels_per_layer,
-                                                            sv.max_voxels_per_layer, px[i], py[i], pz[i], d, dgx, dgy,
-                                                            dgz))
-                                continue;
-                            const float c = -d - rr[i];
-                            if (c < best) {
-                                best = c;
-                                bgx = dgx;
-                                bgy = dgy;
-                                bgz = dgz;
-                            }
-                        }
-                        const float hinge = wm - best;
-                        if (hinge > 0.0f) {
-                            esdf_part += hinge;
-                            if (kGrad) {
-                                gx += w * bgx;
-                                gy += w * bgy;
-                                gz += w * bgz;
-                            }
-                        }
-                    } else {
-                        LaneStats est;
-                        est.zero();
-                        const float clr = sphere_esdf_clearance(sc, sv, px[i], py[i], pz[i], rr[i], eacm, est);
-                        if (kStats) st.v[ST_ESDF] += est.v[ST_ESDF];
-                        esdf_part += fmaxf(0.0f, wm - clr);
-                        // the nearest-voxel lookup is piecewise constant: zero gradient
-                    }
-                }
+            for (int i = 0; i < 4; ++i) {
+                if (!val[i]) continue;
+                float gx, gy, gz;
+                lane_sphere_terms<kGrad, kStats>(M, sc, sv, P, kk[i], px[i], py[i], pz[i], rr[i], ncand > 0, key[i],
+                                                 arg[i], obb_part, esdf_part, gx, gy, gz, st);
                 if (kGrad) {
                     Fx += gx;
                     Fy += gy;
@@ -342,41 +384,48 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
                     Mz += px[i] * gy - py[i] * gx;
                 }
             }
-            k += ng;
+            m0 += ng;
         }
         if (kGrad) {
+            Fx = group_sum(Fx);
+            Fy = group_sum(Fy);
+            Fz = group_sum(Fz);
+            Mx = group_sum(Mx);
+            My = group_sum(My);
+            Mz = group_sum(Mz);
             const bool any = Fx != 0.f || Fy != 0.f || Fz != 0.f || Mx != 0.f || My != 0.f || Mz != 0.f;
-            if (__any_sync(kCostFull, any)) lane_fold(M, ws, lane, p, Fx, Fy, Fz, Mx, My, Mz);
+            if (__any_sync(kCostFull, any) && u == 0) lane_fold(M, ws, slot, p, Fx, Fy, Fz, Mx, My, Mz);
         }
     }
+    __syncwarp();   // frames and bound centres of every joint are written
 
     // ---- self hinge ----
     float self_h = 0.0f;
     if (P.include_self && md.n_sjp > 0) {
         const float smg = P.self_margin, smp = fmaxf(smg, 0.0f);
         float bv = smg;   // pairs at or above the margin cannot set the hinge
-        int bi = -1, bj = -1;
+        int bk = INT_MAX, bi = -1, bj = -1;
         for (int jp = 0; jp < md.n_sjp; ++jp) {
             const uint4 e = __ldg(md.sjp + jp);
             const int a = (int)(e.x & 0xffffu), qj = (int)(e.x >> 16);
             const float4 ba = M.J[a].bound, bq = M.J[qj].bound;
-            const float ax = ws.bc[(a * 3) * 32 + lane], ay = ws.bc[(a * 3 + 1) * 32 + lane],
-                        az = ws.bc[(a * 3 + 2) * 32 + lane];
-            const float qx0 = ws.bc[(qj * 3) * 32 + lane], qy0 = ws.bc[(qj * 3 + 1) * 32 + lane],
-                        qz0 = ws.bc[(qj * 3 + 2) * 32 + lane];
+            const float ax = ws.bc[(a * 3) * kCostSlots + slot], ay = ws.bc[(a * 3 + 1) * kCostSlots + slot],
+                        az = ws.bc[(a * 3 + 2) * kCostSlots + slot];
+            const float qx0 = ws.bc[(qj * 3) * kCostSlots + slot], qy0 = ws.bc[(qj * 3 + 1) * kCostSlots + slot],
+                        qz0 = ws.bc[(qj * 3 + 2) * kCostSlots + slot];
             const float dx = ax - qx0, dy = ay - qy0, dz = az - qz0;
             const float S = fmaxf(fmaxf(fabsf(ax), fmaxf(fabsf(ay), fabsf(az))),
                                   fmaxf(fabsf(qx0), fmaxf(fabsf(qy0), fabsf(qz0))));
             float thr = ba.w + bq.w + smp;
             thr += 4.0f * (S + thr + 1.0f) * PS_GUARD_K;
-            if (kStats) st.v[ST_SELF] += 1;
+            if (kStats && u == 0) st.v[ST_SELF] += 1;
             if (!__any_sync(kCostFull, fmaf(dz, dz, fmaf(dy, dy, dx * dx)) < thr * thr)) continue;
             Affine Ta, Tq;
-            lane_frame(ws.fr, a, lane, Ta);
-            lane_frame(ws.fr, qj, lane, Tq);
+            lane_frame(ws.fr, a, slot, Ta);
+            lane_frame(ws.fr, qj, slot, Tq);
             for (int r = (int)e.y; r < (int)e.z; ++r) {
                 const uint2 run = __ldg(md.sruns + r);
-                const int i = run.x & 0x1ffu, len = (run.x >> 14) & 0x1ffu;
+                const int i = run.x & 0x1ffu, len = (run.x >> 14) & 0x1ffu, j0 = (int)run.y;
                 const float4 si = M.S[i];
                 float pxw, pyw, pzw;
                 sphere_world(Ta, si.x, si.y, si.z, pxw, pyw, pzw);
@@ -390,36 +439,50 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
                                  fmaxf(fabsf(pxw), fmaxf(fabsf(pyw), fabsf(pzw)));
                 float rt = si.w + bq.w + smp;
                 rt += 4.0f * (Sl + rt + 1.0f) * PS_GUARD_K;
-                if (kStats) st.v[ST_SELF] += 1;
+                if (kStats && u == 0) st.v[ST_SELF] += 1;
                 if (!__any_sync(kCostFull, fmaf(ez, ez, fmaf(ey, ey, ex * ex)) < rt * rt)) continue;
-                const int first = (int)run.y;
+                const float ri = si.w;
 #pragma unroll 2
-                for (int u = 0; u < len; ++u) {
-                    const int j = __ldg(md.spairs + first + u);
-                    const float4 sj = M.S[j];
+                for (int m = u; m < len; m += kCostSub) {
+                    const float4 sj = M.S[j0 + m];
                     const float vx = lx - sj.x, vy = ly - sj.y, vz = lz - sj.z;
                     const float d2 = fmaf(vz, vz, fmaf(vy, vy, vx * vx));
-                    const float rs = si.w + sj.w;
+                    const float rs = ri + sj.w;
                     const float t = bv + rs;
+                    if (kStats) st.v[ST_SELF] += 1;
                     if (t > 0.0f && d2 < t * t * (1.0f + 4.0e-6f)) {   // can beat bv: take the root
                         const float c = sqrtf(d2) - rs;
                         if (c < bv) {
                             bv = c;
+                            bk = (r << 9) | m;
                             bi = i;
-                            bj = j;
+                            bj = j0 + m;
                         }
                     }
                 }
-                if (kStats) st.v[ST_SELF] += len;
+            }
+        }
+        // minimum over the group by (value, pair order)
+#pragma unroll
+        for (int o = 1; o < kCostSub; o <<= 1) {
+            const float ov = __shfl_xor_sync(kCostFull, bv, o);
+            const int ok = __shfl_xor_sync(kCostFull, bk, o);
+            const int oi = __shfl_xor_sync(kCostFull, bi, o);
+            const int oj = __shfl_xor_sync(kCostFull, bj, o);
+            if (ov < bv || (ov == bv && ok < bk)) {
+                bv = ov;
+                bk = ok;
+                bi = oi;
+                bj = oj;
             }
         }
         self_h = fmaxf(0.0f, smg - bv);
-        if (kGrad && bi >= 0 && self_h > 0.0f) {
+        if (kGrad && u == 0 && bi >= 0 && self_h > 0.0f) {
             // world positions of the pair: d self_h / d p_i = -(p_i - p_j) / |p_i - p_j|
             const int pi = cb.sph_joint[bi], pj = cb.sph_joint[bj];
             Affine Ti, Tj;
-            lane_frame(ws.fr, pi, lane, Ti);
-            lane_frame(ws.fr, pj, lane, Tj);
+            lane_frame(ws.fr, pi, slot, Ti);
+            lane_frame(ws.fr, pj, slot, Tj);
             const float4 si = M.S[bi], sj = M.S[bj];
             float xi, yi, zi, xj, yj, zj;
             sphere_world(Ti, si.x, si.y, si.z, xi, yi, zi);
@@ -429,29 +492,31 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
             if (dd > 0.0f) {
                 const float s = w / dd;
                 const float gx = -s * dx, gy = -s * dy, gz = -s * dz;   // on p_i; -g on p_j
-                lane_fold(M, ws, lane, pi, gx, gy, gz, yi * gz - zi * gy, zi * gx - xi * gz, xi * gy - yi * gx);
-                lane_fold(M, ws, lane, pj, -gx, -gy, -gz, -(yj * gz - zj * gy), -(zj * gx - xj * gz),
+                lane_fold(M, ws, slot, pi, gx, gy, gz, yi * gz - zi * gy, zi * gx - xi * gz, xi * gy - yi * gx);
+                lane_fold(M, ws, slot, pj, -gx, -gy, -gz, -(yj * gz - zj * gy), -(zj * gx - xj * gz),
                           -(xj * gy - yj * gx));
             }
         }
     }
-    return w * (esdf_part + obb_part + self_h);
+    if (kGrad) __syncwarp();   // the group leaders' folds are visible to lane_write_grad
+    return w * (group_sum(esdf_part) + group_sum(obb_part) + self_h);
 }
 
 // d cost / d q per DoF from the per-joint gradient: a DoF's one joint, or the
-// sum over the joints that share it (DFS order). Writes row[d * stride].
+// sum over the joints that share it (DFS order). The group's lanes write
+// DoFs u, u + kCostSub, ... to row[d * stride].
 __device__ __forceinline__ void lane_write_grad(const ModelSmem& M, const CostBlock& cb, const LaneScratch& ws,
                                                 float* row, int stride) {
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, slot = lane / kCostSub, u = lane % kCostSub;
     const int D = M.H->n_dof, NJ = M.H->n_joints;
-    for (int d = 0; d < D; ++d) {
+    for (int d = u; d < D; d += kCostSub) {
         const int who = cb.dof_joint[d];
         float acc = 0.0f;
         if (who >= 0) {
-            acc = ws.dq[who * 32 + lane];
+            acc = ws.dq[who * kCostSlots + slot];
         } else if (who == -2) {
             for (int p = 1; p < NJ; ++p)
-                if (M.J[p].dof == d && M.J[p].type != PS_FIXED) acc += ws.dq[p * 32 + lane];
+                if (M.J[p].dof == d && M.J[p].type != PS_FIXED) acc += ws.dq[p * kCostSlots + slot];
         }
         row[(size_t)d * stride] = acc;
     }

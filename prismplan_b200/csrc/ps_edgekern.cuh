@@ -166,7 +166,8 @@ __device__ bool process_chunk(const ModelSmem& M, const SceneSmem& sc, const ps_
             const float S = fmaxf(fabsf(mx), fmaxf(fabsf(my), fabsf(mz)));
             float Rc = sqrtf(r2) + jr.bound.w + fmaxf(margin, 0.0f);
             Rc += 4.0f * (S + Rc + sc.Bmax + 1.0f) * PS_GUARD_K;
-            const float Rc2 = Rc * Rc;
+            const float Rcl = Rc * sc.Mscale;   // world radius -> box-frame radius (map stretch)
+        const float Rc2 = Rcl * Rcl;
             int count = 0;
             __syncwarp();   // previous joint's readers of ws.cand are done
             for (int base = 0; base < sc.n_obbs; base += 32) {
@@ -387,7 +388,8 @@ __device__ bool process_chunk_fast(const ModelSmem& M, const SceneSmem& sc, cons
         const float r2c = fmaxf(r2, 1.0e-30f);
         float Rc = r2c * rsqrtf(r2c) * (1.0f + 1.0e-6f) + jr.bound.w + fmaxf(margin, 0.0f);
         Rc += 4.0f * (Sm + Rc + sc.Bmax + 1.0f) * PS_GUARD_K;
-        const float Rc2 = Rc * Rc;
+        const float Rcl = Rc * sc.Mscale;   // world radius -> box-frame radius (map stretch)
+        const float Rc2 = Rcl * Rcl;
         const float Rj = (Rc * (1.0f + 4.0f * PS_GUARD_K) + 4.0f * PS_GUARD_K * (Sm + 1.0f)) * (1.0f + 1.0e-6f);
         int ncand = 0;
         __syncwarp();
@@ -649,7 +651,8 @@ __device__ bool lane_probe_hit(const ModelSmem& M, const SceneSmem& sc, const fl
         const float Sm = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz)));
         float Rc = jr.bound.w + fmaxf(margin, 0.0f);
         Rc += 4.0f * (Sm + Rc + sc.Bmax + 1.0f) * PS_GUARD_K;
-        const float Rc2 = Rc * Rc;
+        const float Rcl = Rc * sc.Mscale;   // world radius -> box-frame radius (map stretch)
+        const float Rc2 = Rcl * Rcl;
         const float Rj = (Rc * (1.0f + 4.0f * PS_GUARD_K) + 4.0f * PS_GUARD_K * (Sm + 1.0f)) * (1.0f + 1.0e-6f);
         int ncand = 0;
         int o = 0;
@@ -805,7 +808,7 @@ int plan_probe(const ps_model* m, const ps_scene_view* sv, int mode, bool stats,
     if ((long long)max_edges < 8ll * 32 * sm_count()) return PS_OK;
     out.k = stats ? edges_probe_kernel<true> : edges_probe_kernel<false>;
     out.smem = probe_smem_bytes(m, sv);
-    PS_TRY_CUDA(cudaFuncSetAttribute(out.k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)out.smem));
+    PS_TRY_CUDA(allow_smem((const void*)out.k, out.smem));
     int per_sm = 0;
     PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, out.k, kProbeThreads, out.smem));
     if (per_sm < 1) return set_error(PS_EINVAL, "edge probe kernel does not fit on an SM with this scene");
@@ -1095,7 +1098,7 @@ int launch_edges_self(const ps_model* m, const ps_edge_params* P, const float* f
     if (!P->check_self || n_edges <= 0) return PS_OK;
     if (int rc = check_self_fits(m)) return rc;
     const size_t smem = self_smem_bytes(m);
-    PS_TRY_CUDA(cudaFuncSetAttribute(edges_self_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PS_TRY_CUDA(allow_smem((const void*)edges_self_kernel, smem));
     int per_sm = 0;
     PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edges_self_kernel, kSelfThreads, smem));
     if (per_sm < 1) return set_error(PS_EINVAL, "self-check kernel does not fit on an SM with this model");

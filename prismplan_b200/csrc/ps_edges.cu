@@ -55,7 +55,7 @@ extern "C" int ps_check_edges_plain(const ps_model* m, const ps_scene_view* scen
     auto kern = pick(fast_path(m, scene, P), g_stats != nullptr, edges_plain_kernel<0, false>,
                      edges_plain_kernel<0, true>, edges_plain_kernel<1, false>, edges_plain_kernel<1, true>,
                      edges_plain_kernel<2, false>, edges_plain_kernel<2, true>);
-    PS_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PS_TRY_CUDA(allow_smem((const void*)kern, smem));
     mark_start(s);
     kern<<<grid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, samples_per_edge, n_edges, valid, cost,
                                           clearance, g_stats);
@@ -110,7 +110,7 @@ int run_persistent(const ps_model* m, const ps_scene_view* scene, const float* f
     auto qk = pick(mode, g_stats != nullptr, edges_queue_kernel<0, false>, edges_queue_kernel<0, true>,
                    edges_queue_kernel<1, false>, edges_queue_kernel<1, true>, edges_queue_kernel<2, false>,
                    edges_queue_kernel<2, true>);
-    PS_TRY_CUDA(cudaFuncSetAttribute(qk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PS_TRY_CUDA(allow_smem((const void*)qk, smem));
     int per_sm = 0;
     PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qk, kEdgeThreads, smem));
     const int qgrid = std::max(1, sm_count() * std::max(per_sm, 1));

@@ -58,6 +58,11 @@ int check_model_device(const ps_model* m);
 // Dynamic shared memory needed to stage model core + scene tables.
 size_t scene_smem_bytes(const ps_scene_view* s);
 
+// Opts `func` into `bytes` of dynamic shared memory on the current device
+// (cudaFuncSetAttribute), remembering the largest amount set per device and
+// kernel so that repeated launches skip the call.
+cudaError_t allow_smem(const void* func, size_t bytes);
+
 // Number of SMs of the current device (cached).
 int sm_count();
 // Largest dynamic shared memory one block may opt into on the current device.

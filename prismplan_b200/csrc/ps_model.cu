@@ -9,6 +9,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -46,6 +48,21 @@ size_t smem_optin() {
         dev_cached = dev;
     }
     return (size_t)bytes;
+}
+
+cudaError_t allow_smem(const void* func, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const auto key = std::make_pair(dev, func);
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = done.find(key);
+    if (it != done.end() && it->second >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) done[key] = bytes;
+    return e;
 }
 
 int sm_count() {
@@ -216,9 +233,10 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
         if (rc) return rc;
     }
 
-    // Self pairs as runs for the cost kernels' prefilter: a run is one sphere
-    // i against the spheres of one joint q, pairs sorted by (i, q, j).
-    // sruns[r] = (i | q << 9 | len << 14, first); spairs[k] = j.
+    // Self pairs as runs for the prefilters of the self check and the cost
+    // kernels: a run is one sphere i against consecutive spheres j0..j0+len-1
+    // of one joint q (pairs sorted by (i, q, j), split where j skips).
+    // sruns[r] = (i | q << 9 | len << 14, j0).
     std::vector<int> sph_pos(std::max(ns, 1), 0);
     for (int p = 0; p < nj; ++p)
         for (int k = sbeg[p]; k < send[p]; ++k) sph_pos[k] = p;
@@ -229,20 +247,20 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
         if (sph_pos[xj] != sph_pos[yj]) return sph_pos[xj] < sph_pos[yj];
         return xj < yj;
     });
+    // A run covers consecutive reordered spheres j0, j0 + 1, ... of one joint.
     struct Run {
         int a, q, i;
         uint32_t w0, w1;
     };
     std::vector<Run> runs;
-    std::vector<uint16_t> spairs(opairs.size());
     for (size_t k = 0; k < opairs.size();) {
         const int i = opairs[k] & 0xffff, q = sph_pos[opairs[k] >> 16];
-        size_t e = k;
-        while (e < opairs.size() && (int)(opairs[e] & 0xffff) == i && sph_pos[opairs[e] >> 16] == q && e - k < 511) {
-            spairs[e] = (uint16_t)(opairs[e] >> 16);
+        const int j0 = (int)(opairs[k] >> 16);
+        size_t e = k + 1;
+        while (e < opairs.size() && (int)(opairs[e] & 0xffff) == i && (int)(opairs[e] >> 16) == j0 + (int)(e - k) &&
+               sph_pos[opairs[e] >> 16] == q && e - k < 511)
             ++e;
-        }
-        runs.push_back({sph_pos[i], q, i, (uint32_t)i | (uint32_t)q << 9 | (uint32_t)(e - k) << 14, (uint32_t)k});
+        runs.push_back({sph_pos[i], q, i, (uint32_t)i | (uint32_t)q << 9 | (uint32_t)(e - k) << 14, (uint32_t)j0});
         k = e;
     }
     if (runs.size() > 65535) return set_error(PS_EINVAL, "too many self-pair runs");
@@ -294,8 +312,6 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
     off += align16(sizeof(uint32_t) * std::max<size_t>(apairs.size(), 1));
     const size_t off_sruns = off;
     off += align16(sizeof(uint32_t) * std::max<size_t>(sruns.size(), 2));
-    const size_t off_spairs = off;
-    off += align16(sizeof(uint16_t) * std::max<size_t>(spairs.size(), 1));
     const size_t off_sjp = off;
     off += align16(sizeof(uint32_t) * std::max<size_t>(sjp.size(), 4));
     const size_t off_lower = off;
@@ -379,7 +395,6 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
     if (!pairs.empty()) std::memcpy(host.data() + off_pairs, pairs.data(), pairs.size() * 4);
     if (!apairs.empty()) std::memcpy(host.data() + off_apairs, apairs.data(), apairs.size() * 4);
     if (!sruns.empty()) std::memcpy(host.data() + off_sruns, sruns.data(), sruns.size() * 4);
-    if (!spairs.empty()) std::memcpy(host.data() + off_spairs, spairs.data(), spairs.size() * 2);
     if (!sjp.empty()) std::memcpy(host.data() + off_sjp, sjp.data(), sjp.size() * 4);
     std::memcpy(host.data() + off_lower, d->joint_lower, sizeof(float) * nd);
     std::memcpy(host.data() + off_upper, d->joint_upper, sizeof(float) * nd);
@@ -402,7 +417,6 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
     m->dev.self_pairs = reinterpret_cast<const uint32_t*>(base + off_pairs);
     m->dev.apx_self_pairs = reinterpret_cast<const uint32_t*>(base + off_apairs);
     m->dev.sruns = reinterpret_cast<const uint2*>(base + off_sruns);
-    m->dev.spairs = reinterpret_cast<const uint16_t*>(base + off_spairs);
     m->dev.n_sruns = (int)(sruns.size() / 2);
     m->dev.sjp = reinterpret_cast<const uint4*>(base + off_sjp);
     m->dev.n_sjp = (int)(sjp.size() / 4);

@@ -25,10 +25,13 @@ __device__ __forceinline__ ObbPrep prep_box(float4 dm, float4 pa, float4 pb) {
 // Builds the prepared box table (compacted enabled boxes, 3x3 maps, exact
 // half extents) and the ESDF layer headers from the caller's
 // SceneCollisionData arrays. Call with all threads; ends with __syncthreads().
+// counters: 4 ints of shared scratch (slot count, stretch bound); bmax_slot:
+// one float.
 __device__ __forceinline__ void stage_scene(const ps_scene_view& sv, ObbPrep* obbs, int* orig, LayerPrep* layers, int* counters,
                             float* bmax_slot, SceneSmem& out) {
     if (threadIdx.x == 0) {
         counters[0] = 0;
+        counters[1] = __float_as_int(1.0f);   // largest map stretch (positive floats order as ints)
         *bmax_slot = 0.0f;
     }
     __syncthreads();
@@ -42,6 +45,7 @@ __device__ __forceinline__ void stage_scene(const ps_scene_view& sv, ObbPrep* ob
         obbs[slot] = p;
         orig[slot] = o;
         atomicMax(reinterpret_cast<int*>(bmax_slot), __float_as_int(B));   // B >= 0: int order == float order
+        atomicMax(&counters[1], __float_as_int(map_stretch(quat_norm_err(p.q.x, p.q.y, p.q.z, p.q.w))));
     }
     for (int l = threadIdx.x; l < sv.n_voxel_layers; l += blockDim.x) {
         LayerPrep L;
@@ -57,6 +61,7 @@ __device__ __forceinline__ void stage_scene(const ps_scene_view& sv, ObbPrep* ob
         L.ny = robust_floor_dev(__fmul_rn(pr.y, inv_vs)) + 1;
         L.nz = robust_floor_dev(__fmul_rn(pr.z, inv_vs)) + 1;
         layers[l] = L;
+        if (L.enabled) atomicMax(&counters[1], __float_as_int(map_stretch(quat_norm_err(pa.w, pb.x, pb.y, pb.z))));
     }
     __syncthreads();
     out.obbs = obbs;
@@ -65,6 +70,7 @@ __device__ __forceinline__ void stage_scene(const ps_scene_view& sv, ObbPrep* ob
     out.n_obbs = counters[0];
     out.n_layers = sv.n_voxel_layers;
     out.Bmax = *bmax_slot;
+    out.Mscale = __int_as_float(counters[1]);
     __syncthreads();
 }
 

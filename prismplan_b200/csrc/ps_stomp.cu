@@ -476,7 +476,7 @@ extern "C" int ps_stomp_optimize(const ps_model* m, const ps_scene_view* scene, 
     const size_t bk_smem = (size_t)(2 * (T + 12) + bk_threads) * sizeof(float);
     auto big = [](auto kernel, size_t bytes) -> int {
         if (bytes > 48 * 1024)
-            PS_TRY_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+            PS_TRY_CUDA(allow_smem((const void*)kernel, bytes));
         return PS_OK;
     };
     if (int rc = big(stomp_rollouts_kernel, ro_smem)) return rc;

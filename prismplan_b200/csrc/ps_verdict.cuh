@@ -60,23 +60,44 @@ __device__ __forceinline__ bool esdf_reachable(const SceneSmem& sc, float cx, fl
         float lx, ly, lz;
         ref_to_local(L.q.x, L.q.y, L.q.z, L.q.w, L.t.x, L.t.y, L.t.z, cx, cy, cz, lx, ly, lz);
         const float S = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))) + fmaxf(fabsf(L.t.x), fmaxf(fabsf(L.t.y), fabsf(L.t.z)));
-        const float slack = 1.0e-4f * (S + R + 1.0f);
-        if (fabsf(lx) <= 0.5f * L.params.x + R + slack && fabsf(ly) <= 0.5f * L.params.y + R + slack &&
-            fabsf(lz) <= 0.5f * L.params.z + R + slack)
+        const float Rl = R * sc.Mscale;   // a world distance R is at most R * Mscale in the layer frame
+        const float slack = 1.0e-4f * (S + Rl + 1.0f);
+        if (fabsf(lx) <= 0.5f * L.params.x + Rl + slack && fabsf(ly) <= 0.5f * L.params.y + Rl + slack &&
+            fabsf(lz) <= 0.5f * L.params.z + Rl + slack)
             return true;
     }
     return false;
 }
 
-// World centre and circumscribed radius of each staged box (local = R p + t,
-// so the centre is -R^T t). Every thread of the block calls it.
+// World centre and circumscribed radius of each staged box: local = M p + t,
+// so the centre is -M^-1 t (M^-1 from its adjugate) and the box's world points
+// lie within |h| |M^-1| of it (quat_norm_err / map_stretch bound |M^-1|; a
+// box outside that bound gets an unbounded radius). Every thread of the block
+// calls it.
 __device__ __forceinline__ void box_spheres(const SceneSmem& sc, float4* obs) {
     for (int o = threadIdx.x; o < sc.n_obbs; o += blockDim.x) {
         const ObbPrep& b = sc.obbs[o];
-        const float cx = -(b.r0.x * b.r0.w + b.r1.x * b.r1.w + b.r2.x * b.r2.w);
-        const float cy = -(b.r0.y * b.r0.w + b.r1.y * b.r1.w + b.r2.y * b.r2.w);
-        const float cz = -(b.r0.z * b.r0.w + b.r1.z * b.r1.w + b.r2.z * b.r2.w);
-        obs[o] = make_float4(cx, cy, cz, sqrtf(b.h.x * b.h.x + b.h.y * b.h.y + b.h.z * b.h.z));
+        const float e = quat_norm_err(b.q.x, b.q.y, b.q.z, b.q.w);
+        const float lo = 1.0f - 4.0f * e * (1.0f + e);
+        // adjugate columns: M^-1 = [r1 x r2, r2 x r0, r0 x r1] / det
+        const float ax = b.r1.y * b.r2.z - b.r1.z * b.r2.y, ay = b.r1.z * b.r2.x - b.r1.x * b.r2.z,
+                    az = b.r1.x * b.r2.y - b.r1.y * b.r2.x;
+        const float bx = b.r2.y * b.r0.z - b.r2.z * b.r0.y, by = b.r2.z * b.r0.x - b.r2.x * b.r0.z,
+                    bz = b.r2.x * b.r0.y - b.r2.y * b.r0.x;
+        const float cx2 = b.r0.y * b.r1.z - b.r0.z * b.r1.y, cy2 = b.r0.z * b.r1.x - b.r0.x * b.r1.z,
+                    cz2 = b.r0.x * b.r1.y - b.r0.y * b.r1.x;
+        const float det = b.r0.x * ax + b.r0.y * ay + b.r0.z * az;
+        float4 out;
+        if (lo >= 0.25f && fabsf(det) > 0.25f) {
+            const float inv = 1.0f / det;
+            out.x = -(b.r0.w * ax + b.r1.w * bx + b.r2.w * cx2) * inv;
+            out.y = -(b.r0.w * ay + b.r1.w * by + b.r2.w * cy2) * inv;
+            out.z = -(b.r0.w * az + b.r1.w * bz + b.r2.w * cz2) * inv;
+            out.w = sqrtf(b.h.x * b.h.x + b.h.y * b.h.y + b.h.z * b.h.z) * rsqrtf(lo) * (1.0f + 1.0e-5f);
+        } else {
+            out = make_float4(0.0f, 0.0f, 0.0f, 1.0e30f);   // never culled by the prefilter
+        }
+        obs[o] = out;
     }
 }
 
@@ -398,7 +419,7 @@ __device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const floa
         st.v[ST_SELF] += 1;
         if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) >= lim * lim * (1.0f + 1.0e-6f)) continue;   // no pair can hit
         for (int k = 0; k < len; ++k) {
-            const int j = __ldg(md.spairs + run.y + k);
+            const int j = (int)run.y + k;
             st.v[ST_SELF] += 1;
             if (ref_self_hit(px, py, pz, ri, at(pos, j, 0), at(pos, j, 1), at(pos, j, 2), M.S[j].w)) return true;
         }

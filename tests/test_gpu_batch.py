@@ -217,3 +217,35 @@ def test_batch_edge_cases(w5):
     batch.close()
     with pytest.raises(RuntimeError):
         batch.launch(sc, ep, cp)
+
+
+@pytest.mark.parametrize("broadcast", [False, True])
+def test_batch_rollouts_equal_rollout_costs(w5, broadcast):
+    """STOMP rollout requests (reference layout [R, D, T]) share the launch
+    with edge and trajectory requests; their state costs equal
+    ps_rollout_costs bit for bit, and the other requests are unchanged."""
+    wl, b, sc = w5
+    rng = np.random.default_rng(55)
+    trajs = wl["trajectories"][:3]
+    rolls = []
+    for q in trajs[:2]:   # noisy copies of a trajectory, reference layout
+        r = q[None].transpose(0, 2, 1) + rng.normal(0.0, 0.05, (9,) + q.T.shape).astype(np.float32)
+        rolls.append(torch.from_numpy(np.ascontiguousarray(r, np.float32)).cuda())
+    nw = sum(len(q) for q in trajs) + sum(r.shape[0] * r.shape[2] for r in rolls)
+    n_req = 4
+    n_e = sum(wl["edge_splits"][:n_req])
+    batch = api.MixedBatch(b, n_req, n_e, 3 + len(rolls), nw, 128)
+    r_out = [batch.add_rollouts(rolls[0], broadcast_d=broadcast)]
+    frm, to, reqs, tr = _fill(batch, wl, n_req=n_req, n_traj=3)
+    r_out.append(batch.add_rollouts(rolls[1], broadcast_d=broadcast))
+    ep = api.EdgeEvalParams(max_joint_step=0.01, max_samples=600)
+    cp = _cost_params(wl, 1.0)
+    batch.launch(sc, ep, cp)
+    torch.cuda.synchronize()
+    for r, out in zip(rolls, r_out):
+        ref = api.rollout_costs(b, sc, r, cp, broadcast_d=broadcast)
+        assert out.shape == ref.shape
+        assert torch.equal(out.view(torch.int32), ref.view(torch.int32))
+    assert float(r_out[0].max()) > 0.0
+    _check_against_calls(b, sc, frm, to, reqs, tr, ep, cp)
+    batch.close()
