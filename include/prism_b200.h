@@ -175,6 +175,9 @@ typedef struct ps_scene_view {
 #define PS_CLEARANCE_OBB    0x02u  /* clearance includes sphere-OBB SDF         */
 #define PS_CLEARANCE_ESDF   0x04u  /* clearance includes ESDF (reference a13)   */
 #define PS_NO_GATE          0x08u  /* skip the approximate gate (diagnostics)   */
+/* Grid of the configuration kernel: k blocks per SM (1..15) in bits 8..11 of
+   flags; 0 = 8. ps_tune_configs picks it. */
+#define PS_CONFIG_BLOCKS_PER_SM(k) (((unsigned)(k) & 15u) << 8)
 
 /* q: device [n*n_dof] row-major. hit: device [n] (1 = in collision).
    clearance: device [n] or NULL; min over spheres (radius + margin) of the
@@ -183,6 +186,21 @@ int ps_check_configs(const ps_model* model, const ps_scene_view* scene,
                      const float* q, int n, float collision_margin,
                      unsigned flags, uint8_t* hit, float* clearance,
                      void* stream);
+
+/* Autotuner of ps_check_configs' grid: times every blocks-per-SM choice on
+   the caller's configurations (same margin, flags and outputs) and returns
+   the fastest in *out and as *tuned_flags (flags with
+   PS_CONFIG_BLOCKS_PER_SM set). Synchronous. No reference counterpart. */
+typedef struct ps_config_tuning {
+    int   blocks_per_sm;    /* the fastest grid                               */
+    float best_ms;          /* median time of one call with it               */
+    float default_ms;       /* same with the default grid                    */
+    int   candidates;       /* grids timed                                   */
+} ps_config_tuning;
+int ps_tune_configs(const ps_model* model, const ps_scene_view* scene,
+                    const float* q, int n, float collision_margin,
+                    unsigned flags, uint8_t* hit, float* clearance,
+                    void* stream, ps_config_tuning* out, unsigned* tuned_flags);
 
 /* =========================================================================
  * Edge checks. Replaces ppln::search::evaluate_edges_batch and
@@ -212,6 +230,15 @@ typedef struct ps_edge_params {
                                planners' own device deadline is the model
                                (pRRTC.cu:1595-1602). 0: no limit. The plain
                                path ignores it. No reference field.          */
+    /* Launch shape of the persistent paths; 0 = automatic, and
+       ps_tune_edges picks them. No reference fields. */
+    int   probe;            /* end-sample probe: 0 automatic (on with at least
+                               8 warps of edges per SM, boxes-only scenes),
+                               1 on (boxes-only scenes), 2 off              */
+    int   queue_blocks_per_sm; /* resident queue blocks per SM: 0 = all that
+                               fit, k > 0 = at most k                       */
+    int   grab;             /* queue items a warp takes per grab: 0 =
+                               automatic (up to 32), 1..32 fixed            */
 } ps_edge_params;
 
 /* Plain per-call path: one warp per edge, samples in order, early exit at the
@@ -264,6 +291,28 @@ int ps_check_edges_static(const ps_model* model, const ps_scene_view* scene,
                           const ps_edge_params* params,
                           uint8_t* valid, float* cost, float* clearance,
                           void* stream);
+
+/* Autotuner of the persistent edge path (ps_check_edges). Times every
+   candidate launch shape -- probe on and off, queue residency from all that
+   fit down by two blocks per SM, grab sizes automatic / 8 / 32 -- on the
+   caller's edges and writes the fastest to *tuned (a copy of *params with
+   probe, queue_blocks_per_sm and grab set; pass it to later calls on edges of
+   that kind and count) and to *out. Verdicts and costs do not depend on the
+   shape. Synchronous; runs ps_check_edges several times on `stream` with the
+   caller's buffers. No reference counterpart. */
+typedef struct ps_edge_tuning {
+    int   probe, queue_blocks_per_sm, grab;   /* the fastest shape            */
+    float best_ms;          /* median time of one call with it               */
+    float default_ms;       /* same with every shape field 0                 */
+    int   candidates;       /* shapes timed                                  */
+} ps_edge_tuning;
+int ps_tune_edges(const ps_model* model, const ps_scene_view* scene,
+                  const float* from, const float* to,
+                  const int* samples_per_edge, int n_edges,
+                  const ps_edge_params* params,
+                  uint8_t* valid, float* cost, float* clearance,
+                  void* workspace, size_t workspace_bytes, void* stream,
+                  ps_edge_tuning* out, ps_edge_params* tuned);
 
 /* Status of the last persistent call that used `workspace` (NULL: the
    built-in workspace of the current device): PS_OK, or PS_ETIMEOUT when its

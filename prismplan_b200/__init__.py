@@ -6,7 +6,8 @@ Drop-in surface (names of the reference ``prrtc`` module and substrate):
 ``build_robot_model``; device-resident torch ops ``check_configs``,
 ``check_edges``, ``traj_cost``, ``rollout_costs``, ``hinge_cost``; the
 batched optimisers ``chomp_solve`` / ``chomp_optimize`` and
-``stomp_solve`` / ``stomp_optimize``.
+``stomp_solve`` / ``stomp_optimize``; the mixed-request batch
+``MixedBatch``; the launch-shape tuners ``tune_edges`` / ``tune_configs``.
 The compute path is the CUDA library ``libprism_b200.so``; importing this
 package does not load it (so CPU-only tooling works), the first call does and
 fails loudly if it is missing.
@@ -35,6 +36,8 @@ from .api import (  # noqa: F401
     stomp_solve,
     stomp_workspace,
     traj_cost,
+    tune_configs,
+    tune_edges,
 )
 from .robot import RobotModelBuilder, build_robot_model, load_robot_asset  # noqa: F401
 from .scene import PlanningScene, SceneCollisionDataBuilder, SceneTensors  # noqa: F401

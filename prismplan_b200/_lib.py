@@ -21,6 +21,11 @@ PS_CLEARANCE_OBB = 0x02
 PS_CLEARANCE_ESDF = 0x04
 PS_NO_GATE = 0x08
 
+
+def PS_CONFIG_BLOCKS_PER_SM(k):
+    return (int(k) & 15) << 8
+
+
 PS_ESDF_NEAREST = 0
 PS_ESDF_TRILINEAR = 1
 PS_LAYOUT_BTD = 0
@@ -102,6 +107,20 @@ class EdgeParams(C.Structure):
         ("max_joint_step", C.c_float), ("max_samples", C.c_int),
         ("collision_margin", C.c_float), ("check_self", C.c_int),
         ("compute_clearance", C.c_int), ("time_budget_ms", C.c_float),
+        ("probe", C.c_int), ("queue_blocks_per_sm", C.c_int), ("grab", C.c_int),
+    ]
+
+
+class EdgeTuning(C.Structure):
+    _fields_ = [
+        ("probe", C.c_int), ("queue_blocks_per_sm", C.c_int), ("grab", C.c_int),
+        ("best_ms", C.c_float), ("default_ms", C.c_float), ("candidates", C.c_int),
+    ]
+
+
+class ConfigTuning(C.Structure):
+    _fields_ = [
+        ("blocks_per_sm", C.c_int), ("best_ms", C.c_float), ("default_ms", C.c_float), ("candidates", C.c_int),
     ]
 
 
@@ -172,6 +191,11 @@ _SIGNATURES = [
     ("ps_model_get_info", C.c_int, [C.c_void_p, C.POINTER(ModelInfo)]),
     ("ps_model_poll_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     ("ps_model_set_wait_limit", C.c_int, [C.c_void_p, C.c_int]),
+    ("ps_tune_edges", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                                C.c_void_p, C.c_void_p]),
+    ("ps_tune_configs", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_uint, C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("ps_debug_obb_pairs", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                      C.c_void_p]),
     ("ps_check_configs", C.c_int,

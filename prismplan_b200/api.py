@@ -65,18 +65,7 @@ def _model(robot: RobotModelBuilder) -> C.c_void_p:
 # ---------------------------------------------------------------------------
 # configurations
 # ---------------------------------------------------------------------------
-def check_configs(robot: RobotModelBuilder, scene, q, collision_margin: float = 0.0,
-                  clearance: Optional[str] = None, check_self: bool = False,
-                  no_gate: bool = False, stream=None):
-    """Two-phase any-collision for every row of ``q`` [N, n_dof] (CUDA).
-
-    ``clearance``: None, "obb", "esdf" or "both" -- min over spheres of the
-    selected signed clearance (radius + margin), 1000.0 when nothing applies.
-    Returns (hit uint8 [N], clearance float32 [N] or None)."""
-    torch = _torch()
-    q = _dev_f32(q, robot.n_dof)
-    n = q.shape[0]
-    hit = torch.empty(n, dtype=torch.uint8, device=q.device)
+def _config_flags(clearance, check_self, no_gate, blocks_per_sm=0):
     flags = 0
     if clearance in ("obb", "both"):
         flags |= _lib.PS_CLEARANCE_OBB
@@ -86,6 +75,23 @@ def check_configs(robot: RobotModelBuilder, scene, q, collision_margin: float = 
         flags |= _lib.PS_CHECK_SELF
     if no_gate:
         flags |= _lib.PS_NO_GATE
+    return flags | _lib.PS_CONFIG_BLOCKS_PER_SM(blocks_per_sm)
+
+
+def check_configs(robot: RobotModelBuilder, scene, q, collision_margin: float = 0.0,
+                  clearance: Optional[str] = None, check_self: bool = False,
+                  no_gate: bool = False, stream=None, blocks_per_sm: int = 0):
+    """Two-phase any-collision for every row of ``q`` [N, n_dof] (CUDA).
+
+    ``clearance``: None, "obb", "esdf" or "both" -- min over spheres of the
+    selected signed clearance (radius + margin), 1000.0 when nothing applies.
+    ``blocks_per_sm``: grid of the kernel (0 = default; tune_configs picks
+    it). Returns (hit uint8 [N], clearance float32 [N] or None)."""
+    torch = _torch()
+    q = _dev_f32(q, robot.n_dof)
+    n = q.shape[0]
+    hit = torch.empty(n, dtype=torch.uint8, device=q.device)
+    flags = _config_flags(clearance, check_self, no_gate, blocks_per_sm)
     clr = torch.empty(n, dtype=torch.float32, device=q.device) if clearance else None
     v = _view(scene)
     _lib.check(_lib.load().ps_check_configs(
@@ -138,6 +144,10 @@ class EdgeEvalParams:
     max_joint_step: float = 0.0
     max_samples: int = 1024
     time_budget_ms: float = 0.0   # persistent paths: stop after this much device time (0 = none)
+    # launch shape of the persistent paths (0 = automatic; tune_edges picks them)
+    probe: int = 0                # 0 automatic, 1 on, 2 off
+    queue_blocks_per_sm: int = 0  # 0 = all that fit
+    grab: int = 0                 # queue items per grab, 0 = automatic
 
     def to_c(self) -> _lib.EdgeParams:
         if self.enable_mesh:
@@ -151,6 +161,9 @@ class EdgeEvalParams:
         p.check_self = int(bool(self.check_self))
         p.compute_clearance = int(bool(self.compute_clearance))
         p.time_budget_ms = float(self.time_budget_ms)
+        p.probe = int(self.probe)
+        p.queue_blocks_per_sm = int(self.queue_blocks_per_sm)
+        p.grab = int(self.grab)
         return p
 
 
@@ -208,6 +221,58 @@ def check_edges(robot: RobotModelBuilder, scene, frm, to, samples=None,
                                             C.byref(p), valid.data_ptr(), cost.data_ptr(), clr.data_ptr(),
                                             _stream(stream)))
     return valid, cost, clr
+
+
+def tune_edges(robot: RobotModelBuilder, scene, frm, to, samples=None, params: Optional[EdgeEvalParams] = None,
+               stream=None):
+    """Autotune the persistent edge path's launch shape (ps_tune_edges) on
+    these edges. Returns (params with probe / queue_blocks_per_sm / grab set,
+    {"probe", "queue_blocks_per_sm", "grab", "best_ms", "default_ms",
+    "candidates"})."""
+    import copy
+
+    torch = _torch()
+    params = params or EdgeEvalParams()
+    frm = _dev_f32(frm, robot.n_dof)
+    to = _dev_f32(to, robot.n_dof)
+    E = frm.shape[0]
+    if samples is not None:
+        samples = torch.as_tensor(samples).to(device=frm.device, dtype=torch.int32).contiguous()
+    valid = torch.empty(E, dtype=torch.uint8, device=frm.device)
+    cost = torch.empty(E, dtype=torch.float32, device=frm.device)
+    clr = torch.empty(E, dtype=torch.float32, device=frm.device)
+    ws = edges_workspace(E, frm.device)
+    p = params.to_c()
+    tuned = _lib.EdgeParams()
+    info = _lib.EdgeTuning()
+    v = _view(scene)
+    _lib.check(_lib.load().ps_tune_edges(_model(robot), C.byref(v), frm.data_ptr(), to.data_ptr(),
+                                         samples.data_ptr() if samples is not None else None, E, C.byref(p),
+                                         valid.data_ptr(), cost.data_ptr(), clr.data_ptr(), ws.data_ptr(),
+                                         ws.numel(), _stream(stream), C.byref(info), C.byref(tuned)))
+    out = copy.copy(params)
+    out.probe, out.queue_blocks_per_sm, out.grab = tuned.probe, tuned.queue_blocks_per_sm, tuned.grab
+    return out, {name: getattr(info, name) for name, _ in info._fields_}
+
+
+def tune_configs(robot: RobotModelBuilder, scene, q, collision_margin: float = 0.0, clearance: Optional[str] = None,
+                 check_self: bool = False, stream=None):
+    """Autotune the configuration kernel's grid (ps_tune_configs). Returns
+    (blocks_per_sm to pass to check_configs, {"blocks_per_sm", "best_ms",
+    "default_ms", "candidates"})."""
+    torch = _torch()
+    q = _dev_f32(q, robot.n_dof)
+    n = q.shape[0]
+    flags = _config_flags(clearance, check_self, False)
+    hit = torch.empty(n, dtype=torch.uint8, device=q.device)
+    clr = torch.empty(n, dtype=torch.float32, device=q.device) if clearance else None
+    info = _lib.ConfigTuning()
+    tuned = C.c_uint(0)
+    v = _view(scene)
+    _lib.check(_lib.load().ps_tune_configs(_model(robot), C.byref(v), q.data_ptr(), n, float(collision_margin), flags,
+                                           hit.data_ptr(), clr.data_ptr() if clr is not None else None,
+                                           _stream(stream), C.byref(info), C.byref(tuned)))
+    return info.blocks_per_sm, {name: getattr(info, name) for name, _ in info._fields_}
 
 
 class EdgeEvalGpu:

@@ -295,7 +295,7 @@ int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, 
         PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L.qk, kEdgeThreads, L.qsmem));
         if (per_sm < 1) return set_error(PS_EINVAL, "edge kernel does not fit on an SM with this scene");
         L.qgrid = std::max(1, (int)(b->edge_share * sms * per_sm + 0.5f));
-        if (int rc = plan_probe(m, sv, L.mode, false, b->edge_share, b->lim.max_edges, L.probe)) return rc;
+        if (int rc = plan_probe(m, sv, L.mode, false, b->edge_share, b->lim.max_edges, ep->probe, L.probe)) return rc;
         L.pgrid = std::max(1, std::min((b->lim.max_edges + 255) / 256, sms * 4));
         L.req_grid_e = std::max(1, std::min(b->lim.max_edge_requests, sms * 8));
         if (ep->check_self) {

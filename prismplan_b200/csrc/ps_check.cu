@@ -430,7 +430,8 @@ extern "C" int ps_check_configs(const ps_model* m, const ps_scene_view* scene, c
     const bool clr = clearance != nullptr && (flags & (PS_CLEARANCE_OBB | PS_CLEARANCE_ESDF));
     size_t smem = (size_t)m->dev.bytes_core + scene_smem_bytes(scene) + (size_t)kCfgThreads * m->info.n_dof * 4;
     const int blocks_needed = (n + kCfgThreads - 1) / kCfgThreads;
-    const int grid = std::max(1, std::min(blocks_needed, sm_count() * 8));
+    const int per_sm = (flags >> 8) & 15u ? (int)((flags >> 8) & 15u) : 8;   // PS_CONFIG_BLOCKS_PER_SM
+    const int grid = std::max(1, std::min(blocks_needed, sm_count() * per_sm));
     // (sphere_obb_acm_mask_approx changes no result: see the approximate gate)
     const bool fast = m->root_slot_only && m->info.approx_shares_chain && !scene->sphere_obb_acm_mask &&
                       !scene->sphere_acm_mask;
@@ -510,5 +511,50 @@ extern "C" int ps_probe_fp32_peak(double* flops_per_s, void* stream) {
     if (e != cudaSuccess) return cuda_error(e, "fma probe");
     const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
     *flops_per_s = flops / (ms * 1e-3);
+    return PS_OK;
+}
+
+extern "C" int ps_tune_configs(const ps_model* m, const ps_scene_view* scene, const float* q, int n, float margin,
+                               unsigned flags, uint8_t* hit, float* clearance, void* stream, ps_config_tuning* out,
+                               unsigned* tuned_flags) {
+    PS_NVTX("ps_tune_configs");
+    clear_error();
+    if (!tuned_flags) return set_error(PS_EINVAL, "tuned_flags is NULL");
+    cudaStream_t s = (cudaStream_t)stream;
+    const unsigned base = flags & ~(15u << 8);
+    cudaEvent_t a = nullptr, z = nullptr;
+    PS_TRY_CUDA(cudaEventCreate(&a));
+    if (cudaEventCreate(&z) != cudaSuccess) {
+        cudaEventDestroy(a);
+        return cuda_error(cudaGetLastError(), "tuning events");
+    }
+    float best = 3.0e38f, def_ms = 0.0f;
+    int best_k = 8, n_cand = 0, rc = PS_OK;
+    for (int k : {8, 1, 2, 3, 4, 6, 12}) {
+        const unsigned f = base | PS_CONFIG_BLOCKS_PER_SM(k);
+        rc = ps_check_configs(m, scene, q, n, margin, f, hit, clearance, stream);   // warm-up
+        float ms[3];
+        for (int r = 0; r < 3 && rc == PS_OK; ++r) {
+            cudaEventRecord(a, s);
+            rc = ps_check_configs(m, scene, q, n, margin, f, hit, clearance, stream);
+            cudaEventRecord(z, s);
+            if (rc == PS_OK && cudaEventSynchronize(z) != cudaSuccess) rc = cuda_error(cudaGetLastError(), "tuning run");
+            ms[r] = 0.0f;
+            cudaEventElapsedTime(&ms[r], a, z);
+        }
+        if (rc) break;
+        std::sort(ms, ms + 3);
+        ++n_cand;
+        if (k == 8) def_ms = ms[1];
+        if (ms[1] < best) {
+            best = ms[1];
+            best_k = k;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(z);
+    if (rc) return rc;
+    *tuned_flags = base | PS_CONFIG_BLOCKS_PER_SM(best_k);
+    if (out) *out = ps_config_tuning{best_k, best, def_ms, n_cand};
     return PS_OK;
 }

@@ -799,13 +799,13 @@ struct ProbePlan {
 };
 
 int plan_probe(const ps_model* m, const ps_scene_view* sv, int mode, bool stats, float share, int max_edges,
-               ProbePlan& out) {
+               int choice, ProbePlan& out) {
     out = ProbePlan{};
-    if (mode != 1 || max_edges <= 0 || sv->n_obbs == 0) return PS_OK;
+    if (mode != 1 || max_edges <= 0 || sv->n_obbs == 0 || choice == 2) return PS_OK;
     // One thread per edge: below 8 warps per SM the probe runs latency-bound
     // and costs more than it retires (measured: the 16 K segment edges of a
-    // 256-request CHOMP iteration ran 3 % slower with it).
-    if ((long long)max_edges < 8ll * 32 * sm_count()) return PS_OK;
+    // 256-request CHOMP iteration ran 3 % slower with it). choice 1 forces it.
+    if (choice != 1 && (long long)max_edges < 8ll * 32 * sm_count()) return PS_OK;
     out.k = stats ? edges_probe_kernel<true> : edges_probe_kernel<false>;
     out.smem = probe_smem_bytes(m, sv);
     PS_TRY_CUDA(allow_smem((const void*)out.k, out.smem));
@@ -868,7 +868,8 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode == 1 ? 5 : (kMode ? 6 : 3)
     const unsigned long long deadline = *((volatile unsigned long long*)&hdr->deadline);
     // Items per grab: up to 32, fewer when the pass has few items, so that
     // every resident warp gets a share.
-    const int grab = (int)max(1ll, min(32ll, total / ((long long)gridDim.x * kWarps * 2)));
+    const int grab = P.grab > 0 ? min(P.grab, 32)
+                                : (int)max(1ll, min(32ll, total / ((long long)gridDim.x * kWarps * 2)));
     volatile int* vbad = bad;
     for (;;) {
         unsigned long long base = 0;

@@ -21,6 +21,7 @@
 #include <cfloat>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "ps_edgekern.cuh"
 
@@ -36,6 +37,8 @@ int check_edge_args(const ps_model* m, const ps_scene_view* scene, const float* 
     if (n > 0 && (!from || !to || !valid || !cost)) return set_error(PS_EINVAL, "from/to/valid/cost NULL");
     if (P->max_samples > 0 && P->max_samples > (1 << 20))
         return set_error(PS_EINVAL, "max_samples above 2^20");
+    if (P->probe < 0 || P->probe > 2 || P->queue_blocks_per_sm < 0 || P->grab < 0 || P->grab > 32)
+        return set_error(PS_EINVAL, "probe must be 0..2, queue_blocks_per_sm >= 0, grab 0..32");
     return validate_scene(m, scene);
 }
 
@@ -113,9 +116,11 @@ int run_persistent(const ps_model* m, const ps_scene_view* scene, const float* f
     PS_TRY_CUDA(allow_smem((const void*)qk, smem));
     int per_sm = 0;
     PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qk, kEdgeThreads, smem));
-    const int qgrid = std::max(1, sm_count() * std::max(per_sm, 1));
+    per_sm = std::max(per_sm, 1);
+    if (P->queue_blocks_per_sm > 0) per_sm = std::min(per_sm, P->queue_blocks_per_sm);
+    const int qgrid = std::max(1, sm_count() * per_sm);
     ProbePlan probe;
-    if (int rc = plan_probe(m, scene, mode, g_stats != nullptr, 1.0f, n_edges, probe)) return rc;
+    if (int rc = plan_probe(m, scene, mode, g_stats != nullptr, 1.0f, n_edges, P->probe, probe)) return rc;
     mark_start(s);
     if (probe.k)
         probe.k<<<probe.grid, kProbeThreads, probe.smem, s>>>(m->dev, *scene, *P, from, to, n_edges, b.hdr, b.G,
@@ -227,5 +232,97 @@ extern "C" int ps_edges_status(const void* workspace, int* status) {
     EdgeWs h;
     PS_TRY_CUDA(cudaMemcpy(&h, ws, sizeof(EdgeWs), cudaMemcpyDeviceToHost));
     *status = h.timed_out ? PS_ETIMEOUT : PS_OK;
+    return PS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner of the persistent path's launch shape.
+// ---------------------------------------------------------------------------
+namespace {
+
+// Median time (ms) of `reps` calls of fn on stream s, after one untimed call.
+template <class F>
+int time_calls(F fn, cudaStream_t s, int reps, float& ms_out) {
+    cudaEvent_t a = nullptr, z = nullptr;
+    PS_TRY_CUDA(cudaEventCreate(&a));
+    if (cudaEventCreate(&z) != cudaSuccess) {
+        cudaEventDestroy(a);
+        return cuda_error(cudaGetLastError(), "tuning events");
+    }
+    int rc = fn();
+    std::vector<float> ms;
+    for (int r = 0; r < reps && rc == PS_OK; ++r) {
+        cudaEventRecord(a, s);
+        rc = fn();
+        cudaEventRecord(z, s);
+        if (rc == PS_OK && cudaEventSynchronize(z) != cudaSuccess) rc = cuda_error(cudaGetLastError(), "tuning run");
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, a, z);
+        ms.push_back(t);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(z);
+    if (rc) return rc;
+    std::sort(ms.begin(), ms.end());
+    ms_out = ms[ms.size() / 2];
+    return PS_OK;
+}
+
+}  // namespace
+
+extern "C" int ps_tune_edges(const ps_model* m, const ps_scene_view* scene, const float* from, const float* to,
+                             const int* samples_per_edge, int n_edges, const ps_edge_params* P, uint8_t* valid,
+                             float* cost, float* clearance, void* workspace, size_t workspace_bytes, void* stream,
+                             ps_edge_tuning* out, ps_edge_params* tuned) {
+    PS_NVTX("ps_tune_edges");
+    clear_error();
+    if (!P || !tuned) return set_error(PS_EINVAL, "params / tuned is NULL");
+    if (int rc = check_edge_args(m, scene, from, to, n_edges, P, valid, cost)) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    ps_edge_params p = *P;
+    auto run = [&]() {
+        return ps_check_edges(m, scene, from, to, samples_per_edge, n_edges, &p, valid, cost, clearance, workspace,
+                              workspace_bytes, stream);
+    };
+    p.probe = p.queue_blocks_per_sm = p.grab = 0;
+    float def_ms = 0.0f;
+    if (int rc = time_calls(run, s, 5, def_ms)) return rc;
+    // candidates: probe on/off (on only where the probe exists), the queue's
+    // residency from all that fit down by two, three grab sizes
+    const int mode = fast_path(m, scene, P);
+    int per_sm = 0;
+    {
+        const size_t smem = edge_smem_bytes(m, scene);
+        auto qk = pick(mode, false, edges_queue_kernel<0, false>, edges_queue_kernel<0, true>,
+                       edges_queue_kernel<1, false>, edges_queue_kernel<1, true>, edges_queue_kernel<2, false>,
+                       edges_queue_kernel<2, true>);
+        PS_TRY_CUDA(allow_smem((const void*)qk, smem));
+        PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qk, kEdgeThreads, smem));
+        per_sm = std::max(per_sm, 1);
+    }
+    std::vector<int> probes = {2};
+    if (mode == 1 && scene->n_obbs > 0) probes.push_back(1);
+    float best = def_ms;
+    ps_edge_params best_p = p;
+    int n_cand = 1;
+    for (int pr : probes)
+        for (int q = per_sm; q >= std::max(1, per_sm - 2); --q)
+            for (int g : {0, 8, 32}) {
+                p.probe = pr;
+                p.queue_blocks_per_sm = q;
+                p.grab = g;
+                float ms = 0.0f;
+                if (int rc = time_calls(run, s, 3, ms)) return rc;
+                ++n_cand;
+                if (ms < best) {
+                    best = ms;
+                    best_p = p;
+                }
+            }
+    *tuned = *P;
+    tuned->probe = best_p.probe;
+    tuned->queue_blocks_per_sm = best_p.queue_blocks_per_sm;
+    tuned->grab = best_p.grab;
+    if (out) *out = ps_edge_tuning{best_p.probe, best_p.queue_blocks_per_sm, best_p.grab, best, def_ms, n_cand};
     return PS_OK;
 }

@@ -2,7 +2,8 @@
 
 Run in a container that has the read-only reference checkout:
 
-    python tests/golden/make_golden.py [/root/reference]
+    python tests/golden/make_golden.py <reference root>
+    (or PRISMPLAN_REF=<reference root> python tests/golden/make_golden.py)
 
 It imports, from the reference (paths inside code/gpu_planning/):
   * python/gpu_planning/substrate/robot_model_loader.py  -- load_robot_asset
@@ -34,7 +35,7 @@ def _import_file(name: str, path: Path):
     return mod
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str) -> None:
     gp = Path(ref_root) / "code" / "gpu_planning"
     sys.path.insert(0, str(gp / "python"))
     from gpu_planning.substrate import planning_scene as ps_mod  # noqa: E402
@@ -89,4 +90,9 @@ def main(ref_root: str = "/root/reference") -> None:
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    import os
+
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PRISMPLAN_REF")
+    if not root:
+        sys.exit("usage: make_golden.py <reference root> (or set PRISMPLAN_REF)")
+    main(root)

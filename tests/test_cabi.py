@@ -45,7 +45,7 @@ STRUCTS = {   # ctypes mirror -> C struct of include/prism_b200.h
     "ModelDesc": "ps_model_desc", "ModelInfo": "ps_model_info", "SceneView": "ps_scene_view",
     "EdgeParams": "ps_edge_params", "CostParams": "ps_cost_params", "BatchLimits": "ps_batch_limits",
     "BatchTuning": "ps_batch_tuning", "ChompParams": "ps_chomp_params", "StompParams": "ps_stomp_params",
-    "StompLayout": "ps_stomp_layout",
+    "StompLayout": "ps_stomp_layout", "EdgeTuning": "ps_edge_tuning", "ConfigTuning": "ps_config_tuning",
 }
 
 
