@@ -28,10 +28,11 @@
 //      (prismatic), a_p and o_p the joint axis and origin from the frames;
 //   5. self hinge: joint pairs whose bound spheres can come within m_self (on
 //      any waypoint of the warp) expand their runs (sphere i of joint a against
-//      consecutive spheres j of joint q), a run whose bound test fails
-//      everywhere is skipped; sphere i is mapped into q's link frame once per
-//      run, so a pair costs one difference against a link-frame centre, split
-//      over the group's lanes. Only pairs within r_i + r_j + m_self can set the
+//      consecutive spheres j of joint q). The group's lanes split the runs; a
+//      lane maps its run's sphere i into q's link frame with the joint pair's
+//      relative transform T_q^-1 T_a, skips the run if i is out of reach of
+//      q's bound sphere, and otherwise costs one difference per pair against
+//      the link-frame centres. Only pairs within r_i + r_j + m_self can set the
 //      hinge, and a square root is taken only for those; the minimum over the
 //      group is taken by (value, pair order), and the argmin pair's force goes
 //      to both joints' ancestors.
@@ -420,36 +421,42 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
             thr += 4.0f * (S + thr + 1.0f) * PS_GUARD_K;
             if (kStats && u == 0) st.v[ST_SELF] += 1;
             if (!__any_sync(kCostFull, fmaf(dz, dz, fmaf(dy, dy, dx * dx)) < thr * thr)) continue;
-            Affine Ta, Tq;
+            // relative transform T_q^-1 T_a: sphere i of joint a straight into q's link frame
+            Affine Ta, Tq, Tqa;
             lane_frame(ws.fr, a, slot, Ta);
             lane_frame(ws.fr, qj, slot, Tq);
-            for (int r = (int)e.y; r < (int)e.z; ++r) {
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    Tqa.m[r * 4 + c] = fmaf(Tq.m[8 + r], Ta.m[8 + c], fmaf(Tq.m[4 + r], Ta.m[4 + c], Tq.m[r] * Ta.m[c]));
+                const float dx0 = Ta.m[3] - Tq.m[3], dy0 = Ta.m[7] - Tq.m[7], dz0 = Ta.m[11] - Tq.m[11];
+                Tqa.m[r * 4 + 3] = fmaf(Tq.m[8 + r], dz0, fmaf(Tq.m[4 + r], dy0, Tq.m[r] * dx0));
+            }
+            const float Sw = fmaxf(fmaxf(fabsf(ax), fmaxf(fabsf(ay), fabsf(az))), 1.0f);
+            // runs split over the group's lanes; a lane tests its run on its own waypoint
+            for (int r0 = (int)e.y; r0 < (int)e.z; r0 += kCostSub) {
+                const int r = r0 + u;
+                if (r >= (int)e.z) continue;
                 const uint2 run = __ldg(md.sruns + r);
                 const int i = run.x & 0x1ffu, len = (run.x >> 14) & 0x1ffu, j0 = (int)run.y;
                 const float4 si = M.S[i];
-                float pxw, pyw, pzw;
-                sphere_world(Ta, si.x, si.y, si.z, pxw, pyw, pzw);
-                // p_i in joint q's link frame: R_q^T (p_i - t_q)
-                const float ux = pxw - Tq.m[3], uy = pyw - Tq.m[7], uz = pzw - Tq.m[11];
-                const float lx = Tq.m[0] * ux + Tq.m[4] * uy + Tq.m[8] * uz;
-                const float ly = Tq.m[1] * ux + Tq.m[5] * uy + Tq.m[9] * uz;
-                const float lz = Tq.m[2] * ux + Tq.m[6] * uy + Tq.m[10] * uz;
+                float lx, ly, lz;
+                sphere_world(Tqa, si.x, si.y, si.z, lx, ly, lz);
                 const float ex = lx - bq.x, ey = ly - bq.y, ez = lz - bq.z;
-                const float Sl = fmaxf(fabsf(lx), fmaxf(fabsf(ly), fabsf(lz))) +
-                                 fmaxf(fabsf(pxw), fmaxf(fabsf(pyw), fabsf(pzw)));
+                const float Sl = fmaxf(fabsf(lx), fmaxf(fabsf(ly), fabsf(lz))) + Sw;
                 float rt = si.w + bq.w + smp;
                 rt += 4.0f * (Sl + rt + 1.0f) * PS_GUARD_K;
-                if (kStats && u == 0) st.v[ST_SELF] += 1;
-                if (!__any_sync(kCostFull, fmaf(ez, ez, fmaf(ey, ey, ex * ex)) < rt * rt)) continue;
+                if (kStats) st.v[ST_SELF] += 1;
+                if (fmaf(ez, ez, fmaf(ey, ey, ex * ex)) >= rt * rt) continue;   // no pair of the run can set the hinge
                 const float ri = si.w;
-#pragma unroll 2
-                for (int m = u; m < len; m += kCostSub) {
+#pragma unroll 4
+                for (int m = 0; m < len; ++m) {
                     const float4 sj = M.S[j0 + m];
                     const float vx = lx - sj.x, vy = ly - sj.y, vz = lz - sj.z;
                     const float d2 = fmaf(vz, vz, fmaf(vy, vy, vx * vx));
                     const float rs = ri + sj.w;
                     const float t = bv + rs;
-                    if (kStats) st.v[ST_SELF] += 1;
                     if (t > 0.0f && d2 < t * t * (1.0f + 4.0e-6f)) {   // can beat bv: take the root
                         const float c = sqrtf(d2) - rs;
                         if (c < bv) {
@@ -460,6 +467,7 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
                         }
                     }
                 }
+                if (kStats) st.v[ST_SELF] += len;
             }
         }
         // minimum over the group by (value, pair order)
