@@ -404,9 +404,8 @@ typedef struct ps_batch_tuning {
                                 slots its persistent grid takes              */
     float traj_share;        /* same for the trajectory kernel's grid         */
     int   traj_threads;      /* threads per block of the trajectory kernel
-                                (64 or 128, one waypoint per thread)         */
-    int   traj_tile;         /* waypoints per thread of the trajectory kernel:
-                                always 1 (one waypoint per lane)             */
+                                (128 or 256; 4 lanes per waypoint)           */
+    int   traj_tile;         /* kept in the record; always 1                  */
     float best_ms;           /* measured time of one launch at this choice    */
 } ps_batch_tuning;
 

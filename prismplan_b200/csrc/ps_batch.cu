@@ -157,9 +157,10 @@ __global__ void __launch_bounds__(kWarps * 32, 16 / kWarps) batch_waypoint_kerne
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int slot = lane / kCostSub, u = lane % kCostSub;
-    const LaneScratch ws =
-        lane_carve(reinterpret_cast<unsigned char*>(cb.wbase) + (size_t)warp * lane_warp_bytes(NJ, D, sv.n_obbs, true),
-                   NJ, D, true);
+    const int NS = M.H->n_spheres;
+    const LaneScratch ws = lane_carve(
+        reinterpret_cast<unsigned char*>(cb.wbase) + (size_t)warp * lane_warp_bytes(NJ, NS, D, sv.n_obbs, true), NJ,
+        NS, D, true);
     LaneStats st;
     for (int c = blockIdx.x * kWarps + warp; c < chunks; c += gridDim.x * kWarps) {
         const bool traj = c < chunks_a;   // uniform over the warp
@@ -257,7 +258,7 @@ struct ps_batch {
     // tuning state
     float edge_share = 1.0f;   // of the edge kernel's full-occupancy grid
     float traj_share = 0.5f;   // of the trajectory kernel's full-occupancy grid
-    int traj_threads = 128;   // threads per block of the trajectory kernel (kCostSub per waypoint)
+    int traj_threads = 256;   // threads per block of the trajectory kernel (kCostSub per waypoint)
     int traj_tile = 1;        // kept for the tuning record: always 1
 };
 
@@ -277,7 +278,7 @@ using WaypointKernel = void (*)(ModelDev, ps_scene_view, ps_cost_params, const C
                                 int);
 
 WaypointKernel pick_waypoint_kernel(int threads) {
-    return threads == 64 ? batch_waypoint_kernel<2> : batch_waypoint_kernel<4>;
+    return threads == 128 ? batch_waypoint_kernel<4> : batch_waypoint_kernel<8>;
 }
 
 // Everything that is not a stream operation happens before the capture.
@@ -611,7 +612,7 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
     if (!b) return set_error(PS_EINVAL, "NULL batch");
     const float edge_shares[] = {0.5f, 0.75f, 1.0f};
     const float traj_shares[] = {0.25f, 0.5f, 1.0f};
-    const int widths[] = {64, 128};
+    const int widths[] = {128, 256};
     const int tiles[] = {1};
     cudaStream_t s = nullptr;
     cudaEvent_t a = nullptr, z = nullptr;
@@ -633,7 +634,7 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
         for (float ts : traj_shares) {
             for (int w : widths) {
                 for (int tl : tiles) {
-                    if (!trajs && (ts != 0.5f || w != 128 || tl != 1)) continue;
+                    if (!trajs && (ts != 0.5f || w != 256 || tl != 1)) continue;
                     b->edge_share = es;
                     b->traj_share = ts;
                     b->traj_threads = w;

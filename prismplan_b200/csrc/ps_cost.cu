@@ -38,7 +38,7 @@ size_t cost_block_smem(const ps_model* m, const ps_scene_view* sv, bool grad) {
 // rows are all skipped does nothing. A waypoint gets the same bits whichever
 // rows share its warp.
 template <bool kGrad, bool kStats>
-__global__ void __launch_bounds__(kLaneCostWarps * 32, 4) waypoint_cost_kernel(
+__global__ void __launch_bounds__(kLaneCostWarps * 32, 2) waypoint_cost_kernel(
     ModelDev md, ps_scene_view sv, const float* __restrict__ q, int n_rows, int T, ps_cost_params P,
     float* __restrict__ wp_cost, int broadcast_d, float* __restrict__ traj_acc, float* __restrict__ grad,
     unsigned long long* stats, const uint8_t* __restrict__ skip) {
@@ -78,9 +78,10 @@ __global__ void __launch_bounds__(kLaneCostWarps * 32, 4) waypoint_cost_kernel(
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int slot = lane / kCostSub, u = lane % kCostSub;
+    const int NS = M.H->n_spheres;
     const LaneScratch ws = lane_carve(reinterpret_cast<unsigned char*>(cb.wbase) +
-                                          (size_t)warp * lane_warp_bytes(NJ, D, sv.n_obbs, kGrad),
-                                      NJ, D, kGrad);
+                                          (size_t)warp * lane_warp_bytes(NJ, NS, D, sv.n_obbs, kGrad),
+                                      NJ, NS, D, kGrad);
     const long long total = (long long)n_rows * T;
     LaneStats st;
     st.zero();

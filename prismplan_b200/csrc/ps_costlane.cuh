@@ -10,8 +10,9 @@
 // uniform over the warp (candidate lists, runs, joint pairs), so lanes do not
 // diverge on them:
 //   1. FK walk in DFS order with accurate sincosf (each lane of a group
-//      repeats it; the group's frames and each joint's world bound centre go
-//      to shared memory, SoA by waypoint slot);
+//      repeats it; the group's frames, each joint's world bound centre and,
+//      in step 3, each sphere's world centre go to shared memory, SoA by
+//      waypoint slot);
 //   2. per joint, one warp broad phase: the joint's bound spheres of the
 //      warp's waypoints are enclosed by one sphere (centre = lane 16's, radius
 //      = a one-instruction warp max), and lanes over boxes keep the boxes
@@ -26,16 +27,16 @@
 //   4. F and M are summed over the group and folded into the joint's
 //      ancestors: dC/dq_p += a_p . (M - o_p x F) (revolute) or a_p . F
 //      (prismatic), a_p and o_p the joint axis and origin from the frames;
-//   5. self hinge: joint pairs whose bound spheres can come within m_self (on
-//      any waypoint of the warp) expand their runs (sphere i of joint a against
-//      consecutive spheres j of joint q). The group's lanes split the runs; a
-//      lane maps its run's sphere i into q's link frame with the joint pair's
-//      relative transform T_q^-1 T_a, skips the run if i is out of reach of
-//      q's bound sphere, and otherwise costs one difference per pair against
-//      the link-frame centres. Only pairs within r_i + r_j + m_self can set the
-//      hinge, and a square root is taken only for those; the minimum over the
-//      group is taken by (value, pair order), and the argmin pair's force goes
-//      to both joints' ancestors.
+//   5. self hinge, on the world sphere centres that step 3 left in shared
+//      memory: the group's lanes split the joint pairs' bound tests (one ballot
+//      gives each pair's OR over the warp's waypoints); a pair that can come
+//      within m_self expands its runs (sphere i of joint a against consecutive
+//      spheres j of joint q), split over the group's lanes; a lane skips its
+//      run when i is out of reach of q's bound sphere on its own waypoint.
+//      Only pairs within r_i + r_j + m_self can set the hinge, and a square
+//      root is taken only for those; the minimum over the group is taken by
+//      (value, pair order), and the argmin pair's force goes to both joints'
+//      ancestors.
 // Every candidate set is a superset of what the waypoint itself needs, and
 // the group size is fixed, so a waypoint gives the same bits whatever other
 // waypoints share its warp; the batch relies on that.
@@ -52,33 +53,38 @@ namespace {
 
 constexpr int kCostSub = 4;                  // lanes per waypoint
 constexpr int kCostSlots = 32 / kCostSub;    // waypoints per warp
-constexpr int kLaneCostWarps = 4;            // warps per block of the cost kernels
+constexpr int kLaneCostWarps = 8;            // warps per block of the cost kernels
 
 // Per-warp scratch floats, SoA over the warp's waypoint slots: frames of
-// joints 1..NJ-1 (joint 0 is the identity), world bound centres, per-joint
-// gradient (gradient only), the waypoint's configuration.
-__host__ __device__ inline int lane_cost_floats(int NJ, int D, bool grad) {
-    return kCostSlots * (12 * (NJ - 1) + 3 * NJ + (grad ? NJ : 0) + D);
+// joints 1..NJ-1 (joint 0 is the identity), world bound centres, world
+// sphere centres, per-joint gradient (gradient only), the waypoint's
+// configuration.
+__host__ __device__ inline int lane_cost_floats(int NJ, int NS, int D, bool grad) {
+    return kCostSlots * (12 * (NJ - 1) + 3 * NJ + 3 * NS + (grad ? NJ : 0) + D);
 }
-__host__ __device__ inline size_t lane_warp_bytes(int NJ, int D, int n_obbs, bool grad) {
-    return (size_t)lane_cost_floats(NJ, D, grad) * 4 + ((((size_t)(n_obbs > 0 ? n_obbs : 1)) * 2 + 15) & ~size_t(15));
+__host__ __device__ inline size_t lane_warp_bytes(int NJ, int NS, int D, int n_obbs, bool grad) {
+    return (size_t)lane_cost_floats(NJ, NS, D, grad) * 4 +
+           ((((size_t)(n_obbs > 0 ? n_obbs : 1)) * 2 + 15) & ~size_t(15));
 }
 
 struct LaneScratch {
     float* fr;        // [(NJ-1)*12][slots]
     float* bc;        // [NJ*3][slots]
+    float* pos;       // [NS*3][slots]
     float* dq;        // [NJ][slots] (gradient only)
     float* q;         // [D][slots]
     uint16_t* cand;   // [n_obbs]: boxes kept by the current joint's broad phase (warp-uniform)
 };
 
-__device__ __forceinline__ LaneScratch lane_carve(unsigned char* base, int NJ, int D, bool grad) {
+__device__ __forceinline__ LaneScratch lane_carve(unsigned char* base, int NJ, int NS, int D, bool grad) {
     LaneScratch s;
     float* f = reinterpret_cast<float*>(base);
     s.fr = f;
     f += kCostSlots * 12 * (NJ - 1);
     s.bc = f;
     f += kCostSlots * 3 * NJ;
+    s.pos = f;
+    f += kCostSlots * 3 * NS;
     s.dq = grad ? f : nullptr;
     if (grad) f += kCostSlots * NJ;
     s.q = f;
@@ -92,7 +98,7 @@ __device__ __forceinline__ LaneScratch lane_carve(unsigned char* base, int NJ, i
 inline size_t lane_block_bytes(const ps_model* m, const ps_scene_view* sv, int warps, bool grad) {
     return (size_t)m->dev.bytes_core + scene_smem_bytes(sv) + (((size_t)m->info.n_spheres + 15) & ~size_t(15)) + 64 +
            (size_t)16 * std::max(sv->n_obbs, 1) +
-           (size_t)warps * lane_warp_bytes(m->info.n_joints, m->info.n_dof, sv->n_obbs, grad);
+           (size_t)warps * lane_warp_bytes(m->info.n_joints, m->info.n_spheres, m->info.n_dof, sv->n_obbs, grad);
 }
 
 __device__ __forceinline__ void lane_frame(const float* fr, int p, int slot, Affine& T) {
@@ -373,6 +379,9 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 if (!val[i]) continue;
+                ws.pos[(kk[i] * 3 + 0) * kCostSlots + slot] = px[i];
+                ws.pos[(kk[i] * 3 + 1) * kCostSlots + slot] = py[i];
+                ws.pos[(kk[i] * 3 + 2) * kCostSlots + slot] = pz[i];
                 float gx, gy, gz;
                 lane_sphere_terms<kGrad, kStats>(M, sc, sv, P, kk[i], px[i], py[i], pz[i], rr[i], ncand > 0, key[i],
                                                  arg[i], obb_part, esdf_part, gx, gy, gz, st);
@@ -406,68 +415,66 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
         const float smg = P.self_margin, smp = fmaxf(smg, 0.0f);
         float bv = smg;   // pairs at or above the margin cannot set the hinge
         int bk = INT_MAX, bi = -1, bj = -1;
-        for (int jp = 0; jp < md.n_sjp; ++jp) {
-            const uint4 e = __ldg(md.sjp + jp);
-            const int a = (int)(e.x & 0xffffu), qj = (int)(e.x >> 16);
-            const float4 ba = M.J[a].bound, bq = M.J[qj].bound;
-            const float ax = ws.bc[(a * 3) * kCostSlots + slot], ay = ws.bc[(a * 3 + 1) * kCostSlots + slot],
-                        az = ws.bc[(a * 3 + 2) * kCostSlots + slot];
-            const float qx0 = ws.bc[(qj * 3) * kCostSlots + slot], qy0 = ws.bc[(qj * 3 + 1) * kCostSlots + slot],
-                        qz0 = ws.bc[(qj * 3 + 2) * kCostSlots + slot];
-            const float dx = ax - qx0, dy = ay - qy0, dz = az - qz0;
-            const float S = fmaxf(fmaxf(fabsf(ax), fmaxf(fabsf(ay), fabsf(az))),
-                                  fmaxf(fabsf(qx0), fmaxf(fabsf(qy0), fabsf(qz0))));
-            float thr = ba.w + bq.w + smp;
-            thr += 4.0f * (S + thr + 1.0f) * PS_GUARD_K;
-            if (kStats && u == 0) st.v[ST_SELF] += 1;
-            if (!__any_sync(kCostFull, fmaf(dz, dz, fmaf(dy, dy, dx * dx)) < thr * thr)) continue;
-            // relative transform T_q^-1 T_a: sphere i of joint a straight into q's link frame
-            Affine Ta, Tq, Tqa;
-            lane_frame(ws.fr, a, slot, Ta);
-            lane_frame(ws.fr, qj, slot, Tq);
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-                    Tqa.m[r * 4 + c] = fmaf(Tq.m[8 + r], Ta.m[8 + c], fmaf(Tq.m[4 + r], Ta.m[4 + c], Tq.m[r] * Ta.m[c]));
-                const float dx0 = Ta.m[3] - Tq.m[3], dy0 = Ta.m[7] - Tq.m[7], dz0 = Ta.m[11] - Tq.m[11];
-                Tqa.m[r * 4 + 3] = fmaf(Tq.m[8 + r], dz0, fmaf(Tq.m[4 + r], dy0, Tq.m[r] * dx0));
-            }
-            const float Sw = fmaxf(fmaxf(fabsf(ax), fmaxf(fabsf(ay), fabsf(az))), 1.0f);
-            // runs split over the group's lanes; a lane tests its run on its own waypoint
-            for (int r0 = (int)e.y; r0 < (int)e.z; r0 += kCostSub) {
-                const int r = r0 + u;
-                if (r >= (int)e.z) continue;
-                const uint2 run = __ldg(md.sruns + r);
-                const int i = run.x & 0x1ffu, len = (run.x >> 14) & 0x1ffu, j0 = (int)run.y;
-                const float4 si = M.S[i];
-                float lx, ly, lz;
-                sphere_world(Tqa, si.x, si.y, si.z, lx, ly, lz);
-                const float ex = lx - bq.x, ey = ly - bq.y, ez = lz - bq.z;
-                const float Sl = fmaxf(fabsf(lx), fmaxf(fabsf(ly), fabsf(lz))) + Sw;
-                float rt = si.w + bq.w + smp;
-                rt += 4.0f * (Sl + rt + 1.0f) * PS_GUARD_K;
+        auto at = [&](const float* a, int k, int c) { return a[(k * 3 + c) * kCostSlots + slot]; };
+        for (int jp0 = 0; jp0 < md.n_sjp; jp0 += kCostSub) {
+            // lane u tests joint pair jp0 + u on its own waypoint; one ballot
+            // gives each pair's OR over the warp's waypoints
+            bool pass = false;
+            if (jp0 + u < md.n_sjp) {
+                const uint4 e = __ldg(md.sjp + jp0 + u);
+                const int a = (int)(e.x & 0xffffu), qj = (int)(e.x >> 16);
+                const float ax = at(ws.bc, a, 0), ay = at(ws.bc, a, 1), az = at(ws.bc, a, 2);
+                const float qx0 = at(ws.bc, qj, 0), qy0 = at(ws.bc, qj, 1), qz0 = at(ws.bc, qj, 2);
+                const float dx = ax - qx0, dy = ay - qy0, dz = az - qz0;
+                const float S = fmaxf(fmaxf(fabsf(ax), fmaxf(fabsf(ay), fabsf(az))),
+                                      fmaxf(fabsf(qx0), fmaxf(fabsf(qy0), fabsf(qz0))));
+                float thr = M.J[a].bound.w + M.J[qj].bound.w + smp;
+                thr += 4.0f * (S + thr + 1.0f) * PS_GUARD_K;
+                pass = fmaf(dz, dz, fmaf(dy, dy, dx * dx)) < thr * thr;
                 if (kStats) st.v[ST_SELF] += 1;
-                if (fmaf(ez, ez, fmaf(ey, ey, ex * ex)) >= rt * rt) continue;   // no pair of the run can set the hinge
-                const float ri = si.w;
+            }
+            const unsigned bal = __ballot_sync(kCostFull, pass);
+            for (int v = 0; v < kCostSub && jp0 + v < md.n_sjp; ++v) {
+                if (!(bal & (0x11111111u << v))) continue;   // uniform
+                const uint4 e = __ldg(md.sjp + jp0 + v);
+                const int qj = (int)(e.x >> 16);
+                const float Rq = M.J[qj].bound.w;
+                const float cqx = at(ws.bc, qj, 0), cqy = at(ws.bc, qj, 1), cqz = at(ws.bc, qj, 2);
+                // the group's lanes split the runs; a lane tests its run on its own waypoint
+                for (int r0 = (int)e.y; r0 < (int)e.z; r0 += kCostSub) {
+                    const int r = r0 + u;
+                    if (r >= (int)e.z) continue;
+                    const uint2 run = __ldg(md.sruns + r);
+                    const int i = run.x & 0x1ffu, len = (run.x >> 14) & 0x1ffu, j0 = (int)run.y;
+                    const float ri = M.S[i].w;
+                    const float pxi = at(ws.pos, i, 0), pyi = at(ws.pos, i, 1), pzi = at(ws.pos, i, 2);
+                    const float ex = pxi - cqx, ey = pyi - cqy, ez = pzi - cqz;
+                    const float Sl = fmaxf(fmaxf(fabsf(pxi), fmaxf(fabsf(pyi), fabsf(pzi))),
+                                           fmaxf(fabsf(cqx), fmaxf(fabsf(cqy), fabsf(cqz))));
+                    float rt = ri + Rq + smp;
+                    rt += 4.0f * (Sl + rt + 1.0f) * PS_GUARD_K;
+                    if (kStats) st.v[ST_SELF] += 1;
+                    if (fmaf(ez, ez, fmaf(ey, ey, ex * ex)) >= rt * rt) continue;   // no pair can set the hinge
 #pragma unroll 4
-                for (int m = 0; m < len; ++m) {
-                    const float4 sj = M.S[j0 + m];
-                    const float vx = lx - sj.x, vy = ly - sj.y, vz = lz - sj.z;
-                    const float d2 = fmaf(vz, vz, fmaf(vy, vy, vx * vx));
-                    const float rs = ri + sj.w;
-                    const float t = bv + rs;
-                    if (t > 0.0f && d2 < t * t * (1.0f + 4.0e-6f)) {   // can beat bv: take the root
-                        const float c = sqrtf(d2) - rs;
-                        if (c < bv) {
-                            bv = c;
-                            bk = (r << 9) | m;
-                            bi = i;
-                            bj = j0 + m;
+                    for (int m = 0; m < len; ++m) {
+                        const int j = j0 + m;
+                        const float vx = pxi - at(ws.pos, j, 0), vy = pyi - at(ws.pos, j, 1),
+                                    vz = pzi - at(ws.pos, j, 2);
+                        const float d2 = fmaf(vz, vz, fmaf(vy, vy, vx * vx));
+                        const float rs = ri + M.S[j].w;
+                        const float t = bv + rs;
+                        if (t > 0.0f && d2 < t * t * (1.0f + 4.0e-6f)) {   // can beat bv: take the root
+                            const float c = sqrtf(d2) - rs;
+                            if (c < bv) {
+                                bv = c;
+                                bk = (r << 9) | m;
+                                bi = i;
+                                bj = j;
+                            }
                         }
                     }
+                    if (kStats) st.v[ST_SELF] += len;
                 }
-                if (kStats) st.v[ST_SELF] += len;
             }
         }
         // minimum over the group by (value, pair order)
@@ -488,13 +495,8 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
         if (kGrad && u == 0 && bi >= 0 && self_h > 0.0f) {
             // world positions of the pair: d self_h / d p_i = -(p_i - p_j) / |p_i - p_j|
             const int pi = cb.sph_joint[bi], pj = cb.sph_joint[bj];
-            Affine Ti, Tj;
-            lane_frame(ws.fr, pi, slot, Ti);
-            lane_frame(ws.fr, pj, slot, Tj);
-            const float4 si = M.S[bi], sj = M.S[bj];
-            float xi, yi, zi, xj, yj, zj;
-            sphere_world(Ti, si.x, si.y, si.z, xi, yi, zi);
-            sphere_world(Tj, sj.x, sj.y, sj.z, xj, yj, zj);
+            const float xi = at(ws.pos, bi, 0), yi = at(ws.pos, bi, 1), zi = at(ws.pos, bi, 2);
+            const float xj = at(ws.pos, bj, 0), yj = at(ws.pos, bj, 1), zj = at(ws.pos, bj, 2);
             const float dx = xi - xj, dy = yi - yj, dz = zi - zj;
             const float dd = sqrtf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
             if (dd > 0.0f) {
