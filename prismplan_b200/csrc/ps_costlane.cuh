@@ -455,18 +455,22 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
                     rt += 4.0f * (Sl + rt + 1.0f) * PS_GUARD_K;
                     if (kStats) st.v[ST_SELF] += 1;
                     if (fmaf(ez, ez, fmaf(ey, ey, ex * ex)) >= rt * rt) continue;   // no pair can set the hinge
+                    // sqrt(d2) - (ri + rj) < bv needs d2 < (bv + ri + rj)^2 (widened for
+                    // rounding); when bv + ri + rj <= 0 the exact test below fails anyway
+                    float tb = bv + ri;
 #pragma unroll 4
                     for (int m = 0; m < len; ++m) {
                         const int j = j0 + m;
                         const float vx = pxi - at(ws.pos, j, 0), vy = pyi - at(ws.pos, j, 1),
                                     vz = pzi - at(ws.pos, j, 2);
                         const float d2 = fmaf(vz, vz, fmaf(vy, vy, vx * vx));
-                        const float rs = ri + M.S[j].w;
-                        const float t = bv + rs;
-                        if (t > 0.0f && d2 < t * t * (1.0f + 4.0e-6f)) {   // can beat bv: take the root
-                            const float c = sqrtf(d2) - rs;
+                        const float rj = M.S[j].w;
+                        const float t = tb + rj;
+                        if (d2 * (1.0f - 4.0e-6f) < t * t) {   // can beat bv: take the root
+                            const float c = sqrtf(d2) - (ri + rj);
                             if (c < bv) {
                                 bv = c;
+                                tb = bv + ri;
                                 bk = (r << 9) | m;
                                 bi = i;
                                 bj = j;
