@@ -178,6 +178,32 @@ __device__ __forceinline__ void lane_keys(const SceneSmem& sc, const uint16_t* c
     }
 }
 
+// kN spheres of one lane: k0, k0 + kCostSub, ... (those at or past kend are
+// marked invalid and replaced by k0), their world centres, radii and, over
+// the candidate boxes, their closest-box keys. Slots kN..3 are invalid.
+template <int kN, bool kGrad>
+__device__ __forceinline__ void lane_group(const ModelSmem& M, const Affine& T, int k0, int kend,
+                                           const SceneSmem& sc, const uint16_t* cand, int ncand, float* px, float* py,
+                                           float* pz, float* rr, float* key, int* arg, int* kk, bool* val) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        key[i] = 3.0e38f;
+        arg[i] = -1;
+        val[i] = false;
+        kk[i] = k0;
+    }
+#pragma unroll
+    for (int i = 0; i < kN; ++i) {
+        const int k = k0 + kCostSub * i;
+        val[i] = k < kend;
+        kk[i] = val[i] ? k : k0;
+        const float4 sp = M.S[kk[i]];
+        sphere_world(T, sp.x, sp.y, sp.z, px[i], py[i], pz[i]);
+        rr[i] = sp.w;
+    }
+    if (ncand > 0) lane_keys<kN, kGrad>(sc, cand, ncand, px, py, pz, key, arg);
+}
+
 // Same for one sphere with its ACM row (global memory): masked boxes skipped.
 __device__ __forceinline__ void lane_key_masked(const SceneSmem& sc, const uint16_t* cand, int ncand, float px,
                                                 float py, float pz, const uint8_t* acm_row, float& key, int& arg) {
@@ -349,33 +375,27 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
             float px[4], py[4], pz[4], rr[4], key[4];
             int arg[4], kk[4];
             bool val[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int k = jr.sph_beg + u + kCostSub * (m0 + i);
-                val[i] = i < ng && k < jr.sph_end;
-                kk[i] = val[i] ? k : jr.sph_beg;
-                const float4 sp = M.S[kk[i]];
-                sphere_world(T, sp.x, sp.y, sp.z, px[i], py[i], pz[i]);
-                rr[i] = sp.w;
-                key[i] = 3.0e38f;
-                arg[i] = -1;
-                if (kStats && val[i]) st.v[ST_SPHERES] += 1;
-            }
-            if (ncand > 0) {
-                if (masked)
+            const int k0 = jr.sph_beg + u + kCostSub * m0;
+            if (ng == 4)
+                lane_group<4, kGrad>(M, T, k0, jr.sph_end, sc, ws.cand, ncand, px, py, pz, rr, key, arg, kk, val);
+            else if (ng == 3)
+                lane_group<3, kGrad>(M, T, k0, jr.sph_end, sc, ws.cand, ncand, px, py, pz, rr, key, arg, kk, val);
+            else if (ng == 2)
+                lane_group<2, kGrad>(M, T, k0, jr.sph_end, sc, ws.cand, ncand, px, py, pz, rr, key, arg, kk, val);
+            else if (!masked)
+                lane_group<1, kGrad>(M, T, k0, jr.sph_end, sc, ws.cand, ncand, px, py, pz, rr, key, arg, kk, val);
+            else {
+                lane_group<1, kGrad>(M, T, k0, jr.sph_end, sc, ws.cand, 0, px, py, pz, rr, key, arg, kk, val);
+                if (ncand > 0)
                     lane_key_masked(sc, ws.cand, ncand, px[0], py[0], pz[0],
                                     sv.sphere_obb_acm_mask + (size_t)M.SO[kk[0]] * sv.n_obbs, key[0], arg[0]);
-                else if (ng == 4)
-                    lane_keys<4, kGrad>(sc, ws.cand, ncand, px, py, pz, key, arg);
-                else if (ng == 3)
-                    lane_keys<3, kGrad>(sc, ws.cand, ncand, px, py, pz, key, arg);
-                else if (ng == 2)
-                    lane_keys<2, kGrad>(sc, ws.cand, ncand, px, py, pz, key, arg);
-                else
-                    lane_keys<1, kGrad>(sc, ws.cand, ncand, px, py, pz, key, arg);
-                if (kStats)
-                    for (int i = 0; i < 4; ++i) st.v[ST_PAIRS] += val[i] ? ncand : 0;
             }
+            if (kStats)
+                for (int i = 0; i < 4; ++i)
+                    if (val[i]) {
+                        st.v[ST_SPHERES] += 1;
+                        st.v[ST_PAIRS] += ncand;
+                    }
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 if (!val[i]) continue;
@@ -437,9 +457,15 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
             for (int v = 0; v < kCostSub && jp0 + v < md.n_sjp; ++v) {
                 if (!(bal & (0x11111111u << v))) continue;   // uniform
                 const uint4 e = __ldg(md.sjp + jp0 + v);
-                const int qj = (int)(e.x >> 16);
-                const float Rq = M.J[qj].bound.w;
+                const int a = (int)(e.x & 0xffffu), qj = (int)(e.x >> 16);
+                const float Ra = M.J[a].bound.w, Rq = M.J[qj].bound.w;
                 const float cqx = at(ws.bc, qj, 0), cqy = at(ws.bc, qj, 1), cqz = at(ws.bc, qj, 2);
+                // run reach: r_i + R_q + max(m_self, 0) plus a guard for the FP32
+                // centres, from bounds that hold for every sphere i of joint a
+                const float Sjp = fmaxf(fmaxf(fabsf(at(ws.bc, a, 0)), fmaxf(fabsf(at(ws.bc, a, 1)),
+                                                                            fabsf(at(ws.bc, a, 2)))) + Ra,
+                                        fmaxf(fabsf(cqx), fmaxf(fabsf(cqy), fabsf(cqz))));
+                const float reach = Rq + smp + 4.0f * (Sjp + Ra + Rq + smp + 1.0f) * PS_GUARD_K;
                 // the group's lanes split the runs; a lane tests its run on its own waypoint
                 for (int r0 = (int)e.y; r0 < (int)e.z; r0 += kCostSub) {
                     const int r = r0 + u;
@@ -449,10 +475,7 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
                     const float ri = M.S[i].w;
                     const float pxi = at(ws.pos, i, 0), pyi = at(ws.pos, i, 1), pzi = at(ws.pos, i, 2);
                     const float ex = pxi - cqx, ey = pyi - cqy, ez = pzi - cqz;
-                    const float Sl = fmaxf(fmaxf(fabsf(pxi), fmaxf(fabsf(pyi), fabsf(pzi))),
-                                           fmaxf(fabsf(cqx), fmaxf(fabsf(cqy), fabsf(cqz))));
-                    float rt = ri + Rq + smp;
-                    rt += 4.0f * (Sl + rt + 1.0f) * PS_GUARD_K;
+                    const float rt = ri + reach;
                     if (kStats) st.v[ST_SELF] += 1;
                     if (fmaf(ez, ez, fmaf(ey, ey, ex * ex)) >= rt * rt) continue;   // no pair can set the hinge
                     // sqrt(d2) - (ri + rj) < bv needs d2 < (bv + ri + rj)^2 (widened for
