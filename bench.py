@@ -188,6 +188,8 @@ def run_ours(args):
     frm = torch.from_numpy(wl["from"]).to(dev)
     to = torch.from_numpy(wl["to"]).to(dev)
     params = api.EdgeEvalParams(max_joint_step=STEP_RAD, max_samples=MAX_SAMPLES)
+    # launch shape chosen by the autotuner on this rank's edges (untimed)
+    params, tuning = api.tune_edges(b, sc, frm, to, params=params)
     wsb = api.edges_workspace(E, dev)
     out = (torch.empty(E, dtype=torch.uint8, device=dev), torch.empty(E, device=dev), torch.empty(E, device=dev))
     stream = torch.cuda.Stream(device=dev)
@@ -241,12 +243,14 @@ def run_ours(args):
     valid_frac = float(out[0].float().mean().item())
     timed_out = (out[0].cpu().numpy().copy(), out[1].cpu().numpy().copy())   # the timed step's verdicts and costs
     del graph
-    # prep, queue pass 0, finalize; the end-sample probe when there are at
-    # least 8 warps of edges per SM; a second queue pass when the edges are
-    # fewer than 8 per resident warp (5 blocks of 4 warps per SM for this
-    # kernel variant)
+    # prep, queue pass 0, finalize; the end-sample probe when the tuned shape
+    # (or, automatic, at least 8 warps of edges per SM) runs it; a second
+    # queue pass when the edges are fewer than 8 per resident warp (the tuned
+    # queue residency, or 5 blocks of 4 warps per SM for this kernel variant)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
-    launches_per_step = 3 + (1 if E >= 8 * 32 * sms else 0) + (1 if E < 8 * sms * 5 * 4 else 0)
+    probe_on = tuning["probe"] == 1 or (tuning["probe"] == 0 and E >= 8 * 32 * sms)
+    qres = tuning["queue_blocks_per_sm"] or 5
+    launches_per_step = 3 + (1 if probe_on else 0) + (1 if E < 8 * sms * qres * 4 else 0)
 
     result = None
     if rank == 0:
@@ -258,7 +262,11 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "edges": E, "samples_per_step": total_samples,
                        "samples_rule": f"G=clamp(ceil(Linf/{STEP_RAD}),1,{MAX_SAMPLES})",
                        "robot": "panda-like 7R, 59 spheres", "obbs": 64, "valid_fraction": valid_frac,
-                       "l2": "flushed between steps (256 MiB write)", "parallelism": f"shard{ws}"},
+                       "l2": "flushed between steps (256 MiB write)", "parallelism": f"shard{ws}",
+                       "tuning": {"probe": {1: "on", 2: "off"}.get(tuning["probe"], "auto"),
+                                  "queue_blocks_per_sm": tuning["queue_blocks_per_sm"], "grab": tuning["grab"],
+                                  "tuned_ms": tuning["best_ms"], "default_ms": tuning["default_ms"],
+                                  "candidates": tuning["candidates"], "by": "ps_tune_edges (untimed)"}},
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(),
             "edges_per_s": ws * E * args.steps / (t_total * 1e-3),
@@ -371,6 +379,7 @@ def bench_edges_sparse(dev, wl, b, frm, to, params, steps=20, with_ref=True):
     lib = _lib.load()
     obbs = workloads.random_obbs(np.random.default_rng(1012), 64, lo=-1.0, hi=1.0, half_lo=0.02, half_hi=0.1)
     sc = SceneTensors(*obbs)
+    params, stune = api.tune_edges(b, sc, frm, to, params=params)   # this scene's own shape (untimed)
     E = len(wl["from"])
     total_samples = int(wl["G"].sum())
     wsb = api.edges_workspace(E, dev)
@@ -423,7 +432,8 @@ def bench_edges_sparse(dev, wl, b, frm, to, params, steps=20, with_ref=True):
                         "flops_per_launch": flops_from_stats(stats),
                         "work_per_launch": dict(zip(["pairs", "exact", "samples", "joints", "spheres", "self",
                                                      "esdf", "cull"], stats))},
-           "scene": "64 OBBs, centres U([-1,1]^3), half-extents U(0.02,0.1), seed 1012"}
+           "scene": "64 OBBs, centres U([-1,1]^3), half-extents U(0.02,0.1), seed 1012",
+           "tuning": dict(stune, by="ps_tune_edges (untimed)")}
     if with_ref:
         try:
             import oracle
@@ -528,21 +538,24 @@ def bench_configs(dev, with_ref=True):
     b = RobotModelBuilder.from_asset(wl["asset"]).build()
     sc = SceneTensors(*wl["obbs"])
     q = torch.from_numpy(np.tile(wl["q"], (256, 1))).to(dev)   # 1M configurations: steady state
+    bps, ctune = api.tune_configs(b, sc, q, clearance="obb")     # grid chosen by the autotuner (untimed)
     for _ in range(3):
-        api.check_configs(b, sc, q, clearance="obb")
+        api.check_configs(b, sc, q, clearance="obb", blocks_per_sm=bps)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(5):
-        api.check_configs(b, sc, q, clearance="obb")
+        api.check_configs(b, sc, q, clearance="obb", blocks_per_sm=bps)
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / 5
     out = {"workload": "configs_panda7_obb16 (4096 tiled to 1,048,576)", "value": q.shape[0] / (ms * 1e-3),
-           "unit": "configs/s", "ms_per_step": ms, "outputs": "hit + OBB min-clearance"}
+           "unit": "configs/s", "ms_per_step": ms, "outputs": "hit + OBB min-clearance",
+           "tuning": dict(ctune, by="ps_tune_configs (untimed)")}
     from prismplan_b200 import _lib
 
-    stats, kms = kernel_roofline(_lib.load(), dev, lambda: api.check_configs(b, sc, q, clearance="obb"))
+    stats, kms = kernel_roofline(_lib.load(), dev,
+                                 lambda: api.check_configs(b, sc, q, clearance="obb", blocks_per_sm=bps))
     peak = probe_peak()
     ach = flops_from_stats(stats) / (kms * 1e-3) / 1e12
     out["roofline"] = {"bound": "fp32", "kernel": "check_configs_kernel<clearance>", "kernel_ms": kms,
