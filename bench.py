@@ -253,6 +253,9 @@ def run_ours(args):
     launches_per_step = 3 + (1 if probe_on else 0) + (1 if E < 8 * sms * qres * 4 else 0)
 
     result = None
+    # With several ranks every rank measures its own end-to-end bridge (the
+    # same collectives on every rank); the other secondary cases run at N=1.
+    e2e_multi = e2e_all_ranks(args, b, sc, wl, params, ws) if ws > 1 and not args.headline_only else None
     if rank == 0:
         value = job_samples * args.steps / (t_total * 1e-3)
         result = {
@@ -273,6 +276,10 @@ def run_ours(args):
         }
         if args.headline_only:
             result["roofline"] = {"kernel": "edges_probe_kernel + edges_queue_kernel", "kernel_ms": statistics.median(kern_ms)}
+        elif ws > 1:
+            result["roofline"], _ = step_roofline(b, sc, frm, to, params, kern_ms, dev)
+            result["e2e"] = e2e_multi
+            result["secondary"] = "the comparison cases, CPU baseline and parity run at N=1 only"
         else:
             result.update(secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev, timed_out))
     if ws > 1:
@@ -281,9 +288,9 @@ def run_ours(args):
     return result
 
 
-def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev, timed_out):
-    """Roofline, e2e, parity, CPU baseline and the comparison paths (rank 0,
-    N=1 data). timed_out: (valid, cost) of the timed graph replay."""
+def step_roofline(b, sc, frm, to, params, kern_ms, dev):
+    """Roofline of the headline step's dominant kernels: executed work of one
+    call (device counters) over their CUDA-event time in the timed replays."""
     import ctypes
 
     import torch
@@ -291,10 +298,6 @@ def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev, timed_out)
     from prismplan_b200 import _lib, api
 
     lib = _lib.load()
-    E = len(wl["from"])
-    total_samples = int(wl["G"].sum())
-    res = {}
-    # ---- executed work of one launch (counters) ----
     st = torch.zeros(8, dtype=torch.int64, device=dev)
     lib.ps_set_stats(ctypes.c_void_p(st.data_ptr()))
     api.check_edges(b, sc, frm, to, params=params)
@@ -305,15 +308,23 @@ def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev, timed_out)
     peak = probe_peak()
     k_ms = statistics.median(kern_ms) if kern_ms else None
     achieved = flops / (k_ms * 1e-3) / 1e12 if k_ms else None
-    res["roofline"] = {
+    return {
         "bound": "fp32", "achieved": achieved, "peak": peak["tflops"], "unit": "TFLOP/s",
         "frac": (achieved / peak["tflops"]) if achieved and peak["tflops"] else None,
         "traffic": traffic_from_profiles("edges_probe_and_queue"),
         "kernel": "edges_probe_kernel + edges_queue_kernel", "kernel_ms": k_ms,
         "peak_source": peak["source"], "flops_per_launch": flops,
         "work_per_launch": dict(zip(["pairs", "exact", "samples", "joints", "spheres", "self", "esdf", "cull"], stats)),
-    }
-    # ---- e2e through the reference-facing bridge (host buffers) ----
+    }, stats
+
+
+def e2e_run(args, b, sc, wl, params):
+    """End-to-end calls of the reference-facing bridge on host buffers
+    (EdgeEvalGpu.evaluate: pinned H2D, kernels, D2H, sync); returns the mean
+    seconds per call and the last call's outputs."""
+    from prismplan_b200 import api
+
+    E = len(wl["from"])
     ev = api.EdgeEvalGpu(7, E, sc, b)
     ff = wl["from"].reshape(-1)
     tt = wl["to"].reshape(-1)
@@ -321,13 +332,48 @@ def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev, timed_out)
         ev.evaluate(ff, tt, E, params)
     t0 = time.perf_counter()
     n_e2e = max(50, 2 * args.steps)   # sub-millisecond host-timed steps: average over many
-    e2e_out = None
+    out = None
     for _ in range(n_e2e):
-        e2e_out = ev.evaluate(ff, tt, E, params)
-    dt = (time.perf_counter() - t0) / n_e2e
-    res["e2e"] = {"value": total_samples / dt, "unit": UNIT, "h2d_bytes_per_step": 2 * E * 7 * 4,
-                  "d2h_bytes_per_step": E * (1 + 4), "ms_per_step": dt * 1e3, "iterations": n_e2e,
-                  "api": "prismplan_b200.EdgeEvalGpu.evaluate (pinned H2D + kernels + D2H + sync)"}
+        out = ev.evaluate(ff, tt, E, params)
+    return (time.perf_counter() - t0) / n_e2e, n_e2e, out
+
+
+def e2e_dict(samples, dt, n_e2e, E, ws=1):
+    return {"value": samples / dt, "unit": UNIT, "h2d_bytes_per_step": 2 * E * 7 * 4 * ws,
+            "d2h_bytes_per_step": E * (1 + 4) * ws, "ms_per_step": dt * 1e3, "iterations": n_e2e,
+            "api": "prismplan_b200.EdgeEvalGpu.evaluate (pinned H2D + kernels + D2H + sync)"}
+
+
+def e2e_all_ranks(args, b, sc, wl, params, ws):
+    """Every rank's bridge on its own edges; the job's samples over the
+    slowest rank's time."""
+    import torch
+    import torch.distributed as dist
+
+    dt, n_e2e, _ = e2e_run(args, b, sc, wl, params)
+    t = torch.tensor([dt, float(wl["G"].sum())], dtype=torch.float64, device="cuda")
+    tmax, tsum = t[:1].clone(), t[1:].clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return e2e_dict(float(tsum.item()), float(tmax.item()), n_e2e, len(wl["from"]), ws)
+
+
+def secondary(args, b, sc, wl, frm, to, params, stream, kern_ms, dev, timed_out):
+    """Roofline, e2e, parity, CPU baseline and the comparison paths (rank 0,
+    N=1 data). timed_out: (valid, cost) of the timed graph replay."""
+    import torch
+
+    from prismplan_b200 import api
+
+    E = len(wl["from"])
+    total_samples = int(wl["G"].sum())
+    res = {}
+    # ---- executed work of one launch (counters) ----
+    res["roofline"], stats = step_roofline(b, sc, frm, to, params, kern_ms, dev)
+    k_ms = res["roofline"]["kernel_ms"]
+    # ---- e2e through the reference-facing bridge (host buffers) ----
+    dt, n_e2e, e2e_out = e2e_run(args, b, sc, wl, params)
+    res["e2e"] = e2e_dict(total_samples, dt, n_e2e, E)
     # ---- plain per-call path (one warp per edge, no queue, no graph) ----
     v_pl = None
     for _ in range(2):
