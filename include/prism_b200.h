@@ -319,6 +319,51 @@ int ps_tune_edges(const ps_model* model, const ps_scene_view* scene,
    time budget ran out. Synchronous (reads the workspace header). */
 int ps_edges_status(const void* workspace, int* status);
 
+/* Host-buffer edge bridge. Replaces ppln::search::EdgeEvalGpu
+   (cpp/src/planning/edge_batch_bridge.hh:27-111): the object owns device
+   buffers for max_edges edges, pinned host mirrors, the persistent path's
+   workspace and a private stream, all allocated at create.
+     ps_edge_bridge_create   <- EdgeEvalGpu(dim, max_edges, scene, model)
+                                (:29-45); dim must equal the model's n_dof.
+                                The scene view is copied (its device pointers
+                                must stay valid); ps_edge_bridge_set_scene
+                                replaces it.
+     ps_edge_bridge_evaluate <- EdgeEvalGpu::evaluate (:60-96): from_flat /
+                                to_flat are HOST row-major [num_edges * dim];
+                                out_valid / out_cost (and out_clearance when
+                                params->compute_clearance) are HOST arrays of
+                                num_edges. Synchronous, like the reference:
+                                stage into the pinned mirrors, copy in, check
+                                (ps_check_edges, replayed from a CUDA graph per
+                                edge count, parameters and scene), copy out,
+                                synchronise. The staging runs in slices and
+                                each slice's copy starts as soon as it is
+                                staged; inputs already in the bridge's own
+                                mirrors (ps_edge_bridge_host_inputs) are not
+                                staged. num_edges <= 0: nothing to do, PS_OK;
+                                num_edges > max_edges: PS_EINVAL (the
+                                reference throws, :67-68).
+     ps_edge_bridge_status   <- PS_ETIMEOUT when the last call's time budget
+                                ran out (ps_edges_status of its workspace).
+     ps_edge_bridge_destroy  <- ~EdgeEvalGpu (:47-53).
+   One bridge per host thread at a time, on the device that was current at
+   create (evaluate returns PS_EINVAL on another). */
+typedef struct ps_edge_bridge ps_edge_bridge;
+int ps_edge_bridge_create(const ps_model* model, const ps_scene_view* scene,
+                          int dim, int max_edges, ps_edge_bridge** out);
+int ps_edge_bridge_set_scene(ps_edge_bridge* bridge, const ps_scene_view* scene);
+int ps_edge_bridge_evaluate(ps_edge_bridge* bridge, const float* from_flat,
+                            const float* to_flat, int num_edges,
+                            const ps_edge_params* params, uint8_t* out_valid,
+                            float* out_cost, float* out_clearance);
+int ps_edge_bridge_status(const ps_edge_bridge* bridge, int* status);
+/* The bridge's pinned host input mirrors (row-major [max_edges * dim]
+   each), valid until destroy. A caller may write its edges there and pass
+   these two pointers to ps_edge_bridge_evaluate, which then skips its staging
+   copy. No reference counterpart (its mirrors are private). */
+int ps_edge_bridge_host_inputs(ps_edge_bridge* bridge, float** from_flat, float** to_flat);
+int ps_edge_bridge_destroy(ps_edge_bridge* bridge);
+
 /* =========================================================================
  * Trajectory cost: summed hinge + self hinge + smoothness, with its exact
  * gradient from a hand-written adjoint.
@@ -407,6 +452,12 @@ typedef struct ps_batch_tuning {
                                 (128 or 256; 4 lanes per waypoint)           */
     int   traj_tile;         /* kept in the record; always 1                  */
     float best_ms;           /* measured time of one launch at this choice    */
+    int   layout;            /* 0: the persistent edge queue and the waypoint
+                                kernel run side by side in two graph branches;
+                                1: one persistent work-queue kernel pulls
+                                edge chunks and waypoint groups (trajectories
+                                and rollouts) from global counters          */
+    int   work_threads;      /* threads per block of that kernel (128, 256)  */
 } ps_batch_tuning;
 
 int ps_batch_create(const ps_model* model, const ps_batch_limits* limits,
@@ -441,6 +492,10 @@ int ps_batch_launch(ps_batch* batch, const ps_scene_view* scene,
    batch's current requests, keeps the fastest for later launches and
    reports it (out may be NULL). Synchronous; launches the batch several
    times. */
+/* Use this launch shape from the next launch on (for example one that
+   ps_batch_tune returned earlier); best_ms and traj_tile are ignored.
+   Shares in (0, 1], thread counts 128 or 256, layout 0 or 1. */
+int ps_batch_set_shape(ps_batch* batch, const ps_batch_tuning* shape);
 int ps_batch_tune(ps_batch* batch, const ps_scene_view* scene,
                   const ps_edge_params* params, const ps_cost_params* cost,
                   ps_batch_tuning* out);

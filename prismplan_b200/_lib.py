@@ -145,6 +145,7 @@ class BatchTuning(C.Structure):
     _fields_ = [
         ("edge_share", C.c_float), ("traj_share", C.c_float),
         ("traj_threads", C.c_int), ("traj_tile", C.c_int), ("best_ms", C.c_float),
+        ("layout", C.c_int), ("work_threads", C.c_int),
     ]
 
 
@@ -219,6 +220,15 @@ _SIGNATURES = [
      [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_int, C.c_int,
       C.POINTER(CostParams), C.c_int, C.c_void_p, C.c_void_p]),
     ("ps_edges_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    ("ps_edge_bridge_create", C.c_int,
+     [C.c_void_p, C.POINTER(SceneView), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    ("ps_edge_bridge_set_scene", C.c_int, [C.c_void_p, C.POINTER(SceneView)]),
+    ("ps_edge_bridge_evaluate", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(EdgeParams), C.c_void_p, C.c_void_p,
+      C.c_void_p]),
+    ("ps_edge_bridge_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    ("ps_edge_bridge_host_inputs", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    ("ps_edge_bridge_destroy", C.c_int, [C.c_void_p]),
     ("ps_batch_create", C.c_int, [C.c_void_p, C.POINTER(BatchLimits), C.POINTER(C.c_void_p)]),
     ("ps_batch_destroy", C.c_int, [C.c_void_p]),
     ("ps_batch_clear", C.c_int, [C.c_void_p]),
@@ -230,6 +240,7 @@ _SIGNATURES = [
     ("ps_batch_launch", C.c_int,
      [C.c_void_p, C.POINTER(SceneView), C.POINTER(EdgeParams), C.POINTER(CostParams), C.c_void_p]),
     ("ps_batch_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    ("ps_batch_set_shape", C.c_int, [C.c_void_p, C.POINTER(BatchTuning)]),
     ("ps_batch_tune", C.c_int,
      [C.c_void_p, C.POINTER(SceneView), C.POINTER(EdgeParams), C.POINTER(CostParams),
       C.POINTER(BatchTuning)]),

@@ -276,75 +276,77 @@ def tune_configs(robot: RobotModelBuilder, scene, q, collision_margin: float = 0
 
 
 class EdgeEvalGpu:
-    """Drop-in for ppln::search::EdgeEvalGpu (edge_batch_bridge.hh:27-111):
-    persistent device buffers, pinned host mirrors and a private stream;
-    ``evaluate`` copies in, runs the persistent edge kernel, copies out and
-    synchronises. Raises on num_edges > max_edges like the reference (:67-68)."""
+    """Drop-in for ppln::search::EdgeEvalGpu (edge_batch_bridge.hh:27-111)
+    over the library's native bridge (ps_edge_bridge_*): device buffers,
+    pinned host mirrors, the persistent path's workspace and a private stream
+    owned by the library. ``evaluate`` hands the host arrays to the bridge,
+    which stages them into its pinned mirrors (OpenMP threads), copies them
+    in, runs the persistent edge check from a CUDA graph per (num_edges,
+    params), copies the outputs back and synchronises. The scene is held as built at
+    construction, like the reference's by-value SceneCollisionData;
+    ``set_scene`` replaces it. Raises on num_edges > max_edges like the
+    reference (:67-68)."""
 
     def __init__(self, dim: int, max_edges: int, scene, model: RobotModelBuilder):
-        torch = _torch()
         self.dim, self.max_edges, self.scene, self.model = int(dim), int(max_edges), scene, model
         if model.n_dof != self.dim:
             raise ValueError("dim must equal the robot's n_dof")
-        dev = torch.device("cuda")
-        self._from = torch.empty((self.max_edges, self.dim), dtype=torch.float32, device=dev)
-        self._to = torch.empty_like(self._from)
-        self._valid = torch.empty(self.max_edges, dtype=torch.uint8, device=dev)
-        self._cost = torch.empty(self.max_edges, dtype=torch.float32, device=dev)
-        self._clr = torch.empty(self.max_edges, dtype=torch.float32, device=dev)
-        self._ws = edges_workspace(self.max_edges, dev)
-        self._h_from = torch.empty((self.max_edges, self.dim), dtype=torch.float32).pin_memory()
-        self._h_to = torch.empty_like(self._h_from).pin_memory()
-        self._h_out = torch.empty((3, self.max_edges), dtype=torch.float32).pin_memory()
-        self._h_valid = torch.empty(self.max_edges, dtype=torch.uint8).pin_memory()
-        self._stream = torch.cuda.Stream()
-        self._graphs = {}
+        self._lib = _lib.load()
+        self._view = _view(scene)
+        h = C.c_void_p()
+        _lib.check(self._lib.ps_edge_bridge_create(_model(model), C.byref(self._view), self.dim, self.max_edges,
+                                                   C.byref(h)))
+        self._h = h
+        self._params_key = None
+        self._params_c = None
 
-    def _enqueue(self, n: int, params: EdgeEvalParams):
-        torch = _torch()
-        with torch.cuda.stream(self._stream):
-            self._from[:n].copy_(self._h_from[:n], non_blocking=True)
-            self._to[:n].copy_(self._h_to[:n], non_blocking=True)
-            check_edges(self.model, self.scene, self._from[:n], self._to[:n], params=params, workspace=self._ws,
-                        out=(self._valid[:n], self._cost[:n], self._clr[:n]), stream=self._stream)
-            self._h_valid[:n].copy_(self._valid[:n], non_blocking=True)
-            self._h_out[0, :n].copy_(self._cost[:n], non_blocking=True)
-            if params.compute_clearance:
-                self._h_out[1, :n].copy_(self._clr[:n], non_blocking=True)
+    def set_scene(self, scene) -> None:
+        """Use another scene (its tensors must outlive the calls)."""
+        view = _view(scene)
+        _lib.check(self._lib.ps_edge_bridge_set_scene(self._h, C.byref(view)))
+        self.scene, self._view = scene, view
 
     def evaluate(self, from_flat, to_flat, num_edges: int, params: EdgeEvalParams):
-        """Copy in, check, copy out, synchronise. The copies and launches of
-        each (num_edges, params) seen before are replayed from a CUDA graph
-        (one launch instead of a dozen API calls); the first call of a key
-        runs eagerly and captures."""
-        torch = _torch()
+        """Copy in, check, copy out, synchronise; returns host arrays
+        (valid uint8 [n], cost float32 [n], clearance float32 [n] when
+        params.compute_clearance else empty)."""
         n = int(num_edges)
         if n <= 0:
             return np.zeros(0, np.uint8), np.zeros(0, np.float32), np.zeros(0, np.float32)
         if n > self.max_edges:
             raise RuntimeError("EdgeEvalGpu: num_edges exceeds max_edges_")
-        self._h_from[:n].copy_(torch.from_numpy(np.asarray(from_flat, np.float32).reshape(-1, self.dim)[:n]))
-        self._h_to[:n].copy_(torch.from_numpy(np.asarray(to_flat, np.float32).reshape(-1, self.dim)[:n]))
-        key = (n, tuple(sorted(vars(params).items())))
-        graph = self._graphs.get(key)
-        if graph is None:
-            self._enqueue(n, params)
-            self._stream.synchronize()
-            graph = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(graph, stream=self._stream):
-                self._enqueue(n, params)
-            if len(self._graphs) >= 8:   # small LRU of captured sizes
-                self._graphs.pop(next(iter(self._graphs)))
-            self._graphs[key] = graph
-        else:
-            self._graphs[key] = self._graphs.pop(key)
-        with torch.cuda.stream(self._stream):   # replay on the stream synchronised below
-            graph.replay()
-        self._stream.synchronize()
-        valid = self._h_valid[:n].numpy().copy()
-        cost = self._h_out[0, :n].numpy().copy()
-        clr = self._h_out[1, :n].numpy().copy() if params.compute_clearance else np.zeros(0, np.float32)
+        f = np.ascontiguousarray(from_flat, dtype=np.float32)
+        t = np.ascontiguousarray(to_flat, dtype=np.float32)
+        k = n * self.dim
+        if f.size < k or t.size < k:
+            raise ValueError("from_flat/to_flat hold fewer than num_edges * dim values")
+        key = tuple(vars(params).values())
+        if key != self._params_key:
+            self._params_c, self._params_key = params.to_c(), key
+        valid = np.empty(n, np.uint8)
+        cost = np.empty(n, np.float32)
+        clr = np.empty(n, np.float32) if params.compute_clearance else np.zeros(0, np.float32)
+        _lib.check(self._lib.ps_edge_bridge_evaluate(self._h, f.ctypes.data, t.ctypes.data, n,
+                                                     C.byref(self._params_c), valid.ctypes.data, cost.ctypes.data,
+                                                     clr.ctypes.data if params.compute_clearance else None))
         return valid, cost, clr
+
+    def status(self) -> int:
+        """PS_ETIMEOUT when the last call's time budget ran out, else PS_OK."""
+        code = C.c_int(0)
+        _lib.check(self._lib.ps_edge_bridge_status(self._h, C.byref(code)))
+        return code.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.ps_edge_bridge_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------
@@ -751,14 +753,27 @@ class MixedBatch:
 
     def tune(self, scene, edge_params: Optional[EdgeEvalParams] = None,
              cost_params: Optional[CostParams] = None) -> dict:
-        """Autotune the SM split and trajectory tile width on the queued requests."""
+        """Autotune the launch shape on the queued requests: the one
+        work-queue kernel (128 or 256 threads per block) against the edge
+        queue and waypoint kernel side by side (SM shares, block width).
+        Returns the chosen shape; later launches use it."""
         ep = (edge_params or EdgeEvalParams()).to_c()
         cp = (cost_params or CostParams()).to_c(_lib.PS_LAYOUT_BTD)
         v = _view(scene)
         t = _lib.BatchTuning()
         _lib.check(_lib.load().ps_batch_tune(self.handle, C.byref(v), C.byref(ep), C.byref(cp), C.byref(t)))
-        return {"edge_share": t.edge_share, "traj_share": t.traj_share, "traj_threads": t.traj_threads,
-                "traj_tile": t.traj_tile, "best_ms": t.best_ms}
+        return {name: getattr(t, name) for name, _ in t._fields_}
+
+    def set_shape(self, layout: int = 0, work_threads: int = 256, edge_share: float = 1.0, traj_share: float = 0.5,
+                  traj_threads: int = 256) -> None:
+        """Launch shape for the next launches: layout 1 = one work-queue
+        kernel for edge chunks and waypoint groups; 0 = the persistent edge
+        queue and the waypoint kernel side by side. Results do not depend
+        on it."""
+        t = _lib.BatchTuning()
+        t.edge_share, t.traj_share, t.traj_threads, t.traj_tile = edge_share, traj_share, traj_threads, 1
+        t.layout, t.work_threads = layout, work_threads
+        _lib.check(_lib.load().ps_batch_set_shape(self.handle, C.byref(t)))
 
     def close(self):
         if self._h is not None:

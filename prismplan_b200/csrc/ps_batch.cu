@@ -183,6 +183,183 @@ __global__ void __launch_bounds__(kWarps * 32, 16 / kWarps) batch_waypoint_kerne
     }
 }
 
+// Per-warp scratch of the work-queue kernel: a warp holds either an edge
+// chunk (32 configurations and the broad phase's candidate list) or a
+// waypoint group (the lane-group scratch), one at a time.
+__host__ __device__ inline size_t work_warp_bytes(int NJ, int NS, int D, int n_obbs) {
+    const size_t edge = (size_t)32 * D * 4 + (size_t)((std::max(n_obbs, 1) + 7) & ~7) * 2;
+    const size_t cost = lane_warp_bytes(NJ, NS, D, n_obbs, true);
+    return ((edge > cost ? edge : cost) + 15) & ~size_t(15);
+}
+
+size_t work_smem_bytes(const ps_model* m, const ps_scene_view* sv, int warps) {
+    const size_t tables = lane_block_bytes(m, sv, 0, true);
+    return tables + (size_t)warps * work_warp_bytes(m->info.n_joints, m->info.n_spheres, m->info.n_dof, sv->n_obbs);
+}
+
+// The whole batch as one persistent work queue. Every warp pulls, from
+// global counters, first the persistent edge path's chunk-major items of
+// this pass (hdr->head[pass]: a chunk of 32 consecutive samples of one edge,
+// skipped once the edge is retired), then, in pass 0, waypoint groups
+// (hdr->wp_next: kCostSlots consecutive packed waypoints; trajectory groups
+// with the adjoint, rollout groups without it), until both are drained.
+// Pass 1 holds the later chunk rounds when the edges are too few to keep
+// round 0 ahead of them (the persistent edge path's split rule). The edge
+// items are processed exactly as by edges_queue_kernel and the waypoint
+// groups exactly as by batch_waypoint_kernel, so every output has the same
+// bits as with the two kernels side by side.
+template <int kMode, int kW>
+__global__ void __launch_bounds__(kW * 32, 16 / kW)
+    batch_work_kernel(ModelDev md, ps_scene_view sv, ps_edge_params EP, ps_cost_params CP,
+                      const Counts* __restrict__ cnt, const float* __restrict__ from, const float* __restrict__ to,
+                      EdgeWs* hdr, const int* __restrict__ Gs, int* bad, int* clr, int* done,
+                      const float* __restrict__ q, float* __restrict__ wp_cost, float* __restrict__ grad, int cap,
+                      int pass) {
+    const int n_edges = cnt->n_edges, n_wp = cnt->n_wp, n_roll = cnt->n_roll;
+    const int chunks_a = (n_wp + kCostSlots - 1) / kCostSlots;
+    const int chunks = pass == 0 ? chunks_a + (n_roll + kCostSlots - 1) / kCostSlots : 0;
+    const int max_rounds = *((volatile int*)&hdr->max_rounds);
+    const bool split = (long long)n_edges < 8ll * gridDim.x * kW;
+    const int r_lo = pass == 0 ? 0 : (split ? 1 : max_rounds);
+    const int r_hi = pass == 0 ? (split ? min(max_rounds, 1) : max_rounds) : max_rounds;
+    const long long total = (long long)max(r_hi - r_lo, 0) * n_edges;   // edge items of this pass
+    if (total == 0 && chunks == 0) return;   // uniform over the grid: nothing staged yet
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ int counters[4];
+    __shared__ float bmax;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int slot = lane / kCostSub, u = lane % kCostSub;
+    if (!stage_model(md, smem, &mbar)) {
+        // fail closed: the edges come back invalid (finalize, timed_out) and
+        // the waypoint groups this block pulls NaN
+        if (threadIdx.x == 0 && total > 0) atomicExch(&hdr->timed_out, 1);
+        const int D = reinterpret_cast<const BlobHeader*>(md.blob)->n_dof;
+        const float nan = __int_as_float(0x7fc00000);
+        for (;;) {
+            int c = 0;
+            if (lane == 0) c = atomicAdd(&hdr->wp_next, 1);
+            c = __shfl_sync(kFull, c, 0);
+            if (c >= chunks) break;
+            const bool traj = c < chunks_a;
+            const int lo = traj ? 0 : cap - n_roll, hi = traj ? n_wp : cap;
+            const int k = lo + (traj ? c : c - chunks_a) * kCostSlots + slot;
+            if (k < hi) {
+                if (u == 0) wp_cost[k] = nan;
+                if (traj)
+                    for (int d = u; d < D; d += kCostSub) grad[(size_t)k * D + d] = nan;
+            }
+        }
+        return;
+    }
+    const ModelSmem M = model_view(smem);
+    const int D = M.H->n_dof, NJ = M.H->n_joints, NS = M.H->n_spheres;
+    ObbPrep* obbs = reinterpret_cast<ObbPrep*>(smem + md.bytes_core);
+    const int nob = max(sv.n_obbs, 1);
+    int* orig = reinterpret_cast<int*>(obbs + nob);
+    LayerPrep* layers = reinterpret_cast<LayerPrep*>(orig + ((nob + 3) & ~3));
+    SceneSmem sc;
+    stage_scene(sv, obbs, orig, layers, counters, &bmax, sc);
+    const CostBlock cb = cost_block_setup(reinterpret_cast<unsigned char*>(layers + PS_MAX_LAYERS), M, sc, sv.n_obbs);
+    __syncthreads();
+    box_limits(sc, const_cast<float4*>(cb.obs));
+    __syncthreads();
+    unsigned char* wbase = reinterpret_cast<unsigned char*>(cb.wbase) + (size_t)warp * work_warp_bytes(NJ, NS, D, sv.n_obbs);
+    LaneStats st;
+    st.zero();
+
+    // ---- edge chunk items (edges_queue_kernel's loop) ----
+    if (total > 0) {
+        float* eq = reinterpret_cast<float*>(wbase);
+        WarpScratch ws{eq, reinterpret_cast<uint16_t*>(eq + 32 * D), cb.obs};
+        unsigned long long* head = &hdr->head[pass == 0 ? 0 : 1];
+        const unsigned long long deadline = *((volatile unsigned long long*)&hdr->deadline);
+        const int grab = EP.grab > 0 ? min(EP.grab, 32) : (int)max(1ll, min(32ll, total / ((long long)gridDim.x * kW * 2)));
+        volatile int* vbad = bad;
+        for (;;) {
+            unsigned long long base = 0;
+            if (lane == 0) {
+                if (deadline && global_ns() > deadline) {
+                    atomicExch(&hdr->timed_out, 1);
+                    base = (unsigned long long)total;
+                } else {
+                    base = atomicAdd(head, (unsigned long long)grab);
+                }
+            }
+            base = __shfl_sync(kFull, base, 0);
+            if ((long long)base >= total) break;
+            const long long item = (long long)base + lane;
+            int e = -1, k = 0, G = 0;
+            bool live = false;
+            if (lane < grab && item < total) {
+                if (total < (1ll << 31)) {   // 32-bit division in the common case
+                    k = (int)((unsigned)item / (unsigned)n_edges);
+                    e = (int)((unsigned)item - (unsigned)k * (unsigned)n_edges);
+                } else {
+                    k = (int)(item / n_edges);
+                    e = (int)(item - (long long)k * n_edges);
+                }
+                k += r_lo;
+                G = __ldg(Gs + e);
+                const ChunkOrder ord(G);
+                if (k < ord.rounds()) {
+                    k = ord.chunk(k);
+                    live = k < ord.nc && (EP.compute_clearance || vbad[e] == 0);
+                }
+            }
+            unsigned todo = __ballot_sync(kFull, live);
+            while (todo) {
+                const int src = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const int ee = __shfl_sync(kFull, e, src);
+                const int kk = __shfl_sync(kFull, k, src);
+                const int GG = __shfl_sync(kFull, G, src);
+                int retired = 0;
+                if (lane == 0) retired = vbad[ee];
+                retired = __shfl_sync(kFull, retired, 0);
+                if (!EP.compute_clearance && retired) continue;
+                float cm = FLT_MAX;
+                const bool h = kMode ? process_chunk_fast<false, kMode == 2>(M, sc, sv, EP, from, to, ee, GG, kk, ws, st)
+                                     : process_chunk(M, sc, sv, EP, from, to, ee, GG, kk, ws,
+                                                     EP.compute_clearance ? &cm : nullptr, st);
+                if (lane == 0) {
+                    if (h) vbad[ee] = 1;
+                    if (EP.compute_clearance) atomicMin(clr + ee, ordered_float(cm));
+                    if (deadline) atomicAdd(done + ee, 1);
+                }
+            }
+        }
+    }
+
+    // ---- waypoint groups (batch_waypoint_kernel's loop) ----
+    if (chunks > 0) {
+        const LaneScratch ws = lane_carve(wbase, NJ, NS, D, true);
+        for (;;) {
+            int c = 0;
+            if (lane == 0) c = atomicAdd(&hdr->wp_next, 1);
+            c = __shfl_sync(kFull, c, 0);
+            if (c >= chunks) break;
+            const bool traj = c < chunks_a;   // uniform over the warp
+            const int lo = traj ? 0 : cap - n_roll, hi = traj ? n_wp : cap;
+            const int k = lo + (traj ? c : c - chunks_a) * kCostSlots + slot;
+            const int kc = k < hi ? k : hi - 1;   // past the end: repeat the last waypoint
+            __syncwarp();   // the previous group's readers of the scratch are done
+            for (int d = u; d < D; d += kCostSub) ws.q[d * kCostSlots + slot] = q[(size_t)kc * D + d];
+            __syncwarp();
+            if (traj) {
+                const float v = lane_cost<true, false>(M, md, sc, sv, CP, cb, ws, st);
+                if (k < hi) {
+                    if (u == 0) wp_cost[k] = v;
+                    lane_write_grad(M, cb, ws, grad + (size_t)k * D, 1);
+                }
+            } else {
+                const float v = lane_cost<false, false>(M, md, sc, sv, CP, cb, ws, st);
+                if (k < hi && u == 0) wp_cost[k] = v;
+            }
+        }
+    }
+}
+
 // One block per trajectory request: outputs waypoint costs, the gradient
 // (adjoint + smoothness) and the total, exactly as ps_traj_cost computes them.
 __global__ void __launch_bounds__(kFinishThreads) batch_traj_finish(const TrajReq* __restrict__ req,
@@ -260,6 +437,8 @@ struct ps_batch {
     float traj_share = 0.5f;   // of the trajectory kernel's full-occupancy grid
     int traj_threads = 256;   // threads per block of the trajectory kernel (kCostSub per waypoint)
     int traj_tile = 1;        // kept for the tuning record: always 1
+    int layout = 0;           // 0: edge queue and waypoint kernel side by side; 1: one work-queue kernel
+    int work_threads = 256;   // threads per block of the work-queue kernel
 };
 
 namespace {
@@ -269,10 +448,20 @@ struct LaunchPlan {
     void (*qk)(ModelDev, ps_scene_view, ps_edge_params, const float*, const float*, int, EdgeWs*, const int*, int*,
                int*, int*, unsigned long long*, int, const int*) = nullptr;
     void (*wk)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*, int) = nullptr;
-    size_t qsmem = 0, wsmem = 0, fsmem = 0, ssmem = 0;
-    int qgrid = 1, wgrid = 1, req_grid_e = 1, req_grid_t = 1, pgrid = 1, sgrid = 1;
+    void (*work)(ModelDev, ps_scene_view, ps_edge_params, ps_cost_params, const Counts*, const float*, const float*,
+                 EdgeWs*, const int*, int*, int*, int*, const float*, float*, float*, int, int) = nullptr;
+    size_t qsmem = 0, wsmem = 0, fsmem = 0, ssmem = 0, ksmem = 0;
+    int qgrid = 1, wgrid = 1, req_grid_e = 1, req_grid_t = 1, pgrid = 1, sgrid = 1, kgrid = 1;
     ProbePlan probe;
 };
+
+using WorkKernel = decltype(LaunchPlan::work);
+
+WorkKernel pick_work_kernel(int mode, int threads) {
+    if (threads == 128)
+        return mode == 1 ? batch_work_kernel<1, 4> : (mode == 2 ? batch_work_kernel<2, 4> : batch_work_kernel<0, 4>);
+    return mode == 1 ? batch_work_kernel<1, 8> : (mode == 2 ? batch_work_kernel<2, 8> : batch_work_kernel<0, 8>);
+}
 
 using WaypointKernel = void (*)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*,
                                 int);
@@ -326,7 +515,58 @@ int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, 
             PS_TRY_CUDA(allow_smem((const void*)batch_traj_finish, L.fsmem));
         L.req_grid_t = std::max(1, std::min(b->lim.max_traj_requests, sms * 8));
     }
+    if (b->layout == 1) {   // one work-queue kernel for edge chunks and waypoint groups
+        const int mode = b->lim.max_edges > 0 ? L.mode : 1;
+        const int kt = b->work_threads;
+        L.work = pick_work_kernel(mode, kt);
+        L.ksmem = work_smem_bytes(m, sv, kt / 32);
+        PS_TRY_CUDA(allow_smem((const void*)L.work, L.ksmem));
+        int per_sm = 0;
+        PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L.work, kt, L.ksmem));
+        if (per_sm < 1) return set_error(PS_EINVAL, "work-queue kernel does not fit on an SM with this model/scene");
+        L.kgrid = std::max(1, sms * per_sm);
+    }
     return PS_OK;
+}
+
+// Layout 1: one stream; gathers, edge prep and the end-sample probe, then
+// the work-queue kernel (pass 0: edge items of round 0, or of every round,
+// and every waypoint group; pass 1: the later rounds when split), the self
+// pass, finalize, scatter and the trajectory outputs.
+void record_work_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, const ps_cost_params* cp,
+                       const LaunchPlan& L) {
+    const ps_model* m = b->model;
+    const int D = m->info.n_dof;
+    cudaStream_t s0 = b->cap0;
+    const int* n_dev = &b->d_cnt->n_edges;
+    const bool edges = b->lim.max_edges > 0, trajs = b->lim.max_waypoints > 0;
+    cudaMemsetAsync(b->d_hdr, 0, sizeof(EdgeWs), s0);
+    if (edges) {
+        batch_gather_edges<<<L.req_grid_e, 128, 0, s0>>>(b->d_ereq, b->d_cnt, *ep, D, b->d_from, b->d_to, b->d_given);
+        edges_prep_kernel<<<L.pgrid, 256, 0, s0>>>(*ep, b->d_from, b->d_to, b->d_given, b->lim.max_edges, D, b->d_hdr,
+                                                   b->d_G, b->d_len, b->d_bad, b->d_clr, b->d_done, n_dev);
+        if (L.probe.k)
+            L.probe.k<<<L.probe.grid, kProbeThreads, L.probe.smem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to,
+                                                                          b->lim.max_edges, b->d_hdr, b->d_G,
+                                                                          b->d_bad, nullptr, n_dev);
+    }
+    if (trajs) batch_gather_traj<<<L.req_grid_t, 128, 0, s0>>>(b->d_treq, b->d_cnt, D, b->d_q);
+    for (int pass = 0; pass < 2; ++pass)
+        L.work<<<L.kgrid, b->work_threads, L.ksmem, s0>>>(m->dev, *sv, *ep, *cp, b->d_cnt, b->d_from, b->d_to,
+                                                          b->d_hdr, b->d_G, b->d_bad, b->d_clr, b->d_done, b->d_q,
+                                                          b->d_wp_cost, b->d_grad, b->lim.max_waypoints, pass);
+    if (edges) {
+        if (ep->check_self)
+            edges_self_kernel<<<L.sgrid, kSelfThreads, L.ssmem, s0>>>(m->dev, *ep, b->d_from, b->d_to, b->d_given,
+                                                                      b->lim.max_edges, b->d_G, b->d_bad, nullptr,
+                                                                      nullptr, b->d_hdr, nullptr, n_dev);
+        edges_finalize_kernel<<<L.pgrid, 256, 0, s0>>>(b->lim.max_edges, *ep, b->d_bad, b->d_len, b->d_clr, b->d_done,
+                                                       b->d_G, b->d_hdr, b->d_valid, b->d_cost, nullptr, n_dev);
+        batch_scatter_edges<<<L.req_grid_e, 128, 0, s0>>>(b->d_ereq, b->d_cnt, b->d_valid, b->d_cost);
+    }
+    if (trajs)
+        batch_traj_finish<<<L.req_grid_t, kFinishThreads, L.fsmem, s0>>>(b->d_treq, b->d_cnt, D, *cp, b->d_q,
+                                                                         b->d_wp_cost, b->d_grad);
 }
 
 void record_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, const ps_cost_params* cp,
@@ -339,6 +579,10 @@ void record_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep
     cudaMemcpyAsync(b->d_treq, b->h_treq, sizeof(TrajReq) * std::max(b->lim.max_traj_requests, 1),
                     cudaMemcpyHostToDevice, s0);
     cudaMemcpyAsync(b->d_cnt, b->h_cnt, sizeof(Counts), cudaMemcpyHostToDevice, s0);
+    if (b->layout == 1) {
+        record_work_graph(b, sv, ep, cp, L);
+        return;
+    }
     cudaEventRecord(b->fork, s0);
     cudaStreamWaitEvent(s1, b->fork, 0);
     if (b->lim.max_edges > 0) {   // edge branch on s0
@@ -396,7 +640,7 @@ int batch_capture(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep
 
 std::vector<unsigned char> make_key(const ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep,
                                     const ps_cost_params* cp) {
-    std::vector<unsigned char> k(sizeof(*sv) + sizeof(*ep) + sizeof(*cp) + 2 * sizeof(float) + 3 * sizeof(int));
+    std::vector<unsigned char> k(sizeof(*sv) + sizeof(*ep) + sizeof(*cp) + 2 * sizeof(float) + 5 * sizeof(int));
     unsigned char* p = k.data();
     auto put = [&](const void* src, size_t n) {
         std::memcpy(p, src, n);
@@ -409,6 +653,8 @@ std::vector<unsigned char> make_key(const ps_batch* b, const ps_scene_view* sv, 
     put(&b->traj_share, sizeof(float));
     put(&b->traj_threads, sizeof(int));
     put(&b->traj_tile, sizeof(int));
+    put(&b->layout, sizeof(int));
+    put(&b->work_threads, sizeof(int));
     put(&b->model->dev.stage_polls, sizeof(int));   // kernels get the model by value at capture
     return k;
 }
@@ -605,6 +851,25 @@ extern "C" int ps_batch_status(ps_batch* b, int* status) {
     return PS_OK;
 }
 
+extern "C" int ps_batch_set_shape(ps_batch* b, const ps_batch_tuning* shape) {
+    clear_error();
+    if (!b || !shape) return set_error(PS_EINVAL, "NULL argument");
+    if (!(shape->edge_share > 0.0f && shape->edge_share <= 1.0f) ||
+        !(shape->traj_share > 0.0f && shape->traj_share <= 1.0f))
+        return set_error(PS_EINVAL, "edge_share and traj_share must lie in (0, 1]");
+    if ((shape->traj_threads != 128 && shape->traj_threads != 256) ||
+        (shape->work_threads != 128 && shape->work_threads != 256))
+        return set_error(PS_EINVAL, "traj_threads and work_threads must be 128 or 256");
+    if (shape->layout != 0 && shape->layout != 1) return set_error(PS_EINVAL, "layout must be 0 or 1");
+    b->edge_share = shape->edge_share;
+    b->traj_share = shape->traj_share;
+    b->traj_threads = shape->traj_threads;
+    b->traj_tile = 1;
+    b->layout = shape->layout;
+    b->work_threads = shape->work_threads;
+    return PS_OK;   // the next launch captures a graph for the new shape
+}
+
 extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep,
                              const ps_cost_params* cp, ps_batch_tuning* out) {
     PS_NVTX("ps_batch_tune");
@@ -624,12 +889,41 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
         return cuda_error(le, "tuning events");
     }
     const float keep_e = b->edge_share, keep_t = b->traj_share;
-    const int keep_w = b->traj_threads, keep_tile = b->traj_tile;
+    const int keep_w = b->traj_threads, keep_tile = b->traj_tile, keep_l = b->layout, keep_k = b->work_threads;
     float best = 3.0e38f, best_e = keep_e, best_t = keep_t;
-    int best_w = keep_w, best_tile = keep_tile;
+    int best_w = keep_w, best_tile = keep_tile, best_l = keep_l, best_k = keep_k;
     int rc = PS_OK;
     const bool edges = b->lim.max_edges > 0, trajs = b->lim.max_waypoints > 0;
+    auto time_now = [&](float& ms_min) {   // capture + warm-up, then the best of 3 launches
+        int r = ps_batch_launch(b, sv, ep, cp, s);
+        ms_min = 3.0e38f;
+        for (int k = 0; k < 3 && r == PS_OK; ++k) {
+            cudaEventRecord(a, s);
+            r = ps_batch_launch(b, sv, ep, cp, s);
+            cudaEventRecord(z, s);
+            if (cudaEventSynchronize(z) != cudaSuccess) r = cuda_error(cudaGetLastError(), "tuning run");
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, a, z);
+            ms_min = std::min(ms_min, ms);
+        }
+        return r;
+    };
+    // layout 1: one work-queue kernel, 128 or 256 threads per block
+    b->layout = 1;
+    for (int kt : widths) {
+        b->work_threads = kt;
+        float ms_min = 0.0f;
+        rc = time_now(ms_min);
+        if (rc) break;
+        if (ms_min < best) {
+            best = ms_min;
+            best_l = 1;
+            best_k = kt;
+        }
+    }
+    b->layout = 0;
     for (float es : edge_shares) {
+        if (rc) break;
         if (!edges && es != 1.0f) continue;
         for (float ts : traj_shares) {
             for (int w : widths) {
@@ -639,21 +933,12 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
                     b->traj_share = ts;
                     b->traj_threads = w;
                     b->traj_tile = tl;
-                    rc = ps_batch_launch(b, sv, ep, cp, s);   // capture + warm-up
-                    if (rc) break;
-                    float ms_min = 3.0e38f;
-                    for (int r = 0; r < 3 && rc == PS_OK; ++r) {
-                        cudaEventRecord(a, s);
-                        rc = ps_batch_launch(b, sv, ep, cp, s);
-                        cudaEventRecord(z, s);
-                        if (cudaEventSynchronize(z) != cudaSuccess) rc = cuda_error(cudaGetLastError(), "tuning run");
-                        float ms = 0.0f;
-                        cudaEventElapsedTime(&ms, a, z);
-                        ms_min = std::min(ms_min, ms);
-                    }
+                    float ms_min = 0.0f;
+                    rc = time_now(ms_min);
                     if (rc) break;
                     if (ms_min < best) {
                         best = ms_min;
+                        best_l = 0;
                         best_e = es;
                         best_t = ts;
                         best_w = w;
@@ -675,18 +960,24 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
         b->traj_share = keep_t;
         b->traj_threads = keep_w;
         b->traj_tile = keep_tile;
+        b->layout = keep_l;
+        b->work_threads = keep_k;
         return rc;
     }
     b->edge_share = best_e;
     b->traj_share = best_t;
     b->traj_threads = best_w;
     b->traj_tile = best_tile;
+    b->layout = best_l;
+    b->work_threads = best_k;
     if (out) {
         out->edge_share = best_e;
         out->traj_share = best_t;
         out->traj_threads = best_w;
         out->traj_tile = best_tile;
         out->best_ms = best;
+        out->layout = best_l;
+        out->work_threads = best_k;
     }
     return PS_OK;
 }

@@ -25,7 +25,8 @@ struct EdgeWs {                         // header of the persistent workspace (6
     int timed_out;                      // set once a queue kernel stops at the deadline
     int self_edges;                     // edges with at least one sample
     int self_next;                      // next window of the self pass
-    int pad[4];
+    int wp_next;                        // next waypoint group (the batch's work-queue kernel)
+    int pad[3];
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {

@@ -54,6 +54,16 @@ def _check_against_calls(b, sc, frm, to, reqs, trajs, ep, cp):
         assert torch.equal(g.view(torch.int32), g1[0].view(torch.int32))
 
 
+# Launch shapes: the default (the edge queue and the waypoint kernel side by
+# side) and the one work-queue kernel (layout 1) at both block widths.
+SHAPES = [None, (1, 128), (1, 256)]
+
+
+def _shape(batch, shape):
+    if shape is not None:
+        batch.set_shape(layout=shape[0], work_threads=shape[1])
+
+
 @pytest.fixture(scope="module")
 def w5():
     wl = workloads.workload(5, scale=1.0 / 4)
@@ -62,10 +72,12 @@ def w5():
     return wl, b, sc
 
 
-def test_batch_equals_per_request_calls(w5):
+@pytest.mark.parametrize("shape", SHAPES)
+def test_batch_equals_per_request_calls(w5, shape):
     wl, b, sc = w5
     nw = sum(len(q) for q in wl["trajectories"])
     batch = api.MixedBatch(b, len(wl["edge_splits"]), len(wl["from"]), len(wl["trajectories"]), nw, 128)
+    _shape(batch, shape)
     frm, to, reqs, trajs = _fill(batch, wl)
     ep = api.EdgeEvalParams(max_joint_step=0.01, max_samples=600)
     cp = _cost_params(wl, smooth=0.5)
@@ -81,11 +93,13 @@ def test_batch_equals_per_request_calls(w5):
     batch.close()
 
 
-def test_batch_edges_bitexact_vs_reference(w5):
+@pytest.mark.parametrize("shape", SHAPES)
+def test_batch_edges_bitexact_vs_reference(w5, shape):
     wl, b, sc = w5
     ref = oracle.RefKernels(b, *wl["obbs"], esdf=wl["esdf"])
     n = len(wl["from"])
     batch = api.MixedBatch(b, len(wl["edge_splits"]), n, 0, 0, 0)
+    _shape(batch, shape)
     frm, to, reqs, _ = _fill(batch, wl, n_traj=0, given_every=1)
     batch.launch(sc, api.EdgeEvalParams(), api.CostParams())
     torch.cuda.synchronize()
@@ -98,7 +112,8 @@ def test_batch_edges_bitexact_vs_reference(w5):
     batch.close()
 
 
-def test_batch_fast_path_panda(w5):
+@pytest.mark.parametrize("shape", SHAPES)
+def test_batch_fast_path_panda(w5, shape):
     """Panda-like chain (the single-frame fast edge kernel) with OBBs only."""
     wl2 = workloads.workload(2, scale=1.0 / 16)
     wl3 = workloads.workload(3, scale=1.0 / 16)
@@ -116,6 +131,7 @@ def test_batch_fast_path_panda(w5):
           "trajectories": list(wl3["q"]), "w": wl3["w"], "eps": wl3["eps"], "self_margin": wl3["self_margin"]}
     nw = sum(len(q) for q in wl["trajectories"])
     batch = api.MixedBatch(b, len(splits), n, len(wl["trajectories"]), nw, 64)
+    _shape(batch, shape)
     frm, to, reqs, trajs = _fill(batch, wl, given_every=1)
     ep = api.EdgeEvalParams(max_joint_step=0.01, max_samples=600)
     cp = _cost_params(wl)
@@ -162,6 +178,8 @@ def test_batch_tune_keeps_results(w5):
     cp = _cost_params(wl)
     t = batch.tune(sc, ep, cp)
     assert t["traj_threads"] in (128, 256) and 0.0 < t["edge_share"] <= 1.0 and t["best_ms"] > 0.0
+    assert t["layout"] in (0, 1) and t["work_threads"] in (128, 256)
+    print(f"tuned batch shape: {t}")
     batch.launch(sc, ep, cp)
     torch.cuda.synchronize()
     _check_against_calls(b, sc, frm, to, reqs, trajs, ep, cp)
@@ -171,6 +189,12 @@ def test_batch_tune_keeps_results(w5):
 def test_batch_argument_errors(w5):
     wl, b, sc = w5
     batch = api.MixedBatch(b, 1, 4, 1, 64, 64)
+    with pytest.raises(PrismError):
+        batch.set_shape(layout=2)
+    with pytest.raises(PrismError):
+        batch.set_shape(layout=1, work_threads=96)
+    with pytest.raises(PrismError):
+        batch.set_shape(edge_share=0.0)
     q = torch.zeros((65, b.n_dof), device="cuda")
     with pytest.raises(PrismError):
         batch.add_trajectory(q)                        # longer than max_traj_len
@@ -188,11 +212,13 @@ def test_batch_argument_errors(w5):
     batch.close()
 
 
-def test_batch_edge_cases(w5):
+@pytest.mark.parametrize("shape", SHAPES)
+def test_batch_edge_cases(w5, shape):
     """Empty launch, G in {0, 1, 33}, a one-waypoint trajectory, replay after
     clear: each equals its per-request call."""
     wl, b, sc = w5
     batch = api.MixedBatch(b, 4, 64, 4, 256, 128)
+    _shape(batch, shape)
     ep = api.EdgeEvalParams(max_joint_step=0.01, max_samples=600)
     cp = _cost_params(wl, smooth=0.5)
     batch.launch(sc, ep, cp)                       # no requests at all
@@ -219,8 +245,9 @@ def test_batch_edge_cases(w5):
         batch.launch(sc, ep, cp)
 
 
+@pytest.mark.parametrize("shape", SHAPES)
 @pytest.mark.parametrize("broadcast", [False, True])
-def test_batch_rollouts_equal_rollout_costs(w5, broadcast):
+def test_batch_rollouts_equal_rollout_costs(w5, broadcast, shape):
     """STOMP rollout requests (reference layout [R, D, T]) share the launch
     with edge and trajectory requests; their state costs equal
     ps_rollout_costs bit for bit, and the other requests are unchanged."""
@@ -235,6 +262,7 @@ def test_batch_rollouts_equal_rollout_costs(w5, broadcast):
     n_req = 4
     n_e = sum(wl["edge_splits"][:n_req])
     batch = api.MixedBatch(b, n_req, n_e, 3 + len(rolls), nw, 128)
+    _shape(batch, shape)
     r_out = [batch.add_rollouts(rolls[0], broadcast_d=broadcast)]
     frm, to, reqs, tr = _fill(batch, wl, n_req=n_req, n_traj=3)
     r_out.append(batch.add_rollouts(rolls[1], broadcast_d=broadcast))
