@@ -1012,6 +1012,24 @@ def bench_mixed(dev, reps: int = 10, with_ref=True):
     stream.synchronize()
     wall_ms = (time.perf_counter() - t0) * 1e3 / reps
     dev_ms = e0.elapsed_time(e1) / reps
+
+    def device_ms_with(layout, threads, cost_warps=None):   # device time of one launch at another shape
+        batch.set_shape(layout=layout, work_threads=threads, work_cost_warps=cost_warps,
+                        edge_share=tune["edge_share"], traj_share=tune["traj_share"],
+                        traj_threads=tune["traj_threads"])
+        for _ in range(3):
+            batch.launch(sc, ep, cp, stream=stream)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(reps):
+                batch.launch(sc, ep, cp, stream=stream)
+            e1.record(stream)
+        stream.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    layouts = {f"work_queue_{t}x{c}_device_ms": device_ms_with(1, t, c) for t, c in ((256, 8), (256, 4), (256, 2),
+                                                                                      (128, 4), (128, 2))}
+    layouts["two_branches_device_ms"] = device_ms_with(0, 256)
     batch.close()
     return {"workload": wl["name"], "requests": {"edge": len(splits), "edges": len(wl["from"]),
                                                   "trajectories": len(trajs), "waypoints": n_wp,
@@ -1023,9 +1041,11 @@ def bench_mixed(dev, reps: int = 10, with_ref=True):
                               "device_ms = CUDA events around the step (launch gaps included), kernel_ms_sum = "
                               "each call's main kernel alone, summed"},
             "batched": {"value": checked / (wall_ms * 1e-3), "ms_per_step": wall_ms, "device_ms": dev_ms,
-                        "path": "ps_batch_launch (one graph replay: edge + trajectory branches)"},
+                        "path": "ps_batch_launch (one graph replay, the autotuned layout: "
+                                + ("one work-queue kernel" if tune["layout"] == 1 else
+                                   "edge queue and waypoint kernel side by side") + ")"},
             "speedup": plain_ms / wall_ms, "speedup_device": plain_dev_ms / dev_ms,
-            "speedup_kernels_only": plain_kernel_ms / dev_ms, "tuning": tune}
+            "speedup_kernels_only": plain_kernel_ms / dev_ms, "tuning": tune, "layouts": layouts}
 
 
 def run_reference(args):

@@ -458,6 +458,9 @@ typedef struct ps_batch_tuning {
                                 edge chunks and waypoint groups (trajectories
                                 and rollouts) from global counters          */
     int   work_threads;      /* threads per block of that kernel (128, 256)  */
+    int   work_cost_warps;   /* warps per block of it that also take waypoint
+                                groups (1 .. work_threads / 32); fewer leave
+                                shared memory for more resident blocks     */
 } ps_batch_tuning;
 
 int ps_batch_create(const ps_model* model, const ps_batch_limits* limits,
@@ -494,7 +497,8 @@ int ps_batch_launch(ps_batch* batch, const ps_scene_view* scene,
    times. */
 /* Use this launch shape from the next launch on (for example one that
    ps_batch_tune returned earlier); best_ms and traj_tile are ignored.
-   Shares in (0, 1], thread counts 128 or 256, layout 0 or 1. */
+   Shares in (0, 1], thread counts 128 or 256, layout 0 or 1,
+   work_cost_warps 1 .. work_threads / 32. */
 int ps_batch_set_shape(ps_batch* batch, const ps_batch_tuning* shape);
 int ps_batch_tune(ps_batch* batch, const ps_scene_view* scene,
                   const ps_edge_params* params, const ps_cost_params* cost,

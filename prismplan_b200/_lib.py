@@ -145,7 +145,7 @@ class BatchTuning(C.Structure):
     _fields_ = [
         ("edge_share", C.c_float), ("traj_share", C.c_float),
         ("traj_threads", C.c_int), ("traj_tile", C.c_int), ("best_ms", C.c_float),
-        ("layout", C.c_int), ("work_threads", C.c_int),
+        ("layout", C.c_int), ("work_threads", C.c_int), ("work_cost_warps", C.c_int),
     ]
 
 

@@ -764,15 +764,17 @@ class MixedBatch:
         _lib.check(_lib.load().ps_batch_tune(self.handle, C.byref(v), C.byref(ep), C.byref(cp), C.byref(t)))
         return {name: getattr(t, name) for name, _ in t._fields_}
 
-    def set_shape(self, layout: int = 0, work_threads: int = 256, edge_share: float = 1.0, traj_share: float = 0.5,
-                  traj_threads: int = 256) -> None:
+    def set_shape(self, layout: int = 0, work_threads: int = 256, work_cost_warps: Optional[int] = None,
+                  edge_share: float = 1.0, traj_share: float = 0.5, traj_threads: int = 256) -> None:
         """Launch shape for the next launches: layout 1 = one work-queue
-        kernel for edge chunks and waypoint groups; 0 = the persistent edge
-        queue and the waypoint kernel side by side. Results do not depend
-        on it."""
+        kernel for edge chunks and waypoint groups (work_cost_warps of its
+        warps per block also take waypoint groups; default all); 0 = the
+        persistent edge queue and the waypoint kernel side by side. Results
+        do not depend on it."""
         t = _lib.BatchTuning()
         t.edge_share, t.traj_share, t.traj_threads, t.traj_tile = edge_share, traj_share, traj_threads, 1
         t.layout, t.work_threads = layout, work_threads
+        t.work_cost_warps = work_threads // 32 if work_cost_warps is None else work_cost_warps
         _lib.check(_lib.load().ps_batch_set_shape(self.handle, C.byref(t)))
 
     def close(self):

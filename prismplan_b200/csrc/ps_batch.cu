@@ -183,28 +183,39 @@ __global__ void __launch_bounds__(kWarps * 32, 16 / kWarps) batch_waypoint_kerne
     }
 }
 
-// Per-warp scratch of the work-queue kernel: a warp holds either an edge
-// chunk (32 configurations and the broad phase's candidate list) or a
-// waypoint group (the lane-group scratch), one at a time.
-__host__ __device__ inline size_t work_warp_bytes(int NJ, int NS, int D, int n_obbs) {
-    const size_t edge = (size_t)32 * D * 4 + (size_t)((std::max(n_obbs, 1) + 7) & ~7) * 2;
+// Per-warp scratch of the work-queue kernel. Every warp holds an edge chunk's
+// (32 configurations and the broad phase's candidate list); the first
+// cost_warps warps of a block also take waypoint groups and hold the
+// lane-group scratch in the same region, one item at a time. Fewer such
+// warps leave room for more resident blocks, so more warps for edge items.
+__host__ __device__ inline size_t work_edge_bytes(int D, int n_obbs) {
+    return ((size_t)32 * D * 4 + (size_t)((n_obbs > 1 ? n_obbs : 1) + 7) / 8 * 8 * 2 + 15) & ~size_t(15);
+}
+__host__ __device__ inline size_t work_cost_bytes(int NJ, int NS, int D, int n_obbs) {
+    const size_t edge = work_edge_bytes(D, n_obbs);
     const size_t cost = lane_warp_bytes(NJ, NS, D, n_obbs, true);
     return ((edge > cost ? edge : cost) + 15) & ~size_t(15);
 }
+__host__ __device__ inline size_t work_warp_offset(int warp, int cost_warps, int NJ, int NS, int D, int n_obbs) {
+    const size_t cb = work_cost_bytes(NJ, NS, D, n_obbs), eb = work_edge_bytes(D, n_obbs);
+    return warp < cost_warps ? (size_t)warp * cb : (size_t)cost_warps * cb + (size_t)(warp - cost_warps) * eb;
+}
 
-size_t work_smem_bytes(const ps_model* m, const ps_scene_view* sv, int warps) {
+size_t work_smem_bytes(const ps_model* m, const ps_scene_view* sv, int warps, int cost_warps) {
     const size_t tables = lane_block_bytes(m, sv, 0, true);
-    return tables + (size_t)warps * work_warp_bytes(m->info.n_joints, m->info.n_spheres, m->info.n_dof, sv->n_obbs);
+    return tables + work_warp_offset(warps, cost_warps, m->info.n_joints, m->info.n_spheres, m->info.n_dof,
+                                     sv->n_obbs);
 }
 
 // The whole batch as one persistent work queue. Every warp pulls, from
 // global counters, first the persistent edge path's chunk-major items of
 // this pass (hdr->head[pass]: a chunk of 32 consecutive samples of one edge,
-// skipped once the edge is retired), then, in pass 0, waypoint groups
+// skipped once the edge is retired), then, in the last pass, waypoint groups
 // (hdr->wp_next: kCostSlots consecutive packed waypoints; trajectory groups
 // with the adjoint, rollout groups without it), until both are drained.
-// Pass 1 holds the later chunk rounds when the edges are too few to keep
-// round 0 ahead of them (the persistent edge path's split rule). The edge
+// Pass 0 holds only chunk round 0 when the edges are too few to keep round 0
+// ahead of the later rounds (the persistent edge path's split rule); pass 1
+// then holds the later rounds and the waypoint groups. The edge
 // items are processed exactly as by edges_queue_kernel and the waypoint
 // groups exactly as by batch_waypoint_kernel, so every output has the same
 // bits as with the two kernels side by side.
@@ -214,12 +225,14 @@ __global__ void __launch_bounds__(kW * 32, 16 / kW)
                       const Counts* __restrict__ cnt, const float* __restrict__ from, const float* __restrict__ to,
                       EdgeWs* hdr, const int* __restrict__ Gs, int* bad, int* clr, int* done,
                       const float* __restrict__ q, float* __restrict__ wp_cost, float* __restrict__ grad, int cap,
-                      int pass) {
+                      int pass, int cost_warps) {
     const int n_edges = cnt->n_edges, n_wp = cnt->n_wp, n_roll = cnt->n_roll;
-    const int chunks_a = (n_wp + kCostSlots - 1) / kCostSlots;
-    const int chunks = pass == 0 ? chunks_a + (n_roll + kCostSlots - 1) / kCostSlots : 0;
     const int max_rounds = *((volatile int*)&hdr->max_rounds);
     const bool split = (long long)n_edges < 8ll * gridDim.x * kW;
+    // the waypoint groups follow the edge items of the last pass, where they
+    // fill the tail of the edge work
+    const int chunks_a = (n_wp + kCostSlots - 1) / kCostSlots;
+    const int chunks = pass == (split ? 1 : 0) ? chunks_a + (n_roll + kCostSlots - 1) / kCostSlots : 0;
     const int r_lo = pass == 0 ? 0 : (split ? 1 : max_rounds);
     const int r_hi = pass == 0 ? (split ? min(max_rounds, 1) : max_rounds) : max_rounds;
     const long long total = (long long)max(r_hi - r_lo, 0) * n_edges;   // edge items of this pass
@@ -236,7 +249,7 @@ __global__ void __launch_bounds__(kW * 32, 16 / kW)
         if (threadIdx.x == 0 && total > 0) atomicExch(&hdr->timed_out, 1);
         const int D = reinterpret_cast<const BlobHeader*>(md.blob)->n_dof;
         const float nan = __int_as_float(0x7fc00000);
-        for (;;) {
+        while (chunks > 0 && warp < cost_warps) {   // (a pass without groups leaves the counter alone)
             int c = 0;
             if (lane == 0) c = atomicAdd(&hdr->wp_next, 1);
             c = __shfl_sync(kFull, c, 0);
@@ -264,7 +277,8 @@ __global__ void __launch_bounds__(kW * 32, 16 / kW)
     __syncthreads();
     box_limits(sc, const_cast<float4*>(cb.obs));
     __syncthreads();
-    unsigned char* wbase = reinterpret_cast<unsigned char*>(cb.wbase) + (size_t)warp * work_warp_bytes(NJ, NS, D, sv.n_obbs);
+    unsigned char* wbase =
+        reinterpret_cast<unsigned char*>(cb.wbase) + work_warp_offset(warp, cost_warps, NJ, NS, D, sv.n_obbs);
     LaneStats st;
     st.zero();
 
@@ -332,7 +346,7 @@ __global__ void __launch_bounds__(kW * 32, 16 / kW)
     }
 
     // ---- waypoint groups (batch_waypoint_kernel's loop) ----
-    if (chunks > 0) {
+    if (chunks > 0 && warp < cost_warps) {
         const LaneScratch ws = lane_carve(wbase, NJ, NS, D, true);
         for (;;) {
             int c = 0;
@@ -439,6 +453,7 @@ struct ps_batch {
     int traj_tile = 1;        // kept for the tuning record: always 1
     int layout = 0;           // 0: edge queue and waypoint kernel side by side; 1: one work-queue kernel
     int work_threads = 256;   // threads per block of the work-queue kernel
+    int work_cost_warps = 8;  // warps per block of it that also take waypoint groups
 };
 
 namespace {
@@ -449,7 +464,7 @@ struct LaunchPlan {
                int*, int*, unsigned long long*, int, const int*) = nullptr;
     void (*wk)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*, int) = nullptr;
     void (*work)(ModelDev, ps_scene_view, ps_edge_params, ps_cost_params, const Counts*, const float*, const float*,
-                 EdgeWs*, const int*, int*, int*, int*, const float*, float*, float*, int, int) = nullptr;
+                 EdgeWs*, const int*, int*, int*, int*, const float*, float*, float*, int, int, int) = nullptr;
     size_t qsmem = 0, wsmem = 0, fsmem = 0, ssmem = 0, ksmem = 0;
     int qgrid = 1, wgrid = 1, req_grid_e = 1, req_grid_t = 1, pgrid = 1, sgrid = 1, kgrid = 1;
     ProbePlan probe;
@@ -519,7 +534,7 @@ int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, 
         const int mode = b->lim.max_edges > 0 ? L.mode : 1;
         const int kt = b->work_threads;
         L.work = pick_work_kernel(mode, kt);
-        L.ksmem = work_smem_bytes(m, sv, kt / 32);
+        L.ksmem = work_smem_bytes(m, sv, kt / 32, std::min(b->work_cost_warps, kt / 32));
         PS_TRY_CUDA(allow_smem((const void*)L.work, L.ksmem));
         int per_sm = 0;
         PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L.work, kt, L.ksmem));
@@ -530,9 +545,9 @@ int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, 
 }
 
 // Layout 1: one stream; gathers, edge prep and the end-sample probe, then
-// the work-queue kernel (pass 0: edge items of round 0, or of every round,
-// and every waypoint group; pass 1: the later rounds when split), the self
-// pass, finalize, scatter and the trajectory outputs.
+// the work-queue kernel twice (split: round 0, then the later rounds and the
+// waypoint groups; otherwise every round and the waypoint groups, then
+// nothing), the self pass, finalize, scatter and the trajectory outputs.
 void record_work_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, const ps_cost_params* cp,
                        const LaunchPlan& L) {
     const ps_model* m = b->model;
@@ -554,7 +569,8 @@ void record_work_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_param
     for (int pass = 0; pass < 2; ++pass)
         L.work<<<L.kgrid, b->work_threads, L.ksmem, s0>>>(m->dev, *sv, *ep, *cp, b->d_cnt, b->d_from, b->d_to,
                                                           b->d_hdr, b->d_G, b->d_bad, b->d_clr, b->d_done, b->d_q,
-                                                          b->d_wp_cost, b->d_grad, b->lim.max_waypoints, pass);
+                                                          b->d_wp_cost, b->d_grad, b->lim.max_waypoints, pass,
+                                                          std::min(b->work_cost_warps, b->work_threads / 32));
     if (edges) {
         if (ep->check_self)
             edges_self_kernel<<<L.sgrid, kSelfThreads, L.ssmem, s0>>>(m->dev, *ep, b->d_from, b->d_to, b->d_given,
@@ -640,7 +656,7 @@ int batch_capture(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep
 
 std::vector<unsigned char> make_key(const ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep,
                                     const ps_cost_params* cp) {
-    std::vector<unsigned char> k(sizeof(*sv) + sizeof(*ep) + sizeof(*cp) + 2 * sizeof(float) + 5 * sizeof(int));
+    std::vector<unsigned char> k(sizeof(*sv) + sizeof(*ep) + sizeof(*cp) + 2 * sizeof(float) + 6 * sizeof(int));
     unsigned char* p = k.data();
     auto put = [&](const void* src, size_t n) {
         std::memcpy(p, src, n);
@@ -655,6 +671,7 @@ std::vector<unsigned char> make_key(const ps_batch* b, const ps_scene_view* sv, 
     put(&b->traj_tile, sizeof(int));
     put(&b->layout, sizeof(int));
     put(&b->work_threads, sizeof(int));
+    put(&b->work_cost_warps, sizeof(int));
     put(&b->model->dev.stage_polls, sizeof(int));   // kernels get the model by value at capture
     return k;
 }
@@ -861,12 +878,15 @@ extern "C" int ps_batch_set_shape(ps_batch* b, const ps_batch_tuning* shape) {
         (shape->work_threads != 128 && shape->work_threads != 256))
         return set_error(PS_EINVAL, "traj_threads and work_threads must be 128 or 256");
     if (shape->layout != 0 && shape->layout != 1) return set_error(PS_EINVAL, "layout must be 0 or 1");
+    if (shape->work_cost_warps < 1 || shape->work_cost_warps > shape->work_threads / 32)
+        return set_error(PS_EINVAL, "work_cost_warps must be 1 .. work_threads / 32");
     b->edge_share = shape->edge_share;
     b->traj_share = shape->traj_share;
     b->traj_threads = shape->traj_threads;
     b->traj_tile = 1;
     b->layout = shape->layout;
     b->work_threads = shape->work_threads;
+    b->work_cost_warps = shape->work_cost_warps;
     return PS_OK;   // the next launch captures a graph for the new shape
 }
 
@@ -889,9 +909,10 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
         return cuda_error(le, "tuning events");
     }
     const float keep_e = b->edge_share, keep_t = b->traj_share;
-    const int keep_w = b->traj_threads, keep_tile = b->traj_tile, keep_l = b->layout, keep_k = b->work_threads;
+    const int keep_w = b->traj_threads, keep_tile = b->traj_tile, keep_l = b->layout, keep_k = b->work_threads,
+              keep_c = b->work_cost_warps;
     float best = 3.0e38f, best_e = keep_e, best_t = keep_t;
-    int best_w = keep_w, best_tile = keep_tile, best_l = keep_l, best_k = keep_k;
+    int best_w = keep_w, best_tile = keep_tile, best_l = keep_l, best_k = keep_k, best_c = keep_c;
     int rc = PS_OK;
     const bool edges = b->lim.max_edges > 0, trajs = b->lim.max_waypoints > 0;
     auto time_now = [&](float& ms_min) {   // capture + warm-up, then the best of 3 launches
@@ -908,17 +929,22 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
         }
         return r;
     };
-    // layout 1: one work-queue kernel, 128 or 256 threads per block
+    // layout 1: one work-queue kernel; (threads per block, warps that also
+    // take waypoint groups)
+    const int work_shapes[][2] = {{256, 8}, {256, 4}, {256, 2}, {128, 4}, {128, 2}};
     b->layout = 1;
-    for (int kt : widths) {
-        b->work_threads = kt;
+    for (const auto& ws : work_shapes) {
+        if (!trajs && ws[1] != ws[0] / 32) continue;   // no waypoints: one shape per width
+        b->work_threads = ws[0];
+        b->work_cost_warps = ws[1];
         float ms_min = 0.0f;
         rc = time_now(ms_min);
         if (rc) break;
         if (ms_min < best) {
             best = ms_min;
             best_l = 1;
-            best_k = kt;
+            best_k = ws[0];
+            best_c = ws[1];
         }
     }
     b->layout = 0;
@@ -962,6 +988,7 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
         b->traj_tile = keep_tile;
         b->layout = keep_l;
         b->work_threads = keep_k;
+        b->work_cost_warps = keep_c;
         return rc;
     }
     b->edge_share = best_e;
@@ -970,6 +997,7 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
     b->traj_tile = best_tile;
     b->layout = best_l;
     b->work_threads = best_k;
+    b->work_cost_warps = best_c;
     if (out) {
         out->edge_share = best_e;
         out->traj_share = best_t;
@@ -978,6 +1006,7 @@ extern "C" int ps_batch_tune(ps_batch* b, const ps_scene_view* sv, const ps_edge
         out->best_ms = best;
         out->layout = best_l;
         out->work_threads = best_k;
+        out->work_cost_warps = best_c;
     }
     return PS_OK;
 }

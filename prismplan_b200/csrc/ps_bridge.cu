@@ -75,16 +75,21 @@ struct GraphEntry {
 
 }  // namespace
 
+// Buffers are packed per call so that each direction is one copy: for n
+// edges the device inputs are d_in = [from (n rows) | to (n rows)] and the
+// device outputs d_out = [cost (n floats) | valid (n bytes)]; the pinned
+// mirrors h_in and h_out hold the same layouts. The in-place input mirrors
+// that ps_edge_bridge_host_inputs hands out are fixed instead (from at
+// h_in, to at h_in + max_edges rows): inputs written there go over in one
+// copy when n == max_edges and in two otherwise.
 struct ps_edge_bridge {
     const ps_model* model = nullptr;
     ps_scene_view scene{};
     int dim = 0, max_edges = 0, device = 0;
-    float *d_from = nullptr, *d_to = nullptr, *d_cost = nullptr, *d_clr = nullptr;
-    uint8_t* d_valid = nullptr;
+    float *d_in = nullptr, *d_out = nullptr, *d_clr = nullptr;
     void* d_ws = nullptr;
     size_t ws_bytes = 0;
-    float *h_from = nullptr, *h_to = nullptr, *h_cost = nullptr, *h_clr = nullptr;
-    uint8_t* h_valid = nullptr;
+    float *h_in = nullptr, *h_out = nullptr, *h_clr = nullptr;
     cudaStream_t stream = nullptr;
     std::list<GraphEntry> graphs;   // most recently used first
 };
@@ -97,22 +102,20 @@ void release(ps_edge_bridge* b) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
     b->graphs.clear();
     if (b->stream) cudaStreamDestroy(b->stream);
-    cudaFree(b->d_from);
-    cudaFree(b->d_to);
-    cudaFree(b->d_valid);
-    cudaFree(b->d_cost);
+    cudaFree(b->d_in);
+    cudaFree(b->d_out);
     cudaFree(b->d_clr);
     cudaFree(b->d_ws);
-    cudaFreeHost(b->h_from);
-    cudaFreeHost(b->h_to);
-    cudaFreeHost(b->h_valid);
-    cudaFreeHost(b->h_cost);
+    cudaFreeHost(b->h_in);
+    cudaFreeHost(b->h_out);
     cudaFreeHost(b->h_clr);
     delete b;
 }
 
 int check_edges_on(ps_edge_bridge* b, int n, const ps_edge_params* P) {
-    return ps_check_edges(b->model, &b->scene, b->d_from, b->d_to, nullptr, n, P, b->d_valid, b->d_cost,
+    const size_t rows = (size_t)n * b->dim;
+    uint8_t* valid = reinterpret_cast<uint8_t*>(b->d_out + n);
+    return ps_check_edges(b->model, &b->scene, b->d_in, b->d_in + rows, nullptr, n, P, valid, b->d_out,
                           P->compute_clearance ? b->d_clr : nullptr, b->d_ws, b->ws_bytes, b->stream);
 }
 
@@ -182,16 +185,12 @@ extern "C" int ps_edge_bridge_create(const ps_model* model, const ps_scene_view*
     auto step = [&](cudaError_t r) {
         if (e == cudaSuccess) e = r;
     };
-    step(cudaMalloc(&b->d_from, cfg));
-    step(cudaMalloc(&b->d_to, cfg));
-    step(cudaMalloc(&b->d_valid, ne));
-    step(cudaMalloc(&b->d_cost, ne * 4));
+    step(cudaMalloc(&b->d_in, 2 * cfg));
+    step(cudaMalloc(&b->d_out, ne * 5));
     step(cudaMalloc(&b->d_clr, ne * 4));
     step(cudaMalloc(&b->d_ws, b->ws_bytes));
-    step(cudaHostAlloc(&b->h_from, cfg, cudaHostAllocDefault));
-    step(cudaHostAlloc(&b->h_to, cfg, cudaHostAllocDefault));
-    step(cudaHostAlloc(&b->h_valid, ne, cudaHostAllocDefault));
-    step(cudaHostAlloc(&b->h_cost, ne * 4, cudaHostAllocDefault));
+    step(cudaHostAlloc(&b->h_in, 2 * cfg, cudaHostAllocDefault));
+    step(cudaHostAlloc(&b->h_out, ne * 5, cudaHostAllocDefault));
     step(cudaHostAlloc(&b->h_clr, ne * 4, cudaHostAllocDefault));
     step(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     if (e != cudaSuccess) {
@@ -213,8 +212,8 @@ extern "C" int ps_edge_bridge_set_scene(ps_edge_bridge* b, const ps_scene_view* 
 extern "C" int ps_edge_bridge_host_inputs(ps_edge_bridge* b, float** from_flat, float** to_flat) {
     clear_error();
     if (!b || !from_flat || !to_flat) return set_error(PS_EINVAL, "bridge or output pointer is NULL");
-    *from_flat = b->h_from;
-    *to_flat = b->h_to;
+    *from_flat = b->h_in;
+    *to_flat = b->h_in + (size_t)b->max_edges * b->dim;
     return PS_OK;
 }
 
@@ -238,32 +237,33 @@ extern "C" int ps_edge_bridge_evaluate(ps_edge_bridge* b, const float* from_flat
     if (dev != b->device)
         return set_error(PS_EINVAL, "bridge created on device " + std::to_string(b->device) +
                                         ", current device is " + std::to_string(dev));
-    const size_t row = (size_t)b->dim * sizeof(float);
-    if (from_flat == b->h_from && to_flat == b->h_to) {   // written in place: nothing to stage
-        const size_t bytes = (size_t)num_edges * row;
-        PS_TRY_CUDA(cudaMemcpyAsync(b->d_from, b->h_from, bytes, cudaMemcpyHostToDevice, b->stream));
-        PS_TRY_CUDA(cudaMemcpyAsync(b->d_to, b->h_to, bytes, cudaMemcpyHostToDevice, b->stream));
+    const size_t rows = (size_t)num_edges * b->dim, bytes = rows * sizeof(float);
+    float* fixed_to = b->h_in + (size_t)b->max_edges * b->dim;
+    if (from_flat == b->h_in && to_flat == fixed_to) {   // written in place: nothing to stage
+        if (num_edges == b->max_edges) {
+            PS_TRY_CUDA(cudaMemcpyAsync(b->d_in, b->h_in, 2 * bytes, cudaMemcpyHostToDevice, b->stream));
+        } else {
+            PS_TRY_CUDA(cudaMemcpyAsync(b->d_in, b->h_in, bytes, cudaMemcpyHostToDevice, b->stream));
+            PS_TRY_CUDA(cudaMemcpyAsync(b->d_in + rows, fixed_to, bytes, cudaMemcpyHostToDevice, b->stream));
+        }
     } else {
-        // Stage into the pinned mirrors on OpenMP threads (one thread copies
-        // 10-20 GB/s, below the host-to-device link), then copy in.
-        const size_t bytes = (size_t)num_edges * row;
-        stage_parallel(b->h_from, from_flat, bytes);
-        stage_parallel(b->h_to, to_flat, bytes);
-        PS_TRY_CUDA(cudaMemcpyAsync(b->d_from, b->h_from, bytes, cudaMemcpyHostToDevice, b->stream));
-        PS_TRY_CUDA(cudaMemcpyAsync(b->d_to, b->h_to, bytes, cudaMemcpyHostToDevice, b->stream));
+        // Stage into the pinned mirror on OpenMP threads (one thread copies
+        // 10-20 GB/s, below the host-to-device link), then copy in at once.
+        stage_parallel(b->h_in, from_flat, bytes);
+        stage_parallel(b->h_in + rows, to_flat, bytes);
+        PS_TRY_CUDA(cudaMemcpyAsync(b->d_in, b->h_in, 2 * bytes, cudaMemcpyHostToDevice, b->stream));
     }
     if (int rc = launch_check(b, num_edges, P)) {
         cudaStreamSynchronize(b->stream);
         return rc;
     }
     const size_t n = (size_t)num_edges;
-    PS_TRY_CUDA(cudaMemcpyAsync(b->h_valid, b->d_valid, n, cudaMemcpyDeviceToHost, b->stream));
-    PS_TRY_CUDA(cudaMemcpyAsync(b->h_cost, b->d_cost, n * 4, cudaMemcpyDeviceToHost, b->stream));
+    PS_TRY_CUDA(cudaMemcpyAsync(b->h_out, b->d_out, n * 5, cudaMemcpyDeviceToHost, b->stream));
     if (P->compute_clearance)
         PS_TRY_CUDA(cudaMemcpyAsync(b->h_clr, b->d_clr, n * 4, cudaMemcpyDeviceToHost, b->stream));
     PS_TRY_CUDA(cudaStreamSynchronize(b->stream));
-    std::memcpy(out_valid, b->h_valid, n);
-    std::memcpy(out_cost, b->h_cost, n * 4);
+    std::memcpy(out_cost, b->h_out, n * 4);
+    std::memcpy(out_valid, reinterpret_cast<const uint8_t*>(b->h_out + n), n);
     if (P->compute_clearance) std::memcpy(out_clearance, b->h_clr, n * 4);
     return PS_OK;
 }

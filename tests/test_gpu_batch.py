@@ -55,13 +55,14 @@ def _check_against_calls(b, sc, frm, to, reqs, trajs, ep, cp):
 
 
 # Launch shapes: the default (the edge queue and the waypoint kernel side by
-# side) and the one work-queue kernel (layout 1) at both block widths.
-SHAPES = [None, (1, 128), (1, 256)]
+# side) and the one work-queue kernel (layout 1) at both block widths, with
+# all or some of its warps taking waypoint groups.
+SHAPES = [None, (1, 128, 4), (1, 256, 2)]
 
 
 def _shape(batch, shape):
     if shape is not None:
-        batch.set_shape(layout=shape[0], work_threads=shape[1])
+        batch.set_shape(layout=shape[0], work_threads=shape[1], work_cost_warps=shape[2])
 
 
 @pytest.fixture(scope="module")
@@ -195,6 +196,8 @@ def test_batch_argument_errors(w5):
         batch.set_shape(layout=1, work_threads=96)
     with pytest.raises(PrismError):
         batch.set_shape(edge_share=0.0)
+    with pytest.raises(PrismError):
+        batch.set_shape(layout=1, work_threads=128, work_cost_warps=5)
     q = torch.zeros((65, b.n_dof), device="cuda")
     with pytest.raises(PrismError):
         batch.add_trajectory(q)                        # longer than max_traj_len

@@ -83,6 +83,23 @@ def test_bridge_equals_device_path_and_reference(w2):
         dv, dc, _ = _device(b, sc, f, t, p)
         np.testing.assert_array_equal(v, dv)
         assert np.array_equal(_bits(c), _bits(dc))
+    # edges written straight into the bridge's pinned input mirrors: no
+    # staging copy (one copy in at full capacity, two below it)
+    pf, pt = C.c_void_p(), C.c_void_p()
+    _lib.check(lib.ps_edge_bridge_host_inputs(ev._h, C.byref(pf), C.byref(pt)))
+    mf = np.ctypeslib.as_array(C.cast(pf, C.POINTER(C.c_float)), shape=(E, 7))
+    mt = np.ctypeslib.as_array(C.cast(pt, C.POINTER(C.c_float)), shape=(E, 7))
+    for n in (E, 12345):
+        perm = rng.permutation(E)[:n]
+        mf[:n] = wl["from"][perm]
+        mt[:n] = wl["to"][perm]
+        v = np.empty(n, np.uint8)
+        c = np.empty(n, np.float32)
+        _lib.check(lib.ps_edge_bridge_evaluate(ev._h, pf, pt, n, C.byref(pc), v.ctypes.data, c.ctypes.data, None))
+        dv, dc, _ = _device(b, sc, np.ascontiguousarray(wl["from"][perm]), np.ascontiguousarray(wl["to"][perm]), p)
+        np.testing.assert_array_equal(v, dv)
+        assert np.array_equal(_bits(c), _bits(dc))
+    del mf, mt
     ev.close()
 
 

@@ -142,14 +142,14 @@ def test_costs_fail_closed(setup, want_grad):
     assert torch.equal(wp2, wp_ok) and torch.equal(tc2, tc_ok)
 
 
-@pytest.mark.parametrize("layout", [0, 1])
+@pytest.mark.parametrize("layout", [0, 1, 2])
 def test_batch_fail_closed(setup, layout):
     b, sc, frm, to, _ = setup
     E = frm.shape[0]
     w3 = workloads.workload(3, scale=1.0 / 64)
     q = torch.from_numpy(w3["q"][:, :, :]).cuda()
     batch = api.MixedBatch(b, 4, E, 4, 4 * q.shape[1], q.shape[1])
-    batch.set_shape(layout=layout)
+    batch.set_shape(layout=min(layout, 1), work_cost_warps=2 if layout == 2 else None)   # 2: some warps edges only
     outs = [batch.add_edges(frm[i::4], to[i::4]) for i in range(4)]
     touts = [batch.add_trajectory(q[i].contiguous()) for i in range(4)]
     ep = api.EdgeEvalParams(max_joint_step=0.01, max_samples=600)
