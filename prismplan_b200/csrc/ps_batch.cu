@@ -563,7 +563,7 @@ void record_work_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_param
         if (L.probe.k)
             L.probe.k<<<L.probe.grid, kProbeThreads, L.probe.smem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to,
                                                                           b->lim.max_edges, b->d_hdr, b->d_G,
-                                                                          b->d_bad, nullptr, n_dev);
+                                                                          b->d_bad, nullptr, n_dev, PrepArgs{});
     }
     if (trajs) batch_gather_traj<<<L.req_grid_t, 128, 0, s0>>>(b->d_treq, b->d_cnt, D, b->d_q);
     for (int pass = 0; pass < 2; ++pass)
@@ -610,7 +610,7 @@ void record_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep
         if (L.probe.k)
             L.probe.k<<<L.probe.grid, kProbeThreads, L.probe.smem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to,
                                                                           b->lim.max_edges, b->d_hdr, b->d_G,
-                                                                          b->d_bad, nullptr, n_dev);
+                                                                          b->d_bad, nullptr, n_dev, PrepArgs{});
         L.qk<<<L.qgrid, kEdgeThreads, L.qsmem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to, b->lim.max_edges, b->d_hdr,
                                                     b->d_G, b->d_bad, b->d_clr, b->d_done, nullptr, 0, n_dev);
         L.qk<<<L.qgrid, kEdgeThreads, L.qsmem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to, b->lim.max_edges, b->d_hdr,

@@ -569,11 +569,14 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_plain_kerne
 // ---------------------------------------------------------------------------
 // n_dev (optional): device-resident edge count overriding n_edges, so a
 // captured graph can be replayed with a different number of edges.
-__global__ void edges_prep_kernel(ps_edge_params P, const float* __restrict__ from, const float* __restrict__ to,
-                                  const int* __restrict__ given, int n_edges, int D, EdgeWs* hdr, int* G_out,
-                                  float* len_out, int* bad, int* clr, int* done, const int* n_dev = nullptr) {
-    if (n_dev) n_edges = *n_dev;
-    // the time budget starts when the call's first kernel runs
+// Per-edge preparation of the persistent path, over the grid-stride edges
+// of this thread: sample count G, length, cleared per-edge state, and the
+// header's maxima and counts (one atomic per warp). The time budget starts
+// here, when the call's first kernel runs. Every thread of the grid calls it.
+__device__ __forceinline__ void prep_edges(const ps_edge_params& P, const float* __restrict__ from,
+                                           const float* __restrict__ to, const int* __restrict__ given,
+                                           int n_edges, int D, EdgeWs* hdr, int* G_out, float* len_out, int* bad,
+                                           int* clr, int* done) {
     if (blockIdx.x == 0 && threadIdx.x == 0)
         hdr->deadline = P.time_budget_ms > 0.0f
                             ? global_ns() + (unsigned long long)((double)P.time_budget_ms * 1.0e6) + 1ull
@@ -605,6 +608,13 @@ __global__ void edges_prep_kernel(ps_edge_params P, const float* __restrict__ fr
         atomicAdd(&hdr->self_samples, local_ns);
         atomicAdd(&hdr->self_edges, local_ne);
     }
+}
+
+__global__ void edges_prep_kernel(ps_edge_params P, const float* __restrict__ from, const float* __restrict__ to,
+                                  const int* __restrict__ given, int n_edges, int D, EdgeWs* hdr, int* G_out,
+                                  float* len_out, int* bad, int* clr, int* done, const int* n_dev = nullptr) {
+    if (n_dev) n_edges = *n_dev;
+    prep_edges(P, from, to, given, n_edges, D, hdr, G_out, len_out, bad, clr, done);
 }
 
 // ---------------------------------------------------------------------------
@@ -736,16 +746,30 @@ size_t probe_smem_bytes(const ps_model* m, const ps_scene_view* sv) {
            (size_t)16 * std::max(sv->n_obbs, 1) + (size_t)kProbeThreads * kProbeStride * 2;
 }
 
-template <bool kStats>
+// With PrepArgs the kernel also does edges_prep_kernel's work first, over the
+// same grid-stride edges (a thread then probes the edges it prepared), which
+// saves a launch and overlaps the preparation with the model staging.
+struct PrepArgs {
+    const int* given;
+    float* len;
+    int* clr;
+    int* done;
+};
+
+template <bool kStats, bool kPrep>
 __global__ void __launch_bounds__(kProbeThreads, 4) edges_probe_kernel(ModelDev md, ps_scene_view sv,
                                                                         ps_edge_params P,
                                                                         const float* __restrict__ from,
                                                                         const float* __restrict__ to, int n_edges,
-                                                                        EdgeWs* hdr, const int* __restrict__ Gs,
+                                                                        EdgeWs* hdr, int* Gs,
                                                                         int* bad, unsigned long long* stats,
-                                                                        const int* n_dev = nullptr) {
+                                                                        const int* n_dev, PrepArgs pa) {
     if (n_dev) n_edges = *n_dev;
     if (n_edges <= 0) return;
+    if (kPrep) {
+        const int D = reinterpret_cast<const BlobHeader*>(md.blob)->n_dof;
+        prep_edges(P, from, to, pa.given, n_edges, D, hdr, Gs, pa.len, bad, pa.clr, pa.done);
+    }
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ int counters[4];
@@ -793,8 +817,12 @@ __global__ void __launch_bounds__(kProbeThreads, 4) edges_probe_kernel(ModelDev 
 // off one lane at a time) with enough edges to fill the GPU. `share` scales
 // the grid (mixed batch).
 struct ProbePlan {
-    void (*k)(ModelDev, ps_scene_view, ps_edge_params, const float*, const float*, int, EdgeWs*, const int*, int*,
-              unsigned long long*, const int*) = nullptr;
+    // k: the probe alone (the preparation ran before it); kp: preparation and
+    // probe in one launch. Same shared memory and grid.
+    void (*k)(ModelDev, ps_scene_view, ps_edge_params, const float*, const float*, int, EdgeWs*, int*, int*,
+              unsigned long long*, const int*, PrepArgs) = nullptr;
+    void (*kp)(ModelDev, ps_scene_view, ps_edge_params, const float*, const float*, int, EdgeWs*, int*, int*,
+               unsigned long long*, const int*, PrepArgs) = nullptr;
     size_t smem = 0;
     int grid = 1;
 };
@@ -807,9 +835,11 @@ int plan_probe(const ps_model* m, const ps_scene_view* sv, int mode, bool stats,
     // and costs more than it retires (measured: the 16 K segment edges of a
     // 256-request CHOMP iteration ran 3 % slower with it). choice 1 forces it.
     if (choice != 1 && (long long)max_edges < 8ll * 32 * sm_count()) return PS_OK;
-    out.k = stats ? edges_probe_kernel<true> : edges_probe_kernel<false>;
+    out.k = stats ? edges_probe_kernel<true, false> : edges_probe_kernel<false, false>;
+    out.kp = stats ? edges_probe_kernel<true, true> : edges_probe_kernel<false, true>;
     out.smem = probe_smem_bytes(m, sv);
     PS_TRY_CUDA(allow_smem((const void*)out.k, out.smem));
+    PS_TRY_CUDA(allow_smem((const void*)out.kp, out.smem));
     int per_sm = 0;
     PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, out.k, kProbeThreads, out.smem));
     if (per_sm < 1) return set_error(PS_EINVAL, "edge probe kernel does not fit on an SM with this scene");

@@ -104,10 +104,6 @@ int run_persistent(const ps_model* m, const ps_scene_view* scene, const float* f
                    float* clearance, const EdgeBufs& b, cudaStream_t s) {
     const int D = m->info.n_dof;
     PS_TRY_CUDA(cudaMemsetAsync(b.hdr, 0, sizeof(EdgeWs), s));   // queue heads, deadline, max rounds, timeout
-    const int pgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
-    edges_prep_kernel<<<pgrid, 256, 0, s>>>(*P, from, to, samples_per_edge, n_edges, D, b.hdr, b.G, b.len, b.bad,
-                                            b.clr, b.done);
-    PS_TRY_CUDA(cudaGetLastError());
     const size_t smem = edge_smem_bytes(m, scene);
     const int mode = fast_path(m, scene, P);
     auto qk = pick(mode, g_stats != nullptr, edges_queue_kernel<0, false>, edges_queue_kernel<0, true>,
@@ -121,10 +117,17 @@ int run_persistent(const ps_model* m, const ps_scene_view* scene, const float* f
     const int qgrid = std::max(1, sm_count() * per_sm);
     ProbePlan probe;
     if (int rc = plan_probe(m, scene, mode, g_stats != nullptr, 1.0f, n_edges, P->probe, probe)) return rc;
+    if (!probe.kp) {   // with the probe, its launch also prepares the edges
+        const int pgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
+        edges_prep_kernel<<<pgrid, 256, 0, s>>>(*P, from, to, samples_per_edge, n_edges, D, b.hdr, b.G, b.len, b.bad,
+                                                b.clr, b.done);
+        PS_TRY_CUDA(cudaGetLastError());
+    }
     mark_start(s);
-    if (probe.k)
-        probe.k<<<probe.grid, kProbeThreads, probe.smem, s>>>(m->dev, *scene, *P, from, to, n_edges, b.hdr, b.G,
-                                                               b.bad, g_stats, nullptr);
+    if (probe.kp)
+        probe.kp<<<probe.grid, kProbeThreads, probe.smem, s>>>(m->dev, *scene, *P, from, to, n_edges, b.hdr, b.G,
+                                                                b.bad, g_stats, nullptr,
+                                                                PrepArgs{samples_per_edge, b.len, b.clr, b.done});
     qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, b.hdr, b.G, b.bad, b.clr, b.done,
                                          g_stats, 0, nullptr);
     if ((long long)n_edges < 8ll * qgrid * kEdgeThreads / 32)   // the kernel's own split rule
