@@ -343,12 +343,14 @@ int ps_edges_status(const void* workspace, int* status);
                                 staged. num_edges <= 0: nothing to do, PS_OK;
                                 num_edges > max_edges: PS_EINVAL (the
                                 reference throws, :67-68).
-     ps_edge_bridge_status   <- PS_ETIMEOUT when the last call's time budget
-                                ran out (ps_edges_status of its workspace).
+     ps_edge_bridge_status   <- PS_ETIMEOUT when the time budget of the call
+                                waited for last ran out (ps_edges_status of
+                                its workspace).
      ps_edge_bridge_destroy  <- ~EdgeEvalGpu (:47-53).
    One bridge per host thread at a time, on the device that was current at
    create (evaluate returns PS_EINVAL on another). */
 typedef struct ps_edge_bridge ps_edge_bridge;
+#define PS_BRIDGE_SLOTS 2
 int ps_edge_bridge_create(const ps_model* model, const ps_scene_view* scene,
                           int dim, int max_edges, ps_edge_bridge** out);
 int ps_edge_bridge_set_scene(ps_edge_bridge* bridge, const ps_scene_view* scene);
@@ -356,9 +358,25 @@ int ps_edge_bridge_evaluate(ps_edge_bridge* bridge, const float* from_flat,
                             const float* to_flat, int num_edges,
                             const ps_edge_params* params, uint8_t* out_valid,
                             float* out_cost, float* out_clearance);
+/* Asynchronous form, no reference counterpart: up to PS_BRIDGE_SLOTS calls
+   in flight, one per slot, each with its own buffers and stream, so that a
+   caller can stage and copy in one batch while the GPU checks another.
+   ps_edge_bridge_submit stages the host edges into the slot's pinned mirror
+   (the caller's arrays may be reused once it returns) and queues the copy
+   in, the check and the copy out; ps_edge_bridge_wait waits for that slot's
+   call and writes its outputs to host arrays (out_clearance when the call's
+   params asked for clearance). A slot takes a new call only after the
+   previous one was waited for (PS_EINVAL otherwise). ps_edge_bridge_evaluate
+   is submit + wait on slot 0. ps_edge_bridge_status reports the call waited
+   for last. */
+int ps_edge_bridge_submit(ps_edge_bridge* bridge, int slot, const float* from_flat,
+                          const float* to_flat, int num_edges,
+                          const ps_edge_params* params);
+int ps_edge_bridge_wait(ps_edge_bridge* bridge, int slot, uint8_t* out_valid,
+                        float* out_cost, float* out_clearance);
 int ps_edge_bridge_status(const ps_edge_bridge* bridge, int* status);
-/* The bridge's pinned host input mirrors (row-major [max_edges * dim]
-   each), valid until destroy. A caller may write its edges there and pass
+/* The bridge's pinned host input mirrors of slot 0 (row-major
+   [max_edges * dim] each), valid until destroy. A caller may write its edges there and pass
    these two pointers to ps_edge_bridge_evaluate, which then skips its staging
    copy. No reference counterpart (its mirrors are private). */
 int ps_edge_bridge_host_inputs(ps_edge_bridge* bridge, float** from_flat, float** to_flat);

@@ -37,6 +37,7 @@ PS_MAX_SPHERES = 512
 PS_MAX_OBBS = 1024
 PS_MAX_LAYERS = 8
 PS_EDGES_STATIC_MAX = 65536
+PS_BRIDGE_SLOTS = 2
 PS_MAX_TRAJ_LEN = 16384
 
 # joint types (utils.cuh:20-26)
@@ -226,6 +227,9 @@ _SIGNATURES = [
     ("ps_edge_bridge_evaluate", C.c_int,
      [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(EdgeParams), C.c_void_p, C.c_void_p,
       C.c_void_p]),
+    ("ps_edge_bridge_submit", C.c_int,
+     [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(EdgeParams)]),
+    ("ps_edge_bridge_wait", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("ps_edge_bridge_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     ("ps_edge_bridge_host_inputs", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     ("ps_edge_bridge_destroy", C.c_int, [C.c_void_p]),

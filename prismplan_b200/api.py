@@ -299,6 +299,7 @@ class EdgeEvalGpu:
         self._h = h
         self._params_key = None
         self._params_c = None
+        self._pending = {}
 
     def set_scene(self, scene) -> None:
         """Use another scene (its tensors must outlive the calls)."""
@@ -331,8 +332,43 @@ class EdgeEvalGpu:
                                                      clr.ctypes.data if params.compute_clearance else None))
         return valid, cost, clr
 
+    def submit(self, from_flat, to_flat, num_edges: int, params: EdgeEvalParams, slot: int = 0) -> int:
+        """Asynchronous half of ``evaluate`` on one of the bridge's two slots:
+        stages the host arrays (they may be reused on return) and queues the
+        copy in, the check and the copy out. ``wait(slot)`` returns the
+        outputs. While the GPU checks one slot's batch, the host can stage and
+        submit the other's."""
+        n = int(num_edges)
+        if n > self.max_edges:
+            raise RuntimeError("EdgeEvalGpu: num_edges exceeds max_edges_")
+        if slot in self._pending:
+            raise RuntimeError(f"EdgeEvalGpu: slot {slot} has a call not yet waited for")
+        f = np.ascontiguousarray(from_flat, dtype=np.float32)
+        t = np.ascontiguousarray(to_flat, dtype=np.float32)
+        if n > 0 and (f.size < n * self.dim or t.size < n * self.dim):
+            raise ValueError("from_flat/to_flat hold fewer than num_edges * dim values")
+        key = tuple(vars(params).values())
+        if key != self._params_key:
+            self._params_c, self._params_key = params.to_c(), key
+        _lib.check(self._lib.ps_edge_bridge_submit(self._h, int(slot), f.ctypes.data, t.ctypes.data, n,
+                                                   C.byref(self._params_c)))
+        self._pending[slot] = (max(n, 0), bool(params.compute_clearance))
+        return slot
+
+    def wait(self, slot: int = 0):
+        """Outputs of the call submitted to ``slot`` (as ``evaluate`` returns them)."""
+        if slot not in self._pending:
+            raise RuntimeError(f"EdgeEvalGpu: slot {slot} has no call to wait for")
+        n, want_clr = self._pending.pop(slot)
+        valid = np.empty(n, np.uint8)
+        cost = np.empty(n, np.float32)
+        clr = np.empty(n, np.float32) if want_clr else np.zeros(0, np.float32)
+        _lib.check(self._lib.ps_edge_bridge_wait(self._h, int(slot), valid.ctypes.data, cost.ctypes.data,
+                                                 clr.ctypes.data if want_clr else None))
+        return valid, cost, clr
+
     def status(self) -> int:
-        """PS_ETIMEOUT when the last call's time budget ran out, else PS_OK."""
+        """PS_ETIMEOUT when the time budget of the call waited for last ran out, else PS_OK."""
         code = C.c_int(0)
         _lib.check(self._lib.ps_edge_bridge_status(self._h, C.byref(code)))
         return code.value

@@ -79,65 +79,83 @@ struct GraphEntry {
 // edges the device inputs are d_in = [from (n rows) | to (n rows)] and the
 // device outputs d_out = [cost (n floats) | valid (n bytes)]; the pinned
 // mirrors h_in and h_out hold the same layouts. The in-place input mirrors
-// that ps_edge_bridge_host_inputs hands out are fixed instead (from at
-// h_in, to at h_in + max_edges rows): inputs written there go over in one
-// copy when n == max_edges and in two otherwise.
+// that ps_edge_bridge_host_inputs hands out (slot 0's) are fixed instead
+// (from at h_in, to at h_in + max_edges rows): inputs written there go over
+// in one copy when n == max_edges and in two otherwise.
+//
+// A slot holds one call in flight: its buffers, workspace, stream, captured
+// graphs and a completion event. Two slots let a caller stage and copy in
+// one batch while the GPU checks the other.
+struct BridgeSlot {
+    float *d_in = nullptr, *d_out = nullptr, *d_clr = nullptr;
+    void* d_ws = nullptr;
+    float *h_in = nullptr, *h_out = nullptr, *h_clr = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    std::list<GraphEntry> graphs;   // most recently used first
+    bool pending = false;           // submitted, not yet waited for
+    int n = 0;
+    bool clearance = false;
+};
+
 struct ps_edge_bridge {
     const ps_model* model = nullptr;
     ps_scene_view scene{};
     int dim = 0, max_edges = 0, device = 0;
-    float *d_in = nullptr, *d_out = nullptr, *d_clr = nullptr;
-    void* d_ws = nullptr;
     size_t ws_bytes = 0;
-    float *h_in = nullptr, *h_out = nullptr, *h_clr = nullptr;
-    cudaStream_t stream = nullptr;
-    std::list<GraphEntry> graphs;   // most recently used first
+    BridgeSlot slot[PS_BRIDGE_SLOTS];
+    int last_slot = 0;   // slot of the last call waited for
 };
 
 namespace {
 
+void release_slot(BridgeSlot& sl) {
+    for (auto& g : sl.graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    sl.graphs.clear();
+    if (sl.done) cudaEventDestroy(sl.done);
+    if (sl.stream) cudaStreamDestroy(sl.stream);
+    cudaFree(sl.d_in);
+    cudaFree(sl.d_out);
+    cudaFree(sl.d_clr);
+    cudaFree(sl.d_ws);
+    cudaFreeHost(sl.h_in);
+    cudaFreeHost(sl.h_out);
+    cudaFreeHost(sl.h_clr);
+}
+
 void release(ps_edge_bridge* b) {
     if (!b) return;
-    for (auto& g : b->graphs)
-        if (g.exec) cudaGraphExecDestroy(g.exec);
-    b->graphs.clear();
-    if (b->stream) cudaStreamDestroy(b->stream);
-    cudaFree(b->d_in);
-    cudaFree(b->d_out);
-    cudaFree(b->d_clr);
-    cudaFree(b->d_ws);
-    cudaFreeHost(b->h_in);
-    cudaFreeHost(b->h_out);
-    cudaFreeHost(b->h_clr);
+    for (auto& sl : b->slot) release_slot(sl);
     delete b;
 }
 
-int check_edges_on(ps_edge_bridge* b, int n, const ps_edge_params* P) {
+int check_edges_on(ps_edge_bridge* b, BridgeSlot& sl, int n, const ps_edge_params* P) {
     const size_t rows = (size_t)n * b->dim;
-    uint8_t* valid = reinterpret_cast<uint8_t*>(b->d_out + n);
-    return ps_check_edges(b->model, &b->scene, b->d_in, b->d_in + rows, nullptr, n, P, valid, b->d_out,
-                          P->compute_clearance ? b->d_clr : nullptr, b->d_ws, b->ws_bytes, b->stream);
+    uint8_t* valid = reinterpret_cast<uint8_t*>(sl.d_out + n);
+    return ps_check_edges(b->model, &b->scene, sl.d_in, sl.d_in + rows, nullptr, n, P, valid, sl.d_out,
+                          P->compute_clearance ? sl.d_clr : nullptr, sl.d_ws, b->ws_bytes, sl.stream);
 }
 
-// The check of n edges with these parameters on the bridge's stream: a graph
+// The check of n edges with these parameters on the slot's stream: a graph
 // replay when the key was seen before; otherwise an eager run, after which
 // the same launches are captured for the next call with this key.
-int launch_check(ps_edge_bridge* b, int n, const ps_edge_params* P) {
+int launch_check(ps_edge_bridge* b, BridgeSlot& sl, int n, const ps_edge_params* P) {
     GraphKey key;
     key.n = n;
     key.p = *P;
     key.v = b->scene;
-    for (auto it = b->graphs.begin(); it != b->graphs.end(); ++it)
+    for (auto it = sl.graphs.begin(); it != sl.graphs.end(); ++it)
         if (it->key == key) {
-            b->graphs.splice(b->graphs.begin(), b->graphs, it);
-            PS_TRY_CUDA(cudaGraphLaunch(it->exec, b->stream));
+            sl.graphs.splice(sl.graphs.begin(), sl.graphs, it);
+            PS_TRY_CUDA(cudaGraphLaunch(it->exec, sl.stream));
             return PS_OK;
         }
-    if (int rc = check_edges_on(b, n, P)) return rc;
-    PS_TRY_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    const int rc = check_edges_on(b, n, P);
+    if (int rc = check_edges_on(b, sl, n, P)) return rc;
+    PS_TRY_CUDA(cudaStreamBeginCapture(sl.stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = check_edges_on(b, sl, n, P);
     cudaGraph_t g = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    const cudaError_t e = cudaStreamEndCapture(sl.stream, &g);
     if (rc != PS_OK || e != cudaSuccess || !g) {   // not kept: the eager run above already did the work
         if (g) cudaGraphDestroy(g);
         cudaGetLastError();
@@ -150,11 +168,23 @@ int launch_check(ps_edge_bridge* b, int n, const ps_edge_params* P) {
         cudaGetLastError();
         return PS_OK;
     }
-    if (b->graphs.size() >= kMaxGraphs) {
-        cudaGraphExecDestroy(b->graphs.back().exec);
-        b->graphs.pop_back();
+    if (sl.graphs.size() >= kMaxGraphs) {
+        cudaGraphExecDestroy(sl.graphs.back().exec);
+        sl.graphs.pop_back();
     }
-    b->graphs.push_front(GraphEntry{key, exec});
+    sl.graphs.push_front(GraphEntry{key, exec});
+    return PS_OK;
+}
+
+int check_slot_arg(const ps_edge_bridge* b, int slot) {
+    if (!b) return set_error(PS_EINVAL, "bridge is NULL");
+    if (slot < 0 || slot >= PS_BRIDGE_SLOTS)
+        return set_error(PS_EINVAL, "slot must be 0 .. " + std::to_string(PS_BRIDGE_SLOTS - 1));
+    int dev = 0;
+    PS_TRY_CUDA(cudaGetDevice(&dev));
+    if (dev != b->device)
+        return set_error(PS_EINVAL, "bridge created on device " + std::to_string(b->device) +
+                                        ", current device is " + std::to_string(dev));
     return PS_OK;
 }
 
@@ -185,14 +215,17 @@ extern "C" int ps_edge_bridge_create(const ps_model* model, const ps_scene_view*
     auto step = [&](cudaError_t r) {
         if (e == cudaSuccess) e = r;
     };
-    step(cudaMalloc(&b->d_in, 2 * cfg));
-    step(cudaMalloc(&b->d_out, ne * 5));
-    step(cudaMalloc(&b->d_clr, ne * 4));
-    step(cudaMalloc(&b->d_ws, b->ws_bytes));
-    step(cudaHostAlloc(&b->h_in, 2 * cfg, cudaHostAllocDefault));
-    step(cudaHostAlloc(&b->h_out, ne * 5, cudaHostAllocDefault));
-    step(cudaHostAlloc(&b->h_clr, ne * 4, cudaHostAllocDefault));
-    step(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    for (auto& sl : b->slot) {
+        step(cudaMalloc(&sl.d_in, 2 * cfg));
+        step(cudaMalloc(&sl.d_out, ne * 5));
+        step(cudaMalloc(&sl.d_clr, ne * 4));
+        step(cudaMalloc(&sl.d_ws, b->ws_bytes));
+        step(cudaHostAlloc(&sl.h_in, 2 * cfg, cudaHostAllocDefault));
+        step(cudaHostAlloc(&sl.h_out, ne * 5, cudaHostAllocDefault));
+        step(cudaHostAlloc(&sl.h_clr, ne * 4, cudaHostAllocDefault));
+        step(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
+        step(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+    }
     if (e != cudaSuccess) {
         release(b);
         return cuda_error(e, "ps_edge_bridge_create allocations");
@@ -212,8 +245,76 @@ extern "C" int ps_edge_bridge_set_scene(ps_edge_bridge* b, const ps_scene_view* 
 extern "C" int ps_edge_bridge_host_inputs(ps_edge_bridge* b, float** from_flat, float** to_flat) {
     clear_error();
     if (!b || !from_flat || !to_flat) return set_error(PS_EINVAL, "bridge or output pointer is NULL");
-    *from_flat = b->h_in;
-    *to_flat = b->h_in + (size_t)b->max_edges * b->dim;
+    *from_flat = b->slot[0].h_in;
+    *to_flat = b->slot[0].h_in + (size_t)b->max_edges * b->dim;
+    return PS_OK;
+}
+
+extern "C" int ps_edge_bridge_submit(ps_edge_bridge* b, int slot, const float* from_flat, const float* to_flat,
+                                     int num_edges, const ps_edge_params* P) {
+    PS_NVTX("ps_edge_bridge_submit");
+    clear_error();
+    if (int rc = check_slot_arg(b, slot)) return rc;
+    if (!P) return set_error(PS_EINVAL, "params is NULL");
+    BridgeSlot& sl = b->slot[slot];
+    if (sl.pending) return set_error(PS_EINVAL, "slot " + std::to_string(slot) + " has a call not yet waited for");
+    if (num_edges > b->max_edges)
+        return set_error(PS_EINVAL, "num_edges " + std::to_string(num_edges) + " exceeds max_edges " +
+                                        std::to_string(b->max_edges));
+    sl.n = num_edges > 0 ? num_edges : 0;
+    sl.clearance = P->compute_clearance != 0;
+    if (sl.n == 0) {   // the reference returns empty outputs (:66)
+        sl.pending = true;
+        return PS_OK;
+    }
+    if (!from_flat || !to_flat) return set_error(PS_EINVAL, "from_flat/to_flat NULL");
+    const size_t rows = (size_t)num_edges * b->dim, bytes = rows * sizeof(float);
+    float* fixed_to = sl.h_in + (size_t)b->max_edges * b->dim;
+    if (from_flat == sl.h_in && to_flat == fixed_to) {   // written in place: nothing to stage
+        if (num_edges == b->max_edges) {
+            PS_TRY_CUDA(cudaMemcpyAsync(sl.d_in, sl.h_in, 2 * bytes, cudaMemcpyHostToDevice, sl.stream));
+        } else {
+            PS_TRY_CUDA(cudaMemcpyAsync(sl.d_in, sl.h_in, bytes, cudaMemcpyHostToDevice, sl.stream));
+            PS_TRY_CUDA(cudaMemcpyAsync(sl.d_in + rows, fixed_to, bytes, cudaMemcpyHostToDevice, sl.stream));
+        }
+    } else {
+        // Stage into the pinned mirror on OpenMP threads (one thread copies
+        // 10-20 GB/s, below the host-to-device link), then copy in at once.
+        // The slot's previous call was waited for, so its mirror is free.
+        stage_parallel(sl.h_in, from_flat, bytes);
+        stage_parallel(sl.h_in + rows, to_flat, bytes);
+        PS_TRY_CUDA(cudaMemcpyAsync(sl.d_in, sl.h_in, 2 * bytes, cudaMemcpyHostToDevice, sl.stream));
+    }
+    if (int rc = launch_check(b, sl, num_edges, P)) {
+        cudaStreamSynchronize(sl.stream);
+        return rc;
+    }
+    const size_t n = (size_t)num_edges;
+    PS_TRY_CUDA(cudaMemcpyAsync(sl.h_out, sl.d_out, n * 5, cudaMemcpyDeviceToHost, sl.stream));
+    if (sl.clearance) PS_TRY_CUDA(cudaMemcpyAsync(sl.h_clr, sl.d_clr, n * 4, cudaMemcpyDeviceToHost, sl.stream));
+    PS_TRY_CUDA(cudaEventRecord(sl.done, sl.stream));
+    sl.pending = true;
+    return PS_OK;
+}
+
+extern "C" int ps_edge_bridge_wait(ps_edge_bridge* b, int slot, uint8_t* out_valid, float* out_cost,
+                                   float* out_clearance) {
+    PS_NVTX("ps_edge_bridge_wait");
+    clear_error();
+    if (int rc = check_slot_arg(b, slot)) return rc;
+    BridgeSlot& sl = b->slot[slot];
+    if (!sl.pending) return set_error(PS_EINVAL, "slot " + std::to_string(slot) + " has no call to wait for");
+    const size_t n = (size_t)sl.n;
+    if (n > 0 && (!out_valid || !out_cost)) return set_error(PS_EINVAL, "out_valid/out_cost NULL");
+    if (n > 0 && sl.clearance && !out_clearance)
+        return set_error(PS_EINVAL, "compute_clearance was set but out_clearance is NULL");
+    sl.pending = false;
+    if (n == 0) return PS_OK;
+    PS_TRY_CUDA(cudaEventSynchronize(sl.done));
+    std::memcpy(out_cost, sl.h_out, n * 4);
+    std::memcpy(out_valid, reinterpret_cast<const uint8_t*>(sl.h_out + n), n);
+    if (sl.clearance) std::memcpy(out_clearance, sl.h_clr, n * 4);
+    b->last_slot = slot;
     return PS_OK;
 }
 
@@ -232,52 +333,25 @@ extern "C" int ps_edge_bridge_evaluate(ps_edge_bridge* b, const float* from_flat
         return set_error(PS_EINVAL, "from_flat/to_flat/out_valid/out_cost NULL");
     if (P->compute_clearance && !out_clearance)
         return set_error(PS_EINVAL, "compute_clearance set but out_clearance is NULL");
-    int dev = 0;
-    PS_TRY_CUDA(cudaGetDevice(&dev));
-    if (dev != b->device)
-        return set_error(PS_EINVAL, "bridge created on device " + std::to_string(b->device) +
-                                        ", current device is " + std::to_string(dev));
-    const size_t rows = (size_t)num_edges * b->dim, bytes = rows * sizeof(float);
-    float* fixed_to = b->h_in + (size_t)b->max_edges * b->dim;
-    if (from_flat == b->h_in && to_flat == fixed_to) {   // written in place: nothing to stage
-        if (num_edges == b->max_edges) {
-            PS_TRY_CUDA(cudaMemcpyAsync(b->d_in, b->h_in, 2 * bytes, cudaMemcpyHostToDevice, b->stream));
-        } else {
-            PS_TRY_CUDA(cudaMemcpyAsync(b->d_in, b->h_in, bytes, cudaMemcpyHostToDevice, b->stream));
-            PS_TRY_CUDA(cudaMemcpyAsync(b->d_in + rows, fixed_to, bytes, cudaMemcpyHostToDevice, b->stream));
-        }
-    } else {
-        // Stage into the pinned mirror on OpenMP threads (one thread copies
-        // 10-20 GB/s, below the host-to-device link), then copy in at once.
-        stage_parallel(b->h_in, from_flat, bytes);
-        stage_parallel(b->h_in + rows, to_flat, bytes);
-        PS_TRY_CUDA(cudaMemcpyAsync(b->d_in, b->h_in, 2 * bytes, cudaMemcpyHostToDevice, b->stream));
-    }
-    if (int rc = launch_check(b, num_edges, P)) {
-        cudaStreamSynchronize(b->stream);
+    if (b->slot[0].pending) return set_error(PS_EINVAL, "slot 0 has a submitted call not yet waited for");
+    if (int rc = ps_edge_bridge_submit(b, 0, from_flat, to_flat, num_edges, P)) {
+        b->slot[0].pending = false;
         return rc;
     }
-    const size_t n = (size_t)num_edges;
-    PS_TRY_CUDA(cudaMemcpyAsync(b->h_out, b->d_out, n * 5, cudaMemcpyDeviceToHost, b->stream));
-    if (P->compute_clearance)
-        PS_TRY_CUDA(cudaMemcpyAsync(b->h_clr, b->d_clr, n * 4, cudaMemcpyDeviceToHost, b->stream));
-    PS_TRY_CUDA(cudaStreamSynchronize(b->stream));
-    std::memcpy(out_cost, b->h_out, n * 4);
-    std::memcpy(out_valid, reinterpret_cast<const uint8_t*>(b->h_out + n), n);
-    if (P->compute_clearance) std::memcpy(out_clearance, b->h_clr, n * 4);
-    return PS_OK;
+    return ps_edge_bridge_wait(b, 0, out_valid, out_cost, out_clearance);
 }
 
 extern "C" int ps_edge_bridge_status(const ps_edge_bridge* b, int* status) {
     clear_error();
     if (!b) return set_error(PS_EINVAL, "bridge is NULL");
-    return ps_edges_status(b->d_ws, status);
+    return ps_edges_status(b->slot[b->last_slot].d_ws, status);
 }
 
 extern "C" int ps_edge_bridge_destroy(ps_edge_bridge* b) {
     clear_error();
     if (!b) return PS_OK;
-    cudaStreamSynchronize(b->stream);
+    for (auto& sl : b->slot)
+        if (sl.stream) cudaStreamSynchronize(sl.stream);
     release(b);
     return PS_OK;
 }

@@ -194,3 +194,50 @@ def test_bridge_argument_errors(w2):
                                        cost.ctypes.data, None) == _lib.PS_EINVAL
     ev.close()
     ev.close()   # a second close is a no-op
+
+
+def test_bridge_submit_wait_slots(w2):
+    """Two slots in flight: every batch equals the synchronous call bit for bit,
+    in a pipelined loop that submits one slot while the other runs."""
+    wl, b, sc = w2
+    E = 8192
+    p = api.EdgeEvalParams(max_joint_step=0.01, max_samples=600)
+    ev = api.EdgeEvalGpu(7, E, sc, b)
+    rng = np.random.default_rng(11)
+    batches = []
+    for k in range(6):
+        n = E if k % 3 else 5000
+        sel = rng.permutation(len(wl["from"]))[:n]
+        batches.append((np.ascontiguousarray(wl["from"][sel]), np.ascontiguousarray(wl["to"][sel]), n))
+    ref = [ev.evaluate(f, t, n, p) for f, t, n in batches]
+    outs = [None] * len(batches)
+    ev.submit(*batches[0], p, slot=0)
+    for k in range(1, len(batches) + 1):
+        if k < len(batches):
+            ev.submit(*batches[k], p, slot=k % 2)
+        outs[k - 1] = ev.wait((k - 1) % 2)
+    for (v, c, _), (rv, rc, _) in zip(outs, ref):
+        np.testing.assert_array_equal(v, rv)
+        assert np.array_equal(_bits(c), _bits(rc))
+    assert ev.status() == _lib.PS_OK
+    # one call per slot at a time; waiting needs a call
+    ev.submit(*batches[0], p, slot=1)
+    with pytest.raises(RuntimeError):
+        ev.submit(*batches[1], p, slot=1)
+    lib = _lib.load()
+    pc = p.to_c()
+    f, t, n = batches[1]
+    assert lib.ps_edge_bridge_submit(ev._h, 1, f.ctypes.data, t.ctypes.data, n, C.byref(pc)) == _lib.PS_EINVAL
+    assert lib.ps_edge_bridge_submit(ev._h, 2, f.ctypes.data, t.ctypes.data, n, C.byref(pc)) == _lib.PS_EINVAL
+    v, c, _ = ev.wait(1)
+    np.testing.assert_array_equal(v, ref[0][0])
+    with pytest.raises(RuntimeError):
+        ev.wait(1)
+    v = np.empty(1, np.uint8)
+    c = np.empty(1, np.float32)
+    assert lib.ps_edge_bridge_wait(ev._h, 0, v.ctypes.data, c.ctypes.data, None) == _lib.PS_EINVAL
+    # an empty submission waits to empty outputs
+    ev.submit(f[:0], t[:0], 0, p, slot=0)
+    v, c, k = ev.wait(0)
+    assert v.size == 0 and c.size == 0 and k.size == 0
+    ev.close()
