@@ -200,6 +200,15 @@ __global__ void __launch_bounds__(kCfgThreads, kClr ? 6 : 4) check_configs_fast_
     stage_scene(sv, obbs, orig, layers, counters, &bmax, sc);
     const ModelSmem M = model_view(blob);
     const int D = M.H->n_dof, NJ = M.H->n_joints;
+    // the clearance loop's box pairs, after the configuration tiles
+    ObbPair* pairs = reinterpret_cast<ObbPair*>(
+        reinterpret_cast<unsigned char*>(qtile) + (((size_t)kCfgThreads * D * 4 + 15) & ~size_t(15)));
+    const int n_pairs = (sc.n_obbs + 1) / 2;
+    if (kClr) {
+        __syncthreads();   // the staged boxes are visible
+        stage_obb_pairs(sc, pairs);
+        __syncthreads();
+    }
     const bool no_gate = (flags & PS_NO_GATE) != 0;
     const bool want_obb_clr = kClr && (flags & PS_CLEARANCE_OBB) != 0;
     const bool want_esdf_clr = kClr && (flags & PS_CLEARANCE_ESDF) != 0;
@@ -259,7 +268,8 @@ __global__ void __launch_bounds__(kCfgThreads, kClr ? 6 : 4) check_configs_fast_
                 }
                 if (kStats) st.v[ST_SPHERES] += 4;
                 if (sc.n_obbs) {
-                    spheres_min_dsq<4>(sc, px, py, pz, mn);
+                    if (kClr) spheres_min_dsq_pairs<4>(pairs, n_pairs, px, py, pz, mn);
+                    else spheres_min_dsq<4>(sc, px, py, pz, mn);
                     if (kStats) st.v[ST_PAIRS] += 4 * sc.n_obbs;
                 }
 #pragma unroll
@@ -429,6 +439,7 @@ extern "C" int ps_check_configs(const ps_model* m, const ps_scene_view* scene, c
     // Without a clearance source the output (if any) is the 1000 sentinel.
     const bool clr = clearance != nullptr && (flags & (PS_CLEARANCE_OBB | PS_CLEARANCE_ESDF));
     size_t smem = (size_t)m->dev.bytes_core + scene_smem_bytes(scene) + (size_t)kCfgThreads * m->info.n_dof * 4;
+    smem = ((smem + 15) & ~size_t(15)) + (size_t)((scene->n_obbs + 1) / 2) * sizeof(ObbPair);   // box pairs
     const int blocks_needed = (n + kCfgThreads - 1) / kCfgThreads;
     const int per_sm = (flags >> 8) & 15u ? (int)((flags >> 8) & 15u) : 8;   // PS_CONFIG_BLOCKS_PER_SM
     const int grid = std::max(1, std::min(blocks_needed, sm_count() * per_sm));

@@ -229,6 +229,108 @@ __device__ __forceinline__ void spheres_min_dsq(const SceneSmem& sc, const float
     }
 }
 
+// Packed two-lane FP32 arithmetic of sm_100 (fma/mul .f32x2): each half is
+// the IEEE-rounded scalar operation, so a packed chain gives the scalar
+// chain's bits; one instruction does the work of two.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2_pack(float lo, float hi) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(f32x2 v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ f32x2 f2_mul(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// Two boxes side by side for the packed loop: every coefficient of box 2k
+// in the low half and of box 2k + 1 in the high half (rows of the map with
+// the translation, exact half extents). A missing second box is a far one.
+struct ObbPair {             // 128 bytes
+    f32x2 r0[4], r1[4], r2[4];
+    f32x2 h[3];
+    f32x2 pad;
+};
+
+// Builds the pair table from the staged boxes (every thread calls it; the
+// caller syncs after).
+__device__ __forceinline__ void stage_obb_pairs(const SceneSmem& sc, ObbPair* pairs) {
+    const int np = (sc.n_obbs + 1) / 2;
+    for (int k = threadIdx.x; k < np; k += blockDim.x) {
+        const ObbPrep& a = sc.obbs[2 * k];
+        // a missing second box: identity rows with a 1e15 m translation,
+        // d^2 ~ 1e30, never the minimum when a real box exists
+        const bool has_b = 2 * k + 1 < sc.n_obbs;
+        const ObbPrep& b = sc.obbs[has_b ? 2 * k + 1 : 2 * k];
+        const float4 b0 = has_b ? b.r0 : make_float4(1.0f, 0.0f, 0.0f, 1.0e15f);
+        const float4 b1 = has_b ? b.r1 : make_float4(0.0f, 1.0f, 0.0f, 1.0e15f);
+        const float4 b2 = has_b ? b.r2 : make_float4(0.0f, 0.0f, 1.0f, 1.0e15f);
+        const float4 bh = has_b ? b.h : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        ObbPair& p = pairs[k];
+        p.r0[0] = f2_pack(a.r0.x, b0.x); p.r0[1] = f2_pack(a.r0.y, b0.y);
+        p.r0[2] = f2_pack(a.r0.z, b0.z); p.r0[3] = f2_pack(a.r0.w, b0.w);
+        p.r1[0] = f2_pack(a.r1.x, b1.x); p.r1[1] = f2_pack(a.r1.y, b1.y);
+        p.r1[2] = f2_pack(a.r1.z, b1.z); p.r1[3] = f2_pack(a.r1.w, b1.w);
+        p.r2[0] = f2_pack(a.r2.x, b2.x); p.r2[1] = f2_pack(a.r2.y, b2.y);
+        p.r2[2] = f2_pack(a.r2.z, b2.z); p.r2[3] = f2_pack(a.r2.w, b2.w);
+        p.h[0] = f2_pack(a.h.x, bh.x); p.h[1] = f2_pack(a.h.y, bh.y); p.h[2] = f2_pack(a.h.z, bh.z);
+        p.pad = 0ull;
+    }
+}
+
+// spheres_min_dsq over the pair table: the box map and the squared distance
+// of two boxes per packed instruction, each half with fast_box_dsq's
+// operation order, so min d^2 has the same bits (min is exact and its order
+// does not matter).
+template <int kN>
+__device__ __forceinline__ void spheres_min_dsq_pairs(const ObbPair* pairs, int n_pairs, const float* px,
+                                                      const float* py, const float* pz, float* mn) {
+    f32x2 X[kN], Y[kN], Z[kN];
+#pragma unroll
+    for (int i = 0; i < kN; ++i) {
+        mn[i] = 3.0e38f;
+        X[i] = f2_pack(px[i], px[i]);
+        Y[i] = f2_pack(py[i], py[i]);
+        Z[i] = f2_pack(pz[i], pz[i]);
+    }
+    for (int k = 0; k < n_pairs; ++k) {
+        const ObbPair& p = pairs[k];
+        const f32x2 a0 = p.r0[0], a1 = p.r0[1], a2 = p.r0[2], a3 = p.r0[3];
+        const f32x2 b0 = p.r1[0], b1 = p.r1[1], b2 = p.r1[2], b3 = p.r1[3];
+        const f32x2 c0 = p.r2[0], c1 = p.r2[1], c2 = p.r2[2], c3 = p.r2[3];
+        float hxa, hxb, hya, hyb, hza, hzb;
+        f2_unpack(p.h[0], hxa, hxb);
+        f2_unpack(p.h[1], hya, hyb);
+        f2_unpack(p.h[2], hza, hzb);
+#pragma unroll
+        for (int i = 0; i < kN; ++i) {
+            const f32x2 lx = f2_fma(a2, Z[i], f2_fma(a1, Y[i], f2_fma(a0, X[i], a3)));
+            const f32x2 ly = f2_fma(b2, Z[i], f2_fma(b1, Y[i], f2_fma(b0, X[i], b3)));
+            const f32x2 lz = f2_fma(c2, Z[i], f2_fma(c1, Y[i], f2_fma(c0, X[i], c3)));
+            float lxa, lxb, lya, lyb, lza, lzb;
+            f2_unpack(lx, lxa, lxb);
+            f2_unpack(ly, lya, lyb);
+            f2_unpack(lz, lza, lzb);
+            const f32x2 cx = f2_pack(fmaxf(fabsf(lxa) - hxa, 0.0f), fmaxf(fabsf(lxb) - hxb, 0.0f));
+            const f32x2 cy = f2_pack(fmaxf(fabsf(lya) - hya, 0.0f), fmaxf(fabsf(lyb) - hyb, 0.0f));
+            const f32x2 cz = f2_pack(fmaxf(fabsf(lza) - hza, 0.0f), fmaxf(fabsf(lzb) - hzb, 0.0f));
+            const f32x2 d = f2_fma(cz, cz, f2_fma(cy, cy, f2_mul(cx, cx)));
+            float da, db;
+            f2_unpack(d, da, db);
+            mn[i] = fminf(mn[i], fminf(da, db));
+        }
+    }
+}
+
 // Decision from a precomputed min d^2 (clearance path): exact rescan only
 // inside the guard band.
 __device__ __forceinline__ bool decide_from_min(const SceneSmem& sc, float px, float py, float pz, float sr,
