@@ -257,14 +257,14 @@ def run_ours(args):
     valid_frac = float(out[0].float().mean().item())
     timed_out = (out[0].cpu().numpy().copy(), out[1].cpu().numpy().copy())   # the timed step's verdicts and costs
     del graph
-    # prep, queue pass 0, finalize; the end-sample probe when the tuned shape
-    # (or, automatic, at least 8 warps of edges per SM) runs it; a second
-    # queue pass when the edges are fewer than 8 per resident warp (the tuned
-    # queue residency, or 5 blocks of 4 warps per SM for this kernel variant)
+    # Kernels per step: the preparation, or the end-sample probe whose launch
+    # also prepares (when the tuned shape, or automatic with at least 8 warps
+    # of edges per SM, runs it); queue pass 0; finalize; and a second queue
+    # pass when the edges are fewer than 8 per resident warp (the tuned queue
+    # residency, or 5 blocks of 4 warps per SM for this kernel variant)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
-    probe_on = tuning["probe"] == 1 or (tuning["probe"] == 0 and E >= 8 * 32 * sms)
     qres = tuning["queue_blocks_per_sm"] or 5
-    launches_per_step = 3 + (1 if probe_on else 0) + (1 if E < 8 * sms * qres * 4 else 0)
+    launches_per_step = 3 + (1 if E < 8 * sms * qres * 4 else 0)
 
     result = None
     # With several ranks every rank measures its own end-to-end bridge (the
