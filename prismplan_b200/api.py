@@ -301,6 +301,19 @@ class EdgeEvalGpu:
         self._params_c = None
         self._pending = {}
 
+    def host_inputs(self):
+        """The bridge's pinned input mirrors (slot 0) as numpy arrays
+        (from, to: [max_edges, dim] float32), valid until ``close``. Edges
+        written there and passed to ``evaluate`` as ``from_flat`` / ``to_flat``
+        go to the device without a staging copy."""
+        if getattr(self, "_views", None) is None:
+            pf, pt = C.c_void_p(), C.c_void_p()
+            _lib.check(self._lib.ps_edge_bridge_host_inputs(self._h, C.byref(pf), C.byref(pt)))
+            shape = (self.max_edges, self.dim)
+            self._views = (np.ctypeslib.as_array(C.cast(pf, C.POINTER(C.c_float)), shape=shape),
+                           np.ctypeslib.as_array(C.cast(pt, C.POINTER(C.c_float)), shape=shape))
+        return self._views
+
     def set_scene(self, scene) -> None:
         """Use another scene (its tensors must outlive the calls)."""
         view = _view(scene)
@@ -375,6 +388,7 @@ class EdgeEvalGpu:
 
     def close(self) -> None:
         if getattr(self, "_h", None):
+            self._views = None   # views of the mirrors the destroy frees
             self._lib.ps_edge_bridge_destroy(self._h)
             self._h = None
 

@@ -30,11 +30,11 @@ namespace {
 constexpr size_t kMaxGraphs = 8;
 
 // Host copy of `bytes` split over OpenMP threads in pieces of at least
-// 256 KiB (a single thread below that). In a process that already runs an
+// 128 KiB (a single thread below that). In a process that already runs an
 // OpenMP runtime under the same soname (a PyTorch process does), the team
 // is that runtime's, whose threads are already up.
 void stage_parallel(void* dst, const void* src, size_t bytes) {
-    constexpr size_t kPiece = 256 << 10;
+    constexpr size_t kPiece = 128 << 10;
     const int pieces = (int)std::min<size_t>((bytes + kPiece - 1) / kPiece, 64);
     const int threads = std::min(pieces, std::max(1, omp_get_max_threads()));
     if (threads <= 1) {
@@ -279,11 +279,13 @@ extern "C" int ps_edge_bridge_submit(ps_edge_bridge* b, int slot, const float* f
         }
     } else {
         // Stage into the pinned mirror on OpenMP threads (one thread copies
-        // 10-20 GB/s, below the host-to-device link), then copy in at once.
-        // The slot's previous call was waited for, so its mirror is free.
+        // 10-20 GB/s, below the host-to-device link): the `from` rows first,
+        // whose copy in then runs while the `to` rows are staged. The slot's
+        // previous call was waited for, so its mirror is free.
         stage_parallel(sl.h_in, from_flat, bytes);
+        PS_TRY_CUDA(cudaMemcpyAsync(sl.d_in, sl.h_in, bytes, cudaMemcpyHostToDevice, sl.stream));
         stage_parallel(sl.h_in + rows, to_flat, bytes);
-        PS_TRY_CUDA(cudaMemcpyAsync(sl.d_in, sl.h_in, 2 * bytes, cudaMemcpyHostToDevice, sl.stream));
+        PS_TRY_CUDA(cudaMemcpyAsync(sl.d_in + rows, sl.h_in + rows, bytes, cudaMemcpyHostToDevice, sl.stream));
     }
     if (int rc = launch_check(b, sl, num_edges, P)) {
         cudaStreamSynchronize(sl.stream);

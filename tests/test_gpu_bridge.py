@@ -241,3 +241,22 @@ def test_bridge_submit_wait_slots(w2):
     v, c, k = ev.wait(0)
     assert v.size == 0 and c.size == 0 and k.size == 0
     ev.close()
+
+
+def test_bridge_host_input_views(w2):
+    """Edges written into the numpy views of the pinned mirrors go in without
+    staging and give the same bits as the same edges passed as plain arrays."""
+    wl, b, sc = w2
+    E = 4096
+    p = api.EdgeEvalParams(max_joint_step=0.01, max_samples=600)
+    ev = api.EdgeEvalGpu(7, E, sc, b)
+    mf, mt = ev.host_inputs()
+    assert mf.shape == (E, 7) and mt.shape == (E, 7) and mf.dtype == np.float32
+    for n in (E, 1000):
+        mf[:n] = wl["from"][:n]
+        mt[:n] = wl["to"][:n]
+        v, c, _ = ev.evaluate(mf, mt, n, p)
+        rv, rc, _ = ev.evaluate(np.ascontiguousarray(wl["from"][:n]), np.ascontiguousarray(wl["to"][:n]), n, p)
+        np.testing.assert_array_equal(v, rv)
+        assert np.array_equal(_bits(c), _bits(rc))
+    ev.close()
