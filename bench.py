@@ -667,7 +667,7 @@ def bench_configs(dev, with_ref=True):
                                  lambda: api.check_configs(b, sc, q, clearance="obb", blocks_per_sm=bps))
     peak = probe_peak()
     ach = flops_from_stats(stats) / (kms * 1e-3) / 1e12
-    out["roofline"] = {"bound": "fp32", "kernel": "check_configs_kernel<clearance>", "kernel_ms": kms,
+    out["roofline"] = {"bound": "fp32", "kernel": "check_configs_fast_kernel<clearance>", "kernel_ms": kms,
                        "achieved": ach, "peak": peak["tflops"], "unit": "TFLOP/s", "frac": ach / peak["tflops"],
                        "flops_per_launch": flops_from_stats(stats),
                        "work_per_launch": dict(zip(["pairs", "exact", "samples", "joints", "spheres", "self",
