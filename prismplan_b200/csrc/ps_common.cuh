@@ -51,7 +51,8 @@ struct JointRec {
 // The same pairs as runs: sruns[r] = (i | q << 9 | len << 14, j0) is sphere i
 // against the len consecutive spheres j0..j0+len-1 of joint q (DFS position).
 // Runs are ordered by joint pair (joint of i, q), then i, then j0;
-// sjp[k] = (a | q << 16, first run, end run, 0) lists the joint pairs.
+// sjp[k] = (a | q << 16, first run, end run, 0) lists the joint pairs, nearest
+// in DFS order (|q - a|) first.
 // Limits (global memory): lower[n_dof], upper[n_dof].
 struct ModelDev {
     const unsigned char* blob;     // device

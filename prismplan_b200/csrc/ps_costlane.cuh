@@ -28,14 +28,17 @@
 //      ancestors: dC/dq_p += a_p . (M - o_p x F) (revolute) or a_p . F
 //      (prismatic), a_p and o_p the joint axis and origin from the frames;
 //   5. self hinge, on the world sphere centres that step 3 left in shared
-//      memory: the group's lanes split the joint pairs' bound tests (one ballot
-//      gives each pair's OR over the warp's waypoints); a pair that can come
-//      within m_self expands its runs (sphere i of joint a against consecutive
-//      spheres j of joint q), split over the group's lanes; a lane skips its
-//      run when i is out of reach of q's bound sphere on its own waypoint.
-//      Only pairs within r_i + r_j + m_self can set the hinge, and a square
-//      root is taken only for those; the minimum over the group is taken by
-//      (value, pair order), and the argmin pair's force goes to both joints'
+//      memory. It is a minimum, so every test culls against the smallest
+//      clearance the group has found so far (the cull level; m_self at the
+//      start), and the joint pairs come nearest in DFS order first, so that
+//      level drops early. The group's lanes split the joint pairs' bound
+//      tests (one ballot gives each pair's OR over the warp's waypoints); a
+//      pair that can come below the level expands its runs (sphere i of joint
+//      a against consecutive spheres j of joint q), split over the group's
+//      lanes; a lane skips its run when i is out of reach of q's bound sphere
+//      on its own waypoint. A square root is taken only for pairs that can
+//      come below the level; the minimum over the group is taken by (value,
+//      pair order), and the argmin pair's force goes to both joints'
 //      ancestors.
 // Every candidate set is a superset of what the waypoint itself needs, and
 // the group size is fixed, so a waypoint gives the same bits whatever other
@@ -435,8 +438,14 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
         const float smg = P.self_margin, smp = fmaxf(smg, 0.0f);
         float bv = smg;   // pairs at or above the margin cannot set the hinge
         int bk = INT_MAX, bi = -1, bj = -1;
+        // cull level: the smallest clearance the group has found (at most bv).
+        // A pair or run that cannot come below it cannot set the group's
+        // minimum; the joint pairs come nearest first, so it drops early.
+        float cl = smg;
         auto at = [&](const float* a, int k, int c) { return a[(k * 3 + c) * kCostSlots + slot]; };
         for (int jp0 = 0; jp0 < md.n_sjp; jp0 += kCostSub) {
+            cl = fminf(cl, __shfl_xor_sync(kCostFull, cl, 1));
+            cl = fminf(cl, __shfl_xor_sync(kCostFull, cl, 2));
             // lane u tests joint pair jp0 + u on its own waypoint; one ballot
             // gives each pair's OR over the warp's waypoints
             bool pass = false;
@@ -448,9 +457,10 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
                 const float dx = ax - qx0, dy = ay - qy0, dz = az - qz0;
                 const float S = fmaxf(fmaxf(fabsf(ax), fmaxf(fabsf(ay), fabsf(az))),
                                       fmaxf(fabsf(qx0), fmaxf(fabsf(qy0), fabsf(qz0))));
-                float thr = M.J[a].bound.w + M.J[qj].bound.w + smp;
-                thr += 4.0f * (S + thr + 1.0f) * PS_GUARD_K;
-                pass = fmaf(dz, dz, fmaf(dy, dy, dx * dx)) < thr * thr;
+                const float rr = M.J[a].bound.w + M.J[qj].bound.w;
+                // clearance of any pair >= |c_a - c_q| - R_a - R_q, plus a guard for the FP32 centres
+                const float thr = rr + cl + 4.0f * (S + rr + smp + 1.0f) * PS_GUARD_K;
+                pass = thr > 0.0f && fmaf(dz, dz, fmaf(dy, dy, dx * dx)) < thr * thr;
                 if (kStats) st.v[ST_SELF] += 1;
             }
             const unsigned bal = __ballot_sync(kCostFull, pass);
@@ -460,12 +470,12 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
                 const int a = (int)(e.x & 0xffffu), qj = (int)(e.x >> 16);
                 const float Ra = M.J[a].bound.w, Rq = M.J[qj].bound.w;
                 const float cqx = at(ws.bc, qj, 0), cqy = at(ws.bc, qj, 1), cqz = at(ws.bc, qj, 2);
-                // run reach: r_i + R_q + max(m_self, 0) plus a guard for the FP32
-                // centres, from bounds that hold for every sphere i of joint a
+                // run reach: clearance of sphere i against any sphere of q >= |p_i - c_q| - R_q - r_i;
+                // the guard covers the FP32 centres, from bounds that hold for every sphere i of joint a
                 const float Sjp = fmaxf(fmaxf(fabsf(at(ws.bc, a, 0)), fmaxf(fabsf(at(ws.bc, a, 1)),
                                                                             fabsf(at(ws.bc, a, 2)))) + Ra,
                                         fmaxf(fabsf(cqx), fmaxf(fabsf(cqy), fabsf(cqz))));
-                const float reach = Rq + smp + 4.0f * (Sjp + Ra + Rq + smp + 1.0f) * PS_GUARD_K;
+                const float reach = Rq + 4.0f * (Sjp + Ra + Rq + smp + 1.0f) * PS_GUARD_K;
                 // the group's lanes split the runs; a lane tests its run on its own waypoint
                 for (int r0 = (int)e.y; r0 < (int)e.z; r0 += kCostSub) {
                     const int r = r0 + u;
@@ -475,12 +485,13 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
                     const float ri = M.S[i].w;
                     const float pxi = at(ws.pos, i, 0), pyi = at(ws.pos, i, 1), pzi = at(ws.pos, i, 2);
                     const float ex = pxi - cqx, ey = pyi - cqy, ez = pzi - cqz;
-                    const float rt = ri + reach;
+                    const float rt = ri + reach + cl;
                     if (kStats) st.v[ST_SELF] += 1;
-                    if (fmaf(ez, ez, fmaf(ey, ey, ex * ex)) >= rt * rt) continue;   // no pair can set the hinge
-                    // sqrt(d2) - (ri + rj) < bv needs d2 < (bv + ri + rj)^2 (widened for
-                    // rounding); when bv + ri + rj <= 0 the exact test below fails anyway
-                    float tb = bv + ri;
+                    if (rt <= 0.0f || fmaf(ez, ez, fmaf(ey, ey, ex * ex)) >= rt * rt) continue;   // none gets below cl
+                    // sqrt(d2) - (ri + rj) < cl needs d2 < (cl + ri + rj)^2 (widened for
+                    // rounding); when cl + ri + rj <= 0 no pair gets below cl and the
+                    // test passes at most pairs that the exact test then keeps out of the group minimum
+                    float tb = cl + ri;
 #pragma unroll 4
                     for (int m = 0; m < len; ++m) {
                         const int j = j0 + m;
@@ -489,14 +500,16 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
                         const float d2 = fmaf(vz, vz, fmaf(vy, vy, vx * vx));
                         const float rj = M.S[j].w;
                         const float t = tb + rj;
-                        if (d2 * (1.0f - 4.0e-6f) < t * t) {   // can beat bv: take the root
+                        if (d2 * (1.0f - 4.0e-6f) < t * t) {   // can get below cl: take the root
                             const float c = sqrtf(d2) - (ri + rj);
-                            if (c < bv) {
+                            const int key = (r << 9) | m;
+                            if (c < bv || (c == bv && key < bk)) {
                                 bv = c;
-                                tb = bv + ri;
-                                bk = (r << 9) | m;
+                                bk = key;
                                 bi = i;
                                 bj = j;
+                                cl = fminf(cl, c);
+                                tb = cl + ri;
                             }
                         }
                     }

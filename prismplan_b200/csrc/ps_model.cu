@@ -286,6 +286,25 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
         sruns.push_back(runs[r].w1);
     }
     if (!sjp.empty()) sjp[sjp.size() - 2] = (uint32_t)runs.size();
+    // The cost kernels visit the joint pairs in this table's order and cull
+    // by the smallest clearance found so far, so pairs likely to be close come
+    // first: by DFS distance |q - a| (on a chain, the number of joints
+    // between them), then (a, q). The runs keep their order, which defines
+    // the tie-break among equal clearances.
+    {
+        const size_t njp = sjp.size() / 4;
+        std::vector<size_t> ord(njp);
+        for (size_t k = 0; k < njp; ++k) ord[k] = k;
+        auto gap = [&](size_t k) {
+            const int a = (int)(sjp[4 * k] & 0xffffu), q = (int)(sjp[4 * k] >> 16);
+            return a > q ? a - q : q - a;
+        };
+        std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return gap(x) < gap(y); });
+        std::vector<uint32_t> sorted(sjp.size());
+        for (size_t k = 0; k < njp; ++k)
+            for (int w = 0; w < 4; ++w) sorted[4 * k + w] = sjp[4 * ord[k] + w];
+        sjp.swap(sorted);
+    }
 
     bool shares = std::memcmp(aft, d->fixed_transforms, sizeof(float) * 16 * nj) == 0;
     for (int i = 0; i < nj && shares; ++i) shares = atypes[i] == d->joint_types[i];
