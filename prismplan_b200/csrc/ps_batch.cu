@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(kWarps * 32, 16 / kWarps) batch_waypoint_kerne
         const int lo = traj ? 0 : cap - n_roll, hi = traj ? n_wp : cap;
         const int k = lo + (traj ? c : c - chunks_a) * kCostSlots + slot;
         const int kc = k < hi ? k : hi - 1;   // past the end: repeat the last waypoint
-        for (int d = u; d < D; d += kCostSub) ws.q[d * kCostSlots + slot] = q[(size_t)kc * D + d];
+        for (int d = u; d < D; d += kCostSub) lane_put_q(ws, slot, d, q[(size_t)kc * D + d]);
         __syncwarp();
         st.zero();
         if (traj) {
@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(kW * 32, 16 / kW)
             const int k = lo + (traj ? c : c - chunks_a) * kCostSlots + slot;
             const int kc = k < hi ? k : hi - 1;   // past the end: repeat the last waypoint
             __syncwarp();   // the previous group's readers of the scratch are done
-            for (int d = u; d < D; d += kCostSub) ws.q[d * kCostSlots + slot] = q[(size_t)kc * D + d];
+            for (int d = u; d < D; d += kCostSub) lane_put_q(ws, slot, d, q[(size_t)kc * D + d]);
             __syncwarp();
             if (traj) {
                 const float v = lane_cost<true, false>(M, md, sc, sv, CP, cb, ws, st);

@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(kLaneCostWarps * 32, 2) waypoint_cost_kernel(
         const bool live = idx < total && !(skip && skip[b]);
         if (!__any_sync(kCostFull, live)) continue;   // uniform
         for (int d = u; d < D; d += kCostSub)
-            ws.q[d * kCostSlots + slot] = bdt ? q[((size_t)b * D + d) * T + tt] : q[((size_t)b * T + tt) * D + d];
+            lane_put_q(ws, slot, d, bdt ? q[((size_t)b * D + d) * T + tt] : q[((size_t)b * T + tt) * D + d]);
         __syncwarp();
         LaneStats ls;
         ls.zero();

@@ -61,9 +61,9 @@ constexpr int kLaneCostWarps = 8;            // warps per block of the cost kern
 // Per-warp scratch floats, SoA over the warp's waypoint slots: frames of
 // joints 1..NJ-1 (joint 0 is the identity), world bound centres, world
 // sphere centres, per-joint gradient (gradient only), the waypoint's
-// configuration.
+// configuration and each DoF's sine and cosine.
 __host__ __device__ inline int lane_cost_floats(int NJ, int NS, int D, bool grad) {
-    return kCostSlots * (12 * (NJ - 1) + 3 * NJ + 3 * NS + (grad ? NJ : 0) + D);
+    return kCostSlots * (12 * (NJ - 1) + 3 * NJ + 3 * NS + (grad ? NJ : 0) + 3 * D);
 }
 __host__ __device__ inline size_t lane_warp_bytes(int NJ, int NS, int D, int n_obbs, bool grad) {
     return (size_t)lane_cost_floats(NJ, NS, D, grad) * 4 +
@@ -76,6 +76,7 @@ struct LaneScratch {
     float* pos;       // [NS*3][slots]
     float* dq;        // [NJ][slots] (gradient only)
     float* q;         // [D][slots]
+    float* sc;        // [2*D][slots]: sin, cos of each DoF (accurate sincosf)
     uint16_t* cand;   // [n_obbs]: boxes kept by the current joint's broad phase (warp-uniform)
 };
 
@@ -92,8 +93,21 @@ __device__ __forceinline__ LaneScratch lane_carve(unsigned char* base, int NJ, i
     if (grad) f += kCostSlots * NJ;
     s.q = f;
     f += kCostSlots * D;
+    s.sc = f;
+    f += kCostSlots * 2 * D;
     s.cand = reinterpret_cast<uint16_t*>(f);
     return s;
+}
+
+// Stages DoF d of the slot's waypoint, with its sine and cosine: the lanes of
+// a group split the DoFs, so each angle's sincosf runs once per waypoint and
+// the FK of every lane of the group reads it (a __syncwarp follows).
+__device__ __forceinline__ void lane_put_q(const LaneScratch& ws, int slot, int d, float v) {
+    float sn, cs;
+    sincosf(v, &sn, &cs);
+    ws.q[d * kCostSlots + slot] = v;
+    ws.sc[(2 * d) * kCostSlots + slot] = sn;
+    ws.sc[(2 * d + 1) * kCostSlots + slot] = cs;
 }
 
 // Bytes of a lane cost block: model core, staged scene, block tables, the
@@ -313,8 +327,14 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
         } else {
             Affine Pf;
             lane_frame(ws.fr, jr.parent_pos, slot, Pf);
-            const float qi = jr.dof >= 0 ? ws.q[jr.dof * kCostSlots + slot] : 0.0f;
-            joint_compose<false>(jr, qi, Pf, T);
+            const int dof = jr.dof;
+            float qi = 0.0f, sn = 0.0f, cs = 1.0f;   // sincosf(0) for a joint without a DoF
+            if (dof >= 0) {
+                qi = ws.q[dof * kCostSlots + slot];
+                sn = ws.sc[(2 * dof) * kCostSlots + slot];
+                cs = ws.sc[(2 * dof + 1) * kCostSlots + slot];
+            }
+            joint_compose_sc(jr, qi, sn, cs, Pf, T);
             if (u == 0) {
                 float* b = ws.fr + (size_t)(p - 1) * 12 * kCostSlots + slot;
 #pragma unroll
