@@ -508,10 +508,13 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
                     const float rt = ri + reach + cl;
                     if (kStats) st.v[ST_SELF] += 1;
                     if (rt <= 0.0f || fmaf(ez, ez, fmaf(ey, ey, ex * ex)) >= rt * rt) continue;   // none gets below cl
-                    // sqrt(d2) - (ri + rj) < cl needs d2 < (cl + ri + rj)^2 (widened for
-                    // rounding); when cl + ri + rj <= 0 no pair gets below cl and the
-                    // test passes at most pairs that the exact test then keeps out of the group minimum
-                    float tb = cl + ri;
+                    // sqrt(d2) - (ri + rj) <= cl needs sqrt(d2) <= cl + ri + rj; the bound t
+                    // adds 2e-6 (|cl| + ri + rj), some 16 ulps of every term that rounds in
+                    // either expression, so a pair at the cull level itself (a tie with a
+                    // pair another lane found) is never rejected here, however close its
+                    // centres. When t <= 0 no pair gets below cl and the test passes at most
+                    // pairs that the exact test then keeps out of the group minimum.
+                    float tb = cl + ri + 2.0e-6f * (fabsf(cl) + ri);
 #pragma unroll 4
                     for (int m = 0; m < len; ++m) {
                         const int j = j0 + m;
@@ -519,7 +522,7 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
                                     vz = pzi - at(ws.pos, j, 2);
                         const float d2 = fmaf(vz, vz, fmaf(vy, vy, vx * vx));
                         const float rj = M.S[j].w;
-                        const float t = tb + rj;
+                        const float t = fmaf(rj, 1.000002f, tb);
                         if (d2 * (1.0f - 4.0e-6f) < t * t) {   // can get below cl: take the root
                             const float c = sqrtf(d2) - (ri + rj);
                             const int key = (r << 9) | m;
@@ -529,7 +532,7 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
                                 bi = i;
                                 bj = j;
                                 cl = fminf(cl, c);
-                                tb = cl + ri;
+                                tb = cl + ri + 2.0e-6f * (fabsf(cl) + ri);
                             }
                         }
                     }
