@@ -452,6 +452,32 @@ def test_rollout_costs_vs_reference_stomp():
     assert rel64.max() < COST_REL_TOL
 
 
+def test_rollout_costs_full_workload_vs_fp64():
+    """All 409,600 rollout waypoints of workload 4 against the FP64 oracle.
+    The self hinge culls against the smallest clearance found so far, so this
+    covers the deep self overlaps (near-concentric spheres of two joints) that
+    only some requests of the full workload reach, where a cull that rejected
+    the minimum pair would lower the cost by several units."""
+    wl = workloads.workload(4)
+    b = RobotModelBuilder.from_asset(wl["asset"]).build()
+    sc = SceneTensors(*wl["obbs"])
+    om = oracle.OracleModel(b, *wl["obbs"])
+    r = wl["rollouts"]
+    p = api.CostParams(collision_cost_weight=wl["w"], world_collision_margin=wl["eps"],
+                       self_collision_margin=wl["self_margin"])
+    ours = api.rollout_costs(b, sc, torch.from_numpy(r).cuda(), p).cpu().numpy().reshape(-1)
+    R, D, T = r.shape
+    q = r.transpose(0, 2, 1).reshape(-1, D)
+    c64 = om.state_cost(q, wl["w"], wl["eps"], wl["self_margin"])
+    no_self = om.state_cost(q, wl["w"], wl["eps"], -1.0e9)
+    deep = int(((c64 - no_self) > wl["w"] * 0.1).sum())   # self term above w * 0.1: overlap deeper than 0.09 m
+    rel = np.abs(ours - c64) / np.maximum(np.abs(c64), 1.0)
+    print(f"rollout cost, full workload: max rel err vs fp64 = {rel.max():.2e}; "
+          f"{deep} waypoints with a self overlap deeper than 0.09 m")
+    assert deep > 0
+    assert rel.max() < COST_REL_TOL
+
+
 def test_edges_probe_path_bitexact():
     """The end-sample probe runs in front of the persistent queue when there
     are at least 8 edges per SM lane group (38 K on a B200): at 0.6 of
