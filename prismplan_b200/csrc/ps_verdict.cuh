@@ -423,10 +423,11 @@ __device__ __forceinline__ void fk_step(const JointRec& jr, int p, const float* 
 // every exact and approximate sphere and every joint's bound centre are
 // staged in shared memory, SoA by thread (stride kLanes).
 //
-// The exact pairs run as the model's runs (sphere i against the spheres of
-// one joint q): a run is skipped when |p_i - c_q| >= r_i + R_q plus the
-// guard band, R_q bounding |p_j - c_q| + r_j for every sphere j of q, so no
-// pair of the run can pass the float test; the others are tested pair by
+// The exact pairs run by joint pair (a, q), then as the model's runs (sphere
+// i of a against the spheres of q): a joint pair is skipped when
+// |c_a - c_q| >= R_a + R_q and a run when |p_i - c_q| >= r_i + R_q, each plus
+// the guard band, R_q bounding |p_j - c_q| + r_j for every sphere j of q, so
+// no pair they hold can pass the float test; the others are tested pair by
 // pair with the reference's float test. The verdict is an OR over pairs, so
 // the order and the skipped runs change the work, not the result.
 // ---------------------------------------------------------------------------
@@ -508,22 +509,42 @@ __device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const floa
                             at(apos, j, 2), M.A[j].w);
     }
     if (!need) return false;
-    for (int r = 0; r < md.n_sruns; ++r) {
-        const uint2 run = __ldg(md.sruns + r);
-        const int i = run.x & 0x1ff, q = (run.x >> 9) & 0x1f, len = run.x >> 14;
-        const float px = at(pos, i, 0), py = at(pos, i, 1), pz = at(pos, i, 2), ri = M.S[i].w;
-        const float4 bq = M.J[q].bound;
-        const float cx = at(cpos, q, 0), cy = at(cpos, q, 1), cz = at(cpos, q, 2);
-        const float dx = px - cx, dy = py - cy, dz = pz - cz;
-        const float S = fmaxf(fmaxf(fabsf(px), fmaxf(fabsf(py), fabsf(pz))), fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))));
-        float lim = ri + bq.w;
-        lim += 4.0f * (S + lim + 1.0f) * PS_GUARD_K;
-        st.v[ST_SELF] += 1;
-        if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) >= lim * lim * (1.0f + 1.0e-6f)) continue;   // no pair can hit
-        for (int k = 0; k < len; ++k) {
-            const int j = (int)run.y + k;
+    // joint pairs (a, q), nearest in DFS order first: a pair whose bound
+    // spheres are apart (|c_a - c_q| >= R_a + R_q plus the guard band) holds
+    // no pair that can pass the float test, so its runs are skipped
+    for (int jp = 0; jp < md.n_sjp; ++jp) {
+        const uint4 e = __ldg(md.sjp + jp);
+        const int a = (int)(e.x & 0xffffu), qj = (int)(e.x >> 16);
+        {
+            const float ax = at(cpos, a, 0), ay = at(cpos, a, 1), az = at(cpos, a, 2);
+            const float bx = at(cpos, qj, 0), by = at(cpos, qj, 1), bz = at(cpos, qj, 2);
+            const float dx = ax - bx, dy = ay - by, dz = az - bz;
+            const float S = fmaxf(fmaxf(fabsf(ax), fmaxf(fabsf(ay), fabsf(az))),
+                                  fmaxf(fabsf(bx), fmaxf(fabsf(by), fabsf(bz))));
+            float lim = M.J[a].bound.w + M.J[qj].bound.w;
+            lim += 4.0f * (S + lim + 1.0f) * PS_GUARD_K;
             st.v[ST_SELF] += 1;
-            if (ref_self_hit(px, py, pz, ri, at(pos, j, 0), at(pos, j, 1), at(pos, j, 2), M.S[j].w)) return true;
+            if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) >= lim * lim * (1.0f + 1.0e-6f)) continue;
+        }
+        const float4 bq = M.J[qj].bound;
+        const float cx = at(cpos, qj, 0), cy = at(cpos, qj, 1), cz = at(cpos, qj, 2);
+        for (int r = (int)e.y; r < (int)e.z; ++r) {
+            const uint2 run = __ldg(md.sruns + r);
+            const int i = run.x & 0x1ff, len = run.x >> 14;
+            const float px = at(pos, i, 0), py = at(pos, i, 1), pz = at(pos, i, 2), ri = M.S[i].w;
+            const float dx = px - cx, dy = py - cy, dz = pz - cz;
+            const float S =
+                fmaxf(fmaxf(fabsf(px), fmaxf(fabsf(py), fabsf(pz))), fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))));
+            float lim = ri + bq.w;
+            lim += 4.0f * (S + lim + 1.0f) * PS_GUARD_K;
+            st.v[ST_SELF] += 1;
+            if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) >= lim * lim * (1.0f + 1.0e-6f)) continue;   // no pair can hit
+            for (int k = 0; k < len; ++k) {
+                const int j = (int)run.y + k;
+                st.v[ST_SELF] += 1;
+                if (ref_self_hit(px, py, pz, ri, at(pos, j, 0), at(pos, j, 1), at(pos, j, 2), M.S[j].w))
+                    return true;
+            }
         }
     }
     return false;
