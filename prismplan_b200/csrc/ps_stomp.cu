@@ -135,14 +135,17 @@ __global__ void stomp_topk_kernel(const float* __restrict__ tot_prev, int* __res
     }
 }
 
-// One block per (rollout r, request b), row = r * B + b:
+// One block per group of kg rollouts r of request b, row = r * B + b:
 //   r < Rn (or < Rn + Ro on the first iteration): fresh rollout
 //     clamp(theta + L z), endpoints pinned (stomp.cu:96-130);
 //   Rn <= r < Rn + Ro afterwards: the previous iteration's reuse row, noise
 //     recomputed against the current optimum (stomp.cu:155-177);
 //   r = R - 1: the optimum itself with its state cost (stomp.cu:180-203).
-// Also writes the cost kernel's skip byte of rows < Rn + Ro.
-__global__ void stomp_rollouts_kernel(const float* __restrict__ theta, int B, int T, int D, int Rn, int Ro,
+// Also writes the cost kernel's skip byte of rows < Rn + Ro. The banded back
+// substitution is sequential over t, one thread per (rollout, DoF) chain:
+// with kg rollouts per block, kg * D threads run chains at once instead of
+// D while the rest of the block waits at the barrier.
+__global__ void stomp_rollouts_kernel(const float* __restrict__ theta, int B, int T, int D, int Rn, int Ro, int kg,
                                       const double* __restrict__ band, const double* __restrict__ amp,
                                       uint32_t key0, uint32_t key1, const float* __restrict__ lower,
                                       const float* __restrict__ upper, float* __restrict__ roll_cur,
@@ -151,60 +154,82 @@ __global__ void stomp_rollouts_kernel(const float* __restrict__ theta, int B, in
                                       const float* __restrict__ opt_sc, const int* __restrict__ topk,
                                       uint8_t* __restrict__ skip, const OptState* __restrict__ state,
                                       const uint8_t* __restrict__ done) {
-    extern __shared__ double zs[];   // [D][T], reversed order: zs[d * T + (T - 1 - t)] = z_t
-    const int r = blockIdx.x, b = blockIdx.y;
+    // shared: the band factor [T][5], then one chain of T + 1 doubles per
+    // (rollout g, DoF d) in reversed order, zs[(g * D + d) * (T + 1) + (T - 1 - t)] = z_t;
+    // the odd stride puts the chains that the threads walk side by side in
+    // different banks
+    extern __shared__ double sm_ro[];
+    double* Ls = sm_ro;
+    double* zs = sm_ro + (size_t)T * 5;
+    const int S = T + 1;
+    const int b = blockIdx.y, r0 = blockIdx.x * kg;
     const int R = Rn + Ro + 1;
+    const int ng = min(kg, R - r0);
     const bool active = stomp_active(state, done, b);
     const int step = state[b].step;
     const bool init = step == 1;
-    const size_t row = (size_t)r * B + b;
-    if (r < Rn + Ro && threadIdx.x == 0) skip[row] = (!active || (r >= Rn && !init)) ? 1 : 0;
+    for (int g = threadIdx.x; g < ng; g += blockDim.x) {
+        const int r = r0 + g;
+        if (r < Rn + Ro) skip[(size_t)r * B + b] = (!active || (r >= Rn && !init)) ? 1 : 0;
+    }
     if (!active) return;
     const float* th = theta + (size_t)b * T * D;
-    float* ro = roll_cur + row * T * D;
-    float* no = noise + row * T * D;
-    if (r == R - 1) {
-        for (int i = threadIdx.x; i < T * D; i += blockDim.x) {
-            ro[i] = th[i];
-            no[i] = 0.0f;
+    // fresh rollouts of the group: r < Rn, or r < Rn + Ro on the first iteration
+    auto fresh = [&](int r) { return r < Rn || (init && r < Rn + Ro); };
+    // copies: the optimum row and the reuse rows
+    for (int g = 0; g < ng; ++g) {
+        const int r = r0 + g;
+        if (fresh(r)) continue;
+        const size_t row = (size_t)r * B + b;
+        float* ro = roll_cur + row * T * D;
+        float* no = noise + row * T * D;
+        if (r == R - 1) {
+            for (int i = threadIdx.x; i < T * D; i += blockDim.x) {
+                ro[i] = th[i];
+                no[i] = 0.0f;
+            }
+            for (int t = threadIdx.x; t < T; t += blockDim.x) sc_cur[row * T + t] = opt_sc[(size_t)b * T + t];
+        } else {
+            const size_t srow = (size_t)topk[(size_t)b * Ro + (r - Rn)] * B + b;
+            const float* src = roll_prev + srow * T * D;
+            for (int i = threadIdx.x; i < T * D; i += blockDim.x) {
+                const float v = src[i];
+                ro[i] = v;
+                no[i] = v - th[i];
+            }
+            for (int t = threadIdx.x; t < T; t += blockDim.x) sc_cur[row * T + t] = sc_prev[srow * T + t];
         }
-        for (int t = threadIdx.x; t < T; t += blockDim.x) sc_cur[row * T + t] = opt_sc[(size_t)b * T + t];
-        return;
     }
-    if (r >= Rn && !init) {
-        const size_t srow = (size_t)topk[(size_t)b * Ro + (r - Rn)] * B + b;
-        const float* src = roll_prev + srow * T * D;
-        for (int i = threadIdx.x; i < T * D; i += blockDim.x) {
-            const float v = src[i];
-            ro[i] = v;
-            no[i] = v - th[i];
-        }
-        for (int t = threadIdx.x; t < T; t += blockDim.x) sc_cur[row * T + t] = sc_prev[srow * T + t];
-        return;
-    }
+    int nf = 0;   // fresh rollouts come first in a group (r ascending)
+    while (nf < ng && fresh(r0 + nf)) ++nf;
+    if (nf == 0) return;   // uniform over the block
+    for (int i = threadIdx.x; i < T * 5; i += blockDim.x) Ls[i] = band[i];
     const int nk = (T + 3) / 4;
-    for (int it = threadIdx.x; it < D * nk; it += blockDim.x) {
-        const int d = it / nk, k = it - d * nk;
-        const U4 o = philox4x32_10(U4{(uint32_t)k, (uint32_t)(r * D + d), (uint32_t)step, 0u}, key0, key1);
+    for (int it = threadIdx.x; it < nf * D * nk; it += blockDim.x) {
+        const int gd = it / nk, k = it - gd * nk;
+        const int g = gd / D, d = gd - g * D;
+        const U4 o = philox4x32_10(U4{(uint32_t)k, (uint32_t)((r0 + g) * D + d), (uint32_t)step, 0u}, key0, key1);
         float z[4];
         box_muller(o.x, o.y, z[0], z[1]);
         box_muller(o.z, o.w, z[2], z[3]);
         for (int j = 0; j < 4; ++j) {
             const int t = 4 * k + j;
-            if (t < T) zs[d * T + (T - 1 - t)] = (double)z[j];
+            if (t < T) zs[gd * S + (T - 1 - t)] = (double)z[j];
         }
     }
     __syncthreads();
-    if (threadIdx.x < D) band_back(band, zs + threadIdx.x * T, T);
+    for (int c = threadIdx.x; c < nf * D; c += blockDim.x) band_back(Ls, zs + (size_t)c * S, T);
     __syncthreads();
     const double a = amp[0];
-    for (int i = threadIdx.x; i < T * D; i += blockDim.x) {
-        const int t = i / D, d = i - t * D;
-        const float n = (t == 0 || t == T - 1) ? 0.0f : (float)(a * zs[d * T + (T - 1 - t)]);
-        const float base = th[i];
+    for (int i = threadIdx.x; i < nf * T * D; i += blockDim.x) {
+        const int g = i / (T * D), e = i - g * (T * D);
+        const int t = e / D, d = e - t * D;
+        const float n = (t == 0 || t == T - 1) ? 0.0f : (float)(a * zs[(g * D + d) * S + (T - 1 - t)]);
+        const float base = th[e];
         const float v = fmaxf(lower[d], fminf(upper[d], base + n));
-        ro[i] = v;
-        no[i] = v - base;
+        const size_t row = (size_t)(r0 + g) * B + b;
+        roll_cur[row * T * D + e] = v;
+        noise[row * T * D + e] = v - base;
     }
 }
 
@@ -468,7 +493,12 @@ extern "C" int ps_stomp_optimize(const ps_model* m, const ps_scene_view* scene, 
     opt_init_kernel<<<(B + 127) / 128, 128, 0, s>>>(o.state, o.done, B, P->num_iterations_after_valid, o.n_done, o.t0);
     PS_TRY_CUDA(cudaGetLastError());
 
-    const size_t ro_smem = sizeof(double) * (size_t)D * T;
+    // rollouts per block of the rollouts kernel: up to 8, within 96 KiB of
+    // shared memory and 128 chains (threads)
+    const size_t ro_one = sizeof(double) * (size_t)D * (T + 1), ro_band = sizeof(double) * 5 * (size_t)T;
+    const int ro_kg = (int)std::max<size_t>(1, std::min<size_t>({(size_t)8, (size_t)(96 * 1024) / ro_one,
+                                                                 (size_t)(128 / std::max(D, 1))}));
+    const size_t ro_smem = ro_band + ro_one * ro_kg;
     const int tot_threads = 128;
     const size_t tot_smem = sizeof(float) * ((size_t)2 * (T + 12) * D + tot_threads);
     const size_t pj_smem = sizeof(double) * 6 * (size_t)T;
@@ -493,7 +523,8 @@ extern "C" int ps_stomp_optimize(const ps_model* m, const ps_scene_view* scene, 
     auto iteration = [&](cudaStream_t q, int i) -> int {
         const int cur = i & 1, prev = cur ^ 1;
         stomp_topk_kernel<<<B, 32, sizeof(float) * R, q>>>(w.tot[prev], w.topk, R, Ro, B, o.state, o.done);
-        stomp_rollouts_kernel<<<dim3(R, B), 128, ro_smem, q>>>(theta, B, T, D, Rn, Ro, o.band, w.amp, key0, key1,
+        stomp_rollouts_kernel<<<dim3((R + ro_kg - 1) / ro_kg, B), 128, ro_smem, q>>>(theta, B, T, D, Rn, Ro, ro_kg,
+                                                              o.band, w.amp, key0, key1,
                                                               m->dev.lower, m->dev.upper, w.roll[cur], w.roll[prev],
                                                               w.noise, w.sc[cur], w.sc[prev], w.opt_sc, w.topk,
                                                               w.skip, o.state, o.done);
