@@ -63,19 +63,57 @@ __global__ void opt_band_kernel(int T, float dt_f, double* __restrict__ L) {
     }
 }
 
+// The two triangular halves of the banded solve, serial in one thread. The
+// last kBand results stay in registers, so a step's chain is its kBand
+// multiply-subtracts (j ascending, as the textbook loop takes them) and no
+// shared-memory round trip; the factor entries do not depend on the chain
+// and load ahead of it.
+static_assert(kBand == 4, "the register windows below hold kBand = 4 values");
+
+// x <- L^-1 x
+__device__ __forceinline__ void band_forward(const double* Ls, double* x, int T) {
+    double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;   // y[i-4], y[i-3], y[i-2], y[i-1]
+#pragma unroll 4
+    for (int i = 0; i < T; ++i) {
+        const double* l = Ls + i * 5;
+        double s = x[i];
+        if (i >= 4) s -= l[4] * w0;
+        if (i >= 3) s -= l[3] * w1;
+        if (i >= 2) s -= l[2] * w2;
+        if (i >= 1) s -= l[1] * w3;
+        const double y = s * l[0];
+        x[i] = y;
+        w0 = w1;
+        w1 = w2;
+        w2 = w3;
+        w3 = y;
+    }
+}
+
+// x <- L^-T x
+__device__ __forceinline__ void band_backward(const double* Ls, double* x, int T) {
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;   // x[i+1], x[i+2], x[i+3], x[i+4]
+#pragma unroll 4
+    for (int i = T - 1; i >= 0; --i) {
+        double s = x[i];
+        if (i + 1 <= T - 1) s -= Ls[(i + 1) * 5 + 1] * v0;
+        if (i + 2 <= T - 1) s -= Ls[(i + 2) * 5 + 2] * v1;
+        if (i + 3 <= T - 1) s -= Ls[(i + 3) * 5 + 3] * v2;
+        if (i + 4 <= T - 1) s -= Ls[(i + 4) * 5 + 4] * v3;
+        const double xi = s * Ls[i * 5];
+        x[i] = xi;
+        v3 = v2;
+        v2 = v1;
+        v1 = v0;
+        v0 = xi;
+    }
+}
+
 // x <- (L L^T)^-1 x for the banded factor of opt_band_kernel (Ls: 5 T
 // doubles, any memory). Serial, one thread.
 __device__ __forceinline__ void band_solve(const double* Ls, double* x, int T) {
-    for (int i = 0; i < T; ++i) {   // L y = g
-        double s = x[i];
-        for (int j = max(0, i - kBand); j < i; ++j) s -= Ls[i * 5 + (i - j)] * x[j];
-        x[i] = s * Ls[i * 5];
-    }
-    for (int i = T - 1; i >= 0; --i) {   // L^T x = y
-        double s = x[i];
-        for (int j = i + 1; j <= min(T - 1, i + kBand); ++j) s -= Ls[j * 5 + (j - i)] * x[j];
-        x[i] = s * Ls[i * 5];
-    }
+    band_forward(Ls, x, T);
+    band_backward(Ls, x, T);
 }
 
 __global__ void opt_init_kernel(OptState* __restrict__ st, uint8_t* __restrict__ done, int B, int polish,

@@ -69,13 +69,7 @@ __device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& z0, fl
 
 // x <- (Lb^T)^-1 x for the banded factor of opt_band_kernel (the second half
 // of band_solve).
-__device__ __forceinline__ void band_back(const double* Ls, double* x, int T) {
-    for (int i = T - 1; i >= 0; --i) {
-        double s = x[i];
-        for (int j = i + 1; j <= min(T - 1, i + kBand); ++j) s -= Ls[j * 5 + (j - i)] * x[j];
-        x[i] = s * Ls[i * 5];
-    }
-}
+__device__ __forceinline__ void band_back(const double* Ls, double* x, int T) { band_backward(Ls, x, T); }
 
 // Column scales of M and the noise amplitude (stomp_precompute.cpp:46-94):
 // with Rinv = (R + 1e-8 I)^-1, s_j = (1/T) / max_i Rinv(i, j) and
@@ -304,7 +298,11 @@ __global__ void stomp_weights_kernel(const float* __restrict__ sc_cur, const flo
             const size_t row = (size_t)r * B + b;
             return sc_cur[row * T + t] + ctrl[row * T * D + rem];
         };
+        // the rollout loops are unrolled so that each thread keeps several
+        // independent loads in flight (the kernel waits on memory otherwise);
+        // the sums still run in rollout order
         float mn = cost(0), mx = mn;
+#pragma unroll 8
         for (int r = 1; r < R; ++r) {
             const float c = cost(r);
             mn = fminf(mn, c);
@@ -312,9 +310,11 @@ __global__ void stomp_weights_kernel(const float* __restrict__ sc_cur, const flo
         }
         const float denom = fmaxf(mx - mn, 1.0e-8f);
         float sum = 0.0f;
+#pragma unroll 8
         for (int r = 0; r < R; ++r) sum += expf(-h * (cost(r) - mn) / denom);
         sum = fmaxf(sum, 1.0e-12f);
         float acc = 0.0f;
+#pragma unroll 8
         for (int r = 0; r < R; ++r) {
             const float p = expf(-h * (cost(r) - mn) / denom) / sum;
             acc += noise[((size_t)r * B + b) * T * D + rem] * p;
