@@ -299,30 +299,31 @@ __global__ void __launch_bounds__(kCfgThreads, kClr ? 6 : 4) check_configs_fast_
     if (kStats) flush_stats(stats, st);
 }
 
-// Self-collision two-phase check, one configuration per lane
-// (lane_self_hit), for the configurations without a scene hit.
-__global__ void __launch_bounds__(kSelfThreads) self_check_kernel(ModelDev md, const float* __restrict__ q, int n,
-                                                                  uint8_t* __restrict__ hit_out,
-                                                                  unsigned long long* stats) {
+// Self-collision two-phase check, a group of kSelfSub lanes per
+// configuration (group_self_hit), for the configurations without a scene hit.
+__global__ void __launch_bounds__(kSelfBlock, 3) self_check_kernel(ModelDev md, const float* __restrict__ q, int n,
+                                                                   uint8_t* __restrict__ hit_out,
+                                                                   unsigned long long* stats) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar;
     unsigned char* blob = smem;
-    if (!stage_model(md, blob, &mbar)) return configs_fail_closed(n, kSelfThreads, hit_out, nullptr);
+    if (!stage_model(md, blob, &mbar)) return configs_fail_closed(n, kSelfBlock, hit_out, nullptr);
     const ModelSmem M = model_view(blob);
     const int D = M.H->n_dof, NS = M.H->n_spheres, NA = M.H->n_approx, NJ = M.H->n_joints;
     const SelfSmem sm = carve_self<kSelfThreads>(smem + md.bytes_core, NS, NA, NJ);
     float* qtile = sm.cpos + (size_t)NJ * 3 * kSelfThreads;
     LaneStats st;
     st.zero();
-    const int lane = threadIdx.x;
+    const int slot = threadIdx.x / kSelfSub, u = threadIdx.x % kSelfSub;
     for (int base = blockIdx.x * kSelfThreads; base < n; base += gridDim.x * kSelfThreads) {
         const int cnt = min(kSelfThreads, n - base);
         __syncthreads();
-        for (int k = threadIdx.x; k < cnt * D; k += kSelfThreads) qtile[k] = q[(size_t)base * D + k];
+        for (int k = threadIdx.x; k < cnt * D; k += kSelfBlock) qtile[k] = q[(size_t)base * D + k];
         __syncthreads();
-        if (lane >= cnt) continue;
-        if (hit_out[base + lane]) continue;   // already in collision with the scene
-        if (lane_self_hit<kSelfThreads>(M, md, qtile + lane * D, sm, lane, st)) hit_out[base + lane] = 1;
+        if (slot >= cnt) continue;                // uniform over the group
+        if (hit_out[base + slot]) continue;       // already in collision with the scene (uniform over the group)
+        if (group_self_hit<kSelfThreads>(M, md, qtile + slot * D, sm, slot, u, st) && u == 0)
+            hit_out[base + slot] = 1;
     }
     flush_stats(stats, st);
 }
@@ -460,7 +461,7 @@ extern "C" int ps_check_configs(const ps_model* m, const ps_scene_view* scene, c
         const size_t ss = self_smem_bytes(m);
         PS_TRY_CUDA(allow_smem((const void*)self_check_kernel, ss));
         const int g2 = std::max(1, std::min((n + kSelfThreads - 1) / kSelfThreads, sm_count() * 8));
-        self_check_kernel<<<g2, kSelfThreads, ss, s>>>(m->dev, q, n, hit, g_stats);
+        self_check_kernel<<<g2, kSelfBlock, ss, s>>>(m->dev, q, n, hit, g_stats);
         PS_TRY_CUDA(cudaGetLastError());
     }
     return PS_OK;

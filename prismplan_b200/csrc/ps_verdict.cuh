@@ -416,12 +416,14 @@ __device__ __forceinline__ void fk_step(const JointRec& jr, int p, const float* 
 }
 
 // ---------------------------------------------------------------------------
-// Two-phase self check of one configuration per thread (two_phase_cc.cuh:
-// 108-131, runtime_kinematics.cuh:249-284 and 383-417): the approximate
-// sphere pairs first; the exact pairs only when an approximate pair
-// overlaps; the collision margin does not apply to self pairs. Positions of
-// every exact and approximate sphere and every joint's bound centre are
-// staged in shared memory, SoA by thread (stride kLanes).
+// Two-phase self check of one configuration (two_phase_cc.cuh:108-131,
+// runtime_kinematics.cuh:249-284 and 383-417): the approximate sphere pairs
+// first; the exact pairs only when an approximate pair overlaps; the
+// collision margin does not apply to self pairs. Positions of every exact and
+// approximate sphere and every joint's bound centre are staged in shared
+// memory, SoA by configuration slot (stride kLanes). lane_self_hit checks a
+// configuration on one thread (the edge self pass); group_self_hit on a
+// group of kSelfSub lanes (the configuration batch).
 //
 // The exact pairs run by joint pair (a, q), then as the model's runs (sphere
 // i of a against the spheres of q): a joint pair is skipped when
@@ -550,7 +552,134 @@ __device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const floa
     return false;
 }
 
-// Shared memory of a kSelfThreads-lane block running lane_self_hit: model
+// kSelfSub consecutive lanes check one configuration (a group; slot = the
+// configuration's column in the staged positions, u = the lane within the
+// group). Every lane of the group walks the FK and stores its share of the
+// sphere positions (spheres u, u + kSelfSub, ... of each joint); the group's
+// lanes then split the approximate pairs and, per joint pair that passes its
+// bound test, the runs, with a group ballot after each round (the verdict is
+// an OR, so the split changes the work, not the result). The check of a few
+// thousand configurations is latency-bound: one lane per configuration left
+// 3 warps per SM for the same shared memory (16,384 CHOMP waypoints: 49.6 ->
+// 26.5 us). The edge self pass keeps lane_self_hit: its windows of samples
+// ran slower with groups (104.7 -> 123.9 us).
+constexpr int kSelfSub = 4;
+constexpr int kSelfBlock = kSelfThreads * kSelfSub;   // threads of a self-check block
+
+template <int kSlots>
+__device__ bool group_self_hit(const ModelSmem& M, const ModelDev& md, const float* qc, const SelfSmem& sm, int slot,
+                               int u, LaneStats& st) {
+    const int NJ = M.H->n_joints;
+    const unsigned gmask = 0xfu << ((threadIdx.x & 31) & ~(kSelfSub - 1));
+    float* pos = sm.pos;
+    float* apos = sm.apos;
+    float* cpos = sm.cpos;
+    Affine s0, s1, T;
+    affine_identity(s0);
+    affine_identity(s1);
+    for (int p = 0; p < NJ; ++p) {
+        const JointRec& jr = M.J[p];
+        fk_step<true>(jr, p, qc, s0, s1, T);
+        for (int k = jr.sph_beg + u; k < jr.sph_end; k += kSelfSub) {
+            const float4 s = M.S[k];
+            float px, py, pz;
+            sphere_world(T, s.x, s.y, s.z, px, py, pz);
+            put3(pos, k, kSlots, slot, px, py, pz);
+        }
+        if (u == 0 && jr.bound.w >= 0.0f) {
+            float px, py, pz;
+            sphere_world(T, jr.bound.x, jr.bound.y, jr.bound.z, px, py, pz);
+            put3(cpos, p, kSlots, slot, px, py, pz);
+        }
+        if (M.H->approx_shares_chain) {
+            for (int k = jr.apx_beg + u; k < jr.apx_end; k += kSelfSub) {
+                const float4 s = M.A[k];
+                float px, py, pz;
+                sphere_world(T, s.x, s.y, s.z, px, py, pz);
+                put3(apos, k, kSlots, slot, px, py, pz);
+            }
+        }
+    }
+    if (!M.H->approx_shares_chain) {
+        affine_identity(s0);
+        affine_identity(s1);
+        for (int p = 0; p < NJ; ++p) {
+            const JointRec& jr = M.JA[p];
+            fk_step<true>(jr, p, qc, s0, s1, T);
+            for (int k = jr.apx_beg + u; k < jr.apx_end; k += kSelfSub) {
+                const float4 s = M.A[k];
+                float px, py, pz;
+                sphere_world(T, s.x, s.y, s.z, px, py, pz);
+                put3(apos, k, kSlots, slot, px, py, pz);
+            }
+        }
+    }
+    __syncwarp(gmask);   // the group's positions are written
+    auto at = [&](const float* a, int k, int c) { return a[(k * 3 + c) * kSlots + slot]; };
+    bool need = false;
+    for (int k0 = 0; k0 < M.H->n_apx_self_pairs; k0 += kSelfSub) {
+        const int k = k0 + u;
+        bool h = false;
+        if (k < M.H->n_apx_self_pairs) {
+            const uint32_t pr = __ldg(md.apx_self_pairs + k);
+            const int i = pr & 0xffff, j = pr >> 16;
+            st.v[ST_SELF] += 1;
+            h = ref_self_hit(at(apos, i, 0), at(apos, i, 1), at(apos, i, 2), M.A[i].w, at(apos, j, 0),
+                             at(apos, j, 1), at(apos, j, 2), M.A[j].w);
+        }
+        if (__ballot_sync(gmask, h)) {
+            need = true;
+            break;
+        }
+    }
+    if (!need) return false;
+    // joint pairs (a, q), nearest in DFS order first: a pair whose bound
+    // spheres are apart (|c_a - c_q| >= R_a + R_q plus the guard band) holds
+    // no pair that can pass the float test, so its runs are skipped
+    for (int jp = 0; jp < md.n_sjp; ++jp) {
+        const uint4 e = __ldg(md.sjp + jp);
+        const int a = (int)(e.x & 0xffffu), qj = (int)(e.x >> 16);
+        {   // the same test on every lane of the group: uniform
+            const float ax = at(cpos, a, 0), ay = at(cpos, a, 1), az = at(cpos, a, 2);
+            const float bx = at(cpos, qj, 0), by = at(cpos, qj, 1), bz = at(cpos, qj, 2);
+            const float dx = ax - bx, dy = ay - by, dz = az - bz;
+            const float S = fmaxf(fmaxf(fabsf(ax), fmaxf(fabsf(ay), fabsf(az))),
+                                  fmaxf(fabsf(bx), fmaxf(fabsf(by), fabsf(bz))));
+            float lim = M.J[a].bound.w + M.J[qj].bound.w;
+            lim += 4.0f * (S + lim + 1.0f) * PS_GUARD_K;
+            if (u == 0) st.v[ST_SELF] += 1;
+            if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) >= lim * lim * (1.0f + 1.0e-6f)) continue;
+        }
+        const float4 bq = M.J[qj].bound;
+        const float cx = at(cpos, qj, 0), cy = at(cpos, qj, 1), cz = at(cpos, qj, 2);
+        for (int r0 = (int)e.y; r0 < (int)e.z; r0 += kSelfSub) {
+            const int r = r0 + u;
+            bool h = false;
+            if (r < (int)e.z) {
+                const uint2 run = __ldg(md.sruns + r);
+                const int i = run.x & 0x1ff, len = run.x >> 14;
+                const float px = at(pos, i, 0), py = at(pos, i, 1), pz = at(pos, i, 2), ri = M.S[i].w;
+                const float dx = px - cx, dy = py - cy, dz = pz - cz;
+                const float S = fmaxf(fmaxf(fabsf(px), fmaxf(fabsf(py), fabsf(pz))),
+                                      fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))));
+                float lim = ri + bq.w;
+                lim += 4.0f * (S + lim + 1.0f) * PS_GUARD_K;
+                st.v[ST_SELF] += 1;
+                if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) < lim * lim * (1.0f + 1.0e-6f)) {   // else no pair can hit
+                    for (int k = 0; k < len && !h; ++k) {
+                        const int j = (int)run.y + k;
+                        st.v[ST_SELF] += 1;
+                        h = ref_self_hit(px, py, pz, ri, at(pos, j, 0), at(pos, j, 1), at(pos, j, 2), M.S[j].w);
+                    }
+                }
+            }
+            if (__ballot_sync(gmask, h)) return true;
+        }
+    }
+    return false;
+}
+
+// Shared memory of a self-check block (kSelfThreads configuration slots): model
 // core, sphere and bound positions and a tile of configurations.
 inline size_t self_smem_bytes(const ps_model* m) {
     return (size_t)m->dev.bytes_core +
