@@ -127,6 +127,11 @@ class ClockSampler:
                 self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(self.handle, nv.NVML_CLOCK_SM)
                 self.t = threading.Thread(target=self._poll, daemon=True)
                 self.t.start()
+                # the timed region is a few milliseconds: start it only once the
+                # poller answers, so that it is sampled throughout
+                t0 = time.perf_counter()
+                while not self.samples and self.error is None and time.perf_counter() - t0 < 0.5:
+                    time.sleep(0.0002)
         except Exception as e:   # no NVML: report no samples rather than fail the bench
             self.error = str(e)[:120]
         return self

@@ -298,24 +298,51 @@ __global__ void stomp_weights_kernel(const float* __restrict__ sc_cur, const flo
             const size_t row = (size_t)r * B + b;
             return sc_cur[row * T + t] + ctrl[row * T * D + rem];
         };
-        // the rollout loops are unrolled so that each thread keeps several
-        // independent loads in flight (the kernel waits on memory otherwise);
-        // the sums still run in rollout order
+        // the rollouts go in batches of 8 whose loads are all issued before
+        // their values are used, so that each thread keeps 16 or 24 loads in
+        // flight (the kernel waited on one load at a time); the min/max, the
+        // sum and the weighted noise still run in rollout order
+        constexpr int kB = 8;
         float mn = cost(0), mx = mn;
-#pragma unroll 8
-        for (int r = 1; r < R; ++r) {
+        int r = 1;
+        for (; r + kB <= R; r += kB) {
+            float c[kB];
+#pragma unroll
+            for (int k = 0; k < kB; ++k) c[k] = cost(r + k);
+#pragma unroll
+            for (int k = 0; k < kB; ++k) {
+                mn = fminf(mn, c[k]);
+                mx = fmaxf(mx, c[k]);
+            }
+        }
+        for (; r < R; ++r) {
             const float c = cost(r);
             mn = fminf(mn, c);
             mx = fmaxf(mx, c);
         }
         const float denom = fmaxf(mx - mn, 1.0e-8f);
         float sum = 0.0f;
-#pragma unroll 8
-        for (int r = 0; r < R; ++r) sum += expf(-h * (cost(r) - mn) / denom);
+        for (r = 0; r + kB <= R; r += kB) {
+            float c[kB];
+#pragma unroll
+            for (int k = 0; k < kB; ++k) c[k] = cost(r + k);
+#pragma unroll
+            for (int k = 0; k < kB; ++k) sum += expf(-h * (c[k] - mn) / denom);
+        }
+        for (; r < R; ++r) sum += expf(-h * (cost(r) - mn) / denom);
         sum = fmaxf(sum, 1.0e-12f);
         float acc = 0.0f;
-#pragma unroll 8
-        for (int r = 0; r < R; ++r) {
+        for (r = 0; r + kB <= R; r += kB) {
+            float c[kB], z[kB];
+#pragma unroll
+            for (int k = 0; k < kB; ++k) {
+                c[k] = cost(r + k);
+                z[k] = noise[((size_t)(r + k) * B + b) * T * D + rem];
+            }
+#pragma unroll
+            for (int k = 0; k < kB; ++k) acc += z[k] * (expf(-h * (c[k] - mn) / denom) / sum);
+        }
+        for (; r < R; ++r) {
             const float p = expf(-h * (cost(r) - mn) / denom) / sum;
             acc += noise[((size_t)r * B + b) * T * D + rem] * p;
         }
