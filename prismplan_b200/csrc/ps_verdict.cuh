@@ -562,7 +562,7 @@ __device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const floa
 // thousand configurations is latency-bound: one lane per configuration left
 // 3 warps per SM for the same shared memory (16,384 CHOMP waypoints: 49.6 ->
 // 26.5 us). The edge self pass keeps lane_self_hit: its windows of samples
-// ran slower with groups (104.7 -> 123.9 us).
+// ran slower with groups of 2 or 4 lanes (107 -> 135 and 124 us).
 constexpr int kSelfSub = 4;
 constexpr int kSelfBlock = kSelfThreads * kSelfSub;   // threads of a self-check block
 
