@@ -557,11 +557,12 @@ __device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const floa
 // group). Every lane of the group walks the FK and stores its share of the
 // sphere positions (spheres u, u + kSelfSub, ... of each joint); the group's
 // lanes then split the approximate pairs and, per joint pair that passes its
-// bound test, the runs, with a group ballot after each round (the verdict is
-// an OR, so the split changes the work, not the result). The check of a few
+// bound test, the runs, each lane to its own first hit, with one group ballot
+// per phase (the verdict is an OR, so the split changes the work, not the
+// result). The check of a few
 // thousand configurations is latency-bound: one lane per configuration left
 // 3 warps per SM for the same shared memory (16,384 CHOMP waypoints: 49.6 ->
-// 26.5 us). The edge self pass keeps lane_self_hit: its windows of samples
+// 26.5 us with a ballot after every round, 24.0 us with one per phase). The edge self pass keeps lane_self_hit: its windows of samples
 // ran slower with groups of 2 or 4 lanes (107 -> 135 and 124 us).
 constexpr int kSelfSub = 4;
 constexpr int kSelfBlock = kSelfThreads * kSelfSub;   // threads of a self-check block
@@ -616,30 +617,25 @@ __device__ bool group_self_hit(const ModelSmem& M, const ModelDev& md, const flo
     }
     __syncwarp(gmask);   // the group's positions are written
     auto at = [&](const float* a, int k, int c) { return a[(k * 3 + c) * kSlots + slot]; };
+    // each lane runs its share to its own first hit; the group ballots once
+    // per phase (the verdict is an OR, so a lane's early stop changes nothing)
     bool need = false;
-    for (int k0 = 0; k0 < M.H->n_apx_self_pairs; k0 += kSelfSub) {
-        const int k = k0 + u;
-        bool h = false;
-        if (k < M.H->n_apx_self_pairs) {
-            const uint32_t pr = __ldg(md.apx_self_pairs + k);
-            const int i = pr & 0xffff, j = pr >> 16;
-            st.v[ST_SELF] += 1;
-            h = ref_self_hit(at(apos, i, 0), at(apos, i, 1), at(apos, i, 2), M.A[i].w, at(apos, j, 0),
-                             at(apos, j, 1), at(apos, j, 2), M.A[j].w);
-        }
-        if (__ballot_sync(gmask, h)) {
-            need = true;
-            break;
-        }
+    for (int k = u; k < M.H->n_apx_self_pairs && !need; k += kSelfSub) {
+        const uint32_t pr = __ldg(md.apx_self_pairs + k);
+        const int i = pr & 0xffff, j = pr >> 16;
+        st.v[ST_SELF] += 1;
+        need = ref_self_hit(at(apos, i, 0), at(apos, i, 1), at(apos, i, 2), M.A[i].w, at(apos, j, 0), at(apos, j, 1),
+                            at(apos, j, 2), M.A[j].w);
     }
-    if (!need) return false;
+    if (!__ballot_sync(gmask, need)) return false;
+    bool hit = false;
     // joint pairs (a, q), nearest in DFS order first: a pair whose bound
     // spheres are apart (|c_a - c_q| >= R_a + R_q plus the guard band) holds
     // no pair that can pass the float test, so its runs are skipped
-    for (int jp = 0; jp < md.n_sjp; ++jp) {
+    for (int jp = 0; jp < md.n_sjp && !hit; ++jp) {
         const uint4 e = __ldg(md.sjp + jp);
         const int a = (int)(e.x & 0xffffu), qj = (int)(e.x >> 16);
-        {   // the same test on every lane of the group: uniform
+        {
             const float ax = at(cpos, a, 0), ay = at(cpos, a, 1), az = at(cpos, a, 2);
             const float bx = at(cpos, qj, 0), by = at(cpos, qj, 1), bz = at(cpos, qj, 2);
             const float dx = ax - bx, dy = ay - by, dz = az - bz;
@@ -652,31 +648,25 @@ __device__ bool group_self_hit(const ModelSmem& M, const ModelDev& md, const flo
         }
         const float4 bq = M.J[qj].bound;
         const float cx = at(cpos, qj, 0), cy = at(cpos, qj, 1), cz = at(cpos, qj, 2);
-        for (int r0 = (int)e.y; r0 < (int)e.z; r0 += kSelfSub) {
-            const int r = r0 + u;
-            bool h = false;
-            if (r < (int)e.z) {
-                const uint2 run = __ldg(md.sruns + r);
-                const int i = run.x & 0x1ff, len = run.x >> 14;
-                const float px = at(pos, i, 0), py = at(pos, i, 1), pz = at(pos, i, 2), ri = M.S[i].w;
-                const float dx = px - cx, dy = py - cy, dz = pz - cz;
-                const float S = fmaxf(fmaxf(fabsf(px), fmaxf(fabsf(py), fabsf(pz))),
-                                      fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))));
-                float lim = ri + bq.w;
-                lim += 4.0f * (S + lim + 1.0f) * PS_GUARD_K;
+        for (int r = (int)e.y + u; r < (int)e.z && !hit; r += kSelfSub) {
+            const uint2 run = __ldg(md.sruns + r);
+            const int i = run.x & 0x1ff, len = run.x >> 14;
+            const float px = at(pos, i, 0), py = at(pos, i, 1), pz = at(pos, i, 2), ri = M.S[i].w;
+            const float dx = px - cx, dy = py - cy, dz = pz - cz;
+            const float S = fmaxf(fmaxf(fabsf(px), fmaxf(fabsf(py), fabsf(pz))),
+                                  fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))));
+            float lim = ri + bq.w;
+            lim += 4.0f * (S + lim + 1.0f) * PS_GUARD_K;
+            st.v[ST_SELF] += 1;
+            if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) >= lim * lim * (1.0f + 1.0e-6f)) continue;   // no pair can hit
+            for (int k = 0; k < len && !hit; ++k) {
+                const int j = (int)run.y + k;
                 st.v[ST_SELF] += 1;
-                if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) < lim * lim * (1.0f + 1.0e-6f)) {   // else no pair can hit
-                    for (int k = 0; k < len && !h; ++k) {
-                        const int j = (int)run.y + k;
-                        st.v[ST_SELF] += 1;
-                        h = ref_self_hit(px, py, pz, ri, at(pos, j, 0), at(pos, j, 1), at(pos, j, 2), M.S[j].w);
-                    }
-                }
+                hit = ref_self_hit(px, py, pz, ri, at(pos, j, 0), at(pos, j, 1), at(pos, j, 2), M.S[j].w);
             }
-            if (__ballot_sync(gmask, h)) return true;
         }
     }
-    return false;
+    return __ballot_sync(gmask, hit) != 0;
 }
 
 // Shared memory of a self-check block (kSelfThreads configuration slots): model
