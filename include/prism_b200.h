@@ -273,7 +273,7 @@ int ps_check_edges(const ps_model* model, const ps_scene_view* scene,
    Same arguments, verdicts and outputs as ps_check_edges minus the
    workspace. Limits and sharing:
      - n_edges <= PS_EDGES_STATIC_MAX (65536); larger batches return PS_EINVAL.
-       The scratch array (about 1 MiB) is a file-scope __device__ array, held
+       The scratch array (about 1.5 MiB) is a file-scope __device__ array, held
        by every GPU that loads the library until the process exits.
      - The first call on each device looks up the array's device address
        (cudaGetSymbolAddress) with that device current; make that first call

@@ -461,7 +461,7 @@ namespace {
 struct LaunchPlan {
     int mode = 0;
     void (*qk)(ModelDev, ps_scene_view, ps_edge_params, const float*, const float*, int, EdgeWs*, const int*, int*,
-               int*, int*, unsigned long long*, int, const int*) = nullptr;
+               int*, int*, unsigned long long*, int, const int*, const int*) = nullptr;
     void (*wk)(ModelDev, ps_scene_view, ps_cost_params, const Counts*, const float*, float*, float*, int) = nullptr;
     void (*work)(ModelDev, ps_scene_view, ps_edge_params, ps_cost_params, const Counts*, const float*, const float*,
                  EdgeWs*, const int*, int*, int*, int*, const float*, float*, float*, int, int, int) = nullptr;
@@ -612,9 +612,9 @@ void record_graph(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep
                                                                           b->lim.max_edges, b->d_hdr, b->d_G,
                                                                           b->d_bad, nullptr, n_dev, PrepArgs{});
         L.qk<<<L.qgrid, kEdgeThreads, L.qsmem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to, b->lim.max_edges, b->d_hdr,
-                                                    b->d_G, b->d_bad, b->d_clr, b->d_done, nullptr, 0, n_dev);
+                                                    b->d_G, b->d_bad, b->d_clr, b->d_done, nullptr, 0, n_dev, nullptr);
         L.qk<<<L.qgrid, kEdgeThreads, L.qsmem, s0>>>(m->dev, *sv, *ep, b->d_from, b->d_to, b->lim.max_edges, b->d_hdr,
-                                                    b->d_G, b->d_bad, b->d_clr, b->d_done, nullptr, 1, n_dev);
+                                                    b->d_G, b->d_bad, b->d_clr, b->d_done, nullptr, 1, n_dev, nullptr);
         if (ep->check_self)
             edges_self_kernel<<<L.sgrid, kSelfThreads, L.ssmem, s0>>>(m->dev, *ep, b->d_from, b->d_to, b->d_given,
                                                                       b->lim.max_edges, b->d_G, b->d_bad, nullptr,

@@ -26,8 +26,10 @@ struct EdgeWs {                         // header of the persistent workspace (6
     int self_edges;                     // edges with at least one sample
     int self_next;                      // next window of the self pass
     int wp_next;                        // next waypoint group (the batch's work-queue kernel)
-    int pad[3];
+    int n_long;                         // edges with more than one chunk round (the long list)
+    int pad[2];
 };
+static_assert(sizeof(EdgeWs) == 64, "the workspace header is 64 B");
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -573,10 +575,13 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode ? 6 : 3) edges_plain_kerne
 // of this thread: sample count G, length, cleared per-edge state, and the
 // header's maxima and counts (one atomic per warp). The time budget starts
 // here, when the call's first kernel runs. Every thread of the grid calls it.
+// With lst, the edges that have more than one chunk round are also appended
+// to lst (in any order; hdr->n_long counts them), so that the queue's rounds
+// >= 1 visit only those edges instead of every edge.
 __device__ __forceinline__ void prep_edges(const ps_edge_params& P, const float* __restrict__ from,
                                            const float* __restrict__ to, const int* __restrict__ given,
                                            int n_edges, int D, EdgeWs* hdr, int* G_out, float* len_out, int* bad,
-                                           int* clr, int* done) {
+                                           int* clr, int* done, int* lst) {
     if (blockIdx.x == 0 && threadIdx.x == 0)
         hdr->deadline = P.time_budget_ms > 0.0f
                             ? global_ns() + (unsigned long long)((double)P.time_budget_ms * 1.0e6) + 1ull
@@ -593,9 +598,19 @@ __device__ __forceinline__ void prep_edges(const ps_edge_params& P, const float*
         bad[e] = 0;
         clr[e] = ordered_float(FLT_MAX);
         done[e] = 0;
-        local_max = max(local_max, ChunkOrder(G).rounds());
+        const int rounds = ChunkOrder(G).rounds();
+        local_max = max(local_max, rounds);
         local_ns += (unsigned long long)(G + ((G % 16) != 0 ? 1 : 0));
         local_ne += G > 0;
+        if (lst) {   // one atomic per group of converged lanes
+            const unsigned am = __activemask();
+            const unsigned lb = __ballot_sync(am, rounds > 1);
+            const int lane = threadIdx.x & 31, leader = __ffs(am) - 1;
+            int base = 0;
+            if (lane == leader && lb) base = atomicAdd(&hdr->n_long, __popc(lb));
+            base = __shfl_sync(am, base, leader);
+            if (rounds > 1) lst[base + __popc(lb & ((1u << lane) - 1u))] = e;
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -612,9 +627,10 @@ __device__ __forceinline__ void prep_edges(const ps_edge_params& P, const float*
 
 __global__ void edges_prep_kernel(ps_edge_params P, const float* __restrict__ from, const float* __restrict__ to,
                                   const int* __restrict__ given, int n_edges, int D, EdgeWs* hdr, int* G_out,
-                                  float* len_out, int* bad, int* clr, int* done, const int* n_dev = nullptr) {
+                                  float* len_out, int* bad, int* clr, int* done, const int* n_dev = nullptr,
+                                  int* lst = nullptr) {
     if (n_dev) n_edges = *n_dev;
-    prep_edges(P, from, to, given, n_edges, D, hdr, G_out, len_out, bad, clr, done);
+    prep_edges(P, from, to, given, n_edges, D, hdr, G_out, len_out, bad, clr, done, lst);
 }
 
 // ---------------------------------------------------------------------------
@@ -754,6 +770,7 @@ struct PrepArgs {
     float* len;
     int* clr;
     int* done;
+    int* lst;   // the long list, or nullptr
 };
 
 template <bool kStats, bool kPrep>
@@ -768,7 +785,7 @@ __global__ void __launch_bounds__(kProbeThreads, 4) edges_probe_kernel(ModelDev 
     if (n_edges <= 0) return;
     if (kPrep) {
         const int D = reinterpret_cast<const BlobHeader*>(md.blob)->n_dof;
-        prep_edges(P, from, to, pa.given, n_edges, D, hdr, Gs, pa.len, bad, pa.clr, pa.done);
+        prep_edges(P, from, to, pa.given, n_edges, D, hdr, Gs, pa.len, bad, pa.clr, pa.done, pa.lst);
     }
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar;
@@ -856,7 +873,8 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode == 1 ? 5 : (kMode ? 6 : 3)
                                                                   const float* __restrict__ to, int n_edges,
                                                                   EdgeWs* hdr, const int* __restrict__ Gs, int* bad,
                                                                   int* clr, int* done, unsigned long long* stats,
-                                                                  int pass, const int* n_dev = nullptr) {
+                                                                  int pass, const int* n_dev = nullptr,
+                                                                  const int* __restrict__ lst = nullptr) {
     if (n_dev) n_edges = *n_dev;
     // Rounds of this launch. With many edges per resident warp (>= 8) one
     // launch (pass 0) runs every round and pass 1 returns at once. With fewer,
@@ -867,8 +885,15 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode == 1 ? 5 : (kMode ? 6 : 3)
     const bool split = (long long)n_edges < 8ll * gridDim.x * kWarps;
     const int r_lo = pass == 0 ? 0 : (split ? 1 : max_rounds);
     const int r_hi = pass == 0 ? (split ? min(max_rounds, 1) : max_rounds) : max_rounds;
-    const long long rounds = max(r_hi - r_lo, 0);
-    const long long total = rounds * (long long)n_edges;   // chunk-major item space
+    // Chunk-major item space. With the long list (lst): round 0 of every edge
+    // (when this pass runs round 0), then rounds k_lo .. r_hi - 1 of the listed
+    // edges only, since an edge with one round has nothing after round 0.
+    // Without it: rounds r_lo .. r_hi - 1 of every edge.
+    const long long n_long = lst ? (long long)*((volatile int*)&hdr->n_long) : (long long)n_edges;
+    const long long items0 = (lst && r_lo == 0 && r_hi >= 1) ? (long long)n_edges : 0ll;
+    const int k_lo = lst ? max(r_lo, 1) : r_lo;
+    const long long itemsL = r_hi > k_lo ? (long long)(r_hi - k_lo) * n_long : 0ll;
+    const long long total = items0 + itemsL;
     if (total == 0) return;   // uniform over the grid: nothing staged yet
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar;
@@ -919,14 +944,22 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode == 1 ? 5 : (kMode ? 6 : 3)
         int e = -1, k = 0, G = 0;
         bool live = false;
         if (lane < grab && item < total) {
-            if (total < (1ll << 31)) {   // 32-bit division in the common case
-                k = (int)((unsigned)item / (unsigned)n_edges);
-                e = (int)((unsigned)item - (unsigned)k * (unsigned)n_edges);
+            if (item < items0) {
+                k = 0;
+                e = (int)item;
             } else {
-                k = (int)(item / n_edges);
-                e = (int)(item - (long long)k * n_edges);
+                const long long i2 = item - items0;
+                int idx;
+                if (i2 < (1ll << 31)) {   // 32-bit division in the common case
+                    k = (int)((unsigned)i2 / (unsigned)n_long);
+                    idx = (int)((unsigned)i2 - (unsigned)k * (unsigned)n_long);
+                } else {
+                    k = (int)(i2 / n_long);
+                    idx = (int)(i2 - (long long)k * n_long);
+                }
+                k += k_lo;
+                e = lst ? __ldg(lst + idx) : idx;
             }
-            k += r_lo;
             G = __ldg(Gs + e);
             const ChunkOrder ord(G);
             if (k < ord.rounds()) {

@@ -70,16 +70,17 @@ extern "C" int ps_check_edges_plain(const ps_model* m, const ps_scene_view* scen
 
 extern "C" size_t ps_edges_workspace_bytes(int n_edges) {
     const size_t n = (size_t)std::max(n_edges, 1);
-    return align256(sizeof(EdgeWs)) + 5 * align256(n * 4);
+    return align256(sizeof(EdgeWs)) + 6 * align256(n * 4);
 }
 
 namespace {
 
 // Workspace layout: header, then per-edge G, length, retire flag,
-// ordered-int clearance and completed-chunk count (4 B each).
+// ordered-int clearance, completed-chunk count and the long list (the edges
+// with more than one chunk round), 4 B each.
 struct EdgeBufs {
     EdgeWs* hdr;
-    int *G, *bad, *clr, *done;
+    int *G, *bad, *clr, *done, *lst;
     float* len;
 };
 
@@ -94,6 +95,7 @@ EdgeBufs carve_workspace(void* ws, int n_edges) {
     b.bad = reinterpret_cast<int*>(p + 2 * seg);
     b.clr = reinterpret_cast<int*>(p + 3 * seg);
     b.done = reinterpret_cast<int*>(p + 4 * seg);
+    b.lst = reinterpret_cast<int*>(p + 5 * seg);
     return b;
 }
 
@@ -115,24 +117,30 @@ int run_persistent(const ps_model* m, const ps_scene_view* scene, const float* f
     per_sm = std::max(per_sm, 1);
     if (P->queue_blocks_per_sm > 0) per_sm = std::min(per_sm, P->queue_blocks_per_sm);
     const int qgrid = std::max(1, sm_count() * per_sm);
+    // With few edges per resident warp the queue runs round 0 in a pass of its
+    // own; the second pass then visits only the edges listed as having more
+    // rounds (a CHOMP loop's 16 K short segments: 34.7 -> 29.9 ms per call).
+    // With many, one pass runs every round over every edge, as before.
+    const bool split = (long long)n_edges < 8ll * qgrid * kEdgeThreads / 32;   // the kernel's own split rule
+    int* lst = split ? b.lst : nullptr;
     ProbePlan probe;
     if (int rc = plan_probe(m, scene, mode, g_stats != nullptr, 1.0f, n_edges, P->probe, probe)) return rc;
     if (!probe.kp) {   // with the probe, its launch also prepares the edges
         const int pgrid = std::max(1, std::min((n_edges + 255) / 256, sm_count() * 4));
         edges_prep_kernel<<<pgrid, 256, 0, s>>>(*P, from, to, samples_per_edge, n_edges, D, b.hdr, b.G, b.len, b.bad,
-                                                b.clr, b.done);
+                                                b.clr, b.done, nullptr, lst);
         PS_TRY_CUDA(cudaGetLastError());
     }
     mark_start(s);
     if (probe.kp)
         probe.kp<<<probe.grid, kProbeThreads, probe.smem, s>>>(m->dev, *scene, *P, from, to, n_edges, b.hdr, b.G,
                                                                 b.bad, g_stats, nullptr,
-                                                                PrepArgs{samples_per_edge, b.len, b.clr, b.done});
+                                                                PrepArgs{samples_per_edge, b.len, b.clr, b.done, lst});
     qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, b.hdr, b.G, b.bad, b.clr, b.done,
-                                         g_stats, 0, nullptr);
-    if ((long long)n_edges < 8ll * qgrid * kEdgeThreads / 32)   // the kernel's own split rule
+                                         g_stats, 0, nullptr, lst);
+    if (split)
         qk<<<qgrid, kEdgeThreads, smem, s>>>(m->dev, *scene, *P, from, to, n_edges, b.hdr, b.G, b.bad, b.clr, b.done,
-                                             g_stats, 1, nullptr);
+                                             g_stats, 1, nullptr, lst);
     mark_stop(s);
     PS_TRY_CUDA(cudaGetLastError());
     if (int rc = launch_edges_self(m, P, from, to, samples_per_edge, n_edges, b.G, b.bad, nullptr, nullptr, b.hdr,
@@ -182,7 +190,7 @@ extern "C" int ps_check_edges(const ps_model* m, const ps_scene_view* scene, con
 namespace {
 
 constexpr size_t kStaticWsBytes =
-    ((sizeof(EdgeWs) + 255) & ~size_t(255)) + 5 * (((size_t)PS_EDGES_STATIC_MAX * 4 + 255) & ~size_t(255));
+    ((sizeof(EdgeWs) + 255) & ~size_t(255)) + 6 * (((size_t)PS_EDGES_STATIC_MAX * 4 + 255) & ~size_t(255));
 
 static __device__ __align__(256) unsigned char g_edges_static_ws[kStaticWsBytes];
 
