@@ -310,8 +310,8 @@ __global__ void __launch_bounds__(kSelfBlock, 3) self_check_kernel(ModelDev md, 
     if (!stage_model(md, blob, &mbar)) return configs_fail_closed(n, kSelfBlock, hit_out, nullptr);
     const ModelSmem M = model_view(blob);
     const int D = M.H->n_dof, NS = M.H->n_spheres, NA = M.H->n_approx, NJ = M.H->n_joints;
-    const SelfSmem sm = carve_self<kSelfThreads>(smem + md.bytes_core, NS, NA, NJ);
-    float* qtile = sm.cpos + (size_t)NJ * 3 * kSelfThreads;
+    const SelfSmem sm = carve_self<kSelfThreads>(smem + md.bytes_core, NS, NA, NJ, md.bound_from_apx != 0);
+    float* qtile = sm.end;
     LaneStats st;
     st.zero();
     const int slot = threadIdx.x / kSelfSub, u = threadIdx.x % kSelfSub;

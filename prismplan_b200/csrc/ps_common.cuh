@@ -62,6 +62,8 @@ struct ModelDev {
     int n_sruns;
     const uint4* sjp;              // device, joint pairs: (a | q << 16, first run, end run, 0)
     int n_sjp;
+    int bound_from_apx;            // 1: every joint with exact spheres has an approximate sphere on the same
+                                   // chain, whose centre is the joint's bound centre (the self check reads it there)
     const float* lower;            // device
     const float* upper;            // device
     int* status;                   // device error latch

@@ -1038,9 +1038,9 @@ __global__ void __launch_bounds__(kSelfThreads) edges_self_kernel(ModelDev md, p
     }
     const ModelSmem M = model_view(smem);
     const int D = M.H->n_dof, NS = M.H->n_spheres, NA = M.H->n_approx, NJ = M.H->n_joints;
-    const SelfSmem sm = carve_self<kSelfThreads>(smem + md.bytes_core, NS, NA, NJ);
+    const SelfSmem sm = carve_self<kSelfThreads>(smem + md.bytes_core, NS, NA, NJ, md.bound_from_apx != 0);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    float* qc = sm.cpos + (size_t)NJ * 3 * kSelfThreads + tid * D;
+    float* qc = sm.end + tid * D;
     const bool persistent = bad != nullptr;
     const unsigned long long deadline = hdr ? *((volatile unsigned long long*)&hdr->deadline) : 0ull;
     LaneStats st;

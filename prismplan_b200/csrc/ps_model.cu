@@ -308,6 +308,12 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
 
     bool shares = std::memcmp(aft, d->fixed_transforms, sizeof(float) * 16 * nj) == 0;
     for (int i = 0; i < nj && shares; ++i) shares = atypes[i] == d->joint_types[i];
+    // The bound centre of a joint with an approximate sphere is that sphere's
+    // centre (fill_joints below); on a shared chain its world position is the
+    // approximate sphere's, bit for bit.
+    bool bound_from_apx = shares;
+    for (int p = 0; p < nj && bound_from_apx; ++p)
+        if (send[p] > sbeg[p] && aend[p] <= abeg[p]) bound_from_apx = false;
 
     // ---- blob layout ----
     BlobHeader h{};
@@ -439,6 +445,7 @@ extern "C" int ps_model_create(const ps_model_desc* d, ps_model** out) {
     m->dev.n_sruns = (int)(sruns.size() / 2);
     m->dev.sjp = reinterpret_cast<const uint4*>(base + off_sjp);
     m->dev.n_sjp = (int)(sjp.size() / 4);
+    m->dev.bound_from_apx = bound_from_apx ? 1 : 0;
     m->dev.lower = reinterpret_cast<const float*>(base + off_lower);
     m->dev.upper = reinterpret_cast<const float*>(base + off_upper);
     m->dev.status = reinterpret_cast<int*>(base + off_status);

@@ -435,16 +435,21 @@ __device__ __forceinline__ void fk_step(const JointRec& jr, int p, const float* 
 // ---------------------------------------------------------------------------
 constexpr int kSelfThreads = 64;
 
+// Bound centres are staged only when some joint's cannot be read off its
+// first approximate sphere (ModelDev::bound_from_apx); that saves 3 floats per
+// joint and slot, which on the Panda lets a fourth self-check block fit on an SM.
 struct SelfSmem {
-    float *pos, *apos, *cpos;   // [n_spheres*3][L], [n_approx*3][L], [n_joints*3][L]
+    float *pos, *apos, *cpos;   // [n_spheres*3][L], [n_approx*3][L], [n_joints*3][L] (or none)
+    float* end;                 // first float after them
 };
 
 template <int kLanes>
-__device__ __forceinline__ SelfSmem carve_self(unsigned char* base, int NS, int NA, int NJ) {
+__device__ __forceinline__ SelfSmem carve_self(unsigned char* base, int NS, int NA, int NJ, bool bound_from_apx) {
     SelfSmem s;
     s.pos = reinterpret_cast<float*>(base);
     s.apos = s.pos + (size_t)NS * 3 * kLanes;
     s.cpos = s.apos + (size_t)NA * 3 * kLanes;
+    s.end = s.cpos + (bound_from_apx ? 0 : (size_t)NJ * 3 * kLanes);
     return s;
 }
 
@@ -473,7 +478,7 @@ __device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const floa
             sphere_world(T, s.x, s.y, s.z, px, py, pz);
             put3(pos, k, kLanes, lane, px, py, pz);
         }
-        if (jr.bound.w >= 0.0f) {
+        if (jr.bound.w >= 0.0f && !md.bound_from_apx) {
             float px, py, pz;
             sphere_world(T, jr.bound.x, jr.bound.y, jr.bound.z, px, py, pz);
             put3(cpos, p, kLanes, lane, px, py, pz);
@@ -502,6 +507,8 @@ __device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const floa
         }
     }
     auto at = [&](const float* a, int k, int c) { return a[(k * 3 + c) * kLanes + lane]; };
+    // a joint's world bound centre (its first approximate sphere's when the model says so)
+    auto bc = [&](int p, int c) { return md.bound_from_apx ? at(apos, M.J[p].apx_beg, c) : at(cpos, p, c); };
     bool need = false;
     for (int k = 0; k < M.H->n_apx_self_pairs && !need; ++k) {
         const uint32_t pr = __ldg(md.apx_self_pairs + k);
@@ -518,8 +525,8 @@ __device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const floa
         const uint4 e = __ldg(md.sjp + jp);
         const int a = (int)(e.x & 0xffffu), qj = (int)(e.x >> 16);
         {
-            const float ax = at(cpos, a, 0), ay = at(cpos, a, 1), az = at(cpos, a, 2);
-            const float bx = at(cpos, qj, 0), by = at(cpos, qj, 1), bz = at(cpos, qj, 2);
+            const float ax = bc(a, 0), ay = bc(a, 1), az = bc(a, 2);
+            const float bx = bc(qj, 0), by = bc(qj, 1), bz = bc(qj, 2);
             const float dx = ax - bx, dy = ay - by, dz = az - bz;
             const float S = fmaxf(fmaxf(fabsf(ax), fmaxf(fabsf(ay), fabsf(az))),
                                   fmaxf(fabsf(bx), fmaxf(fabsf(by), fabsf(bz))));
@@ -529,7 +536,7 @@ __device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const floa
             if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) >= lim * lim * (1.0f + 1.0e-6f)) continue;
         }
         const float4 bq = M.J[qj].bound;
-        const float cx = at(cpos, qj, 0), cy = at(cpos, qj, 1), cz = at(cpos, qj, 2);
+        const float cx = bc(qj, 0), cy = bc(qj, 1), cz = bc(qj, 2);
         for (int r = (int)e.y; r < (int)e.z; ++r) {
             const uint2 run = __ldg(md.sruns + r);
             const int i = run.x & 0x1ff, len = run.x >> 14;
@@ -587,7 +594,7 @@ __device__ bool group_self_hit(const ModelSmem& M, const ModelDev& md, const flo
             sphere_world(T, s.x, s.y, s.z, px, py, pz);
             put3(pos, k, kSlots, slot, px, py, pz);
         }
-        if (u == 0 && jr.bound.w >= 0.0f) {
+        if (u == 0 && jr.bound.w >= 0.0f && !md.bound_from_apx) {
             float px, py, pz;
             sphere_world(T, jr.bound.x, jr.bound.y, jr.bound.z, px, py, pz);
             put3(cpos, p, kSlots, slot, px, py, pz);
@@ -617,6 +624,8 @@ __device__ bool group_self_hit(const ModelSmem& M, const ModelDev& md, const flo
     }
     __syncwarp(gmask);   // the group's positions are written
     auto at = [&](const float* a, int k, int c) { return a[(k * 3 + c) * kSlots + slot]; };
+    // a joint's world bound centre (its first approximate sphere's when the model says so)
+    auto bc = [&](int p, int c) { return md.bound_from_apx ? at(apos, M.J[p].apx_beg, c) : at(cpos, p, c); };
     // each lane runs its share to its own first hit; the group ballots once
     // per phase (the verdict is an OR, so a lane's early stop changes nothing)
     bool need = false;
@@ -636,8 +645,8 @@ __device__ bool group_self_hit(const ModelSmem& M, const ModelDev& md, const flo
         const uint4 e = __ldg(md.sjp + jp);
         const int a = (int)(e.x & 0xffffu), qj = (int)(e.x >> 16);
         {
-            const float ax = at(cpos, a, 0), ay = at(cpos, a, 1), az = at(cpos, a, 2);
-            const float bx = at(cpos, qj, 0), by = at(cpos, qj, 1), bz = at(cpos, qj, 2);
+            const float ax = bc(a, 0), ay = bc(a, 1), az = bc(a, 2);
+            const float bx = bc(qj, 0), by = bc(qj, 1), bz = bc(qj, 2);
             const float dx = ax - bx, dy = ay - by, dz = az - bz;
             const float S = fmaxf(fmaxf(fabsf(ax), fmaxf(fabsf(ay), fabsf(az))),
                                   fmaxf(fabsf(bx), fmaxf(fabsf(by), fabsf(bz))));
@@ -647,7 +656,7 @@ __device__ bool group_self_hit(const ModelSmem& M, const ModelDev& md, const flo
             if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) >= lim * lim * (1.0f + 1.0e-6f)) continue;
         }
         const float4 bq = M.J[qj].bound;
-        const float cx = at(cpos, qj, 0), cy = at(cpos, qj, 1), cz = at(cpos, qj, 2);
+        const float cx = bc(qj, 0), cy = bc(qj, 1), cz = bc(qj, 2);
         for (int r = (int)e.y + u; r < (int)e.z && !hit; r += kSelfSub) {
             const uint2 run = __ldg(md.sruns + r);
             const int i = run.x & 0x1ff, len = run.x >> 14;
@@ -672,8 +681,9 @@ __device__ bool group_self_hit(const ModelSmem& M, const ModelDev& md, const flo
 // Shared memory of a self-check block (kSelfThreads configuration slots): model
 // core, sphere and bound positions and a tile of configurations.
 inline size_t self_smem_bytes(const ps_model* m) {
+    const int nc = m->dev.bound_from_apx ? 0 : m->info.n_joints;
     return (size_t)m->dev.bytes_core +
-           (size_t)(m->info.n_spheres + m->info.n_approx_spheres + m->info.n_joints) * 3 * kSelfThreads * 4 +
+           (size_t)(m->info.n_spheres + m->info.n_approx_spheres + nc) * 3 * kSelfThreads * 4 +
            (size_t)kSelfThreads * m->info.n_dof * 4;
 }
 
