@@ -325,8 +325,6 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
         if (p == 0) {
             affine_identity(T);
         } else {
-            Affine Pf;
-            lane_frame(ws.fr, jr.parent_pos, slot, Pf);
             const int dof = jr.dof;
             float qi = 0.0f, sn = 0.0f, cs = 1.0f;   // sincosf(0) for a joint without a DoF
             if (dof >= 0) {
@@ -334,7 +332,16 @@ __device__ float lane_cost(const ModelSmem& M, const ModelDev& md, const SceneSm
                 sn = ws.sc[(2 * dof) * kCostSlots + slot];
                 cs = ws.sc[(2 * dof + 1) * kCostSlots + slot];
             }
-            joint_compose_sc(jr, qi, sn, cs, Pf, T);
+            if (jr.parent_pos == p - 1) {
+                // the parent is the previous joint, whose frame is still in T (the
+                // compose reads each parent row before writing it): no shared-memory
+                // round trip on the chain's critical path
+                joint_compose_sc(jr, qi, sn, cs, T, T);
+            } else {
+                Affine Pf;
+                lane_frame(ws.fr, jr.parent_pos, slot, Pf);
+                joint_compose_sc(jr, qi, sn, cs, Pf, T);
+            }
             if (u == 0) {
                 float* b = ws.fr + (size_t)(p - 1) * 12 * kCostSlots + slot;
 #pragma unroll
