@@ -114,3 +114,50 @@ def test_self_pass_respects_time_budget(case):
     assert api.edges_status(ws) == _lib.PS_ETIMEOUT
     v = v.cpu().numpy()
     assert not np.any((v == 1) & (rv == 0))   # never free when not shown free
+
+
+def _without_last_approx_sphere(asset):
+    """The asset with its last approximate sphere removed (and the approximate
+    self ranges that name it trimmed): that joint keeps its exact spheres but
+    has no approximate sphere, so its bound centre cannot be read off one."""
+    a = {k: (list(v) if isinstance(v, (list, tuple, np.ndarray)) else v) for k, v in asset.items()}
+    na = len(a["approx_sphere_to_joint"])
+    last = na - 1
+    a["approx_spheres_flat"] = list(a["approx_spheres_flat"][: 4 * last])
+    a["approx_sphere_to_joint"] = list(a["approx_sphere_to_joint"][:last])
+    r = np.asarray(a["approx_self_cc_ranges_flat"], dtype=np.int64).reshape(-1, 3)
+    keep = []
+    for i, s, e in r:
+        e = min(int(e), last - 1)
+        if int(i) != last and int(s) <= e:
+            keep.append((int(i), int(s), e))
+    a["approx_self_cc_ranges_flat"] = [x for t in keep for x in t]
+    return a
+
+
+def test_self_checks_with_staged_bound_centres(case):
+    """The self checks read a joint's bound centre off its first approximate
+    sphere when every joint with exact spheres has one on the shared chain, and
+    stage every bound centre otherwise. This model takes the second layout. The
+    reference's kernels assume one approximate sphere per joint with spheres
+    (their approximate pass indexes by joint), so this model is held to the
+    FP64 oracle: edges with check_self and the configuration self check may
+    differ from it only at contact."""
+    asset, obbs, _, sc, frm, to, G, _ = case
+    a2 = _without_last_approx_sphere(asset)
+    b2 = RobotModelBuilder.from_asset(a2).build()
+    om = oracle.OracleModel(b2, *obbs)
+    rv, _, _, gap_e, _ = om.check_edges(frm, to, G, check_self=True, early_exit=False, want_gap=True)
+    f, t, g = (torch.from_numpy(x).cuda() for x in (frm, to, G))
+    v = api.check_edges(b2, sc, f, t, samples=g, params=api.EdgeEvalParams(check_self=True))[0].cpu().numpy()
+    ef = np.nonzero(v != rv)[0]
+    q = np.concatenate([frm, to])[:2048].astype(np.float32)
+    h, _ = api.check_configs(b2, None, torch.from_numpy(q).cuda(), check_self=True)
+    om0 = oracle.OracleModel(b2, np.zeros((0, 4)), np.zeros((0, 8)))
+    h64, _, gap = om0.check_configs(q, flags=_lib.PS_CHECK_SELF, want_gap=True)
+    flips = np.nonzero(h.cpu().numpy() != h64)[0]
+    print(f"staged bound centres: edges {len(ef)} flips of {len(G)} (distance to contact {gap_e[ef].tolist()}), "
+          f"configurations {len(flips)} of {len(q)} ({gap[flips].tolist()}); edges free {rv.mean():.3f}")
+    assert np.all(gap_e[ef] < 1e-5) and np.all(gap[flips] < 1e-5)
+    assert 0.0 < rv.mean() < 1.0 and h64.mean() > 0.0
+    b2.destroy()
