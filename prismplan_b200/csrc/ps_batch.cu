@@ -505,7 +505,7 @@ int plan_launch(ps_batch* b, const ps_scene_view* sv, const ps_edge_params* ep, 
         L.req_grid_e = std::max(1, std::min(b->lim.max_edge_requests, sms * 8));
         if (ep->check_self) {
             if (int rc = check_self_fits(m)) return rc;
-            L.ssmem = self_smem_bytes(m);
+            L.ssmem = self_lane_smem_bytes(m);
             PS_TRY_CUDA(allow_smem((const void*)edges_self_kernel, L.ssmem));
             int s_per_sm = 0;
             PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s_per_sm, edges_self_kernel, kSelfThreads,

@@ -1008,7 +1008,7 @@ __global__ void __launch_bounds__(kEdgeThreads, kMode == 1 ? 5 : (kMode ? 6 : 3)
 // Persistent mode (bad != nullptr): bad[e] goes from 0 to 1 (self hit) or 2
 // (checked, free); an edge still at 0 after a deadline comes back invalid.
 // Plain mode (valid, cost): a self hit turns a free edge invalid.
-__global__ void __launch_bounds__(kSelfThreads) edges_self_kernel(ModelDev md, ps_edge_params P,
+__global__ void __launch_bounds__(kSelfThreads, 6) edges_self_kernel(ModelDev md, ps_edge_params P,
                                                                   const float* __restrict__ from,
                                                                   const float* __restrict__ to,
                                                                   const int* __restrict__ given, int n_edges,
@@ -1037,8 +1037,8 @@ __global__ void __launch_bounds__(kSelfThreads) edges_self_kernel(ModelDev md, p
         return;
     }
     const ModelSmem M = model_view(smem);
-    const int D = M.H->n_dof, NS = M.H->n_spheres, NA = M.H->n_approx, NJ = M.H->n_joints;
-    const SelfSmem sm = carve_self<kSelfThreads>(smem + md.bytes_core, NS, NA, NJ, md.bound_from_apx != 0);
+    const int D = M.H->n_dof, NA = M.H->n_approx, NJ = M.H->n_joints;
+    const SelfFrames sm = carve_self_frames<kSelfThreads>(smem + md.bytes_core, NA, NJ, md.bound_from_apx != 0);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float* qc = sm.end + tid * D;
     const bool persistent = bad != nullptr;
@@ -1162,7 +1162,7 @@ int launch_edges_self(const ps_model* m, const ps_edge_params* P, const float* f
                       EdgeWs* hdr, const int* n_dev, cudaStream_t s) {
     if (!P->check_self || n_edges <= 0) return PS_OK;
     if (int rc = check_self_fits(m)) return rc;
-    const size_t smem = self_smem_bytes(m);
+    const size_t smem = self_lane_smem_bytes(m);
     PS_TRY_CUDA(allow_smem((const void*)edges_self_kernel, smem));
     int per_sm = 0;
     PS_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edges_self_kernel, kSelfThreads, smem));

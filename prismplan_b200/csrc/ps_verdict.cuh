@@ -459,11 +459,32 @@ __device__ __forceinline__ void put3(float* a, int k, int L, int lane, float x, 
     a[(k * 3 + 2) * L + lane] = z;
 }
 
+// The one-thread check of the edge self pass stages each joint's frame (12
+// floats) instead of each exact sphere's position (3 floats per sphere: 177
+// on the Panda against 96), and transforms a sphere where a joint pair that
+// passes its bound test needs it, with the frame it would have been staged
+// from, so the positions and the verdict are the same bits. Less shared
+// memory per sample lets more samples run per SM.
+struct SelfFrames {
+    float *fr, *apos, *cpos;   // [n_joints*12][L], [n_approx*3][L], [n_joints*3][L] (or none)
+    float* end;                // first float after them
+};
+
 template <int kLanes>
-__device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const float* qc, const SelfSmem& sm, int lane,
+__device__ __forceinline__ SelfFrames carve_self_frames(unsigned char* base, int NA, int NJ, bool bound_from_apx) {
+    SelfFrames s;
+    s.fr = reinterpret_cast<float*>(base);
+    s.apos = s.fr + (size_t)NJ * 12 * kLanes;
+    s.cpos = s.apos + (size_t)NA * 3 * kLanes;
+    s.end = s.cpos + (bound_from_apx ? 0 : (size_t)NJ * 3 * kLanes);
+    return s;
+}
+
+template <int kLanes>
+__device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const float* qc, const SelfFrames& sm, int lane,
                               LaneStats& st) {
     const int NJ = M.H->n_joints;
-    float* pos = sm.pos;
+    float* fr = sm.fr;
     float* apos = sm.apos;
     float* cpos = sm.cpos;
     Affine s0, s1, T;
@@ -472,12 +493,8 @@ __device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const floa
     for (int p = 0; p < NJ; ++p) {
         const JointRec& jr = M.J[p];
         fk_step<true>(jr, p, qc, s0, s1, T);
-        for (int k = jr.sph_beg; k < jr.sph_end; ++k) {
-            const float4 s = M.S[k];
-            float px, py, pz;
-            sphere_world(T, s.x, s.y, s.z, px, py, pz);
-            put3(pos, k, kLanes, lane, px, py, pz);
-        }
+#pragma unroll
+        for (int k = 0; k < 12; ++k) fr[(p * 12 + k) * kLanes + lane] = T.m[k];
         if (jr.bound.w >= 0.0f && !md.bound_from_apx) {
             float px, py, pz;
             sphere_world(T, jr.bound.x, jr.bound.y, jr.bound.z, px, py, pz);
@@ -509,6 +526,10 @@ __device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const floa
     auto at = [&](const float* a, int k, int c) { return a[(k * 3 + c) * kLanes + lane]; };
     // a joint's world bound centre (its first approximate sphere's when the model says so)
     auto bc = [&](int p, int c) { return md.bound_from_apx ? at(apos, M.J[p].apx_beg, c) : at(cpos, p, c); };
+    auto frame = [&](int p, Affine& F) {
+#pragma unroll
+        for (int k = 0; k < 12; ++k) F.m[k] = fr[(p * 12 + k) * kLanes + lane];
+    };
     bool need = false;
     for (int k = 0; k < M.H->n_apx_self_pairs && !need; ++k) {
         const uint32_t pr = __ldg(md.apx_self_pairs + k);
@@ -535,24 +556,31 @@ __device__ bool lane_self_hit(const ModelSmem& M, const ModelDev& md, const floa
             st.v[ST_SELF] += 1;
             if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) >= lim * lim * (1.0f + 1.0e-6f)) continue;
         }
+        Affine Ta, Tq;
+        frame(a, Ta);
+        frame(qj, Tq);
         const float4 bq = M.J[qj].bound;
         const float cx = bc(qj, 0), cy = bc(qj, 1), cz = bc(qj, 2);
         for (int r = (int)e.y; r < (int)e.z; ++r) {
             const uint2 run = __ldg(md.sruns + r);
             const int i = run.x & 0x1ff, len = run.x >> 14;
-            const float px = at(pos, i, 0), py = at(pos, i, 1), pz = at(pos, i, 2), ri = M.S[i].w;
+            const float4 si = M.S[i];
+            float px, py, pz;
+            sphere_world(Ta, si.x, si.y, si.z, px, py, pz);
+            const float ri = si.w;
             const float dx = px - cx, dy = py - cy, dz = pz - cz;
-            const float S =
-                fmaxf(fmaxf(fabsf(px), fmaxf(fabsf(py), fabsf(pz))), fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))));
+            const float S = fmaxf(fmaxf(fabsf(px), fmaxf(fabsf(py), fabsf(pz))), fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))));
             float lim = ri + bq.w;
             lim += 4.0f * (S + lim + 1.0f) * PS_GUARD_K;
             st.v[ST_SELF] += 1;
             if (fmaf(dz, dz, fmaf(dy, dy, dx * dx)) >= lim * lim * (1.0f + 1.0e-6f)) continue;   // no pair can hit
             for (int k = 0; k < len; ++k) {
                 const int j = (int)run.y + k;
+                const float4 sj = M.S[j];
+                float qx, qy, qz;
+                sphere_world(Tq, sj.x, sj.y, sj.z, qx, qy, qz);
                 st.v[ST_SELF] += 1;
-                if (ref_self_hit(px, py, pz, ri, at(pos, j, 0), at(pos, j, 1), at(pos, j, 2), M.S[j].w))
-                    return true;
+                if (ref_self_hit(px, py, pz, ri, qx, qy, qz, sj.w)) return true;
             }
         }
     }
@@ -691,6 +719,16 @@ inline size_t self_smem_bytes(const ps_model* m) {
 // memory: about 280 spheres, approximate spheres and joints together on a
 // B200 (the reference's edge kernel stages at most 125 spheres, 52
 // approximate ones: edge_eval.cuh:83-84).
+// Shared memory of an edge self-pass block (lane_self_hit, kSelfThreads
+// samples): model core, frames, approximate sphere positions, bound centres
+// when they are staged, a tile of configurations.
+inline size_t self_lane_smem_bytes(const ps_model* m) {
+    const int nc = m->dev.bound_from_apx ? 0 : m->info.n_joints;
+    return (size_t)m->dev.bytes_core +
+           (size_t)(12 * m->info.n_joints + 3 * m->info.n_approx_spheres + 3 * nc) * kSelfThreads * 4 +
+           (size_t)kSelfThreads * m->info.n_dof * 4;
+}
+
 inline int check_self_fits(const ps_model* m) {
     const size_t need = self_smem_bytes(m), have = smem_optin();
     if (need <= have) return PS_OK;
