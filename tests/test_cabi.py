@@ -41,6 +41,17 @@ def test_binding_loads_and_reports_version():
     assert lib.ps_edges_workspace_bytes(65536) >= 65536 * 16
 
 
+def test_edges_workspace_layout():
+    """The persistent edge workspace: a 64-B header (in its own 256-B block)
+    and six 4-B per-edge arrays (G, length, retire flag, clearance, completed
+    chunks, the long list), each starting on a 256-B boundary."""
+    lib = _lib.load()
+    up = lambda x: (x + 255) // 256 * 256
+    for n in (1, 7, 1000, 65536):
+        assert lib.ps_edges_workspace_bytes(n) == up(64) + 6 * up(4 * n)
+    assert lib.ps_edges_workspace_bytes(0) == lib.ps_edges_workspace_bytes(1)
+
+
 STRUCTS = {   # ctypes mirror -> C struct of include/prism_b200.h
     "ModelDesc": "ps_model_desc", "ModelInfo": "ps_model_info", "SceneView": "ps_scene_view",
     "EdgeParams": "ps_edge_params", "CostParams": "ps_cost_params", "BatchLimits": "ps_batch_limits",
